@@ -1,0 +1,237 @@
+/*
+ * ua_ssa.h — C-ABI of the B200 SSA (SSTREAM) Newton library (libuassa.so).
+ *
+ * Drop-in boundary for Úa's shallow-shelf hot path.  Each entry point names
+ * the reference MATLAB function it replaces (paths relative to the Úa source
+ * tree).  The MEX gateways under mex/ marshal MATLAB structs into these
+ * plain-pointer calls; Python binds the same symbols with ctypes.
+ *
+ * Conventions
+ *  - All arrays are caller-owned.  Host pointers unless a struct says
+ *    otherwise (ua_fields.location).  The library owns all device memory.
+ *  - Node and element indices follow ua_mesh_desc.index_base (1 for MATLAB).
+ *  - Connectivity is Nele x nod, column-major (MATLAB layout): entry (e,a) is
+ *    connectivity[a*Nele + e].  Coordinates are Nnodes x 2 column-major.
+ *  - Degrees of freedom are ordered as in Úa: [u(1..Nn); v(1..Nn); h(1..Nn)].
+ *  - The tangent is returned on the structural pattern of the mesh (every
+ *    pair of nodes sharing an element), CSR with sorted columns; for the uv
+ *    system CSR == CSC because the pattern is symmetric.  ua_mesh_pattern()
+ *    gives the pattern.  MATLAB's sparse() drops exact zeros; the MEX gateway
+ *    does the same when it builds the mxArray.
+ *  - Status: 0 = OK, negative = error (UA_ERR_*).  ua_last_error() returns a
+ *    message for the last failing call on the calling thread.
+ *  - Thread safety: one handle per thread; calls on one handle are serialised
+ *    on the handle's CUDA stream.
+ */
+#ifndef UA_SSA_H
+#define UA_SSA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UA_OK                 0
+#define UA_ERR_INVALID       -1   /* bad argument / size */
+#define UA_ERR_NAN_INPUT     -2   /* uvMatrixAssembly:NaN, SSTREAM2dNR2.m:42-66 */
+#define UA_ERR_NOT_CONVERGED -3   /* RunInfo.Forward.uvConverged=0 */
+#define UA_ERR_OOM           -4   /* device allocation failed / admission */
+#define UA_ERR_TIMEOUT       -5   /* bounded device wait expired */
+#define UA_ERR_BAD_MESH      -6   /* degenerate element (detJ==0) or bad index */
+#define UA_ERR_CUDA          -7   /* CUDA runtime error */
+#define UA_ERR_KRYLOV        -8   /* Krylov breakdown / iteration cap */
+#define UA_ERR_NO_DEVICE     -9   /* no CUDA device or extension unusable */
+
+/* Precision forms. */
+#define UA_PREC_FP64   0   /* all FP64 (the plain form) */
+#define UA_PREC_MIXED  1   /* FP32 element tangents + FP32 PCG with FP64 reductions */
+
+/* Assembly modes of uvMatrixAssembly (uvMatrixAssemblySSTREAM.m:17-28). */
+#define UA_ASM_R      0   /* CtrlVar.uvMatrixAssembly.Ronly=true */
+#define UA_ASM_RK     1   /* R and K */
+#define UA_ASM_ZERO_R 2   /* CtrlVar.uvAssembly.ZeroFields=true, Ronly */
+
+/* Field location. */
+#define UA_HOST   0
+#define UA_DEVICE 1
+
+typedef struct ua_mesh ua_mesh;   /* opaque device-resident mesh (MUA) */
+
+/* One mesh: MUA.coordinates / MUA.connectivity (CreateMUA.m:31-98). */
+typedef struct ua_mesh_desc {
+    int32_t nnodes;
+    int32_t nele;
+    int32_t nod;                 /* 3 (P1) or 6 (P2) */
+    int32_t index_base;          /* 1 for MATLAB, 0 for C/Python */
+    const double*  coordinates;  /* nnodes x 2, column-major */
+    const int32_t* connectivity; /* nele x nod, column-major */
+} ua_mesh_desc;
+
+/* CtrlVar fields that change hot-path arithmetic (defaults from
+ * Ua2D_DefaultParameters.m; ua_params_default() fills them). */
+typedef struct ua_params {
+    double kH, Hh0;                               /* :2288, :2295 */
+    double SpeedZero, EpsZero, etaZero;           /* :412, :413, :415 */
+    double Czero, Cmin, AGlenmin;                 /* :441, :456-460, :463 */
+    int32_t Picard;                               /* :593 */
+    double NRviscosity;                           /* :594 */
+    int32_t NRitmax, NRitmin;                     /* :597, :600 */
+    double NewtonAcceptRatio;                     /* :601 */
+    double BacktrackingGammaMin;                  /* :604 */
+    int32_t LineSearchAllowedToUseExtrapolation;  /* :603 */
+    double BackTrackBeta;                         /* :616 */
+    int32_t BackTrackMaxIterations;               /* :617 */
+    int32_t BackTrackMaxExtrapolations;           /* :618 */
+    double BackTrackExtrapolationRatio;           /* :619 */
+    double BackTrackMinXfrac;                     /* :620 */
+    int32_t BackTrackMaxFuncSame;                 /* :621 */
+    double BackTrackGuardLower, BackTrackGuardUpper; /* :625-626 */
+    double NLtol;                                 /* BackTracking.m:125-127 */
+    double uvDesiredWorkAndForceTolerances[2];    /* :508 */
+    double uvDesiredWorkOrForceTolerances[2];     /* :509 */
+    double uvExitBackTrackingStepLength;          /* :510 */
+    double uvAcceptableWorkAndForceTolerances[2]; /* :511 */
+    double uvAcceptableWorkOrForceTolerances[2];  /* :512 */
+    int32_t ModifiedNRuvIntervalCriterion;        /* :582 */
+    double ModifiedNRuvReductionCriterion;        /* :583 */
+    /* uvh */
+    double theta, SUPG_beta0, uvh_SUPG_tauMultiplier; /* :377, :376, :555 */
+    int32_t uvh_SUPG_tau;                         /* 0=taus (:551), 1=taut, 2=tau1, 3=tau2 */
+    double uvhDesiredWorkAndForceTolerances[2];   /* :496 */
+    double uvhDesiredWorkOrForceTolerances[2];    /* :498 */
+    double uvhExitBackTrackingStepLength;         /* :502 */
+    double uvhAcceptableWorkAndForceTolerances[2];/* :504 */
+    double uvhAcceptableWorkOrForceTolerances[2]; /* :505 */
+    /* inner Krylov solve (replaces ABfgPreEliminate.m:110 decomposition) */
+    double krylov_rtol;        /* relative residual of the preconditioned solve */
+    int32_t krylov_maxit;
+    int32_t precision;         /* UA_PREC_* */
+    int32_t patch_nodes;       /* assembly patch size (0 = autotune) */
+    int32_t verbose;           /* per-iteration log line to stderr */
+    int32_t profile;           /* 1: time assembly and SpMV launches with CUDA events */
+} ua_params;
+
+/* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */
+typedef struct ua_fields {
+    int32_t location;          /* UA_HOST or UA_DEVICE (device pointers on the handle's device) */
+    const double *h, *S, *B, *rho, *AGlen, *n, *C, *m;
+    double *ub, *vb;           /* in: start / current velocities, out (newton): solution */
+    double rhow, g, alpha;
+    /* uvh only (SSTREAM_TransientImplicit.m): state at t0 and mass balance */
+    const double *h0, *u0, *v0, *as0, *ab0, *as1, *ab1, *dadh;
+    double *h1;                /* in: start thickness, out: solution */
+    double dt;
+} ua_fields;
+
+/* Boundary conditions (BCs2MLC.m, CreateLuv.m).  Index base as the mesh. */
+typedef struct ua_bcs {
+    int32_t n_ufixed; const int32_t* ufixed_node; const double* ufixed_value;
+    int32_t n_vfixed; const int32_t* vfixed_node; const double* vfixed_value;
+    int32_t n_utied;  const int32_t* utied_a; const int32_t* utied_b;
+    int32_t n_vtied;  const int32_t* vtied_a; const int32_t* vtied_b;
+    int32_t n_hfixed; const int32_t* hfixed_node; const double* hfixed_value;
+} ua_bcs;
+
+/* One Newton iteration (the SSTREAM2dNR2.m:386-387 log line). */
+typedef struct ua_newton_iter {
+    int32_t iteration, iarm, krylov_its, direction; /* direction 0=full Newton, 1=backtracked */
+    double gamma, r0, r, rForce, rWork;
+} ua_newton_iter;
+
+/* RunInfo.Forward subset (UaRunInfo.m:42-98) plus timing. */
+typedef struct ua_newton_report {
+    int32_t converged;          /* uvConverged */
+    int32_t iterations;         /* uvIterations */
+    int32_t backtrack_steps;    /* uvBackTrackSteps (last iteration's iarm) */
+    int32_t krylov_its_total;
+    int32_t cauchy_fallbacks;   /* times rLineminUa.m:96 would continue with the M-Cauchy step */
+    int32_t retried;            /* uv.m:107-112 reset-and-retry happened */
+    double r, rForce, rWork;    /* uvResidual (= r) */
+    double assembly_ms, solve_ms, total_ms;  /* host wall clock of the phases */
+    double device_ms;           /* CUDA-event time on the handle's stream, whole call */
+    double kasmK_ms, kasmR_ms, kspmv_ms;     /* summed launch durations (profile=1) */
+    int32_t kasmK_n, kasmR_n, kspmv_n;       /* launches timed */
+    int32_t gpu_launches;       /* kernels launched by the library during the call */
+    int32_t n_iter_records;     /* entries filled in iters (<= iters_capacity) */
+    int32_t iters_capacity;
+    ua_newton_iter* iters;      /* caller-owned, may be NULL */
+} ua_newton_report;
+
+/* --------------------------------------------------------------------- */
+
+/* Library version string and device check. */
+const char* ua_version(void);
+const char* ua_last_error(void);
+int ua_device_count(void);
+
+/* ABI check for foreign bindings: sizes (bytes) of ua_mesh_desc, ua_params,
+ * ua_fields, ua_bcs, ua_newton_iter, ua_newton_report, in that order (n <= 6).
+ * No counterpart in the reference; it needs no GPU. */
+int ua_struct_sizes(int64_t* sizes, int32_t n);
+
+/* Fill CtrlVar defaults (Ua2D_DefaultParameters.m lines cited in ua_params). */
+void ua_params_default(ua_params* p);
+
+/* MUA setup: CreateMUA.m:31-98 (element orientation check as
+ * TestAndCorrectForInsideOutElements.m, quadrature per QuadratureRuleDegree.m)
+ * plus the symbolic CSR pattern, node patches and the element-to-CSR
+ * contribution map used by the deterministic segmented-sum scatter.
+ * ndof = 2 (uv) or 3 (uvh).  device = CUDA ordinal. */
+int ua_mesh_create(const ua_mesh_desc* desc, int32_t ndof, int32_t device, ua_mesh** out);
+
+/* Batched form: several independent meshes in one handle (one system each);
+ * every stage of the Newton solve runs for all systems in the same launches. */
+int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, int32_t ndof, int32_t device,
+                         ua_mesh** out);
+void ua_mesh_destroy(ua_mesh* m);
+
+/* Structural pattern of the ndof-block tangent of system `sys`:
+ * nnz, row pointer (nrows+1) and column indices (0-based, sorted).
+ * Pass NULL arrays to query nnz only. */
+int ua_mesh_pattern(const ua_mesh* m, int32_t sys, int64_t* nnz, int64_t* rowptr, int64_t* colind);
+
+/* Number of systems, nodes and elements of system `sys`; device bytes held. */
+int ua_mesh_info(const ua_mesh* m, int32_t sys, int32_t* nsys, int32_t* nnodes, int32_t* nele,
+                 int64_t* device_bytes);
+
+/* Elements flipped by the inside-out correction (0 when all had detJ>0). */
+int ua_mesh_flipped(const ua_mesh* m, int32_t* nflipped);
+
+/* uvMatrixAssembly (uvMatrixAssembly.m:5, uvMatrixAssemblySSTREAM.m:6-553)
+ * for system 0 of a single-mesh handle.  mode = UA_ASM_*.
+ * R: 2*Nnodes (Tint-Fext, uvMatrixAssemblySSTREAM.m:483-488);
+ * K: nnz values on the structural pattern, symmetrised as (K+K.')/2
+ * (uvMatrixAssemblySSTREAM.m:530-531); NULL for mode R. Tint/Fext optional. */
+int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs,
+                   int32_t mode, double* R, double* Kvals, double* Tint, double* Fext);
+
+/* Whole uv Newton solve: SSTREAM2dNR2.m:3-431 with the reset-and-retry of
+ * uv.m:107-112.  F->ub/F->vb: start values in, solution out.  lubvb: Lagrange
+ * multipliers l.ubvb (length = number of constraints), in/out, may be NULL.
+ * Kvals/R (optional): the last tangent and residual, as returned by SSTREAM2dNR2. */
+int ua_uv_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs,
+                 double* lubvb, int32_t nl, ua_newton_report* rep, double* Kvals, double* R);
+
+/* Batched uv Newton: fields[i], bcs[i], reports[i] for system i of a batch
+ * handle.  All systems advance together; converged ones stop contributing. */
+int ua_uv_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fields, const ua_bcs* bcs,
+                       ua_newton_report* reports);
+
+/* Number of rows of the constraint matrix L built from bcs (CreateLuv.m). */
+int ua_constraint_count(const ua_mesh* m, const ua_bcs* bcs, int32_t ndof, int32_t* nc);
+
+/* solveKApeSymmetric (solveKApeSymmetric.m:71-113) -> ABfgPreEliminate
+ * (ABfgPreEliminate.m:29-160) for an SPD block A given in CSR on the host:
+ * [A L'; L 0][x;y] = [f;g] with L given in CSR (nl rows, at most one non-zero
+ * per column, rows with orthogonal support).  Solved with projected PCG on
+ * the device.  x0/y0 are ignored (the reference ignores them too). */
+int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const int64_t* Acol, const double* Aval,
+                            int32_t nl, const int64_t* Lrowptr, const int64_t* Lcol, const double* Lval,
+                            const double* f, const double* g, double* x, double* y,
+                            double rtol, int32_t maxit, int32_t* its, int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UA_SSA_H */

@@ -1,0 +1,1087 @@
+"""CPU oracle for the Úa SSA (SSTREAM) Newton hot path.
+
+TEST INFRASTRUCTURE ONLY.  This module is a plain numpy/scipy restatement of
+the reference MATLAB code and exists to check the CUDA implementation.  Only
+``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import it; the product path (``uasource_b200``) never does.
+
+Parity status: the reference is MATLAB and cannot run here (no MATLAB, no
+Octave).  The restatement is pinned by the reference's own known-answer
+material instead: the analytic floating-shelf solution
+(``UaUtilities/AnalyticalOneDimentionalIceShelf.m``), the analytic grounded
+ice-stream solution (``UaMain/Simple1dIceStreamSolution.m``), the saddle-point
+examples of ``UaMain/TestABfgPreEliminate.m`` and the quadrature exactness of
+``UaMain/TestFEintegrate.m``; see ``tests/test_oracle_kat.py``.
+
+Every function names the reference file:line it follows (paths relative to
+the reference project root).  The vectorisation mirrors MATLAB's: arrays are
+``Nele x nod`` gathers, with loops over integration points and local nodes in
+the reference's order.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+EPS = np.finfo(float).eps
+
+# ---------------------------------------------------------------------------
+# Quadrature rules (UaMain/quadtriangle.m)
+# ---------------------------------------------------------------------------
+
+
+def _orbit_points(m, b1, b2, w):
+    """Expand symmetric orbits to points on the domain [0 0;1 0;0 1].
+
+    Follows quadTrianglePointsAndWeights (UaMain/quadtriangle.m:3674-3750):
+    vertices a=(0,0), b=(1,0), c=(0,1), area=1/2; a barycentric triple
+    (β1,β2,β3) maps to (x,y)=(β2,β3).
+    """
+    pts, wts = [], []
+    for mi, p, q, wi in zip(m, b1, b2, w):
+        if mi == 1:
+            q = p
+        r = 1.0 - (p + q)
+        if mi == 1:
+            orbit = [(p, q, r)]
+        elif mi == 3:
+            orbit = [(p, q, r), (q, r, p), (r, p, q)]
+        elif mi == 6:
+            orbit = [(p, q, r), (q, r, p), (r, p, q), (p, r, q), (q, p, r), (r, q, p)]
+        else:  # pragma: no cover - not used by the rules below
+            raise ValueError(mi)
+        for (_, bb, cc) in orbit:
+            pts.append((bb, cc))
+            wts.append(0.5 * wi)
+    return np.array(pts, dtype=float), np.array(wts, dtype=float)
+
+
+def quad_rule(degree: int):
+    """Degree-4 (6 point) and degree-8 (16 point) fully symmetric PI rules.
+
+    quadTriangleNonProductDegree4 (UaMain/quadtriangle.m:505-516) and
+    quadTriangleNonProductDegree8 'full' branch (UaMain/quadtriangle.m:725-745);
+    selected by QuadratureRuleDegree.m:13-21 (TriNodes 3 -> 4, 6 -> 8).
+    """
+    if degree == 4:
+        s = math.sqrt(38.0 - 44.0 * math.sqrt(2.0 / 5.0))
+        b1 = [(8.0 - math.sqrt(10.0) + s) / 18.0, (8.0 - math.sqrt(10.0) - s) / 18.0]
+        t = math.sqrt(213125.0 - 53320.0 * math.sqrt(10.0))
+        w = [(620.0 + t) / 3720.0, (620.0 - t) / 3720.0]
+        return _orbit_points([3, 3], b1, b1, w)
+    if degree == 8:
+        b1 = [0.3333333333333333333333333333333333, 0.1705693077517602066222935014914645,
+              0.0505472283170309754584235505965989, 0.4592925882927231560288155144941693,
+              0.2631128296346381134217857862846436]
+        b2 = list(b1)
+        b2[4] = 0.0083947774099576053372138345392944
+        w = [0.1443156076777871682510911104890646, 0.1032173705347182502817915502921290,
+             0.0324584976231980803109259283417806, 0.0950916342672846247938961043885843,
+             0.0272303141744349942648446900739089]
+        return _orbit_points([1, 3, 3, 3, 6], b1, b2, w)
+    raise ValueError(f"quadrature degree {degree} not restated")
+
+
+def rule_degree_for_nod(nod: int) -> int:
+    """QuadratureRuleDegree.m:11-21."""
+    return {3: 4, 6: 8}[nod]
+
+
+# ---------------------------------------------------------------------------
+# Shape functions (UaMain/shape_fun.m, UaMain/shape_der.m)
+# ---------------------------------------------------------------------------
+
+
+def shape_fun(nod, pt):
+    """shape_fun.m:52-71 (2-D, nod=3 and nod=6)."""
+    c1, c2 = pt
+    c3 = 1.0 - c1 - c2
+    if nod == 3:
+        return np.array([c1, c3, c2])
+    if nod == 6:
+        return np.array([(2 * c1 - 1) * c1, 4 * c3 * c1, (2 * c3 - 1) * c3,
+                         4 * c2 * c3, (2 * c2 - 1) * c2, 4 * c1 * c2])
+    raise ValueError(nod)
+
+
+def shape_der(nod, pt):
+    """shape_der.m:54-98 (2-D, nod=3 and nod=6); rows d/dxi, d/deta."""
+    c1, c2 = pt
+    c3 = 1.0 - c1 - c2
+    if nod == 3:
+        return np.array([[1.0, -1.0, 0.0], [0.0, -1.0, 1.0]])
+    if nod == 6:
+        return np.array([[4 * c1 - 1, 4 * (c3 - c1), -(4 * c3 - 1), -4 * c2, 0.0, 4 * c2],
+                         [0.0, -4 * c1, -(4 * c3 - 1), 4 * (c3 - c2), 4 * c2 - 1, 4 * c1]])
+    raise ValueError(nod)
+
+
+# ---------------------------------------------------------------------------
+# Mesh (MUA) — CreateMUA.m:31-98, derivVector.m:96-109
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class MUA:
+    coordinates: np.ndarray            # Nnodes x 2
+    connectivity: np.ndarray           # Nele x nod, 0-based
+    points: np.ndarray = None
+    weights: np.ndarray = None
+    Deriv: np.ndarray = None           # Nele x 2 x nod x nip
+    DetJ: np.ndarray = None            # Nele x nip
+    EleAreas: np.ndarray = None
+
+    @property
+    def Nnodes(self):
+        return self.coordinates.shape[0]
+
+    @property
+    def Nele(self):
+        return self.connectivity.shape[0]
+
+    @property
+    def nod(self):
+        return self.connectivity.shape[1]
+
+    @property
+    def nip(self):
+        return self.points.shape[0]
+
+
+def deriv_vector(coordinates, connectivity, points, Iint):
+    """derivVector.m:25-109."""
+    nod = connectivity.shape[1]
+    coox = coordinates[connectivity, 0]
+    cooy = coordinates[connectivity, 1]
+    der = shape_der(nod, points[Iint])
+    J11 = coox @ der[0]
+    J12 = cooy @ der[0]
+    J21 = coox @ der[1]
+    J22 = cooy @ der[1]
+    detJ = J11 * J22 - J12 * J21
+    Deriv = np.zeros((connectivity.shape[0], 2, nod))
+    for J in range(nod):
+        Deriv[:, 0, J] = (J22 * der[0, J] - J12 * der[1, J]) / detJ
+        Deriv[:, 1, J] = (-J21 * der[0, J] + J11 * der[1, J]) / detJ
+    return Deriv, detJ
+
+
+def create_mua(coordinates, connectivity):
+    """CreateMUA.m:31-98 restricted to what the SSA kernels use.
+
+    Quadrature from QuadratureRuleDegree/quadtriangle (CreateMUA.m:36-47),
+    inside-out flip (TestAndCorrectForInsideOutElements.m), Deriv/DetJ
+    (CalcMuaMeshDerivatives.m:27-31) and element areas.
+    """
+    coordinates = np.asarray(coordinates, dtype=float)
+    connectivity = np.asarray(connectivity, dtype=np.int64).copy()
+    nod = connectivity.shape[1]
+    points, weights = quad_rule(rule_degree_for_nod(nod))
+    # TestAndCorrectForInsideOutElements.m: detJ at the centroid must be > 0
+    _, detc = deriv_vector(coordinates, connectivity, np.array([[1 / 3, 1 / 3]]), 0)
+    bad = detc < 0
+    if np.any(bad):
+        connectivity[bad] = flip_elements(connectivity[bad])
+    mua = MUA(coordinates, connectivity, points, weights)
+    nip = points.shape[0]
+    mua.Deriv = np.zeros((mua.Nele, 2, nod, nip))
+    mua.DetJ = np.zeros((mua.Nele, nip))
+    for Iint in range(nip):
+        D, dJ = deriv_vector(coordinates, connectivity, points, Iint)
+        mua.Deriv[:, :, :, Iint] = D
+        mua.DetJ[:, Iint] = dJ
+    # TriAreaFE: area = sum_ip detJ*w
+    mua.EleAreas = mua.DetJ @ weights
+    return mua
+
+
+def flip_elements(conn):
+    """FlipElements.m: reverse orientation (P1: swap nodes 2,3; P2: corners 3<->5, mids 2<->6)."""
+    conn = conn.copy()
+    if conn.shape[1] == 3:
+        conn[:, [1, 2]] = conn[:, [2, 1]]
+    elif conn.shape[1] == 6:
+        conn[:, [1, 2, 3, 4, 5]] = conn[:, [5, 4, 3, 2, 1]]
+    return conn
+
+
+# ---------------------------------------------------------------------------
+# Parameters (the CtrlVar fields that change hot-path arithmetic)
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class Params:
+    """Subset of CtrlVar; defaults from Ua2D_DefaultParameters.m (line given)."""
+    kH: float = 1.0                  # :2288
+    Hh0: float = 0.0                 # :2295
+    SpeedZero: float = 1e-4          # :412
+    EpsZero: float = 1e-10           # :413
+    etaZero: float = 10.0            # :415
+    Czero: float = 0.0               # :441
+    Cmin: float = 1e-20              # :456-460 (SSTREAM)
+    AGlenmin: float = 1e-20          # :463
+    Picard: int = 0                  # :593
+    NRviscosity: float = 1.0         # :594
+    NRitmax: int = 50                # :597
+    NRitmin: int = 1                 # :600
+    NewtonAcceptRatio: float = 0.5   # :601
+    BacktrackingGammaMin: float = 1e-10  # :604
+    LineSearchAllowedToUseExtrapolation: bool = False  # :603
+    BackTrackBeta: float = 0.1       # :616
+    BackTrackMaxIterations: int = 50  # :617
+    BackTrackMaxExtrapolations: int = 50  # :618
+    BackTrackExtrapolationRatio: float = 2.5  # :619
+    BackTrackMinXfrac: float = 1e-10  # :620
+    BackTrackMaxFuncSame: int = 3    # :621
+    BackTrackGuardLower: float = 0.25  # :625
+    BackTrackGuardUpper: float = 0.95  # :626
+    uvDesiredWorkAndForceTolerances: tuple = (math.inf, 1e-15)   # :508
+    uvDesiredWorkOrForceTolerances: tuple = (math.inf, 1e-15)    # :509
+    uvExitBackTrackingStepLength: float = 1e-10                  # :510
+    uvAcceptableWorkAndForceTolerances: tuple = (math.inf, 1e-15)  # :511
+    uvAcceptableWorkOrForceTolerances: tuple = (math.inf, 1e-15)   # :512
+    ModifiedNRuvIntervalCriterion: int = 1       # :582
+    ModifiedNRuvReductionCriterion: float = 0.5  # :583
+    # uvh
+    theta: float = 0.5               # :377
+    SUPG_beta0: float = 1.0          # :376
+    uvh_SUPG_tau: str = "taus"       # :551
+    uvh_SUPG_tauMultiplier: float = 1.0  # :555
+    uvhDesiredWorkAndForceTolerances: tuple = (math.inf, 1e-15)    # :496
+    uvhDesiredWorkOrForceTolerances: tuple = (math.inf, 1e-15)     # :498
+    uvhExitBackTrackingStepLength: float = 1e-3                    # :502
+    uvhAcceptableWorkAndForceTolerances: tuple = (math.inf, 1e-6)  # :504
+    uvhAcceptableWorkOrForceTolerances: tuple = (1.0, 1e-8)        # :505
+    ModifiedNRuvhIntervalCriterion: int = 1        # :584
+    ModifiedNRuvhReductionCriterion: float = 0.5   # :585
+    NLtol: float = 1e-15             # BackTracking.m:125-127 default
+
+    def set_force_tolerance(self, tol):
+        """Set every force tolerance (desired and acceptable) to ``tol``."""
+        self.uvDesiredWorkAndForceTolerances = (math.inf, tol)
+        self.uvDesiredWorkOrForceTolerances = (math.inf, tol)
+        self.uvAcceptableWorkAndForceTolerances = (math.inf, tol)
+        self.uvAcceptableWorkOrForceTolerances = (math.inf, tol)
+
+
+@dataclass
+class Fields:
+    """UaFields.m subset: nodal column vectors plus scalars."""
+    h: np.ndarray
+    S: np.ndarray
+    B: np.ndarray
+    rho: np.ndarray
+    AGlen: np.ndarray
+    n: np.ndarray
+    C: np.ndarray
+    m: np.ndarray
+    ub: np.ndarray
+    vb: np.ndarray
+    rhow: float = 1030.0
+    g: float = 9.81 / 1000
+    alpha: float = 0.0
+    s: np.ndarray = None
+    b: np.ndarray = None
+    GF: np.ndarray = None
+    # uvh
+    as_: np.ndarray = None
+    ab: np.ndarray = None
+    dasdh: np.ndarray = None
+    dabdh: np.ndarray = None
+
+    def copy(self):
+        out = Fields(**{k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items()})
+        return out
+
+
+@dataclass
+class BCs:
+    """BoundaryConditions subset (fixed and tied nodes, 0-based)."""
+    ubFixedNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    ubFixedValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    vbFixedNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    vbFixedValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    ubTiedNodeA: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    ubTiedNodeB: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    vbTiedNodeA: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    vbTiedNodeB: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    hFixedNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    hFixedValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
+
+
+# ---------------------------------------------------------------------------
+# Physics (EffectiveViscositySSTREAM.m, BasalDrag.m, HeavisideApprox.m,
+# DiracDelta.m, Calc_bs_From_hBS.m)
+# ---------------------------------------------------------------------------
+
+
+def heaviside_approx(k, x, x0):
+    """HeavisideApprox.m:86: 0.5 + 0.5 tanh(k (x-x0))."""
+    return 0.5 + 0.5 * np.tanh(k * (x - x0))
+
+
+def dirac_delta(k, x, x0):
+    """DiracDelta.m:29: 0.5 k sech^2(k (x-x0))."""
+    with np.errstate(over="ignore"):
+        return 0.5 * k * (1.0 / np.cosh(k * (x - x0))) ** 2
+
+
+def calc_bs_from_hBS(p: Params, h, S, B, rho, rhow):
+    """Calc_bs_From_hBS.m:71-79,109 (Enforce_bAboveB=false, no thickness reset)."""
+    hf = rhow * (S - B) / rho
+    GF = heaviside_approx(p.kH, h - hf, p.Hh0)
+    bfloat = S - rho * h / rhow
+    b = GF * B + (1 - GF) * bfloat
+    s = b + h
+    return b, s, GF
+
+
+def effective_viscosity(p: Params, A, n, exx, eyy, exy):
+    """EffectiveViscositySSTREAM.m:7-9."""
+    e = np.sqrt(p.EpsZero ** 2 + exx ** 2 + eyy ** 2 + exx * eyy + exy ** 2)
+    eta = 0.5 * A ** (-1.0 / n) * e ** ((1 - n) / n) + p.etaZero
+    E = (1 - n) / (4 * n) * A ** (-1.0 / n) * e ** ((1 - 3 * n) / n)
+    return eta, E
+
+
+def basal_drag_weertman(p: Params, He, delta, ub, vb, C, m):
+    """BasalDrag.m:54-77 (clamps, β², Dβ²), :184-186 dispatch, Weertman :410-446.
+
+    Returns taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, dtauxdh, dtauydh.
+    """
+    delta = np.where(delta < 0, 0.0, delta)
+    He = np.where(He < 0, 0.0, He)
+    C0 = p.Czero
+    u0 = p.SpeedZero
+    speed = np.sqrt(ub * ub + vb * vb + u0 ** 2)
+    Um = speed ** (1.0 / m - 1)
+    beta2 = (C + C0) ** (-1.0 / m) * Um
+    Dbeta2 = (1.0 / m - 1) * (C + C0) ** (-1.0 / m) * (ub ** 2 + vb ** 2 + u0 ** 2) ** ((1 - 3 * m) / (2 * m))
+    taux = He * beta2 * ub
+    tauy = He * beta2 * vb
+    dtauxdu = He * (beta2 + Dbeta2 * ub * ub)
+    dtauydv = He * (beta2 + Dbeta2 * vb * vb)
+    dtauxdv = He * Dbeta2 * ub * vb
+    dtauydu = dtauxdv
+    dtauxdh = delta * beta2 * ub
+    dtauydh = delta * beta2 * vb
+    return taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, dtauxdh, dtauydh
+
+
+# ---------------------------------------------------------------------------
+# uv assembly — UaMain/uvMatrixAssemblySSTREAM.m
+# ---------------------------------------------------------------------------
+
+
+def _matlab_sparse(I, J, V, m, n):
+    """MATLAB ``sparse(I,J,V,m,n)``: sum duplicates, keep non-zeros only (CSC)."""
+    A = sp.coo_matrix((V, (I, J)), shape=(m, n)).tocsc()
+    A.sum_duplicates()
+    A.eliminate_zeros()
+    A.sort_indices()
+    return A
+
+
+def uv_matrix_assembly(p: Params, mua: MUA, F: Fields, bcs: BCs = None, Ronly=False, ZeroFields=False,
+                       return_parts=False):
+    """uvMatrixAssemblySSTREAM.m:6-553 (post-2025 default, no melange, Weertman).
+
+    Returns (R, K) with R a dense 2Nn vector (Tint-Fext) and K the symmetrised
+    CSC tangent ``(K+K.')/2`` (None when Ronly).  ``return_parts`` also returns
+    Tint and Fext.
+    """
+    ub, vb = F.ub, F.vb
+    if ZeroFields:  # :24-28
+        ub = np.zeros_like(ub)
+        vb = np.zeros_like(vb)
+        if bcs is not None:
+            ub[bcs.ubFixedNode] = bcs.ubFixedValue
+            vb[bcs.vbFixedNode] = bcs.vbFixedValue
+    if np.any(np.isnan(ub)) or np.any(np.isnan(vb)):  # :63-64
+        raise FloatingPointError("uvMatrixAssembly:NaN")
+    Dvisk = 0.0 if p.Picard else p.NRviscosity  # :67-71
+    g = F.g
+    Nele, nod, Nn = mua.Nele, mua.nod, mua.Nnodes
+    neq = 2 * Nn
+    conn = mua.connectivity
+    hnod = F.h[conn]; snod = F.s[conn]
+    ubnod = ub[conn]; vbnod = vb[conn]
+    Cnod = F.C[conn]; mnod = F.m[conn]
+    AGlennod = F.AGlen[conn]; nnod = F.n[conn]
+    Snod = F.S[conn]; Bnod = F.B[conn]
+    rhonod = F.rho[conn]
+    ca, sa = math.cos(F.alpha), math.sin(F.alpha)
+
+    if not Ronly:
+        d1d1 = np.zeros((Nele, nod, nod)); d2d2 = np.zeros((Nele, nod, nod))
+        d1d2 = np.zeros((Nele, nod, nod)); d2d1 = np.zeros((Nele, nod, nod))
+    Tx = np.zeros((Nele, nod)); Ty = np.zeros((Nele, nod))
+    Fx = np.zeros((Nele, nod)); Fy = np.zeros((Nele, nod))
+
+    for Iint in range(mua.nip):  # :168
+        fun = shape_fun(nod, mua.points[Iint])
+        Deriv = mua.Deriv[:, :, :, Iint]
+        detJ = mua.DetJ[:, Iint]
+        hint = hnod @ fun; sint = snod @ fun
+        uint = ubnod @ fun; vint = vbnod @ fun
+        Cint = Cnod @ fun
+        Cint = np.where(Cint < p.Cmin, p.Cmin, Cint)  # :205
+        mint = mnod @ fun
+        AGlenint = AGlennod @ fun
+        AGlenint = np.where(AGlenint < p.AGlenmin, p.AGlenmin, AGlenint)  # :243
+        nint = nnod @ fun
+        Bint = Bnod @ fun; Sint = Snod @ fun
+        Hint = Sint - Bint
+        rhoint = rhonod @ fun
+        # post-2025 flotation at integration points :300-310
+        hfint = F.rhow * Hint / rhoint
+        Heint = heaviside_approx(p.kH, hint - hfint, p.Hh0)
+        HEint = heaviside_approx(p.kH, hfint - hint, p.Hh0)
+        deltaint = dirac_delta(p.kH, hint - hfint, p.Hh0)
+        Hposint = heaviside_approx(p.kH, Hint, p.Hh0) * Hint
+        dint = HEint * rhoint * hint / F.rhow + Heint * Hposint
+        # nodal-derivative sums :322-347
+        dsdx = np.zeros(Nele); dhdx = np.zeros(Nele); dsdy = np.zeros(Nele); dhdy = np.zeros(Nele)
+        exx = np.zeros(Nele); eyy = np.zeros(Nele); exy = np.zeros(Nele)
+        for Inod in range(nod):
+            dsdx = dsdx + Deriv[:, 0, Inod] * snod[:, Inod]
+            dhdx = dhdx + Deriv[:, 0, Inod] * hnod[:, Inod]
+            dsdy = dsdy + Deriv[:, 1, Inod] * snod[:, Inod]
+            dhdy = dhdy + Deriv[:, 1, Inod] * hnod[:, Inod]
+            exx = exx + Deriv[:, 0, Inod] * ubnod[:, Inod]
+            eyy = eyy + Deriv[:, 1, Inod] * vbnod[:, Inod]
+            exy = exy + 0.5 * (Deriv[:, 0, Inod] * vbnod[:, Inod] + Deriv[:, 1, Inod] * ubnod[:, Inod])
+        taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, _, _ = basal_drag_weertman(
+            p, Heint, deltaint, uint, vint, Cint, mint)  # :351-352
+        etaint, Eint = effective_viscosity(p, AGlenint, nint, exx, eyy, exy)  # :353
+        dbdx = dsdx - dhdx; dbdy = dsdy - dhdy  # :357
+        detJw = detJ * mua.weights[Iint]  # :359
+        for Inod in range(nod):  # :362
+            if not Ronly:
+                for Jnod in range(nod):
+                    d1d1[:, Inod, Jnod] += (4 * hint * etaint * Deriv[:, 0, Inod] * Deriv[:, 0, Jnod]
+                                            + hint * etaint * Deriv[:, 1, Inod] * Deriv[:, 1, Jnod]
+                                            + dtauxdu * fun[Jnod] * fun[Inod]) * detJw
+                    d2d2[:, Inod, Jnod] += (4 * hint * etaint * Deriv[:, 1, Inod] * Deriv[:, 1, Jnod]
+                                            + hint * etaint * Deriv[:, 0, Inod] * Deriv[:, 0, Jnod]
+                                            + dtauydv * fun[Jnod] * fun[Inod]) * detJw
+                    d1d2[:, Inod, Jnod] += (etaint * hint * (2 * Deriv[:, 0, Inod] * Deriv[:, 1, Jnod]
+                                                             + Deriv[:, 1, Inod] * Deriv[:, 0, Jnod])
+                                            + dtauxdv * fun[Jnod] * fun[Inod]) * detJw
+                    d2d1[:, Inod, Jnod] += (etaint * hint * (2 * Deriv[:, 1, Inod] * Deriv[:, 0, Jnod]
+                                                             + Deriv[:, 0, Inod] * Deriv[:, 1, Jnod])
+                                            + dtauydu * fun[Jnod] * fun[Inod]) * detJw
+                    Deu = Eint * ((2 * exx + eyy) * Deriv[:, 0, Jnod] + exy * Deriv[:, 1, Jnod])  # :398
+                    Dev = Eint * ((2 * eyy + exx) * Deriv[:, 1, Jnod] + exy * Deriv[:, 0, Jnod])
+                    E11 = hint * (4 * exx + 2 * eyy) * Deu * Deriv[:, 0, Inod] + 2 * hint * exy * Deu * Deriv[:, 1, Inod]
+                    E12 = hint * (4 * exx + 2 * eyy) * Dev * Deriv[:, 0, Inod] + 2 * hint * exy * Dev * Deriv[:, 1, Inod]
+                    E22 = hint * (4 * eyy + 2 * exx) * Dev * Deriv[:, 1, Inod] + 2 * hint * exy * Dev * Deriv[:, 0, Inod]
+                    E21 = hint * (4 * eyy + 2 * exx) * Deu * Deriv[:, 1, Inod] + 2 * hint * exy * Deu * Deriv[:, 0, Inod]
+                    d1d1[:, Inod, Jnod] += Dvisk * E11 * detJw  # :421-424
+                    d2d2[:, Inod, Jnod] += Dvisk * E22 * detJw
+                    d1d2[:, Inod, Jnod] += Dvisk * E12 * detJw
+                    d2d1[:, Inod, Jnod] += Dvisk * E21 * detJw
+            # residual terms :431-449
+            t1 = -g * (rhoint * hint - F.rhow * dint) * dbdx * fun[Inod] * ca + rhoint * g * hint * sa * fun[Inod]
+            t2 = 0.5 * g * ca * (rhoint * hint ** 2 - F.rhow * dint ** 2) * Deriv[:, 0, Inod]
+            t3 = hint * etaint * (4 * exx + 2 * eyy) * Deriv[:, 0, Inod]
+            t4 = hint * etaint * 2 * exy * Deriv[:, 1, Inod]
+            t5 = taux * fun[Inod]
+            Tx[:, Inod] += (t3 + t4 + t5) * detJw
+            Fx[:, Inod] += (t1 + t2) * detJw
+            t1 = -g * (rhoint * hint - F.rhow * dint) * dbdy * fun[Inod] * ca
+            t2 = 0.5 * ca * g * (rhoint * hint ** 2 - F.rhow * dint ** 2) * Deriv[:, 1, Inod]
+            t3 = hint * etaint * (4 * eyy + 2 * exx) * Deriv[:, 1, Inod]
+            t4 = hint * etaint * 2 * exy * Deriv[:, 0, Inod]
+            t5 = tauy * fun[Inod]
+            Ty[:, Inod] += (t3 + t4 + t5) * detJw
+            Fy[:, Inod] += (t1 + t2) * detJw
+
+    # R scatter :462-488 (sparse accumulate, here dense bincount)
+    iR = np.concatenate([np.concatenate([conn[:, I], conn[:, I] + Nn]) for I in range(nod)])
+    Tval = np.concatenate([np.concatenate([Tx[:, I], Ty[:, I]]) for I in range(nod)])
+    Fval = np.concatenate([np.concatenate([Fx[:, I], Fy[:, I]]) for I in range(nod)])
+    Tint = np.bincount(iR, weights=Tval, minlength=neq)
+    Fext = np.bincount(iR, weights=Fval, minlength=neq)
+    R = Tint - Fext
+    K = None
+    if not Ronly:  # :490-534
+        Ii, Jj, Xv = [], [], []
+        for Inod in range(nod):
+            for Jnod in range(nod):
+                Ii += [conn[:, Inod], conn[:, Inod] + Nn, conn[:, Inod], conn[:, Inod] + Nn]
+                Jj += [conn[:, Jnod], conn[:, Jnod] + Nn, conn[:, Jnod] + Nn, conn[:, Jnod]]
+                Xv += [d1d1[:, Inod, Jnod], d2d2[:, Inod, Jnod], d1d2[:, Inod, Jnod], d2d1[:, Inod, Jnod]]
+        K = _matlab_sparse(np.concatenate(Ii), np.concatenate(Jj), np.concatenate(Xv), neq, neq)
+        K = (K + K.T) / 2  # :530-531
+        K = K.tocsc()
+        K.eliminate_zeros()
+        K.sort_indices()
+    if return_parts:
+        return R, K, Tint, Fext
+    return R, K
+
+
+def structural_pattern(mua: MUA, ndof: int):
+    """Structural (connectivity-implied) pattern of the ndof-block tangent, CSR with sorted columns."""
+    conn = mua.connectivity
+    Nn, nod = mua.Nnodes, mua.nod
+    I = np.repeat(conn, nod, axis=1).ravel()
+    J = np.tile(conn, (1, nod)).ravel()
+    rows, cols = [], []
+    for a in range(ndof):
+        for b in range(ndof):
+            rows.append(I + a * Nn)
+            cols.append(J + b * Nn)
+    A = sp.coo_matrix((np.ones(len(I) * ndof * ndof), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(ndof * Nn, ndof * Nn)).tocsr()
+    A.sum_duplicates()
+    A.sort_indices()
+    return A.indptr.copy(), A.indices.copy()
+
+
+# ---------------------------------------------------------------------------
+# Constraints — CreateLuv.m:2-78, ScaleL.m:28-33, BCs2MLC.m:19-20,49
+# ---------------------------------------------------------------------------
+
+
+def create_Luv(Nnodes, bcs: BCs):
+    """BCs2MLC.m:19-29 + CreateLuv.m:28-76 + ScaleL.m:28-33 (ties, then fixed u, fixed v)."""
+    ufn, ui = np.unique(bcs.ubFixedNode, return_index=True)
+    ufv = np.asarray(bcs.ubFixedValue, dtype=float)[ui]
+    vfn, vi = np.unique(bcs.vbFixedNode, return_index=True)
+    vfv = np.asarray(bcs.vbFixedValue, dtype=float)[vi]
+    ia, ib, xv, b = [], [], [], []
+    JJ = 0
+    for A_, B_ in zip(bcs.ubTiedNodeA, bcs.ubTiedNodeB):
+        ia += [JJ, JJ]; ib += [A_, B_]; xv += [1.0, -1.0]; b.append(0.0); JJ += 1
+    for A_, B_ in zip(bcs.vbTiedNodeA, bcs.vbTiedNodeB):
+        ia += [JJ, JJ]; ib += [A_ + Nnodes, B_ + Nnodes]; xv += [1.0, -1.0]; b.append(0.0); JJ += 1
+    for nI, val in zip(ufn, ufv):
+        ia.append(JJ); ib.append(nI); xv.append(1.0); b.append(val); JJ += 1
+    for nI, val in zip(vfn, vfv):
+        ia.append(JJ); ib.append(nI + Nnodes); xv.append(1.0); b.append(val); JJ += 1
+    if JJ == 0:
+        return None, None
+    L = _matlab_sparse(np.array(ia), np.array(ib), np.array(xv), JJ, 2 * Nnodes).tocsr()
+    c = np.array(b)
+    Lscale = np.sqrt(np.asarray(L.multiply(L).sum(axis=1)).ravel())  # ScaleL.m:29
+    S = sp.diags(1.0 / Lscale)
+    return (S @ L).tocsr(), S @ c
+
+
+# ---------------------------------------------------------------------------
+# Linear solve — ABfgPreEliminate.m:29-160
+# ---------------------------------------------------------------------------
+
+
+def abfg_pre_eliminate(A, B, f, g):
+    """ABfgPreEliminate.m:29-160 with SuperLU in place of MATLAB ``decomposition``."""
+    A = sp.csc_matrix(A)
+    if B is None or B.shape[0] == 0:
+        return spla.spsolve(A, f), np.zeros(0)
+    B = sp.csr_matrix(B)
+    BBT = (B @ B.T).toarray()
+    if not np.allclose(BBT, np.diag(np.diag(BBT)), atol=0, rtol=0):
+        raise ValueError("ABfgPreEliminate:B B*B^T not diagonal")
+    Scale = np.ones(B.shape[0])
+    if not np.all(np.abs(np.diag(BBT) - 1) < 1000 * EPS):  # :38-45
+        Lscale = np.sqrt(np.diag(BBT))
+        Scale = 1.0 / Lscale
+        B = sp.diags(Scale) @ B
+        g = Scale * g
+    dA = np.abs(A.diagonal())
+    factor = 1.0 / np.mean(dA) if np.mean(dA) != 0 else 1.0  # :49-53
+    if not np.isfinite(factor):
+        factor = 1.0
+    BtB = (B.T @ B).tocsc()
+    As = factor * A
+    fs = factor * f
+    Q = sp.identity(A.shape[0], format="csc") - BtB  # :61
+    Atilde = (Q @ As + BtB).tocsc()  # :62
+    btilde = Q @ fs + B.T @ g  # :63
+    # :110-115 decomposition(Atilde) and solve.  MATLAB factors a square sparse
+    # unsymmetric matrix with UMFPACK, which applies iterative refinement
+    # (UMFPACK_IRSTEP, default 2 steps); SuperLU is used here with the same
+    # number of refinement steps.
+    lu = spla.splu(Atilde)
+    x = lu.solve(btilde)
+    for _ in range(2):
+        x = x + lu.solve(btilde - Atilde @ x)
+    y = B @ (fs - As @ x)  # :138
+    y = y / factor  # :142
+    y = Scale * y  # :159
+    return x, y
+
+
+# ---------------------------------------------------------------------------
+# Cost function and convergence tests
+# ---------------------------------------------------------------------------
+
+
+def calc_cost_function_nr(p, mua, gamma, F, fext0, L, lubvb, cuv, dub, dvb, dl, bcs=None):
+    """CalcCostFunctionNR.m:14-47.  Returns (r, rForce, rWork, D2, frhs, grhs)."""
+    if gamma != gamma:
+        raise ValueError("gamma is nan")
+    Fg = F.copy()
+    Fg.ub = F.ub + gamma * dub
+    Fg.vb = F.vb + gamma * dvb
+    lg = lubvb + gamma * dl if L is not None else None
+    R, _ = uv_matrix_assembly(p, mua, Fg, bcs, Ronly=True)
+    if L is not None:
+        frhs = -R - L.T @ lg
+        grhs = cuv - L @ np.concatenate([Fg.ub, Fg.vb])
+        fg = np.concatenate([frhs, grhs])
+        dd = np.concatenate([dub, dvb, dl])
+    else:
+        frhs = -R
+        grhs = np.zeros(0)
+        fg = frhs
+        dd = np.concatenate([dub, dvb])
+    Normalisation = fext0 @ fext0 + 1000 * EPS
+    rForce = (fg @ fg) / Normalisation
+    D2 = fg @ dd
+    rWork = D2 ** 2
+    return rForce, rForce, rWork, D2, frhs, grhs
+
+
+def uv_residuals_criteria(p: Params, rForce, rWork, iteration, gamma):
+    """uvResidualsCriteria.m:1-23."""
+    if gamma > max(p.uvExitBackTrackingStepLength, p.BacktrackingGammaMin):
+        a, o = p.uvDesiredWorkAndForceTolerances, p.uvDesiredWorkOrForceTolerances
+    else:
+        a, o = p.uvAcceptableWorkAndForceTolerances, p.uvAcceptableWorkOrForceTolerances
+    return ((rWork < a[0] and rForce < a[1]) and (rWork < o[0] or rForce < o[1])
+            and iteration >= p.NRitmin)
+
+
+# ---------------------------------------------------------------------------
+# Line search — BackTracking.m, CubicFit.m, parabolamin.m, rLineminUa.m
+# ---------------------------------------------------------------------------
+
+
+def parabolamin(a, b, c, fa, fb, fc):
+    """parabolamin.m (3-point parabola minimum with non-convex fallbacks)."""
+    if c < b:
+        b, c, fb, fc = c, b, fc, fb
+    if not (a < b < c):
+        return math.nan, 1
+    if math.isinf(fa) and math.isinf(fb) and math.isinf(fc):
+        return a / 100, 1
+    if math.isinf(fb) and math.isinf(fc):
+        return (b / 100 if b == b else 1e-5), 1
+    t1 = (b - a) ** 2 * (fb - fc)
+    t2 = (b - c) ** 2 * (fb - fa)
+    t3 = (b - a) * (fb - fc)
+    t4 = (b - c) * (fb - fa)
+    status = 0
+    if t3 != t4:
+        xmin = b - 0.5 * (t1 - t2) / (t3 - t4)
+    else:
+        xmin, status = math.nan, 1
+    if xmin != xmin or (fa + (b - a) * (fc - fa) / (c - a) < fb):
+        if fc < fb < fa:
+            xmin = 5 * c
+        elif fc > fb > fa:
+            xmin = a + b / 10
+        elif fc > fa and fb > fa:
+            xmin = a + b / 100
+        else:
+            xmin = (a + b) / 3
+    return xmin, status
+
+
+def cubic_fit(slope, y0, y1, y2, x1, x2):
+    """CubicFit.m: minimum of the cubic through (0,y0) with slope, (x1,y1), (x2,y2)."""
+    if any(v != v for v in (y0, y1, y2, x1, x2)):
+        raise ValueError("CubicFit:nanOnInput")
+    if x1 > x2:
+        x1, x2, y1, y2 = x2, x1, y2, y1
+    status = 0
+    if x1 == x2:
+        D = (y1 - y0) / x1 - slope
+        xmin = -x1 * slope / 2 / D if D != 0 else x1 * 0.9
+    else:
+        M = np.array([[1 / x1 ** 2, -1 / x2 ** 2], [-x2 / x1 ** 2, x1 / x2 ** 2]])
+        ab = (M @ np.array([y1 - slope * x1 - y0, y2 - slope * x2 - y0])) / (x1 - x2)
+        disc = ab[1] ** 2 - 3 * ab[0] * slope
+        if ab[0] == 0 or disc < 0:
+            xmin = math.nan
+        else:
+            xmin = (-ab[1] + math.sqrt(disc)) / 3 / ab[0]
+        if ab[0] == 0 or xmin != xmin:
+            if slope == slope:
+                D = (y1 - y0) / x1 - slope
+                xmin = -x1 * slope / 2 / D if D != 0 else math.nan
+            else:
+                xmin, status = parabolamin(0, x1, x2, y0, y1, y2)
+    if xmin != xmin:
+        if y0 < y1 < y2:
+            xmin = x1 / 2
+        elif y0 > y1 > y2:
+            xmin = x1 + (x2 - x1) / 2
+        elif y0 < y1 and y1 > y2:
+            xmin = x1 + (x2 - x1) / 2 if y2 < y0 else x1 / 2
+    return xmin, status
+
+
+@dataclass
+class BackTrackInfo:
+    Converged: int = 0
+    iarm: int = 0
+    nFuncEval: int = 0
+    nExtrapolationSteps: int = 0
+    Infovector: list = field(default_factory=list)
+
+
+def backtracking(slope0, b, fa, fb, func, p: Params, GammaMin=None, AcceptRatio=None, AllowExtrapolation=None):
+    """BackTracking.m:54-759 (no plotting).  ``func(gamma) -> f``.
+
+    ``GammaMin``/``AcceptRatio``/``AllowExtrapolation`` are the CtrlVar
+    overrides rLineminUa.m sets before calling (e.g. :87, :241-243).
+    """
+    beta = p.BackTrackBeta
+    MaxIterations = p.BackTrackMaxIterations
+    MaxExtrapolations = p.BackTrackMaxExtrapolations
+    ExtrapolationRatio = p.BackTrackExtrapolationRatio
+    MinXfrac = p.BackTrackMinXfrac * b
+    MaxFuncSame = p.BackTrackMaxFuncSame
+    BacktrackingGammaMin = p.BacktrackingGammaMin if GammaMin is None else GammaMin
+    NewtonAcceptRatio = p.NewtonAcceptRatio if AcceptRatio is None else AcceptRatio
+    allow_ext = p.LineSearchAllowedToUseExtrapolation if AllowExtrapolation is None else AllowExtrapolation
+    GL, GU = p.BackTrackGuardLower, p.BackTrackGuardUpper
+    ContinueRatio = 0.5  # :147
+    info = BackTrackInfo()
+    nfe = 0
+    NoSlope = slope0 is None or slope0 != slope0
+    if not NoSlope and slope0 > 0:
+        return math.nan, math.nan, info
+    target = max(NewtonAcceptRatio * fa, p.NLtol)  # :160
+    if not NoSlope:
+        tws = min(fa + beta * slope0 * b, NewtonAcceptRatio * fa)
+        target = max(target, tws)
+        if target < 0:
+            target = max(NewtonAcceptRatio * fa, p.NLtol)
+    xfrac = 1e10
+    iMinSame = 0
+    iMinSameWB = 0
+    iarm = 0
+    a = 0.0
+    if fa is None or fa != fa:
+        fa = func(a); nfe += 1
+    f0 = fa
+    if fb is None or fb != fb:
+        if b is None or b != b:
+            b = 1.0
+        fb = func(b); nfe += 1
+    Info = [[a, fa], [b, fb]]
+
+    def cur_min():
+        fm = min(v[1] for v in Info)
+        for v in Info:
+            if v[1] == fm:
+                return v[0], fm
+
+    gmin, fmin = cur_min()
+    if fb < target:  # :239-265
+        info.Converged = 1
+        info.nFuncEval = nfe
+        info.Infovector = Info
+        return gmin, fmin, info
+    if not NoSlope:
+        gamma = -b * slope0 / 2 / ((fb - fa) / b - slope0)  # :268
+    else:
+        gamma = a + 0.9 * (b - a)
+    if gamma > GU * b:
+        gamma = GU * b
+    elif gamma < GL * b:
+        gamma = GL * b
+    if fmin > target:  # :282
+        iarm = 1
+        fgamma = func(gamma); nfe += 1
+        gammaOld = gamma
+        Info.append([gamma, fgamma])
+    else:
+        gammaOld = gamma; gamma = b; fgamma = fb
+    gmin, fmin = cur_min()
+    c = b; fc = fb; b = gamma; fb = fgamma  # :306
+    Extrapolation = 0
+    fbOld = bOld = None
+    if allow_ext:
+        while fb < fa and fc < fb and fmin > target:
+            Extrapolation += 1
+            gamma = ExtrapolationRatio * c
+            gammaOld = gamma
+            fgamma = func(gamma); nfe += 1
+            Info.append([gamma, fgamma]); gmin, fmin = cur_min()
+            fbOld, bOld = fb, b
+            fb, b = fc, c
+            fc, c = fgamma, gamma
+            if Extrapolation > MaxExtrapolations:
+                break
+    if Extrapolation > 0:  # :388-405
+        a, fa = bOld, fbOld
+        b = (a + c) / 2
+        NoSlope = True
+        fb = func(b); nfe += 1
+        Info.append([b, fb]); gmin, fmin = cur_min()
+    fLastReduction = 1.0
+    while fgamma > target or fLastReduction < ContinueRatio:  # :408
+        iarm += 1
+        if NoSlope:
+            gamma, _ = parabolamin(a, b, c, fa, fb, fc)
+            if gamma != gamma:
+                raise ValueError("BackTrack:nan")
+        else:
+            gamma, _ = cubic_fit(slope0, fa, fb, fc, b, c)
+            if gamma != gamma:
+                raise ValueError("BackTrack:nan")
+        if iarm == 2 and Extrapolation > 0:  # :433-470
+            if gamma > b + 0.95 * (c - b):
+                gamma = b + 0.95 * (c - b)
+            elif gamma < a + 0.25 * (b - a):
+                gamma = a + 0.25 * (b - a)
+            fgamma = func(gamma); nfe += 1
+            if gamma < b and fgamma < fb:
+                c, fc = b, fb
+                b, fb = gamma, fgamma
+            elif gamma > b and fgamma < fb:
+                b, fb = c, fc
+                c, fc = gamma, fgamma
+        else:
+            if b < gamma < c:  # :479-502
+                if gamma < (b + GU * (c - a)):
+                    gamma = b + GU * (c - a)
+                elif gamma > (c - GL * (c - b)):
+                    gamma = c - GL * (c - b)
+                fgamma = func(gamma); nfe += 1
+                b, fb = gamma, fgamma
+            else:  # :503-534
+                if gamma > (a + GU * (b - a)):
+                    gamma = a + GU * (b - a)
+                elif gamma < (a + GL * (b - a)):
+                    gamma = a + GL * (b - a)
+                fgamma = func(gamma); nfe += 1
+                c, fc, b, fb = b, fb, gamma, fgamma
+        fminOld, gminOld = fmin, gmin
+        Info.append([gamma, fgamma]); gmin, fmin = cur_min()
+        fLastReduction = fmin / fminOld
+        if gmin != gminOld:
+            xfrac = abs(gmin - gminOld)
+            MinXfrac = gmin * 1e-10
+        iMinSame = iMinSame + 1 if fmin == fminOld else 0
+        iMinSameWB = iMinSameWB + 1 if (gamma < gammaOld and fmin == fminOld) else 0
+        gammaOld = gamma
+        if not NoSlope:
+            target = fa + beta * slope0 * b  # :567
+            if target < 0:
+                target = max(NewtonAcceptRatio * fa, p.NLtol)
+        if iMinSame > MaxFuncSame and fmin < f0:
+            break
+        if iarm > 5 and iMinSameWB > 2 and fmin < f0:
+            break
+        if xfrac < MinXfrac and fmin < f0:
+            break
+        if b < BacktrackingGammaMin:
+            break
+        if iarm > MaxIterations:
+            break
+    if fgamma < (target - EPS):  # :626-633
+        info.Converged = 1
+    elif abs(fmin - fa) / fa > 1e-5 and gamma > BacktrackingGammaMin:
+        info.Converged = 1
+    else:
+        info.Converged = 0
+    Info.sort(key=lambda v: v[0])  # :646-649 (sorted copy for the record only)
+    info.Infovector = Info
+    info.nExtrapolationSteps = Extrapolation
+    info.iarm = iarm
+    info.nFuncEval = nfe
+    return gmin, fmin, info
+
+
+@dataclass
+class LineSearchResult:
+    gamma: float
+    r: float
+    du: np.ndarray
+    dv: np.ndarray
+    dl: np.ndarray
+    info: BackTrackInfo
+    rForce: float
+    rWork: float
+    D2: float
+    needs_cauchy: bool = False
+
+
+def rlinemin_newton(p: Params, func, r0, r1, du0, dv0, dl0):
+    """rLineminUa.m:57-135: Newton-direction backtracking (the '-Auto-' first stage).
+
+    ``func(gamma) -> (r, rForce, rWork, D2)``.  ``needs_cauchy`` reports the
+    :96 condition under which the reference continues with the mass-matrix
+    Cauchy step (:159-322); that continuation is not restated here.
+    """
+    rmin = r0
+    out = LineSearchResult(0.0, r0, du0 * 0, dv0 * 0, dl0 * 0, BackTrackInfo(), r0, math.nan, math.nan)
+    fN = lambda gm: func(gm)[0]
+    gN, rN, info = backtracking(-2 * r0, 1.0, r0, r1, fN, p, GammaMin=0.001)  # :84-89
+    out.info = info
+    if gN < 0.75 and rN / r0 > 0.7:  # :94-104
+        out.needs_cauchy = True
+    if rN < rmin:  # :108-133
+        out.du, out.dv, out.dl = gN * du0, gN * dv0, gN * dl0
+        out.gamma, out.r = gN, rN
+        rT, rF, rW, D2 = func(gN)
+        out.rForce, out.rWork, out.D2 = rF, rW, D2
+        if abs(rT - rN) > 1000 * EPS:
+            raise ValueError("rLineMinUa:inconsistent")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# uv Newton driver — SSTREAM2dNR2.m:3-431 (+ uv.m:34-51)
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class NewtonRecord:
+    iteration: int
+    gamma: float
+    r0: float
+    r: float
+    rForce: float
+    rWork: float
+    iarm: int
+
+
+@dataclass
+class UvResult:
+    ub: np.ndarray
+    vb: np.ndarray
+    lubvb: np.ndarray
+    converged: bool
+    iterations: int
+    records: list
+    K: object = None
+    R: np.ndarray = None
+    L: object = None
+    cauchy_needed: int = 0
+
+
+def prepare_fields(p: Params, F: Fields):
+    """uv.m:34-51: expand scalar m,n, then Calc_bs_From_hBS."""
+    F = F.copy()
+    Nn = F.h.shape[0]
+    for name in ("m", "n"):
+        v = getattr(F, name)
+        if np.isscalar(v) or np.ndim(v) == 0:
+            setattr(F, name, np.zeros(Nn) + float(v))
+    F.b, F.s, F.GF = calc_bs_from_hBS(p, F.h, F.S, F.B, F.rho, F.rhow)
+    return F
+
+
+def sstream2dnr2(p: Params, mua: MUA, bcs: BCs, F: Fields, lubvb=None, solver=None, verbose=False):
+    """SSTREAM2dNR2.m:3-431 (full-Newton default, interval criterion 1).
+
+    ``solver(K, L, frhs, grhs) -> (dx, dl)`` defaults to ABfgPreEliminate.
+    """
+    if solver is None:
+        solver = abfg_pre_eliminate
+    F = F.copy()
+    Nn = mua.Nnodes
+    L, cuv = create_Luv(Nn, bcs)  # :32
+    nc = 0 if cuv is None else cuv.shape[0]
+    if lubvb is None or lubvb.shape[0] != nc:
+        lubvb = np.zeros(nc)
+    if np.any(np.isnan(F.C)) or np.any(np.isnan(F.AGlen)):  # :42-56
+        return UvResult(F.ub + np.nan, F.vb + np.nan, lubvb, False, 0, [])
+    F.ub = F.ub.copy(); F.vb = F.vb.copy()
+    F.ub[bcs.ubFixedNode] = bcs.ubFixedValue  # :101-104
+    F.vb[bcs.vbFixedNode] = bcs.vbFixedValue
+    dub = np.zeros(Nn); dvb = np.zeros(Nn); dl = np.zeros(nc)
+    fext0, _ = uv_matrix_assembly(p, mua, F, bcs, Ronly=True, ZeroFields=True)  # :122-124
+    Ruv, _ = uv_matrix_assembly(p, mua, F, bcs, Ronly=True)  # :138-140
+
+    def Func(gamma, Du, Dv, Dl):
+        r, rF, rW, D2, fr, gr = calc_cost_function_nr(p, mua, gamma, F, fext0, L, lubvb, cuv, Du, Dv, Dl, bcs)
+        return r, rF, rW, D2
+
+    r, rForce, _, _ = Func(0.0, dub, dvb, dl)  # :149-150
+    rWork = 0.0
+    gamma = 1.0
+    iteration = 0
+    ResidualReduction = 1e10
+    records = []
+    converged = True
+    Kuv = None
+    cauchy = 0
+    while True:
+        if uv_residuals_criteria(p, rForce, rWork, iteration, gamma):  # :160-174
+            converged = True
+            break
+        if iteration > p.NRitmax:  # :177-187
+            converged = False
+            break
+        iteration += 1
+        if (iteration - 1) % p.ModifiedNRuvIntervalCriterion == 0 or ResidualReduction > p.ModifiedNRuvReductionCriterion:
+            Ruv, Kuv = uv_matrix_assembly(p, mua, F, bcs, Ronly=False)  # :200-203
+        else:
+            Ruv, _ = uv_matrix_assembly(p, mua, F, bcs, Ronly=True)
+        if L is not None:  # :234-240
+            frhs = -Ruv - L.T @ lubvb
+            grhs = cuv - L @ np.concatenate([F.ub, F.vb])
+        else:
+            frhs = -Ruv
+            grhs = np.zeros(0)
+        sol, dl = solver(Kuv, L, frhs, grhs)  # :245
+        dub = sol[:Nn].copy(); dvb = sol[Nn:2 * Nn].copy()
+        if dl is None:
+            dl = np.zeros(nc)
+        r0, rForce0, rWork0, D20 = Func(0.0, dub, dvb, dl)  # :260-261
+        if iteration == 1 and uv_residuals_criteria(p, rForce0, rWork0, iteration, 1.0):  # :263-283
+            iteration -= 1
+            converged = True
+            break
+        r1, rForce1, rWork1, D21 = Func(1.0, dub, dvb, dl)  # :288
+        if r1 / r0 < p.NewtonAcceptRatio:  # :290-296
+            r, rForce, rWork = r1, rForce1, rWork1
+            du, dv, dlu = dub, dvb, dl
+            gamma = 1.0
+            iarm = 0
+            bt_conv = 1
+        else:  # :300-308
+            ls = rlinemin_newton(p, lambda gm: Func(gm, dub, dvb, dl), r0, r1, dub, dvb, dl)
+            gamma, r, du, dv, dlu = ls.gamma, ls.r, ls.du, ls.dv, ls.dl
+            rForce, rWork = ls.rForce, ls.rWork
+            iarm = ls.info.iarm
+            bt_conv = ls.info.Converged
+            cauchy += int(ls.needs_cauchy)
+        records.append(NewtonRecord(iteration, gamma, r0, r, rForce, rWork, iarm))
+        if verbose:
+            print(f"NR-SSTREAM(uv):{iteration:3d}/{iarm:<2d} g={gamma:<14.7g} r/r0={r / r0:<14.7g} "
+                  f"r0={r0:<14.7g} r={r:<14.7g} rForce={rForce:<14.7g} rWork={rWork:<14.7g}")
+        if bt_conv == 0:  # :322-327
+            converged = False
+            break
+        F.ub = F.ub + du  # :367-369
+        F.vb = F.vb + dv
+        lubvb = lubvb + dlu
+        ResidualReduction = r / r0  # :371
+    return UvResult(F.ub, F.vb, lubvb, converged, iteration, records, Kuv, Ruv, L, cauchy)
+
+
+def uv(p: Params, mua: MUA, bcs: BCs, F: Fields, lubvb=None, solver=None, verbose=False):
+    """uv.m:34-112: prepare fields, Newton solve, one reset-and-retry on failure."""
+    F = prepare_fields(p, F)
+    res = sstream2dnr2(p, mua, bcs, F, lubvb, solver, verbose)
+    if not res.converged:  # uv.m:107-112
+        F2 = F.copy()
+        F2.ub = F2.ub * 0; F2.vb = F2.vb * 0
+        l0 = res.lubvb * 0 if res.lubvb is not None else None
+        res = sstream2dnr2(p, mua, bcs, F2, l0, solver, verbose)
+    return res

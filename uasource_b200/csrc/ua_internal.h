@@ -1,0 +1,133 @@
+// Internal structures of libuassa: device layout of the resident mesh
+// ("MUA" of Úa, CreateMUA.m) extended with the symbolic scatter plan.
+//
+// Layout in HBM (all systems of a handle concatenated, system-major):
+//   nodes      : global node id g = node_off[s] + local node i
+//   elements   : conn[a*ne_total + e] (SoA, element fastest) = global node id
+//   dofs       : dof_off[s] + c*nn_s + i   (c = 0:u, 1:v, 2:h), Úa ordering
+//   tangent    : CSR over dofs.  Row (c,g) of system s starts at
+//                knz_off[s] + c*ndof*NNZn_s + ndof*(nodeptr[g]-nodeptr[node_off[s]])
+//                and holds ndof blocks of deg(g) columns (block b, k-th neighbour).
+//   scatter    : node patches.  A patch is a set of nodes of one system plus
+//                every element touching them.  The assembly kernel computes
+//                the patch's element tangents into shared memory, then sums
+//                them per node-level non-zero through the precomputed
+//                contribution list (element-local id, local row node,
+//                local col node), in increasing global element order: a
+//                deterministic segmented sum with no atomics whose result does
+//                not depend on the patch partition.
+#pragma once
+#include <cstdint>
+#include <vector>
+#include <string>
+#include <cuda_runtime.h>
+#include "../../include/ua_ssa.h"
+
+namespace ua {
+
+constexpr int kMaxNip = 16;
+constexpr int kMaxNod = 6;
+
+// contribution packing: element-local id (10 bits) | row node a (3) | col node b (3)
+__host__ __device__ inline uint16_t pack_contrib(int el, int a, int b) {
+  return (uint16_t)((el << 6) | (a << 3) | b);
+}
+
+struct QuadTable {
+  int nip;
+  double w[kMaxNip];
+  double fun[kMaxNip][kMaxNod];
+  double der[kMaxNip][2][kMaxNod];
+};
+
+// Device view of a handle (passed to kernels by value).
+struct DevMesh {
+  int nsys, nn, ne, nod, nip, ndof;
+  const int* conn;            // [nod][ne]
+  const double* x;            // [nn]
+  const double* y;            // [nn]
+  const int* nodeptr;         // node-level CSR [nn+1] (global)
+  const int* nodecol;         // node-level columns (global node ids)
+  const int* node_sys;        // [nn]
+  // per system
+  const int* sys_node_off;    // [nsys+1]
+  const int* sys_dof_off;     // [nsys+1]
+  const int* sys_knz_off;     // [nsys+1] (dof-level nnz offset)
+  const int* sys_nnzn;        // [nsys]  node-level nnz of the system
+  // patches
+  int npatch;
+  const int* patch_sys;       // [npatch]
+  const int* patch_node_ptr;  // [npatch+1]
+  const int* patch_nodes;     // global node ids
+  const int* patch_elem_ptr;  // [npatch+1]
+  const int* patch_elems;     // global element ids (sorted)
+  const int* patch_q_ptr;     // [npatch+1] into pq arrays
+  const uint32_t* pq_rk;      // (local row << 16) | k
+  const int* pq_cptr;         // [total_pq+1] into contrib
+  const uint16_t* contrib;
+  const int* prow_diag;       // per patch row (aligned with patch_nodes): pq index of diagonal
+  int max_patch_elems;
+};
+
+// Host-side mirror plus ownership of device buffers.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct HostSystem {
+  int nn = 0, ne = 0;
+  std::vector<double> x, y;        // coordinates
+  std::vector<int> conn;           // [nod][ne] local node ids (0-based)
+  int nflipped = 0;
+};
+
+struct Constraints {
+  // constraint matrix L (scaled rows), CSR by constraint row over global dofs
+  int nc = 0;                      // total over systems
+  std::vector<int> sys_c_off;      // [nsys+1]
+  std::vector<int> rowptr;         // [nc+1]
+  std::vector<int> col;            // global dof
+  std::vector<double> val;
+  std::vector<double> rhs;         // c (scaled)
+  bool mask_only = true;           // every row has exactly one entry
+};
+
+struct Work;
+
+}  // namespace ua
+
+struct ua_mesh {
+  int device = 0;
+  int ndof = 2;
+  int nod = 3;
+  int nip = 6;
+  cudaStream_t stream = nullptr;
+  std::vector<ua::HostSystem> sys;
+  // host copies of symbolic data needed on the host
+  std::vector<int> h_node_off, h_dof_off, h_knz_off, h_nnzn, h_elem_off;
+  std::vector<int> h_nodeptr, h_nodecol;
+  int nn_total = 0, ne_total = 0, ndof_total = 0;
+  long long nnz_total = 0;
+  ua::DevMesh dm{};
+  std::vector<ua::DeviceBuffer> owned;
+  size_t device_bytes = 0;
+  // reusable work buffers
+  ua::Work* work = nullptr;
+};
+
+namespace ua {
+// allocation helpers (record ownership in the mesh)
+void* dev_alloc(ua_mesh* m, size_t bytes);
+void dev_free_all(ua_mesh* m);
+int set_error(int code, const char* fmt, ...);
+const QuadTable& quad_table(int nod);
+}  // namespace ua
+
+#define UA_CUDA_TRY(call)                                                        \
+  do {                                                                            \
+    cudaError_t _e = (call);                                                      \
+    if (_e != cudaSuccess)                                                        \
+      return ua::set_error(UA_ERR_CUDA, "%s failed: %s (%s:%d)", #call,           \
+                           cudaGetErrorString(_e), __FILE__, __LINE__);           \
+  } while (0)

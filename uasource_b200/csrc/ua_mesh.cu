@@ -1,0 +1,403 @@
+// Mesh handle: CreateMUA.m:31-98 restated for the device, plus the symbolic
+// scatter plan (node patches, CSR pattern, contribution lists).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include "ua_internal.h"
+
+namespace ua {
+
+static thread_local char g_err[1024] = "";
+
+int set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+const char* last_error_message() { return g_err; }
+
+void* dev_alloc(ua_mesh* m, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  m->owned.push_back({p, bytes});
+  m->device_bytes += bytes;
+  return p;
+}
+
+void dev_free_all(ua_mesh* m) {
+  for (auto& b : m->owned) cudaFree(b.ptr);
+  m->owned.clear();
+  m->device_bytes = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Quadrature tables: quadtriangle.m nonproduct PI rules of degree 4 (6 points,
+// :505-516) and degree 8 (16 points, :725-745), expanded over their symmetry
+// orbits onto the domain [0 0;1 0;0 1] as quadTrianglePointsAndWeights does
+// (:3674-3750): barycentric (b1,b2,b3) -> (x,y) = (b2,b3), weight = w/2.
+// Shape functions shape_fun.m:52-71 and derivatives shape_der.m:54-98.
+// ---------------------------------------------------------------------------
+static void orbit(int mult, double p, double q, double w, std::vector<double>& X, std::vector<double>& Y,
+                  std::vector<double>& W) {
+  if (mult == 1) q = p;
+  double r = 1.0 - (p + q);
+  double o[6][3] = {{p, q, r}, {q, r, p}, {r, p, q}, {p, r, q}, {q, p, r}, {r, q, p}};
+  for (int i = 0; i < mult; ++i) {
+    X.push_back(o[i][1]);
+    Y.push_back(o[i][2]);
+    W.push_back(0.5 * w);
+  }
+}
+
+static void shape(int nod, double c1, double c2, double* fun, double (*der)[kMaxNod]) {
+  double c3 = 1.0 - c1 - c2;
+  if (nod == 3) {
+    fun[0] = c1; fun[1] = c3; fun[2] = c2;
+    der[0][0] = 1; der[0][1] = -1; der[0][2] = 0;
+    der[1][0] = 0; der[1][1] = -1; der[1][2] = 1;
+  } else {
+    fun[0] = (2 * c1 - 1) * c1; fun[1] = 4 * c3 * c1; fun[2] = (2 * c3 - 1) * c3;
+    fun[3] = 4 * c2 * c3;       fun[4] = (2 * c2 - 1) * c2; fun[5] = 4 * c1 * c2;
+    der[0][0] = 4 * c1 - 1; der[0][1] = 4 * (c3 - c1); der[0][2] = -(4 * c3 - 1);
+    der[0][3] = -4 * c2;    der[0][4] = 0;             der[0][5] = 4 * c2;
+    der[1][0] = 0;          der[1][1] = -4 * c1;       der[1][2] = -(4 * c3 - 1);
+    der[1][3] = 4 * (c3 - c2); der[1][4] = 4 * c2 - 1; der[1][5] = 4 * c1;
+  }
+}
+
+static QuadTable make_table(int nod) {
+  QuadTable t{};
+  std::vector<double> X, Y, W;
+  if (nod == 3) {
+    double s = std::sqrt(38.0 - 44.0 * std::sqrt(2.0 / 5.0));
+    double b1 = (8.0 - std::sqrt(10.0) + s) / 18.0, b2 = (8.0 - std::sqrt(10.0) - s) / 18.0;
+    double tt = std::sqrt(213125.0 - 53320.0 * std::sqrt(10.0));
+    orbit(3, b1, b1, (620.0 + tt) / 3720.0, X, Y, W);
+    orbit(3, b2, b2, (620.0 - tt) / 3720.0, X, Y, W);
+  } else {
+    const double b1[5] = {0.3333333333333333333333333333333333, 0.1705693077517602066222935014914645,
+                          0.0505472283170309754584235505965989, 0.4592925882927231560288155144941693,
+                          0.2631128296346381134217857862846436};
+    const double b2_5 = 0.0083947774099576053372138345392944;
+    const double w[5] = {0.1443156076777871682510911104890646, 0.1032173705347182502817915502921290,
+                         0.0324584976231980803109259283417806, 0.0950916342672846247938961043885843,
+                         0.0272303141744349942648446900739089};
+    const int mult[5] = {1, 3, 3, 3, 6};
+    for (int i = 0; i < 5; ++i) orbit(mult[i], b1[i], i == 4 ? b2_5 : b1[i], w[i], X, Y, W);
+  }
+  t.nip = (int)X.size();
+  for (int i = 0; i < t.nip; ++i) {
+    t.w[i] = W[i];
+    shape(nod, X[i], Y[i], t.fun[i], t.der[i]);
+  }
+  return t;
+}
+
+const QuadTable& quad_table(int nod) {
+  static QuadTable t3 = make_table(3);
+  static QuadTable t6 = make_table(6);
+  return nod == 3 ? t3 : t6;
+}
+
+// Morton code of 16-bit quantised coordinates.
+static uint32_t spread16(uint32_t v) {
+  v &= 0xffff;
+  v = (v | (v << 8)) & 0x00FF00FF;
+  v = (v | (v << 4)) & 0x0F0F0F0F;
+  v = (v | (v << 2)) & 0x33333333;
+  v = (v | (v << 1)) & 0x55555555;
+  return v;
+}
+
+}  // namespace ua
+
+using namespace ua;
+
+static int upload(ua_mesh* m, const void* h, size_t bytes, void** d) {
+  *d = dev_alloc(m, bytes);
+  if (!*d) return set_error(UA_ERR_OOM, "device allocation of %zu bytes failed", bytes);
+  if (bytes) UA_CUDA_TRY(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
+  return UA_OK;
+}
+
+template <class T>
+static int upload_vec(ua_mesh* m, const std::vector<T>& v, const T** d) {
+  void* p = nullptr;
+  int rc = upload(m, v.data(), v.size() * sizeof(T), &p);
+  *d = (const T*)p;
+  return rc;
+}
+
+// detJ at the element centroid as derivVector.m:96-100 (for the orientation test of
+// TestAndCorrectForInsideOutElements.m).
+static double centroid_detJ(int nod, const double* xe, const double* ye) {
+  double fun[kMaxNod], der[2][kMaxNod];
+  shape(nod, 1.0 / 3.0, 1.0 / 3.0, fun, der);
+  double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+  for (int a = 0; a < nod; ++a) {
+    J11 += xe[a] * der[0][a];
+    J12 += ye[a] * der[0][a];
+    J21 += xe[a] * der[1][a];
+    J22 += ye[a] * der[1][a];
+  }
+  return J11 * J22 - J12 * J21;
+}
+
+// FlipElements.m: reverse orientation.
+static void flip(int nod, int* l) {
+  if (nod == 3) {
+    std::swap(l[1], l[2]);
+  } else {
+    int t[6] = {l[0], l[5], l[4], l[3], l[2], l[1]};
+    for (int a = 0; a < 6; ++a) l[a] = t[a];
+  }
+}
+
+// Shared-memory bytes of one element in the assembly kernel (symmetric uu/vv
+// blocks, full uv block, and Tx,Fx,Ty,Fy) for ndof=2; for ndof=3 nine full blocks
+// and six residual parts.
+static size_t elem_smem_bytes(int nod, int ndof) {
+  if (ndof == 2) return (size_t)(nod * (nod + 1) + nod * nod + 4 * nod) * sizeof(double);
+  return (size_t)(9 * nod * nod + 6 * nod) * sizeof(double);
+}
+
+extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, int32_t ndof, int32_t device,
+                                    ua_mesh** out) {
+  if (!descs || count <= 0 || !out) return set_error(UA_ERR_INVALID, "ua_mesh_create_batch: bad arguments");
+  if (ndof != 2 && ndof != 3) return set_error(UA_ERR_INVALID, "ndof must be 2 or 3");
+  int nod = descs[0].nod;
+  if (nod != 3 && nod != 6) return set_error(UA_ERR_INVALID, "nod must be 3 or 6 (got %d)", nod);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_error(UA_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return set_error(UA_ERR_INVALID, "bad device ordinal %d", device);
+  UA_CUDA_TRY(cudaSetDevice(device));
+
+  ua_mesh* m = new ua_mesh();
+  m->device = device;
+  m->ndof = ndof;
+  m->nod = nod;
+  m->nip = quad_table(nod).nip;
+  int nsys = count;
+  m->sys.resize(nsys);
+  // ---- validate, convert, orient -------------------------------------------------
+  for (int s = 0; s < nsys; ++s) {
+    const ua_mesh_desc& d = descs[s];
+    if (d.nod != nod) { delete m; return set_error(UA_ERR_INVALID, "all meshes of a batch must have the same nod"); }
+    if (d.nnodes <= 0 || d.nele <= 0 || !d.coordinates || !d.connectivity) {
+      delete m; return set_error(UA_ERR_INVALID, "mesh %d: empty or null arrays", s);
+    }
+    HostSystem& hs = m->sys[s];
+    hs.nn = d.nnodes; hs.ne = d.nele;
+    hs.x.assign(d.coordinates, d.coordinates + d.nnodes);
+    hs.y.assign(d.coordinates + d.nnodes, d.coordinates + 2 * (size_t)d.nnodes);
+    hs.conn.resize((size_t)nod * d.nele);
+    for (size_t i = 0; i < hs.conn.size(); ++i) {
+      int v = d.connectivity[i] - d.index_base;
+      if (v < 0 || v >= d.nnodes) { delete m; return set_error(UA_ERR_BAD_MESH, "mesh %d: connectivity index out of range", s); }
+      hs.conn[i] = v;
+    }
+    for (int e = 0; e < hs.ne; ++e) {
+      int l[kMaxNod]; double xe[kMaxNod], ye[kMaxNod];
+      for (int a = 0; a < nod; ++a) { l[a] = hs.conn[(size_t)a * hs.ne + e]; xe[a] = hs.x[l[a]]; ye[a] = hs.y[l[a]]; }
+      double dj = centroid_detJ(nod, xe, ye);
+      if (!(dj != 0.0) || !std::isfinite(dj)) { delete m; return set_error(UA_ERR_BAD_MESH, "mesh %d element %d: degenerate (detJ=%g)", s, e, dj); }
+      if (dj < 0) {
+        flip(nod, l);
+        for (int a = 0; a < nod; ++a) hs.conn[(size_t)a * hs.ne + e] = l[a];
+        hs.nflipped++;
+      }
+    }
+  }
+  // ---- offsets -----------------------------------------------------------------
+  m->h_node_off.assign(nsys + 1, 0);
+  m->h_elem_off.assign(nsys + 1, 0);
+  for (int s = 0; s < nsys; ++s) {
+    m->h_node_off[s + 1] = m->h_node_off[s] + m->sys[s].nn;
+    m->h_elem_off[s + 1] = m->h_elem_off[s] + m->sys[s].ne;
+  }
+  int NN = m->h_node_off[nsys], NE = m->h_elem_off[nsys];
+  m->nn_total = NN; m->ne_total = NE;
+  std::vector<int> conn((size_t)nod * NE);
+  std::vector<double> X(NN), Y(NN);
+  std::vector<int> node_sys(NN);
+  for (int s = 0; s < nsys; ++s) {
+    const HostSystem& hs = m->sys[s];
+    int no = m->h_node_off[s], eo = m->h_elem_off[s];
+    for (int i = 0; i < hs.nn; ++i) { X[no + i] = hs.x[i]; Y[no + i] = hs.y[i]; node_sys[no + i] = s; }
+    for (int a = 0; a < nod; ++a)
+      for (int e = 0; e < hs.ne; ++e) conn[(size_t)a * NE + eo + e] = no + hs.conn[(size_t)a * hs.ne + e];
+  }
+  // ---- node -> element CSR -------------------------------------------------------
+  std::vector<int> n2e_ptr(NN + 1, 0), n2e;
+  for (int a = 0; a < nod; ++a)
+    for (int e = 0; e < NE; ++e) n2e_ptr[conn[(size_t)a * NE + e] + 1]++;
+  for (int i = 0; i < NN; ++i) n2e_ptr[i + 1] += n2e_ptr[i];
+  n2e.resize(n2e_ptr[NN]);
+  {
+    std::vector<int> fill(n2e_ptr.begin(), n2e_ptr.end() - 1);
+    for (int e = 0; e < NE; ++e)       // increasing e => each list sorted
+      for (int a = 0; a < nod; ++a) {
+        int g = conn[(size_t)a * NE + e];
+        // an element lists a node once, so no duplicate within a list
+        n2e[fill[g]++] = e;
+      }
+    for (int g = 0; g < NN; ++g) std::sort(n2e.begin() + n2e_ptr[g], n2e.begin() + n2e_ptr[g + 1]);
+  }
+  for (int g = 0; g < NN; ++g)
+    if (n2e_ptr[g + 1] == n2e_ptr[g]) { delete m; return set_error(UA_ERR_BAD_MESH, "node %d belongs to no element", g); }
+  // ---- node-level adjacency (sorted, includes self) ------------------------------
+  std::vector<int>& nodeptr = m->h_nodeptr;
+  std::vector<int>& nodecol = m->h_nodecol;
+  nodeptr.assign(NN + 1, 0);
+  nodecol.clear();
+  {
+    std::vector<int> buf;
+    for (int g = 0; g < NN; ++g) {
+      buf.clear();
+      for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t) {
+        int e = n2e[t];
+        for (int a = 0; a < nod; ++a) buf.push_back(conn[(size_t)a * NE + e]);
+      }
+      std::sort(buf.begin(), buf.end());
+      buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+      nodecol.insert(nodecol.end(), buf.begin(), buf.end());
+      nodeptr[g + 1] = (int)nodecol.size();
+    }
+  }
+  // ---- per-system dof / nnz offsets ----------------------------------------------
+  m->h_dof_off.assign(nsys + 1, 0);
+  m->h_knz_off.assign(nsys + 1, 0);
+  m->h_nnzn.assign(nsys, 0);
+  long long knz = 0;
+  for (int s = 0; s < nsys; ++s) {
+    int nnzn = nodeptr[m->h_node_off[s + 1]] - nodeptr[m->h_node_off[s]];
+    m->h_nnzn[s] = nnzn;
+    m->h_dof_off[s + 1] = m->h_dof_off[s] + ndof * m->sys[s].nn;
+    knz += (long long)ndof * ndof * nnzn;
+    if (knz >= (1LL << 31)) { delete m; return set_error(UA_ERR_INVALID, "tangent has more than 2^31 non-zeros"); }
+    m->h_knz_off[s + 1] = (int)knz;
+  }
+  m->ndof_total = m->h_dof_off[nsys];
+  m->nnz_total = knz;
+  // ---- patches (Morton-ordered node groups within each system) --------------------
+  const size_t smem_budget = 160 * 1024;
+  int emax = (int)std::min<size_t>(1023, smem_budget / elem_smem_bytes(nod, ndof));
+  std::vector<int> patch_sys, patch_node_ptr(1, 0), patch_nodes, patch_elem_ptr(1, 0), patch_elems;
+  std::vector<int> patch_q_ptr(1, 0), pq_cptr(1, 0), prow_diag;
+  std::vector<uint32_t> pq_rk;
+  std::vector<uint16_t> contrib;
+  std::vector<int> mark(NE, -1);
+  std::vector<int> elocal(NE, -1);
+  for (int s = 0; s < nsys; ++s) {
+    int no = m->h_node_off[s], nn = m->sys[s].nn;
+    double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+    for (int i = 0; i < nn; ++i) {
+      xmin = std::min(xmin, X[no + i]); xmax = std::max(xmax, X[no + i]);
+      ymin = std::min(ymin, Y[no + i]); ymax = std::max(ymax, Y[no + i]);
+    }
+    double span = std::max(xmax - xmin, ymax - ymin);
+    if (!(span > 0)) span = 1;
+    std::vector<std::pair<uint32_t, int>> key(nn);
+    for (int i = 0; i < nn; ++i) {
+      uint32_t qx = (uint32_t)std::min(65535.0, std::floor((X[no + i] - xmin) / span * 65535.0));
+      uint32_t qy = (uint32_t)std::min(65535.0, std::floor((Y[no + i] - ymin) / span * 65535.0));
+      key[i] = {spread16(qx) | (spread16(qy) << 1), no + i};
+    }
+    std::stable_sort(key.begin(), key.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    // patch size: enough patches to fill 148 SMs several times, at most 128 nodes
+    int pn = std::max(16, std::min(128, nn / 600));
+    size_t idx = 0;
+    while (idx < key.size()) {
+      std::vector<int> nodes, elems;
+      int stamp = (int)patch_sys.size();
+      while (idx < key.size() && (int)nodes.size() < pn) {
+        int g = key[idx].second;
+        int add = 0;
+        for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t) add += (mark[n2e[t]] != stamp);
+        if (!nodes.empty() && (int)elems.size() + add > emax) break;
+        if ((int)elems.size() + add > emax) { delete m; return set_error(UA_ERR_BAD_MESH, "node %d touches too many elements", g); }
+        nodes.push_back(g);
+        for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t)
+          if (mark[n2e[t]] != stamp) { mark[n2e[t]] = stamp; elems.push_back(n2e[t]); }
+        ++idx;
+      }
+      std::sort(elems.begin(), elems.end());
+      for (int i = 0; i < (int)elems.size(); ++i) elocal[elems[i]] = i;
+      patch_sys.push_back(s);
+      // rows of this patch
+      for (int r = 0; r < (int)nodes.size(); ++r) {
+        int g = nodes[r];
+        int deg = nodeptr[g + 1] - nodeptr[g];
+        for (int k = 0; k < deg; ++k) {
+          int j = nodecol[nodeptr[g] + k];
+          if (j == g) prow_diag.push_back((int)pq_rk.size());
+          pq_rk.push_back(((uint32_t)r << 16) | (uint32_t)k);
+          for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t) {  // sorted global element order
+            int e = n2e[t];
+            int a = -1, b = -1;
+            for (int c = 0; c < nod; ++c) {
+              int v = conn[(size_t)c * NE + e];
+              if (v == g) a = c;
+              if (v == j) b = c;
+            }
+            if (b >= 0) contrib.push_back(pack_contrib(elocal[e], a, b));
+          }
+          pq_cptr.push_back((int)contrib.size());
+        }
+      }
+      patch_nodes.insert(patch_nodes.end(), nodes.begin(), nodes.end());
+      patch_node_ptr.push_back((int)patch_nodes.size());
+      patch_elems.insert(patch_elems.end(), elems.begin(), elems.end());
+      patch_elem_ptr.push_back((int)patch_elems.size());
+      patch_q_ptr.push_back((int)pq_rk.size());
+      m->dm.max_patch_elems = std::max(m->dm.max_patch_elems, (int)elems.size());
+    }
+  }
+  // ---- upload ----------------------------------------------------------------------
+  UA_CUDA_TRY(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  DevMesh& dm = m->dm;
+  dm.nsys = nsys; dm.nn = NN; dm.ne = NE; dm.nod = nod; dm.nip = m->nip; dm.ndof = ndof;
+  dm.npatch = (int)patch_sys.size();
+  int rc = UA_OK;
+  std::vector<int> knz_off(m->h_knz_off.begin(), m->h_knz_off.end());
+  if ((rc = upload_vec(m, conn, &dm.conn))) goto fail;
+  if ((rc = upload_vec(m, X, &dm.x))) goto fail;
+  if ((rc = upload_vec(m, Y, &dm.y))) goto fail;
+  if ((rc = upload_vec(m, nodeptr, &dm.nodeptr))) goto fail;
+  if ((rc = upload_vec(m, nodecol, &dm.nodecol))) goto fail;
+  if ((rc = upload_vec(m, node_sys, &dm.node_sys))) goto fail;
+  if ((rc = upload_vec(m, m->h_node_off, &dm.sys_node_off))) goto fail;
+  if ((rc = upload_vec(m, m->h_dof_off, &dm.sys_dof_off))) goto fail;
+  if ((rc = upload_vec(m, knz_off, &dm.sys_knz_off))) goto fail;
+  if ((rc = upload_vec(m, m->h_nnzn, &dm.sys_nnzn))) goto fail;
+  if ((rc = upload_vec(m, patch_sys, &dm.patch_sys))) goto fail;
+  if ((rc = upload_vec(m, patch_node_ptr, &dm.patch_node_ptr))) goto fail;
+  if ((rc = upload_vec(m, patch_nodes, &dm.patch_nodes))) goto fail;
+  if ((rc = upload_vec(m, patch_elem_ptr, &dm.patch_elem_ptr))) goto fail;
+  if ((rc = upload_vec(m, patch_elems, &dm.patch_elems))) goto fail;
+  if ((rc = upload_vec(m, patch_q_ptr, &dm.patch_q_ptr))) goto fail;
+  if ((rc = upload_vec(m, pq_rk, &dm.pq_rk))) goto fail;
+  if ((rc = upload_vec(m, pq_cptr, &dm.pq_cptr))) goto fail;
+  if ((rc = upload_vec(m, contrib, &dm.contrib))) goto fail;
+  if ((rc = upload_vec(m, prow_diag, &dm.prow_diag))) goto fail;
+  *out = m;
+  return UA_OK;
+fail:
+  dev_free_all(m);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return rc;
+}

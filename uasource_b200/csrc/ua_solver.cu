@@ -1,0 +1,1373 @@
+// uv Newton-Raphson solve on the device: SSTREAM2dNR2.m:3-431 with the inner
+// linear solve of ABfgPreEliminate.m replaced by a constrained, Jacobi-
+// preconditioned conjugate-gradient solve, and the cost function of
+// CalcCostFunctionNR.m:14-47 fused into residual-only assembly launches.
+//
+// All kernels work on every system of a handle at once (batched form):
+// per-system scalars live in small device arrays and a per-system selection
+// flag masks systems that have converged or are not part of the current
+// stage.  Reductions are deterministic: each CTA writes one partial sum and a
+// one-CTA-per-system kernel adds the partials in a fixed order, so a
+// system's result does not depend on which other systems share the launch.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include "ua_internal.h"
+#include "ua_kernels.h"
+#include "ua_linesearch.h"
+
+namespace ua {
+
+constexpr int kRB = 256;        // rows per row block (one CTA)
+
+// Kernel launches issued by the library on the calling thread (reported per call).
+static thread_local long long g_launches = 0;
+
+// Optional per-launch timing with CUDA events recorded on the handle's stream.
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;  // (kind, (start, stop))
+  cudaEvent_t get() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void reset() { used = 0; marks.clear(); }
+  ~Prof() { for (auto e : pool) cudaEventDestroy(e); }
+};
+enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2 };
+constexpr int kRedThreads = 256;
+enum { SV_RZ = 0, SV_PQ, SV_ALPHA, SV_BETA, SV_RR, SV_RR0, SV_TOL2, SV_NORM, SV_FF, SV_FD, SV_COUNT };
+
+struct Work {
+  int nsys = 0, nrb = 0, nc = 0;
+  int prec = -1;
+  // dof CSR
+  int *rowptr = nullptr, *colind = nullptr, *diagpos = nullptr;
+  int *rb_start = nullptr, *rb_sys = nullptr, *sys_rb_off = nullptr;
+  // nodal fields
+  double *h, *s, *S, *B, *rho, *A, *n, *C, *m;
+  SysScal* scal;
+  // dof vectors
+  double *X, *X0, *dX, *R, *frhs, *Tint, *Fext;
+  double* Kd = nullptr;
+  float* Kf = nullptr;
+  // Krylov (VT = double or float, allocated as double-sized)
+  void *kr, *kz, *kp, *kq, *invd;
+  double* part;    // [4][nrb]
+  double* sysv;    // [SV_COUNT][nsys]
+  int* done;       // [nsys]
+  int* its;        // [nsys]
+  int* status;     // [nsys] 0 ok, 1 breakdown
+  int* sel;        // [nsys]
+  double* gamma;   // [nsys]
+  unsigned char* cmask;  // [ndof]
+  int* dof_con;    // [ndof]
+  // constraints (mask form: one unit entry per row)
+  int* con_dof = nullptr;
+  int* con_sys = nullptr;
+  int* sys_con_off = nullptr;
+  double* con_rhs = nullptr;
+  double *lam = nullptr, *dlam = nullptr, *grhs = nullptr;
+  // pinned host staging
+  double* h_sysv = nullptr;
+  int* h_int = nullptr;
+  double* h_gamma = nullptr;
+  std::vector<int> h_sys_rb_off, h_sys_con_off;
+  Prof prof;
+};
+
+static void prof_begin(ua_mesh* m, int kind, cudaEvent_t* ev) {
+  Work* w = m->work;
+  if (!w->prof.on) return;
+  ev[0] = w->prof.get();
+  ev[1] = w->prof.get();
+  cudaEventRecord(ev[0], m->stream);
+  w->prof.marks.push_back({kind, {ev[0], ev[1]}});
+}
+
+static void prof_end(ua_mesh* m, cudaEvent_t* ev) {
+  if (!m->work->prof.on) return;
+  cudaEventRecord(ev[1], m->stream);
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// Dof-level CSR rows of node g (all ndof components).
+__global__ void k_dof_csr(DevMesh M, int* rowptr, int* colind, int* diagpos) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= M.nn) return;
+  const int s = M.node_sys[g];
+  const int no = M.sys_node_off[s], nn_s = M.sys_node_off[s + 1] - no;
+  const int doff = M.sys_dof_off[s];
+  const int np0 = M.nodeptr[g], deg = M.nodeptr[g + 1] - np0;
+  const int lp = np0 - M.nodeptr[no];
+  const int nd = M.ndof;
+  int kd = 0;
+  for (int k = 0; k < deg; ++k)
+    if (M.nodecol[np0 + k] == g) kd = k;
+  for (int c = 0; c < nd; ++c) {
+    const int dof = doff + c * nn_s + (g - no);
+    const int start = M.sys_knz_off[s] + c * nd * M.sys_nnzn[s] + nd * lp;
+    rowptr[dof] = start;
+    diagpos[dof] = start + c * deg + kd;
+    for (int b = 0; b < nd; ++b)
+      for (int k = 0; k < deg; ++k) colind[start + b * deg + k] = doff + b * nn_s + (M.nodecol[np0 + k] - no);
+  }
+}
+
+// Calc_bs_From_hBS.m:71-79,109 (nodal flotation mask, b and s).
+__global__ void k_calc_bs(int nn, const int* node_sys, const SysScal* scal, double kH, double Hh0, const double* h,
+                          const double* S, const double* B, const double* rho, double* s) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nn) return;
+  const double rhow = scal[node_sys[g]].rhow;
+  const double hf = rhow * (S[g] - B[g]) / rho[g];
+  const double GF = heaviside_approx(kH, h[g] - hf, Hh0);
+  const double bfloat = S[g] - rho[g] * h[g] / rhow;
+  const double b = GF * B[g] + (1 - GF) * bfloat;
+  s[g] = b + h[g];
+}
+
+template <typename KT, typename VT>
+__global__ void k_invdiag(int n, const KT* K, const int* diagpos, const unsigned char* cmask, VT* invd) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double d = (double)K[diagpos[i]];
+  invd[i] = (VT)((cmask[i] || d == 0.0) ? 0.0 : 1.0 / d);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block reduction of up to 4 values; thread 0 writes part[j*nrb + blk].
+template <int NV>
+__device__ __forceinline__ void block_partials(double (&v)[NV], double* part, int nrb, int blk) {
+  __shared__ double red[NV][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double t = warp_sum(v[j]);
+    if (lane == 0) red[j][w] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double t = 0;
+      for (int i = 0; i < nw; ++i) t += red[j][i];
+      part[j * nrb + blk] = t;
+    }
+  }
+}
+
+// Row-block SpMV with LPR lanes per row: y = mask(K x) (or mask(f - K x) in init mode).
+template <typename KT, typename XT, int LPR>
+__device__ __forceinline__ double row_dot(const int* rowptr, const int* colind, const KT* K, const XT* x, int row,
+                                          bool valid, int lane) {
+  // every lane of the warp reaches the shuffles; `valid` masks rows past the block end
+  double acc = 0;
+  if (valid) {
+    const int r0 = rowptr[row], r1 = rowptr[row + 1];
+    for (int j = r0 + lane; j < r1; j += LPR) acc += (double)K[j] * (double)x[colind[j]];
+  }
+#pragma unroll
+  for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+  return acc;
+}
+
+// PCG initial residual: r = mask(f - K x0), z = invd r, p = z; partials rz, rr.
+template <typename KT, typename VT, int LPR>
+__global__ void __launch_bounds__(256) k_pcg_init(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
+                                                  const int* rowptr, const int* colind, const KT* K,
+                                                  const double* x0, const double* f, const unsigned char* cmask,
+                                                  const VT* invd, VT* r, VT* z, VT* p, double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double v[2] = {0, 0};
+  if (sel[s]) {
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread
+      const int row = row0 + grp;
+      const bool valid = row < re;
+      double ax = row_dot<KT, double, LPR>(rowptr, colind, K, x0, row, valid, lane);
+      if (valid && lane == 0) {
+        double rv = cmask[row] ? 0.0 : f[row] - ax;
+        VT rr = (VT)rv;
+        VT zz = (VT)((double)invd[row] * (double)rr);
+        r[row] = rr; z[row] = zz; p[row] = zz;
+        v[0] += (double)rr * (double)zz;
+        v[1] += (double)rr * (double)rr;
+      }
+    }
+  }
+  block_partials<2>(v, part, nrb, blk);
+}
+
+// q = mask(K p); partial p.q
+template <typename KT, typename VT, int LPR>
+__global__ void __launch_bounds__(256) k_pcg_spmv(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
+                                                  const int* done, const int* rowptr, const int* colind,
+                                                  const KT* K, const VT* p, const unsigned char* cmask, VT* q,
+                                                  double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double v[1] = {0};
+  if (sel[s] && !done[s]) {
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread
+      const int row = row0 + grp;
+      const bool valid = row < re;
+      double ax = row_dot<KT, VT, LPR>(rowptr, colind, K, p, row, valid, lane);
+      if (valid && lane == 0) {
+        double qv = cmask[row] ? 0.0 : ax;
+        q[row] = (VT)qv;
+        v[0] += (double)p[row] * qv;
+      }
+    }
+  }
+  block_partials<1>(v, part, nrb, blk);
+}
+
+// x += alpha p; r -= alpha q; z = invd r; partials rz, rr
+template <typename VT>
+__global__ void __launch_bounds__(256) k_pcg_update1(const int* rb_start, const int* rb_sys, int nrb,
+                                                     const int* sel, const int* done, const double* sysv,
+                                                     int nsys, double* x, VT* r, VT* z, const VT* p, const VT* q,
+                                                     const VT* invd, double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double v[2] = {0, 0};
+  if (sel[s] && !done[s]) {
+    const double alpha = sysv[SV_ALPHA * nsys + s];
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    for (int i = rs + threadIdx.x; i < re; i += blockDim.x) {
+      x[i] += alpha * (double)p[i];
+      VT rr = (VT)((double)r[i] - alpha * (double)q[i]);
+      VT zz = (VT)((double)invd[i] * (double)rr);
+      r[i] = rr; z[i] = zz;
+      v[0] += (double)rr * (double)zz;
+      v[1] += (double)rr * (double)rr;
+    }
+  }
+  block_partials<2>(v, part, nrb, blk);
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(256) k_pcg_update2(const int* rb_start, const int* rb_sys, const int* sel,
+                                                     const int* done, const double* sysv, int nsys, VT* p,
+                                                     const VT* z) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const double beta = sysv[SV_BETA * nsys + s];
+  const int rs = rb_start[blk], re = rb_start[blk + 1];
+  for (int i = rs + threadIdx.x; i < re; i += blockDim.x) p[i] = (VT)((double)z[i] + beta * (double)p[i]);
+}
+
+// Sum NV partial arrays of one system in a fixed order.
+template <int NV>
+__device__ __forceinline__ void sys_sum(const double* part, int nrb, int b0, int b1, double (&out)[NV]) {
+  __shared__ double red[NV][kRedThreads];
+  double acc[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) acc[j] = 0;
+  for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] += part[j * nrb + b];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) red[j][threadIdx.x] = acc[j];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+#pragma unroll
+      for (int j = 0; j < NV; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + st];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < NV; ++j) out[j] = red[j][0];
+}
+
+// stage: 0 = init (rz, rr0), 1 = alpha (pq), 2 = beta (rz_new, rr)
+__global__ void k_pcg_reduce(int stage, const int* sys_rb_off, int nrb, const int* sel, int* done, int* its,
+                             int* status, double* sysv, int nsys, const double* part, int maxit) {
+  const int s = blockIdx.x;
+  if (!sel[s] || (stage > 0 && done[s])) return;
+  const int b0 = sys_rb_off[s], b1 = sys_rb_off[s + 1];
+  if (stage == 1) {
+    double o[1];
+    sys_sum<1>(part, nrb, b0, b1, o);
+    if (threadIdx.x == 0) {
+      const double pq = o[0];
+      if (!(pq > 0)) {  // not positive definite on the free dofs, or breakdown
+        status[s] = 1;
+        done[s] = 1;
+        sysv[SV_ALPHA * nsys + s] = 0;
+      } else {
+        sysv[SV_ALPHA * nsys + s] = sysv[SV_RZ * nsys + s] / pq;
+      }
+    }
+    return;
+  }
+  double o[2];
+  sys_sum<2>(part, nrb, b0, b1, o);
+  if (threadIdx.x != 0) return;
+  if (stage == 0) {
+    sysv[SV_RZ * nsys + s] = o[0];
+    sysv[SV_RR0 * nsys + s] = o[1];
+    sysv[SV_RR * nsys + s] = o[1];
+    its[s] = 0;
+    status[s] = 0;
+    done[s] = (o[1] == 0.0) ? 1 : 0;
+    return;
+  }
+  const double rz_new = o[0], rr = o[1];
+  its[s] += 1;
+  sysv[SV_RR * nsys + s] = rr;
+  sysv[SV_BETA * nsys + s] = rz_new / sysv[SV_RZ * nsys + s];
+  sysv[SV_RZ * nsys + s] = rz_new;
+  if (rr <= sysv[SV_TOL2 * nsys + s] * sysv[SV_RR0 * nsys + s] || its[s] >= maxit || !(rr == rr)) done[s] = 1;
+}
+
+// Constraint rows of the Newton system (mask form):
+// dX[dof_c] = grhs_c = c_c - X[dof_c] (particular solution x_p = L' g).
+__global__ void k_con_particular(int nc, const int* con_dof, const int* con_sys, const int* sel,
+                                 const double* con_rhs, const double* X, double* dX, double* grhs) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc || !sel[con_sys[c]]) return;
+  const int d = con_dof[c];
+  const double gv = con_rhs[c] - X[d];
+  grhs[c] = gv;
+  dX[d] = gv;
+}
+
+// dl_c = (frhs - K dX)[dof_c]  (ABfgPreEliminate.m:138 with B a selection)
+template <typename KT>
+__global__ void k_con_multiplier(int nc, const int* con_dof, const int* con_sys, const int* sel, const int* rowptr,
+                                 const int* colind, const KT* K, const double* dX, const double* frhs,
+                                 double* dlam) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc || !sel[con_sys[c]]) return;
+  const int d = con_dof[c];
+  double acc = 0;
+  for (int j = rowptr[d]; j < rowptr[d + 1]; ++j) acc += (double)K[j] * dX[colind[j]];
+  dlam[c] = frhs[d] - acc;
+}
+
+// frhs = -R - L' l  (SSTREAM2dNR2.m:235)
+__global__ void k_frhs(const int* rb_start, const int* rb_sys, const int* sel, const double* R, const int* dof_con,
+                       const double* lam, double* frhs) {
+  const int blk = blockIdx.x;
+  if (!sel[rb_sys[blk]]) return;
+  for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) {
+    const int c = dof_con[i];
+    frhs[i] = -R[i] - (c >= 0 ? lam[c] : 0.0);
+  }
+}
+
+// Cost function rows (CalcCostFunctionNR.m:24-41): f = -R - L'(l + gamma dl);
+// partials sum f^2 and sum f.dX
+__global__ void __launch_bounds__(256) k_cost_rows(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
+                                                   const double* R, const int* dof_con, const double* lam,
+                                                   const double* dlam, const double* gamma, const double* dX,
+                                                   double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double v[2] = {0, 0};
+  if (sel[s]) {
+    const double gm = gamma ? gamma[s] : 0.0;
+    for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) {
+      const int c = dof_con ? dof_con[i] : -1;
+      double f = -R[i];
+      if (c >= 0) f -= lam[c] + gm * dlam[c];
+      v[0] += f * f;
+      if (dX) v[1] += f * dX[i];
+    }
+  }
+  block_partials<2>(v, part, nrb, blk);
+}
+
+// Per-system cost: adds the constraint rows g = c - L(X + gamma dX), then
+// rForce = (f'f + g'g)/Normalisation and D2 = [f;g]'[dX;dl].
+__global__ void k_cost_reduce(const int* sys_rb_off, int nrb, const int* sel, const double* part, int nsys,
+                              double* sysv, const int* sys_con_off, const int* con_dof, const double* con_rhs,
+                              const double* X, const double* dX, const double* dlam, const double* gamma,
+                              int write_norm) {
+  const int s = blockIdx.x;
+  if (!sel[s]) return;
+  double o[2];
+  sys_sum<2>(part, nrb, sys_rb_off[s], sys_rb_off[s + 1], o);
+  if (threadIdx.x != 0) return;
+  double gg = 0, gd = 0;
+  if (sys_con_off) {
+    const double gm = gamma ? gamma[s] : 0.0;
+    for (int c = sys_con_off[s]; c < sys_con_off[s + 1]; ++c) {
+      const int d = con_dof[c];
+      const double xv = X[d] + (dX ? gm * dX[d] : 0.0);
+      const double gv = con_rhs[c] - xv;
+      gg += gv * gv;
+      if (dlam) gd += gv * dlam[c];
+    }
+  }
+  if (write_norm) {
+    sysv[SV_NORM * nsys + s] = o[0] + 1000.0 * 2.220446049250313e-16;  // fext0'fext0+1000*eps
+    return;
+  }
+  sysv[SV_FF * nsys + s] = (o[0] + gg) / sysv[SV_NORM * nsys + s];
+  sysv[SV_FD * nsys + s] = o[1] + gd;
+}
+
+// X += gamma dX, l += gamma dl for selected systems.
+__global__ void k_newton_update(const int* rb_start, const int* rb_sys, const int* sel, const double* gamma,
+                                double* X, const double* dX) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s]) return;
+  const double gm = gamma[s];
+  for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) X[i] += gm * dX[i];
+}
+
+__global__ void k_lam_update(int nc, const int* con_sys, const int* sel, const double* gamma, double* lam,
+                             const double* dlam) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc || !sel[con_sys[c]]) return;
+  lam[c] += gamma[con_sys[c]] * dlam[c];
+}
+
+__global__ void k_set_con_values(int nc, const int* con_dof, const int* con_sys, const int* sel,
+                                 const double* con_rhs, double* X) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nc && (!sel || sel[con_sys[c]])) X[con_dof[c]] = con_rhs[c];
+}
+
+__global__ void k_zero_sel(const int* rb_start, const int* rb_sys, const int* sel, double* v) {
+  const int blk = blockIdx.x;
+  if (!sel[rb_sys[blk]]) return;
+  for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) v[i] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+
+template <class T>
+static T* walloc(ua_mesh* m, size_t n) {
+  return (T*)dev_alloc(m, n * sizeof(T));
+}
+
+static int ensure_work(ua_mesh* m) {
+  if (m->work) return UA_OK;
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  Work* w = new Work();
+  const int nsys = m->dm.nsys, N = m->ndof_total, NN = m->nn_total;
+  w->nsys = nsys;
+  // row blocks
+  std::vector<int> rb_start, rb_sys;
+  w->h_sys_rb_off.assign(nsys + 1, 0);
+  for (int s = 0; s < nsys; ++s) {
+    for (int r = m->h_dof_off[s]; r < m->h_dof_off[s + 1]; r += kRB) {
+      rb_start.push_back(r);
+      rb_sys.push_back(s);
+    }
+    w->h_sys_rb_off[s + 1] = (int)rb_start.size();
+  }
+  rb_start.push_back(N);
+  w->nrb = (int)rb_sys.size();
+  bool ok = true;
+  auto up = [&](const std::vector<int>& v) -> int* {
+    int* d = walloc<int>(m, v.size());
+    if (!d) { ok = false; return nullptr; }
+    cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice);
+    return d;
+  };
+  w->rb_start = up(rb_start);
+  w->rb_sys = up(rb_sys);
+  w->sys_rb_off = up(w->h_sys_rb_off);
+  w->rowptr = walloc<int>(m, N + 1);
+  w->colind = walloc<int>(m, (size_t)m->nnz_total);
+  w->diagpos = walloc<int>(m, N);
+  double** fp[] = {&w->h, &w->s, &w->S, &w->B, &w->rho, &w->A, &w->n, &w->C, &w->m};
+  for (auto f : fp) { *f = walloc<double>(m, NN); ok = ok && *f; }
+  w->scal = walloc<SysScal>(m, nsys);
+  double** dv[] = {&w->X, &w->X0, &w->dX, &w->R, &w->frhs, &w->Tint, &w->Fext};
+  for (auto f : dv) { *f = walloc<double>(m, N); ok = ok && *f; }
+  void** kv[] = {&w->kr, &w->kz, &w->kp, &w->kq, &w->invd};
+  for (auto f : kv) { *f = walloc<double>(m, N); ok = ok && *f; }
+  w->part = walloc<double>(m, 4 * (size_t)w->nrb);
+  w->sysv = walloc<double>(m, SV_COUNT * (size_t)nsys);
+  w->done = walloc<int>(m, nsys);
+  w->its = walloc<int>(m, nsys);
+  w->status = walloc<int>(m, nsys);
+  w->sel = walloc<int>(m, nsys);
+  w->gamma = walloc<double>(m, nsys);
+  w->cmask = walloc<unsigned char>(m, N);
+  w->dof_con = walloc<int>(m, N);
+  ok = ok && w->rowptr && w->colind && w->diagpos && w->scal && w->part && w->sysv && w->done && w->its &&
+       w->status && w->sel && w->gamma && w->cmask && w->dof_con && w->rb_start && w->rb_sys && w->sys_rb_off;
+  if (!ok) { delete w; return set_error(UA_ERR_OOM, "device allocation of work buffers failed"); }
+  if (cudaMallocHost(&w->h_sysv, SV_COUNT * sizeof(double) * nsys) != cudaSuccess ||
+      cudaMallocHost(&w->h_int, 4 * sizeof(int) * (nsys + 1)) != cudaSuccess ||
+      cudaMallocHost(&w->h_gamma, sizeof(double) * nsys) != cudaSuccess) {
+    delete w;
+    return set_error(UA_ERR_OOM, "pinned host allocation failed");
+  }
+  k_dof_csr<<<(NN + 127) / 128, 128, 0, m->stream>>>(m->dm, w->rowptr, w->colind, w->diagpos), ++g_launches;
+  int nnz = (int)m->nnz_total;
+  UA_CUDA_TRY(cudaMemcpyAsync(w->rowptr + N, &nnz, sizeof(int), cudaMemcpyHostToDevice, m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  m->work = w;
+  return UA_OK;
+}
+
+static int ensure_K(ua_mesh* m, int prec) {
+  Work* w = m->work;
+  if (prec == UA_PREC_MIXED) {
+    if (!w->Kf) w->Kf = walloc<float>(m, (size_t)m->nnz_total);
+    if (!w->Kf) return set_error(UA_ERR_OOM, "device allocation of the FP32 tangent failed");
+  } else {
+    if (!w->Kd) w->Kd = walloc<double>(m, (size_t)m->nnz_total);
+    if (!w->Kd) return set_error(UA_ERR_OOM, "device allocation of the FP64 tangent failed");
+  }
+  return UA_OK;
+}
+
+static UvPhys make_phys(const ua_params* p) {
+  UvPhys P;
+  P.kH = p->kH; P.Hh0 = p->Hh0; P.SpeedZero = p->SpeedZero; P.EpsZero = p->EpsZero; P.etaZero = p->etaZero;
+  P.Czero = p->Czero; P.Cmin = p->Cmin; P.AGlenmin = p->AGlenmin;
+  P.Dvisk = p->Picard ? 0.0 : p->NRviscosity;  // uvMatrixAssemblySSTREAM.m:67-71
+  return P;
+}
+
+static bool any_nan(const double* v, int n) {
+  for (int i = 0; i < n; ++i)
+    if (v[i] != v[i]) return true;
+  return false;
+}
+
+// Upload nodal fields of every system (host or device pointers) and compute s.
+static int upload_fields(ua_mesh* m, const ua_params* p, const ua_fields* F, int nF) {
+  Work* w = m->work;
+  std::vector<SysScal> sc(m->dm.nsys);
+  for (int s = 0; s < m->dm.nsys; ++s) {
+    const ua_fields& f = F[nF == 1 ? 0 : s];
+    const int no = m->h_node_off[s], nn = m->sys[s].nn;
+    const double* src[] = {f.h, f.S, f.B, f.rho, f.AGlen, f.n, f.C, f.m};
+    double* dst[] = {w->h, w->S, w->B, w->rho, w->A, w->n, w->C, w->m};
+    const char* names[] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
+    for (int k = 0; k < 8; ++k) {
+      if (!src[k]) return set_error(UA_ERR_INVALID, "system %d: null field pointer %s", s, names[k]);
+      // SSTREAM2dNR2.m:42-65: NaN in C or A (warning + NaN solution in the
+      // reference) and NaN in S, h, rho (error) all stop the solve here.
+      if (f.location == UA_HOST && any_nan(src[k], nn))
+        return set_error(UA_ERR_NAN_INPUT, "SSTREAM2dNR2: nan in %s (system %d)", names[k], s);
+      UA_CUDA_TRY(cudaMemcpyAsync(dst[k] + no, src[k], nn * sizeof(double),
+                                  f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                  m->stream));
+    }
+    sc[s].rhow = f.rhow; sc[s].g = f.g; sc[s].ca = std::cos(f.alpha); sc[s].sa = std::sin(f.alpha);
+    sc[s].dt = f.dt;
+  }
+  UA_CUDA_TRY(cudaMemcpyAsync(w->scal, sc.data(), sc.size() * sizeof(SysScal), cudaMemcpyHostToDevice, m->stream));
+  k_calc_bs<<<(m->nn_total + 255) / 256, 256, 0, m->stream>>>(m->nn_total, m->dm.node_sys, w->scal, p->kH, p->Hh0,
+                                                               w->h, w->S, w->B, w->rho, w->s), ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
+  return UA_OK;
+}
+
+// Velocities of the fields into the dof vector X.
+static int upload_velocity(ua_mesh* m, const ua_fields* F, int nF) {
+  Work* w = m->work;
+  for (int s = 0; s < m->dm.nsys; ++s) {
+    const ua_fields& f = F[nF == 1 ? 0 : s];
+    const int d0 = m->h_dof_off[s], nn = m->sys[s].nn;
+    if (!f.ub || !f.vb) return set_error(UA_ERR_INVALID, "null ub/vb");
+    if (f.location == UA_HOST && (any_nan(f.ub, nn) || any_nan(f.vb, nn)))
+      return set_error(UA_ERR_NAN_INPUT, "uvMatrixAssembly:NaN NaN in F.ub or F.vb");
+    auto kind = f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0, f.ub, nn * sizeof(double), kind, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0 + nn, f.vb, nn * sizeof(double), kind, m->stream));
+  }
+  return UA_OK;
+}
+
+// BCs2MLC.m:19-25 + CreateLuv.m:28-76 + ScaleL.m for fixed-node BCs: one unit row
+// per unique fixed node (first occurrence's value), u rows then v rows.
+static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
+  Work* w = m->work;
+  const int nsys = m->dm.nsys;
+  std::vector<int> con_dof, con_sys, sys_off(nsys + 1, 0);
+  std::vector<double> rhs;
+  for (int s = 0; s < nsys; ++s) {
+    const ua_bcs* b = bcs ? &bcs[nB == 1 ? 0 : s] : nullptr;
+    if (b && (b->n_utied > 0 || b->n_vtied > 0))
+      return set_error(UA_ERR_INVALID, "tied-node constraints are not supported by the device solver");
+    const int nn = m->sys[s].nn, d0 = m->h_dof_off[s];
+    const int base = 0;  // indices are 0-based at this layer
+    for (int comp = 0; b && comp < 2; ++comp) {
+      int n = comp == 0 ? b->n_ufixed : b->n_vfixed;
+      const int* nodes = comp == 0 ? b->ufixed_node : b->vfixed_node;
+      const double* vals = comp == 0 ? b->ufixed_value : b->vfixed_value;
+      std::vector<std::pair<int, int>> idx;  // (node, first position)
+      for (int i = 0; i < n; ++i) {
+        int nd = nodes[i] - base;
+        if (nd < 0 || nd >= nn) return set_error(UA_ERR_INVALID, "system %d: fixed node index out of range", s);
+        idx.push_back({nd, i});
+      }
+      std::stable_sort(idx.begin(), idx.end(), [](auto& x, auto& y) { return x.first < y.first; });
+      for (size_t i = 0; i < idx.size(); ++i) {
+        if (i > 0 && idx[i].first == idx[i - 1].first) continue;  // unique, first occurrence
+        double v = vals ? vals[idx[i].second] : 0.0;
+        if (v != v) return set_error(UA_ERR_NAN_INPUT, "nan in fixed value");
+        con_dof.push_back(d0 + comp * nn + idx[i].first);
+        con_sys.push_back(s);
+        rhs.push_back(v);
+      }
+    }
+    sys_off[s + 1] = (int)con_dof.size();
+  }
+  const int nc = (int)con_dof.size();
+  if (nc > w->nc || !w->con_dof) {
+    int cap = std::max(nc, 1);
+    w->con_dof = walloc<int>(m, cap);
+    w->con_sys = walloc<int>(m, cap);
+    w->con_rhs = walloc<double>(m, cap);
+    w->lam = walloc<double>(m, cap);
+    w->dlam = walloc<double>(m, cap);
+    w->grhs = walloc<double>(m, cap);
+    if (!w->sys_con_off) w->sys_con_off = walloc<int>(m, nsys + 1);
+    if (!w->con_dof || !w->con_sys || !w->con_rhs || !w->lam || !w->dlam || !w->grhs || !w->sys_con_off)
+      return set_error(UA_ERR_OOM, "constraint allocation failed");
+  }
+  w->nc = nc;
+  w->h_sys_con_off = sys_off;
+  if (nc) {
+    UA_CUDA_TRY(cudaMemcpyAsync(w->con_dof, con_dof.data(), nc * sizeof(int), cudaMemcpyHostToDevice, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->con_sys, con_sys.data(), nc * sizeof(int), cudaMemcpyHostToDevice, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->con_rhs, rhs.data(), nc * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+  }
+  UA_CUDA_TRY(cudaMemcpyAsync(w->sys_con_off, sys_off.data(), (nsys + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                              m->stream));
+  // dof masks
+  std::vector<unsigned char> cmask(m->ndof_total, 0);
+  std::vector<int> dof_con(m->ndof_total, -1);
+  for (int c = 0; c < nc; ++c) { cmask[con_dof[c]] = 1; dof_con[con_dof[c]] = c; }
+  UA_CUDA_TRY(cudaMemcpyAsync(w->cmask, cmask.data(), cmask.size(), cudaMemcpyHostToDevice, m->stream));
+  UA_CUDA_TRY(cudaMemcpyAsync(w->dof_con, dof_con.data(), dof_con.size() * sizeof(int), cudaMemcpyHostToDevice,
+                              m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return UA_OK;
+}
+
+static int set_sel(ua_mesh* m, const std::vector<int>& sel) {
+  Work* w = m->work;
+  for (int s = 0; s < w->nsys; ++s) w->h_int[s] = sel[s];
+  UA_CUDA_TRY(cudaMemcpyAsync(w->sel, w->h_int, w->nsys * sizeof(int), cudaMemcpyHostToDevice, m->stream));
+  return UA_OK;
+}
+
+static int set_gamma(ua_mesh* m, const std::vector<double>& g) {
+  Work* w = m->work;
+  for (int s = 0; s < w->nsys; ++s) w->h_gamma[s] = g[s];
+  UA_CUDA_TRY(cudaMemcpyAsync(w->gamma, w->h_gamma, w->nsys * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+  return UA_OK;
+}
+
+// Residual-only or residual+tangent assembly of the selected systems at X (+gamma dX).
+static int assemble(ua_mesh* m, const ua_params* p, bool withK, bool useDir, const double* X, bool parts) {
+  Work* w = m->work;
+  UvIn in{w->h, w->s, w->S, w->B, w->rho, w->A, w->n, w->C, w->m, X, useDir ? w->dX : nullptr,
+          useDir ? w->gamma : nullptr, w->scal, w->sel};
+  bool fp32 = p->precision == UA_PREC_MIXED;
+  UvOut out{w->R, withK ? (fp32 ? (void*)w->Kf : (void*)w->Kd) : nullptr, parts ? w->Tint : nullptr,
+            parts ? w->Fext : nullptr};
+  cudaEvent_t ev[2];
+  prof_begin(m, withK ? PK_ASMK : PK_ASMR, ev);
+  cudaError_t e = launch_uv_assembly(m, make_phys(p), in, out, withK, fp32);
+  prof_end(m, ev);
+  ++g_launches;
+  if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "uv assembly launch: %s", cudaGetErrorString(e));
+  return UA_OK;
+}
+
+// Cost function of every selected system at X + gamma dX with direction (dX, dl):
+// CalcCostFunctionNR.m:14-41.  Result in sysv[SV_FF] (rForce) and sysv[SV_FD] (D2).
+static int cost_eval(ua_mesh* m, const ua_params* p, bool useDir) {
+  Work* w = m->work;
+  int rc = assemble(m, p, false, useDir, w->X, false);
+  if (rc) return rc;
+  k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, w->dof_con, w->lam,
+                                             w->dlam, useDir ? w->gamma : nullptr, w->dX, w->part), ++g_launches;
+  k_cost_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, w->nsys, w->sysv,
+                                                         w->sys_con_off, w->con_dof, w->con_rhs, w->X,
+                                                         useDir ? w->dX : nullptr, w->dlam,
+                                                         useDir ? w->gamma : nullptr, 0), ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
+  UA_CUDA_TRY(cudaMemcpyAsync(w->h_sysv, w->sysv, SV_COUNT * w->nsys * sizeof(double), cudaMemcpyDeviceToHost,
+                              m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return UA_OK;
+}
+
+template <typename KT, typename VT>
+static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, std::vector<int>& its_out) {
+  Work* w = m->work;
+  const int N = m->ndof_total;
+  const int lpr = (m->nod == 3 && m->ndof == 2) ? 8 : 16;
+  // per-system tolerance
+  for (int s = 0; s < w->nsys; ++s) w->h_sysv[s] = p->krylov_rtol * p->krylov_rtol;
+  UA_CUDA_TRY(cudaMemcpyAsync(w->sysv + SV_TOL2 * w->nsys, w->h_sysv, w->nsys * sizeof(double),
+                              cudaMemcpyHostToDevice, m->stream));
+  k_invdiag<KT, VT><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, (VT*)w->invd), ++g_launches;
+  // particular solution on the constrained dofs
+  k_zero_sel<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->dX), ++g_launches;
+  if (w->nc)
+    k_con_particular<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs,
+                                                                 w->X, w->dX, w->grhs), ++g_launches;
+  VT *r = (VT*)w->kr, *z = (VT*)w->kz, *pp = (VT*)w->kp, *q = (VT*)w->kq;
+  const VT* invd = (const VT*)w->invd;
+  if (lpr == 8)
+    k_pcg_init<KT, VT, 8><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr,
+                                                         w->colind, K, w->dX, w->frhs, w->cmask, invd, r, z, pp,
+                                                         w->part), ++g_launches;
+  else
+    k_pcg_init<KT, VT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr,
+                                                          w->colind, K, w->dX, w->frhs, w->cmask, invd, r, z, pp,
+                                                          w->part), ++g_launches;
+  k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(0, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                        w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
+  const int chunk = 16;
+  int it = 0;
+  while (true) {
+    for (int k = 0; k < chunk; ++k) {
+      cudaEvent_t ev[2];
+      prof_begin(m, PK_SPMV, ev);
+      if (lpr == 8)
+        k_pcg_spmv<KT, VT, 8><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done,
+                                                             w->rowptr, w->colind, K, pp, w->cmask, q, w->part), ++g_launches;
+      else
+        k_pcg_spmv<KT, VT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done,
+                                                              w->rowptr, w->colind, K, pp, w->cmask, q, w->part), ++g_launches;
+      prof_end(m, ev);
+      k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                            w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+      k_pcg_update1<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->sysv,
+                                                       w->nsys, w->dX, r, z, pp, q, invd, w->part), ++g_launches;
+      k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                            w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+      k_pcg_update2<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys,
+                                                       pp, z), ++g_launches;
+    }
+    it += chunk;
+    UA_CUDA_TRY(cudaGetLastError());
+    UA_CUDA_TRY(cudaMemcpyAsync(w->h_int, w->done, w->nsys * sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+    UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    bool all = true;
+    for (int s = 0; s < w->nsys; ++s) all = all && (w->h_int[s] || !its_out[s]);
+    if (all || it >= p->krylov_maxit + chunk) break;
+  }
+  if (w->nc)
+    k_con_multiplier<KT><<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel,
+                                                                     w->rowptr, w->colind, K, w->dX, w->frhs,
+                                                                     w->dlam), ++g_launches;
+  UA_CUDA_TRY(cudaMemcpyAsync(w->h_int, w->its, w->nsys * sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  for (int s = 0; s < w->nsys; ++s) its_out[s] = its_out[s] ? w->h_int[s] : 0;
+  return UA_OK;
+}
+
+// Solve [K L';L 0][dX;dl] = [frhs;grhs] for the selected systems (sel set on device,
+// its_out[s] != 0 marks selected on input).
+static int linear_solve(ua_mesh* m, const ua_params* p, std::vector<int>& its_out) {
+  Work* w = m->work;
+  if (p->precision == UA_PREC_MIXED) return pcg_t<float, float>(m, p, w->Kf, its_out);
+  return pcg_t<double, double>(m, p, w->Kd, its_out);
+}
+
+// uvResidualsCriteria.m:1-23
+static bool residual_criteria(const ua_params* p, double rForce, double rWork, int iteration, double gamma) {
+  const double *a, *o;
+  if (gamma > std::max(p->uvExitBackTrackingStepLength, p->BacktrackingGammaMin)) {
+    a = p->uvDesiredWorkAndForceTolerances; o = p->uvDesiredWorkOrForceTolerances;
+  } else {
+    a = p->uvAcceptableWorkAndForceTolerances; o = p->uvAcceptableWorkOrForceTolerances;
+  }
+  return (rWork < a[0] && rForce < a[1]) && (rWork < o[0] || rForce < o[1]) && iteration >= p->NRitmin;
+}
+
+struct SysState {
+  bool active = false, converged = false;
+  int iteration = 0, iarm = 0;
+  double r = 0, rForce = 0, rWork = 0, gamma = 1, ResidualReduction = 1e10;
+  double r0 = 0, rForce0 = 0, rWork0 = 0, r1 = 0, rForce1 = 0, rWork1 = 0;
+  int kits = 0;
+  // line search
+  bool in_ls = false;
+  BackTrack bt;
+  std::vector<double> ls_g, ls_rF, ls_D2;
+};
+
+static double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Newton driver for the systems with run[s]=1 (SSTREAM2dNR2.m:100-392).
+static int newton_run(ua_mesh* m, const ua_params* p, std::vector<int> run, std::vector<ua_newton_report*>& rep,
+                      std::vector<SysState>& st) {
+  Work* w = m->work;
+  const int nsys = w->nsys;
+  double t_asm = 0, t_sol = 0;
+  int rc;
+  // make the iterate feasible (:101-104) and compute fext0 at ZeroFields (:122-124)
+  UA_CUDA_TRY(cudaMemsetAsync(w->X0, 0, m->ndof_total * sizeof(double), m->stream));
+  if ((rc = set_sel(m, run))) return rc;
+  if (w->nc) {
+    k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel,
+                                                                 w->con_rhs, w->X), ++g_launches;
+    k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel,
+                                                                 w->con_rhs, w->X0), ++g_launches;
+  }
+  {
+    if ((rc = assemble(m, p, false, false, w->X0, false))) return rc;
+    k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, nullptr, nullptr,
+                                               nullptr, nullptr, nullptr, w->part), ++g_launches;
+    k_cost_reduce<<<nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, nsys, w->sysv,
+                                                       nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                       nullptr, 1), ++g_launches;
+    UA_CUDA_TRY(cudaGetLastError());
+  }
+  // initial cost (:149-152) with zero direction
+  UA_CUDA_TRY(cudaMemsetAsync(w->dX, 0, m->ndof_total * sizeof(double), m->stream));
+  if (w->nc) UA_CUDA_TRY(cudaMemsetAsync(w->dlam, 0, w->nc * sizeof(double), m->stream));
+  if ((rc = cost_eval(m, p, false))) return rc;
+  for (int s = 0; s < nsys; ++s) {
+    if (!run[s]) continue;
+    st[s] = SysState();
+    st[s].active = true;
+    st[s].r = st[s].rForce = w->h_sysv[SV_FF * nsys + s];
+    st[s].rWork = 0;
+    st[s].gamma = 1;
+  }
+  std::vector<int> sel(nsys), its(nsys);
+  std::vector<double> gam(nsys, 0.0);
+  while (true) {
+    // convergence / iteration cap (:160-190)
+    bool any = false;
+    for (int s = 0; s < nsys; ++s) {
+      SysState& S = st[s];
+      if (!S.active) continue;
+      if (residual_criteria(p, S.rForce, S.rWork, S.iteration, S.gamma)) { S.converged = true; S.active = false; continue; }
+      if (S.iteration > p->NRitmax) { S.converged = false; S.active = false; continue; }
+      S.iteration++;
+      any = true;
+    }
+    if (!any) break;
+    for (int s = 0; s < nsys; ++s) sel[s] = st[s].active ? 1 : 0;
+    if ((rc = set_sel(m, sel))) return rc;
+    // R and K (:197-213); the interval criterion 1 (default) always refreshes K
+    double t0 = now_ms();
+    bool refreshK = false;
+    for (int s = 0; s < nsys; ++s)
+      if (st[s].active && (((st[s].iteration - 1) % std::max(1, p->ModifiedNRuvIntervalCriterion)) == 0 ||
+                           st[s].ResidualReduction > p->ModifiedNRuvReductionCriterion))
+        refreshK = true;
+    if ((rc = assemble(m, p, refreshK, false, w->X, false))) return rc;
+    k_frhs<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->R, w->dof_con, w->lam, w->frhs), ++g_launches;
+    UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    double t1 = now_ms();
+    t_asm += t1 - t0;
+    // linear solve (:242-257)
+    for (int s = 0; s < nsys; ++s) its[s] = sel[s];
+    if ((rc = linear_solve(m, p, its))) return rc;
+    double t2 = now_ms();
+    t_sol += t2 - t1;
+    for (int s = 0; s < nsys; ++s) if (sel[s]) st[s].kits = its[s];
+    // gamma=0 (:260-283)
+    for (int s = 0; s < nsys; ++s) gam[s] = 0.0;
+    if ((rc = set_gamma(m, gam))) return rc;
+    if ((rc = cost_eval(m, p, true))) return rc;
+    for (int s = 0; s < nsys; ++s) {
+      if (!sel[s]) continue;
+      SysState& S = st[s];
+      S.r0 = S.rForce0 = w->h_sysv[SV_FF * nsys + s];
+      double D2 = w->h_sysv[SV_FD * nsys + s];
+      S.rWork0 = D2 * D2;
+      if (S.iteration == 1 && residual_criteria(p, S.rForce0, S.rWork0, S.iteration, 1.0)) {
+        S.iteration -= 1; S.converged = true; S.active = false; sel[s] = 0;
+      }
+    }
+    // gamma=1 (:288)
+    for (int s = 0; s < nsys; ++s) gam[s] = 1.0;
+    if ((rc = set_sel(m, sel))) return rc;
+    if ((rc = set_gamma(m, gam))) return rc;
+    if ((rc = cost_eval(m, p, true))) return rc;
+    for (int s = 0; s < nsys; ++s) {
+      if (!sel[s]) continue;
+      SysState& S = st[s];
+      S.r1 = S.rForce1 = w->h_sysv[SV_FF * nsys + s];
+      double D2 = w->h_sysv[SV_FD * nsys + s];
+      S.rWork1 = D2 * D2;
+      if (S.r1 / S.r0 < p->NewtonAcceptRatio) {  // :290-296
+        S.in_ls = false;
+        S.gamma = 1.0; S.r = S.r1; S.rForce = S.rForce1; S.rWork = S.rWork1; S.iarm = 0;
+      } else {  // rLineminUa.m:57-135 (Newton-direction backtracking)
+        S.in_ls = true;
+        S.bt = BackTrack();
+        BTConfig& c = S.bt.cfg;
+        c.beta = p->BackTrackBeta; c.ExtrapolationRatio = p->BackTrackExtrapolationRatio;
+        c.MinXfracRel = p->BackTrackMinXfrac; c.GL = p->BackTrackGuardLower; c.GU = p->BackTrackGuardUpper;
+        c.NewtonAcceptRatio = p->NewtonAcceptRatio; c.GammaMin = 0.001; c.NLtol = p->NLtol;
+        c.MaxIterations = p->BackTrackMaxIterations; c.MaxExtrapolations = p->BackTrackMaxExtrapolations;
+        c.MaxFuncSame = p->BackTrackMaxFuncSame; c.allow_ext = p->LineSearchAllowedToUseExtrapolation != 0;
+        S.ls_g.assign({0.0, 1.0});
+        S.ls_rF.assign({S.rForce0, S.rForce1});
+        S.ls_D2.assign({std::sqrt(S.rWork0), std::sqrt(S.rWork1)});
+        S.bt.start(-2 * S.r0, 1.0, S.r0, S.r1);
+      }
+    }
+    // line-search rounds
+    while (true) {
+      bool need = false;
+      for (int s = 0; s < nsys; ++s) {
+        sel[s] = (st[s].active && st[s].in_ls && !st[s].bt.done) ? 1 : 0;
+        gam[s] = sel[s] ? st[s].bt.request : 0.0;
+        need = need || sel[s];
+      }
+      if (!need) break;
+      if ((rc = set_sel(m, sel))) return rc;
+      if ((rc = set_gamma(m, gam))) return rc;
+      if ((rc = cost_eval(m, p, true))) return rc;
+      for (int s = 0; s < nsys; ++s) {
+        if (!sel[s]) continue;
+        double rf = w->h_sysv[SV_FF * nsys + s], d2 = w->h_sysv[SV_FD * nsys + s];
+        st[s].ls_g.push_back(gam[s]); st[s].ls_rF.push_back(rf); st[s].ls_D2.push_back(d2);
+        st[s].bt.feed(rf);
+      }
+    }
+    // finish line searches, update (:313-371)
+    for (int s = 0; s < nsys; ++s) {
+      sel[s] = 0;
+      SysState& S = st[s];
+      if (!S.active) continue;
+      int bt_conv = 1;
+      if (S.in_ls) {
+        BackTrack& bt = S.bt;
+        double gN = bt.gmin, rN = bt.fmin;
+        if (rep[s] && gN < 0.75 && rN / S.r0 > 0.7) rep[s]->cauchy_fallbacks++;  // rLineminUa.m:96
+        S.iarm = bt.iarm;
+        bt_conv = bt.converged && !bt.error;
+        if (rN < S.r0) {
+          S.gamma = gN; S.r = rN; S.rForce = rN;
+          S.rWork = std::nan("");
+          for (size_t k = 0; k < S.ls_g.size(); ++k)
+            if (S.ls_g[k] == gN) { S.rWork = S.ls_D2[k] * S.ls_D2[k]; break; }
+        } else {
+          S.gamma = 0; S.r = S.r0; S.rForce = S.r0; S.rWork = std::nan("");
+        }
+      }
+      if (rep[s] && rep[s]->iters && rep[s]->n_iter_records < rep[s]->iters_capacity) {
+        ua_newton_iter& it = rep[s]->iters[rep[s]->n_iter_records++];
+        it.iteration = S.iteration; it.iarm = S.iarm; it.krylov_its = S.kits; it.direction = S.in_ls ? 1 : 0;
+        it.gamma = S.gamma; it.r0 = S.r0; it.r = S.r; it.rForce = S.rForce; it.rWork = S.rWork;
+      }
+      if (rep[s]) rep[s]->krylov_its_total += S.kits;
+      if (p->verbose)
+        fprintf(stderr, "NR-SSTREAM(uv)[%d]:%3d/%-2d g=%-14.7g , r/r0=%-14.7g ,  r0=%-14.7g , r=%-14.7g , rForce=%-14.7g , rWork=%-14.7g , pcg=%d\n",
+                s, S.iteration, S.iarm, S.gamma, S.r / S.r0, S.r0, S.r, S.rForce, S.rWork, S.kits);
+      if (!bt_conv) { S.converged = false; S.active = false; continue; }  // :322-327
+      sel[s] = 1;
+      gam[s] = S.gamma;
+      S.ResidualReduction = S.r / S.r0;
+    }
+    if ((rc = set_sel(m, sel))) return rc;
+    if ((rc = set_gamma(m, gam))) return rc;
+    k_newton_update<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->gamma, w->X, w->dX), ++g_launches;
+    if (w->nc)
+      k_lam_update<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_sys, w->sel, w->gamma, w->lam,
+                                                               w->dlam), ++g_launches;
+    UA_CUDA_TRY(cudaGetLastError());
+  }
+  for (int s = 0; s < nsys; ++s) {
+    if (!run[s] || !rep[s]) continue;
+    rep[s]->converged = st[s].converged ? 1 : 0;
+    rep[s]->iterations = st[s].iteration;
+    rep[s]->backtrack_steps = st[s].iarm;
+    rep[s]->r = st[s].r; rep[s]->rForce = st[s].rForce; rep[s]->rWork = st[s].rWork;
+    rep[s]->assembly_ms += t_asm; rep[s]->solve_ms += t_sol;
+  }
+  return UA_OK;
+}
+
+}  // namespace ua
+
+using namespace ua;
+
+extern "C" void ua_params_default(ua_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->kH = 1; p->Hh0 = 0;
+  p->SpeedZero = 1e-4; p->EpsZero = 1e-10; p->etaZero = 10;
+  p->Czero = 0; p->Cmin = 1e-20; p->AGlenmin = 1e-20;
+  p->Picard = 0; p->NRviscosity = 1;
+  p->NRitmax = 50; p->NRitmin = 1; p->NewtonAcceptRatio = 0.5; p->BacktrackingGammaMin = 1e-10;
+  p->LineSearchAllowedToUseExtrapolation = 0;
+  p->BackTrackBeta = 0.1; p->BackTrackMaxIterations = 50; p->BackTrackMaxExtrapolations = 50;
+  p->BackTrackExtrapolationRatio = 2.5; p->BackTrackMinXfrac = 1e-10; p->BackTrackMaxFuncSame = 3;
+  p->BackTrackGuardLower = 0.25; p->BackTrackGuardUpper = 0.95; p->NLtol = 1e-15;
+  const double inf = INFINITY;
+  double d[2] = {inf, 1e-15};
+  std::memcpy(p->uvDesiredWorkAndForceTolerances, d, sizeof d);
+  std::memcpy(p->uvDesiredWorkOrForceTolerances, d, sizeof d);
+  std::memcpy(p->uvAcceptableWorkAndForceTolerances, d, sizeof d);
+  std::memcpy(p->uvAcceptableWorkOrForceTolerances, d, sizeof d);
+  p->uvExitBackTrackingStepLength = 1e-10;
+  p->ModifiedNRuvIntervalCriterion = 1; p->ModifiedNRuvReductionCriterion = 0.5;
+  p->theta = 0.5; p->SUPG_beta0 = 1; p->uvh_SUPG_tauMultiplier = 1; p->uvh_SUPG_tau = 0;
+  std::memcpy(p->uvhDesiredWorkAndForceTolerances, d, sizeof d);
+  std::memcpy(p->uvhDesiredWorkOrForceTolerances, d, sizeof d);
+  p->uvhExitBackTrackingStepLength = 1e-3;
+  double a1[2] = {inf, 1e-6}, a2[2] = {1, 1e-8};
+  std::memcpy(p->uvhAcceptableWorkAndForceTolerances, a1, sizeof a1);
+  std::memcpy(p->uvhAcceptableWorkOrForceTolerances, a2, sizeof a2);
+  p->krylov_rtol = 1e-12; p->krylov_maxit = 20000; p->precision = UA_PREC_FP64;
+  p->patch_nodes = 0; p->verbose = 0;
+}
+
+extern "C" int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs, int32_t mode,
+                              double* R, double* Kvals, double* Tint, double* Fext) {
+  if (!m || !p || !F) return set_error(UA_ERR_INVALID, "ua_uv_assemble: null argument");
+  if (m->ndof != 2) return set_error(UA_ERR_INVALID, "ua_uv_assemble needs a ndof=2 mesh handle");
+  if (m->dm.nsys != 1) return set_error(UA_ERR_INVALID, "ua_uv_assemble takes a single-mesh handle");
+  if (mode != UA_ASM_R && mode != UA_ASM_RK && mode != UA_ASM_ZERO_R) return set_error(UA_ERR_INVALID, "bad mode");
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  int rc;
+  if ((rc = ensure_work(m))) return rc;
+  Work* w = m->work;
+  bool withK = mode == UA_ASM_RK;
+  if (withK && (rc = ensure_K(m, p->precision))) return rc;
+  if ((rc = upload_fields(m, p, F, 1))) return rc;
+  if ((rc = upload_velocity(m, F, 1))) return rc;
+  if (mode == UA_ASM_ZERO_R) {  // uvMatrixAssemblySSTREAM.m:24-28
+    if ((rc = build_constraints(m, bcs, 1))) return rc;
+    UA_CUDA_TRY(cudaMemsetAsync(w->X, 0, m->ndof_total * sizeof(double), m->stream));
+    if (w->nc)
+      k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, nullptr,
+                                                                   w->con_rhs, w->X), ++g_launches;
+  }
+  std::vector<int> sel(1, 1);
+  if ((rc = set_sel(m, sel))) return rc;
+  if ((rc = assemble(m, p, withK, false, w->X, Tint || Fext))) return rc;
+  const int N = m->ndof_total;
+  if (R) UA_CUDA_TRY(cudaMemcpyAsync(R, w->R, N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (Tint) UA_CUDA_TRY(cudaMemcpyAsync(Tint, w->Tint, N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (Fext) UA_CUDA_TRY(cudaMemcpyAsync(Fext, w->Fext, N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (withK && Kvals) {
+    if (p->precision == UA_PREC_MIXED) {
+      std::vector<float> tmp(m->nnz_total);
+      UA_CUDA_TRY(cudaMemcpyAsync(tmp.data(), w->Kf, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+      UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+      for (size_t i = 0; i < tmp.size(); ++i) Kvals[i] = tmp[i];
+    } else {
+      UA_CUDA_TRY(cudaMemcpyAsync(Kvals, w->Kd, m->nnz_total * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    }
+  }
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return UA_OK;
+}
+
+static int newton_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs, int nF,
+                         std::vector<ua_newton_report*>& rep, double** lam_io, const int* nl_io) {
+  if (m->ndof != 2) return set_error(UA_ERR_INVALID, "uv Newton needs a ndof=2 mesh handle");
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  int rc;
+  double t0 = now_ms();
+  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_K(m, p->precision))) return rc;
+  if ((rc = upload_fields(m, p, F, nF))) return rc;
+  if ((rc = upload_velocity(m, F, nF))) return rc;
+  if ((rc = build_constraints(m, bcs, nF))) return rc;
+  Work* w = m->work;
+  const int nsys = w->nsys;
+  g_launches = 0;
+  w->prof.reset();
+  w->prof.on = p->profile != 0;
+  cudaEvent_t call_ev[2];
+  {
+    bool on = w->prof.on;
+    w->prof.on = true;
+    call_ev[0] = w->prof.get();
+    call_ev[1] = w->prof.get();
+    w->prof.on = on;
+  }
+  UA_CUDA_TRY(cudaEventRecord(call_ev[0], m->stream));
+  // Lagrange multipliers l.ubvb (:35-39): zero unless the caller's vector matches
+  if (w->nc) UA_CUDA_TRY(cudaMemsetAsync(w->lam, 0, w->nc * sizeof(double), m->stream));
+  for (int s = 0; s < nsys && lam_io; ++s) {
+    int nc_s = w->h_sys_con_off[s + 1] - w->h_sys_con_off[s];
+    if (lam_io[s] && nl_io[s] == nc_s && nc_s > 0)
+      UA_CUDA_TRY(cudaMemcpyAsync(w->lam + w->h_sys_con_off[s], lam_io[s], nc_s * sizeof(double),
+                                  cudaMemcpyHostToDevice, m->stream));
+  }
+  for (auto r : rep)
+    if (r) { int cap = r->iters_capacity; ua_newton_iter* it = r->iters; std::memset(r, 0, sizeof(*r)); r->iters_capacity = cap; r->iters = it; }
+  std::vector<SysState> st(nsys);
+  std::vector<int> run(nsys, 1);
+  if ((rc = newton_run(m, p, run, rep, st))) return rc;
+  // uv.m:107-112: reset u=v=l=0 and solve again once
+  std::vector<int> retry(nsys, 0);
+  bool any = false;
+  for (int s = 0; s < nsys; ++s)
+    if (!st[s].converged) { retry[s] = 1; any = true; }
+  if (any) {
+    for (int s = 0; s < nsys; ++s) {
+      if (!retry[s]) continue;
+      const int d0 = m->h_dof_off[s], nd = m->h_dof_off[s + 1] - d0;
+      UA_CUDA_TRY(cudaMemsetAsync(w->X + d0, 0, nd * sizeof(double), m->stream));
+      int c0 = w->h_sys_con_off[s], nc_s = w->h_sys_con_off[s + 1] - c0;
+      if (nc_s) UA_CUDA_TRY(cudaMemsetAsync(w->lam + c0, 0, nc_s * sizeof(double), m->stream));
+      if (rep[s]) rep[s]->retried = 1;
+    }
+    if ((rc = newton_run(m, p, retry, rep, st))) return rc;
+  }
+  // results back
+  for (int s = 0; s < nsys; ++s) {
+    ua_fields& f = F[nF == 1 ? 0 : s];
+    const int d0 = m->h_dof_off[s], nn = m->sys[s].nn;
+    auto kind = f.location == UA_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    UA_CUDA_TRY(cudaMemcpyAsync(f.ub, w->X + d0, nn * sizeof(double), kind, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(f.vb, w->X + d0 + nn, nn * sizeof(double), kind, m->stream));
+    if (lam_io && lam_io[s]) {
+      int nc_s = w->h_sys_con_off[s + 1] - w->h_sys_con_off[s];
+      if (nl_io[s] >= nc_s && nc_s > 0)
+        UA_CUDA_TRY(cudaMemcpyAsync(lam_io[s], w->lam + w->h_sys_con_off[s], nc_s * sizeof(double),
+                                    cudaMemcpyDeviceToHost, m->stream));
+    }
+  }
+  UA_CUDA_TRY(cudaEventRecord(call_ev[1], m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  double t1 = now_ms();
+  float dev_ms = 0;
+  cudaEventElapsedTime(&dev_ms, call_ev[0], call_ev[1]);
+  double kms[3] = {0, 0, 0};
+  int kn[3] = {0, 0, 0};
+  for (auto& mk : w->prof.marks) {
+    float t = 0;
+    cudaEventElapsedTime(&t, mk.second.first, mk.second.second);
+    kms[mk.first] += t;
+    kn[mk.first]++;
+  }
+  bool all_conv = true;
+  for (int s = 0; s < nsys; ++s) {
+    if (rep[s]) {
+      rep[s]->total_ms = t1 - t0;
+      rep[s]->device_ms = dev_ms;
+      rep[s]->kasmK_ms = kms[PK_ASMK]; rep[s]->kasmK_n = kn[PK_ASMK];
+      rep[s]->kasmR_ms = kms[PK_ASMR]; rep[s]->kasmR_n = kn[PK_ASMR];
+      rep[s]->kspmv_ms = kms[PK_SPMV]; rep[s]->kspmv_n = kn[PK_SPMV];
+      rep[s]->gpu_launches = (int)g_launches;
+    }
+    all_conv = all_conv && st[s].converged;
+  }
+  return all_conv ? UA_OK : UA_ERR_NOT_CONVERGED;
+}
+
+extern "C" int ua_uv_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs, double* lubvb,
+                            int32_t nl, ua_newton_report* rep, double* Kvals, double* R) {
+  if (!m || !p || !F) return set_error(UA_ERR_INVALID, "ua_uv_newton: null argument");
+  if (m->dm.nsys != 1) return set_error(UA_ERR_INVALID, "ua_uv_newton takes a single-mesh handle");
+  std::vector<ua_newton_report*> reps(1, rep);
+  double* lam[1] = {lubvb};
+  int nls[1] = {nl};
+  int rc = newton_common(m, p, F, bcs, 1, reps, lam, nls);
+  if (rc != UA_OK && rc != UA_ERR_NOT_CONVERGED) return rc;
+  Work* w = m->work;
+  if (R) UA_CUDA_TRY(cudaMemcpy(R, w->R, m->ndof_total * sizeof(double), cudaMemcpyDeviceToHost));
+  if (Kvals) {
+    if (p->precision == UA_PREC_MIXED) {
+      std::vector<float> tmp(m->nnz_total);
+      UA_CUDA_TRY(cudaMemcpy(tmp.data(), w->Kf, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < tmp.size(); ++i) Kvals[i] = tmp[i];
+    } else {
+      UA_CUDA_TRY(cudaMemcpy(Kvals, w->Kd, m->nnz_total * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+  }
+  return rc;
+}
+
+extern "C" int ua_uv_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fields, const ua_bcs* bcs,
+                                  ua_newton_report* reports) {
+  if (!m || !p || !fields) return set_error(UA_ERR_INVALID, "ua_uv_newton_batch: null argument");
+  std::vector<ua_newton_report*> reps(m->dm.nsys);
+  for (int s = 0; s < m->dm.nsys; ++s) reps[s] = reports ? &reports[s] : nullptr;
+  return newton_common(m, p, fields, bcs, m->dm.nsys, reps, nullptr, nullptr);
+}
+
+extern "C" int ua_constraint_count(const ua_mesh* m, const ua_bcs* bcs, int32_t ndof, int32_t* nc) {
+  if (!m || !nc) return set_error(UA_ERR_INVALID, "null argument");
+  int n = 0;
+  if (bcs) {
+    for (int comp = 0; comp < 2; ++comp) {
+      int k = comp == 0 ? bcs->n_ufixed : bcs->n_vfixed;
+      const int* nodes = comp == 0 ? bcs->ufixed_node : bcs->vfixed_node;
+      std::vector<int> v(nodes, nodes + k);
+      std::sort(v.begin(), v.end());
+      n += (int)(std::unique(v.begin(), v.end()) - v.begin());
+    }
+    n += bcs->n_utied + bcs->n_vtied;
+    if (ndof == 3) n += bcs->n_hfixed;
+  }
+  *nc = n;
+  return UA_OK;
+}
+
+extern "C" void ua_mesh_destroy(ua_mesh* m) {
+  if (!m) return;
+  cudaSetDevice(m->device);
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  if (m->work) {
+    Work* w = m->work;
+    if (w->h_sysv) cudaFreeHost(w->h_sysv);
+    if (w->h_int) cudaFreeHost(w->h_int);
+    if (w->h_gamma) cudaFreeHost(w->h_gamma);
+    delete w;
+  }
+  dev_free_all(m);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+}
+
+// solveKApeSymmetric.m:71-113 -> ABfgPreEliminate.m:29-160 for an SPD A with
+// selection-type constraints (one non-zero per row of L): x_d = g/l on the
+// constrained dofs, projected PCG on the rest, y = (f - A x)_d / l
+// (ABfgPreEliminate.m:138 with the ScaleL factor undone as at :159).
+extern "C" int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const int64_t* Acol, const double* Aval,
+                                       int32_t nl, const int64_t* Lrowptr, const int64_t* Lcol, const double* Lval,
+                                       const double* f, const double* g, double* x, double* y, double rtol,
+                                       int32_t maxit, int32_t* its, int32_t device) {
+  if (n <= 0 || !Arowptr || !Acol || !Aval || !f || !x) return set_error(UA_ERR_INVALID, "ua_solve_kape_symmetric: bad arguments");
+  if (nl > 0 && (!Lrowptr || !Lcol || !Lval || !g || !y)) return set_error(UA_ERR_INVALID, "constraint arrays missing");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return set_error(UA_ERR_NO_DEVICE, "no CUDA device"); }
+  UA_CUDA_TRY(cudaSetDevice(device));
+  const long long nnz = Arowptr[n] - Arowptr[0];
+  if (nnz >= (1LL << 31)) return set_error(UA_ERR_INVALID, "too many non-zeros");
+  std::vector<int> rowptr(n + 1), col(nnz), diagpos(n, -1);
+  for (int i = 0; i <= n; ++i) rowptr[i] = (int)(Arowptr[i] - Arowptr[0]);
+  for (long long j = 0; j < nnz; ++j) {
+    long long c = Acol[Arowptr[0] + j];
+    if (c < 0 || c >= n) return set_error(UA_ERR_INVALID, "column index out of range");
+    col[j] = (int)c;
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = rowptr[i]; j < rowptr[i + 1]; ++j)
+      if (col[j] == i) diagpos[i] = j;
+  std::vector<int> con_dof;
+  std::vector<double> con_rhs, con_l;
+  std::vector<unsigned char> cmask(n, 0);
+  std::vector<int> dof_con(n, -1);
+  for (int c = 0; c < nl; ++c) {
+    if (Lrowptr[c + 1] - Lrowptr[c] != 1)
+      return set_error(UA_ERR_INVALID, "constraint row %d: only single-entry rows are supported", c);
+    long long d = Lcol[Lrowptr[c]];
+    double l = Lval[Lrowptr[c]];
+    if (d < 0 || d >= n || l == 0) return set_error(UA_ERR_INVALID, "constraint row %d: bad entry", c);
+    if (cmask[d]) return set_error(UA_ERR_INVALID, "B*B' not diagonal (dof %lld constrained twice)", d);
+    cmask[d] = 1; dof_con[d] = c;
+    con_dof.push_back((int)d); con_rhs.push_back(g[c] / l); con_l.push_back(l);
+  }
+  for (int i = 0; i < n; ++i)
+    if (diagpos[i] < 0 && !cmask[i]) return set_error(UA_ERR_INVALID, "row %d has no diagonal entry", i);
+    else if (diagpos[i] < 0) diagpos[i] = rowptr[i];
+  // a one-system scratch handle
+  ua_mesh tmp;
+  tmp.device = device; tmp.ndof = 2; tmp.nod = 6; tmp.ndof_total = n; tmp.nnz_total = nnz;
+  tmp.dm.nsys = 1;
+  tmp.h_dof_off = {0, n};
+  int rc = UA_OK;
+  Work* w = new Work();
+  tmp.work = w;
+  UA_CUDA_TRY(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking));
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(tmp.stream);
+    if (w->h_sysv) cudaFreeHost(w->h_sysv);
+    if (w->h_int) cudaFreeHost(w->h_int);
+    if (w->h_gamma) cudaFreeHost(w->h_gamma);
+    delete w;
+    tmp.work = nullptr;
+    dev_free_all(&tmp);
+    cudaStreamDestroy(tmp.stream);
+  };
+  {
+    w->nsys = 1;
+    std::vector<int> rb_start, rb_sys;
+    for (int r = 0; r < n; r += kRB) { rb_start.push_back(r); rb_sys.push_back(0); }
+    w->nrb = (int)rb_sys.size();
+    rb_start.push_back(n);
+    w->h_sys_rb_off = {0, w->nrb};
+    std::vector<int> sel1 = {1}, coff = {0, (int)con_dof.size()}, csys(con_dof.size(), 0);
+    auto up_i = [&](const std::vector<int>& v) { int* d = walloc<int>(&tmp, v.size()); if (d) cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice); return d; };
+    auto up_d = [&](const double* v, size_t k) { double* d = walloc<double>(&tmp, k); if (d && k) cudaMemcpy(d, v, k * sizeof(double), cudaMemcpyHostToDevice); return d; };
+    w->rb_start = up_i(rb_start); w->rb_sys = up_i(rb_sys); w->sys_rb_off = up_i(w->h_sys_rb_off);
+    w->rowptr = up_i(rowptr); w->colind = up_i(col); w->diagpos = up_i(diagpos);
+    w->Kd = up_d(Aval + Arowptr[0], nnz);
+    w->frhs = up_d(f, n);
+    w->X = walloc<double>(&tmp, n); w->dX = walloc<double>(&tmp, n);
+    void** kv[] = {&w->kr, &w->kz, &w->kp, &w->kq, &w->invd};
+    for (auto v : kv) *v = walloc<double>(&tmp, n);
+    w->part = walloc<double>(&tmp, 4 * (size_t)w->nrb);
+    w->sysv = walloc<double>(&tmp, SV_COUNT);
+    w->done = walloc<int>(&tmp, 1); w->its = walloc<int>(&tmp, 1); w->status = walloc<int>(&tmp, 1);
+    w->sel = up_i(sel1);
+    w->cmask = walloc<unsigned char>(&tmp, n);
+    w->dof_con = up_i(dof_con);
+    w->nc = (int)con_dof.size();
+    if (w->nc) {
+      w->con_dof = up_i(con_dof); w->con_sys = up_i(csys); w->sys_con_off = up_i(coff);
+      w->con_rhs = up_d(con_rhs.data(), w->nc);
+      w->dlam = walloc<double>(&tmp, w->nc); w->grhs = walloc<double>(&tmp, w->nc);
+    }
+    if (!w->Kd || !w->X || !w->dX || !w->kr || !w->kz || !w->kp || !w->kq || !w->invd || !w->part || !w->cmask ||
+        cudaMallocHost(&w->h_sysv, SV_COUNT * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&w->h_int, 8 * sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&w->h_gamma, sizeof(double)) != cudaSuccess) {
+      cleanup();
+      return set_error(UA_ERR_OOM, "allocation failed");
+    }
+    cudaMemcpy(w->cmask, cmask.data(), n, cudaMemcpyHostToDevice);
+    cudaMemset(w->X, 0, n * sizeof(double));
+    ua_params p;
+    ua_params_default(&p);
+    p.krylov_rtol = rtol > 0 ? rtol : 1e-12;
+    p.krylov_maxit = maxit > 0 ? maxit : 10 * n + 100;
+    std::vector<int> kits(1, 1);
+    rc = pcg_t<double, double>(&tmp, &p, w->Kd, kits);
+    if (rc == UA_OK) {
+      std::vector<double> dl(w->nc);
+      int st = 0;
+      cudaMemcpy(x, w->dX, n * sizeof(double), cudaMemcpyDeviceToHost);
+      if (w->nc) cudaMemcpy(dl.data(), w->dlam, w->nc * sizeof(double), cudaMemcpyDeviceToHost);
+      cudaMemcpy(&st, w->status, sizeof(int), cudaMemcpyDeviceToHost);
+      for (int c = 0; c < w->nc; ++c) y[c] = dl[c] / con_l[c];
+      if (its) *its = kits[0];
+      if (st) rc = set_error(UA_ERR_KRYLOV, "PCG breakdown: A is not positive definite on the free dofs");
+    }
+  }
+  cleanup();
+  return rc;
+}

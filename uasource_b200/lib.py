@@ -1,0 +1,176 @@
+"""ctypes binding of libuassa.so (the C-ABI declared in include/ua_ssa.h).
+
+The shared library is built in-tree (``uasource_b200/libuassa.so``) by
+``python -m uasource_b200.build`` or ``make -C uasource_b200/csrc``.  There is
+no fallback: if the library or a CUDA device is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libuassa.so")
+
+UA_OK = 0
+UA_ERR_INVALID = -1
+UA_ERR_NAN_INPUT = -2
+UA_ERR_NOT_CONVERGED = -3
+UA_ERR_OOM = -4
+UA_ERR_TIMEOUT = -5
+UA_ERR_BAD_MESH = -6
+UA_ERR_CUDA = -7
+UA_ERR_KRYLOV = -8
+UA_ERR_NO_DEVICE = -9
+
+UA_PREC_FP64 = 0
+UA_PREC_MIXED = 1
+UA_ASM_R = 0
+UA_ASM_RK = 1
+UA_ASM_ZERO_R = 2
+UA_HOST = 0
+UA_DEVICE = 1
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+
+
+class ua_mesh_desc(C.Structure):
+    _fields_ = [("nnodes", C.c_int32), ("nele", C.c_int32), ("nod", C.c_int32), ("index_base", C.c_int32),
+                ("coordinates", _dp), ("connectivity", _ip)]
+
+
+class ua_params(C.Structure):
+    _fields_ = [
+        ("kH", C.c_double), ("Hh0", C.c_double),
+        ("SpeedZero", C.c_double), ("EpsZero", C.c_double), ("etaZero", C.c_double),
+        ("Czero", C.c_double), ("Cmin", C.c_double), ("AGlenmin", C.c_double),
+        ("Picard", C.c_int32), ("NRviscosity", C.c_double),
+        ("NRitmax", C.c_int32), ("NRitmin", C.c_int32),
+        ("NewtonAcceptRatio", C.c_double), ("BacktrackingGammaMin", C.c_double),
+        ("LineSearchAllowedToUseExtrapolation", C.c_int32),
+        ("BackTrackBeta", C.c_double), ("BackTrackMaxIterations", C.c_int32),
+        ("BackTrackMaxExtrapolations", C.c_int32), ("BackTrackExtrapolationRatio", C.c_double),
+        ("BackTrackMinXfrac", C.c_double), ("BackTrackMaxFuncSame", C.c_int32),
+        ("BackTrackGuardLower", C.c_double), ("BackTrackGuardUpper", C.c_double),
+        ("NLtol", C.c_double),
+        ("uvDesiredWorkAndForceTolerances", C.c_double * 2),
+        ("uvDesiredWorkOrForceTolerances", C.c_double * 2),
+        ("uvExitBackTrackingStepLength", C.c_double),
+        ("uvAcceptableWorkAndForceTolerances", C.c_double * 2),
+        ("uvAcceptableWorkOrForceTolerances", C.c_double * 2),
+        ("ModifiedNRuvIntervalCriterion", C.c_int32), ("ModifiedNRuvReductionCriterion", C.c_double),
+        ("theta", C.c_double), ("SUPG_beta0", C.c_double), ("uvh_SUPG_tauMultiplier", C.c_double),
+        ("uvh_SUPG_tau", C.c_int32),
+        ("uvhDesiredWorkAndForceTolerances", C.c_double * 2),
+        ("uvhDesiredWorkOrForceTolerances", C.c_double * 2),
+        ("uvhExitBackTrackingStepLength", C.c_double),
+        ("uvhAcceptableWorkAndForceTolerances", C.c_double * 2),
+        ("uvhAcceptableWorkOrForceTolerances", C.c_double * 2),
+        ("krylov_rtol", C.c_double), ("krylov_maxit", C.c_int32), ("precision", C.c_int32),
+        ("patch_nodes", C.c_int32), ("verbose", C.c_int32), ("profile", C.c_int32),
+    ]
+
+
+class ua_fields(C.Structure):
+    _fields_ = [("location", C.c_int32),
+                ("h", _dp), ("S", _dp), ("B", _dp), ("rho", _dp), ("AGlen", _dp), ("n", _dp), ("C", _dp),
+                ("m", _dp), ("ub", _dp), ("vb", _dp),
+                ("rhow", C.c_double), ("g", C.c_double), ("alpha", C.c_double),
+                ("h0", _dp), ("u0", _dp), ("v0", _dp), ("as0", _dp), ("ab0", _dp), ("as1", _dp), ("ab1", _dp),
+                ("dadh", _dp), ("h1", _dp), ("dt", C.c_double)]
+
+
+class ua_bcs(C.Structure):
+    _fields_ = [("n_ufixed", C.c_int32), ("ufixed_node", _ip), ("ufixed_value", _dp),
+                ("n_vfixed", C.c_int32), ("vfixed_node", _ip), ("vfixed_value", _dp),
+                ("n_utied", C.c_int32), ("utied_a", _ip), ("utied_b", _ip),
+                ("n_vtied", C.c_int32), ("vtied_a", _ip), ("vtied_b", _ip),
+                ("n_hfixed", C.c_int32), ("hfixed_node", _ip), ("hfixed_value", _dp)]
+
+
+class ua_newton_iter(C.Structure):
+    _fields_ = [("iteration", C.c_int32), ("iarm", C.c_int32), ("krylov_its", C.c_int32), ("direction", C.c_int32),
+                ("gamma", C.c_double), ("r0", C.c_double), ("r", C.c_double), ("rForce", C.c_double),
+                ("rWork", C.c_double)]
+
+
+class ua_newton_report(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("backtrack_steps", C.c_int32),
+                ("krylov_its_total", C.c_int32), ("cauchy_fallbacks", C.c_int32), ("retried", C.c_int32),
+                ("r", C.c_double), ("rForce", C.c_double), ("rWork", C.c_double),
+                ("assembly_ms", C.c_double), ("solve_ms", C.c_double), ("total_ms", C.c_double),
+                ("device_ms", C.c_double), ("kasmK_ms", C.c_double), ("kasmR_ms", C.c_double),
+                ("kspmv_ms", C.c_double), ("kasmK_n", C.c_int32), ("kasmR_n", C.c_int32), ("kspmv_n", C.c_int32),
+                ("gpu_launches", C.c_int32),
+                ("n_iter_records", C.c_int32), ("iters_capacity", C.c_int32),
+                ("iters", C.POINTER(ua_newton_iter))]
+
+
+# symbol -> (restype, argtypes); every function declared in include/ua_ssa.h
+SIGNATURES = {
+    "ua_version": (C.c_char_p, []),
+    "ua_last_error": (C.c_char_p, []),
+    "ua_device_count": (C.c_int, []),
+    "ua_struct_sizes": (C.c_int, [_lp, C.c_int32]),
+    "ua_params_default": (None, [C.POINTER(ua_params)]),
+    "ua_mesh_create": (C.c_int, [C.POINTER(ua_mesh_desc), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "ua_mesh_create_batch": (C.c_int, [C.POINTER(ua_mesh_desc), C.c_int32, C.c_int32, C.c_int32,
+                                       C.POINTER(C.c_void_p)]),
+    "ua_mesh_destroy": (None, [C.c_void_p]),
+    "ua_mesh_pattern": (C.c_int, [C.c_void_p, C.c_int32, _lp, _lp, _lp]),
+    "ua_mesh_info": (C.c_int, [C.c_void_p, C.c_int32, _ip, _ip, _ip, _lp]),
+    "ua_mesh_flipped": (C.c_int, [C.c_void_p, _ip]),
+    "ua_uv_assemble": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),
+                                 C.c_int32, _dp, _dp, _dp, _dp]),
+    "ua_uv_newton": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs), _dp,
+                               C.c_int32, C.POINTER(ua_newton_report), _dp, _dp]),
+    "ua_uv_newton_batch": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),
+                                     C.POINTER(ua_newton_report)]),
+    "ua_constraint_count": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), C.c_int32, _ip]),
+    "ua_solve_kape_symmetric": (C.c_int, [C.c_int32, _lp, _lp, _dp, C.c_int32, _lp, _lp, _dp, _dp, _dp, _dp, _dp,
+                                          C.c_double, C.c_int32, _ip, C.c_int32]),
+}
+
+_lib = None
+
+
+class UaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libuassa error {code}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load libuassa.so (raises if it is missing: there is no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m uasource_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc, allow=()):
+    if rc != UA_OK and rc not in allow:
+        raise UaError(rc, load().ua_last_error().decode())
+    return rc
+
+
+def dptr(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def iptr(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def lptr(a):
+    return a.ctypes.data_as(_lp) if a is not None else None
