@@ -1,0 +1,246 @@
+/*
+ * Shared helpers of the MEX gateways: read Úa's MATLAB structs (CtrlVar, MUA,
+ * F, BCs) by field name and marshal them into the plain-pointer C-ABI of
+ * libuassa (include/ua_ssa.h).  Builds with `mex` (MATLAB) or
+ * `mkoctfile --mex` (GNU Octave):
+ *
+ *   mex -I../include uvMatrixAssemblySSTREAM_mex.c -L../uasource_b200 -luassa
+ *
+ * The device-resident mesh handle persists across calls (static storage,
+ * mexLock) and is rebuilt only when MUA.coordinates/connectivity change; it is
+ * freed at exit (mexAtExit).  All mx* calls run on MATLAB's interpreter thread.
+ */
+#ifndef UA_MEX_COMMON_H
+#define UA_MEX_COMMON_H
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mex.h"
+#include "ua_ssa.h"
+
+static ua_mesh* g_mesh = NULL;
+static uint64_t g_mesh_key = 0;
+static int g_locked = 0;
+
+static void ua_mex_cleanup(void) {
+    if (g_mesh) ua_mesh_destroy(g_mesh);
+    g_mesh = NULL;
+    g_mesh_key = 0;
+}
+
+/* FNV-1a over the raw bytes of the mesh arrays: detects a changed MUA. */
+static uint64_t ua_mex_hash(const void* p, size_t n, uint64_t h) {
+    const unsigned char* b = (const unsigned char*)p;
+    size_t i;
+    for (i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ULL;
+    return h;
+}
+
+static const mxArray* ua_mex_field(const mxArray* s, const char* name, int required) {
+    const mxArray* f = (s && mxIsStruct(s)) ? mxGetField(s, 0, name) : NULL;
+    if (!f && required) mexErrMsgIdAndTxt("Ua:mex:MissingField", "missing field %s", name);
+    return f;
+}
+
+static double ua_mex_scalar(const mxArray* s, const char* name, double dflt) {
+    const mxArray* f = ua_mex_field(s, name, 0);
+    if (!f || mxIsEmpty(f)) return dflt;
+    return mxGetScalar(f);
+}
+
+/* CtrlVar -> ua_params (fields named as in Ua2D_DefaultParameters.m). */
+static void ua_mex_params(const mxArray* C, ua_params* p) {
+    const mxArray* f;
+    ua_params_default(p);
+    p->kH = ua_mex_scalar(C, "kH", p->kH);
+    p->Hh0 = ua_mex_scalar(C, "Hh0", p->Hh0);
+    p->SpeedZero = ua_mex_scalar(C, "SpeedZero", p->SpeedZero);
+    p->EpsZero = ua_mex_scalar(C, "EpsZero", p->EpsZero);
+    p->etaZero = ua_mex_scalar(C, "etaZero", p->etaZero);
+    p->Czero = ua_mex_scalar(C, "Czero", p->Czero);
+    p->Cmin = ua_mex_scalar(C, "Cmin", p->Cmin);
+    p->AGlenmin = ua_mex_scalar(C, "AGlenmin", p->AGlenmin);
+    p->Picard = (int32_t)ua_mex_scalar(C, "Picard", p->Picard);
+    p->NRviscosity = ua_mex_scalar(C, "NRviscosity", p->NRviscosity);
+    p->NRitmax = (int32_t)ua_mex_scalar(C, "NRitmax", p->NRitmax);
+    p->NRitmin = (int32_t)ua_mex_scalar(C, "NRitmin", p->NRitmin);
+    p->NewtonAcceptRatio = ua_mex_scalar(C, "NewtonAcceptRatio", p->NewtonAcceptRatio);
+    p->BacktrackingGammaMin = ua_mex_scalar(C, "BacktrackingGammaMin", p->BacktrackingGammaMin);
+    p->LineSearchAllowedToUseExtrapolation =
+        (int32_t)ua_mex_scalar(C, "LineSearchAllowedToUseExtrapolation", p->LineSearchAllowedToUseExtrapolation);
+    p->BackTrackBeta = ua_mex_scalar(C, "BackTrackBeta", p->BackTrackBeta);
+    p->BackTrackMaxIterations = (int32_t)ua_mex_scalar(C, "BackTrackMaxIterations", p->BackTrackMaxIterations);
+    p->BackTrackGuardLower = ua_mex_scalar(C, "BackTrackGuardLower", p->BackTrackGuardLower);
+    p->BackTrackGuardUpper = ua_mex_scalar(C, "BackTrackGuardUpper", p->BackTrackGuardUpper);
+    p->uvExitBackTrackingStepLength = ua_mex_scalar(C, "uvExitBackTrackingStepLength", p->uvExitBackTrackingStepLength);
+    p->ModifiedNRuvIntervalCriterion =
+        (int32_t)ua_mex_scalar(C, "ModifiedNRuvIntervalCriterion", p->ModifiedNRuvIntervalCriterion);
+    p->ModifiedNRuvReductionCriterion =
+        ua_mex_scalar(C, "ModifiedNRuvReductionCriterion", p->ModifiedNRuvReductionCriterion);
+    {
+        const char* pairs[4] = {"uvDesiredWorkAndForceTolerances", "uvDesiredWorkOrForceTolerances",
+                                "uvAcceptableWorkAndForceTolerances", "uvAcceptableWorkOrForceTolerances"};
+        double* dst[4] = {p->uvDesiredWorkAndForceTolerances, p->uvDesiredWorkOrForceTolerances,
+                          p->uvAcceptableWorkAndForceTolerances, p->uvAcceptableWorkOrForceTolerances};
+        int k;
+        for (k = 0; k < 4; ++k) {
+            f = ua_mex_field(C, pairs[k], 0);
+            if (f && mxGetNumberOfElements(f) == 2) {
+                dst[k][0] = mxGetPr(f)[0];
+                dst[k][1] = mxGetPr(f)[1];
+            }
+        }
+    }
+    /* the GPU form selected by a CtrlVar.UseGPU-style switch (0=FP64, 1=mixed) */
+    p->precision = (int32_t)ua_mex_scalar(C, "GPUPrecision", p->precision);
+    p->krylov_rtol = ua_mex_scalar(C, "GPUKrylovTol", p->krylov_rtol);
+}
+
+/* MUA -> cached device mesh (rebuilt when coordinates/connectivity change). */
+static ua_mesh* ua_mex_mesh(const mxArray* MUA) {
+    const mxArray* co = ua_mex_field(MUA, "coordinates", 1);
+    const mxArray* cn = ua_mex_field(MUA, "connectivity", 1);
+    size_t nn = mxGetM(co), ne = mxGetM(cn), nod = mxGetN(cn), i;
+    uint64_t key = 1469598103934665603ULL;
+    int32_t* conn;
+    ua_mesh_desc d;
+    int rc;
+    if (mxGetN(co) != 2 || !mxIsDouble(co) || !mxIsDouble(cn))
+        mexErrMsgIdAndTxt("Ua:mex:BadMUA", "MUA.coordinates must be Nnodes x 2 double, connectivity double");
+    key = ua_mex_hash(mxGetPr(co), nn * 2 * sizeof(double), key);
+    key = ua_mex_hash(mxGetPr(cn), ne * nod * sizeof(double), key);
+    if (g_mesh && key == g_mesh_key) return g_mesh;
+    ua_mex_cleanup();
+    conn = (int32_t*)mxMalloc(ne * nod * sizeof(int32_t));
+    for (i = 0; i < ne * nod; ++i) conn[i] = (int32_t)mxGetPr(cn)[i];
+    d.nnodes = (int32_t)nn;
+    d.nele = (int32_t)ne;
+    d.nod = (int32_t)nod;
+    d.index_base = 1;
+    d.coordinates = mxGetPr(co);
+    d.connectivity = conn;
+    rc = ua_mesh_create(&d, 2, 0, &g_mesh);
+    mxFree(conn);
+    if (rc != UA_OK) {
+        g_mesh = NULL;
+        mexErrMsgIdAndTxt(rc == UA_ERR_BAD_MESH ? "Ua:TestAndCorrectForInsideOutElements:InsideOutelements"
+                                                : "Ua:mex:MeshCreate",
+                          "%s", ua_last_error());
+    }
+    g_mesh_key = key;
+    if (!g_locked) {
+        mexLock();
+        mexAtExit(ua_mex_cleanup);
+        g_locked = 1;
+    }
+    return g_mesh;
+}
+
+/* A nodal field: Nn-vector, or a scalar expanded as uv.m:34-40 does for m and n. */
+static const double* ua_mex_nodal(const mxArray* F, const char* name, size_t nn, double** owned) {
+    const mxArray* f = ua_mex_field(F, name, 1);
+    size_t k = mxGetNumberOfElements(f), i;
+    *owned = NULL;
+    if (k == nn) return mxGetPr(f);
+    if (k == 1) {
+        *owned = (double*)mxMalloc(nn * sizeof(double));
+        for (i = 0; i < nn; ++i) (*owned)[i] = mxGetScalar(f);
+        return *owned;
+    }
+    mexErrMsgIdAndTxt("Ua:mex:BadField", "F.%s must have Nnodes elements", name);
+    return NULL;
+}
+
+/* BCs node lists (double, 1-based) -> int32 arrays owned by the caller. */
+static int32_t* ua_mex_nodes(const mxArray* B, const char* name, int32_t* n) {
+    const mxArray* f = ua_mex_field(B, name, 0);
+    size_t k = f ? mxGetNumberOfElements(f) : 0, i;
+    int32_t* out;
+    *n = (int32_t)k;
+    if (!k) return NULL;
+    out = (int32_t*)mxMalloc(k * sizeof(int32_t));
+    for (i = 0; i < k; ++i) out[i] = (int32_t)mxGetPr(f)[i];
+    return out;
+}
+
+static const double* ua_mex_values(const mxArray* B, const char* name) {
+    const mxArray* f = ua_mex_field(B, name, 0);
+    return (f && !mxIsEmpty(f)) ? mxGetPr(f) : NULL;
+}
+
+/* The mesh's 1-based BC lists.  The library takes 0-based indices for
+ * index_base handles created from MATLAB too, so shift here. */
+static void ua_mex_bcs(const mxArray* B, ua_bcs* b) {
+    int32_t i;
+    memset(b, 0, sizeof(*b));
+    if (!B || !mxIsStruct(B)) return;
+    b->ufixed_node = ua_mex_nodes(B, "ubFixedNode", &b->n_ufixed);
+    b->ufixed_value = ua_mex_values(B, "ubFixedValue");
+    b->vfixed_node = ua_mex_nodes(B, "vbFixedNode", &b->n_vfixed);
+    b->vfixed_value = ua_mex_values(B, "vbFixedValue");
+    b->utied_a = ua_mex_nodes(B, "ubTiedNodeA", &b->n_utied);
+    b->utied_b = ua_mex_nodes(B, "ubTiedNodeB", &b->n_utied);
+    b->vtied_a = ua_mex_nodes(B, "vbTiedNodeA", &b->n_vtied);
+    b->vtied_b = ua_mex_nodes(B, "vbTiedNodeB", &b->n_vtied);
+    for (i = 0; i < b->n_ufixed; ++i) ((int32_t*)b->ufixed_node)[i] -= 1;
+    for (i = 0; i < b->n_vfixed; ++i) ((int32_t*)b->vfixed_node)[i] -= 1;
+    for (i = 0; i < b->n_utied; ++i) { ((int32_t*)b->utied_a)[i] -= 1; ((int32_t*)b->utied_b)[i] -= 1; }
+    for (i = 0; i < b->n_vtied; ++i) { ((int32_t*)b->vtied_a)[i] -= 1; ((int32_t*)b->vtied_b)[i] -= 1; }
+}
+
+static void ua_mex_fail(int rc) {
+    const char* id = "Ua:mex:Error";
+    if (rc == UA_ERR_NAN_INPUT) id = "uvMatrixAssembly:NaN";
+    else if (rc == UA_ERR_NO_DEVICE) id = "Ua:mex:NoDevice";
+    else if (rc == UA_ERR_OOM) id = "Ua:mex:OutOfMemory";
+    mexErrMsgIdAndTxt(id, "%s", ua_last_error());
+}
+
+/* CSR values on the structural pattern -> MATLAB sparse (CSC, sorted rows, no
+ * explicit zeros).  The uv pattern and values are symmetric, so the CSR arrays
+ * are read as CSC. */
+static mxArray* ua_mex_sparse(ua_mesh* m, int32_t n, const double* vals) {
+    int64_t nnz = 0, j, k, out = 0;
+    int64_t *rp, *ci;
+    mxArray* S;
+    mwIndex *jc, *ir;
+    double* pr;
+    ua_mesh_pattern(m, 0, &nnz, NULL, NULL);
+    rp = (int64_t*)mxMalloc((n + 1) * sizeof(int64_t));
+    ci = (int64_t*)mxMalloc(nnz * sizeof(int64_t));
+    ua_mesh_pattern(m, 0, &nnz, rp, ci);
+    for (k = 0; k < nnz; ++k) out += vals[k] != 0.0;
+    S = mxCreateSparse(n, n, out > 0 ? out : 1, mxREAL);
+    jc = mxGetJc(S); ir = mxGetIr(S); pr = mxGetPr(S);
+    out = 0;
+    for (j = 0; j < n; ++j) {
+        jc[j] = (mwIndex)out;
+        for (k = rp[j]; k < rp[j + 1]; ++k)
+            if (vals[k] != 0.0) { ir[out] = (mwIndex)ci[k]; pr[out] = vals[k]; ++out; }
+    }
+    jc[n] = (mwIndex)out;
+    mxFree(rp); mxFree(ci);
+    return S;
+}
+
+/* A dense vector as an n x 1 sparse (MATLAB's Tint-Fext is sparse-typed). */
+static mxArray* ua_mex_sparse_vector(int32_t n, const double* v) {
+    int32_t i, nz = 0;
+    mxArray* S;
+    mwIndex *jc, *ir;
+    double* pr;
+    for (i = 0; i < n; ++i) nz += v[i] != 0.0;
+    S = mxCreateSparse(n, 1, nz > 0 ? nz : 1, mxREAL);
+    jc = mxGetJc(S); ir = mxGetIr(S); pr = mxGetPr(S);
+    jc[0] = 0;
+    nz = 0;
+    for (i = 0; i < n; ++i)
+        if (v[i] != 0.0) { ir[nz] = (mwIndex)i; pr[nz] = v[i]; ++nz; }
+    jc[1] = (mwIndex)nz;
+    return S;
+}
+
+#endif

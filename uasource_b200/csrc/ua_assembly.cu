@@ -116,28 +116,61 @@ __device__ __forceinline__ void uv_element(const QuadTable& Q, const UvPhys& P, 
     const double dbdx = dsdx - dhdx, dbdy = dsdy - dhdy;
     const double detJw = detJ * Q.w[ip];
     if (WITHK) {
-      const KT he = (KT)(hint * eta * detJw);
-      const KT hE2 = (KT)(P.Dvisk * 2.0 * hint * E * detJw);
       const KT cxu = (KT)(d.dxu * detJw), cyv = (KT)(d.dyv * detJw), cxv = (KT)(d.dxv * detJw);
-      KT Pu[NOD], Pv[NOD], dx[NOD], dy[NOD], Nk[NOD];
+      KT Nk[NOD];
 #pragma unroll
-      for (int a = 0; a < NOD; ++a) {
-        Pu[a] = (KT)((2 * exx + eyy) * Dx[a] + exy * Dy[a]);
-        Pv[a] = (KT)((2 * eyy + exx) * Dy[a] + exy * Dx[a]);
-        dx[a] = (KT)Dx[a]; dy[a] = (KT)Dy[a]; Nk[a] = (KT)N[a];
-      }
+      for (int a = 0; a < NOD; ++a) Nk[a] = (KT)N[a];
+      if constexpr (sizeof(KT) == 8) {
+        const KT he = hint * eta * detJw;
+        const KT hE2 = P.Dvisk * 2.0 * hint * E * detJw;
+        KT Pu[NOD], Pv[NOD];
 #pragma unroll
-      for (int a = 0; a < NOD; ++a) {
-#pragma unroll
-        for (int b = a; b < NOD; ++b) {
-          const int i = I::sym(a, b);
-          const KT NN = Nk[a] * Nk[b];
-          Kuu[i] += he * (4 * dx[a] * dx[b] + dy[a] * dy[b]) + cxu * NN + hE2 * Pu[a] * Pu[b];
-          Kvv[i] += he * (4 * dy[a] * dy[b] + dx[a] * dx[b]) + cyv * NN + hE2 * Pv[a] * Pv[b];
+        for (int a = 0; a < NOD; ++a) {
+          Pu[a] = (2 * exx + eyy) * Dx[a] + exy * Dy[a];
+          Pv[a] = (2 * eyy + exx) * Dy[a] + exy * Dx[a];
         }
 #pragma unroll
-        for (int b = 0; b < NOD; ++b)
-          Kuv[a * NOD + b] += he * (2 * dx[a] * dy[b] + dy[a] * dx[b]) + cxv * Nk[a] * Nk[b] + hE2 * Pu[a] * Pv[b];
+        for (int a = 0; a < NOD; ++a) {
+#pragma unroll
+          for (int b = a; b < NOD; ++b) {
+            const int i = I::sym(a, b);
+            const KT NN = Nk[a] * Nk[b];
+            Kuu[i] += he * (4 * Dx[a] * Dx[b] + Dy[a] * Dy[b]) + cxu * NN + hE2 * Pu[a] * Pu[b];
+            Kvv[i] += he * (4 * Dy[a] * Dy[b] + Dx[a] * Dx[b]) + cyv * NN + hE2 * Pv[a] * Pv[b];
+          }
+#pragma unroll
+          for (int b = 0; b < NOD; ++b)
+            Kuv[a * NOD + b] += he * (2 * Dx[a] * Dy[b] + Dy[a] * Dx[b]) + cxv * Nk[a] * Nk[b] + hE2 * Pu[a] * Pv[b];
+        }
+      } else {
+        // FP32 tangent: h*eta*detJw and 2*h*E*detJw span far beyond the float
+        // range (E grows as e^((1-3n)/n) when the strain rate e -> EpsZero), so
+        // their square roots are folded into the per-node vectors in FP64 and
+        // only the bounded products are rounded to float.
+        const double he = hint * eta * detJw;
+        const double hE2 = P.Dvisk * 2.0 * hint * E * detJw;
+        const double sh = sqrt(he), sE = sqrt(fabs(hE2));
+        const KT sgn = hE2 < 0 ? KT(-1) : KT(1);
+        KT dx[NOD], dy[NOD], Pu[NOD], Pv[NOD];
+#pragma unroll
+        for (int a = 0; a < NOD; ++a) {
+          dx[a] = (KT)(sh * Dx[a]); dy[a] = (KT)(sh * Dy[a]);
+          Pu[a] = (KT)(sE * ((2 * exx + eyy) * Dx[a] + exy * Dy[a]));
+          Pv[a] = (KT)(sE * ((2 * eyy + exx) * Dy[a] + exy * Dx[a]));
+        }
+#pragma unroll
+        for (int a = 0; a < NOD; ++a) {
+#pragma unroll
+          for (int b = a; b < NOD; ++b) {
+            const int i = I::sym(a, b);
+            const KT NN = Nk[a] * Nk[b];
+            Kuu[i] += (4 * dx[a] * dx[b] + dy[a] * dy[b]) + cxu * NN + sgn * Pu[a] * Pu[b];
+            Kvv[i] += (4 * dy[a] * dy[b] + dx[a] * dx[b]) + cyv * NN + sgn * Pv[a] * Pv[b];
+          }
+#pragma unroll
+          for (int b = 0; b < NOD; ++b)
+            Kuv[a * NOD + b] += (2 * dx[a] * dy[b] + dy[a] * dx[b]) + cxv * Nk[a] * Nk[b] + sgn * Pu[a] * Pv[b];
+        }
       }
     }
     const double rr = rhoint * hint - rhow * dint;

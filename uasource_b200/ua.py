@@ -376,7 +376,7 @@ def uv(ctrl: CtrlVar, mua: MUA, bcs: BCs, F: Fields, l=None, return_K=False):
     L.check(lib.ua_constraint_count(mua.handle, C.byref(cb), 2, C.byref(nc)))
     lam = np.zeros(nc.value) if l is None or len(l) != nc.value else _f64(l).copy()
     rep = L.ua_newton_report()
-    recs = (L.ua_newton_iter * (ctrl.NRitmax + 2) * 2)()
+    recs = (L.ua_newton_iter * ((ctrl.NRitmax + 2) * 2))()
     rep.iters = C.cast(recs, C.POINTER(L.ua_newton_iter))
     rep.iters_capacity = (ctrl.NRitmax + 2) * 2
     Kv = np.zeros(mua.pattern()[1].size) if return_K else None
