@@ -231,6 +231,25 @@ int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const int64_t* Ac
                             const double* f, const double* g, double* x, double* y,
                             double rtol, int32_t maxit, int32_t* its, int32_t device);
 
+/* Allocation-free variant of ua_solve_kape_symmetric.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory (a MEX
+ * working on gpuArray data, where MATLAB owns the device allocator; a plugin
+ * in a host application that forbids cudaMalloc on its solve path).  Every
+ * array argument is a device pointer on `device` (CSR of A with int32 indices,
+ * L as one (dof, value) pair per constraint row).  Temporaries live in a
+ * library-owned static device array of about 8.5 MB that each device keeps
+ * until exit; n <= UA_NOALLOC_MAX_ROWS and nl <= UA_NOALLOC_MAX_CONSTRAINTS,
+ * larger sizes return UA_ERR_INVALID.  The array is shared by all calls on a
+ * device, so overlapping calls race; the first call on a device looks up the
+ * array's address and should come before any stream capture.  Work runs on
+ * cudaStreamPerThread and the call returns after it completes. */
+#define UA_NOALLOC_MAX_ROWS 131072
+#define UA_NOALLOC_MAX_CONSTRAINTS 16384
+int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr, const int32_t* Acol, const double* Aval,
+                                    int32_t nl, const int32_t* Ldof, const double* Lval,
+                                    const double* f, const double* g, double* x, double* y,
+                                    double rtol, int32_t maxit, int32_t* its, int32_t device);
+
 #ifdef __cplusplus
 }
 #endif

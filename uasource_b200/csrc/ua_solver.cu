@@ -726,7 +726,7 @@ static int cost_eval(ua_mesh* m, const ua_params* p, bool useDir) {
 }
 
 template <typename KT, typename VT>
-static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, std::vector<int>& its_out) {
+static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out) {
   Work* w = m->work;
   const int N = m->ndof_total;
   const int lpr = (m->nod == 3 && m->ndof == 2) ? 8 : 16;
@@ -797,8 +797,8 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, std::vector<int>& 
 // its_out[s] != 0 marks selected on input).
 static int linear_solve(ua_mesh* m, const ua_params* p, std::vector<int>& its_out) {
   Work* w = m->work;
-  if (p->precision == UA_PREC_MIXED) return pcg_t<float, float>(m, p, w->Kf, its_out);
-  return pcg_t<double, double>(m, p, w->Kd, its_out);
+  if (p->precision == UA_PREC_MIXED) return pcg_t<float, float>(m, p, w->Kf, its_out.data());
+  return pcg_t<double, double>(m, p, w->Kd, its_out.data());
 }
 
 // uvResidualsCriteria.m:1-23
@@ -1356,7 +1356,7 @@ extern "C" int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const 
     p.krylov_rtol = rtol > 0 ? rtol : 1e-12;
     p.krylov_maxit = maxit > 0 ? maxit : 10 * n + 100;
     std::vector<int> kits(1, 1);
-    rc = pcg_t<double, double>(&tmp, &p, w->Kd, kits);
+    rc = pcg_t<double, double>(&tmp, &p, w->Kd, kits.data());
     if (rc == UA_OK) {
       std::vector<double> dl(w->nc);
       int st = 0;
@@ -1369,5 +1369,220 @@ extern "C" int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const 
     }
   }
   cleanup();
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free constrained PCG solve.
+//
+// For callers that cannot allocate device memory themselves: a MEX file that
+// works on gpuArray data (MATLAB owns the device allocator and its memory
+// pool), a plugin inside a host application that forbids cudaMalloc on its
+// solve path, or a code running under a fixed device-memory budget.  Inputs
+// and outputs are the caller's device arrays; every temporary (Krylov
+// vectors, partial sums, constraint masks, per-solve scalars) lives in the
+// file-scope array g_na_scratch, sized for at most UA_NOALLOC_MAX_ROWS
+// unknowns and UA_NOALLOC_MAX_CONSTRAINTS constraint rows (about 8.5 MB).
+// Every device that loads the library holds this array until the process
+// exits.  All calls on a device share it and each call overwrites it, so
+// calls that overlap on the GPU (two host threads, or calls queued on
+// different streams) race and must be serialised by the caller.  The first
+// call on a device looks up the array's device address with
+// cudaGetSymbolAddress (make that first call before any stream capture);
+// later calls reuse the address.  Work is queued on cudaStreamPerThread.
+// ---------------------------------------------------------------------------
+constexpr size_t kNaAlign = 256;
+constexpr size_t na_align(size_t b) { return (b + kNaAlign - 1) & ~(kNaAlign - 1); }
+constexpr int kNaMaxRb = (UA_NOALLOC_MAX_ROWS + kRB - 1) / kRB;
+constexpr int kNaSmallInts = 2 * kNaMaxRb + 16;
+constexpr size_t kNaScratchBytes =
+    na_align(6 * sizeof(double) * (size_t)UA_NOALLOC_MAX_ROWS) +        // X, r, z, p, q, invd
+    na_align(2 * sizeof(int) * (size_t)UA_NOALLOC_MAX_ROWS) +           // diagpos, dof_con
+    na_align((size_t)UA_NOALLOC_MAX_ROWS) +                             // cmask
+    na_align(sizeof(int) * (size_t)kNaSmallInts) +                      // row blocks, offsets, flags
+    na_align(sizeof(double) * (4 * (size_t)kNaMaxRb + SV_COUNT)) +     // partial sums, scalars
+    na_align(2 * sizeof(int) * (size_t)UA_NOALLOC_MAX_CONSTRAINTS) +    // con_dof, con_sys
+    na_align(3 * sizeof(double) * (size_t)UA_NOALLOC_MAX_CONSTRAINTS);  // con_rhs, dlam, grhs
+
+static __device__ __align__(256) unsigned char g_na_scratch[kNaScratchBytes];
+
+constexpr int kNaMaxDevices = 64;
+static void* g_na_addr[kNaMaxDevices];
+
+// Clears the per-call state.  flags[0]: a free row has no diagonal entry;
+// flags[1]: a dof is constrained twice (B*B' not diagonal); flags[2]: a
+// constraint entry is out of range or zero.
+__global__ void k_na_setup(int n, const int* rowptr, const int* col, int* diagpos, unsigned char* cmask,
+                           int* dof_con, double* X, int* rb_start, int* rb_sys, int nrb, int* sys_rb_off,
+                           int* sys_con_off, int nl, int* sel, int* flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    int dp = -1;
+    for (int j = rowptr[i]; j < rowptr[i + 1]; ++j)
+      if (col[j] == i) dp = j;
+    diagpos[i] = dp;
+    cmask[i] = 0;
+    dof_con[i] = -1;
+    X[i] = 0.0;
+  }
+  if (i <= nrb) rb_start[i] = i < nrb ? i * kRB : n;
+  if (i < nrb) rb_sys[i] = 0;
+  if (i == 0) {
+    sys_rb_off[0] = 0; sys_rb_off[1] = nrb;
+    sys_con_off[0] = 0; sys_con_off[1] = nl;
+    sel[0] = 1;
+    flags[0] = flags[1] = flags[2] = 0;
+  }
+}
+
+__global__ void k_na_constraints(int n, int nl, const int* Ldof, const double* Lval, const double* g,
+                                 unsigned char* cmask, int* dof_con, int* con_dof, int* con_sys, double* con_rhs,
+                                 int* flags) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nl) return;
+  const int d = Ldof[c];
+  const double l = Lval[c];
+  con_sys[c] = 0;
+  if (d < 0 || d >= n || l == 0.0) {
+    atomicExch(&flags[2], 1);
+    con_dof[c] = 0;
+    con_rhs[c] = 0;
+    return;
+  }
+  if (atomicCAS(&dof_con[d], -1, c) != -1) atomicExch(&flags[1], 1);
+  cmask[d] = 1;
+  con_dof[c] = d;
+  con_rhs[c] = g[c] / l;  // x_d = g/l (ABfgPreEliminate.m:63 with the row scaled to unit norm)
+}
+
+__global__ void k_na_check_diag(int n, const unsigned char* cmask, int* diagpos, const int* rowptr, int* flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || diagpos[i] >= 0) return;
+  if (!cmask[i]) atomicExch(&flags[0], 1);
+  diagpos[i] = rowptr[i] < rowptr[n] ? rowptr[i] : 0;  // constrained row: the value read is not used
+}
+
+__global__ void k_na_multiplier(int nl, const double* dlam, const double* Lval, double* y) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nl) y[c] = dlam[c] / Lval[c];
+}
+
+extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr, const int32_t* Acol,
+                                               const double* Aval, int32_t nl, const int32_t* Ldof,
+                                               const double* Lval, const double* f, const double* g, double* x,
+                                               double* y, double rtol, int32_t maxit, int32_t* its,
+                                               int32_t device) {
+  if (n <= 0 || n > UA_NOALLOC_MAX_ROWS)
+    return set_error(UA_ERR_INVALID, "ua_solve_kape_symmetric_noalloc: n=%d is outside 1..%d (UA_NOALLOC_MAX_ROWS)",
+                     n, UA_NOALLOC_MAX_ROWS);
+  if (nl < 0 || nl > UA_NOALLOC_MAX_CONSTRAINTS)
+    return set_error(UA_ERR_INVALID,
+                     "ua_solve_kape_symmetric_noalloc: nl=%d is outside 0..%d (UA_NOALLOC_MAX_CONSTRAINTS)", nl,
+                     UA_NOALLOC_MAX_CONSTRAINTS);
+  if (!Arowptr || !Acol || !Aval || !f || !x || (nl > 0 && (!Ldof || !Lval || !g || !y)))
+    return set_error(UA_ERR_INVALID, "ua_solve_kape_symmetric_noalloc: null device pointer");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_error(UA_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= ndev || device >= kNaMaxDevices) return set_error(UA_ERR_INVALID, "bad device ordinal %d", device);
+  UA_CUDA_TRY(cudaSetDevice(device));
+  if (!g_na_addr[device]) {  // once per device, with that device current
+    void* a = nullptr;
+    UA_CUDA_TRY(cudaGetSymbolAddress(&a, g_na_scratch));
+    g_na_addr[device] = a;
+  }
+  // carve the scratch array
+  unsigned char* base = (unsigned char*)g_na_addr[device];
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    void* q = base + off;
+    off += na_align(bytes);
+    return q;
+  };
+  const size_t R = UA_NOALLOC_MAX_ROWS, Cn = UA_NOALLOC_MAX_CONSTRAINTS;
+  double* vec = (double*)carve(6 * sizeof(double) * R);
+  int* ivec = (int*)carve(2 * sizeof(int) * R);
+  unsigned char* cmask = (unsigned char*)carve(R);
+  int* small = (int*)carve(sizeof(int) * kNaSmallInts);
+  double* dsmall = (double*)carve(sizeof(double) * (4 * (size_t)kNaMaxRb + SV_COUNT));
+  int* con_i = (int*)carve(2 * sizeof(int) * Cn);
+  double* con_d = (double*)carve(3 * sizeof(double) * Cn);
+  const int nrb = (n + kRB - 1) / kRB;
+
+  // a one-system view: scratch for temporaries, the caller's arrays in place
+  ua_mesh view;
+  view.device = device;
+  view.ndof = 2;
+  view.nod = 6;
+  view.ndof_total = n;
+  view.dm.nsys = 1;
+  view.stream = cudaStreamPerThread;
+  Work w;
+  static thread_local double h_sysv[SV_COUNT];
+  static thread_local int h_int[8];
+  w.nsys = 1; w.nrb = nrb; w.nc = nl;
+  w.X = vec; w.kr = vec + R; w.kz = vec + 2 * R; w.kp = vec + 3 * R; w.kq = vec + 4 * R; w.invd = vec + 5 * R;
+  w.diagpos = ivec; w.dof_con = ivec + R;
+  w.cmask = cmask;
+  w.rb_start = small;                          // kNaMaxRb + 1
+  w.rb_sys = small + kNaMaxRb + 1;             // kNaMaxRb
+  w.sys_rb_off = small + 2 * kNaMaxRb + 1;     // 2
+  w.sys_con_off = small + 2 * kNaMaxRb + 3;    // 2
+  w.sel = small + 2 * kNaMaxRb + 5;
+  w.done = small + 2 * kNaMaxRb + 6;
+  w.its = small + 2 * kNaMaxRb + 7;
+  w.status = small + 2 * kNaMaxRb + 8;
+  int* flags = small + 2 * kNaMaxRb + 9;       // 3
+  w.part = dsmall; w.sysv = dsmall + 4 * kNaMaxRb;
+  w.con_dof = con_i; w.con_sys = con_i + Cn;
+  w.con_rhs = con_d; w.dlam = con_d + Cn; w.grhs = con_d + 2 * Cn;
+  w.rowptr = const_cast<int*>(Arowptr);
+  w.colind = const_cast<int*>(Acol);
+  w.Kd = const_cast<double*>(Aval);
+  w.frhs = const_cast<double*>(f);
+  w.dX = x;
+  w.h_sysv = h_sysv;
+  w.h_int = h_int;
+  view.work = &w;
+  cudaStream_t st = view.stream;
+  const int nb = (std::max(n, nrb + 1) + 255) / 256;
+  k_na_setup<<<nb, 256, 0, st>>>(n, Arowptr, Acol, w.diagpos, cmask, w.dof_con, w.X, w.rb_start, w.rb_sys, nrb,
+                                 w.sys_rb_off, w.sys_con_off, nl, w.sel, flags);
+  if (nl)
+    k_na_constraints<<<(nl + 255) / 256, 256, 0, st>>>(n, nl, Ldof, Lval, g, cmask, w.dof_con, w.con_dof, w.con_sys,
+                                                      w.con_rhs, flags);
+  k_na_check_diag<<<(n + 255) / 256, 256, 0, st>>>(n, cmask, w.diagpos, Arowptr, flags);
+  int rc = UA_OK;
+  int hf[3] = {0, 0, 0};
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    view.work = nullptr;
+    return set_error(UA_ERR_CUDA, "no-alloc set-up failed");
+  }
+  if (hf[2]) rc = set_error(UA_ERR_INVALID, "constraint row with a dof out of range or a zero coefficient");
+  else if (hf[1]) rc = set_error(UA_ERR_INVALID, "B*B' not diagonal (a dof constrained twice)");
+  else if (hf[0]) rc = set_error(UA_ERR_INVALID, "a free row has no diagonal entry");
+  if (rc == UA_OK) {
+    ua_params p;
+    ua_params_default(&p);
+    p.krylov_rtol = rtol > 0 ? rtol : 1e-12;
+    p.krylov_maxit = maxit > 0 ? maxit : 10 * n + 100;
+    int kits[1] = {1};
+    rc = pcg_t<double, double>(&view, &p, w.Kd, kits);
+    if (rc == UA_OK) {
+      if (nl) k_na_multiplier<<<(nl + 255) / 256, 256, 0, st>>>(nl, w.dlam, Lval, y), ++g_launches;
+      int status = 0;
+      if (cudaMemcpyAsync(&status, w.status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess)
+        rc = set_error(UA_ERR_CUDA, "no-alloc solve failed");
+      else if (status)
+        rc = set_error(UA_ERR_KRYLOV, "PCG breakdown: A is not positive definite on the free dofs");
+      if (its) *its = kits[0];
+    }
+  }
+  view.work = nullptr;
   return rc;
 }
