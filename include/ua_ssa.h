@@ -218,6 +218,27 @@ int ua_uv_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs
 int ua_uv_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fields, const ua_bcs* bcs,
                        ua_newton_report* reports);
 
+/* uvhAssembly (uvhAssembly.m:1 -> uvhMatrixAssembly.m:6-585, integration
+ * points uvhAssemblyIntPointImplicitSUPG.m:10-531, nodal loop
+ * uvhNodalLoopSSTREAM.m:1-229) for a single-mesh ndof=3 handle.  Level 1 is
+ * F->ub, F->vb, F->h1 (u, v, h at t+dt); level 0 is F->h0, u0, v0, as0, ab0;
+ * F->as1, ab1, dadh (NULL = 0) the mass balance; F->dt the time step.
+ * mode UA_ASM_ZERO_R is CtrlVar.uvhMatrixAssembly.ZeroFields.  R: 3*Nnodes;
+ * K: the unsymmetric tangent on the structural pattern (9 blocks per node pair). */
+int ua_uvh_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, int32_t mode,
+                    double* R, double* Kvals, double* Tint, double* Fext);
+
+/* Implicit uvh step: SSTREAM_TransientImplicit.m:6-717 (via uvh.m:45 ->
+ * uvh2D.m:20, no active-set thickness constraints).  F->ub, vb, h1: start
+ * values in, solution out.  luvh: [l.ubvb; l.h] in/out (may be NULL).  The
+ * inner solve is Jacobi-preconditioned BiCGStab on the constrained system. */
+int ua_uvh_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs,
+                  double* luvh, int32_t nl, ua_newton_report* rep);
+
+/* Batched implicit uvh step: fields[i], bcs[i], reports[i] per system. */
+int ua_uvh_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fields, const ua_bcs* bcs,
+                        ua_newton_report* reports);
+
 /* Number of rows of the constraint matrix L built from bcs (CreateLuv.m). */
 int ua_constraint_count(const ua_mesh* m, const ua_bcs* bcs, int32_t ndof, int32_t* nc);
 

@@ -1085,3 +1085,350 @@ def uv(p: Params, mua: MUA, bcs: BCs, F: Fields, lubvb=None, solver=None, verbos
         l0 = res.lubvb * 0 if res.lubvb is not None else None
         res = sstream2dnr2(p, mua, bcs, F2, l0, solver, verbose)
     return res
+
+
+# ---------------------------------------------------------------------------
+# uvh implicit transient step — uvhMatrixAssembly.m, uvhAssemblyIntPointImplicitSUPG.m,
+# uvhNodalLoopSSTREAM.m, SUPGtau.m, CalcCostFunctionNRuvh.m, AssembleLuvhSSTREAM.m,
+# SSTREAM_TransientImplicit.m
+# ---------------------------------------------------------------------------
+
+
+def tri_area_fe(coordinates, connectivity):
+    """TriAreaFE.m / TriArea.m: area from the three corner nodes."""
+    nod = connectivity.shape[1]
+    c = connectivity if nod == 3 else connectivity[:, [0, 2, 4]]
+    x = coordinates[c, 0]; y = coordinates[c, 1]
+    return 0.5 * np.abs((x[:, 0] - x[:, 2]) * (y[:, 1] - y[:, 0]) - (x[:, 0] - x[:, 1]) * (y[:, 2] - y[:, 0]))
+
+
+def supg_tau(p: Params, v, l, dt):
+    """SUPGtau.m:7-111 for the configured option (default "taus", :61-62)."""
+    taut = dt / 2 + EPS
+    taus = l / (2 * v + p.SpeedZero)
+    if p.uvh_SUPG_tau == "taus":
+        tau = taus
+    elif p.uvh_SUPG_tau == "taut":
+        tau = taut + 0 * v
+    elif p.uvh_SUPG_tau == "tau2":
+        ECN = taut / taus
+        tau = (dt / 2) / (1 + ECN)
+    elif p.uvh_SUPG_tau == "tau1":
+        ECN = taut / taus
+        with np.errstate(divide="ignore", invalid="ignore"):
+            K = 1 / np.tanh(ECN) - 1 / ECN
+        K = np.where(ECN < 1e-6, ECN / 3, K)
+        tau = K * taus
+    else:
+        raise ValueError(p.uvh_SUPG_tau)
+    return p.uvh_SUPG_tauMultiplier * tau
+
+
+@dataclass
+class UvhState:
+    """Fields of the two time levels (F0 at t, F1 at t+dt), UaFields.m subset."""
+    h: np.ndarray
+    ub: np.ndarray
+    vb: np.ndarray
+    as_: np.ndarray
+    ab: np.ndarray
+
+    def copy(self):
+        return UvhState(self.h.copy(), self.ub.copy(), self.vb.copy(), self.as_.copy(), self.ab.copy())
+
+
+def uvh_matrix_assembly(p: Params, mua: MUA, F: Fields, S0: UvhState, S1: UvhState, dt, Ronly=False,
+                        ZeroFields=False):
+    """uvhMatrixAssembly.m:6-585 (sequential; no level set, no thickness penalty or
+    barrier, MassBalanceGeometryFeedback=0 so dadh=0; post-2025 Kxh/Kyh).
+
+    F carries the time-independent fields (S, B, rho, AGlen, n, C, m, rhow, g,
+    alpha).  Returns (R, K) with R = Tint-Fext (3Nn) and K the unsymmetrised CSC.
+    """
+    S0 = S0.copy(); S1 = S1.copy()
+    if ZeroFields:  # :9-15
+        S1.ub = S1.ub * 0; S1.vb = S1.vb * 0
+        S0.ub = S0.ub * 0; S0.vb = S0.vb * 0
+        S1.h = S0.h.copy()
+        S1.as_ = np.abs(S1.ab) + 1; S1.ab = np.abs(S1.ab)
+        S0.as_ = np.abs(S0.ab) + 1; S0.ab = np.abs(S0.ab)
+    g = F.g; rhow = F.rhow; theta = p.theta
+    ca, sa = math.cos(F.alpha), math.sin(F.alpha)
+    b1, s1, _ = calc_bs_from_hBS(p, S1.h, F.S, F.B, F.rho, rhow)  # :36
+    Nele, nod, Nn = mua.Nele, mua.nod, mua.Nnodes
+    neq = 3 * Nn
+    conn = mua.connectivity
+    G = lambda v: v[conn]
+    hnod, unod, vnod = G(S1.h), G(S1.ub), G(S1.vb)
+    Cnod, mnod, Anod, nnod = G(F.C), G(F.m), G(F.AGlen), G(F.n)
+    Snod, Bnod, rhonod, bnod = G(F.S), G(F.B), G(F.rho), G(b1)
+    h0nod, u0nod, v0nod = G(S0.h), G(S0.ub), G(S0.vb)
+    as0nod, ab0nod, as1nod, ab1nod = G(S0.as_), G(S0.ab), G(S1.as_), G(S1.ab)
+    dadhnod = np.zeros((Nele, nod))
+    if not Ronly:
+        Kb = {k: np.zeros((Nele, nod, nod)) for k in ("xu", "xv", "xh", "yu", "yv", "yh", "hu", "hv", "hh")}
+    Tx = np.zeros((Nele, nod)); Ty = np.zeros((Nele, nod)); Th = np.zeros((Nele, nod))
+    Fx = np.zeros((Nele, nod)); Fy = np.zeros((Nele, nod)); Fh = np.zeros((Nele, nod))
+    areas = tri_area_fe(mua.coordinates, conn)
+    for Iint in range(mua.nip):  # :356-383 -> uvhAssemblyIntPointImplicitSUPG.m
+        fun = shape_fun(nod, mua.points[Iint])
+        Deriv = mua.Deriv[:, :, :, Iint]
+        detJ = mua.DetJ[:, Iint]
+        hint = hnod @ fun; uint = unod @ fun; vint = vnod @ fun
+        Cint = Cnod @ fun; mint = mnod @ fun
+        AGlenint = Anod @ fun; nint = nnod @ fun
+        h0int = h0nod @ fun; u0int = u0nod @ fun; v0int = v0nod @ fun
+        a1int = as1nod @ fun + ab1nod @ fun  # :64-66 (as1int+ab1int)
+        a0int = as0nod @ fun + ab0nod @ fun
+        dadhint = dadhnod @ fun
+        h1barr = 0.0; h0barr = 0.0; lambda_h = 1.0  # :77
+        Bint = Bnod @ fun; Sint = Snod @ fun; rhoint = rhonod @ fun
+        Hint = Sint - Bint
+        hfint = rhow * Hint / rhoint  # :106
+        Heint = heaviside_approx(p.kH, hint - hfint, p.Hh0)  # :114-120
+        HEint = heaviside_approx(p.kH, hfint - hint, p.Hh0)
+        deltaint = dirac_delta(p.kH, hint - hfint, p.Hh0)
+        Deltaint = dirac_delta(p.kH, hfint - hint, p.Hh0)
+        Hposint = heaviside_approx(p.kH, Hint, p.Hh0) * Hint
+        dint = HEint * rhoint * hint / rhow + Heint * Hposint
+        Dddhint = HEint * rhoint / rhow - Deltaint * hint * rhoint / rhow + deltaint * Hposint
+        z = lambda: np.zeros(Nele)
+        dhdx, dhdy, dh0dx, dh0dy = z(), z(), z(), z()
+        exx0, eyy0, exx, eyy, exy = z(), z(), z(), z(), z()
+        dbdx, dbdy, drhodx, drhody = z(), z(), z(), z()
+        for Inod in range(nod):  # :132-148
+            Dx = Deriv[:, 0, Inod]; Dy = Deriv[:, 1, Inod]
+            dhdx = dhdx + Dx * hnod[:, Inod]; dhdy = dhdy + Dy * hnod[:, Inod]
+            dh0dx = dh0dx + Dx * h0nod[:, Inod]; dh0dy = dh0dy + Dy * h0nod[:, Inod]
+            exx0 = exx0 + Dx * u0nod[:, Inod]; eyy0 = eyy0 + Dy * v0nod[:, Inod]
+            dbdx = dbdx + Dx * bnod[:, Inod]; dbdy = dbdy + Dy * bnod[:, Inod]
+            drhodx = drhodx + Dx * rhonod[:, Inod]; drhody = drhody + Dy * rhonod[:, Inod]
+            exx = exx + Dx * unod[:, Inod]; eyy = eyy + Dy * vnod[:, Inod]
+            exy = exy + 0.5 * (Dx * vnod[:, Inod] + Dy * unod[:, Inod])
+        etaint, Eint = effective_viscosity(p, AGlenint, nint, exx, eyy, exy)  # :149
+        taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, dtauxdh, dtauydh = basal_drag_weertman(
+            p, Heint, deltaint, uint, vint, Cint, mint)  # :150-151
+        l = np.sqrt(2 * areas)  # :156
+        speed0 = np.sqrt(u0int * u0int + v0int * v0int + p.SpeedZero ** 2)  # :157
+        tau0 = p.SUPG_beta0 * supg_tau(p, speed0, l, dt)  # :158-159
+        detJw = detJ * mua.weights[Iint]
+        # uvhNodalLoopSSTREAM.m
+        qx1dx = rhoint * exx * hint + rhoint * uint * dhdx + drhodx * uint * hint  # :39
+        qy1dy = rhoint * eyy * hint + rhoint * vint * dhdy + drhody * vint * hint
+        qx0dx = rhoint * exx0 * h0int + rhoint * u0int * dh0dx + drhodx * u0int * h0int
+        qy0dy = rhoint * eyy0 * h0int + rhoint * v0int * dh0dy + drhody * v0int * h0int
+        for Inod in range(nod):
+            DxI = Deriv[:, 0, Inod]; DyI = Deriv[:, 1, Inod]
+            SUPG = fun[Inod] + 0.5 * tau0 * (u0int * DxI + v0int * DyI)  # :55
+            funI = fun[Inod]
+            if not Ronly:
+                for Jnod in range(nod):
+                    DxJ = Deriv[:, 0, Jnod]; DyJ = Deriv[:, 1, Jnod]; fJ = fun[Jnod]
+                    Deu = Eint * ((2 * exx + eyy) * DxJ + exy * DyJ)
+                    Dev = Eint * ((2 * eyy + exx) * DyJ + exy * DxJ)
+                    E11 = hint * (4 * exx + 2 * eyy) * Deu * DxI + 2 * hint * exy * Deu * DyI
+                    E12 = hint * (4 * exx + 2 * eyy) * Dev * DxI + 2 * hint * exy * Dev * DyI
+                    E22 = hint * (4 * eyy + 2 * exx) * Dev * DyI + 2 * hint * exy * Dev * DxI
+                    E21 = hint * (4 * eyy + 2 * exx) * Deu * DyI + 2 * hint * exy * Deu * DxI
+                    Kb["xu"][:, Inod, Jnod] += (4 * hint * etaint * DxI * DxJ + hint * etaint * DyI * DyJ + E11
+                                                + dtauxdu * fJ * funI) * detJw
+                    Kb["yv"][:, Inod, Jnod] += (4 * hint * etaint * DyI * DyJ + hint * etaint * DxI * DxJ + E22
+                                                + dtauydv * fJ * funI) * detJw
+                    Kb["xv"][:, Inod, Jnod] += (etaint * hint * (2 * DxI * DyJ + DyI * DxJ) + E12
+                                                + dtauxdv * fJ * funI) * detJw
+                    Kb["yu"][:, Inod, Jnod] += (etaint * hint * (2 * DyI * DxJ + DxI * DyJ) + E21
+                                                + dtauydu * fJ * funI) * detJw
+                    Kb["xh"][:, Inod, Jnod] += (etaint * (4 * exx + 2 * eyy) * DxI * fJ
+                                                + etaint * 2 * exy * DyI * fJ
+                                                + dtauxdh * funI * fJ
+                                                + ca * g * (rhoint - rhow * Dddhint) * dbdx * funI * fJ
+                                                - sa * g * rhoint * funI * fJ
+                                                - ca * g * (rhoint * hint - rhow * dint * Dddhint) * DxI * fJ) * detJw
+                    Kb["yh"][:, Inod, Jnod] += (etaint * (4 * eyy + 2 * exx) * DyI * fJ
+                                                + etaint * 2 * exy * DxI * fJ
+                                                + dtauydh * funI * fJ
+                                                + ca * g * (rhoint - rhow * Dddhint) * dbdy * funI * fJ
+                                                - ca * g * (rhoint * hint - rhow * dint * Dddhint) * DyI * fJ) * detJw
+                    Kb["hu"][:, Inod, Jnod] += theta * (rhoint * dhdx * fJ + drhodx * hint * fJ
+                                                        + rhoint * hint * DxJ) * SUPG * detJw * dt
+                    Kb["hv"][:, Inod, Jnod] += theta * (rhoint * dhdy * fJ + drhody * hint * fJ
+                                                        + rhoint * hint * DyJ) * SUPG * detJw * dt
+                    Kb["hh"][:, Inod, Jnod] += (rhoint * fJ - dt * theta * rhoint * dadhint * fJ
+                                                + dt * theta * rhoint * fJ * h1barr / lambda_h
+                                                + dt * theta * (rhoint * exx * fJ + drhodx * uint * fJ + rhoint * uint * DxJ
+                                                                + rhoint * eyy * fJ + drhody * vint * fJ
+                                                                + rhoint * vint * DyJ)) * SUPG * detJw
+            t1 = -ca * g * (rhoint * hint - rhow * dint) * dbdx * funI + rhoint * g * hint * sa * funI  # :189
+            t2 = 0.5 * ca * g * (rhoint * hint ** 2 - rhow * dint ** 2) * DxI
+            t3 = hint * etaint * (4 * exx + 2 * eyy) * DxI
+            t4 = hint * etaint * 2 * exy * DyI
+            t5 = taux * funI
+            Tx[:, Inod] += (t3 + t4 + t5) * detJw
+            Fx[:, Inod] += (t1 + t2) * detJw
+            t1 = -ca * g * (rhoint * hint - rhow * dint) * dbdy * funI
+            t2 = 0.5 * ca * g * (rhoint * hint ** 2 - rhow * dint ** 2) * DyI
+            t3 = hint * etaint * (4 * eyy + 2 * exx) * DyI
+            t4 = hint * etaint * 2 * exy * DxI
+            t5 = tauy * funI
+            Ty[:, Inod] += (t3 + t4 + t5) * detJw
+            Fy[:, Inod] += (t1 + t2) * detJw
+            qterm = dt * (theta * qx1dx + (1 - theta) * qx0dx + theta * qy1dy + (1 - theta) * qy0dy) * SUPG  # :212
+            dhdt = rhoint * (h0int - hint + dt * (1 - theta) * h0barr + dt * theta * h1barr) * SUPG
+            accterm = dt * rhoint * ((1 - theta) * a0int + theta * a1int) * SUPG
+            th = -dhdt
+            fh = accterm - qterm
+            Th[:, Inod] += th * detJw
+            Fh[:, Inod] += fh * detJw
+    iR = np.concatenate([np.concatenate([conn[:, I], conn[:, I] + Nn, conn[:, I] + 2 * Nn]) for I in range(nod)])
+    Tval = np.concatenate([np.concatenate([Tx[:, I], Ty[:, I], Th[:, I]]) for I in range(nod)])
+    Fval = np.concatenate([np.concatenate([Fx[:, I], Fy[:, I], Fh[:, I]]) for I in range(nod)])
+    R = np.bincount(iR, weights=Tval, minlength=neq) - np.bincount(iR, weights=Fval, minlength=neq)  # :238
+    if any(np.isnan(R)):
+        raise FloatingPointError("uvhMatrixAssembly:NaNinR")
+    K = None
+    if not Ronly:  # :241-297
+        off = {"x": 0, "y": Nn, "h": 2 * Nn}
+        Ii, Jj, Xv = [], [], []
+        for Inod in range(nod):
+            for Jnod in range(nod):
+                for key in ("xu", "xv", "xh", "yu", "yv", "yh", "hu", "hv", "hh"):
+                    Ii.append(conn[:, Inod] + off[key[0]])
+                    Jj.append(conn[:, Jnod] + {"u": 0, "v": Nn, "h": 2 * Nn}[key[1]])
+                    Xv.append(Kb[key][:, Inod, Jnod])
+        K = _matlab_sparse(np.concatenate(Ii), np.concatenate(Jj), np.concatenate(Xv), neq, neq)
+    return R, K
+
+
+def create_Luvh(Nnodes, bcs: BCs):
+    """AssembleLuvhSSTREAM.m:5-72 with BCs2MLC.m (Luv as create_Luv; Lh from
+    createLh.m: ties, then fixed h nodes in the given order), rows scaled by ScaleL."""
+    Luv, cuv = create_Luv(Nnodes, bcs)
+    hn = np.asarray(bcs.hFixedNode, dtype=np.int64)
+    if hn.size:
+        Lh = _matlab_sparse(np.arange(hn.size), hn, np.ones(hn.size), hn.size, Nnodes).tocsr()
+        ch = np.asarray(bcs.hFixedValue, dtype=float)
+    else:
+        Lh, ch = None, None
+    blocks, rhs = [], []
+    if Luv is not None:
+        blocks.append(sp.hstack([Luv, sp.csr_matrix((Luv.shape[0], Nnodes))]))
+        rhs.append(cuv)
+    if Lh is not None:
+        blocks.append(sp.hstack([sp.csr_matrix((Lh.shape[0], 2 * Nnodes)), Lh]))
+        rhs.append(ch)
+    if not blocks:
+        return None, None
+    return sp.vstack(blocks).tocsr(), np.concatenate(rhs)
+
+
+def calc_cost_function_nr_uvh(p, mua, F, S0, S1, dt, dub, dvb, dh, dl, L, luvh, cuvh, gamma, fext0):
+    """CalcCostFunctionNRuvh.m:12-105.  Returns (r, rForce, rWork, D2)."""
+    if gamma != gamma:
+        raise ValueError("CalcCostFunctionNRuvh:nan")
+    S1g = S1.copy()
+    S1g.ub = S1.ub + gamma * dub; S1g.vb = S1.vb + gamma * dvb; S1g.h = S1.h + gamma * dh
+    R, _ = uvh_matrix_assembly(p, mua, F, S0, S1g, dt, Ronly=True)
+    if L is not None:
+        lg = luvh + gamma * dl
+        frhs = -R - L.T @ lg
+        grhs = cuvh - L @ np.concatenate([S1g.ub, S1g.vb, S1g.h])
+        fg = np.concatenate([frhs, grhs]); dd = np.concatenate([dub, dvb, dh, dl])
+    else:
+        fg = -R; dd = np.concatenate([dub, dvb, dh])
+    D2 = fg @ dd
+    rWork = D2 ** 2
+    rForce = (fg @ fg) / (fext0 @ fext0 + 1000 * EPS)
+    return rForce, rForce, rWork, D2
+
+
+def uvh_criteria(p: Params, rForce, rWork, iteration, gamma):
+    """SSTREAM_TransientImplicit.m:81-89."""
+    if gamma > max(p.uvhExitBackTrackingStepLength, p.BacktrackingGammaMin):
+        a, o = p.uvhDesiredWorkAndForceTolerances, p.uvhDesiredWorkOrForceTolerances
+    else:
+        a, o = p.uvhAcceptableWorkAndForceTolerances, p.uvhAcceptableWorkOrForceTolerances
+    return ((rWork < a[0] and rForce < a[1]) and (rWork < o[0] or rForce < o[1]) and iteration >= p.NRitmin)
+
+
+@dataclass
+class UvhResult:
+    ub: np.ndarray
+    vb: np.ndarray
+    h: np.ndarray
+    luvh: np.ndarray
+    converged: bool
+    iterations: int
+    records: list
+
+
+def sstream_transient_implicit(p: Params, mua: MUA, bcs: BCs, F: Fields, S0: UvhState, S1: UvhState, dt,
+                               luvh=None, verbose=False, solver=None):
+    """SSTREAM_TransientImplicit.m:6-717 (uvh2D.m:20), NRitmin>=1 branch, no mass-balance
+    geometry feedback, GuardAgainstWildExtrapolation off."""
+    if solver is None:
+        solver = abfg_pre_eliminate
+    Nn = mua.Nnodes
+    S1 = S1.copy()
+    L, cuvh = create_Luvh(Nn, bcs)  # :35
+    nc = 0 if cuvh is None else cuvh.size
+    luvh = np.zeros(nc) if luvh is None or len(luvh) != nc else luvh.copy()
+    dl = np.zeros(nc)
+    # uvhMakeInitialIterateFeasible (:37-41)
+    S1.ub = S1.ub.copy(); S1.vb = S1.vb.copy(); S1.h = S1.h.copy()
+    S1.ub[bcs.ubFixedNode] = bcs.ubFixedValue
+    S1.vb[bcs.vbFixedNode] = bcs.vbFixedValue
+    if len(bcs.hFixedNode):
+        S1.h[bcs.hFixedNode] = bcs.hFixedValue
+    fext0, _ = uvh_matrix_assembly(p, mua, F, S0, S1, dt, Ronly=True, ZeroFields=True)  # :53-56
+    rWork = math.nan; rForce = math.inf; r = math.inf; r0 = math.inf  # :66-71
+    iteration = 0
+    converged = False
+    bt_conv = 1
+    gamma = 1.0
+    rRatioVector = np.zeros(3)
+    records = []
+    while True:
+        if rWork != rWork:
+            rWork = 0.0
+        if uvh_criteria(p, rForce, rWork, iteration, gamma):
+            converged = True
+            break
+        if iteration > p.NRitmax:
+            converged = False
+            break
+        if bt_conv == 0 or gamma == 0:  # :104-110
+            converged = False
+            break
+        with np.errstate(invalid="ignore"):
+            rRatio = r / r0
+        rRatioVector[iteration % 3] = rRatio  # :111-124
+        if np.all(rRatioVector > 0.98):
+            converged = rWork < 1e-14
+            break
+        iteration += 1
+        Ruvh, K = uvh_matrix_assembly(p, mua, F, S0, S1, dt)  # :127
+        if L is not None:
+            frhs = -Ruvh - L.T @ luvh
+            grhs = cuvh - L @ np.concatenate([S1.ub, S1.vb, S1.h])
+        else:
+            frhs = -Ruvh; grhs = np.zeros(0)
+        duvh, dl = solver(K, L, frhs, grhs)  # :136 solveKApe -> ABfgPreEliminate
+        dub = duvh[:Nn].copy(); dvb = duvh[Nn:2 * Nn].copy(); dh = duvh[2 * Nn:].copy()
+        if dl is None:
+            dl = np.zeros(nc)
+        func = lambda gm: calc_cost_function_nr_uvh(p, mua, F, S0, S1, dt, dub, dvb, dh, dl, L, luvh, cuvh, gm, fext0)
+        r0 = func(0.0)[0]
+        r1 = func(1.0)[0]
+        ls = rlinemin_newton(p, func, r0, r1, dub, dvb, dl)  # :157 (rLineminUa)
+        gamma, r = ls.gamma, ls.r
+        rForce, rWork = ls.rForce, ls.rWork
+        bt_conv = ls.info.Converged
+        S1.ub = S1.ub + gamma * dub  # :191-194
+        S1.vb = S1.vb + gamma * dvb
+        S1.h = S1.h + gamma * dh
+        luvh = luvh + gamma * dl
+        records.append(NewtonRecord(iteration, gamma, r0, r, rForce, rWork, ls.info.iarm))
+        if verbose:
+            print(f"NR-SSTREAM(uvh):{iteration:3d}/{ls.info.iarm:<2d} g={gamma:<14.7g} r/r0={r / r0:<14.7g} "
+                  f"r0={r0:<14.7g} r={r:<14.7g} rForce={rForce:<14.7g} rWork={rWork:<14.7g}")
+    return UvhResult(S1.ub, S1.vb, S1.h, luvh, converged, iteration, records)

@@ -38,3 +38,21 @@ def test_oracle_reproduces_fixture(path):
     u_ref = np.concatenate([z["sol_ub"], z["sol_vb"]])
     u = np.concatenate([res.ub, res.vb])
     assert np.linalg.norm(u - u_ref) <= 1e-10 * np.linalg.norm(u_ref)
+
+
+UVH_FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "uvh_*.npz")))
+
+
+@pytest.mark.parametrize("path", UVH_FIXTURES, ids=[os.path.basename(p) for p in UVH_FIXTURES])
+def test_oracle_reproduces_uvh_fixture(path):
+    z = np.load(path)
+    mua = R.create_mua(z["coordinates"], z["connectivity"])
+    F = R.Fields(h=z["h0"], S=z["S"], B=z["B"], rho=z["rho"], AGlen=z["AGlen"], n=z["n"], C=z["C"], m=z["m"],
+                 ub=z["u0"], vb=z["v0"], rhow=float(z["rhow"]), g=float(z["g"]))
+    S0 = R.UvhState(z["h0"], z["u0"], z["v0"], z["as_"], z["ab"])
+    S1 = R.UvhState(z["state_h"], z["state_ub"], z["state_vb"], z["as_"], z["ab"])
+    p = R.Params()
+    Rv, K = R.uvh_matrix_assembly(p, mua, F, S0, S1, float(z["dt"]))
+    Kz = sp.coo_matrix((z["K_val"], (z["K_row"], z["K_col"])), shape=K.shape).tocsc()
+    assert abs(K - Kz).max() <= 1e-13 * abs(Kz).max()
+    assert np.max(np.abs(Rv - z["R"])) <= 1e-13 * np.max(np.abs(z["R"]))

@@ -143,3 +143,54 @@ def test_newton_converges_quadratically():
     assert r[-1] < 1e-20
     # last steps: r_{k+1} <= C r_k^2 style reduction (ratio r/r0 falls super-linearly)
     assert res.records[-1].r / res.records[-1].r0 < 1e-6
+
+
+# --- uvh (implicit transient) ---------------------------------------------------------
+
+@pytest.mark.parametrize("nod", [3, 6])
+def test_uvh_tangent_is_reference_jacobian(nod):
+    """K of uvhMatrixAssembly matches the finite-difference derivative of R up to the
+    term the reference leaves out: the h-derivative of b inside t1 (uvhNodalLoopSSTREAM.m
+    :141-157 keeps (rho - rhow*Dddh)*dbdx but not (rho*h - rhow*d)*d(dbdx)/dh), which
+    vanishes for floating ice and for grounded ice away from the grounding line."""
+    Pb = synth.ice_stream_shelf(13, 7, nod=nod, seed=0, transient=True)
+    mua = R.create_mua(Pb.coordinates, Pb.connectivity)
+    rng = np.random.default_rng(1)
+    F = R.Fields(h=Pb.h, S=Pb.S, B=Pb.B, rho=Pb.rho, AGlen=Pb.AGlen, n=Pb.n, C=Pb.C, m=Pb.m, ub=Pb.ub, vb=Pb.vb)
+    N = mua.Nnodes
+    S0 = R.UvhState(Pb.h.copy(), 100 + 50 * rng.random(N), 20 * rng.standard_normal(N), Pb.as_, Pb.ab)
+    S1 = R.UvhState(Pb.h + 5 * rng.standard_normal(N), 100 + 50 * rng.random(N), 20 * rng.standard_normal(N),
+                    Pb.as_, Pb.ab)
+    p = R.Params()
+    Rv, K = R.uvh_matrix_assembly(p, mua, F, S0, S1, 0.1)
+    d = rng.standard_normal(3 * N)
+
+    def Rat(eps):
+        S = S1.copy()
+        S.ub = S1.ub + eps * d[:N]; S.vb = S1.vb + eps * d[N:2 * N]; S.h = S1.h + eps * d[2 * N:]
+        return R.uvh_matrix_assembly(p, mua, F, S0, S, 0.1, Ronly=True)[0]
+
+    fd = (Rat(1e-3) - Rat(-1e-3)) / 2e-3
+    assert np.linalg.norm(fd - K @ d) < 1e-3 * np.linalg.norm(K @ d)
+    # the velocity blocks are exact: perturb u, v only
+    d[2 * N:] = 0
+    fd = (Rat(1e-3) - Rat(-1e-3)) / 2e-3
+    assert np.linalg.norm(fd - K @ d) < 1e-6 * np.linalg.norm(K @ d)
+
+
+def test_uvh_newton_converges():
+    P = synth.ice_stream_shelf(21, 11, nod=3, seed=0, transient=True)
+    mua = R.create_mua(P.coordinates, P.connectivity)
+    p = R.Params()
+    p.set_force_tolerance(1e-20)
+    p.uvhDesiredWorkAndForceTolerances = (np.inf, 1e-20)
+    p.uvhDesiredWorkOrForceTolerances = (np.inf, 1e-20)
+    F = R.Fields(h=P.h, S=P.S, B=P.B, rho=P.rho, AGlen=P.AGlen, n=P.n, C=P.C, m=P.m, ub=P.ub, vb=P.vb)
+    bcs = R.BCs(ubFixedNode=P.ubFixedNode, ubFixedValue=P.ubFixedValue, vbFixedNode=P.vbFixedNode,
+                vbFixedValue=P.vbFixedValue)
+    uv = R.uv(p, mua, bcs, F)
+    S0 = R.UvhState(P.h.copy(), uv.ub, uv.vb, P.as_, P.ab)
+    res = R.sstream_transient_implicit(p, mua, bcs, F, S0, S0.copy(), 0.1)
+    assert res.converged and res.records[-1].rForce < 1e-20
+    # mass conservation sanity: with u=v from the diagnostic state, h changes by O(dt*div(q))
+    assert np.all(np.isfinite(res.h))

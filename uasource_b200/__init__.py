@@ -4,6 +4,7 @@ The compute path is libuassa.so (CUDA, sm_100a) behind the C-ABI in
 include/ua_ssa.h; ``uasource_b200.ua`` mirrors the reference's MATLAB
 interface on top of it.
 """
-from .ua import (CtrlVar, Fields, BCs, MUA, CreateMUA, CreateMUABatch, uvMatrixAssembly, uv, uv_batch, uv_resident,  # noqa: F401,E501
+from .ua import (CtrlVar, Fields, BCs, HBCs, MUA, CreateMUA, CreateMUABatch, uvMatrixAssembly, uv, uv_batch,  # noqa: F401,E501
+                 uv_resident, uvhAssembly, uvh,
                  solveKApeSymmetric, RunInfo)
 from .lib import UaError  # noqa: F401

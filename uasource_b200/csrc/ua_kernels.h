@@ -24,7 +24,29 @@ struct UvOut {
   double* Fext;           // optional
 };
 
+// Inputs of the uvh assembly (fields at both time levels; level-1 u, v, h in
+// the dof vector X, evaluated at X + gamma[s]*dX when dX is given).
+struct UvhIn {
+  const double *S, *B, *rho, *A, *n, *C, *m;
+  const double *h0, *u0, *v0, *as0, *ab0, *as1, *ab1, *dadh;  // dadh may be null (zero)
+  const double* X;
+  const double* dX;
+  const double* gamma;
+  const SysScal* scal;
+  const int* active;
+  int zero_fields;        // uvhMatrixAssembly.m:9-15
+};
+
+struct UvhPhys {
+  UvPhys uv;
+  double kH, Hh0, SpeedZero, theta, beta0, tau_mult;
+  int tau_kind;           // 0 taus, 1 taut, 2 tau1, 3 tau2
+};
+
 size_t uv_patch_smem(int nod, bool withK, bool fp32, int E);
+size_t uvh_patch_smem(int nod, bool withK, bool fp32, int E);
+int uvh_fields_per_node();
+cudaError_t launch_uvh_assembly(const ua_mesh* m, const UvhPhys& P, const UvhIn& in, const UvOut& out, bool withK);
 cudaError_t launch_uv_assembly(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, bool withK,
                                bool fp32K);
 

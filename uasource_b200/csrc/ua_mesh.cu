@@ -168,7 +168,16 @@ static void flip(int nod, int* l) {
 // and six residual parts.
 static size_t elem_smem_bytes(int nod, int ndof) {
   if (ndof == 2) return (size_t)(nod * (nod + 1) + nod * nod + 4 * nod) * sizeof(double);
-  return (size_t)(9 * nod * nod + 6 * nod) * sizeof(double);
+  return (size_t)(9 * nod * nod + 6 * nod + 19 * nod) * sizeof(double);  // + staged nodal fields
+}
+
+// Largest element count per patch: shared memory of the assembly kernel and,
+// for the uvh kernel (one thread per element node), its block size.
+static int max_patch_elements(int nod, int ndof) {
+  const size_t budget = ndof == 2 ? 160 * 1024 : 200 * 1024;
+  int e = (int)std::min<size_t>(1023, budget / elem_smem_bytes(nod, ndof));
+  if (ndof == 3) e = std::min(e, (nod == 3 ? 512 : 320) / nod);
+  return e;
 }
 
 extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, int32_t ndof, int32_t device,
@@ -293,8 +302,7 @@ extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, in
   m->ndof_total = m->h_dof_off[nsys];
   m->nnz_total = knz;
   // ---- patches (Morton-ordered node groups within each system) --------------------
-  const size_t smem_budget = 160 * 1024;
-  int emax = (int)std::min<size_t>(1023, smem_budget / elem_smem_bytes(nod, ndof));
+  const int emax = max_patch_elements(nod, ndof);
   std::vector<int> patch_sys, patch_node_ptr(1, 0), patch_nodes, patch_elem_ptr(1, 0), patch_elems;
   std::vector<int> patch_q_ptr(1, 0), pq_cptr(1, 0), prow_diag;
   std::vector<uint32_t> pq_rk;

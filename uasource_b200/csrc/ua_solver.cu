@@ -45,7 +45,7 @@ struct Prof {
 };
 enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2 };
 constexpr int kRedThreads = 256;
-enum { SV_RZ = 0, SV_PQ, SV_ALPHA, SV_BETA, SV_RR, SV_RR0, SV_TOL2, SV_NORM, SV_FF, SV_FD, SV_COUNT };
+enum { SV_RZ = 0, SV_PQ, SV_ALPHA, SV_BETA, SV_RR, SV_RR0, SV_TOL2, SV_NORM, SV_FF, SV_FD, SV_OMEGA, SV_COUNT };
 
 struct Work {
   int nsys = 0, nrb = 0, nc = 0;
@@ -77,6 +77,10 @@ struct Work {
   int* sys_con_off = nullptr;
   double* con_rhs = nullptr;
   double *lam = nullptr, *dlam = nullptr, *grhs = nullptr;
+  // uvh: level-0 state and mass balance (nodal), BiCGStab vectors
+  double *h0 = nullptr, *u0 = nullptr, *v0 = nullptr, *as0 = nullptr, *ab0 = nullptr, *as1 = nullptr,
+         *ab1 = nullptr, *dadh = nullptr;
+  void *krh = nullptr, *ks = nullptr, *ksh = nullptr, *kt = nullptr;
   // pinned host staging
   double* h_sysv = nullptr;
   int* h_int = nullptr;
@@ -509,6 +513,12 @@ static int ensure_work(ua_mesh* m) {
   for (auto f : dv) { *f = walloc<double>(m, N); ok = ok && *f; }
   void** kv[] = {&w->kr, &w->kz, &w->kp, &w->kq, &w->invd};
   for (auto f : kv) { *f = walloc<double>(m, N); ok = ok && *f; }
+  if (m->ndof == 3) {
+    double** uf[] = {&w->h0, &w->u0, &w->v0, &w->as0, &w->ab0, &w->as1, &w->ab1, &w->dadh};
+    for (auto f : uf) { *f = walloc<double>(m, NN); ok = ok && *f; }
+    void** bv[] = {&w->krh, &w->ks, &w->ksh, &w->kt};
+    for (auto f : bv) { *f = walloc<double>(m, N); ok = ok && *f; }
+  }
   w->part = walloc<double>(m, 4 * (size_t)w->nrb);
   w->sysv = walloc<double>(m, SV_COUNT * (size_t)nsys);
   w->done = walloc<int>(m, nsys);
@@ -636,6 +646,20 @@ static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
         double v = vals ? vals[idx[i].second] : 0.0;
         if (v != v) return set_error(UA_ERR_NAN_INPUT, "nan in fixed value");
         con_dof.push_back(d0 + comp * nn + idx[i].first);
+        con_sys.push_back(s);
+        rhs.push_back(v);
+      }
+    }
+    if (b && m->ndof == 3 && b->n_hfixed > 0) {  // createLh.m: fixed h nodes in the given order
+      std::vector<unsigned char> seen(nn, 0);
+      for (int i = 0; i < b->n_hfixed; ++i) {
+        int nd = b->hfixed_node[i];
+        if (nd < 0 || nd >= nn) return set_error(UA_ERR_INVALID, "system %d: fixed h node index out of range", s);
+        if (seen[nd]) return set_error(UA_ERR_INVALID, "ABfgPreEliminate:B B*B^T not diagonal (h node %d fixed twice)", nd);
+        seen[nd] = 1;
+        double v = b->hfixed_value ? b->hfixed_value[i] : 0.0;
+        if (v != v) return set_error(UA_ERR_NAN_INPUT, "nan in fixed h value");
+        con_dof.push_back(d0 + 2 * nn + nd);
         con_sys.push_back(s);
         rhs.push_back(v);
       }
@@ -1006,6 +1030,456 @@ static int newton_run(ua_mesh* m, const ua_params* p, std::vector<int> run, std:
   }
   for (int s = 0; s < nsys; ++s) {
     if (!run[s] || !rep[s]) continue;
+    rep[s]->converged = st[s].converged ? 1 : 0;
+    rep[s]->iterations = st[s].iteration;
+    rep[s]->backtrack_steps = st[s].iarm;
+    rep[s]->r = st[s].r; rep[s]->rForce = st[s].rForce; rep[s]->rWork = st[s].rWork;
+    rep[s]->assembly_ms += t_asm; rep[s]->solve_ms += t_sol;
+  }
+  return UA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab for the unsymmetric uvh tangent (the reference's solveKApe ->
+// ABfgPreEliminate direct solve, SSTREAM_TransientImplicit.m:136), Jacobi
+// right-preconditioned, on the free dofs; constrained dofs are masked as in
+// the PCG.  Per-system scalars, deterministic reductions.
+// ---------------------------------------------------------------------------
+
+// y = mask(K x); partials: a.y (a may be null), y.y
+template <typename KT, int LPR>
+__global__ void __launch_bounds__(256) k_bicg_spmv(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
+                                                   const int* done, const int* rowptr, const int* colind,
+                                                   const KT* K, const double* x, const unsigned char* cmask,
+                                                   double* y, const double* a, double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double v[2] = {0, 0};
+  if (sel[s] && !done[s]) {
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    for (int row0 = rs; row0 < re; row0 += ngrp) {
+      const int row = row0 + grp;
+      const bool valid = row < re;
+      double ax = row_dot<KT, double, LPR>(rowptr, colind, K, x, row, valid, lane);
+      if (valid && lane == 0) {
+        const double yv = cmask[row] ? 0.0 : ax;
+        y[row] = yv;
+        if (a) v[0] += a[row] * yv;
+        v[1] += yv * yv;
+      }
+    }
+  }
+  block_partials<2>(v, part, nrb, blk);
+}
+
+// r = mask(f - K x0), rhat = r, p = v = 0; partials rhat.r, r.r
+template <typename KT, int LPR>
+__global__ void __launch_bounds__(256) k_bicg_init(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
+                                                   const int* rowptr, const int* colind, const KT* K,
+                                                   const double* x0, const double* f, const unsigned char* cmask,
+                                                   double* r, double* rhat, double* p, double* vv, double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double v[2] = {0, 0};
+  if (sel[s]) {
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    for (int row0 = rs; row0 < re; row0 += ngrp) {
+      const int row = row0 + grp;
+      const bool valid = row < re;
+      double ax = row_dot<KT, double, LPR>(rowptr, colind, K, x0, row, valid, lane);
+      if (valid && lane == 0) {
+        const double rv = cmask[row] ? 0.0 : f[row] - ax;
+        r[row] = rv; rhat[row] = rv; p[row] = 0; vv[row] = 0;
+        v[0] += rv * rv;
+        v[1] += rv * rv;
+      }
+    }
+  }
+  block_partials<2>(v, part, nrb, blk);
+}
+
+// p = r + beta (p - omega v); phat = invd p
+__global__ void __launch_bounds__(256) k_bicg_p(const int* rb_start, const int* rb_sys, const int* sel,
+                                                const int* done, const double* sysv, int nsys, const double* r,
+                                                double* p, const double* vv, const double* invd, double* phat) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const double beta = sysv[SV_BETA * nsys + s], omega = sysv[SV_OMEGA * nsys + s];
+  for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) {
+    const double pv = r[i] + beta * (p[i] - omega * vv[i]);
+    p[i] = pv;
+    phat[i] = invd[i] * pv;
+  }
+}
+
+// s = r - alpha v; shat = invd s
+__global__ void __launch_bounds__(256) k_bicg_s(const int* rb_start, const int* rb_sys, const int* sel,
+                                                const int* done, const double* sysv, int nsys, const double* r,
+                                                const double* vv, const double* invd, double* sv, double* shat) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const double alpha = sysv[SV_ALPHA * nsys + s];
+  for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) {
+    const double x = r[i] - alpha * vv[i];
+    sv[i] = x;
+    shat[i] = invd[i] * x;
+  }
+}
+
+// x += alpha phat + omega shat; r = s - omega t; partials rhat.r, r.r
+__global__ void __launch_bounds__(256) k_bicg_x(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
+                                                const int* done, const double* sysv, int nsys, double* x,
+                                                const double* phat, const double* shat, const double* sv,
+                                                const double* t, double* r, const double* rhat, double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double v[2] = {0, 0};
+  if (sel[s] && !done[s]) {
+    const double alpha = sysv[SV_ALPHA * nsys + s], omega = sysv[SV_OMEGA * nsys + s];
+    for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) {
+      x[i] += alpha * phat[i] + omega * shat[i];
+      const double rv = sv[i] - omega * t[i];
+      r[i] = rv;
+      v[0] += rhat[i] * rv;
+      v[1] += rv * rv;
+    }
+  }
+  block_partials<2>(v, part, nrb, blk);
+}
+
+// stage 0: init (rho, rr0); 1: alpha = rho/(rhat.v); 2: omega = (t.s)/(t.t); 3: rho, beta, convergence
+__global__ void k_bicg_reduce(int stage, const int* sys_rb_off, int nrb, const int* sel, int* done, int* its,
+                              int* status, double* sysv, int nsys, const double* part, int maxit) {
+  const int s = blockIdx.x;
+  if (!sel[s] || (stage > 0 && done[s])) return;
+  double o[2];
+  sys_sum<2>(part, nrb, sys_rb_off[s], sys_rb_off[s + 1], o);
+  if (threadIdx.x != 0) return;
+  double* sv = sysv;
+  if (stage == 0) {
+    sv[SV_RZ * nsys + s] = o[0];
+    sv[SV_RR0 * nsys + s] = o[1];
+    sv[SV_RR * nsys + s] = o[1];
+    sv[SV_ALPHA * nsys + s] = 1.0;
+    sv[SV_OMEGA * nsys + s] = 1.0;
+    sv[SV_BETA * nsys + s] = 0.0;  // first direction p = r
+    its[s] = 0;
+    status[s] = 0;
+    done[s] = (o[1] == 0.0) ? 1 : 0;
+  } else if (stage == 1) {
+    const double rv = o[0];
+    if (rv == 0.0 || !(rv == rv)) { status[s] = 1; done[s] = 1; sv[SV_ALPHA * nsys + s] = 0; return; }
+    sv[SV_ALPHA * nsys + s] = sv[SV_RZ * nsys + s] / rv;
+  } else if (stage == 2) {
+    // partials: [0] = s.t, [1] = t.t
+    sv[SV_OMEGA * nsys + s] = o[1] > 0 ? o[0] / o[1] : 0.0;
+  } else {
+    const double rho_new = o[0], rr = o[1];
+    its[s] += 1;
+    sv[SV_RR * nsys + s] = rr;
+    const double omega = sv[SV_OMEGA * nsys + s];
+    sv[SV_BETA * nsys + s] = (rho_new / sv[SV_RZ * nsys + s]) * (sv[SV_ALPHA * nsys + s] / omega);
+    sv[SV_RZ * nsys + s] = rho_new;
+    if (rr <= sv[SV_TOL2 * nsys + s] * sv[SV_RR0 * nsys + s] || its[s] >= maxit || !(rr == rr)) done[s] = 1;
+    else if (omega == 0.0 || rho_new == 0.0) { status[s] = 1; done[s] = 1; }
+  }
+}
+
+// (s.t) partials: the spmv kernel gives a.y with a = s
+template <typename KT>
+static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out) {
+  Work* w = m->work;
+  const int N = m->ndof_total;
+  const int lpr = 16;
+  for (int s = 0; s < w->nsys; ++s) w->h_sysv[s] = p->krylov_rtol * p->krylov_rtol;
+  UA_CUDA_TRY(cudaMemcpyAsync(w->sysv + SV_TOL2 * w->nsys, w->h_sysv, w->nsys * sizeof(double),
+                              cudaMemcpyHostToDevice, m->stream));
+  double *r = (double*)w->kr, *rhat = (double*)w->krh, *pp = (double*)w->kp, *phat = (double*)w->kz;
+  double *vv = (double*)w->kq, *sv = (double*)w->ks, *shat = (double*)w->ksh, *t = (double*)w->kt;
+  double* invd = (double*)w->invd;
+  k_invdiag<KT, double><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, invd), ++g_launches;
+  k_zero_sel<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->dX), ++g_launches;
+  if (w->nc)
+    k_con_particular<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs,
+                                                                 w->X, w->dX, w->grhs), ++g_launches;
+  k_bicg_init<KT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr, w->colind, K,
+                                                     w->dX, w->frhs, w->cmask, r, rhat, pp, vv, w->part), ++g_launches;
+  k_bicg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(0, w->sys_rb_off, w->nrb, w->sel, w->done, w->its, w->status,
+                                                         w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
+  (void)lpr;
+  const int chunk = 8;
+  int it = 0;
+  while (true) {
+    for (int k = 0; k < chunk; ++k) {
+      k_bicg_p<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys, r, pp, vv,
+                                              invd, phat), ++g_launches;
+      cudaEvent_t ev[2];
+      prof_begin(m, PK_SPMV, ev);
+      k_bicg_spmv<KT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr,
+                                                         w->colind, K, phat, w->cmask, vv, rhat, w->part), ++g_launches;
+      prof_end(m, ev);
+      k_bicg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                             w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+      k_bicg_s<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys, r, vv, invd,
+                                              sv, shat), ++g_launches;
+      k_bicg_spmv<KT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr,
+                                                         w->colind, K, shat, w->cmask, t, sv, w->part), ++g_launches;
+      k_bicg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                             w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+      k_bicg_x<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->sysv, w->nsys, w->dX,
+                                              phat, shat, sv, t, r, rhat, w->part), ++g_launches;
+      k_bicg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(3, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                             w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+    }
+    it += chunk;
+    UA_CUDA_TRY(cudaGetLastError());
+    UA_CUDA_TRY(cudaMemcpyAsync(w->h_int, w->done, w->nsys * sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+    UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    bool all = true;
+    for (int s = 0; s < w->nsys; ++s) all = all && (w->h_int[s] || !its_out[s]);
+    if (all || it >= p->krylov_maxit + chunk) break;
+  }
+  if (w->nc)
+    k_con_multiplier<KT><<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->rowptr,
+                                                                     w->colind, K, w->dX, w->frhs, w->dlam), ++g_launches;
+  UA_CUDA_TRY(cudaMemcpyAsync(w->h_int, w->its, w->nsys * sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  for (int s = 0; s < w->nsys; ++s) its_out[s] = its_out[s] ? w->h_int[s] : 0;
+  return UA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// uvh driver: SSTREAM_TransientImplicit.m:6-717
+// ---------------------------------------------------------------------------
+
+static UvhPhys make_uvh_phys(const ua_params* p) {
+  UvhPhys P;
+  P.uv = make_phys(p);
+  P.kH = p->kH; P.Hh0 = p->Hh0; P.SpeedZero = p->SpeedZero;
+  P.theta = p->theta; P.beta0 = p->SUPG_beta0; P.tau_mult = p->uvh_SUPG_tauMultiplier;
+  P.tau_kind = p->uvh_SUPG_tau;
+  return P;
+}
+
+static int upload_fields_uvh(ua_mesh* m, const ua_params* p, const ua_fields* F, int nF) {
+  Work* w = m->work;
+  std::vector<SysScal> sc(m->dm.nsys);
+  for (int s = 0; s < m->dm.nsys; ++s) {
+    const ua_fields& f = F[nF == 1 ? 0 : s];
+    const int no = m->h_node_off[s], nn = m->sys[s].nn, d0 = m->h_dof_off[s];
+    const double* src[] = {f.S, f.B, f.rho, f.AGlen, f.n, f.C, f.m, f.h0, f.u0, f.v0, f.as0, f.ab0, f.as1, f.ab1};
+    double* dst[] = {w->S, w->B, w->rho, w->A, w->n, w->C, w->m, w->h0, w->u0, w->v0, w->as0, w->ab0, w->as1, w->ab1};
+    const char* names[] = {"S", "B", "rho", "AGlen", "n", "C", "m", "h0", "u0", "v0", "as0", "ab0", "as1", "ab1"};
+    auto kind = f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int k = 0; k < 14; ++k) {
+      if (!src[k]) return set_error(UA_ERR_INVALID, "system %d: null uvh field %s", s, names[k]);
+      if (f.location == UA_HOST && any_nan(src[k], nn))
+        return set_error(UA_ERR_NAN_INPUT, "uvhMatrixAssembly:NaN nan in %s (system %d)", names[k], s);
+      UA_CUDA_TRY(cudaMemcpyAsync(dst[k] + no, src[k], nn * sizeof(double), kind, m->stream));
+    }
+    if (f.dadh) UA_CUDA_TRY(cudaMemcpyAsync(w->dadh + no, f.dadh, nn * sizeof(double), kind, m->stream));
+    else UA_CUDA_TRY(cudaMemsetAsync(w->dadh + no, 0, nn * sizeof(double), m->stream));
+    if (!f.ub || !f.vb || !f.h1) return set_error(UA_ERR_INVALID, "system %d: null ub/vb/h1", s);
+    if (f.location == UA_HOST && (any_nan(f.ub, nn) || any_nan(f.vb, nn) || any_nan(f.h1, nn)))
+      return set_error(UA_ERR_NAN_INPUT, "uvhMatrixAssembly:NaN nan in F1.ub, F1.vb or F1.h");
+    UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0, f.ub, nn * sizeof(double), kind, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0 + nn, f.vb, nn * sizeof(double), kind, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0 + 2 * nn, f.h1, nn * sizeof(double), kind, m->stream));
+    sc[s].rhow = f.rhow; sc[s].g = f.g; sc[s].ca = std::cos(f.alpha); sc[s].sa = std::sin(f.alpha);
+    sc[s].dt = f.dt;
+  }
+  UA_CUDA_TRY(cudaMemcpyAsync(w->scal, sc.data(), sc.size() * sizeof(SysScal), cudaMemcpyHostToDevice, m->stream));
+  (void)p;
+  return UA_OK;
+}
+
+static int assemble_uvh(ua_mesh* m, const ua_params* p, bool withK, bool useDir, bool zero, bool parts) {
+  Work* w = m->work;
+  UvhIn in{w->S, w->B, w->rho, w->A, w->n, w->C, w->m, w->h0, w->u0, w->v0, w->as0, w->ab0, w->as1, w->ab1,
+           w->dadh, w->X, useDir ? w->dX : nullptr, useDir ? w->gamma : nullptr, w->scal, w->sel, zero ? 1 : 0};
+  UvOut out{w->R, withK ? (void*)w->Kd : nullptr, parts ? w->Tint : nullptr, parts ? w->Fext : nullptr};
+  cudaEvent_t ev[2];
+  prof_begin(m, withK ? PK_ASMK : PK_ASMR, ev);
+  cudaError_t e = launch_uvh_assembly(m, make_uvh_phys(p), in, out, withK);
+  prof_end(m, ev);
+  ++g_launches;
+  if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "uvh assembly launch: %s", cudaGetErrorString(e));
+  return UA_OK;
+}
+
+// CalcCostFunctionNRuvh.m:12-105 for the selected systems
+static int cost_eval_uvh(ua_mesh* m, const ua_params* p) {
+  Work* w = m->work;
+  int rc = assemble_uvh(m, p, false, true, false, false);
+  if (rc) return rc;
+  k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, w->dof_con, w->lam,
+                                             w->dlam, w->gamma, w->dX, w->part), ++g_launches;
+  k_cost_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, w->nsys, w->sysv,
+                                                         w->sys_con_off, w->con_dof, w->con_rhs, w->X, w->dX, w->dlam,
+                                                         w->gamma, 0), ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
+  UA_CUDA_TRY(cudaMemcpyAsync(w->h_sysv, w->sysv, SV_COUNT * w->nsys * sizeof(double), cudaMemcpyDeviceToHost,
+                              m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return UA_OK;
+}
+
+static bool uvh_criteria(const ua_params* p, double rForce, double rWork, int iteration, double gamma) {
+  const double *a, *o;
+  if (gamma > std::max(p->uvhExitBackTrackingStepLength, p->BacktrackingGammaMin)) {
+    a = p->uvhDesiredWorkAndForceTolerances; o = p->uvhDesiredWorkOrForceTolerances;
+  } else {
+    a = p->uvhAcceptableWorkAndForceTolerances; o = p->uvhAcceptableWorkOrForceTolerances;
+  }
+  return (rWork < a[0] && rForce < a[1]) && (rWork < o[0] || rForce < o[1]) && iteration >= p->NRitmin;
+}
+
+struct UvhSys {
+  bool active = false, converged = false, bt_ok = true;
+  int iteration = 0, iarm = 0, kits = 0;
+  double r = INFINITY, r0 = INFINITY, rForce = INFINITY, rWork = NAN, gamma = 1, r1 = 0;
+  double rRatio[3] = {0, 0, 0};
+  BackTrack bt;
+  std::vector<double> ls_g, ls_D2;
+};
+
+static int newton_run_uvh(ua_mesh* m, const ua_params* p, std::vector<ua_newton_report*>& rep,
+                          std::vector<UvhSys>& st) {
+  Work* w = m->work;
+  const int nsys = w->nsys;
+  int rc;
+  double t_asm = 0, t_sol = 0;
+  std::vector<int> sel(nsys, 1), its(nsys);
+  std::vector<double> gam(nsys, 0.0);
+  if ((rc = set_sel(m, sel))) return rc;
+  // uvhMakeInitialIterateFeasible (:37-41)
+  if (w->nc)
+    k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs,
+                                                                 w->X), ++g_launches;
+  // Fext0 at ZeroFields (:53-56); the normalisation of CalcCostFunctionNRuvh
+  if ((rc = assemble_uvh(m, p, false, false, true, false))) return rc;
+  k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, nullptr, nullptr, nullptr,
+                                             nullptr, nullptr, w->part), ++g_launches;
+  k_cost_reduce<<<nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, nsys, w->sysv, nullptr,
+                                                     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 1), ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
+  for (int s = 0; s < nsys; ++s) { st[s] = UvhSys(); st[s].active = true; }
+  while (true) {
+    bool any = false;
+    for (int s = 0; s < nsys; ++s) {
+      UvhSys& S = st[s];
+      if (!S.active) continue;
+      if (S.rWork != S.rWork) S.rWork = 0;  // :78-80
+      if (uvh_criteria(p, S.rForce, S.rWork, S.iteration, S.gamma)) { S.converged = true; S.active = false; continue; }
+      if (S.iteration > p->NRitmax) { S.converged = false; S.active = false; continue; }
+      if (!S.bt_ok || S.gamma == 0) { S.converged = false; S.active = false; continue; }  // :104-110
+      const double ratio = S.r / S.r0;
+      S.rRatio[S.iteration % 3] = ratio;  // :111-124 stagnation
+      if (S.rRatio[0] > 0.98 && S.rRatio[1] > 0.98 && S.rRatio[2] > 0.98) {
+        S.converged = S.rWork < 1e-14; S.active = false; continue;
+      }
+      S.iteration++;
+      any = true;
+    }
+    if (!any) break;
+    for (int s = 0; s < nsys; ++s) sel[s] = st[s].active ? 1 : 0;
+    if ((rc = set_sel(m, sel))) return rc;
+    double t0 = now_ms();
+    if ((rc = assemble_uvh(m, p, true, false, false, false))) return rc;  // :127
+    k_frhs<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->R, w->dof_con, w->lam, w->frhs), ++g_launches;
+    UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    double t1 = now_ms();
+    t_asm += t1 - t0;
+    for (int s = 0; s < nsys; ++s) its[s] = sel[s];
+    if ((rc = bicgstab_t<double>(m, p, w->Kd, its.data()))) return rc;  // :136
+    t_sol += now_ms() - t1;
+    for (int s = 0; s < nsys; ++s) if (sel[s]) st[s].kits = its[s];
+    // r0 = func(0), r1 = func(1) (:155-156)
+    for (int g1 = 0; g1 < 2; ++g1) {
+      for (int s = 0; s < nsys; ++s) gam[s] = (double)g1;
+      if ((rc = set_gamma(m, gam))) return rc;
+      if ((rc = cost_eval_uvh(m, p))) return rc;
+      for (int s = 0; s < nsys; ++s) {
+        if (!sel[s]) continue;
+        const double rf = w->h_sysv[SV_FF * nsys + s], d2 = w->h_sysv[SV_FD * nsys + s];
+        UvhSys& S = st[s];
+        if (g1 == 0) { S.r0 = rf; S.ls_g.assign({0.0}); S.ls_D2.assign({d2}); }
+        else { S.r1 = rf; S.ls_g.push_back(1.0); S.ls_D2.push_back(d2); }
+      }
+    }
+    // rLineminUa (:157): Newton-direction backtracking, BackTracking accepts
+    // gamma=1 at once when r1 is below its target
+    for (int s = 0; s < nsys; ++s) {
+      if (!sel[s]) continue;
+      UvhSys& S = st[s];
+      S.bt = BackTrack();
+      BTConfig& c = S.bt.cfg;
+      c.beta = p->BackTrackBeta; c.ExtrapolationRatio = p->BackTrackExtrapolationRatio;
+      c.MinXfracRel = p->BackTrackMinXfrac; c.GL = p->BackTrackGuardLower; c.GU = p->BackTrackGuardUpper;
+      c.NewtonAcceptRatio = p->NewtonAcceptRatio; c.GammaMin = 0.001; c.NLtol = p->NLtol;
+      c.MaxIterations = p->BackTrackMaxIterations; c.MaxExtrapolations = p->BackTrackMaxExtrapolations;
+      c.MaxFuncSame = p->BackTrackMaxFuncSame; c.allow_ext = p->LineSearchAllowedToUseExtrapolation != 0;
+      S.bt.start(-2 * S.r0, 1.0, S.r0, S.r1);
+    }
+    while (true) {
+      bool need = false;
+      for (int s = 0; s < nsys; ++s) {
+        sel[s] = (st[s].active && !st[s].bt.done) ? 1 : 0;
+        gam[s] = sel[s] ? st[s].bt.request : 0.0;
+        need = need || sel[s];
+      }
+      if (!need) break;
+      if ((rc = set_sel(m, sel))) return rc;
+      if ((rc = set_gamma(m, gam))) return rc;
+      if ((rc = cost_eval_uvh(m, p))) return rc;
+      for (int s = 0; s < nsys; ++s) {
+        if (!sel[s]) continue;
+        st[s].ls_g.push_back(gam[s]);
+        st[s].ls_D2.push_back(w->h_sysv[SV_FD * nsys + s]);
+        st[s].bt.feed(w->h_sysv[SV_FF * nsys + s]);
+      }
+    }
+    for (int s = 0; s < nsys; ++s) {
+      sel[s] = 0;
+      UvhSys& S = st[s];
+      if (!S.active) continue;
+      const double gN = S.bt.gmin, rN = S.bt.fmin;
+      if (rep[s] && gN < 0.75 && rN / S.r0 > 0.7) rep[s]->cauchy_fallbacks++;  // rLineminUa.m:96
+      S.iarm = S.bt.iarm;
+      S.bt_ok = S.bt.converged && !S.bt.error;
+      if (rN < S.r0) {
+        S.gamma = gN; S.r = rN; S.rForce = rN; S.rWork = NAN;
+        for (size_t k = 0; k < S.ls_g.size(); ++k)
+          if (S.ls_g[k] == gN) { S.rWork = S.ls_D2[k] * S.ls_D2[k]; break; }
+      } else {
+        S.gamma = 0; S.r = S.r0; S.rForce = S.r0; S.rWork = NAN;  // rLineminUa.m:27-28
+      }
+      if (rep[s] && rep[s]->iters && rep[s]->n_iter_records < rep[s]->iters_capacity) {
+        ua_newton_iter& it = rep[s]->iters[rep[s]->n_iter_records++];
+        it.iteration = S.iteration; it.iarm = S.iarm; it.krylov_its = S.kits; it.direction = S.iarm > 0;
+        it.gamma = S.gamma; it.r0 = S.r0; it.r = S.r; it.rForce = S.rForce; it.rWork = S.rWork;
+      }
+      if (rep[s]) rep[s]->krylov_its_total += S.kits;
+      if (p->verbose)
+        fprintf(stderr, "NR-SSTREAM(uvh)[%d]:%3d/%-2d g=%-14.7g , r/r0=%-14.7g ,  r0=%-14.7g , r=%-14.7g , rForce=%-14.7g , rWork=%-14.7g , bicg=%d\n",
+                s, S.iteration, S.iarm, S.gamma, S.r / S.r0, S.r0, S.r, S.rForce, S.rWork, S.kits);
+      sel[s] = 1;
+      gam[s] = S.gamma;
+    }
+    if ((rc = set_sel(m, sel))) return rc;
+    if ((rc = set_gamma(m, gam))) return rc;
+    k_newton_update<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->gamma, w->X, w->dX), ++g_launches;
+    if (w->nc)
+      k_lam_update<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_sys, w->sel, w->gamma, w->lam, w->dlam), ++g_launches;
+    UA_CUDA_TRY(cudaGetLastError());
+  }
+  for (int s = 0; s < nsys; ++s) {
+    if (!rep[s]) continue;
     rep[s]->converged = st[s].converged ? 1 : 0;
     rep[s]->iterations = st[s].iteration;
     rep[s]->backtrack_steps = st[s].iarm;
@@ -1585,4 +2059,118 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
   }
   view.work = nullptr;
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// uvh C-ABI
+// ---------------------------------------------------------------------------
+extern "C" int ua_uvh_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, int32_t mode, double* R,
+                               double* Kvals, double* Tint, double* Fext) {
+  if (!m || !p || !F) return set_error(UA_ERR_INVALID, "ua_uvh_assemble: null argument");
+  if (m->ndof != 3) return set_error(UA_ERR_INVALID, "ua_uvh_assemble needs a ndof=3 mesh handle");
+  if (m->dm.nsys != 1) return set_error(UA_ERR_INVALID, "ua_uvh_assemble takes a single-mesh handle");
+  if (mode != UA_ASM_R && mode != UA_ASM_RK && mode != UA_ASM_ZERO_R) return set_error(UA_ERR_INVALID, "bad mode");
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  int rc;
+  if ((rc = ensure_work(m))) return rc;
+  Work* w = m->work;
+  const bool withK = mode == UA_ASM_RK;
+  if (withK && (rc = ensure_K(m, UA_PREC_FP64))) return rc;
+  if ((rc = upload_fields_uvh(m, p, F, 1))) return rc;
+  std::vector<int> sel(1, 1);
+  if ((rc = set_sel(m, sel))) return rc;
+  if ((rc = assemble_uvh(m, p, withK, false, mode == UA_ASM_ZERO_R, Tint || Fext))) return rc;
+  const int N = m->ndof_total;
+  if (R) UA_CUDA_TRY(cudaMemcpyAsync(R, w->R, N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (Tint) UA_CUDA_TRY(cudaMemcpyAsync(Tint, w->Tint, N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (Fext) UA_CUDA_TRY(cudaMemcpyAsync(Fext, w->Fext, N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (withK && Kvals)
+    UA_CUDA_TRY(cudaMemcpyAsync(Kvals, w->Kd, m->nnz_total * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return UA_OK;
+}
+
+static int uvh_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs, int nF,
+                      std::vector<ua_newton_report*>& rep, double* luvh, int32_t nl) {
+  if (m->ndof != 3) return set_error(UA_ERR_INVALID, "uvh Newton needs a ndof=3 mesh handle");
+  if (p->precision != UA_PREC_FP64) return set_error(UA_ERR_INVALID, "the uvh solve runs in FP64 only");
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  int rc;
+  double t0 = now_ms();
+  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_K(m, UA_PREC_FP64))) return rc;
+  if ((rc = upload_fields_uvh(m, p, F, nF))) return rc;
+  if ((rc = build_constraints(m, bcs, nF))) return rc;
+  Work* w = m->work;
+  const int nsys = w->nsys;
+  g_launches = 0;
+  w->prof.reset();
+  w->prof.on = p->profile != 0;
+  cudaEvent_t call_ev[2];
+  {
+    bool on = w->prof.on;
+    w->prof.on = true;
+    call_ev[0] = w->prof.get();
+    call_ev[1] = w->prof.get();
+    w->prof.on = on;
+  }
+  UA_CUDA_TRY(cudaEventRecord(call_ev[0], m->stream));
+  if (w->nc) UA_CUDA_TRY(cudaMemsetAsync(w->lam, 0, w->nc * sizeof(double), m->stream));
+  if (luvh && nsys == 1 && nl == w->nc && nl > 0)
+    UA_CUDA_TRY(cudaMemcpyAsync(w->lam, luvh, nl * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+  for (auto r : rep)
+    if (r) { int cap = r->iters_capacity; ua_newton_iter* it = r->iters; std::memset(r, 0, sizeof(*r)); r->iters_capacity = cap; r->iters = it; }
+  std::vector<UvhSys> st(nsys);
+  if ((rc = newton_run_uvh(m, p, rep, st))) return rc;
+  for (int s = 0; s < nsys; ++s) {
+    ua_fields& f = F[nF == 1 ? 0 : s];
+    const int d0 = m->h_dof_off[s], nn = m->sys[s].nn;
+    auto kind = f.location == UA_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    UA_CUDA_TRY(cudaMemcpyAsync(f.ub, w->X + d0, nn * sizeof(double), kind, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(f.vb, w->X + d0 + nn, nn * sizeof(double), kind, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(f.h1, w->X + d0 + 2 * nn, nn * sizeof(double), kind, m->stream));
+  }
+  if (luvh && nsys == 1 && nl >= w->nc && w->nc > 0)
+    UA_CUDA_TRY(cudaMemcpyAsync(luvh, w->lam, w->nc * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  UA_CUDA_TRY(cudaEventRecord(call_ev[1], m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  float dev_ms = 0;
+  cudaEventElapsedTime(&dev_ms, call_ev[0], call_ev[1]);
+  double kms[3] = {0, 0, 0};
+  int kn[3] = {0, 0, 0};
+  for (auto& mk : w->prof.marks) {
+    float t = 0;
+    cudaEventElapsedTime(&t, mk.second.first, mk.second.second);
+    kms[mk.first] += t;
+    kn[mk.first]++;
+  }
+  bool all_conv = true;
+  const double t1 = now_ms();
+  for (int s = 0; s < nsys; ++s) {
+    if (rep[s]) {
+      rep[s]->total_ms = t1 - t0; rep[s]->device_ms = dev_ms;
+      rep[s]->kasmK_ms = kms[PK_ASMK]; rep[s]->kasmK_n = kn[PK_ASMK];
+      rep[s]->kasmR_ms = kms[PK_ASMR]; rep[s]->kasmR_n = kn[PK_ASMR];
+      rep[s]->kspmv_ms = kms[PK_SPMV]; rep[s]->kspmv_n = kn[PK_SPMV];
+      rep[s]->gpu_launches = (int)g_launches;
+    }
+    all_conv = all_conv && st[s].converged;
+  }
+  return all_conv ? UA_OK : UA_ERR_NOT_CONVERGED;
+}
+
+extern "C" int ua_uvh_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs, double* luvh,
+                             int32_t nl, ua_newton_report* rep) {
+  if (!m || !p || !F) return set_error(UA_ERR_INVALID, "ua_uvh_newton: null argument");
+  if (m->dm.nsys != 1) return set_error(UA_ERR_INVALID, "ua_uvh_newton takes a single-mesh handle");
+  std::vector<ua_newton_report*> reps(1, rep);
+  return uvh_common(m, p, F, bcs, 1, reps, luvh, nl);
+}
+
+extern "C" int ua_uvh_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fields, const ua_bcs* bcs,
+                                   ua_newton_report* reports) {
+  if (!m || !p || !fields) return set_error(UA_ERR_INVALID, "ua_uvh_newton_batch: null argument");
+  std::vector<ua_newton_report*> reps(m->dm.nsys);
+  for (int s = 0; s < m->dm.nsys; ++s) reps[s] = reports ? &reports[s] : nullptr;
+  return uvh_common(m, p, fields, bcs, m->dm.nsys, reps, nullptr, 0);
 }

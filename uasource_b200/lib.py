@@ -128,6 +128,12 @@ SIGNATURES = {
                                C.c_int32, C.POINTER(ua_newton_report), _dp, _dp]),
     "ua_uv_newton_batch": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),
                                      C.POINTER(ua_newton_report)]),
+    "ua_uvh_assemble": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.c_int32, _dp, _dp, _dp,
+                                  _dp]),
+    "ua_uvh_newton": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs), _dp,
+                                C.c_int32, C.POINTER(ua_newton_report)]),
+    "ua_uvh_newton_batch": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),
+                                      C.POINTER(ua_newton_report)]),
     "ua_constraint_count": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), C.c_int32, _ip]),
     "ua_solve_kape_symmetric": (C.c_int, [C.c_int32, _lp, _lp, _dp, C.c_int32, _lp, _lp, _dp, _dp, _dp, _dp, _dp,
                                           C.c_double, C.c_int32, _ip, C.c_int32]),

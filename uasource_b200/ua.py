@@ -81,6 +81,12 @@ class CtrlVar:
             setattr(self, name, (math.inf, tol))
         return self
 
+    def set_uvh_force_tolerance(self, tol):
+        """Set the desired uvh force tolerances (rForce < tol); acceptable ones keep their defaults."""
+        self.uvhDesiredWorkAndForceTolerances = (math.inf, tol)
+        self.uvhDesiredWorkOrForceTolerances = (math.inf, tol)
+        return self
+
     def to_c(self) -> L.ua_params:
         p = L.ua_params()
         L.load().ua_params_default(C.byref(p))
@@ -110,11 +116,18 @@ class Fields:
     rhow: float = 1030.0
     g: float = 9.81 / 1000
     alpha: float = 0.0
+    as_: np.ndarray = None      # surface mass balance F.as (transient solves)
+    ab: np.ndarray = None       # basal mass balance F.ab
+    dadh: np.ndarray = None     # d(as+ab)/dh (MassBalanceGeometryFeedback=3), None = 0
 
     @staticmethod
     def from_problem(P):
         return Fields(h=P.h, S=P.S, B=P.B, rho=P.rho, AGlen=P.AGlen, n=P.n, C=P.C, m=P.m,
-                      ub=P.ub.copy(), vb=P.vb.copy(), rhow=P.rhow, g=P.g, alpha=P.alpha)
+                      ub=P.ub.copy(), vb=P.vb.copy(), rhow=P.rhow, g=P.g, alpha=P.alpha,
+                      as_=None if P.as_ is None else P.as_.copy(), ab=None if P.ab is None else P.ab.copy())
+
+    def copy(self):
+        return Fields(**{k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items()})
 
 
 @dataclass
@@ -416,6 +429,84 @@ def uv_batch(ctrl: CtrlVar, mua: MUA, Fs, bcss):
     rc = lib.ua_uv_newton_batch(mua.handle, C.byref(p), cfs, cbs, reps)
     L.check(rc, allow=(L.UA_ERR_NOT_CONVERGED,))
     return [(outs[s][0], outs[s][1], _report(reps[s], recs[s])) for s in range(ns)]
+
+
+def _c_fields_uvh(F0: Fields, F1: Fields, dt, keep: _Keep, Nn: int):
+    """uvh inputs: time-independent fields and level-1 state from F1, level 0 from F0."""
+    cf, ub, vb = _c_fields(F1, keep, Nn)
+    h1 = _f64(F1.h).copy()
+    keep.refs.append(h1)
+    cf.h1 = L.dptr(h1)
+    cf.h0 = keep.d(F0.h); cf.u0 = keep.d(F0.ub); cf.v0 = keep.d(F0.vb)
+    z = np.zeros(Nn)
+    cf.as0 = keep.d(F0.as_ if F0.as_ is not None else z); cf.ab0 = keep.d(F0.ab if F0.ab is not None else z)
+    cf.as1 = keep.d(F1.as_ if F1.as_ is not None else z); cf.ab1 = keep.d(F1.ab if F1.ab is not None else z)
+    cf.dadh = keep.d(F1.dadh) if F1.dadh is not None else None
+    cf.dt = float(dt)
+    return cf, ub, vb, h1
+
+
+def uvhAssembly(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, dt, Ronly=False, ZeroFields=False,
+                return_parts=False):
+    """uvhAssembly.m:1 -> uvhMatrixAssembly.m:6-585 on the GPU (ndof=3 handle).
+
+    Returns ``(R, K)``: R = Tint-Fext (3Nn), K the unsymmetric tangent (scipy
+    CSR on the structural pattern; None when Ronly or ZeroFields).
+    """
+    lib = L.load()
+    keep = _Keep()
+    Nn = mua.Nnodes()
+    cf, _, _, _ = _c_fields_uvh(F0, F1, dt, keep, Nn)
+    p = ctrl.to_c()
+    mode = L.UA_ASM_ZERO_R if ZeroFields else (L.UA_ASM_R if Ronly else L.UA_ASM_RK)
+    R = np.zeros(3 * Nn)
+    Kv = np.zeros(mua.pattern()[1].size) if mode == L.UA_ASM_RK else None
+    T = np.zeros(3 * Nn) if return_parts else None
+    Fx = np.zeros(3 * Nn) if return_parts else None
+    L.check(lib.ua_uvh_assemble(mua.handle, C.byref(p), C.byref(cf), mode, L.dptr(R), L.dptr(Kv), L.dptr(T),
+                                L.dptr(Fx)))
+    K = _csr(mua, 0, Kv, False) if Kv is not None else None
+    if return_parts:
+        return R, K, T, Fx
+    return R, K
+
+
+@dataclass
+class HBCs(BCs):
+    """Velocity and thickness boundary conditions (0-based node indices)."""
+    hFixedNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    hFixedValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
+
+
+def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None):
+    """uvh.m:5 -> uvh2D.m:20 -> SSTREAM_TransientImplicit.m:6-717 on the GPU.
+
+    F0: state at t (h, ub, vb, as_, ab); F1: start values at t+dt and the
+    time-independent fields.  Returns ``(F1, luvh, RunInfo)`` with F1.ub,
+    F1.vb, F1.h solved.
+    """
+    lib = L.load()
+    keep = _Keep()
+    Nn = mua.Nnodes()
+    cf, ub, vb, h1 = _c_fields_uvh(F0, F1, dt, keep, Nn)
+    cb = _c_bcs(bcs, keep)
+    hn = getattr(bcs, "hFixedNode", None) if bcs is not None else None
+    if hn is not None and len(hn):
+        cb.n_hfixed = len(hn); cb.hfixed_node = keep.i(hn); cb.hfixed_value = keep.d(bcs.hFixedValue)
+    p = ctrl.to_c()
+    nc = C.c_int32()
+    L.check(lib.ua_constraint_count(mua.handle, C.byref(cb), 3, C.byref(nc)))
+    lam = np.zeros(nc.value) if l is None or len(l) != nc.value else _f64(l).copy()
+    rep = L.ua_newton_report()
+    cap = (ctrl.NRitmax + 2) * 2
+    recs = (L.ua_newton_iter * cap)()
+    rep.iters = C.cast(recs, C.POINTER(L.ua_newton_iter))
+    rep.iters_capacity = cap
+    rc = lib.ua_uvh_newton(mua.handle, C.byref(p), C.byref(cf), C.byref(cb), L.dptr(lam), len(lam), C.byref(rep))
+    L.check(rc, allow=(L.UA_ERR_NOT_CONVERGED,))
+    Fo = F1.copy()
+    Fo.ub, Fo.vb, Fo.h = ub, vb, h1
+    return Fo, lam, _report(rep, recs)
 
 
 def solveKApeSymmetric(A, B, f, g, rtol=1e-12, maxit=0, device=0):
