@@ -239,6 +239,24 @@ int ua_uvh_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bc
 int ua_uvh_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fields, const ua_bcs* bcs,
                         ua_newton_report* reports);
 
+/* Serving (continuous batching of uv solves over the systems of a batch
+ * handle, used as slots).  No single reference counterpart: each slot runs
+ * SSTREAM2dNR2.m:3-431 (with the retry of uv.m:107-112) and requests join
+ * between Newton iterations while other slots iterate.
+ *   ua_serve_setup : BCs of every slot (bcs[i] for slot i), once.
+ *   ua_serve_begin : admit count requests into free slots sys[k] with fields
+ *                    F[k] (start velocities = warm start).
+ *   ua_serve_step  : one Newton iteration of every active slot; finished[i]=1
+ *                    for slots whose solve ended in this step; *nactive = busy slots.
+ *   ua_serve_result: solution and report of a finished slot. */
+int ua_serve_setup(ua_mesh* m, const ua_params* p, const ua_bcs* bcs);
+int ua_serve_begin(ua_mesh* m, const ua_params* p, int32_t count, const int32_t* sys, const ua_fields* F);
+int ua_serve_step(ua_mesh* m, const ua_params* p, int32_t* finished, int32_t* nactive);
+int ua_serve_result(ua_mesh* m, int32_t sys, double* ub, double* vb, ua_newton_report* rep);
+
+/* Free and total device memory (admission by free HBM). */
+int ua_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
+
 /* Number of rows of the constraint matrix L built from bcs (CreateLuv.m). */
 int ua_constraint_count(const ua_mesh* m, const ua_bcs* bcs, int32_t ndof, int32_t* nc);
 

@@ -87,6 +87,7 @@ struct Work {
   double* h_gamma = nullptr;
   std::vector<int> h_sys_rb_off, h_sys_con_off;
   Prof prof;
+  struct ServeState* serve = nullptr;
 };
 
 static void prof_begin(ua_mesh* m, int kind, cudaEvent_t* ev) {
@@ -571,48 +572,65 @@ static bool any_nan(const double* v, int n) {
   return false;
 }
 
-// Upload nodal fields of every system (host or device pointers) and compute s.
-static int upload_fields(ua_mesh* m, const ua_params* p, const ua_fields* F, int nF) {
+// Nodal fields of system s (host or device pointers); SysScal staged in sc.
+static int upload_fields_sys(ua_mesh* m, const ua_fields& f, int s, SysScal& sc) {
   Work* w = m->work;
-  std::vector<SysScal> sc(m->dm.nsys);
-  for (int s = 0; s < m->dm.nsys; ++s) {
-    const ua_fields& f = F[nF == 1 ? 0 : s];
-    const int no = m->h_node_off[s], nn = m->sys[s].nn;
-    const double* src[] = {f.h, f.S, f.B, f.rho, f.AGlen, f.n, f.C, f.m};
-    double* dst[] = {w->h, w->S, w->B, w->rho, w->A, w->n, w->C, w->m};
-    const char* names[] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
-    for (int k = 0; k < 8; ++k) {
-      if (!src[k]) return set_error(UA_ERR_INVALID, "system %d: null field pointer %s", s, names[k]);
-      // SSTREAM2dNR2.m:42-65: NaN in C or A (warning + NaN solution in the
-      // reference) and NaN in S, h, rho (error) all stop the solve here.
-      if (f.location == UA_HOST && any_nan(src[k], nn))
-        return set_error(UA_ERR_NAN_INPUT, "SSTREAM2dNR2: nan in %s (system %d)", names[k], s);
-      UA_CUDA_TRY(cudaMemcpyAsync(dst[k] + no, src[k], nn * sizeof(double),
-                                  f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
-                                  m->stream));
-    }
-    sc[s].rhow = f.rhow; sc[s].g = f.g; sc[s].ca = std::cos(f.alpha); sc[s].sa = std::sin(f.alpha);
-    sc[s].dt = f.dt;
+  const int no = m->h_node_off[s], nn = m->sys[s].nn;
+  const double* src[] = {f.h, f.S, f.B, f.rho, f.AGlen, f.n, f.C, f.m};
+  double* dst[] = {w->h, w->S, w->B, w->rho, w->A, w->n, w->C, w->m};
+  const char* names[] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
+  for (int k = 0; k < 8; ++k) {
+    if (!src[k]) return set_error(UA_ERR_INVALID, "system %d: null field pointer %s", s, names[k]);
+    // SSTREAM2dNR2.m:42-65: NaN in C or A (warning + NaN solution in the
+    // reference) and NaN in S, h, rho (error) all stop the solve here.
+    if (f.location == UA_HOST && any_nan(src[k], nn))
+      return set_error(UA_ERR_NAN_INPUT, "SSTREAM2dNR2: nan in %s (system %d)", names[k], s);
+    UA_CUDA_TRY(cudaMemcpyAsync(dst[k] + no, src[k], nn * sizeof(double),
+                                f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                m->stream));
   }
-  UA_CUDA_TRY(cudaMemcpyAsync(w->scal, sc.data(), sc.size() * sizeof(SysScal), cudaMemcpyHostToDevice, m->stream));
+  sc.rhow = f.rhow; sc.g = f.g; sc.ca = std::cos(f.alpha); sc.sa = std::sin(f.alpha);
+  sc.dt = f.dt;
+  return UA_OK;
+}
+
+static int finish_fields(ua_mesh* m, const ua_params* p, const std::vector<SysScal>& sc, int s0, int count) {
+  Work* w = m->work;
+  UA_CUDA_TRY(cudaMemcpyAsync(w->scal + s0, sc.data(), count * sizeof(SysScal), cudaMemcpyHostToDevice, m->stream));
   k_calc_bs<<<(m->nn_total + 255) / 256, 256, 0, m->stream>>>(m->nn_total, m->dm.node_sys, w->scal, p->kH, p->Hh0,
                                                                w->h, w->S, w->B, w->rho, w->s), ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
   return UA_OK;
 }
 
+// Upload nodal fields of every system (host or device pointers) and compute s.
+static int upload_fields(ua_mesh* m, const ua_params* p, const ua_fields* F, int nF) {
+  std::vector<SysScal> sc(m->dm.nsys);
+  for (int s = 0; s < m->dm.nsys; ++s) {
+    int rc = upload_fields_sys(m, F[nF == 1 ? 0 : s], s, sc[s]);
+    if (rc) return rc;
+  }
+  return finish_fields(m, p, sc, 0, m->dm.nsys);
+}
+
+// Velocities of system s into the dof vector X.
+static int upload_velocity_sys(ua_mesh* m, const ua_fields& f, int s) {
+  Work* w = m->work;
+  const int d0 = m->h_dof_off[s], nn = m->sys[s].nn;
+  if (!f.ub || !f.vb) return set_error(UA_ERR_INVALID, "null ub/vb");
+  if (f.location == UA_HOST && (any_nan(f.ub, nn) || any_nan(f.vb, nn)))
+    return set_error(UA_ERR_NAN_INPUT, "uvMatrixAssembly:NaN NaN in F.ub or F.vb");
+  auto kind = f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0, f.ub, nn * sizeof(double), kind, m->stream));
+  UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0 + nn, f.vb, nn * sizeof(double), kind, m->stream));
+  return UA_OK;
+}
+
 // Velocities of the fields into the dof vector X.
 static int upload_velocity(ua_mesh* m, const ua_fields* F, int nF) {
-  Work* w = m->work;
   for (int s = 0; s < m->dm.nsys; ++s) {
-    const ua_fields& f = F[nF == 1 ? 0 : s];
-    const int d0 = m->h_dof_off[s], nn = m->sys[s].nn;
-    if (!f.ub || !f.vb) return set_error(UA_ERR_INVALID, "null ub/vb");
-    if (f.location == UA_HOST && (any_nan(f.ub, nn) || any_nan(f.vb, nn)))
-      return set_error(UA_ERR_NAN_INPUT, "uvMatrixAssembly:NaN NaN in F.ub or F.vb");
-    auto kind = f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0, f.ub, nn * sizeof(double), kind, m->stream));
-    UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0 + nn, f.vb, nn * sizeof(double), kind, m->stream));
+    int rc = upload_velocity_sys(m, F[nF == 1 ? 0 : s], s);
+    if (rc) return rc;
   }
   return UA_OK;
 }
@@ -848,16 +866,25 @@ struct SysState {
   std::vector<double> ls_g, ls_rF, ls_D2;
 };
 
+// Per-slot state of the serving loop (ua_serve_*).
+struct ServeState {
+  std::vector<SysState> st;
+  std::vector<ua_newton_report> rep;
+  std::vector<std::vector<ua_newton_iter>> recs;
+  std::vector<int> retried, busy;
+  double t_asm = 0, t_sol = 0;
+};
+
 static double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// Newton driver for the systems with run[s]=1 (SSTREAM2dNR2.m:100-392).
-static int newton_run(ua_mesh* m, const ua_params* p, std::vector<int> run, std::vector<ua_newton_report*>& rep,
-                      std::vector<SysState>& st) {
+// Start the Newton solve of the systems with run[s]=1 (SSTREAM2dNR2.m:100-156):
+// make the iterate feasible, fext0 at ZeroFields, cost at the start iterate.
+// Other systems are left untouched, so a system can join while others iterate.
+static int newton_init(ua_mesh* m, const ua_params* p, const std::vector<int>& run, std::vector<SysState>& st) {
   Work* w = m->work;
   const int nsys = w->nsys;
-  double t_asm = 0, t_sol = 0;
   int rc;
   // make the iterate feasible (:101-104) and compute fext0 at ZeroFields (:122-124)
   UA_CUDA_TRY(cudaMemsetAsync(w->X0, 0, m->ndof_total * sizeof(double), m->stream));
@@ -889,9 +916,19 @@ static int newton_run(ua_mesh* m, const ua_params* p, std::vector<int> run, std:
     st[s].rWork = 0;
     st[s].gamma = 1;
   }
+  return UA_OK;
+}
+
+// One Newton iteration (SSTREAM2dNR2.m:157-392) of every active system.
+// *any is false when no system was active.
+static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_report*>& rep,
+                       std::vector<SysState>& st, double& t_asm, double& t_sol, bool* any_out) {
+  Work* w = m->work;
+  const int nsys = w->nsys;
+  int rc;
   std::vector<int> sel(nsys), its(nsys);
   std::vector<double> gam(nsys, 0.0);
-  while (true) {
+  {
     // convergence / iteration cap (:160-190)
     bool any = false;
     for (int s = 0; s < nsys; ++s) {
@@ -902,7 +939,8 @@ static int newton_run(ua_mesh* m, const ua_params* p, std::vector<int> run, std:
       S.iteration++;
       any = true;
     }
-    if (!any) break;
+    *any_out = any;
+    if (!any) return UA_OK;
     for (int s = 0; s < nsys; ++s) sel[s] = st[s].active ? 1 : 0;
     if ((rc = set_sel(m, sel))) return rc;
     // R and K (:197-213); the interval criterion 1 (default) always refreshes K
@@ -1028,6 +1066,22 @@ static int newton_run(ua_mesh* m, const ua_params* p, std::vector<int> run, std:
                                                                w->dlam), ++g_launches;
     UA_CUDA_TRY(cudaGetLastError());
   }
+  return UA_OK;
+}
+
+// Newton driver for the systems with run[s]=1 (SSTREAM2dNR2.m:100-392).
+static int newton_run(ua_mesh* m, const ua_params* p, std::vector<int> run, std::vector<ua_newton_report*>& rep,
+                      std::vector<SysState>& st) {
+  Work* w = m->work;
+  const int nsys = w->nsys;
+  double t_asm = 0, t_sol = 0;
+  int rc;
+  if ((rc = newton_init(m, p, run, st))) return rc;
+  for (int s = 0; s < nsys; ++s)
+    if (!run[s]) st[s].active = false;
+  bool any = true;
+  while (any)
+    if ((rc = newton_step(m, p, rep, st, t_asm, t_sol, &any))) return rc;
   for (int s = 0; s < nsys; ++s) {
     if (!run[s] || !rep[s]) continue;
     rep[s]->converged = st[s].converged ? 1 : 0;
@@ -1716,6 +1770,7 @@ extern "C" void ua_mesh_destroy(ua_mesh* m) {
   if (m->stream) cudaStreamSynchronize(m->stream);
   if (m->work) {
     Work* w = m->work;
+    delete w->serve;
     if (w->h_sysv) cudaFreeHost(w->h_sysv);
     if (w->h_int) cudaFreeHost(w->h_int);
     if (w->h_gamma) cudaFreeHost(w->h_gamma);
@@ -2173,4 +2228,172 @@ extern "C" int ua_uvh_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fi
   std::vector<ua_newton_report*> reps(m->dm.nsys);
   for (int s = 0; s < m->dm.nsys; ++s) reps[s] = reports ? &reports[s] : nullptr;
   return uvh_common(m, p, fields, bcs, m->dm.nsys, reps, nullptr, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Serving: continuous batching over the systems (slots) of a handle.  A
+// request is admitted into a free slot with ua_serve_begin (its fields and
+// warm start are uploaded and its Newton solve initialised) while the other
+// slots keep iterating; ua_serve_step advances every active slot by one
+// Newton iteration and reports the slots that finished.  Each slot's
+// arithmetic is independent of the others (per-system reductions and line
+// searches), so a result is the same alone and in the mix.
+// ---------------------------------------------------------------------------
+
+extern "C" int ua_serve_setup(ua_mesh* m, const ua_params* p, const ua_bcs* bcs) {
+  if (!m || !p || !bcs) return set_error(UA_ERR_INVALID, "ua_serve_setup: null argument");
+  if (m->ndof != 2) return set_error(UA_ERR_INVALID, "serving runs the uv solve (ndof=2 handle)");
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  int rc;
+  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_K(m, p->precision))) return rc;
+  if ((rc = build_constraints(m, bcs, m->dm.nsys))) return rc;
+  Work* w = m->work;
+  delete w->serve;
+  w->serve = new ServeState();
+  const int nsys = w->nsys;
+  w->serve->st.assign(nsys, SysState());
+  w->serve->rep.assign(nsys, ua_newton_report());
+  w->serve->recs.assign(nsys, std::vector<ua_newton_iter>(2 * (p->NRitmax + 2)));
+  w->serve->retried.assign(nsys, 0);
+  w->serve->busy.assign(nsys, 0);
+  if (w->nc) UA_CUDA_TRY(cudaMemsetAsync(w->lam, 0, w->nc * sizeof(double), m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return UA_OK;
+}
+
+static int serve_reset_lam(ua_mesh* m, int s) {
+  Work* w = m->work;
+  const int c0 = w->h_sys_con_off[s], nc_s = w->h_sys_con_off[s + 1] - c0;
+  if (nc_s) UA_CUDA_TRY(cudaMemsetAsync(w->lam + c0, 0, nc_s * sizeof(double), m->stream));
+  return UA_OK;
+}
+
+extern "C" int ua_serve_begin(ua_mesh* m, const ua_params* p, int32_t count, const int32_t* sys,
+                              const ua_fields* F) {
+  if (!m || !p || !sys || !F || count <= 0) return set_error(UA_ERR_INVALID, "ua_serve_begin: bad arguments");
+  if (!m->work || !m->work->serve) return set_error(UA_ERR_INVALID, "ua_serve_setup has not been called");
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  Work* w = m->work;
+  ServeState& S = *w->serve;
+  const int nsys = w->nsys;
+  std::vector<int> run(nsys, 0);
+  std::vector<SysScal> sc(nsys);
+  UA_CUDA_TRY(cudaMemcpy(sc.data(), w->scal, nsys * sizeof(SysScal), cudaMemcpyDeviceToHost));
+  int rc;
+  for (int k = 0; k < count; ++k) {
+    const int s = sys[k];
+    if (s < 0 || s >= nsys) return set_error(UA_ERR_INVALID, "slot %d out of range", s);
+    if (S.busy[s]) return set_error(UA_ERR_INVALID, "slot %d is busy", s);
+    if ((rc = upload_fields_sys(m, F[k], s, sc[s]))) return rc;
+    if ((rc = upload_velocity_sys(m, F[k], s))) return rc;
+    if ((rc = serve_reset_lam(m, s))) return rc;
+    run[s] = 1;
+  }
+  if ((rc = finish_fields(m, p, sc, 0, nsys))) return rc;
+  if ((rc = newton_init(m, p, run, S.st))) return rc;
+  for (int s = 0; s < nsys; ++s) {
+    if (!run[s]) continue;
+    S.busy[s] = 1;
+    S.retried[s] = 0;
+    ua_newton_report& r = S.rep[s];
+    std::memset(&r, 0, sizeof(r));
+    r.iters = S.recs[s].data();
+    r.iters_capacity = (int)S.recs[s].size();
+  }
+  return UA_OK;
+}
+
+extern "C" int ua_serve_step(ua_mesh* m, const ua_params* p, int32_t* finished, int32_t* nactive) {
+  if (!m || !p || !m->work || !m->work->serve) return set_error(UA_ERR_INVALID, "ua_serve_step: not set up");
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  Work* w = m->work;
+  ServeState& S = *w->serve;
+  const int nsys = w->nsys;
+  std::vector<ua_newton_report*> rep(nsys);
+  for (int s = 0; s < nsys; ++s) rep[s] = S.busy[s] ? &S.rep[s] : nullptr;
+  bool any = false;
+  int rc;
+  if ((rc = newton_step(m, p, rep, S.st, S.t_asm, S.t_sol, &any))) return rc;
+  // systems that stopped during this step (checked at the start of the next
+  // step in the batch driver; here they are retired at once)
+  std::vector<int> retry(nsys, 0);
+  bool need_retry = false;
+  int act = 0;
+  for (int s = 0; s < nsys; ++s) {
+    if (finished) finished[s] = 0;
+    if (!S.busy[s]) continue;
+    SysState& T = S.st[s];
+    bool stop = !T.active;
+    if (T.active) {  // apply the exit tests of the next iteration now (:160-190)
+      if (residual_criteria(p, T.rForce, T.rWork, T.iteration, T.gamma)) { T.converged = true; T.active = false; stop = true; }
+      else if (T.iteration > p->NRitmax) { T.converged = false; T.active = false; stop = true; }
+    }
+    if (stop && !T.converged && !S.retried[s]) {  // uv.m:107-112 reset-and-retry
+      retry[s] = 1;
+      need_retry = true;
+      continue;
+    }
+    if (stop) {
+      ua_newton_report& r = S.rep[s];
+      r.converged = T.converged ? 1 : 0;
+      r.iterations = T.iteration;
+      r.backtrack_steps = T.iarm;
+      r.r = T.r; r.rForce = T.rForce; r.rWork = T.rWork;
+      r.retried = S.retried[s];
+      S.busy[s] = 0;
+      if (finished) finished[s] = 1;
+    } else {
+      ++act;
+    }
+  }
+  if (need_retry) {
+    for (int s = 0; s < nsys; ++s) {
+      if (!retry[s]) continue;
+      const int d0 = m->h_dof_off[s], nd = m->h_dof_off[s + 1] - d0;
+      UA_CUDA_TRY(cudaMemsetAsync(w->X + d0, 0, nd * sizeof(double), m->stream));
+      if ((rc = serve_reset_lam(m, s))) return rc;
+      S.retried[s] = 1;
+      ++act;
+    }
+    if ((rc = newton_init(m, p, retry, S.st))) return rc;
+  }
+  if (nactive) *nactive = act;
+  (void)any;
+  return UA_OK;
+}
+
+extern "C" int ua_serve_result(ua_mesh* m, int32_t sys, double* ub, double* vb, ua_newton_report* rep) {
+  if (!m || !m->work || !m->work->serve) return set_error(UA_ERR_INVALID, "ua_serve_result: not set up");
+  if (sys < 0 || sys >= m->work->nsys) return set_error(UA_ERR_INVALID, "slot %d out of range", sys);
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  Work* w = m->work;
+  const int d0 = m->h_dof_off[sys], nn = m->sys[sys].nn;
+  if (ub) UA_CUDA_TRY(cudaMemcpyAsync(ub, w->X + d0, nn * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (vb) UA_CUDA_TRY(cudaMemcpyAsync(vb, w->X + d0 + nn, nn * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  if (rep) {
+    ua_newton_iter* it = rep->iters;
+    int cap = rep->iters_capacity;
+    *rep = w->serve->rep[sys];
+    rep->iters = it;
+    rep->iters_capacity = cap;
+    if (it) {
+      int n = std::min(cap, w->serve->rep[sys].n_iter_records);
+      for (int k = 0; k < n; ++k) it[k] = w->serve->recs[sys][k];
+      rep->n_iter_records = n;
+    } else {
+      rep->n_iter_records = 0;
+    }
+  }
+  return UA_OK;
+}
+
+extern "C" int ua_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes) {
+  UA_CUDA_TRY(cudaSetDevice(device));
+  size_t f = 0, t = 0;
+  UA_CUDA_TRY(cudaMemGetInfo(&f, &t));
+  if (free_bytes) *free_bytes = (int64_t)f;
+  if (total_bytes) *total_bytes = (int64_t)t;
+  return UA_OK;
 }

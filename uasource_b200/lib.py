@@ -134,6 +134,11 @@ SIGNATURES = {
                                 C.c_int32, C.POINTER(ua_newton_report)]),
     "ua_uvh_newton_batch": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),
                                       C.POINTER(ua_newton_report)]),
+    "ua_serve_setup": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_bcs)]),
+    "ua_serve_begin": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.c_int32, _ip, C.POINTER(ua_fields)]),
+    "ua_serve_step": (C.c_int, [C.c_void_p, C.POINTER(ua_params), _ip, _ip]),
+    "ua_serve_result": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, C.POINTER(ua_newton_report)]),
+    "ua_mem_info": (C.c_int, [C.c_int32, _lp, _lp]),
     "ua_constraint_count": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), C.c_int32, _ip]),
     "ua_solve_kape_symmetric": (C.c_int, [C.c_int32, _lp, _lp, _dp, C.c_int32, _lp, _lp, _dp, _dp, _dp, _dp, _dp,
                                           C.c_double, C.c_int32, _ip, C.c_int32]),

@@ -193,3 +193,19 @@ def elements_to_grid(nele_target: int, aspect: float = 2.0):
     ny1 = max(1, int(round(math.sqrt(nele_target / (2.0 * aspect)))))
     nx1 = max(1, int(round(aspect * ny1)))
     return nx1 + 1, ny1 + 1
+
+
+def batch_sizes(count=256, lo=2e3, hi=2e5, seed=12345):
+    """Element counts of the batched workload: log-uniform in [lo, hi] (seeded)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), count))
+
+
+def batch_problems(count=256, lo=2e3, hi=2e5, seed=12345):
+    """256 independent ice-stream/shelf problems on 100 km x 50 km rectangles of
+    log-uniform size (P1), each with its own seed for bumps, A and C."""
+    out = []
+    for k, ne in enumerate(batch_sizes(count, lo, hi, seed)):
+        nx, ny = elements_to_grid(int(ne), aspect=2.0)
+        out.append(ice_stream_shelf(nx, ny, nod=3, seed=1000 + k))
+    return out
