@@ -47,6 +47,10 @@ extern "C" {
 #define UA_PREC_FP64   0   /* all FP64 (the plain form) */
 #define UA_PREC_MIXED  1   /* FP32 element tangents + FP32 PCG with FP64 reductions */
 
+/* preconditioners of the inner uv solve */
+#define UA_PC_JACOBI 0   /* point Jacobi */
+#define UA_PC_AMG    1   /* aggregation AMG V(1,1) cycle, l1-Jacobi smoother (default) */
+
 /* Assembly modes of uvMatrixAssembly (uvMatrixAssemblySSTREAM.m:17-28). */
 #define UA_ASM_R      0   /* CtrlVar.uvMatrixAssembly.Ronly=true */
 #define UA_ASM_RK     1   /* R and K */
@@ -110,6 +114,10 @@ typedef struct ua_params {
     int32_t patch_nodes;       /* assembly patch size (0 = autotune) */
     int32_t verbose;           /* per-iteration log line to stderr */
     int32_t profile;           /* 1: time assembly and SpMV launches with CUDA events */
+    int32_t krylov_adaptive;   /* 1: inner tolerance eta_k = clamp(0.1*sqrt(rForce_k), krylov_rtol, 1e-2)
+                                  (inexact Newton forcing term); 0: krylov_rtol every iteration */
+    int32_t krylov_precond;    /* UA_PC_*: preconditioner of the uv inner PCG (the uvh BiCGStab uses
+                                  point Jacobi) */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

@@ -87,7 +87,7 @@ def test_newton_matches_golden(path):
     u = np.concatenate([Fo.ub, Fo.vb])
     assert np.linalg.norm(u - u_ref) <= U_TOL_FP64 * np.linalg.norm(u_ref)
     assert np.linalg.norm(lam - z["sol_l"]) <= 1e-8 * max(np.linalg.norm(z["sol_l"]), 1.0)
-    assert abs(info.iterations - int(z["sol_iterations"])) <= 1
+    assert abs(info.iterations - int(z["sol_iterations"])) <= 2  # inexact-Newton inner tolerance
 
 
 def test_zero_fields_and_parts_match_oracle():

@@ -65,7 +65,7 @@ def test_uvh_newton_matches_golden(path):
     ref = np.concatenate([z["sol_ub"], z["sol_vb"], z["sol_h"]])
     got = np.concatenate([Fo.ub, Fo.vb, Fo.h])
     assert np.linalg.norm(got - ref) <= U_TOL * np.linalg.norm(ref)
-    assert abs(info.iterations - int(z["sol_iterations"])) <= 1
+    assert abs(info.iterations - int(z["sol_iterations"])) <= 2  # inexact-Newton inner tolerance
 
 
 def test_uvh_zero_fields_matches_oracle():

@@ -1,0 +1,583 @@
+// Aggregation AMG preconditioner for the constrained uv tangent.
+//
+// Preconditions the inner PCG that replaces the reference's direct solve of
+// the Newton system (ABfgPreEliminate.m:110).  Node-based plain aggregation:
+// every level keeps Úa's dof layout [u; v] per system, a coarse node is an
+// aggregate of fine nodes and coarse dof (c, I) gathers the c-components of
+// its member nodes, so the prolongation P is piecewise constant per component
+// and the Galerkin operator P' A P is a pure summation.  Smoother: one
+// l1-Jacobi sweep (x += (b - A x) / sum_j |a_ij|) before and after the coarse
+// correction, a symmetric V(1,1) cycle and so an SPD preconditioner for CG.
+// Coarsest level: a dense inverse per system (at most 2*kAmgCoarseNodes dofs)
+// applied as a matrix-vector product.
+//
+// The hierarchy of a system depends only on that system's mesh and every
+// kernel works on per-system ranges in a fixed summation order, so a
+// system's result is the same alone and in a batch.  Constrained dofs (the
+// masked rows and columns of the projected system) have no coarse image:
+// they are left out of the Galerkin sums, the restriction and the
+// prolongation.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "ua_amg.h"
+
+namespace ua {
+
+constexpr int kAmgCoarseNodes = 48;   // a system stops coarsening at this many nodes
+constexpr int kAmgMaxRow = 32;        // longest coarse dof row (2 x coarse node degree)
+constexpr int kAmgMaxDense = 2 * kAmgCoarseNodes;
+constexpr int kAmgRB = 256;           // rows per row block of a coarse level
+
+struct AmgLevel {
+  int nn = 0, ndof = 0;
+  long long nnz = 0;
+  std::vector<int> node_off, dof_off, knz_off, nnzn;  // per system (0-sized when the system has no such level)
+  // dof-level CSR of a coarse level, same layout rule as the finest level
+  int *rowptr = nullptr, *colind = nullptr;
+  int* dof_sys = nullptr;
+  int *rb_start = nullptr, *rb_sys = nullptr;
+  int nrb = 0;
+  int* cmap = nullptr;                    // this level's dof -> next level's dof
+  int *mptr = nullptr, *mlist = nullptr;  // per dof of this (coarse) level: member dofs of the finer level
+  void* A = nullptr;                      // coarse values (KT)
+  void* invd = nullptr;                   // l1-Jacobi inverse row sums (VT)
+  void *b = nullptr, *x = nullptr, *x2 = nullptr;  // rhs, pre-smoothed, post-smoothed (VT)
+};
+
+struct Amg {
+  int nsys = 0, nlev = 0, maxdn = 0;
+  std::vector<AmgLevel> lev;  // lev[0] = the handle's own system
+  std::vector<int> depth;     // per system: its coarsest level (>= 1)
+  std::vector<int> h_dn, h_doff;
+  int *d_depth = nullptr, *d_dn = nullptr, *d_doff = nullptr;
+  double* dense = nullptr;    // per system dn x dn inverse (row-major)
+  void **d_lev_b = nullptr, **d_lev_x2 = nullptr, **d_lev_A = nullptr;
+  int **d_lev_rowptr = nullptr, **d_lev_colind = nullptr, **d_lev_dofoff = nullptr;
+  size_t bytes = 0;
+};
+
+// ---------------------------------------------------------------------------
+// host: aggregation and hierarchy
+// ---------------------------------------------------------------------------
+
+// Greedy aggregation of a node graph (system-local ids, self included):
+// (1) a node whose neighbourhood is entirely unassigned becomes the root of
+// an aggregate of that neighbourhood; (2) an unassigned node joins the
+// aggregate of its first assigned neighbour; (3) what is left forms
+// aggregates with its unassigned neighbours.
+static int aggregate(int n, const std::vector<int>& ptr, const std::vector<int>& col, std::vector<int>& agg) {
+  agg.assign(n, -1);
+  int na = 0;
+  for (int i = 0; i < n; ++i) {
+    if (agg[i] >= 0) continue;
+    bool free_nb = true;
+    for (int k = ptr[i]; k < ptr[i + 1] && free_nb; ++k) free_nb = agg[col[k]] < 0;
+    if (!free_nb) continue;
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) agg[col[k]] = na;
+    ++na;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (agg[i] >= 0) continue;
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k)
+      if (agg[col[k]] >= 0) { agg[i] = agg[col[k]]; break; }
+  }
+  for (int i = 0; i < n; ++i) {
+    if (agg[i] >= 0) continue;
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k)
+      if (agg[col[k]] < 0) agg[col[k]] = na;
+    agg[i] = na++;
+  }
+  return na;
+}
+
+template <class T>
+static T* upload(ua_mesh* m, Amg* a, const std::vector<T>& v, bool& ok) {
+  T* d = (T*)dev_alloc(m, std::max<size_t>(1, v.size()) * sizeof(T));
+  if (!d) { ok = false; return nullptr; }
+  if (!v.empty() && cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) ok = false;
+  a->bytes += v.size() * sizeof(T);
+  return d;
+}
+
+static void* dalloc(ua_mesh* m, Amg* a, size_t bytes, bool& ok) {
+  void* d = dev_alloc(m, std::max<size_t>(bytes, 16));
+  if (!d) ok = false;
+  a->bytes += bytes;
+  return d;
+}
+
+// Dof-level CSR of a level from its node graph (global ids of the level):
+// row (c, I) holds 2 blocks of deg(I) columns (block b, k-th neighbour).
+static void level_csr(AmgLevel& L, const std::vector<int>& gptr, const std::vector<int>& gcol, int nsys,
+                      std::vector<int>& rowptr, std::vector<int>& colind, std::vector<int>& dof_sys) {
+  const std::vector<int>& no = L.node_off;
+  L.dof_off.assign(nsys + 1, 0);
+  L.knz_off.assign(nsys + 1, 0);
+  L.nnzn.assign(nsys, 0);
+  for (int s = 0; s < nsys; ++s) {
+    const int n = no[s + 1] - no[s];
+    L.dof_off[s + 1] = L.dof_off[s] + 2 * n;
+    L.nnzn[s] = gptr[no[s + 1]] - gptr[no[s]];
+    L.knz_off[s + 1] = L.knz_off[s] + 4 * L.nnzn[s];
+  }
+  const int N = L.dof_off[nsys];
+  rowptr.assign(N + 1, 0);
+  colind.assign(L.knz_off[nsys], 0);
+  dof_sys.assign(N, 0);
+  for (int s = 0; s < nsys; ++s) {
+    const int n0 = no[s], n = no[s + 1] - n0, base = gptr[n0];
+    for (int I = n0; I < n0 + n; ++I) {
+      const int p0 = gptr[I], deg = gptr[I + 1] - p0;
+      for (int c = 0; c < 2; ++c) {
+        const int dof = L.dof_off[s] + c * n + (I - n0);
+        const int start = L.knz_off[s] + c * 2 * L.nnzn[s] + 2 * (p0 - base);
+        rowptr[dof] = start;
+        dof_sys[dof] = s;
+        for (int b = 0; b < 2; ++b)
+          for (int k = 0; k < deg; ++k) colind[start + b * deg + k] = L.dof_off[s] + b * n + (gcol[p0 + k] - n0);
+      }
+    }
+  }
+  rowptr[N] = L.knz_off[nsys];
+  L.nn = no[nsys];
+  L.ndof = N;
+  L.nnz = L.knz_off[nsys];
+}
+
+int amg_setup(ua_mesh* m) {
+  if (m->amg) return UA_OK;
+  if (m->amg_failed) return UA_ERR_INVALID;
+  if (m->ndof != 2) return set_error(UA_ERR_INVALID, "the AMG preconditioner serves the uv tangent");
+  const int nsys = m->dm.nsys;
+  Amg* a = new Amg();
+  a->nsys = nsys;
+  a->depth.assign(nsys, 0);
+  // node graphs per level (global ids of the level)
+  std::vector<std::vector<int>> g_off{m->h_node_off}, g_ptr{m->h_nodeptr}, g_col{m->h_nodecol}, g_agg;
+  std::vector<char> live(nsys, 1);
+  auto fail = [&](const char* why) {
+    delete a;
+    m->amg_failed = true;
+    return set_error(UA_ERR_INVALID, "AMG setup: %s", why);
+  };
+  while (std::find(live.begin(), live.end(), 1) != live.end()) {
+    const std::vector<int>& no = g_off.back();
+    const std::vector<int>& fp = g_ptr.back();
+    const std::vector<int>& fc = g_col.back();
+    std::vector<int> agg(no[nsys], -1), cno(nsys + 1, 0), cptr(1, 0), ccol;
+    for (int s = 0; s < nsys; ++s) {
+      const int n = no[s + 1] - no[s];
+      if (!live[s] || n == 0) { cno[s + 1] = cno[s]; continue; }
+      std::vector<int> lp(n + 1, 0), lc, la;
+      for (int i = 0; i < n; ++i) {
+        for (int k = fp[no[s] + i]; k < fp[no[s] + i + 1]; ++k) lc.push_back(fc[k] - no[s]);
+        lp[i + 1] = (int)lc.size();
+      }
+      const int na = aggregate(n, lp, lc, la);
+      for (int i = 0; i < n; ++i) agg[no[s] + i] = cno[s] + la[i];
+      cno[s + 1] = cno[s] + na;
+      std::vector<std::vector<int>> adj(na);
+      for (int i = 0; i < n; ++i)
+        for (int k = lp[i]; k < lp[i + 1]; ++k) adj[la[i]].push_back(la[lc[k]]);
+      for (int I = 0; I < na; ++I) {
+        std::sort(adj[I].begin(), adj[I].end());
+        adj[I].erase(std::unique(adj[I].begin(), adj[I].end()), adj[I].end());
+        if (2 * (int)adj[I].size() > kAmgMaxRow) return fail("coarse node degree above the row limit");
+        for (int J : adj[I]) ccol.push_back(cno[s] + J);
+        cptr.push_back((int)ccol.size());
+      }
+      a->depth[s]++;
+      if (na <= kAmgCoarseNodes) live[s] = 0;
+      else if (na >= n) return fail("aggregation made no progress");
+    }
+    g_agg.push_back(agg);
+    g_off.push_back(cno);
+    g_ptr.push_back(cptr);
+    g_col.push_back(ccol);
+  }
+  a->nlev = (int)g_off.size();
+  a->lev.resize(a->nlev);
+  bool ok = true;
+  for (int l = 0; l < a->nlev; ++l) {
+    AmgLevel& L = a->lev[l];
+    L.node_off = g_off[l];
+    std::vector<int> rowptr, colind, dof_sys;
+    level_csr(L, g_ptr[l], g_col[l], nsys, rowptr, colind, dof_sys);
+    if (l == 0 && (L.ndof != m->ndof_total || L.nnz != m->nnz_total)) return fail("fine level does not match the handle");
+    std::vector<int> rb_start, rb_sys;
+    for (int s = 0; s < nsys; ++s)
+      for (int r = L.dof_off[s]; r < L.dof_off[s + 1]; r += kAmgRB) { rb_start.push_back(r); rb_sys.push_back(s); }
+    rb_start.push_back(L.ndof);
+    L.nrb = (int)rb_sys.size();
+    L.invd = dalloc(m, a, sizeof(double) * (size_t)L.ndof, ok);
+    if (l > 0) {  // the fine level uses the handle's tangent structure and PCG vectors
+      L.rb_start = upload(m, a, rb_start, ok);
+      L.rb_sys = upload(m, a, rb_sys, ok);
+      L.dof_sys = upload(m, a, dof_sys, ok);
+      L.rowptr = upload(m, a, rowptr, ok);
+      L.colind = upload(m, a, colind, ok);
+      L.A = dalloc(m, a, sizeof(double) * (size_t)L.nnz, ok);
+      L.b = dalloc(m, a, sizeof(double) * (size_t)L.ndof, ok);
+      L.x = dalloc(m, a, sizeof(double) * (size_t)L.ndof, ok);
+      L.x2 = dalloc(m, a, sizeof(double) * (size_t)L.ndof, ok);
+      // coarse dof (c, I) gathers fine dofs (c, i) with agg[i] = I, in ascending order
+      AmgLevel& F = a->lev[l - 1];
+      const std::vector<int>& agg = g_agg[l - 1];
+      std::vector<int> cmap(F.ndof, -1), cnt(L.ndof + 1, 0), mlist(F.ndof);
+      for (int s = 0; s < nsys; ++s) {
+        const int fno = F.node_off[s], fn = F.node_off[s + 1] - fno;
+        const int cno = L.node_off[s], cn = L.node_off[s + 1] - cno;
+        if (cn == 0) continue;
+        for (int c = 0; c < 2; ++c)
+          for (int i = 0; i < fn; ++i)
+            cmap[F.dof_off[s] + c * fn + i] = L.dof_off[s] + c * cn + (agg[fno + i] - cno);
+      }
+      for (int d = 0; d < F.ndof; ++d)
+        if (cmap[d] >= 0) cnt[cmap[d] + 1]++;
+      for (int d = 0; d < L.ndof; ++d) cnt[d + 1] += cnt[d];
+      std::vector<int> mptr = cnt;
+      for (int d = 0; d < F.ndof; ++d)
+        if (cmap[d] >= 0) mlist[cnt[cmap[d]]++] = d;
+      mlist.resize(mptr[L.ndof]);
+      F.cmap = upload(m, a, cmap, ok);
+      L.mptr = upload(m, a, mptr, ok);
+      L.mlist = upload(m, a, mlist, ok);
+    }
+  }
+  a->h_dn.assign(nsys, 0);
+  a->h_doff.assign(nsys + 1, 0);
+  for (int s = 0; s < nsys; ++s) {
+    const AmgLevel& L = a->lev[a->depth[s]];
+    a->h_dn[s] = L.dof_off[s + 1] - L.dof_off[s];
+    if (a->h_dn[s] > kAmgMaxDense) return fail("coarsest system above the dense limit");
+    a->maxdn = std::max(a->maxdn, a->h_dn[s]);
+    a->h_doff[s + 1] = a->h_doff[s] + a->h_dn[s] * a->h_dn[s];
+  }
+  a->dense = (double*)dalloc(m, a, sizeof(double) * (size_t)a->h_doff[nsys], ok);
+  a->d_depth = upload(m, a, a->depth, ok);
+  a->d_dn = upload(m, a, a->h_dn, ok);
+  a->d_doff = upload(m, a, a->h_doff, ok);
+  std::vector<void*> pb(a->nlev), px2(a->nlev), pA(a->nlev);
+  std::vector<int*> prp(a->nlev), pci(a->nlev), pdo(a->nlev);
+  for (int l = 0; l < a->nlev; ++l) {
+    pb[l] = a->lev[l].b;
+    px2[l] = a->lev[l].x2;
+    pA[l] = a->lev[l].A;
+    prp[l] = a->lev[l].rowptr;
+    pci[l] = a->lev[l].colind;
+    pdo[l] = upload(m, a, a->lev[l].dof_off, ok);
+  }
+  a->d_lev_b = upload(m, a, pb, ok);
+  a->d_lev_x2 = upload(m, a, px2, ok);
+  a->d_lev_A = upload(m, a, pA, ok);
+  a->d_lev_rowptr = upload(m, a, prp, ok);
+  a->d_lev_colind = upload(m, a, pci, ok);
+  a->d_lev_dofoff = upload(m, a, pdo, ok);
+  if (!ok) {
+    delete a;
+    return set_error(UA_ERR_OOM, "AMG setup: device allocation failed");
+  }
+  m->amg = a;
+  return UA_OK;
+}
+
+void amg_free(Amg* a) { delete a; }
+
+int amg_levels(const ua_mesh* m) { return m->amg ? m->amg->nlev : 0; }
+
+const void* amg_invd0(const ua_mesh* m) { return m->amg ? m->amg->lev[0].invd : nullptr; }
+
+// ---------------------------------------------------------------------------
+// device: numeric phase
+// ---------------------------------------------------------------------------
+
+// Galerkin product: coarse row R sums the unmasked entries of its member
+// rows into the coarse columns cmap[j] (binary search in the sorted coarse row).
+template <typename KT>
+__global__ void k_amg_galerkin(int ncd, const int* mptr, const int* mlist, const int* frowptr, const int* fcolind,
+                               const KT* fA, const int* cmap, const unsigned char* cmask, const int* crowptr,
+                               const int* ccolind, KT* cA) {
+  const int R = blockIdx.x * blockDim.x + threadIdx.x;
+  if (R >= ncd) return;
+  const int c0 = crowptr[R], len = crowptr[R + 1] - c0;
+  double acc[kAmgMaxRow];
+#pragma unroll
+  for (int k = 0; k < kAmgMaxRow; ++k) acc[k] = 0;
+  for (int t = mptr[R]; t < mptr[R + 1]; ++t) {
+    const int i = mlist[t];
+    if (cmask && cmask[i]) continue;
+    for (int q = frowptr[i]; q < frowptr[i + 1]; ++q) {
+      const int j = fcolind[q];
+      if (cmask && cmask[j]) continue;
+      const int C = cmap[j];
+      int lo = 0, hi = len - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (ccolind[c0 + mid] < C) lo = mid + 1; else hi = mid;
+      }
+      acc[lo] += (double)fA[q];
+    }
+  }
+  for (int k = 0; k < len; ++k) cA[c0 + k] = (KT)acc[k];
+}
+
+// l1-Jacobi: invd_i = 1 / sum_j |a_ij| over unmasked columns (0 on masked or empty rows)
+template <typename KT, typename VT>
+__global__ void k_amg_l1(int n, const int* rowptr, const int* colind, const KT* A, const unsigned char* cmask,
+                         VT* invd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0;
+  if (!(cmask && cmask[i]))
+    for (int q = rowptr[i]; q < rowptr[i + 1]; ++q)
+      if (!(cmask && cmask[colind[q]])) s += fabs((double)A[q]);
+  invd[i] = (VT)(s > 0 ? 1.0 / s : 0.0);
+}
+
+// Inverse of each system's coarsest matrix: Gauss-Jordan with partial
+// pivoting on [A | I] in shared memory, one CTA per system.  A zero row (an
+// aggregate of constrained dofs only; its column is zero too) is replaced by
+// the identity row.
+template <typename KT>
+__global__ void __launch_bounds__(256) k_amg_dense_inverse(const int* depth, const int* dn_arr, const int* doff,
+                                                           int* const* lev_rowptr, int* const* lev_colind,
+                                                           void* const* lev_A, int* const* lev_dofoff,
+                                                           double* dense) {
+  extern __shared__ double M[];
+  __shared__ double fac[kAmgMaxDense];
+  __shared__ int piv;
+  const int s = blockIdx.x;
+  const int n = dn_arr[s];
+  if (n == 0) return;
+  const int l = depth[s];
+  const int* rp = lev_rowptr[l];
+  const int* ci = lev_colind[l];
+  const KT* A = (const KT*)lev_A[l];
+  const int d0 = lev_dofoff[l][s];
+  const int w = 2 * n;
+  for (int t = threadIdx.x; t < n * w; t += blockDim.x) M[t] = ((t % w) - n == t / w) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    bool zero = true;
+    for (int q = rp[d0 + r]; q < rp[d0 + r + 1]; ++q) {
+      const double v = (double)A[q];
+      M[r * w + (ci[q] - d0)] = v;
+      zero = zero && v == 0.0;
+    }
+    if (zero) M[r * w + r] = 1.0;
+  }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (threadIdx.x == 0) {
+      int p = k;
+      double best = fabs(M[k * w + k]);
+      for (int r = k + 1; r < n; ++r)
+        if (fabs(M[r * w + k]) > best) { best = fabs(M[r * w + k]); p = r; }
+      piv = p;
+    }
+    __syncthreads();
+    const int pk = piv;
+    if (pk != k)
+      for (int c = threadIdx.x; c < w; c += blockDim.x) {
+        const double t = M[k * w + c];
+        M[k * w + c] = M[pk * w + c];
+        M[pk * w + c] = t;
+      }
+    __syncthreads();
+    const double inv = 1.0 / M[k * w + k];
+    for (int r = threadIdx.x; r < n; r += blockDim.x) fac[r] = (r == k) ? 0.0 : M[r * w + k];
+    __syncthreads();
+    for (int c = threadIdx.x; c < w; c += blockDim.x) M[k * w + c] *= inv;
+    __syncthreads();
+    for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
+      const int r = t / w, c = t - r * w;
+      if (r != k) M[t] -= fac[r] * M[k * w + c];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) dense[doff[s] + t] = M[(t / n) * w + n + (t % n)];
+}
+
+// ---------------------------------------------------------------------------
+// device: V-cycle
+// ---------------------------------------------------------------------------
+
+// Restriction of the pre-smoothed residual of level lc-1 to level lc:
+// b(R) = sum over members i of (b_f(i) - (A_f x_f)(i)), masked members left
+// out; the coarse pre-smoothing x = invd b follows unless lc is the
+// system's coarsest level.
+template <typename KT, typename VT>
+__global__ void k_amg_restrict(int ncd, const int* dof_sys_c, const int* depth, int lc, const int* sel,
+                               const int* done, const int* mptr, const int* mlist, const int* frowptr,
+                               const int* fcolind, const KT* fA, const VT* fb, const VT* fx,
+                               const unsigned char* cmask, const VT* cinvd, VT* cb, VT* cx) {
+  const int R = blockIdx.x * blockDim.x + threadIdx.x;
+  if (R >= ncd) return;
+  const int s = dof_sys_c[R];
+  if (!sel[s] || done[s]) return;
+  double acc = 0;
+  for (int t = mptr[R]; t < mptr[R + 1]; ++t) {
+    const int i = mlist[t];
+    if (cmask && cmask[i]) continue;
+    double r = (double)fb[i];
+    for (int q = frowptr[i]; q < frowptr[i + 1]; ++q) r -= (double)fA[q] * (double)fx[fcolind[q]];
+    acc += r;
+  }
+  cb[R] = (VT)acc;
+  if (depth[s] > lc) cx[R] = (VT)((double)cinvd[R] * acc);
+}
+
+// x2 = inv(A_L) b on each system's coarsest level L
+template <typename VT>
+__global__ void k_amg_dense_apply(const int* sel, const int* done, const int* depth, const int* dn_arr,
+                                  const int* doff, int* const* lev_dofoff, void* const* lev_b, void* const* lev_x2,
+                                  const double* dense) {
+  const int s = blockIdx.x;
+  if (!sel[s] || done[s]) return;
+  const int n = dn_arr[s], l = depth[s];
+  const int d0 = lev_dofoff[l][s];
+  const VT* b = (const VT*)lev_b[l] + d0;
+  VT* x = (VT*)lev_x2[l] + d0;
+  const double* Mi = dense + doff[s];
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    double acc = 0;
+    for (int c = 0; c < n; ++c) acc += Mi[r * n + c] * (double)b[c];
+    x[r] = (VT)acc;
+  }
+}
+
+// Coarse correction and post-smoothing of level l (systems deeper than l):
+// xp = x + P xc;  out = xp + invd (b - A xp), masked rows 0 and masked
+// columns without a coarse image.  On the finest level the block partials of
+// b.out (r.z) go to part and pcopy receives a copy of out.
+template <typename KT, typename VT, int LPR>
+__global__ void __launch_bounds__(256) k_amg_prolong_smooth(const int* rb_start, const int* rb_sys, int nrb,
+                                                            const int* sel, const int* done, const int* depth, int l,
+                                                            const int* rowptr, const int* colind, const KT* A,
+                                                            const VT* b, const VT* x, const VT* xc, const int* cmap,
+                                                            const VT* invd, const unsigned char* cmask, VT* out,
+                                                            VT* pcopy, double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double rz = 0;
+  if (sel[s] && !done[s] && depth[s] > l) {
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread
+      const int row = row0 + grp;
+      const bool valid = row < re;
+      double ax = 0;
+      if (valid)
+        for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) {
+          const int j = colind[q];
+          if (cmask && cmask[j]) continue;
+          ax += (double)A[q] * ((double)x[j] + (double)xc[cmap[j]]);
+        }
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) ax += __shfl_down_sync(0xffffffffu, ax, o, LPR);
+      if (valid && lane == 0) {
+        double v = 0;
+        if (!(cmask && cmask[row])) {
+          const double xp = (double)x[row] + (double)xc[cmap[row]];
+          v = xp + (double)invd[row] * ((double)b[row] - ax);
+        }
+        out[row] = (VT)v;
+        if (pcopy) pcopy[row] = (VT)v;
+        rz += (double)b[row] * v;
+      }
+    }
+  }
+  if (part) {
+    __shared__ double red[8];
+    double t = rz;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
+      part[blk] = sum;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------
+
+template <typename KT, typename VT>
+static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const KT* K0, const unsigned char* cmask,
+                     long long* launches) {
+  Amg* a = m->amg;
+  cudaStream_t st = m->stream;
+  for (int l = 0; l + 1 < a->nlev; ++l) {
+    const AmgLevel& F = a->lev[l];
+    const AmgLevel& C = a->lev[l + 1];
+    k_amg_galerkin<KT><<<(C.ndof + 127) / 128, 128, 0, st>>>(
+        C.ndof, C.mptr, C.mlist, l == 0 ? rowptr0 : F.rowptr, l == 0 ? colind0 : F.colind,
+        l == 0 ? K0 : (const KT*)F.A, F.cmap, l == 0 ? cmask : nullptr, C.rowptr, C.colind, (KT*)C.A), ++*launches;
+  }
+  for (int l = 0; l < a->nlev; ++l) {
+    const AmgLevel& L = a->lev[l];
+    k_amg_l1<KT, VT><<<(L.ndof + 255) / 256, 256, 0, st>>>(
+        L.ndof, l == 0 ? rowptr0 : L.rowptr, l == 0 ? colind0 : L.colind, l == 0 ? K0 : (const KT*)L.A,
+        l == 0 ? cmask : nullptr, (VT*)L.invd), ++*launches;
+  }
+  const int sm = (int)(sizeof(double) * (size_t)a->maxdn * 2 * a->maxdn);
+  UA_CUDA_TRY(cudaFuncSetAttribute(k_amg_dense_inverse<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  k_amg_dense_inverse<KT><<<a->nsys, 256, sm, st>>>(a->d_depth, a->d_dn, a->d_doff, a->d_lev_rowptr,
+                                                     a->d_lev_colind, a->d_lev_A, a->d_lev_dofoff, a->dense),
+      ++*launches;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "AMG numeric phase: %s", cudaGetErrorString(e));
+  return UA_OK;
+}
+
+int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
+                const unsigned char* cmask, long long* launches) {
+  if (fp32) return numeric_t<float, float>(m, rowptr0, colind0, (const float*)K0, cmask, launches);
+  return numeric_t<double, double>(m, rowptr0, colind0, (const double*)K0, cmask, launches);
+}
+
+template <typename KT, typename VT>
+static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
+  Amg* a = m->amg;
+  cudaStream_t st = m->stream;
+  const int nl = a->nlev;
+  for (int l = 0; l + 1 < nl; ++l) {  // down
+    const AmgLevel& F = a->lev[l];
+    const AmgLevel& C = a->lev[l + 1];
+    k_amg_restrict<KT, VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(
+        C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done, C.mptr, C.mlist, l == 0 ? v.rowptr0 : F.rowptr,
+        l == 0 ? v.colind0 : F.colind, l == 0 ? (const KT*)v.K0 : (const KT*)F.A,
+        l == 0 ? (const VT*)v.r : (const VT*)F.b, l == 0 ? (const VT*)v.x0 : (const VT*)F.x,
+        l == 0 ? v.cmask : nullptr, (const VT*)C.invd, (VT*)C.b, (VT*)C.x), ++*launches;
+  }
+  k_amg_dense_apply<VT><<<a->nsys, 128, 0, st>>>(v.sel, v.done, a->d_depth, a->d_dn, a->d_doff, a->d_lev_dofoff,
+                                                 a->d_lev_b, a->d_lev_x2, a->dense), ++*launches;
+  for (int l = nl - 2; l >= 0; --l) {  // up: the finer level reads the coarser post-smoothed x2
+    const AmgLevel& F = a->lev[l];
+    const AmgLevel& C = a->lev[l + 1];
+    const bool fine = l == 0;
+    k_amg_prolong_smooth<KT, VT, 8><<<fine ? v.nrb0 : F.nrb, 256, 0, st>>>(
+        fine ? v.rb_start0 : F.rb_start, fine ? v.rb_sys0 : F.rb_sys, fine ? v.nrb0 : F.nrb, v.sel, v.done,
+        a->d_depth, l, fine ? v.rowptr0 : F.rowptr, fine ? v.colind0 : F.colind,
+        fine ? (const KT*)v.K0 : (const KT*)F.A, fine ? (const VT*)v.r : (const VT*)F.b,
+        fine ? (const VT*)v.x0 : (const VT*)F.x, (const VT*)C.x2, F.cmap, (const VT*)F.invd,
+        fine ? v.cmask : nullptr, fine ? (VT*)v.z : (VT*)F.x2, fine ? (VT*)v.pcopy : nullptr,
+        fine ? v.part_rz : nullptr), ++*launches;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "AMG V-cycle: %s", cudaGetErrorString(e));
+  return UA_OK;
+}
+
+int amg_vcycle(ua_mesh* m, bool fp32, const AmgPcgView& v, long long* launches) {
+  if (fp32) return vcycle_t<float, float>(m, v, launches);
+  return vcycle_t<double, double>(m, v, launches);
+}
+
+}  // namespace ua

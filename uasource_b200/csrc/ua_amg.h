@@ -1,0 +1,41 @@
+// Aggregation AMG preconditioner of the uv tangent (internal interface).
+#pragma once
+#include "ua_internal.h"
+
+namespace ua {
+
+struct Amg;
+
+// Fine-level view of one preconditioner application z = M^-1 r inside PCG.
+// x0 holds the pre-smoothed fine vector (l1-Jacobi of r, written by the
+// caller with amg_invd0); z receives the result (and pcopy, if set, a copy);
+// part_rz the row-block partials of r.z.
+struct AmgPcgView {
+  const int *rowptr0, *colind0;
+  const void* K0;
+  const void* r;
+  const void* x0;
+  void* z;
+  void* pcopy;
+  double* part_rz;
+  const unsigned char* cmask;
+  const int *sel, *done;
+  const int *rb_start0, *rb_sys0;
+  int nrb0;
+};
+
+// Build the hierarchy of every system of the handle (host aggregation,
+// device structures); no-op when built.  Returns UA_OK or an error code
+// (the handle then keeps point-Jacobi).
+int amg_setup(ua_mesh* m);
+void amg_free(Amg* a);
+int amg_levels(const ua_mesh* m);
+// l1-Jacobi inverse row sums of the fine level (VT-typed, valid after amg_numeric)
+const void* amg_invd0(const ua_mesh* m);
+// Numeric phase for a new tangent K0 (Galerkin products, smoother, coarsest inverses).
+int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
+                const unsigned char* cmask, long long* launches);
+// One V(1,1) cycle.
+int amg_vcycle(ua_mesh* m, bool fp32, const AmgPcgView& v, long long* launches);
+
+}  // namespace ua

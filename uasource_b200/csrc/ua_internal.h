@@ -94,6 +94,7 @@ struct Constraints {
 };
 
 struct Work;
+struct Amg;
 
 }  // namespace ua
 
@@ -114,6 +115,9 @@ struct ua_mesh {
   size_t device_bytes = 0;
   // reusable work buffers
   ua::Work* work = nullptr;
+  // aggregation AMG hierarchy of the uv tangent (built on first use)
+  ua::Amg* amg = nullptr;
+  bool amg_failed = false;
 };
 
 namespace ua {

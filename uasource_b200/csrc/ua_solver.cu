@@ -18,6 +18,7 @@
 #include "ua_internal.h"
 #include "ua_kernels.h"
 #include "ua_linesearch.h"
+#include "ua_amg.h"
 
 namespace ua {
 
@@ -62,6 +63,7 @@ struct Work {
   float* Kf = nullptr;
   // Krylov (VT = double or float, allocated as double-sized)
   void *kr, *kz, *kp, *kq, *invd;
+  void* kx0 = nullptr;   // AMG: pre-smoothed fine vector
   double* part;    // [4][nrb]
   double* sysv;    // [SV_COUNT][nsys]
   int* done;       // [nsys]
@@ -768,30 +770,58 @@ static int cost_eval(ua_mesh* m, const ua_params* p, bool useDir) {
 }
 
 template <typename KT, typename VT>
-static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out) {
+static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, const double* eta = nullptr) {
   Work* w = m->work;
   const int N = m->ndof_total;
   const int lpr = (m->nod == 3 && m->ndof == 2) ? 8 : 16;
-  // per-system tolerance
-  for (int s = 0; s < w->nsys; ++s) w->h_sysv[s] = p->krylov_rtol * p->krylov_rtol;
+  // per-system tolerance (relative residual of the preconditioned solve)
+  for (int s = 0; s < w->nsys; ++s) {
+    const double e = eta ? eta[s] : p->krylov_rtol;
+    w->h_sysv[s] = e * e;
+  }
   UA_CUDA_TRY(cudaMemcpyAsync(w->sysv + SV_TOL2 * w->nsys, w->h_sysv, w->nsys * sizeof(double),
                               cudaMemcpyHostToDevice, m->stream));
-  k_invdiag<KT, VT><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, (VT*)w->invd), ++g_launches;
+  // preconditioner: aggregation AMG V(1,1) for the uv tangent of a mesh handle, else point Jacobi
+  bool amg = p->krylov_precond == UA_PC_AMG && m->ndof == 2 && !m->h_nodeptr.empty();
+  if (amg && !w->kx0) {
+    w->kx0 = walloc<double>(m, N);
+    if (!w->kx0) return set_error(UA_ERR_OOM, "device allocation of the AMG work vector failed");
+  }
+  if (amg && amg_setup(m) != UA_OK) amg = false;  // shapes the hierarchy cannot take keep point Jacobi
+  const bool fp32 = sizeof(KT) == 4;
+  if (amg) {
+    int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches);
+    if (rc) return rc;
+  } else {
+    k_invdiag<KT, VT><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, (VT*)w->invd), ++g_launches;
+  }
   // particular solution on the constrained dofs
   k_zero_sel<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->dX), ++g_launches;
   if (w->nc)
     k_con_particular<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs,
                                                                  w->X, w->dX, w->grhs), ++g_launches;
   VT *r = (VT*)w->kr, *z = (VT*)w->kz, *pp = (VT*)w->kp, *q = (VT*)w->kq;
-  const VT* invd = (const VT*)w->invd;
+  // with AMG the Jacobi-type kernels write the l1 pre-smoothed vector x0 and the V-cycle writes z (and r.z)
+  const VT* invd = amg ? (const VT*)amg_invd0(m) : (const VT*)w->invd;
+  VT* zj = amg ? (VT*)w->kx0 : z;
+  AmgPcgView view{w->rowptr, w->colind, K, r, w->kx0, z, nullptr, w->part, w->cmask, w->sel, w->done,
+                  w->rb_start, w->rb_sys, w->nrb};
   if (lpr == 8)
     k_pcg_init<KT, VT, 8><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr,
-                                                         w->colind, K, w->dX, w->frhs, w->cmask, invd, r, z, pp,
+                                                         w->colind, K, w->dX, w->frhs, w->cmask, invd, r, zj, pp,
                                                          w->part), ++g_launches;
   else
     k_pcg_init<KT, VT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr,
-                                                          w->colind, K, w->dX, w->frhs, w->cmask, invd, r, z, pp,
+                                                          w->colind, K, w->dX, w->frhs, w->cmask, invd, r, zj, pp,
                                                           w->part), ++g_launches;
+  if (amg) {
+    // done[] is reset by the stage-0 reduction below; the V-cycle must see every selected system
+    UA_CUDA_TRY(cudaMemsetAsync(w->done, 0, w->nsys * sizeof(int), m->stream));
+    view.pcopy = pp;
+    int rc = amg_vcycle(m, fp32, view, &g_launches);
+    if (rc) return rc;
+    view.pcopy = nullptr;
+  }
   k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(0, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                         w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
@@ -811,7 +841,11 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out) {
       k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                             w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
       k_pcg_update1<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->sysv,
-                                                       w->nsys, w->dX, r, z, pp, q, invd, w->part), ++g_launches;
+                                                       w->nsys, w->dX, r, zj, pp, q, invd, w->part), ++g_launches;
+      if (amg) {
+        int rc = amg_vcycle(m, fp32, view, &g_launches);
+        if (rc) return rc;
+      }
       k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                             w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
       k_pcg_update2<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys,
@@ -837,10 +871,18 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out) {
 
 // Solve [K L';L 0][dX;dl] = [frhs;grhs] for the selected systems (sel set on device,
 // its_out[s] != 0 marks selected on input).
-static int linear_solve(ua_mesh* m, const ua_params* p, std::vector<int>& its_out) {
+static int linear_solve(ua_mesh* m, const ua_params* p, std::vector<int>& its_out, const double* eta) {
   Work* w = m->work;
-  if (p->precision == UA_PREC_MIXED) return pcg_t<float, float>(m, p, w->Kf, its_out.data());
-  return pcg_t<double, double>(m, p, w->Kd, its_out.data());
+  if (p->precision == UA_PREC_MIXED) return pcg_t<float, float>(m, p, w->Kf, its_out.data(), eta);
+  return pcg_t<double, double>(m, p, w->Kd, its_out.data(), eta);
+}
+
+// Inner tolerance of Newton iteration with cost rForce: the forcing term
+// eta = 0.1*sqrt(rForce) (relative residual ~ ||[f;g]||/||fext0||), clamped to
+// [krylov_rtol, 1e-2]; krylov_rtol itself when adaptive tolerances are off.
+static double forcing_term(const ua_params* p, double rForce) {
+  if (!p->krylov_adaptive || !(rForce == rForce)) return p->krylov_rtol;
+  return std::min(1e-2, std::max(p->krylov_rtol, 0.1 * std::sqrt(std::max(rForce, 0.0))));
 }
 
 // uvResidualsCriteria.m:1-23
@@ -957,7 +999,9 @@ static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_rep
     t_asm += t1 - t0;
     // linear solve (:242-257)
     for (int s = 0; s < nsys; ++s) its[s] = sel[s];
-    if ((rc = linear_solve(m, p, its))) return rc;
+    std::vector<double> eta(nsys);
+    for (int s = 0; s < nsys; ++s) eta[s] = forcing_term(p, st[s].rForce);
+    if ((rc = linear_solve(m, p, its, eta.data()))) return rc;
     double t2 = now_ms();
     t_sol += t2 - t1;
     for (int s = 0; s < nsys; ++s) if (sel[s]) st[s].kits = its[s];
@@ -1245,11 +1289,14 @@ __global__ void k_bicg_reduce(int stage, const int* sys_rb_off, int nrb, const i
 
 // (s.t) partials: the spmv kernel gives a.y with a = s
 template <typename KT>
-static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out) {
+static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, const double* eta = nullptr) {
   Work* w = m->work;
   const int N = m->ndof_total;
   const int lpr = 16;
-  for (int s = 0; s < w->nsys; ++s) w->h_sysv[s] = p->krylov_rtol * p->krylov_rtol;
+  for (int s = 0; s < w->nsys; ++s) {
+    const double e = eta ? eta[s] : p->krylov_rtol;
+    w->h_sysv[s] = e * e;
+  }
   UA_CUDA_TRY(cudaMemcpyAsync(w->sysv + SV_TOL2 * w->nsys, w->h_sysv, w->nsys * sizeof(double),
                               cudaMemcpyHostToDevice, m->stream));
   double *r = (double*)w->kr, *rhat = (double*)w->krh, *pp = (double*)w->kp, *phat = (double*)w->kz;
@@ -1450,7 +1497,9 @@ static int newton_run_uvh(ua_mesh* m, const ua_params* p, std::vector<ua_newton_
     double t1 = now_ms();
     t_asm += t1 - t0;
     for (int s = 0; s < nsys; ++s) its[s] = sel[s];
-    if ((rc = bicgstab_t<double>(m, p, w->Kd, its.data()))) return rc;  // :136
+    std::vector<double> eta(nsys);
+    for (int s = 0; s < nsys; ++s) eta[s] = forcing_term(p, st[s].rForce == INFINITY ? 1.0 : st[s].rForce);
+    if ((rc = bicgstab_t<double>(m, p, w->Kd, its.data(), eta.data()))) return rc;  // :136
     t_sol += now_ms() - t1;
     for (int s = 0; s < nsys; ++s) if (sel[s]) st[s].kits = its[s];
     // r0 = func(0), r1 = func(1) (:155-156)
@@ -1574,7 +1623,8 @@ extern "C" void ua_params_default(ua_params* p) {
   std::memcpy(p->uvhAcceptableWorkAndForceTolerances, a1, sizeof a1);
   std::memcpy(p->uvhAcceptableWorkOrForceTolerances, a2, sizeof a2);
   p->krylov_rtol = 1e-12; p->krylov_maxit = 20000; p->precision = UA_PREC_FP64;
-  p->patch_nodes = 0; p->verbose = 0;
+  p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1;
+  p->krylov_precond = UA_PC_JACOBI;
 }
 
 extern "C" int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs, int32_t mode,
@@ -1776,6 +1826,8 @@ extern "C" void ua_mesh_destroy(ua_mesh* m) {
     if (w->h_gamma) cudaFreeHost(w->h_gamma);
     delete w;
   }
+  amg_free(m->amg);
+  m->amg = nullptr;
   dev_free_all(m);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
@@ -1884,6 +1936,7 @@ extern "C" int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const 
     ua_params_default(&p);
     p.krylov_rtol = rtol > 0 ? rtol : 1e-12;
     p.krylov_maxit = maxit > 0 ? maxit : 10 * n + 100;
+    p.krylov_precond = UA_PC_JACOBI;  // a bare matrix has no mesh to aggregate
     std::vector<int> kits(1, 1);
     rc = pcg_t<double, double>(&tmp, &p, w->Kd, kits.data());
     if (rc == UA_OK) {
@@ -2099,6 +2152,7 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
     ua_params_default(&p);
     p.krylov_rtol = rtol > 0 ? rtol : 1e-12;
     p.krylov_maxit = maxit > 0 ? maxit : 10 * n + 100;
+    p.krylov_precond = UA_PC_JACOBI;  // a bare matrix has no mesh to aggregate (and no allocation here)
     int kits[1] = {1};
     rc = pcg_t<double, double>(&view, &p, w.Kd, kits);
     if (rc == UA_OK) {

@@ -25,6 +25,8 @@ UA_ERR_NO_DEVICE = -9
 
 UA_PREC_FP64 = 0
 UA_PREC_MIXED = 1
+UA_PC_JACOBI = 0
+UA_PC_AMG = 1
 UA_ASM_R = 0
 UA_ASM_RK = 1
 UA_ASM_ZERO_R = 2
@@ -70,6 +72,7 @@ class ua_params(C.Structure):
         ("uvhAcceptableWorkOrForceTolerances", C.c_double * 2),
         ("krylov_rtol", C.c_double), ("krylov_maxit", C.c_int32), ("precision", C.c_int32),
         ("patch_nodes", C.c_int32), ("verbose", C.c_int32), ("profile", C.c_int32),
+        ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32),
     ]
 
 

@@ -73,6 +73,8 @@ class CtrlVar:
     patch_nodes: int = 0
     verbose: int = 0
     profile: int = 0
+    krylov_adaptive: int = 1
+    krylov_precond: int = L.UA_PC_JACOBI
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
