@@ -1,26 +1,36 @@
-"""Benchmark: uv Newton solves/s of the SSA (SSTREAM) diagnostic solve on B200.
+"""Benchmark: uv Newton solves/s of the SSA (SSTREAM) diagnostic solve on B200,
+mixed precision vs plain FP64, batched and served.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (one "step" = one complete uv Newton solve from u=v=0 to rForce<1e-20):
-the ice-stream/ice-shelf rectangle of 100 km x 50 km, 141x71 vertices,
-19,600 P1 elements (seeded synthetic fields: bed, thickness with bumps,
-smoothed Glen A and Weertman C, n=m=3; u=v=0 at x=0, free-slip sides,
-calving front).  Inputs are ~4 MB, far below the 126 MB L2, so a 512 MB
-buffer is written between timed steps to flush L2.
+Headline workload (one "step" = one batched uv Newton solve of 256 meshes):
+256 independent ice-stream/ice-shelf problems on 100 km x 50 km rectangles,
+P1 triangles, sizes log-uniform in 2k-200k elements (10.56M elements, 5.35M
+nodes in total, seeded synthetic fields: bed, thickness with bumps, smoothed
+Glen A and Weertman C, n=m=3; u=v=0 at x=0, free-slip sides, calving front),
+each solved from u=v=0 to rForce<1e-20.  The inputs (~0.5 GB) exceed the
+126 MB L2; a 512 MB buffer is also written between timed steps.
 
-Reported: ``value`` = solves/s of the mixed-precision form (FP32 tangents and
-PCG, FP64 residual/line search/update) with inputs resident in HBM;
-``plain_fp64`` = the same for the all-FP64 form; ``e2e`` = the mixed form
-through the public C-ABI with host buffers (host->device copies and the
-device->host read of the solution inside the timed region).  Errors of each
-form against the FP64 result are reported; the CPU baseline is the numpy
-restatement of the reference algorithm (oracle/ua_ref.py).
+Reported:
+  value         solves/s of the batched mixed-precision form (FP32 tangents
+                and PCG, FP64 residual/line search/update), inputs resident in HBM
+  plain_fp64    the plain form: one mesh at a time, all FP64, on a size-stratified
+                sample of 64 of the 256 meshes
+  batched_fp64  the batched form in FP64
+  e2e           the batched mixed form through the public API with host arrays
+                (host->device copies and the device->host read of every solution
+                inside the timed region)
+  serving       the served form: Poisson arrivals (200 req/s) over 16 resident
+                templates of 5k-500k elements, lognormal C perturbations, warm
+                starts; p50/p99 latency and solves/s
+  roofline      the dominant kernel by measured device time (CUDA events)
+  cpu_baseline  the numpy restatement of the reference (oracle/ua_ref.py) on a
+                bounded sample, one core
 
-Multi-GPU: independent replicas (the diagnostic solve of one mesh does not
-shard; whole meshes are independent work units), one process per GPU, time
-= max over ranks.  ``--impl reference`` times the CPU restatement on the
-host cores (a process pool, one solve per worker per step).
+Multi-GPU: independent replicas (whole meshes are the independent units; one
+solve of one mesh does not shard), one process per GPU, time = max over ranks.
+``--impl reference`` times the CPU restatement on the host cores (a process
+pool, one mesh per worker per step, size-stratified over the batch).
 """
 from __future__ import annotations
 
@@ -35,28 +45,23 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-NX, NY, SEED = 141, 71, 0
-WORKLOAD = (f"uv diagnostic Newton solve (SSTREAM2dNR2), ice stream/shelf 100x50 km, {NX}x{NY} vertices, "
-            f"{2 * (NX - 1) * (NY - 1)} P1 elements, 10011 nodes, seed {SEED}, rForce<1e-20")
-METRIC = "uv Newton solves/s (mixed FP32/FP64, <=1e-8 rel err vs FP64)"
+BATCH = 256
+METRIC = "uv Newton solves/s (batched, mixed FP32/FP64, <=1e-8 rel err vs FP64)"
 
 
-MESH = (NX, NY)
-
-
-def _problem():
-    from uasource_b200 import synth
-    return synth.ice_stream_shelf(MESH[0], MESH[1], nod=3, seed=SEED)
+def _workload(count):
+    return (f"batched uv diagnostic Newton solves (SSTREAM2dNR2): {count} independent ice stream/shelf meshes "
+            f"100x50 km, P1, log-uniform 2k-200k elements (seed 12345), u=v=0 start, rForce<1e-20")
 
 
 # ----------------------------------------------------------------------------- CPU reference arm
 
-def _ref_solve_once(seed):
-    """One full oracle solve (child process)."""
-    import numpy as np  # noqa: F401
+def _oracle_solve(k, count):
+    """One full oracle solve of batch problem k (child process); returns (seconds, converged, Nele)."""
     sys.path.insert(0, ROOT)
     from oracle import ua_ref as R
-    P = _problem()
+    from uasource_b200 import synth
+    P = synth.batch_problem(k, count)
     mua = R.create_mua(P.coordinates, P.connectivity)
     p = R.Params()
     p.set_force_tolerance(1e-20)
@@ -65,19 +70,23 @@ def _ref_solve_once(seed):
                 vbFixedValue=P.vbFixedValue)
     t = time.perf_counter()
     res = R.uv(p, mua, bcs, F)
-    return time.perf_counter() - t, bool(res.converged)
+    return time.perf_counter() - t, bool(res.converged), int(P.Nele)
 
 
-def _cpu_baseline_single(max_seconds=25.0):
-    """Oracle port on one core: solves until ~max_seconds of CPU work."""
-    ts = []
-    t0 = time.perf_counter()
-    while time.perf_counter() - t0 < max_seconds * 0.5 or not ts:
-        dt, ok = _ref_solve_once(SEED)
-        ts.append(dt)
-        if time.perf_counter() - t0 > max_seconds:
-            break
-    return len(ts) / sum(ts), len(ts)
+def _oracle_solve_args(a):
+    return _oracle_solve(*a)
+
+
+def _size_ranks(count):
+    from uasource_b200 import synth
+    import numpy as np
+    return np.argsort(synth.batch_sizes(count), kind="stable")
+
+
+def _stratified(count, n, offset):
+    """n batch indices, one per size stratum (strata of equal count), at a fractional offset."""
+    order = _size_ranks(count)
+    return [int(order[min(count - 1, int((j + offset) * count / n))]) for j in range(n)]
 
 
 def run_reference(args):
@@ -87,31 +96,64 @@ def run_reference(args):
     import multiprocessing as mp
     for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[v] = "1"
+    count = args.batch
     cores = os.cpu_count() or 1
     workers = max(1, min(cores, 32))
+    order = _size_ranks(count)
     ctx = mp.get_context("spawn")
+    res = []
     with ctx.Pool(workers) as pool:
-        for _ in range(args.warmup):
-            pool.map(_ref_solve_once, [SEED] * workers)
+        for _ in range(args.warmup):  # imports and page cache: the smallest mesh on every worker
+            pool.map(_oracle_solve_args, [(int(order[0]), count)] * workers)
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            res = pool.map(_ref_solve_once, [SEED] * workers)
+        for k in range(args.steps):
+            idx = _stratified(count, workers, (0.5 + 0.618034 * k) % 1.0)
+            res += pool.map(_oracle_solve_args, [(i, count) for i in idx])
         el = time.perf_counter() - t0
-    solves = args.steps * workers
+    solves = len(res)
     value = solves / el
+    sizes = sorted(r[2] for r in res)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "l2": "n/a (CPU)"},
+        "config": {"workload": _workload(count), "l2": "n/a (CPU)"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "port",
-                         "sample": f"{workers} concurrent oracle solves per step (numpy/scipy restatement, "
-                                   f"one process per core)"},
+                         "sample": f"per step {workers} meshes of the batch, one per size stratum "
+                                   f"({sizes[0]}-{sizes[-1]} elements over the run), one oracle "
+                                   f"(numpy/scipy restatement) process per core"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "converged": all(ok for _, ok in res),
+        "converged": all(r[1] for r in res),
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _cpu_baseline_single(count, max_seconds):
+    """Oracle on one core over a size-stratified sample until ~max_seconds of work.
+    Returns the sample's solves/s and an extrapolation to the whole batch
+    (per-solve time fitted as a*Nele^b over the sample, summed over all sizes)."""
+    import numpy as np
+    from uasource_b200 import synth
+    order = _size_ranks(count)
+    picks = [int(order[int(q * (count - 1))]) for q in (0.0, 0.125, 0.25, 0.375, 0.5, 0.625, 0.75)]
+    ts, ns = [], []
+    t0 = time.perf_counter()
+    for k in picks:
+        dt, ok, ne = _oracle_solve(k, count)
+        ts.append(dt); ns.append(ne)
+        if time.perf_counter() - t0 > max_seconds:
+            break
+    out = {"value": len(ts) / sum(ts), "unit": "solves/s", "cores": 1, "kind": "port",
+           "sample": f"{len(ts)} full oracle solves of batch meshes at size quantiles 0-{12.5 * (len(ts) - 1):.1f}% "
+                     f"({min(ns)}-{max(ns)} elements), single process"}
+    if len(ts) >= 2:
+        b, loga = np.polyfit(np.log(ns), np.log(ts), 1)
+        sizes = synth.batch_sizes(count)
+        t_all = float(np.sum(np.exp(loga) * sizes ** b))
+        out["extrapolated_batch_solves_per_s"] = count / t_all
+        out["extrapolation"] = f"t = {np.exp(loga):.3g}*Nele^{b:.3f} s fitted on the sample, summed over {count} sizes"
+    return out
 
 
 # ----------------------------------------------------------------------------- GPU arm
@@ -162,8 +204,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def _flush_l2(buf):
-    buf.add_(1.0)
+NAMES = ("h", "S", "B", "rho", "AGlen", "n", "C", "m")
 
 
 def run_ours(args):
@@ -171,7 +212,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     import uasource_b200 as ua
-    from uasource_b200 import lib as L
+    from uasource_b200 import lib as L, synth
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -193,160 +234,202 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return t.item()
 
-    P = _problem()
-    mua = ua.CreateMUA(P.coordinates, P.connectivity, device=local)
-    bcs = ua.BCs.from_problem(P)
-    names = ("h", "S", "B", "rho", "AGlen", "n", "C", "m")
-    dev_in = {k: torch.tensor(getattr(P, k), dtype=torch.float64, device=dev) for k in names}
-    ub = torch.zeros(P.Nnodes, dtype=torch.float64, device=dev)
+    count = args.batch
+    probs = synth.batch_problems(count)
+    node_off = np.concatenate([[0], np.cumsum([P.Nnodes for P in probs])])
+    Nn_tot = int(node_off[-1])
+    mua = ua.CreateMUABatch([(P.coordinates, P.connectivity) for P in probs], device=local)
+    bcss = [ua.BCs.from_problem(P) for P in probs]
+    # resident inputs: one concatenated float64 tensor per field, system-major
+    dev_in = {k: torch.tensor(np.concatenate([getattr(P, k) for P in probs]), dtype=torch.float64, device=dev)
+              for k in NAMES}
+    ub = torch.zeros(Nn_tot, dtype=torch.float64, device=dev)
     vb = torch.zeros_like(ub)
-    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float64, device=dev)  # 512 MB > L2
-    ctrl64 = ua.CtrlVar(precision=L.UA_PREC_FP64, krylov_rtol=1e-12).set_force_tolerance(1e-20)
-    ctrlmx = ua.CtrlVar(precision=L.UA_PREC_MIXED, krylov_rtol=1e-6).set_force_tolerance(1e-20)
-    if args.newton_its:
-        ctrl64.NRitmax = ctrlmx.NRitmax = args.newton_its
-    if args.krylov_maxit:
-        ctrl64.krylov_maxit = ctrlmx.krylov_maxit = args.krylov_maxit
 
-    def solve_resident(ctrl):
+    def ptrs(s):
+        o = 8 * int(node_off[s])
+        d = {k: v.data_ptr() + o for k, v in dev_in.items()}
+        d["ub"] = ub.data_ptr() + o
+        d["vb"] = vb.data_ptr() + o
+        return d
+
+    F_devs = [ptrs(s) for s in range(count)]
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float64, device=dev)  # 512 MB > L2
+
+    def ctrl_of(prec, **kw):
+        c = ua.CtrlVar(precision=prec, krylov_rtol=1e-12 if prec == L.UA_PREC_FP64 else 1e-6, **kw)
+        return c.set_force_tolerance(1e-20)
+
+    ctrlmx = ctrl_of(L.UA_PREC_MIXED)
+    ctrl64 = ctrl_of(L.UA_PREC_FP64)
+
+    def solve_batch(ctrl):
         ub.zero_(); vb.zero_()
         torch.cuda.synchronize()
-        ptrs = {k: v.data_ptr() for k, v in dev_in.items()}
-        ptrs["ub"] = ub.data_ptr(); ptrs["vb"] = vb.data_ptr()
-        _, info = ua.uv_resident(ctrl, mua, bcs, ptrs, rhow=P.rhow, g=P.g)
-        return info
+        return ua.uv_batch_resident(ctrl, mua, F_devs, bcss, rhow=probs[0].rhow, g=probs[0].g)
 
-    def timed(ctrl, steps, warmup, sampler=None):
+    def timed(fn, steps, warmup, sampler=None):
         for _ in range(warmup):
-            solve_resident(ctrl)
+            fn()
         barrier()
         torch.cuda.synchronize()
         if sampler:
             sampler.start()
-        per, lat, launches, infos = [], [], 0, []
+        per, out = [], []
         e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
         for _ in range(steps):
-            _flush_l2(flush)
+            flush.add_(1.0)
             torch.cuda.synchronize()
             e0.record()
-            info = solve_resident(ctrl)
+            r = fn()
             e1.record()
             torch.cuda.synchronize()
             per.append(e0.elapsed_time(e1))
-            lat.append(info.device_ms)
-            launches += info.gpu_launches
-            infos.append(info)
+            out.append(r)
         clocks = sampler.stop() if sampler else None
         barrier()
-        return per, lat, launches, infos, clocks
+        return per, out, clocks
 
-    if args.legs == "mixed":  # profiling runs: the timed mixed-precision solves only
-        timed(ctrlmx, args.steps, args.warmup)
+    if args.legs == "mixed":  # profiling runs: the timed batched mixed-precision solves only
+        timed(lambda: solve_batch(ctrlmx), args.steps, args.warmup)
         mua.close()
         if world > 1:
             dist.destroy_process_group()
         return 0
-    # reference solution of the plain FP64 form (for the error report)
-    info64 = solve_resident(ctrl64)
-    u64 = torch.cat([ub, vb]).cpu().numpy()
+
+    # FP64 batched solution: the reference for the error report
+    infos64 = solve_batch(ctrl64)
+    u64 = [torch.cat([ub[node_off[s]:node_off[s + 1]], vb[node_off[s]:node_off[s + 1]]]).cpu().numpy()
+           for s in range(count)]
+
+    # headline: batched mixed precision, resident inputs
     sampler = ClockSampler(local)
-    per_mx, lat_mx, launches_mx, infos_mx, clocks = timed(ctrlmx, args.steps, args.warmup, sampler)
-    u_mx = torch.cat([ub, vb]).cpu().numpy()
-    per_64, lat_64, launches_64, infos_64, _ = timed(ctrl64, args.steps, max(1, args.warmup // 2))
-    err_mx = float(np.linalg.norm(u_mx - u64) / np.linalg.norm(u64))
+    per_mx, outs_mx, clocks = timed(lambda: solve_batch(ctrlmx), args.steps, args.warmup, sampler)
+    infos_mx = outs_mx[-1]
+    errs = []
+    for s in range(count):
+        u = torch.cat([ub[node_off[s]:node_off[s + 1]], vb[node_off[s]:node_off[s + 1]]]).cpu().numpy()
+        errs.append(float(np.linalg.norm(u - u64[s]) / np.linalg.norm(u64[s])))
+    launches_mx = sum(o[0].gpu_launches for o in outs_mx)
 
-    # kernel timings (separate profiled solves; CUDA events on the library's stream)
-    prof = solve_resident(ua.CtrlVar(precision=L.UA_PREC_MIXED, krylov_rtol=1e-6, profile=1)
-                          .set_force_tolerance(1e-20))
-    prof64 = solve_resident(ua.CtrlVar(precision=L.UA_PREC_FP64, krylov_rtol=1e-12, profile=1)
-                            .set_force_tolerance(1e-20))
+    # batched FP64
+    per_b64, outs_b64, _ = timed(lambda: solve_batch(ctrl64), max(1, args.steps // 2), 1)
 
-    # e2e: the public API with host buffers (pinned), copies inside the timed region
-    pin = {k: torch.tensor(getattr(P, k), dtype=torch.float64).pin_memory() for k in names}
-    pin_u = torch.zeros(P.Nnodes, dtype=torch.float64).pin_memory()
-    Fh = ua.Fields(**{k: pin[k].numpy() for k in names}, ub=pin_u.numpy(), vb=pin_u.numpy(), rhow=P.rhow, g=P.g)
-    for _ in range(max(1, args.warmup // 2)):
-        ua.uv(ctrlmx, mua, bcs, Fh)
-    barrier(); torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
-    e2e_ms = []
-    for _ in range(args.steps):
-        _flush_l2(flush); torch.cuda.synchronize()
-        e0.record()
-        Fo, _, _, _, info_e = ua.uv(ctrlmx, mua, bcs, Fh)
-        e1.record(); torch.cuda.synchronize()
-        e2e_ms.append(e0.elapsed_time(e1))
-    barrier()
-    Nn = P.Nnodes
-    h2d = 8 * Nn * (len(names) + 2) + 12 * (len(bcs.ubFixedNode) + len(bcs.vbFixedNode))
-    d2h = 8 * 2 * Nn + 8 * (len(bcs.ubFixedNode) + len(bcs.vbFixedNode))
+    # plain FP64: one mesh at a time on a size-stratified sample
+    sample = _stratified(count, min(64, count), 0.5)
+    singles = [(s, ua.CreateMUA(probs[s].coordinates, probs[s].connectivity, device=local)) for s in sample]
+
+    def plain_pass():
+        its = 0
+        for s, m1 in singles:
+            ub[node_off[s]:node_off[s + 1]] = 0; vb[node_off[s]:node_off[s + 1]] = 0
+            _, info = ua.uv_resident(ctrl64, m1, bcss[s], F_devs[s], rhow=probs[s].rhow, g=probs[s].g)
+            its += info.krylov_its_total
+        return its
+
+    per_plain, _, _ = timed(plain_pass, 1, 1)
+    for _, m1 in singles:
+        m1.close()
+
+    # e2e: public API with host arrays in pinned memory
+    pin = {k: torch.tensor(np.concatenate([getattr(P, k) for P in probs]), dtype=torch.float64).pin_memory()
+           for k in NAMES}
+    pin_u = torch.zeros(Nn_tot, dtype=torch.float64).pin_memory()
+    Fh = []
+    for s, P in enumerate(probs):
+        a, b = int(node_off[s]), int(node_off[s + 1])
+        Fh.append(ua.Fields(**{k: pin[k].numpy()[a:b] for k in NAMES}, ub=pin_u.numpy()[a:b],
+                            vb=pin_u.numpy()[a:b], rhow=P.rhow, g=P.g))
+    per_e2e, _, _ = timed(lambda: ua.uv_batch(ctrlmx, mua, Fh, bcss), args.steps, 1)
+    ncon = sum(len(b.ubFixedNode) + len(b.vbFixedNode) for b in bcss)
+    h2d = 8 * Nn_tot * (len(NAMES) + 2) + 12 * ncon
+    d2h = 8 * 2 * Nn_tot
+
+    # per-kernel device time (a profiled batched mixed solve: CUDA events on the library's stream)
+    prof = solve_batch(ctrl_of(L.UA_PREC_MIXED, profile=1))[0].kernels
+
+    # served form
+    serving = None
+    if not args.skip_serve:
+        serving = _serve_leg(args, ua, L, synth, np, local)
 
     t_mx = max_over_ranks(sum(per_mx))
-    t_64 = max_over_ranks(sum(per_64))
-    t_e2e = max_over_ranks(sum(e2e_ms))
-    value = world * args.steps / (t_mx / 1000)
-    value64 = world * args.steps / (t_64 / 1000)
-    e2e_value = world * args.steps / (t_e2e / 1000)
+    t_b64 = max_over_ranks(sum(per_b64))
+    t_plain = max_over_ranks(sum(per_plain))
+    t_e2e = max_over_ranks(sum(per_e2e))
+    value = world * count * args.steps / (t_mx / 1000)
+    value_b64 = world * count * len(per_b64) / (t_b64 / 1000)
+    value_plain = world * len(sample) / (t_plain / 1000)
+    e2e_value = world * count * args.steps / (t_e2e / 1000)
 
-    # roofline of the dominant kernel class (by measured device time)
-    nnz = int(mua.pattern()[1].size)
-    Ne = P.Nele
-    rows = 2 * Nn
+    # roofline of the dominant kernel class (by measured device time); algorithmic bytes per launch
+    # (whole batch, FP32 values and vectors, 4-byte indices)
+    nnz = sum(mua.nnz(s) for s in range(count))
+    Ne = sum(P.Nele for P in probs)
+    rows = 2 * Nn_tot
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    k = prof.kernels
     cand = {
         "uv_patch_kernel<3,K,float> (tangent+residual assembly)":
-            (k["asmK_ms"], k["asmK_n"], 12 * Ne + 16 * Nn + 80 * Nn + 4 * nnz + 8 * rows),
+            (prof["asmK_ms"], prof["asmK_n"], 12 * Ne + 16 * Nn_tot + 80 * Nn_tot + 4 * nnz + 8 * rows),
         "uv_patch_kernel<3,R> (residual-only assembly)":
-            (k["asmR_ms"], k["asmR_n"], 12 * Ne + 16 * Nn + 80 * Nn + 8 * rows),
-        "k_pcg_spmv<float,float> (PCG SpMV + p.q)":
-            (k["spmv_ms"], k["spmv_n"], 8 * nnz + 4 * (rows + 1) + 4 * rows + 4 * rows + rows),
+            (prof["asmR_ms"], prof["asmR_n"], 12 * Ne + 16 * Nn_tot + 80 * Nn_tot + 8 * rows),
+        "k_pcg_spmv<float,float,8> (PCG SpMV + p.q)":
+            (prof["spmv_ms"], prof["spmv_n"], 8 * nnz + 4 * (rows + 1) + 4 * rows + 4 * rows + rows),
+        "k_amg_restrict<float,float> (fine residual + aggregation)":
+            (prof["amgR_ms"], prof["amgR_n"], 8 * nnz + 4 * (rows + 1) + 4 * rows + 4 * rows + 4 * rows + 4 * rows + rows),
+        "k_amg_prolong_smooth<float,float,8> (coarse correction + l1-Jacobi + r.z)":
+            (prof["amgP_ms"], prof["amgP_n"], 8 * nnz + 4 * (rows + 1) + 4 * rows * 6 + rows),
     }
     dom = max(cand, key=lambda c: cand[c][0])
     ms, n, alg = cand[dom]
     avg_ms = ms / max(n, 1)
     achieved = alg / (avg_ms / 1000) / 1e9 if n else 0.0
+    total_k = sum(v[0] for v in cand.values())
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "traffic": None,
             "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms, "launches": n,
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if "hbm_gbs" in peaks else "fallback 6650",
-            "kernel_share": {c: v[0] / max(sum(x[0] for x in cand.values()), 1e-12) for c, v in cand.items()}}
+            "peak_source": ("MEASURED_PEAKS.json hbm_gbs (burst copy), of measured" if "hbm_gbs" in peaks
+                            else "fallback 6650 GB/s, of fallback"),
+            "kernel_share_of_timed_classes": {c: v[0] / max(total_k, 1e-12) for c, v in cand.items()}}
 
     cpu = None
-    if rank == 0 and not args.skip_cpu:
-        v, nsamp = _cpu_baseline_single(args.cpu_seconds)
-        cpu = {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
-               "sample": f"{nsamp} full oracle solve(s) of the same workload, single process"}
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = _cpu_baseline_single(count, args.cpu_seconds)
 
     if rank == 0:
-        lat_sorted = sorted(lat_mx)
-        p99 = lat_sorted[min(len(lat_sorted) - 1, int(0.99 * len(lat_sorted)))]
+        lat = sorted(per_mx)
+        its = [i.iterations for i in infos_mx]
+        kits = [i.krylov_its_total for i in infos_mx]
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_mx / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "l2": "flushed (512 MB write) between timed steps",
-                       "parallelism": f"replicas x{world}", "precision": "mixed", "krylov": "Jacobi-PCG",
-                       "newton_iterations": infos_mx[-1].iterations,
-                       "pcg_iterations": infos_mx[-1].krylov_its_total},
-            "p50_ms": statistics.median(lat_mx), "p99_ms": p99,
-            "rel_err_vs_fp64": err_mx,
-            "plain_fp64": {"value": value64, "unit": "solves/s", "ms_per_step": t_64 / args.steps,
-                           "newton_iterations": infos_64[-1].iterations,
-                           "pcg_iterations": infos_64[-1].krylov_its_total,
-                           "p99_ms": sorted(lat_64)[min(len(lat_64) - 1, int(0.99 * len(lat_64)))]},
-            "mixed_over_plain": value / value64,
+            "config": {"workload": _workload(count), "systems_per_step": count, "elements": int(Ne),
+                       "nodes": Nn_tot, "nnz": int(nnz),
+                       "l2": "inputs 0.5 GB > L2; 512 MB buffer written between timed steps",
+                       "parallelism": f"replicas x{world}", "precision": "mixed",
+                       "krylov": "PCG, aggregation AMG V(1,1), adaptive forcing, CUDA-graph chunks",
+                       "newton_iterations_mean": float(np.mean(its)), "newton_iterations_max": int(max(its)),
+                       "pcg_iterations_mean": float(np.mean(kits)), "converged": int(sum(i.converged for i in infos_mx))},
+            "batch_latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "rel_err_vs_fp64": {"max": max(errs), "median": statistics.median(errs)},
+            "plain_fp64": {"value": value_plain, "unit": "solves/s", "form": "one mesh at a time, all FP64",
+                           "sample": f"{len(sample)} meshes, one per size stratum of the batch",
+                           "ms_per_pass": t_plain},
+            "batched_fp64": {"value": value_b64, "unit": "solves/s", "ms_per_step": t_b64 / len(per_b64),
+                             "converged": int(sum(i.converged for i in infos64))},
+            "mixed_batched_over_plain_fp64": value / value_plain,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "serving": serving,
             "roofline": roof,
-            "kernels_fp64": prof64.kernels,
             "cpu_baseline": cpu,
             "clocks": clocks,
-            "gpu_launches": launches_mx,
+            "gpu_launches": int(launches_mx),
         }
         print(json.dumps(line), flush=True)
     mua.close()
@@ -355,23 +438,70 @@ def run_ours(args):
     return 0
 
 
+def _serve_leg(args, ua, L, synth, np, device):
+    """Served form: Poisson arrivals over resident templates; p50/p99 and solves/s,
+    with a sample of results checked against plain FP64 solves."""
+    from uasource_b200.serve import Request, SsaServer, perturbed_C, poisson_arrivals
+    tpl = synth.serve_templates(args.serve_templates)
+    ctrl = ua.CtrlVar(precision=L.UA_PREC_MIXED, krylov_rtol=1e-6).set_force_tolerance(1e-20)
+    ctrl64 = ua.CtrlVar().set_force_tolerance(1e-20)
+    # warm starts: each template's own solution
+    base = ua.CreateMUABatch([(P.coordinates, P.connectivity) for P in tpl], device=device)
+    warm = ua.uv_batch(ctrl, base, [ua.Fields.from_problem(P) for P in tpl], [ua.BCs.from_problem(P) for P in tpl])
+    base.close()
+    srv = SsaServer(tpl, ctrl, device=device)
+    rng = np.random.default_rng(2024)
+
+    def requests(n, t0):
+        arr = poisson_arrivals(n, args.serve_rate, rng)
+        out = []
+        for i in range(n):
+            k = int(rng.integers(len(tpl)))
+            out.append(Request(rid=i, template=k, C=perturbed_C(tpl[k], rng), ub0=warm[k][0], vb0=warm[k][1],
+                               arrival=t0 + arr[i]))
+        return out
+
+    srv.run(requests(min(8, args.serve_requests), 0.0), realtime=False)  # warm-up (graphs, hierarchies)
+    reqs = requests(args.serve_requests, 0.0)
+    st = srv.run(reqs, realtime=True)
+    srv.close()
+    # accuracy: a sample of requests against the plain FP64 form
+    errs = []
+    for r in reqs[:: max(1, len(reqs) // 6)]:
+        P = tpl[r.template]
+        m1 = ua.CreateMUA(P.coordinates, P.connectivity, device=device)
+        F = ua.Fields.from_problem(P)
+        F.C = r.C
+        F.ub = r.ub0.copy(); F.vb = r.vb0.copy()
+        Fo, _, _, _, _ = ua.uv(ctrl64, m1, ua.BCs.from_problem(P), F)
+        m1.close()
+        u64 = np.concatenate([Fo.ub, Fo.vb]); u = np.concatenate([r.ub, r.vb])
+        errs.append(float(np.linalg.norm(u - u64) / np.linalg.norm(u64)))
+    sizes = [P.Nele for P in tpl]
+    return {"workload": f"{len(tpl)} resident templates of {min(sizes)}-{max(sizes)} P1 elements, Poisson arrivals "
+                        f"{args.serve_rate:g} req/s, {len(reqs)} requests, lognormal C (sigma 0.3), warm starts",
+            "solves_per_s": st.solves_per_s, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+            "mean_queue_ms": st.mean_queue_ms, "slots": st.slots, "max_active": st.max_active,
+            "makespan_s": st.makespan_s, "converged": int(sum(bool(r.info.converged) for r in reqs)),
+            "rel_err_vs_fp64_max": max(errs) if errs else None, "checked": len(errs)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--skip-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-templates", type=int, default=16)
     # profiling-only options (ncu captures on bounded cases); the bench line uses the defaults
     ap.add_argument("--legs", default="all", choices=["all", "mixed"])
-    ap.add_argument("--mesh", default=None, help="NXxNY vertices instead of the workload mesh")
-    ap.add_argument("--newton-its", type=int, default=0)
-    ap.add_argument("--krylov-maxit", type=int, default=0)
+    ap.add_argument("--batch", type=int, default=BATCH, help="meshes per step (default 256)")
     args = ap.parse_args()
-    if args.mesh:
-        global MESH
-        MESH = tuple(int(v) for v in args.mesh.lower().split("x"))
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

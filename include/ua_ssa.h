@@ -160,6 +160,8 @@ typedef struct ua_newton_report {
     double device_ms;           /* CUDA-event time on the handle's stream, whole call */
     double kasmK_ms, kasmR_ms, kspmv_ms;     /* summed launch durations (profile=1) */
     int32_t kasmK_n, kasmR_n, kspmv_n;       /* launches timed */
+    double kamgR_ms, kamgP_ms;  /* fine-level AMG restriction / prolongation+smoothing (profile=1) */
+    int32_t kamgR_n, kamgP_n;
     int32_t gpu_launches;       /* kernels launched by the library during the call */
     int32_t n_iter_records;     /* entries filled in iters (<= iters_capacity) */
     int32_t iters_capacity;

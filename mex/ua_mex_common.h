@@ -97,6 +97,8 @@ static void ua_mex_params(const mxArray* C, ua_params* p) {
     /* the GPU form selected by a CtrlVar.UseGPU-style switch (0=FP64, 1=mixed) */
     p->precision = (int32_t)ua_mex_scalar(C, "GPUPrecision", p->precision);
     p->krylov_rtol = ua_mex_scalar(C, "GPUKrylovTol", p->krylov_rtol);
+    p->krylov_precond = (int32_t)ua_mex_scalar(C, "GPUPreconditioner", p->krylov_precond);
+    p->krylov_adaptive = (int32_t)ua_mex_scalar(C, "GPUKrylovAdaptive", p->krylov_adaptive);
 }
 
 /* MUA -> cached device mesh (rebuilt when coordinates/connectivity change). */

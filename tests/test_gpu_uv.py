@@ -270,3 +270,35 @@ def test_analytic_ice_stream_on_gpu(nod):
     assert info.converged
     err = np.max(np.abs(Fo.ub - u_exact)) / np.max(np.abs(u_exact))
     assert err < (3e-3 if nod == 3 else 6e-5)
+
+
+@pytest.mark.parametrize("nod", [3, 6])
+def test_amg_and_jacobi_preconditioners_agree(nod):
+    """The aggregation-AMG and point-Jacobi inner solves reach the same Newton solution;
+    AMG needs far fewer Krylov iterations."""
+    P = synth.ice_stream_shelf(61, 31, nod=nod, seed=3)
+    mua = ua.CreateMUA(P.coordinates, P.connectivity)
+    res = {}
+    for pc in (L.UA_PC_JACOBI, L.UA_PC_AMG):
+        ctrl = ua.CtrlVar(krylov_precond=pc).set_force_tolerance(1e-20)
+        Fo, _, _, _, info = ua.uv(ctrl, mua, ua.BCs.from_problem(P), ua.Fields.from_problem(P))
+        assert info.converged
+        res[pc] = (np.concatenate([Fo.ub, Fo.vb]), info.krylov_its_total)
+    uj, u_amg = res[L.UA_PC_JACOBI][0], res[L.UA_PC_AMG][0]
+    assert np.linalg.norm(u_amg - uj) <= U_TOL_FP64 * np.linalg.norm(uj)
+    assert res[L.UA_PC_AMG][1] * 3 < res[L.UA_PC_JACOBI][1]
+
+
+@pytest.mark.parametrize("precision,rtol", [(L.UA_PREC_FP64, 1e-12), (L.UA_PREC_MIXED, 1e-6)])
+def test_graph_replay_equals_direct_launches(precision, rtol):
+    """PCG chunks replayed from a captured CUDA graph give bit-identical results to the
+    same kernels launched one by one (profile=1 launches them directly)."""
+    P = synth.ice_stream_shelf(41, 21, seed=4)
+    mua = ua.CreateMUA(P.coordinates, P.connectivity)
+    out = []
+    for prof in (0, 1, 0):
+        ctrl = ua.CtrlVar(precision=precision, krylov_rtol=rtol, profile=prof).set_force_tolerance(1e-20)
+        Fo, _, _, _, info = ua.uv(ctrl, mua, ua.BCs.from_problem(P), ua.Fields.from_problem(P))
+        assert info.converged
+        out.append(np.concatenate([Fo.ub, Fo.vb]))
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])

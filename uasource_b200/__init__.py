@@ -5,6 +5,6 @@ include/ua_ssa.h; ``uasource_b200.ua`` mirrors the reference's MATLAB
 interface on top of it.
 """
 from .ua import (CtrlVar, Fields, BCs, HBCs, MUA, CreateMUA, CreateMUABatch, uvMatrixAssembly, uv, uv_batch,  # noqa: F401,E501
-                 uv_resident, uvhAssembly, uvh,
+                 uv_resident, uv_batch_resident, uvhAssembly, uvh,
                  solveKApeSymmetric, RunInfo)
 from .lib import UaError  # noqa: F401

@@ -504,6 +504,100 @@ __global__ void __launch_bounds__(256) k_amg_prolong_smooth(const int* rb_start,
   }
 }
 
+// Finest level, split form (coalesced row blocks instead of one thread per
+// aggregate).  Residual of the pre-smoothed vector: res = mask(b - A x).
+template <typename KT, typename VT, int LPR>
+__global__ void __launch_bounds__(256) k_amg_residual(const int* rb_start, const int* rb_sys, const int* sel,
+                                                      const int* done, const int* rowptr, const int* colind,
+                                                      const KT* A, const VT* b, const VT* x,
+                                                      const unsigned char* cmask, VT* res) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const int rs = rb_start[blk], re = rb_start[blk + 1];
+  const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+  for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
+    const int row = row0 + grp;
+    const bool valid = row < re;
+    double ax = 0;
+    if (valid)
+      for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) ax += (double)A[q] * (double)x[colind[q]];
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) ax += __shfl_down_sync(0xffffffffu, ax, o, LPR);
+    if (valid && lane == 0) res[row] = (VT)(cmask[row] ? 0.0 : (double)b[row] - ax);
+  }
+}
+
+// Aggregation of a fine vector: b(R) = sum over members (ascending) of res;
+// coarse pre-smoothing x = invd b unless lc is the system's coarsest level.
+template <typename VT>
+__global__ void k_amg_gather(int ncd, const int* dof_sys_c, const int* depth, int lc, const int* sel,
+                             const int* done, const int* mptr, const int* mlist, const VT* res, const VT* cinvd,
+                             VT* cb, VT* cx) {
+  const int R = blockIdx.x * blockDim.x + threadIdx.x;
+  if (R >= ncd) return;
+  const int s = dof_sys_c[R];
+  if (!sel[s] || done[s]) return;
+  double acc = 0;
+  for (int t = mptr[R]; t < mptr[R + 1]; ++t) acc += (double)res[mlist[t]];
+  cb[R] = (VT)acc;
+  if (depth[s] > lc) cx[R] = (VT)((double)cinvd[R] * acc);
+}
+
+// Coarse correction of the finest level: xp = mask(x + xc[cmap]).
+template <typename VT>
+__global__ void __launch_bounds__(256) k_amg_correct(const int* rb_start, const int* rb_sys, const int* sel,
+                                                     const int* done, const VT* x, const VT* xc, const int* cmap,
+                                                     const unsigned char* cmask, VT* xp) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x)
+    xp[i] = cmask[i] ? (VT)0 : (VT)((double)x[i] + (double)xc[cmap[i]]);
+}
+
+// Post-smoothing of the finest level: z = xp + invd (b - A xp) (0 on masked
+// rows), p = z when pcopy is set, block partials of b.z.
+template <typename KT, typename VT, int LPR>
+__global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const int* rb_sys, const int* sel,
+                                                    const int* done, const int* rowptr, const int* colind,
+                                                    const KT* A, const VT* b, const VT* xp, const VT* invd,
+                                                    const unsigned char* cmask, VT* z, VT* pcopy, double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double rz = 0;
+  if (sel[s] && !done[s]) {
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
+      const int row = row0 + grp;
+      const bool valid = row < re;
+      double ax = 0;
+      if (valid)
+        for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) ax += (double)A[q] * (double)xp[colind[q]];
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) ax += __shfl_down_sync(0xffffffffu, ax, o, LPR);
+      if (valid && lane == 0) {
+        const double v = cmask[row] ? 0.0 : (double)xp[row] + (double)invd[row] * ((double)b[row] - ax);
+        z[row] = (VT)v;
+        if (pcopy) pcopy[row] = (VT)v;
+        rz += (double)b[row] * v;
+      }
+    }
+  }
+  __shared__ double red[8];
+  double t = rz;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sum = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
+    part[blk] = sum;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
@@ -547,28 +641,58 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
   Amg* a = m->amg;
   cudaStream_t st = m->stream;
   const int nl = a->nlev;
-  for (int l = 0; l + 1 < nl; ++l) {  // down
+  const KT* K0 = (const KT*)v.K0;
+  const VT* r = (const VT*)v.r;
+  const VT* x0 = (const VT*)v.x0;
+  VT* tmp = (VT*)v.tmp;
+  // down, finest level: residual of the pre-smoothed vector, then aggregation
+  {
+    const AmgLevel& C = a->lev[1];
+    if (v.mark) v.mark(v.mark_ctx, 0, 0);
+    if (v.lpr == 16)
+      k_amg_residual<KT, VT, 16><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, v.rowptr0, v.colind0,
+                                                         K0, r, x0, v.cmask, tmp), ++*launches;
+    else
+      k_amg_residual<KT, VT, 8><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, v.rowptr0, v.colind0,
+                                                        K0, r, x0, v.cmask, tmp), ++*launches;
+    if (v.mark) v.mark(v.mark_ctx, 0, 1);
+    k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, 1, v.sel, v.done, C.mptr,
+                                                           C.mlist, tmp, (const VT*)C.invd, (VT*)C.b, (VT*)C.x),
+        ++*launches;
+  }
+  for (int l = 1; l + 1 < nl; ++l) {  // down, coarse levels: one thread per aggregate
     const AmgLevel& F = a->lev[l];
     const AmgLevel& C = a->lev[l + 1];
     k_amg_restrict<KT, VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(
-        C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done, C.mptr, C.mlist, l == 0 ? v.rowptr0 : F.rowptr,
-        l == 0 ? v.colind0 : F.colind, l == 0 ? (const KT*)v.K0 : (const KT*)F.A,
-        l == 0 ? (const VT*)v.r : (const VT*)F.b, l == 0 ? (const VT*)v.x0 : (const VT*)F.x,
-        l == 0 ? v.cmask : nullptr, (const VT*)C.invd, (VT*)C.b, (VT*)C.x), ++*launches;
+        C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done, C.mptr, C.mlist, F.rowptr, F.colind, (const KT*)F.A,
+        (const VT*)F.b, (const VT*)F.x, nullptr, (const VT*)C.invd, (VT*)C.b, (VT*)C.x), ++*launches;
   }
   k_amg_dense_apply<VT><<<a->nsys, 128, 0, st>>>(v.sel, v.done, a->d_depth, a->d_dn, a->d_doff, a->d_lev_dofoff,
                                                  a->d_lev_b, a->d_lev_x2, a->dense), ++*launches;
-  for (int l = nl - 2; l >= 0; --l) {  // up: the finer level reads the coarser post-smoothed x2
+  for (int l = nl - 2; l >= 1; --l) {  // up, coarse levels: the finer level reads the coarser post-smoothed x2
     const AmgLevel& F = a->lev[l];
     const AmgLevel& C = a->lev[l + 1];
-    const bool fine = l == 0;
-    k_amg_prolong_smooth<KT, VT, 8><<<fine ? v.nrb0 : F.nrb, 256, 0, st>>>(
-        fine ? v.rb_start0 : F.rb_start, fine ? v.rb_sys0 : F.rb_sys, fine ? v.nrb0 : F.nrb, v.sel, v.done,
-        a->d_depth, l, fine ? v.rowptr0 : F.rowptr, fine ? v.colind0 : F.colind,
-        fine ? (const KT*)v.K0 : (const KT*)F.A, fine ? (const VT*)v.r : (const VT*)F.b,
-        fine ? (const VT*)v.x0 : (const VT*)F.x, (const VT*)C.x2, F.cmap, (const VT*)F.invd,
-        fine ? v.cmask : nullptr, fine ? (VT*)v.z : (VT*)F.x2, fine ? (VT*)v.pcopy : nullptr,
-        fine ? v.part_rz : nullptr), ++*launches;
+    k_amg_prolong_smooth<KT, VT, 8><<<F.nrb, 256, 0, st>>>(
+        F.rb_start, F.rb_sys, F.nrb, v.sel, v.done, a->d_depth, l, F.rowptr, F.colind, (const KT*)F.A,
+        (const VT*)F.b, (const VT*)F.x, (const VT*)C.x2, F.cmap, (const VT*)F.invd, nullptr, (VT*)F.x2, nullptr,
+        nullptr), ++*launches;
+  }
+  // up, finest level: coarse correction, then post-smoothing with r.z
+  {
+    const AmgLevel& F = a->lev[0];
+    const AmgLevel& C = a->lev[1];
+    k_amg_correct<VT><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, x0, (const VT*)C.x2, F.cmap,
+                                              v.cmask, tmp), ++*launches;
+    if (v.mark) v.mark(v.mark_ctx, 1, 0);
+    if (v.lpr == 16)
+      k_amg_smooth<KT, VT, 16><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, v.rowptr0, v.colind0,
+                                                       K0, r, tmp, (const VT*)F.invd, v.cmask, (VT*)v.z,
+                                                       (VT*)v.pcopy, v.part_rz), ++*launches;
+    else
+      k_amg_smooth<KT, VT, 8><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, v.rowptr0, v.colind0,
+                                                      K0, r, tmp, (const VT*)F.invd, v.cmask, (VT*)v.z,
+                                                      (VT*)v.pcopy, v.part_rz), ++*launches;
+    if (v.mark) v.mark(v.mark_ctx, 1, 1);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "AMG V-cycle: %s", cudaGetErrorString(e));

@@ -22,6 +22,12 @@ struct AmgPcgView {
   const int *sel, *done;
   const int *rb_start0, *rb_sys0;
   int nrb0;
+  int lpr;     // lanes per fine row (8 or 16)
+  void* tmp;   // a free fine-level vector (residual, then corrected iterate)
+  // optional timing hook around the fine-level launches (kind 0 restriction, 1 prolongation;
+  // phase 0 before, 1 after)
+  void (*mark)(void* ctx, int kind, int phase) = nullptr;
+  void* mark_ctx = nullptr;
 };
 
 // Build the hierarchy of every system of the handle (host aggregation,
@@ -35,7 +41,8 @@ const void* amg_invd0(const ua_mesh* m);
 // Numeric phase for a new tangent K0 (Galerkin products, smoother, coarsest inverses).
 int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
                 const unsigned char* cmask, long long* launches);
-// One V(1,1) cycle.
+// One V(1,1) cycle.  The finest level runs as row-block kernels (residual,
+// aggregation, correction, smoothing); coarser levels use one thread per aggregate.
 int amg_vcycle(ua_mesh* m, bool fp32, const AmgPcgView& v, long long* launches);
 
 }  // namespace ua

@@ -44,7 +44,7 @@ struct Prof {
   void reset() { used = 0; marks.clear(); }
   ~Prof() { for (auto e : pool) cudaEventDestroy(e); }
 };
-enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2 };
+enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2, PK_AMGR = 3, PK_AMGP = 4, PK_COUNT = 5 };
 constexpr int kRedThreads = 256;
 enum { SV_RZ = 0, SV_PQ, SV_ALPHA, SV_BETA, SV_RR, SV_RR0, SV_TOL2, SV_NORM, SV_FF, SV_FD, SV_OMEGA, SV_COUNT };
 
@@ -90,6 +90,12 @@ struct Work {
   std::vector<int> h_sys_rb_off, h_sys_con_off;
   Prof prof;
   struct ServeState* serve = nullptr;
+  // replayable PCG chunks, index (fp32 ? 2 : 0) + (amg ? 1 : 0)
+  bool no_graph = false;
+  cudaGraphExec_t pcg_exec[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long pcg_exec_nodes[4] = {0, 0, 0, 0};
+  int pcg_exec_maxit[4] = {0, 0, 0, 0};
+  int pcg_exec_lpr[4] = {0, 0, 0, 0};
 };
 
 static void prof_begin(ua_mesh* m, int kind, cudaEvent_t* ev) {
@@ -104,6 +110,13 @@ static void prof_begin(ua_mesh* m, int kind, cudaEvent_t* ev) {
 static void prof_end(ua_mesh* m, cudaEvent_t* ev) {
   if (!m->work->prof.on) return;
   cudaEventRecord(ev[1], m->stream);
+}
+// timing hook of the fine-level AMG launches (kind: 0 restriction, 1 prolongation)
+static void prof_amg(void* ctx, int kind, int phase) {
+  static thread_local cudaEvent_t ev[2];
+  ua_mesh* m = (ua_mesh*)ctx;
+  if (phase == 0) prof_begin(m, kind == 0 ? PK_AMGR : PK_AMGP, ev);
+  else prof_end(m, ev);
 }
 
 // ---------------------------------------------------------------------------
@@ -804,8 +817,10 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   // with AMG the Jacobi-type kernels write the l1 pre-smoothed vector x0 and the V-cycle writes z (and r.z)
   const VT* invd = amg ? (const VT*)amg_invd0(m) : (const VT*)w->invd;
   VT* zj = amg ? (VT*)w->kx0 : z;
+  // q is free between update1 and the next SpMV: the V-cycle's fine-level scratch
   AmgPcgView view{w->rowptr, w->colind, K, r, w->kx0, z, nullptr, w->part, w->cmask, w->sel, w->done,
-                  w->rb_start, w->rb_sys, w->nrb};
+                  w->rb_start, w->rb_sys, w->nrb, lpr, q};
+  if (w->prof.on) { view.mark = prof_amg; view.mark_ctx = m; }
   if (lpr == 8)
     k_pcg_init<KT, VT, 8><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr,
                                                          w->colind, K, w->dX, w->frhs, w->cmask, invd, r, zj, pp,
@@ -826,30 +841,67 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
                                                         w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
   const int chunk = 16;
+  // one PCG iteration for every selected, unfinished system
+  auto iteration = [&]() -> int {
+    cudaEvent_t ev[2];
+    prof_begin(m, PK_SPMV, ev);
+    if (lpr == 8)
+      k_pcg_spmv<KT, VT, 8><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done,
+                                                           w->rowptr, w->colind, K, pp, w->cmask, q, w->part), ++g_launches;
+    else
+      k_pcg_spmv<KT, VT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done,
+                                                            w->rowptr, w->colind, K, pp, w->cmask, q, w->part), ++g_launches;
+    prof_end(m, ev);
+    k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                          w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+    k_pcg_update1<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->sysv,
+                                                     w->nsys, w->dX, r, zj, pp, q, invd, w->part), ++g_launches;
+    if (amg) {
+      int rc = amg_vcycle(m, fp32, view, &g_launches);
+      if (rc) return rc;
+    }
+    k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                          w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+    k_pcg_update2<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys,
+                                                     pp, z), ++g_launches;
+    return UA_OK;
+  };
+  // A chunk of iterations is captured once per (handle, precision, preconditioner) as a CUDA
+  // graph and replayed: every argument is a fixed device buffer of the handle, and systems that
+  // have converged skip their rows on the device (done[s]), so a replay equals the launches.
+  const bool graph = !w->no_graph && !p->profile;
+  const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0);
+  if (graph && w->pcg_exec[gk] && (w->pcg_exec_maxit[gk] != p->krylov_maxit || w->pcg_exec_lpr[gk] != lpr)) {
+    cudaGraphExecDestroy(w->pcg_exec[gk]);
+    w->pcg_exec[gk] = nullptr;
+  }
+  if (graph && !w->pcg_exec[gk]) {
+    const long long l0 = g_launches;
+    cudaGraph_t gr = nullptr;
+    UA_CUDA_TRY(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = UA_OK;
+    for (int k = 0; k < chunk && rc == UA_OK; ++k) rc = iteration();
+    cudaError_t ce = cudaStreamEndCapture(m->stream, &gr);
+    if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+    if (ce != cudaSuccess) return set_error(UA_ERR_CUDA, "PCG graph capture: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&w->pcg_exec[gk], gr, 0);
+    cudaGraphDestroy(gr);
+    if (ce != cudaSuccess) return set_error(UA_ERR_CUDA, "PCG graph instantiation: %s", cudaGetErrorString(ce));
+    w->pcg_exec_nodes[gk] = g_launches - l0;
+    w->pcg_exec_maxit[gk] = p->krylov_maxit;
+    w->pcg_exec_lpr[gk] = lpr;
+    g_launches = l0;  // capture launches nothing
+  }
   int it = 0;
   while (true) {
-    for (int k = 0; k < chunk; ++k) {
-      cudaEvent_t ev[2];
-      prof_begin(m, PK_SPMV, ev);
-      if (lpr == 8)
-        k_pcg_spmv<KT, VT, 8><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done,
-                                                             w->rowptr, w->colind, K, pp, w->cmask, q, w->part), ++g_launches;
-      else
-        k_pcg_spmv<KT, VT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done,
-                                                              w->rowptr, w->colind, K, pp, w->cmask, q, w->part), ++g_launches;
-      prof_end(m, ev);
-      k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
-                                                            w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
-      k_pcg_update1<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->sysv,
-                                                       w->nsys, w->dX, r, zj, pp, q, invd, w->part), ++g_launches;
-      if (amg) {
-        int rc = amg_vcycle(m, fp32, view, &g_launches);
+    if (graph) {
+      UA_CUDA_TRY(cudaGraphLaunch(w->pcg_exec[gk], m->stream));
+      g_launches += w->pcg_exec_nodes[gk];
+    } else {
+      for (int k = 0; k < chunk; ++k) {
+        int rc = iteration();
         if (rc) return rc;
       }
-      k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
-                                                            w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
-      k_pcg_update2<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys,
-                                                       pp, z), ++g_launches;
     }
     it += chunk;
     UA_CUDA_TRY(cudaGetLastError());
@@ -1624,7 +1676,7 @@ extern "C" void ua_params_default(ua_params* p) {
   std::memcpy(p->uvhAcceptableWorkOrForceTolerances, a2, sizeof a2);
   p->krylov_rtol = 1e-12; p->krylov_maxit = 20000; p->precision = UA_PREC_FP64;
   p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1;
-  p->krylov_precond = UA_PC_JACOBI;
+  p->krylov_precond = UA_PC_AMG;
 }
 
 extern "C" int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs, int32_t mode,
@@ -1742,8 +1794,8 @@ static int newton_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_
   double t1 = now_ms();
   float dev_ms = 0;
   cudaEventElapsedTime(&dev_ms, call_ev[0], call_ev[1]);
-  double kms[3] = {0, 0, 0};
-  int kn[3] = {0, 0, 0};
+  double kms[PK_COUNT] = {};
+  int kn[PK_COUNT] = {};
   for (auto& mk : w->prof.marks) {
     float t = 0;
     cudaEventElapsedTime(&t, mk.second.first, mk.second.second);
@@ -1758,6 +1810,8 @@ static int newton_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_
       rep[s]->kasmK_ms = kms[PK_ASMK]; rep[s]->kasmK_n = kn[PK_ASMK];
       rep[s]->kasmR_ms = kms[PK_ASMR]; rep[s]->kasmR_n = kn[PK_ASMR];
       rep[s]->kspmv_ms = kms[PK_SPMV]; rep[s]->kspmv_n = kn[PK_SPMV];
+      rep[s]->kamgR_ms = kms[PK_AMGR]; rep[s]->kamgR_n = kn[PK_AMGR];
+      rep[s]->kamgP_ms = kms[PK_AMGP]; rep[s]->kamgP_n = kn[PK_AMGP];
       rep[s]->gpu_launches = (int)g_launches;
     }
     all_conv = all_conv && st[s].converged;
@@ -1821,6 +1875,8 @@ extern "C" void ua_mesh_destroy(ua_mesh* m) {
   if (m->work) {
     Work* w = m->work;
     delete w->serve;
+    for (auto& e : w->pcg_exec)
+      if (e) cudaGraphExecDestroy(e);
     if (w->h_sysv) cudaFreeHost(w->h_sysv);
     if (w->h_int) cudaFreeHost(w->h_int);
     if (w->h_gamma) cudaFreeHost(w->h_gamma);
@@ -1882,6 +1938,7 @@ extern "C" int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const 
   tmp.h_dof_off = {0, n};
   int rc = UA_OK;
   Work* w = new Work();
+  w->no_graph = true;  // a one-off solve: nothing to replay
   tmp.work = w;
   UA_CUDA_TRY(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking));
   auto cleanup = [&]() {
@@ -2102,6 +2159,7 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
   view.dm.nsys = 1;
   view.stream = cudaStreamPerThread;
   Work w;
+  w.no_graph = true;  // no graph instantiation (it may allocate)
   static thread_local double h_sysv[SV_COUNT];
   static thread_local int h_int[8];
   w.nsys = 1; w.nrb = nrb; w.nc = nl;
@@ -2245,8 +2303,8 @@ static int uvh_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs
   UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   float dev_ms = 0;
   cudaEventElapsedTime(&dev_ms, call_ev[0], call_ev[1]);
-  double kms[3] = {0, 0, 0};
-  int kn[3] = {0, 0, 0};
+  double kms[PK_COUNT] = {};
+  int kn[PK_COUNT] = {};
   for (auto& mk : w->prof.marks) {
     float t = 0;
     cudaEventElapsedTime(&t, mk.second.first, mk.second.second);
@@ -2261,6 +2319,8 @@ static int uvh_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs
       rep[s]->kasmK_ms = kms[PK_ASMK]; rep[s]->kasmK_n = kn[PK_ASMK];
       rep[s]->kasmR_ms = kms[PK_ASMR]; rep[s]->kasmR_n = kn[PK_ASMR];
       rep[s]->kspmv_ms = kms[PK_SPMV]; rep[s]->kspmv_n = kn[PK_SPMV];
+      rep[s]->kamgR_ms = kms[PK_AMGR]; rep[s]->kamgR_n = kn[PK_AMGR];
+      rep[s]->kamgP_ms = kms[PK_AMGP]; rep[s]->kamgP_n = kn[PK_AMGP];
       rep[s]->gpu_launches = (int)g_launches;
     }
     all_conv = all_conv && st[s].converged;

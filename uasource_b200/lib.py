@@ -106,6 +106,7 @@ class ua_newton_report(C.Structure):
                 ("assembly_ms", C.c_double), ("solve_ms", C.c_double), ("total_ms", C.c_double),
                 ("device_ms", C.c_double), ("kasmK_ms", C.c_double), ("kasmR_ms", C.c_double),
                 ("kspmv_ms", C.c_double), ("kasmK_n", C.c_int32), ("kasmR_n", C.c_int32), ("kspmv_n", C.c_int32),
+                ("kamgR_ms", C.c_double), ("kamgP_ms", C.c_double), ("kamgR_n", C.c_int32), ("kamgP_n", C.c_int32),
                 ("gpu_launches", C.c_int32),
                 ("n_iter_records", C.c_int32), ("iters_capacity", C.c_int32),
                 ("iters", C.POINTER(ua_newton_iter))]

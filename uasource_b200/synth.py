@@ -201,11 +201,24 @@ def batch_sizes(count=256, lo=2e3, hi=2e5, seed=12345):
     return np.exp(rng.uniform(np.log(lo), np.log(hi), count))
 
 
+def batch_problem(k, count=256, lo=2e3, hi=2e5, seed=12345):
+    """Problem k of the batched workload (see ``batch_problems``)."""
+    ne = batch_sizes(count, lo, hi, seed)[k]
+    nx, ny = elements_to_grid(int(ne), aspect=2.0)
+    return ice_stream_shelf(nx, ny, nod=3, seed=1000 + k)
+
+
 def batch_problems(count=256, lo=2e3, hi=2e5, seed=12345):
     """256 independent ice-stream/shelf problems on 100 km x 50 km rectangles of
     log-uniform size (P1), each with its own seed for bumps, A and C."""
+    return [batch_problem(k, count, lo, hi, seed) for k in range(count)]
+
+
+def serve_templates(count=16, lo=5e3, hi=5e5, seed=777):
+    """Resident mesh templates of the served workload: ``count`` ice-stream/shelf
+    problems (P1) of log-uniform size in [lo, hi] elements, each with its own seed."""
     out = []
     for k, ne in enumerate(batch_sizes(count, lo, hi, seed)):
         nx, ny = elements_to_grid(int(ne), aspect=2.0)
-        out.append(ice_stream_shelf(nx, ny, nod=3, seed=1000 + k))
+        out.append(ice_stream_shelf(nx, ny, nod=3, seed=5000 + k))
     return out

@@ -74,7 +74,7 @@ class CtrlVar:
     verbose: int = 0
     profile: int = 0
     krylov_adaptive: int = 1
-    krylov_precond: int = L.UA_PC_JACOBI
+    krylov_precond: int = L.UA_PC_AMG
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
@@ -264,6 +264,12 @@ class MUA:
         L.check(L.load().ua_mesh_flipped(self._h, C.byref(n)))
         return n.value
 
+    def nnz(self, s=0):
+        """Non-zeros of system s's structural tangent pattern."""
+        nnz = C.c_int64()
+        L.check(L.load().ua_mesh_pattern(self._h, s, C.byref(nnz), None, None))
+        return nnz.value
+
     def pattern(self, s=0):
         """(rowptr, colind) of the structural tangent pattern (0-based, sorted)."""
         if s not in self._pattern:
@@ -368,7 +374,8 @@ def _report(rep, recs):
         its.append(dict(iteration=it.iteration, iarm=it.iarm, krylov_its=it.krylov_its, direction=it.direction,
                         gamma=it.gamma, r0=it.r0, r=it.r, rForce=it.rForce, rWork=it.rWork))
     kern = dict(asmK_ms=rep.kasmK_ms, asmK_n=rep.kasmK_n, asmR_ms=rep.kasmR_ms, asmR_n=rep.kasmR_n,
-                spmv_ms=rep.kspmv_ms, spmv_n=rep.kspmv_n)
+                spmv_ms=rep.kspmv_ms, spmv_n=rep.kspmv_n, amgR_ms=rep.kamgR_ms, amgR_n=rep.kamgR_n,
+                amgP_ms=rep.kamgP_ms, amgP_n=rep.kamgP_n)
     return RunInfo(bool(rep.converged), rep.iterations, rep.backtrack_steps, rep.krylov_its_total,
                    rep.cauchy_fallbacks, bool(rep.retried), rep.r, rep.rForce, rep.rWork, rep.assembly_ms,
                    rep.solve_ms, rep.total_ms, rep.device_ms, kern, rep.gpu_launches, its)
@@ -431,6 +438,37 @@ def uv_batch(ctrl: CtrlVar, mua: MUA, Fs, bcss):
     rc = lib.ua_uv_newton_batch(mua.handle, C.byref(p), cfs, cbs, reps)
     L.check(rc, allow=(L.UA_ERR_NOT_CONVERGED,))
     return [(outs[s][0], outs[s][1], _report(reps[s], recs[s])) for s in range(ns)]
+
+
+def uv_batch_resident(ctrl: CtrlVar, mua: MUA, F_devs, bcss, rhow=1030.0, g=9.81 / 1000, alpha=0.0):
+    """Batched uv Newton with every system's fields already resident in device memory.
+
+    ``F_devs[s]`` maps h, S, B, rho, AGlen, n, C, m, ub, vb to device addresses of
+    system s (see ``uv_resident``); ub/vb are overwritten with the solutions.
+    Returns a list of RunInfo.
+    """
+    lib = L.load()
+    keep = _Keep()
+    ns = mua.nsys
+    cfs = (L.ua_fields * ns)()
+    cbs = (L.ua_bcs * ns)()
+    reps = (L.ua_newton_report * ns)()
+    recs = []
+    for s in range(ns):
+        cf = cfs[s]
+        cf.location = L.UA_DEVICE
+        for name in ("h", "S", "B", "rho", "AGlen", "n", "C", "m", "ub", "vb"):
+            setattr(cf, name, C.cast(C.c_void_p(int(F_devs[s][name])), L._dp))
+        cf.rhow, cf.g, cf.alpha = float(rhow), float(g), float(alpha)
+        cbs[s] = _c_bcs(bcss[s], keep)
+        r = (L.ua_newton_iter * ((ctrl.NRitmax + 2) * 2))()
+        recs.append(r)
+        reps[s].iters = C.cast(r, C.POINTER(L.ua_newton_iter))
+        reps[s].iters_capacity = (ctrl.NRitmax + 2) * 2
+    p = ctrl.to_c()
+    rc = lib.ua_uv_newton_batch(mua.handle, C.byref(p), cfs, cbs, reps)
+    L.check(rc, allow=(L.UA_ERR_NOT_CONVERGED,))
+    return [_report(reps[s], recs[s]) for s in range(ns)]
 
 
 def _c_fields_uvh(F0: Fields, F1: Fields, dt, keep: _Keep, Nn: int):
