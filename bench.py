@@ -362,8 +362,10 @@ def run_ours(args):
     value_plain = world * len(sample) / (t_plain / 1000)
     e2e_value = world * count * args.steps / (t_e2e / 1000)
 
-    # roofline of the dominant kernel class (by measured device time); algorithmic bytes per launch
-    # (whole batch, FP32 values and vectors, 4-byte indices)
+    # roofline of the dominant kernel class (by measured device time).  Algorithmic bytes of each
+    # timed launch follow from the tangent non-zeros and dof rows of the systems it processed
+    # (counted on the device per launch; converged systems drop out of the Krylov kernels);
+    # FP32 values and vectors, 4-byte indices.
     nnz = sum(mua.nnz(s) for s in range(count))
     Ne = sum(P.Nele for P in probs)
     rows = 2 * Nn_tot
@@ -373,29 +375,39 @@ def run_ours(args):
     except Exception:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    wn, wr = prof["work_nnz"], prof["work_rows"]
+    ele_per_row = Ne / rows
+    # per class: (ms, launches, algorithmic bytes summed over the launches, bytes per non-zero / row)
     cand = {
         "uv_patch_kernel<3,K,float> (tangent+residual assembly)":
-            (prof["asmK_ms"], prof["asmK_n"], 12 * Ne + 16 * Nn_tot + 80 * Nn_tot + 4 * nnz + 8 * rows),
+            (prof["asmK_ms"], prof["asmK_n"], 4 * wn["asmK"] + (12 * ele_per_row + 48 + 8) * wr["asmK"],
+             "4 B/nnz (K write) + per row: 12*Ne/rows connectivity + 48 nodal fields + 8 R"),
         "uv_patch_kernel<3,R> (residual-only assembly)":
-            (prof["asmR_ms"], prof["asmR_n"], 12 * Ne + 16 * Nn_tot + 80 * Nn_tot + 8 * rows),
-        "k_pcg_spmv<float,float,8> (PCG SpMV + p.q)":
-            (prof["spmv_ms"], prof["spmv_n"], 8 * nnz + 4 * (rows + 1) + 4 * rows + 4 * rows + rows),
-        "k_amg_restrict<float,float> (fine residual + aggregation)":
-            (prof["amgR_ms"], prof["amgR_n"], 8 * nnz + 4 * (rows + 1) + 4 * rows + 4 * rows + 4 * rows + 4 * rows + rows),
-        "k_amg_prolong_smooth<float,float,8> (coarse correction + l1-Jacobi + r.z)":
-            (prof["amgP_ms"], prof["amgP_n"], 8 * nnz + 4 * (rows + 1) + 4 * rows * 6 + rows),
+            (prof["asmR_ms"], prof["asmR_n"], (12 * ele_per_row + 48 + 8) * wr["asmR"],
+             "per row: 12*Ne/rows connectivity + 48 nodal fields + 8 R"),
+        "k_pcg_spmv<float,float,1> (PCG SpMV + p.q)":
+            (prof["spmv_ms"], prof["spmv_n"], 8 * wn["spmv"] + 13 * wr["spmv"],
+             "8 B/nnz (value + column) + per row: 4 rowptr + 4 p + 4 q + 1 mask"),
+        "k_amg_residual<float,float,1> (finest-level residual of the pre-smoothed vector)":
+            (prof["amgR_ms"], prof["amgR_n"], 8 * wn["amgR"] + 17 * wr["amgR"],
+             "8 B/nnz + per row: 4 rowptr + 4 b + 4 x + 4 res + 1 mask"),
+        "k_amg_smooth<float,float,1> (finest-level l1-Jacobi post-smoothing + r.z)":
+            (prof["amgP_ms"], prof["amgP_n"], 8 * wn["amgP"] + 21 * wr["amgP"],
+             "8 B/nnz + per row: 4 rowptr + 4 b + 4 xp + 4 invd + 4 z + 1 mask"),
     }
     dom = max(cand, key=lambda c: cand[c][0])
-    ms, n, alg = cand[dom]
+    ms, n, alg_total, rule = cand[dom]
     avg_ms = ms / max(n, 1)
-    achieved = alg / (avg_ms / 1000) / 1e9 if n else 0.0
+    achieved = alg_total / (ms / 1000) / 1e9 if ms > 0 else 0.0
     total_k = sum(v[0] for v in cand.values())
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "traffic": None,
-            "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms, "launches": n,
+            "alg_bytes_per_launch": alg_total / max(n, 1), "alg_bytes_rule": rule,
+            "avg_launch_ms": avg_ms, "launches": n,
             "peak_source": ("MEASURED_PEAKS.json hbm_gbs (burst copy), of measured" if "hbm_gbs" in peaks
                             else "fallback 6650 GB/s, of fallback"),
-            "kernel_share_of_timed_classes": {c: v[0] / max(total_k, 1e-12) for c, v in cand.items()}}
+            "kernel_share_of_timed_classes": {c: v[0] / max(total_k, 1e-12) for c, v in cand.items()},
+            "classes_gbs": {c: (v[2] / (v[0] / 1000) / 1e9 if v[0] > 0 else None) for c, v in cand.items()}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -486,6 +498,102 @@ def _serve_leg(args, ua, L, synth, np, device):
             "rel_err_vs_fp64_max": max(errs) if errs else None, "checked": len(errs)}
 
 
+def _big_p2_problem(transient):
+    """The 400 km x 200 km P2 mesh of ~1M elements (1001x501 vertices before mid-nodes)."""
+    from uasource_b200 import synth
+    return synth.ice_stream_shelf(1001, 501, Lx=400e3, Ly=200e3, nod=6, seed=0, transient=transient)
+
+
+def _timed_calls(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    per, out = [], None
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        per.append(e0.elapsed_time(e1))
+    return per, out
+
+
+def run_uv1m(args):
+    """Precision form on the 1M-element P2 mesh: one uv solve, mixed vs plain FP64."""
+    import numpy as np
+    import uasource_b200 as ua
+    from uasource_b200 import lib as L
+    P = _big_p2_problem(False)
+    mua = ua.CreateMUA(P.coordinates, P.connectivity)
+    bcs = ua.BCs.from_problem(P)
+    res = {}
+    for name, prec, rtol in (("fp64", L.UA_PREC_FP64, 1e-12), ("mixed", L.UA_PREC_MIXED, 1e-6)):
+        ctrl = ua.CtrlVar(precision=prec, krylov_rtol=rtol).set_force_tolerance(1e-20)
+        per, out = _timed_calls(lambda: ua.uv(ctrl, mua, bcs, ua.Fields.from_problem(P)), args.steps,
+                                max(1, min(args.warmup, 1)))
+        Fo, _, _, _, info = out
+        res[name] = (per, np.concatenate([Fo.ub, Fo.vb]), info)
+    u64 = res["fp64"][1]
+    err = float(np.linalg.norm(res["mixed"][1] - u64) / np.linalg.norm(u64))
+    v_mx = 1000 * len(res["mixed"][0]) / sum(res["mixed"][0])
+    v_64 = 1000 * len(res["fp64"][0]) / sum(res["fp64"][0])
+    line = {"metric": "uv Newton solves/s, 1M-element P2 mesh (mixed vs plain FP64)", "value": v_mx,
+            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": 1,
+            "ms_per_step": sum(res["mixed"][0]) / len(res["mixed"][0]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic",
+            "config": {"workload": f"uv solve from u=v=0, ice stream/shelf 400x200 km, P2, {P.Nele} elements, "
+                                   f"{P.Nnodes} nodes, seed 0, rForce<1e-20"},
+            "plain_fp64": {"value": v_64, "unit": "solves/s",
+                           "newton_iterations": res["fp64"][2].iterations,
+                           "pcg_iterations": res["fp64"][2].krylov_its_total},
+            "mixed": {"newton_iterations": res["mixed"][2].iterations,
+                      "pcg_iterations": res["mixed"][2].krylov_its_total},
+            "rel_err_mixed_vs_fp64": err, "mixed_over_plain": v_mx / v_64}
+    print(json.dumps(line), flush=True)
+    mua.close()
+    return 0
+
+
+def run_uvh1m(args):
+    """Plain FP64 implicit uvh step (dt = 0.1 a) on the 1M-element P2 mesh."""
+    import numpy as np
+    import uasource_b200 as ua
+    from uasource_b200 import lib as L
+    P = _big_p2_problem(True)
+    bcs = ua.BCs.from_problem(P)
+    m2 = ua.CreateMUA(P.coordinates, P.connectivity)
+    F = ua.Fields.from_problem(P)
+    Fo, _, _, _, info_uv = ua.uv(ua.CtrlVar(precision=L.UA_PREC_MIXED, krylov_rtol=1e-6).set_force_tolerance(1e-20),
+                                 m2, bcs, F)
+    m2.close()
+    m3 = ua.CreateMUA(P.coordinates, P.connectivity, ndof=3)
+    F0 = ua.Fields.from_problem(P)
+    F0.ub, F0.vb = Fo.ub, Fo.vb
+    F1 = F0.copy()
+    ctrl = ua.CtrlVar().set_force_tolerance(1e-20)
+    hb = ua.HBCs(ubFixedNode=bcs.ubFixedNode, ubFixedValue=bcs.ubFixedValue, vbFixedNode=bcs.vbFixedNode,
+                 vbFixedValue=bcs.vbFixedValue)
+    per, out = _timed_calls(lambda: ua.uvh(ctrl, m3, F0, F1, hb, 0.1), args.steps, 1)
+    F1o, _, info = out
+    prof = ua.uvh(ua.CtrlVar(profile=1).set_force_tolerance(1e-20), m3, F0, F1, hb, 0.1)[2]
+    line = {"metric": "uvh implicit steps/s, 1M-element P2 mesh (plain FP64)", "value": 1000 * len(per) / sum(per),
+            "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": sum(per) / len(per),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"implicit uvh step dt=0.1 a (SSTREAM_TransientImplicit, SUPG), ice stream/shelf "
+                                   f"400x200 km, P2, {P.Nele} elements, {P.Nnodes} nodes, a=0.3+0.1N(0,1), "
+                                   f"start: converged diagnostic state"},
+            "newton_iterations": info.iterations, "krylov_iterations": info.krylov_its_total,
+            "converged": bool(info.converged), "rForce": info.rForce,
+            "kernels": prof.kernels, "device_ms": prof.device_ms,
+            "dh_max_m": float(np.max(np.abs(F1o.h - P.h)))}
+    print(json.dumps(line), flush=True)
+    m3.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -501,9 +609,15 @@ def main():
     # profiling-only options (ncu captures on bounded cases); the bench line uses the defaults
     ap.add_argument("--legs", default="all", choices=["all", "mixed"])
     ap.add_argument("--batch", type=int, default=BATCH, help="meshes per step (default 256)")
+    # the 1M-element P2 workloads (their own JSON line; the headline line is the batched one)
+    ap.add_argument("--workload", default="batch", choices=["batch", "uv1m", "uvh1m"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "uv1m":
+        return run_uv1m(args)
+    if args.workload == "uvh1m":
+        return run_uvh1m(args)
     return run_ours(args)
 
 

@@ -118,6 +118,8 @@ typedef struct ua_params {
                                   (inexact Newton forcing term); 0: krylov_rtol every iteration */
     int32_t krylov_precond;    /* UA_PC_*: preconditioner of the uv inner PCG (the uvh BiCGStab uses
                                   point Jacobi) */
+    int32_t spmv_lanes;        /* lanes per row of the uv PCG/AMG row products: 0 = by element type
+                                  (1 for P1, 2 for P2), else 1, 2, 4, 8, 16 or 32 */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */
@@ -162,6 +164,9 @@ typedef struct ua_newton_report {
     int32_t kasmK_n, kasmR_n, kspmv_n;       /* launches timed */
     double kamgR_ms, kamgP_ms;  /* fine-level AMG restriction / prolongation+smoothing (profile=1) */
     int32_t kamgR_n, kamgP_n;
+    double kwork_nnz[5], kwork_rows[5];  /* per timed class (asmK, asmR, spmv, amgR, amgP): tangent
+                                            non-zeros and dof rows of the systems each timed launch
+                                            processed, summed over the launches (profile=1) */
     int32_t gpu_launches;       /* kernels launched by the library during the call */
     int32_t n_iter_records;     /* entries filled in iters (<= iters_capacity) */
     int32_t iters_capacity;

@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <vector>
+#include <type_traits>
 #include "ua_amg.h"
 
 namespace ua {
@@ -29,6 +30,19 @@ constexpr int kAmgCoarseNodes = 48;   // a system stops coarsening at this many 
 constexpr int kAmgMaxRow = 32;        // longest coarse dof row (2 x coarse node degree)
 constexpr int kAmgMaxDense = 2 * kAmgCoarseNodes;
 constexpr int kAmgRB = 256;           // rows per row block of a coarse level
+
+// Calls f(std::integral_constant<int, LPR>) for the lanes-per-row value lpr (1, 2, 4, 8, 16 or 32).
+template <class F>
+static void dispatch_lpr(int lpr, F&& f) {
+  switch (lpr) {
+    case 1: f(std::integral_constant<int, 1>()); break;
+    case 2: f(std::integral_constant<int, 2>()); break;
+    case 4: f(std::integral_constant<int, 4>()); break;
+    case 16: f(std::integral_constant<int, 16>()); break;
+    case 32: f(std::integral_constant<int, 32>()); break;
+    default: f(std::integral_constant<int, 8>());
+  }
+}
 
 struct AmgLevel {
   int nn = 0, ndof = 0;
@@ -336,8 +350,12 @@ __global__ void k_amg_l1(int n, const int* rowptr, const int* colind, const KT* 
   invd[i] = (VT)(s > 0 ? 1.0 / s : 0.0);
 }
 
-// Inverse of each system's coarsest matrix: Gauss-Jordan with partial
-// pivoting on [A | I] in shared memory, one CTA per system.  A zero row (an
+// Inverse of each system's coarsest matrix: Gauss-Jordan on [A | I] in
+// shared memory, one CTA per system, row-major result.  A is the Galerkin
+// product of the SPD tangent (symmetric positive definite on the free dofs),
+// so the diagonal pivots stay positive and no pivoting is needed.  At step k
+// only columns k..n+k of the augmented matrix can be non-zero off the
+// finished part, so the update covers those n+1 columns.  A zero row (an
 // aggregate of constrained dofs only; its column is zero too) is replaced by
 // the identity row.
 template <typename KT>
@@ -347,7 +365,6 @@ __global__ void __launch_bounds__(256) k_amg_dense_inverse(const int* depth, con
                                                            double* dense) {
   extern __shared__ double M[];
   __shared__ double fac[kAmgMaxDense];
-  __shared__ int piv;
   const int s = blockIdx.x;
   const int n = dn_arr[s];
   if (n == 0) return;
@@ -369,31 +386,16 @@ __global__ void __launch_bounds__(256) k_amg_dense_inverse(const int* depth, con
     if (zero) M[r * w + r] = 1.0;
   }
   __syncthreads();
+  const int nc = n + 1;  // active columns k..n+k
   for (int k = 0; k < n; ++k) {
-    if (threadIdx.x == 0) {
-      int p = k;
-      double best = fabs(M[k * w + k]);
-      for (int r = k + 1; r < n; ++r)
-        if (fabs(M[r * w + k]) > best) { best = fabs(M[r * w + k]); p = r; }
-      piv = p;
-    }
-    __syncthreads();
-    const int pk = piv;
-    if (pk != k)
-      for (int c = threadIdx.x; c < w; c += blockDim.x) {
-        const double t = M[k * w + c];
-        M[k * w + c] = M[pk * w + c];
-        M[pk * w + c] = t;
-      }
-    __syncthreads();
     const double inv = 1.0 / M[k * w + k];
     for (int r = threadIdx.x; r < n; r += blockDim.x) fac[r] = (r == k) ? 0.0 : M[r * w + k];
     __syncthreads();
-    for (int c = threadIdx.x; c < w; c += blockDim.x) M[k * w + c] *= inv;
+    for (int c = k + threadIdx.x; c <= n + k; c += blockDim.x) M[k * w + c] *= inv;
     __syncthreads();
-    for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
-      const int r = t / w, c = t - r * w;
-      if (r != k) M[t] -= fac[r] * M[k * w + c];
+    for (int t = threadIdx.x; t < n * nc; t += blockDim.x) {
+      const int r = t / nc, c = k + (t - r * nc);
+      if (r != k) M[r * w + c] -= fac[r] * M[k * w + c];
     }
     __syncthreads();
   }
@@ -404,116 +406,48 @@ __global__ void __launch_bounds__(256) k_amg_dense_inverse(const int* depth, con
 // device: V-cycle
 // ---------------------------------------------------------------------------
 
-// Restriction of the pre-smoothed residual of level lc-1 to level lc:
-// b(R) = sum over members i of (b_f(i) - (A_f x_f)(i)), masked members left
-// out; the coarse pre-smoothing x = invd b follows unless lc is the
-// system's coarsest level.
-template <typename KT, typename VT>
-__global__ void k_amg_restrict(int ncd, const int* dof_sys_c, const int* depth, int lc, const int* sel,
-                               const int* done, const int* mptr, const int* mlist, const int* frowptr,
-                               const int* fcolind, const KT* fA, const VT* fb, const VT* fx,
-                               const unsigned char* cmask, const VT* cinvd, VT* cb, VT* cx) {
-  const int R = blockIdx.x * blockDim.x + threadIdx.x;
-  if (R >= ncd) return;
-  const int s = dof_sys_c[R];
-  if (!sel[s] || done[s]) return;
-  double acc = 0;
-  for (int t = mptr[R]; t < mptr[R + 1]; ++t) {
-    const int i = mlist[t];
-    if (cmask && cmask[i]) continue;
-    double r = (double)fb[i];
-    for (int q = frowptr[i]; q < frowptr[i + 1]; ++q) r -= (double)fA[q] * (double)fx[fcolind[q]];
-    acc += r;
-  }
-  cb[R] = (VT)acc;
-  if (depth[s] > lc) cx[R] = (VT)((double)cinvd[R] * acc);
-}
-
-// x2 = inv(A_L) b on each system's coarsest level L
+// x2 = inv(A_L) b on each system's coarsest level L: grid (system, 32-row
+// slab), one warp per row with the lanes over the columns (row-major inverse,
+// coalesced), b staged in shared memory.
 template <typename VT>
-__global__ void k_amg_dense_apply(const int* sel, const int* done, const int* depth, const int* dn_arr,
-                                  const int* doff, int* const* lev_dofoff, void* const* lev_b, void* const* lev_x2,
-                                  const double* dense) {
+__global__ void __launch_bounds__(256) k_amg_dense_apply(const int* sel, const int* done, const int* depth,
+                                                         const int* dn_arr, const int* doff, int* const* lev_dofoff,
+                                                         void* const* lev_b, void* const* lev_x2,
+                                                         const double* dense) {
+  __shared__ double sb[kAmgMaxDense];
   const int s = blockIdx.x;
   if (!sel[s] || done[s]) return;
-  const int n = dn_arr[s], l = depth[s];
+  const int n = dn_arr[s], r0 = blockIdx.y * 32;
+  if (r0 >= n) return;
+  const int l = depth[s];
   const int d0 = lev_dofoff[l][s];
   const VT* b = (const VT*)lev_b[l] + d0;
   VT* x = (VT*)lev_x2[l] + d0;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) sb[c] = (double)b[c];
+  __syncthreads();
   const double* Mi = dense + doff[s];
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int r1 = min(r0 + 32, n);
+  for (int r = r0 + warp; r < r1; r += nw) {  // warp-uniform
     double acc = 0;
-    for (int c = 0; c < n; ++c) acc += Mi[r * n + c] * (double)b[c];
-    x[r] = (VT)acc;
+    for (int c = lane; c < n; c += 32) acc += Mi[r * n + c] * sb[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) x[r] = (VT)acc;
   }
 }
 
-// Coarse correction and post-smoothing of level l (systems deeper than l):
-// xp = x + P xc;  out = xp + invd (b - A xp), masked rows 0 and masked
-// columns without a coarse image.  On the finest level the block partials of
-// b.out (r.z) go to part and pcopy receives a copy of out.
-template <typename KT, typename VT, int LPR>
-__global__ void __launch_bounds__(256) k_amg_prolong_smooth(const int* rb_start, const int* rb_sys, int nrb,
-                                                            const int* sel, const int* done, const int* depth, int l,
-                                                            const int* rowptr, const int* colind, const KT* A,
-                                                            const VT* b, const VT* x, const VT* xc, const int* cmap,
-                                                            const VT* invd, const unsigned char* cmask, VT* out,
-                                                            VT* pcopy, double* part) {
-  const int blk = blockIdx.x;
-  const int s = rb_sys[blk];
-  double rz = 0;
-  if (sel[s] && !done[s] && depth[s] > l) {
-    const int rs = rb_start[blk], re = rb_start[blk + 1];
-    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
-    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread
-      const int row = row0 + grp;
-      const bool valid = row < re;
-      double ax = 0;
-      if (valid)
-        for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) {
-          const int j = colind[q];
-          if (cmask && cmask[j]) continue;
-          ax += (double)A[q] * ((double)x[j] + (double)xc[cmap[j]]);
-        }
-#pragma unroll
-      for (int o = LPR / 2; o > 0; o >>= 1) ax += __shfl_down_sync(0xffffffffu, ax, o, LPR);
-      if (valid && lane == 0) {
-        double v = 0;
-        if (!(cmask && cmask[row])) {
-          const double xp = (double)x[row] + (double)xc[cmap[row]];
-          v = xp + (double)invd[row] * ((double)b[row] - ax);
-        }
-        out[row] = (VT)v;
-        if (pcopy) pcopy[row] = (VT)v;
-        rz += (double)b[row] * v;
-      }
-    }
-  }
-  if (part) {
-    __shared__ double red[8];
-    double t = rz;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double sum = 0;
-      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
-      part[blk] = sum;
-    }
-  }
-}
-
-// Finest level, split form (coalesced row blocks instead of one thread per
-// aggregate).  Residual of the pre-smoothed vector: res = mask(b - A x).
+// Split V-cycle kernels (every level; coalesced row blocks with LPR lanes per
+// row instead of one thread per aggregate).  Residual of the pre-smoothed
+// vector of level l: res = mask(b - A x), for systems deeper than l.
 template <typename KT, typename VT, int LPR>
 __global__ void __launch_bounds__(256) k_amg_residual(const int* rb_start, const int* rb_sys, const int* sel,
-                                                      const int* done, const int* rowptr, const int* colind,
-                                                      const KT* A, const VT* b, const VT* x,
+                                                      const int* done, const int* depth, int l, const int* rowptr,
+                                                      const int* colind, const KT* A, const VT* b, const VT* x,
                                                       const unsigned char* cmask, VT* res) {
   const int blk = blockIdx.x;
   const int s = rb_sys[blk];
-  if (!sel[s] || done[s]) return;
+  if (!sel[s] || done[s] || depth[s] <= l) return;
   const int rs = rb_start[blk], re = rb_start[blk + 1];
   const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
   for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
@@ -524,7 +458,7 @@ __global__ void __launch_bounds__(256) k_amg_residual(const int* rb_start, const
       for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) ax += (double)A[q] * (double)x[colind[q]];
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) ax += __shfl_down_sync(0xffffffffu, ax, o, LPR);
-    if (valid && lane == 0) res[row] = (VT)(cmask[row] ? 0.0 : (double)b[row] - ax);
+    if (valid && lane == 0) res[row] = (VT)((cmask && cmask[row]) ? 0.0 : (double)b[row] - ax);
   }
 }
 
@@ -544,29 +478,31 @@ __global__ void k_amg_gather(int ncd, const int* dof_sys_c, const int* depth, in
   if (depth[s] > lc) cx[R] = (VT)((double)cinvd[R] * acc);
 }
 
-// Coarse correction of the finest level: xp = mask(x + xc[cmap]).
+// Coarse correction of level l, in place: x = mask(x + xc[cmap]) for systems deeper than l.
 template <typename VT>
 __global__ void __launch_bounds__(256) k_amg_correct(const int* rb_start, const int* rb_sys, const int* sel,
-                                                     const int* done, const VT* x, const VT* xc, const int* cmap,
-                                                     const unsigned char* cmask, VT* xp) {
+                                                     const int* done, const int* depth, int l, VT* x,
+                                                     const VT* xc, const int* cmap, const unsigned char* cmask) {
   const int blk = blockIdx.x;
   const int s = rb_sys[blk];
-  if (!sel[s] || done[s]) return;
+  if (!sel[s] || done[s] || depth[s] <= l) return;
   for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x)
-    xp[i] = cmask[i] ? (VT)0 : (VT)((double)x[i] + (double)xc[cmap[i]]);
+    x[i] = (cmask && cmask[i]) ? (VT)0 : (VT)((double)x[i] + (double)xc[cmap[i]]);
 }
 
-// Post-smoothing of the finest level: z = xp + invd (b - A xp) (0 on masked
-// rows), p = z when pcopy is set, block partials of b.z.
+// Post-smoothing of level l: out = xp + invd (b - A xp) (0 on masked rows)
+// for systems deeper than l; on the finest level pcopy (if set) receives a
+// copy and part the block partials of b.out.
 template <typename KT, typename VT, int LPR>
 __global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const int* rb_sys, const int* sel,
-                                                    const int* done, const int* rowptr, const int* colind,
-                                                    const KT* A, const VT* b, const VT* xp, const VT* invd,
-                                                    const unsigned char* cmask, VT* z, VT* pcopy, double* part) {
+                                                    const int* done, const int* depth, int l, const int* rowptr,
+                                                    const int* colind, const KT* A, const VT* b, const VT* xp,
+                                                    const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
+                                                    double* part) {
   const int blk = blockIdx.x;
   const int s = rb_sys[blk];
   double rz = 0;
-  if (sel[s] && !done[s]) {
+  if (sel[s] && !done[s] && depth[s] > l) {
     const int rs = rb_start[blk], re = rb_start[blk + 1];
     const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
     for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
@@ -578,13 +514,15 @@ __global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const i
 #pragma unroll
       for (int o = LPR / 2; o > 0; o >>= 1) ax += __shfl_down_sync(0xffffffffu, ax, o, LPR);
       if (valid && lane == 0) {
-        const double v = cmask[row] ? 0.0 : (double)xp[row] + (double)invd[row] * ((double)b[row] - ax);
-        z[row] = (VT)v;
+        const double v =
+            (cmask && cmask[row]) ? 0.0 : (double)xp[row] + (double)invd[row] * ((double)b[row] - ax);
+        out[row] = (VT)v;
         if (pcopy) pcopy[row] = (VT)v;
         rz += (double)b[row] * v;
       }
     }
   }
+  if (!part) return;  // uniform per launch
   __shared__ double red[8];
   double t = rz;
 #pragma unroll
@@ -641,58 +579,49 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
   Amg* a = m->amg;
   cudaStream_t st = m->stream;
   const int nl = a->nlev;
-  const KT* K0 = (const KT*)v.K0;
-  const VT* r = (const VT*)v.r;
-  const VT* x0 = (const VT*)v.x0;
-  VT* tmp = (VT*)v.tmp;
-  // down, finest level: residual of the pre-smoothed vector, then aggregation
-  {
-    const AmgLevel& C = a->lev[1];
-    if (v.mark) v.mark(v.mark_ctx, 0, 0);
-    if (v.lpr == 16)
-      k_amg_residual<KT, VT, 16><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, v.rowptr0, v.colind0,
-                                                         K0, r, x0, v.cmask, tmp), ++*launches;
-    else
-      k_amg_residual<KT, VT, 8><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, v.rowptr0, v.colind0,
-                                                        K0, r, x0, v.cmask, tmp), ++*launches;
-    if (v.mark) v.mark(v.mark_ctx, 0, 1);
-    k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, 1, v.sel, v.done, C.mptr,
-                                                           C.mlist, tmp, (const VT*)C.invd, (VT*)C.b, (VT*)C.x),
-        ++*launches;
+  // per level l: row blocks, matrix, rhs b, pre-smoothed x, residual / post-smoothed buffer
+  auto rbs = [&](int l) { return l == 0 ? v.rb_start0 : a->lev[l].rb_start; };
+  auto rbsys = [&](int l) { return l == 0 ? v.rb_sys0 : a->lev[l].rb_sys; };
+  auto nrb = [&](int l) { return l == 0 ? v.nrb0 : a->lev[l].nrb; };
+  auto rp = [&](int l) { return l == 0 ? v.rowptr0 : a->lev[l].rowptr; };
+  auto ci = [&](int l) { return l == 0 ? v.colind0 : a->lev[l].colind; };
+  auto A = [&](int l) { return l == 0 ? (const KT*)v.K0 : (const KT*)a->lev[l].A; };
+  auto B = [&](int l) { return l == 0 ? (const VT*)v.r : (const VT*)a->lev[l].b; };
+  auto X = [&](int l) { return l == 0 ? (VT*)v.x0 : (VT*)a->lev[l].x; };
+  auto W = [&](int l) { return l == 0 ? (VT*)v.tmp : (VT*)a->lev[l].x2; };
+  auto mask = [&](int l) { return l == 0 ? v.cmask : nullptr; };
+  const int lpr0 = v.lpr;
+  for (int l = 0; l + 1 < nl; ++l) {  // down: residual of level l, aggregated into level l+1
+    const AmgLevel& C = a->lev[l + 1];
+    if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 0);
+    dispatch_lpr(lpr0, [&](auto L) {
+      k_amg_residual<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
+          rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l));
+    });
+    ++*launches;
+    if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 1);
+    k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done,
+                                                           C.mptr, C.mlist, W(l), (const VT*)C.invd, (VT*)C.b,
+                                                           (VT*)C.x), ++*launches;
   }
-  for (int l = 1; l + 1 < nl; ++l) {  // down, coarse levels: one thread per aggregate
+  k_amg_dense_apply<VT><<<dim3(a->nsys, (a->maxdn + 31) / 32), 256, 0, st>>>(
+      v.sel, v.done, a->d_depth, a->d_dn, a->d_doff, a->d_lev_dofoff, a->d_lev_b, a->d_lev_x2, a->dense), ++*launches;
+  for (int l = nl - 2; l >= 0; --l) {  // up: correction from level l+1's post-smoothed x2, then smoothing
     const AmgLevel& F = a->lev[l];
     const AmgLevel& C = a->lev[l + 1];
-    k_amg_restrict<KT, VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(
-        C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done, C.mptr, C.mlist, F.rowptr, F.colind, (const KT*)F.A,
-        (const VT*)F.b, (const VT*)F.x, nullptr, (const VT*)C.invd, (VT*)C.b, (VT*)C.x), ++*launches;
-  }
-  k_amg_dense_apply<VT><<<a->nsys, 128, 0, st>>>(v.sel, v.done, a->d_depth, a->d_dn, a->d_doff, a->d_lev_dofoff,
-                                                 a->d_lev_b, a->d_lev_x2, a->dense), ++*launches;
-  for (int l = nl - 2; l >= 1; --l) {  // up, coarse levels: the finer level reads the coarser post-smoothed x2
-    const AmgLevel& F = a->lev[l];
-    const AmgLevel& C = a->lev[l + 1];
-    k_amg_prolong_smooth<KT, VT, 8><<<F.nrb, 256, 0, st>>>(
-        F.rb_start, F.rb_sys, F.nrb, v.sel, v.done, a->d_depth, l, F.rowptr, F.colind, (const KT*)F.A,
-        (const VT*)F.b, (const VT*)F.x, (const VT*)C.x2, F.cmap, (const VT*)F.invd, nullptr, (VT*)F.x2, nullptr,
-        nullptr), ++*launches;
-  }
-  // up, finest level: coarse correction, then post-smoothing with r.z
-  {
-    const AmgLevel& F = a->lev[0];
-    const AmgLevel& C = a->lev[1];
-    k_amg_correct<VT><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, x0, (const VT*)C.x2, F.cmap,
-                                              v.cmask, tmp), ++*launches;
-    if (v.mark) v.mark(v.mark_ctx, 1, 0);
-    if (v.lpr == 16)
-      k_amg_smooth<KT, VT, 16><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, v.rowptr0, v.colind0,
-                                                       K0, r, tmp, (const VT*)F.invd, v.cmask, (VT*)v.z,
-                                                       (VT*)v.pcopy, v.part_rz), ++*launches;
-    else
-      k_amg_smooth<KT, VT, 8><<<v.nrb0, 256, 0, st>>>(v.rb_start0, v.rb_sys0, v.sel, v.done, v.rowptr0, v.colind0,
-                                                      K0, r, tmp, (const VT*)F.invd, v.cmask, (VT*)v.z,
-                                                      (VT*)v.pcopy, v.part_rz), ++*launches;
-    if (v.mark) v.mark(v.mark_ctx, 1, 1);
+    k_amg_correct<VT><<<nrb(l), 256, 0, st>>>(rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, X(l),
+                                              (const VT*)C.x2, F.cmap, mask(l)), ++*launches;
+    VT* out = l == 0 ? (VT*)v.z : (VT*)F.x2;
+    VT* pcopy = l == 0 ? (VT*)v.pcopy : nullptr;
+    double* part = l == 0 ? v.part_rz : nullptr;
+    if (l == 0 && v.mark) v.mark(v.mark_ctx, 1, 0);
+    dispatch_lpr(lpr0, [&](auto L) {
+      k_amg_smooth<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
+          rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), (const VT*)F.invd, mask(l),
+          out, pcopy, part);
+    });
+    ++*launches;
+    if (l == 0 && v.mark) v.mark(v.mark_ctx, 1, 1);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "AMG V-cycle: %s", cudaGetErrorString(e));

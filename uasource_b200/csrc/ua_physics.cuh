@@ -25,13 +25,16 @@ __device__ __forceinline__ double dirac_delta(double k, double x, double x0) {
   return 0.5 * k / (c * c);
 }
 
-// EffectiveViscositySSTREAM.m:7-9
+// EffectiveViscositySSTREAM.m:7-9.  e^((1-3n)/n) = e^((1-n)/n) / e^2, so one
+// power of the strain rate serves eta and E (e >= EpsZero > 0).
 __device__ __forceinline__ void effective_viscosity(const UvPhys& P, double A, double n, double exx, double eyy,
                                                     double exy, double& eta, double& E) {
-  double e = sqrt(P.EpsZero * P.EpsZero + exx * exx + eyy * eyy + exx * eyy + exy * exy);
-  double Am = pow(A, -1.0 / n);
-  eta = 0.5 * Am * pow(e, (1.0 - n) / n) + P.etaZero;
-  E = (1.0 - n) / (4.0 * n) * Am * pow(e, (1.0 - 3.0 * n) / n);
+  const double e2 = P.EpsZero * P.EpsZero + exx * exx + eyy * eyy + exx * eyy + exy * exy;
+  const double e = sqrt(e2);
+  const double Am = pow(A, -1.0 / n);
+  const double pe = pow(e, (1.0 - n) / n);
+  eta = 0.5 * Am * pe + P.etaZero;
+  E = (1.0 - n) / (4.0 * n) * Am * pe / e2;
 }
 
 // BasalDrag.m:54-77 (clamps, beta^2, Dbeta^2) and the Weertman branch
@@ -44,12 +47,14 @@ __device__ __forceinline__ Drag basal_drag_weertman(const UvPhys& P, double He, 
                                                     double C, double m) {
   if (delta < 0) delta = 0;
   if (He < 0) He = 0;
-  double u0 = P.SpeedZero;
-  double sp2 = u * u + v * v + u0 * u0;
-  double speed = sqrt(sp2);
-  double Cm = pow(C + P.Czero, -1.0 / m);
-  double beta2 = Cm * pow(speed, 1.0 / m - 1.0);
-  double Dbeta2 = (1.0 / m - 1.0) * Cm * pow(sp2, (1.0 - 3.0 * m) / (2.0 * m));
+  const double u0 = P.SpeedZero;
+  const double sp2 = u * u + v * v + u0 * u0;
+  const double Cm = pow(C + P.Czero, -1.0 / m);
+  // speed^(1/m-1) = sp2^((1-m)/(2m)), and sp2^((1-3m)/(2m)) = sp2^((1-m)/(2m)) / sp2:
+  // one power serves beta^2 and its derivative (sp2 >= SpeedZero^2 > 0)
+  const double ps = pow(sp2, (1.0 - m) / (2.0 * m));
+  const double beta2 = Cm * ps;
+  const double Dbeta2 = (1.0 / m - 1.0) * Cm * ps / sp2;
   Drag d;
   d.taux = He * beta2 * u;
   d.tauy = He * beta2 * v;

@@ -17,12 +17,26 @@
 #include <vector>
 #include "ua_internal.h"
 #include "ua_kernels.h"
+#include <type_traits>
 #include "ua_linesearch.h"
 #include "ua_amg.h"
 
 namespace ua {
 
 constexpr int kRB = 256;        // rows per row block (one CTA)
+
+// Calls f(std::integral_constant<int, LPR>) for the lanes-per-row value lpr (1, 2, 4, 8, 16 or 32).
+template <class F>
+static void dispatch_lpr(int lpr, F&& f) {
+  switch (lpr) {
+    case 1: f(std::integral_constant<int, 1>()); break;
+    case 2: f(std::integral_constant<int, 2>()); break;
+    case 4: f(std::integral_constant<int, 4>()); break;
+    case 16: f(std::integral_constant<int, 16>()); break;
+    case 32: f(std::integral_constant<int, 32>()); break;
+    default: f(std::integral_constant<int, 8>());
+  }
+}
 
 // Kernel launches issued by the library on the calling thread (reported per call).
 static thread_local long long g_launches = 0;
@@ -43,6 +57,9 @@ struct Prof {
   }
   void reset() { used = 0; marks.clear(); }
   ~Prof() { for (auto e : pool) cudaEventDestroy(e); }
+  // per mark: tangent non-zeros and rows of the systems the timed launch works on
+  long long* d_act = nullptr;
+  int act_cap = 0;
 };
 enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2, PK_AMGR = 3, PK_AMGP = 4, PK_COUNT = 5 };
 constexpr int kRedThreads = 256;
@@ -98,13 +115,71 @@ struct Work {
   int pcg_exec_lpr[4] = {0, 0, 0, 0};
 };
 
+// Work of a timed launch: sum of the tangent non-zeros and dof rows of the
+// systems it processes (selected; for Krylov kernels also not yet converged).
+__global__ void k_count_active(int nsys, const int* sel, const int* done, const int* knz_off, const int* dof_off,
+                               long long* out) {
+  __shared__ long long a[256], b[256];
+  long long x = 0, y = 0;
+  for (int s = threadIdx.x; s < nsys; s += blockDim.x)
+    if (sel[s] && !(done && done[s])) {
+      x += knz_off[s + 1] - knz_off[s];
+      y += dof_off[s + 1] - dof_off[s];
+    }
+  a[threadIdx.x] = x;
+  b[threadIdx.x] = y;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) { a[threadIdx.x] += a[threadIdx.x + st]; b[threadIdx.x] += b[threadIdx.x + st]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { out[0] = a[0]; out[1] = b[0]; }
+}
+
 static void prof_begin(ua_mesh* m, int kind, cudaEvent_t* ev) {
   Work* w = m->work;
   if (!w->prof.on) return;
   ev[0] = w->prof.get();
   ev[1] = w->prof.get();
+  const int idx = (int)w->prof.marks.size();
+  if (!w->prof.d_act) {
+    w->prof.act_cap = 1 << 16;
+    w->prof.d_act = (long long*)dev_alloc(m, sizeof(long long) * 2 * w->prof.act_cap);
+  }
+  if (w->prof.d_act && idx < w->prof.act_cap)
+    k_count_active<<<1, 256, 0, m->stream>>>(w->nsys, w->sel, kind >= PK_SPMV ? w->done : nullptr,
+                                             m->dm.sys_knz_off, m->dm.sys_dof_off, w->prof.d_act + 2 * idx),
+        ++g_launches;
   cudaEventRecord(ev[0], m->stream);
   w->prof.marks.push_back({kind, {ev[0], ev[1]}});
+}
+
+// Summed launch times, launch counts and work per timed kernel class.
+static void prof_collect(Work* w, double* kms, int* kn, double* knnz, double* krows) {
+  const int nm = (int)w->prof.marks.size();
+  std::vector<long long> act;
+  if (w->prof.d_act && nm) {
+    act.resize(2 * (size_t)std::min(nm, w->prof.act_cap));
+    cudaMemcpy(act.data(), w->prof.d_act, act.size() * sizeof(long long), cudaMemcpyDeviceToHost);
+  }
+  for (int i = 0; i < nm; ++i) {
+    const auto& mk = w->prof.marks[i];
+    float t = 0;
+    cudaEventElapsedTime(&t, mk.second.first, mk.second.second);
+    kms[mk.first] += t;
+    kn[mk.first]++;
+    if (2 * i + 1 < (int)act.size()) { knnz[mk.first] += (double)act[2 * i]; krows[mk.first] += (double)act[2 * i + 1]; }
+  }
+}
+
+static void prof_report(ua_newton_report* r, const double* kms, const int* kn, const double* knnz,
+                        const double* krows) {
+  r->kasmK_ms = kms[PK_ASMK]; r->kasmK_n = kn[PK_ASMK];
+  r->kasmR_ms = kms[PK_ASMR]; r->kasmR_n = kn[PK_ASMR];
+  r->kspmv_ms = kms[PK_SPMV]; r->kspmv_n = kn[PK_SPMV];
+  r->kamgR_ms = kms[PK_AMGR]; r->kamgR_n = kn[PK_AMGR];
+  r->kamgP_ms = kms[PK_AMGP]; r->kamgP_n = kn[PK_AMGP];
+  for (int k = 0; k < PK_COUNT; ++k) { r->kwork_nnz[k] = knnz[k]; r->kwork_rows[k] = krows[k]; }
 }
 
 static void prof_end(ua_mesh* m, cudaEvent_t* ev) {
@@ -433,11 +508,12 @@ __global__ void k_cost_reduce(const int* sys_rb_off, int nrb, const int* sel, co
   if (!sel[s]) return;
   double o[2];
   sys_sum<2>(part, nrb, sys_rb_off[s], sys_rb_off[s + 1], o);
-  if (threadIdx.x != 0) return;
+  // constraint rows, strided over the block, then a fixed-order tree sum
+  __shared__ double cg[2][kRedThreads];
   double gg = 0, gd = 0;
   if (sys_con_off) {
     const double gm = gamma ? gamma[s] : 0.0;
-    for (int c = sys_con_off[s]; c < sys_con_off[s + 1]; ++c) {
+    for (int c = sys_con_off[s] + threadIdx.x; c < sys_con_off[s + 1]; c += blockDim.x) {
       const int d = con_dof[c];
       const double xv = X[d] + (dX ? gm * dX[d] : 0.0);
       const double gv = con_rhs[c] - xv;
@@ -445,6 +521,19 @@ __global__ void k_cost_reduce(const int* sys_rb_off, int nrb, const int* sel, co
       if (dlam) gd += gv * dlam[c];
     }
   }
+  cg[0][threadIdx.x] = gg;
+  cg[1][threadIdx.x] = gd;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) {
+      cg[0][threadIdx.x] += cg[0][threadIdx.x + st];
+      cg[1][threadIdx.x] += cg[1][threadIdx.x + st];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  gg = cg[0][0];
+  gd = cg[1][0];
   if (write_norm) {
     sysv[SV_NORM * nsys + s] = o[0] + 1000.0 * 2.220446049250313e-16;  // fext0'fext0+1000*eps
     return;
@@ -765,10 +854,14 @@ static int assemble(ua_mesh* m, const ua_params* p, bool withK, bool useDir, con
 
 // Cost function of every selected system at X + gamma dX with direction (dX, dl):
 // CalcCostFunctionNR.m:14-41.  Result in sysv[SV_FF] (rForce) and sysv[SV_FD] (D2).
-static int cost_eval(ua_mesh* m, const ua_params* p, bool useDir) {
+// Cost function at X + gamma dX.  assembleR = false takes w->R as it stands:
+// the residual just assembled at X, which is the R-only assembly at gamma = 0.
+static int cost_eval(ua_mesh* m, const ua_params* p, bool useDir, bool assembleR = true) {
   Work* w = m->work;
-  int rc = assemble(m, p, false, useDir, w->X, false);
-  if (rc) return rc;
+  if (assembleR) {
+    int rc = assemble(m, p, false, useDir, w->X, false);
+    if (rc) return rc;
+  }
   k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, w->dof_con, w->lam,
                                              w->dlam, useDir ? w->gamma : nullptr, w->dX, w->part), ++g_launches;
   k_cost_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, w->nsys, w->sysv,
@@ -786,7 +879,12 @@ template <typename KT, typename VT>
 static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, const double* eta = nullptr) {
   Work* w = m->work;
   const int N = m->ndof_total;
-  const int lpr = (m->nod == 3 && m->ndof == 2) ? 8 : 16;
+  // lanes per row of the row-block products: the caller's choice, else one thread per row for
+  // P1 uv rows (about 14 entries) and two lanes for P2 rows (about 30); measured on B200 over
+  // 1/2/4/8/16 lanes, thread-per-row keeps the most independent loads in flight per warp
+  const int lpr = p->spmv_lanes ? p->spmv_lanes : (m->nod == 3 ? 1 : 2);
+  if (lpr != 1 && lpr != 2 && lpr != 4 && lpr != 8 && lpr != 16 && lpr != 32)
+    return set_error(UA_ERR_INVALID, "spmv_lanes must be 0, 1, 2, 4, 8, 16 or 32");
   // per-system tolerance (relative residual of the preconditioned solve)
   for (int s = 0; s < w->nsys; ++s) {
     const double e = eta ? eta[s] : p->krylov_rtol;
@@ -821,14 +919,12 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   AmgPcgView view{w->rowptr, w->colind, K, r, w->kx0, z, nullptr, w->part, w->cmask, w->sel, w->done,
                   w->rb_start, w->rb_sys, w->nrb, lpr, q};
   if (w->prof.on) { view.mark = prof_amg; view.mark_ctx = m; }
-  if (lpr == 8)
-    k_pcg_init<KT, VT, 8><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr,
-                                                         w->colind, K, w->dX, w->frhs, w->cmask, invd, r, zj, pp,
-                                                         w->part), ++g_launches;
-  else
-    k_pcg_init<KT, VT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr,
-                                                          w->colind, K, w->dX, w->frhs, w->cmask, invd, r, zj, pp,
-                                                          w->part), ++g_launches;
+  dispatch_lpr(lpr, [&](auto L) {
+    k_pcg_init<KT, VT, decltype(L)::value><<<w->nrb, 256, 0, m->stream>>>(
+        w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr, w->colind, K, w->dX, w->frhs, w->cmask, invd, r, zj, pp,
+        w->part);
+  });
+  ++g_launches;
   if (amg) {
     // done[] is reset by the stage-0 reduction below; the V-cycle must see every selected system
     UA_CUDA_TRY(cudaMemsetAsync(w->done, 0, w->nsys * sizeof(int), m->stream));
@@ -845,12 +941,11 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   auto iteration = [&]() -> int {
     cudaEvent_t ev[2];
     prof_begin(m, PK_SPMV, ev);
-    if (lpr == 8)
-      k_pcg_spmv<KT, VT, 8><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done,
-                                                           w->rowptr, w->colind, K, pp, w->cmask, q, w->part), ++g_launches;
-    else
-      k_pcg_spmv<KT, VT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done,
-                                                            w->rowptr, w->colind, K, pp, w->cmask, q, w->part), ++g_launches;
+    dispatch_lpr(lpr, [&](auto L) {
+      k_pcg_spmv<KT, VT, decltype(L)::value><<<w->nrb, 256, 0, m->stream>>>(
+          w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q, w->part);
+    });
+    ++g_launches;
     prof_end(m, ev);
     k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                           w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
@@ -1057,10 +1152,10 @@ static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_rep
     double t2 = now_ms();
     t_sol += t2 - t1;
     for (int s = 0; s < nsys; ++s) if (sel[s]) st[s].kits = its[s];
-    // gamma=0 (:260-283)
+    // gamma=0 (:260-283): R at X is the residual assembled with K above
     for (int s = 0; s < nsys; ++s) gam[s] = 0.0;
     if ((rc = set_gamma(m, gam))) return rc;
-    if ((rc = cost_eval(m, p, true))) return rc;
+    if ((rc = cost_eval(m, p, true, false))) return rc;
     for (int s = 0; s < nsys; ++s) {
       if (!sel[s]) continue;
       SysState& S = st[s];
@@ -1466,10 +1561,14 @@ static int assemble_uvh(ua_mesh* m, const ua_params* p, bool withK, bool useDir,
 }
 
 // CalcCostFunctionNRuvh.m:12-105 for the selected systems
-static int cost_eval_uvh(ua_mesh* m, const ua_params* p) {
+// uvh cost function at X + gamma dX; assembleR = false takes w->R as it stands
+// (the residual just assembled at X, i.e. gamma = 0).
+static int cost_eval_uvh(ua_mesh* m, const ua_params* p, bool assembleR = true) {
   Work* w = m->work;
-  int rc = assemble_uvh(m, p, false, true, false, false);
-  if (rc) return rc;
+  if (assembleR) {
+    int rc = assemble_uvh(m, p, false, true, false, false);
+    if (rc) return rc;
+  }
   k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, w->dof_con, w->lam,
                                              w->dlam, w->gamma, w->dX, w->part), ++g_launches;
   k_cost_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, w->nsys, w->sysv,
@@ -1558,7 +1657,7 @@ static int newton_run_uvh(ua_mesh* m, const ua_params* p, std::vector<ua_newton_
     for (int g1 = 0; g1 < 2; ++g1) {
       for (int s = 0; s < nsys; ++s) gam[s] = (double)g1;
       if ((rc = set_gamma(m, gam))) return rc;
-      if ((rc = cost_eval_uvh(m, p))) return rc;
+      if ((rc = cost_eval_uvh(m, p, g1 != 0))) return rc;  // R at gamma = 0 was assembled with K
       for (int s = 0; s < nsys; ++s) {
         if (!sel[s]) continue;
         const double rf = w->h_sysv[SV_FF * nsys + s], d2 = w->h_sysv[SV_FD * nsys + s];
@@ -1675,7 +1774,7 @@ extern "C" void ua_params_default(ua_params* p) {
   std::memcpy(p->uvhAcceptableWorkAndForceTolerances, a1, sizeof a1);
   std::memcpy(p->uvhAcceptableWorkOrForceTolerances, a2, sizeof a2);
   p->krylov_rtol = 1e-12; p->krylov_maxit = 20000; p->precision = UA_PREC_FP64;
-  p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1;
+  p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1; p->spmv_lanes = 0;
   p->krylov_precond = UA_PC_AMG;
 }
 
@@ -1794,24 +1893,15 @@ static int newton_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_
   double t1 = now_ms();
   float dev_ms = 0;
   cudaEventElapsedTime(&dev_ms, call_ev[0], call_ev[1]);
-  double kms[PK_COUNT] = {};
+  double kms[PK_COUNT] = {}, knnz[PK_COUNT] = {}, krows[PK_COUNT] = {};
   int kn[PK_COUNT] = {};
-  for (auto& mk : w->prof.marks) {
-    float t = 0;
-    cudaEventElapsedTime(&t, mk.second.first, mk.second.second);
-    kms[mk.first] += t;
-    kn[mk.first]++;
-  }
+  prof_collect(w, kms, kn, knnz, krows);
   bool all_conv = true;
   for (int s = 0; s < nsys; ++s) {
     if (rep[s]) {
       rep[s]->total_ms = t1 - t0;
       rep[s]->device_ms = dev_ms;
-      rep[s]->kasmK_ms = kms[PK_ASMK]; rep[s]->kasmK_n = kn[PK_ASMK];
-      rep[s]->kasmR_ms = kms[PK_ASMR]; rep[s]->kasmR_n = kn[PK_ASMR];
-      rep[s]->kspmv_ms = kms[PK_SPMV]; rep[s]->kspmv_n = kn[PK_SPMV];
-      rep[s]->kamgR_ms = kms[PK_AMGR]; rep[s]->kamgR_n = kn[PK_AMGR];
-      rep[s]->kamgP_ms = kms[PK_AMGP]; rep[s]->kamgP_n = kn[PK_AMGP];
+      prof_report(rep[s], kms, kn, knnz, krows);
       rep[s]->gpu_launches = (int)g_launches;
     }
     all_conv = all_conv && st[s].converged;
@@ -2303,24 +2393,15 @@ static int uvh_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs
   UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   float dev_ms = 0;
   cudaEventElapsedTime(&dev_ms, call_ev[0], call_ev[1]);
-  double kms[PK_COUNT] = {};
+  double kms[PK_COUNT] = {}, knnz[PK_COUNT] = {}, krows[PK_COUNT] = {};
   int kn[PK_COUNT] = {};
-  for (auto& mk : w->prof.marks) {
-    float t = 0;
-    cudaEventElapsedTime(&t, mk.second.first, mk.second.second);
-    kms[mk.first] += t;
-    kn[mk.first]++;
-  }
+  prof_collect(w, kms, kn, knnz, krows);
   bool all_conv = true;
   const double t1 = now_ms();
   for (int s = 0; s < nsys; ++s) {
     if (rep[s]) {
       rep[s]->total_ms = t1 - t0; rep[s]->device_ms = dev_ms;
-      rep[s]->kasmK_ms = kms[PK_ASMK]; rep[s]->kasmK_n = kn[PK_ASMK];
-      rep[s]->kasmR_ms = kms[PK_ASMR]; rep[s]->kasmR_n = kn[PK_ASMR];
-      rep[s]->kspmv_ms = kms[PK_SPMV]; rep[s]->kspmv_n = kn[PK_SPMV];
-      rep[s]->kamgR_ms = kms[PK_AMGR]; rep[s]->kamgR_n = kn[PK_AMGR];
-      rep[s]->kamgP_ms = kms[PK_AMGP]; rep[s]->kamgP_n = kn[PK_AMGP];
+      prof_report(rep[s], kms, kn, knnz, krows);
       rep[s]->gpu_launches = (int)g_launches;
     }
     all_conv = all_conv && st[s].converged;

@@ -72,7 +72,7 @@ class ua_params(C.Structure):
         ("uvhAcceptableWorkOrForceTolerances", C.c_double * 2),
         ("krylov_rtol", C.c_double), ("krylov_maxit", C.c_int32), ("precision", C.c_int32),
         ("patch_nodes", C.c_int32), ("verbose", C.c_int32), ("profile", C.c_int32),
-        ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32),
+        ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32), ("spmv_lanes", C.c_int32),
     ]
 
 
@@ -107,6 +107,7 @@ class ua_newton_report(C.Structure):
                 ("device_ms", C.c_double), ("kasmK_ms", C.c_double), ("kasmR_ms", C.c_double),
                 ("kspmv_ms", C.c_double), ("kasmK_n", C.c_int32), ("kasmR_n", C.c_int32), ("kspmv_n", C.c_int32),
                 ("kamgR_ms", C.c_double), ("kamgP_ms", C.c_double), ("kamgR_n", C.c_int32), ("kamgP_n", C.c_int32),
+                ("kwork_nnz", C.c_double * 5), ("kwork_rows", C.c_double * 5),
                 ("gpu_launches", C.c_int32),
                 ("n_iter_records", C.c_int32), ("iters_capacity", C.c_int32),
                 ("iters", C.POINTER(ua_newton_iter))]

@@ -75,6 +75,7 @@ class CtrlVar:
     profile: int = 0
     krylov_adaptive: int = 1
     krylov_precond: int = L.UA_PC_AMG
+    spmv_lanes: int = 0
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
@@ -375,7 +376,9 @@ def _report(rep, recs):
                         gamma=it.gamma, r0=it.r0, r=it.r, rForce=it.rForce, rWork=it.rWork))
     kern = dict(asmK_ms=rep.kasmK_ms, asmK_n=rep.kasmK_n, asmR_ms=rep.kasmR_ms, asmR_n=rep.kasmR_n,
                 spmv_ms=rep.kspmv_ms, spmv_n=rep.kspmv_n, amgR_ms=rep.kamgR_ms, amgR_n=rep.kamgR_n,
-                amgP_ms=rep.kamgP_ms, amgP_n=rep.kamgP_n)
+                amgP_ms=rep.kamgP_ms, amgP_n=rep.kamgP_n,
+                work_nnz=dict(zip(("asmK", "asmR", "spmv", "amgR", "amgP"), list(rep.kwork_nnz))),
+                work_rows=dict(zip(("asmK", "asmR", "spmv", "amgR", "amgP"), list(rep.kwork_rows))))
     return RunInfo(bool(rep.converged), rep.iterations, rep.backtrack_steps, rep.krylov_its_total,
                    rep.cauchy_fallbacks, bool(rep.retried), rep.r, rep.rForce, rep.rWork, rep.assembly_ms,
                    rep.solve_ms, rep.total_ms, rep.device_ms, kern, rep.gpu_launches, its)
