@@ -207,6 +207,31 @@ class ClockSampler:
 NAMES = ("h", "S", "B", "rho", "AGlen", "n", "C", "m")
 
 
+# ----------------------------------------------------------------------------- replicas over ranks
+
+def rank_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks_on(x, world, device):
+    """Max of a per-rank time over all ranks (an all-reduce on `device`; identity at world 1)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def replica_throughput(world, solves_per_rank, t_max_ms):
+    """Whole-job solves/s of `world` independent replicas that each ran `solves_per_rank`
+    solves, timed as the slowest rank."""
+    return world * solves_per_rank / (t_max_ms / 1000.0)
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -224,15 +249,10 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        rank_barrier(world)
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.item()
+        return max_over_ranks_on(x, world, dev)
 
     count = args.batch
     probs = synth.batch_problems(count)
@@ -357,10 +377,10 @@ def run_ours(args):
     t_b64 = max_over_ranks(sum(per_b64))
     t_plain = max_over_ranks(sum(per_plain))
     t_e2e = max_over_ranks(sum(per_e2e))
-    value = world * count * args.steps / (t_mx / 1000)
-    value_b64 = world * count * len(per_b64) / (t_b64 / 1000)
-    value_plain = world * len(sample) / (t_plain / 1000)
-    e2e_value = world * count * args.steps / (t_e2e / 1000)
+    value = replica_throughput(world, count * args.steps, t_mx)
+    value_b64 = replica_throughput(world, count * len(per_b64), t_b64)
+    value_plain = replica_throughput(world, len(sample), t_plain)
+    e2e_value = replica_throughput(world, count * args.steps, t_e2e)
 
     # roofline of the dominant kernel class (by measured device time).  Algorithmic bytes of each
     # timed launch follow from the tangent non-zeros and dof rows of the systems it processed

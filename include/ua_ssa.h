@@ -120,6 +120,7 @@ typedef struct ua_params {
                                   point Jacobi) */
     int32_t spmv_lanes;        /* lanes per row of the uv PCG/AMG row products: 0 = by element type
                                   (1 for P1, 2 for P2), else 1, 2, 4, 8, 16 or 32 */
+    int32_t asm_threads;       /* CTA size of the P1 uv assembly: 0 = default, else 128 or 256 */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

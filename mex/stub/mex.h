@@ -18,6 +18,8 @@ void mxSetField(mxArray* s, mwIndex i, const char* name, mxArray* v);
 int mxIsStruct(const mxArray* a);
 int mxIsDouble(const mxArray* a);
 int mxIsEmpty(const mxArray* a);
+int mxIsChar(const mxArray* a);
+char* mxArrayToString(const mxArray* a);
 double mxGetScalar(const mxArray* a);
 double* mxGetPr(const mxArray* a);
 size_t mxGetM(const mxArray* a);

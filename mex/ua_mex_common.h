@@ -21,14 +21,18 @@
 #include "mex.h"
 #include "ua_ssa.h"
 
-static ua_mesh* g_mesh = NULL;
-static uint64_t g_mesh_key = 0;
+/* one resident handle per dof count: [0] uv (ndof 2), [1] uvh (ndof 3) */
+static ua_mesh* g_meshes[2] = {NULL, NULL};
+static uint64_t g_mesh_keys[2] = {0, 0};
 static int g_locked = 0;
 
 static void ua_mex_cleanup(void) {
-    if (g_mesh) ua_mesh_destroy(g_mesh);
-    g_mesh = NULL;
-    g_mesh_key = 0;
+    int k;
+    for (k = 0; k < 2; ++k) {
+        if (g_meshes[k]) ua_mesh_destroy(g_meshes[k]);
+        g_meshes[k] = NULL;
+        g_mesh_keys[k] = 0;
+    }
 }
 
 /* FNV-1a over the raw bytes of the mesh arrays: detects a changed MUA. */
@@ -94,6 +98,47 @@ static void ua_mex_params(const mxArray* C, ua_params* p) {
             }
         }
     }
+    /* uvh: CtrlVar.theta, CtrlVar.SUPG.beta0, CtrlVar.uvh.SUPG.{tau,tauMultiplier} and the uvh
+     * tolerances (Ua2D_DefaultParameters.m:376-377, :494-505, :551-555) */
+    p->theta = ua_mex_scalar(C, "theta", p->theta);
+    {
+        const mxArray* sg = ua_mex_field(C, "SUPG", 0);
+        const mxArray* uvh = ua_mex_field(C, "uvh", 0);
+        const mxArray* us = uvh ? ua_mex_field(uvh, "SUPG", 0) : NULL;
+        if (sg) p->SUPG_beta0 = ua_mex_scalar(sg, "beta0", p->SUPG_beta0);
+        if (us) {
+            const mxArray* t = ua_mex_field(us, "tau", 0);
+            p->uvh_SUPG_tauMultiplier = ua_mex_scalar(us, "tauMultiplier", p->uvh_SUPG_tauMultiplier);
+            if (t && mxIsChar(t)) {
+                char* name = mxArrayToString(t);
+                if (name) {
+                    if (!strcmp(name, "taus")) p->uvh_SUPG_tau = 0;
+                    else if (!strcmp(name, "taut")) p->uvh_SUPG_tau = 1;
+                    else if (!strcmp(name, "tau1")) p->uvh_SUPG_tau = 2;
+                    else if (!strcmp(name, "tau2")) p->uvh_SUPG_tau = 3;
+                    mxFree(name);
+                }
+            }
+        }
+        /* a MATLAB string object is not readable through the C API: numeric override */
+        p->uvh_SUPG_tau = (int32_t)ua_mex_scalar(C, "GPUuvhSUPGtau", p->uvh_SUPG_tau);
+    }
+    p->uvhExitBackTrackingStepLength =
+        ua_mex_scalar(C, "uvhExitBackTrackingStepLength", p->uvhExitBackTrackingStepLength);
+    {
+        const char* pairs[4] = {"uvhDesiredWorkAndForceTolerances", "uvhDesiredWorkOrForceTolerances",
+                                "uvhAcceptableWorkAndForceTolerances", "uvhAcceptableWorkOrForceTolerances"};
+        double* dst[4] = {p->uvhDesiredWorkAndForceTolerances, p->uvhDesiredWorkOrForceTolerances,
+                          p->uvhAcceptableWorkAndForceTolerances, p->uvhAcceptableWorkOrForceTolerances};
+        int k;
+        for (k = 0; k < 4; ++k) {
+            const mxArray* f = ua_mex_field(C, pairs[k], 0);
+            if (f && mxGetNumberOfElements(f) == 2) {
+                dst[k][0] = mxGetPr(f)[0];
+                dst[k][1] = mxGetPr(f)[1];
+            }
+        }
+    }
     /* the GPU form selected by a CtrlVar.UseGPU-style switch (0=FP64, 1=mixed) */
     p->precision = (int32_t)ua_mex_scalar(C, "GPUPrecision", p->precision);
     p->krylov_rtol = ua_mex_scalar(C, "GPUKrylovTol", p->krylov_rtol);
@@ -101,8 +146,9 @@ static void ua_mex_params(const mxArray* C, ua_params* p) {
     p->krylov_adaptive = (int32_t)ua_mex_scalar(C, "GPUKrylovAdaptive", p->krylov_adaptive);
 }
 
-/* MUA -> cached device mesh (rebuilt when coordinates/connectivity change). */
-static ua_mesh* ua_mex_mesh(const mxArray* MUA) {
+/* MUA -> cached device mesh with ndof dofs per node (2: uv, 3: uvh), rebuilt
+ * when coordinates/connectivity change. */
+static ua_mesh* ua_mex_mesh_ndof(const mxArray* MUA, int ndof) {
     const mxArray* co = ua_mex_field(MUA, "coordinates", 1);
     const mxArray* cn = ua_mex_field(MUA, "connectivity", 1);
     size_t nn = mxGetM(co), ne = mxGetM(cn), nod = mxGetN(cn), i;
@@ -112,10 +158,12 @@ static ua_mesh* ua_mex_mesh(const mxArray* MUA) {
     int rc;
     if (mxGetN(co) != 2 || !mxIsDouble(co) || !mxIsDouble(cn))
         mexErrMsgIdAndTxt("Ua:mex:BadMUA", "MUA.coordinates must be Nnodes x 2 double, connectivity double");
+    const int slot = ndof == 3 ? 1 : 0;
     key = ua_mex_hash(mxGetPr(co), nn * 2 * sizeof(double), key);
     key = ua_mex_hash(mxGetPr(cn), ne * nod * sizeof(double), key);
-    if (g_mesh && key == g_mesh_key) return g_mesh;
-    ua_mex_cleanup();
+    if (g_meshes[slot] && key == g_mesh_keys[slot]) return g_meshes[slot];
+    if (g_meshes[slot]) ua_mesh_destroy(g_meshes[slot]);
+    g_meshes[slot] = NULL;
     conn = (int32_t*)mxMalloc(ne * nod * sizeof(int32_t));
     for (i = 0; i < ne * nod; ++i) conn[i] = (int32_t)mxGetPr(cn)[i];
     d.nnodes = (int32_t)nn;
@@ -124,22 +172,24 @@ static ua_mesh* ua_mex_mesh(const mxArray* MUA) {
     d.index_base = 1;
     d.coordinates = mxGetPr(co);
     d.connectivity = conn;
-    rc = ua_mesh_create(&d, 2, 0, &g_mesh);
+    rc = ua_mesh_create(&d, ndof, 0, &g_meshes[slot]);
     mxFree(conn);
     if (rc != UA_OK) {
-        g_mesh = NULL;
+        g_meshes[slot] = NULL;
         mexErrMsgIdAndTxt(rc == UA_ERR_BAD_MESH ? "Ua:TestAndCorrectForInsideOutElements:InsideOutelements"
                                                 : "Ua:mex:MeshCreate",
                           "%s", ua_last_error());
     }
-    g_mesh_key = key;
+    g_mesh_keys[slot] = key;
     if (!g_locked) {
         mexLock();
         mexAtExit(ua_mex_cleanup);
         g_locked = 1;
     }
-    return g_mesh;
+    return g_meshes[slot];
 }
+
+static ua_mesh* ua_mex_mesh(const mxArray* MUA) { return ua_mex_mesh_ndof(MUA, 2); }
 
 /* A nodal field: Nn-vector, or a scalar expanded as uv.m:34-40 does for m and n. */
 static const double* ua_mex_nodal(const mxArray* F, const char* name, size_t nn, double** owned) {
@@ -154,6 +204,19 @@ static const double* ua_mex_nodal(const mxArray* F, const char* name, size_t nn,
     }
     mexErrMsgIdAndTxt("Ua:mex:BadField", "F.%s must have Nnodes elements", name);
     return NULL;
+}
+
+/* dadh of uvhMatrixAssembly.m:152-158: F1.dasdh + F1.dabdh when
+ * CtrlVar.MassBalanceGeometryFeedback is 3, else none (NULL = zero). */
+static const double* ua_mex_dadh(const mxArray* C, const mxArray* F1, size_t nn, double** owned) {
+    const mxArray *a = ua_mex_field(F1, "dasdh", 0), *b = ua_mex_field(F1, "dabdh", 0);
+    size_t i;
+    *owned = NULL;
+    if ((int)ua_mex_scalar(C, "MassBalanceGeometryFeedback", 0) != 3) return NULL;
+    *owned = (double*)mxCalloc(nn, sizeof(double));
+    if (a && mxGetNumberOfElements(a) == nn) for (i = 0; i < nn; ++i) (*owned)[i] += mxGetPr(a)[i];
+    if (b && mxGetNumberOfElements(b) == nn) for (i = 0; i < nn; ++i) (*owned)[i] += mxGetPr(b)[i];
+    return *owned;
 }
 
 /* BCs node lists (double, 1-based) -> int32 arrays owned by the caller. */
@@ -191,6 +254,9 @@ static void ua_mex_bcs(const mxArray* B, ua_bcs* b) {
     for (i = 0; i < b->n_vfixed; ++i) ((int32_t*)b->vfixed_node)[i] -= 1;
     for (i = 0; i < b->n_utied; ++i) { ((int32_t*)b->utied_a)[i] -= 1; ((int32_t*)b->utied_b)[i] -= 1; }
     for (i = 0; i < b->n_vtied; ++i) { ((int32_t*)b->vtied_a)[i] -= 1; ((int32_t*)b->vtied_b)[i] -= 1; }
+    b->hfixed_node = ua_mex_nodes(B, "hFixedNode", &b->n_hfixed);
+    b->hfixed_value = ua_mex_values(B, "hFixedValue");
+    for (i = 0; i < b->n_hfixed; ++i) ((int32_t*)b->hfixed_node)[i] -= 1;
 }
 
 static void ua_mex_fail(int rc) {
@@ -225,6 +291,35 @@ static mxArray* ua_mex_sparse(ua_mesh* m, int32_t n, const double* vals) {
     }
     jc[n] = (mwIndex)out;
     mxFree(rp); mxFree(ci);
+    return S;
+}
+
+/* CSR values of an unsymmetric tangent (uvh) on the structural pattern ->
+ * MATLAB sparse: a column-count pass, then the transpose (CSC, sorted rows,
+ * no explicit zeros). */
+static mxArray* ua_mex_sparse_unsym(ua_mesh* m, int32_t n, const double* vals) {
+    int64_t nnz = 0, i, k, out = 0;
+    int64_t *rp, *ci;
+    mwIndex *jc, *ir, *next;
+    mxArray* S;
+    double* pr;
+    ua_mesh_pattern(m, 0, &nnz, NULL, NULL);
+    rp = (int64_t*)mxMalloc((n + 1) * sizeof(int64_t));
+    ci = (int64_t*)mxMalloc(nnz * sizeof(int64_t));
+    ua_mesh_pattern(m, 0, &nnz, rp, ci);
+    for (k = 0; k < nnz; ++k) out += vals[k] != 0.0;
+    S = mxCreateSparse(n, n, out > 0 ? out : 1, mxREAL);
+    jc = mxGetJc(S); ir = mxGetIr(S); pr = mxGetPr(S);
+    next = (mwIndex*)mxCalloc(n + 1, sizeof(mwIndex));
+    for (i = 0; i < n; ++i)
+        for (k = rp[i]; k < rp[i + 1]; ++k)
+            if (vals[k] != 0.0) next[ci[k] + 1]++;
+    for (i = 0; i < n; ++i) next[i + 1] += next[i];
+    for (i = 0; i <= n; ++i) jc[i] = next[i];
+    for (i = 0; i < n; ++i)  /* rows in increasing order: each column's rows come out sorted */
+        for (k = rp[i]; k < rp[i + 1]; ++k)
+            if (vals[k] != 0.0) { ir[next[ci[k]]] = (mwIndex)i; pr[next[ci[k]]] = vals[k]; next[ci[k]]++; }
+    mxFree(next); mxFree(rp); mxFree(ci);
     return S;
 }
 

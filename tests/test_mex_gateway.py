@@ -9,7 +9,8 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-@pytest.mark.parametrize("src", ["uvMatrixAssemblySSTREAM_mex.c", "SSTREAM2dNR2_mex.c"])
+@pytest.mark.parametrize("src", ["uvMatrixAssemblySSTREAM_mex.c", "SSTREAM2dNR2_mex.c", "uvhAssembly_mex.c",
+                                 "SSTREAM_TransientImplicit_mex.c"])
 def test_gateway_compiles(src):
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:

@@ -51,6 +51,7 @@ struct AmgLevel {
   // dof-level CSR of a coarse level, same layout rule as the finest level
   int *rowptr = nullptr, *colind = nullptr;
   int* dof_sys = nullptr;
+  int* d_dof_off = nullptr;               // per-system dof offsets on the device
   int *rb_start = nullptr, *rb_sys = nullptr;
   int nrb = 0;
   int* cmap = nullptr;                    // this level's dof -> next level's dof
@@ -282,6 +283,7 @@ int amg_setup(ua_mesh* m) {
     prp[l] = a->lev[l].rowptr;
     pci[l] = a->lev[l].colind;
     pdo[l] = upload(m, a, a->lev[l].dof_off, ok);
+    a->lev[l].d_dof_off = pdo[l];
   }
   a->d_lev_b = upload(m, a, pb, ok);
   a->d_lev_x2 = upload(m, a, px2, ok);
@@ -440,24 +442,54 @@ __global__ void __launch_bounds__(256) k_amg_dense_apply(const int* sel, const i
 // Split V-cycle kernels (every level; coalesced row blocks with LPR lanes per
 // row instead of one thread per aggregate).  Residual of the pre-smoothed
 // vector of level l: res = mask(b - A x), for systems deeper than l.
+// Row product in the uv block layout of every level: row (c, I) holds the u
+// block then the v block of deg(I) entries on the same node columns, v column
+// = u column + nhalf, so only the u block's indices are read (used for FP64
+// values, where it is faster).
+template <typename KT, typename XT, int LPR>
+__device__ __forceinline__ double row_dot_uv(const int* rowptr, const int* colind, const KT* A, const XT* x, int row,
+                                             bool valid, int lane, int nhalf) {
+  double acc = 0;
+  if (valid) {
+    const int r0 = rowptr[row], deg = (rowptr[row + 1] - r0) >> 1;
+    for (int k = lane; k < deg; k += LPR) {
+      const int j = colind[r0 + k];
+      acc += (double)A[r0 + k] * (double)x[j] + (double)A[r0 + deg + k] * (double)x[j + nhalf];
+    }
+  }
+#pragma unroll
+  for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+  return acc;
+}
+
+// Plain CSR row product (every index read); the form that is faster for FP32 values.
+template <typename KT, typename XT, int LPR>
+__device__ __forceinline__ double row_dot_csr(const int* rowptr, const int* colind, const KT* A, const XT* x, int row,
+                                              bool valid, int lane) {
+  double acc = 0;
+  if (valid)
+    for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) acc += (double)A[q] * (double)x[colind[q]];
+#pragma unroll
+  for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+  return acc;
+}
+
 template <typename KT, typename VT, int LPR>
 __global__ void __launch_bounds__(256) k_amg_residual(const int* rb_start, const int* rb_sys, const int* sel,
                                                       const int* done, const int* depth, int l, const int* rowptr,
                                                       const int* colind, const KT* A, const VT* b, const VT* x,
-                                                      const unsigned char* cmask, VT* res) {
+                                                      const unsigned char* cmask, VT* res, const int* dof_off) {
   const int blk = blockIdx.x;
   const int s = rb_sys[blk];
   if (!sel[s] || done[s] || depth[s] <= l) return;
   const int rs = rb_start[blk], re = rb_start[blk + 1];
+  const int nhalf = (dof_off[s + 1] - dof_off[s]) >> 1;
   const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
   for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
     const int row = row0 + grp;
     const bool valid = row < re;
-    double ax = 0;
-    if (valid)
-      for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) ax += (double)A[q] * (double)x[colind[q]];
-#pragma unroll
-    for (int o = LPR / 2; o > 0; o >>= 1) ax += __shfl_down_sync(0xffffffffu, ax, o, LPR);
+    const double ax = sizeof(KT) == 8 ? row_dot_uv<KT, VT, LPR>(rowptr, colind, A, x, row, valid, lane, nhalf)
+                                      : row_dot_csr<KT, VT, LPR>(rowptr, colind, A, x, row, valid, lane);
     if (valid && lane == 0) res[row] = (VT)((cmask && cmask[row]) ? 0.0 : (double)b[row] - ax);
   }
 }
@@ -498,21 +530,19 @@ __global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const i
                                                     const int* done, const int* depth, int l, const int* rowptr,
                                                     const int* colind, const KT* A, const VT* b, const VT* xp,
                                                     const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
-                                                    double* part) {
+                                                    double* part, const int* dof_off) {
   const int blk = blockIdx.x;
   const int s = rb_sys[blk];
   double rz = 0;
   if (sel[s] && !done[s] && depth[s] > l) {
     const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int nhalf = (dof_off[s + 1] - dof_off[s]) >> 1;
     const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
     for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
       const int row = row0 + grp;
       const bool valid = row < re;
-      double ax = 0;
-      if (valid)
-        for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) ax += (double)A[q] * (double)xp[colind[q]];
-#pragma unroll
-      for (int o = LPR / 2; o > 0; o >>= 1) ax += __shfl_down_sync(0xffffffffu, ax, o, LPR);
+      const double ax = sizeof(KT) == 8 ? row_dot_uv<KT, VT, LPR>(rowptr, colind, A, xp, row, valid, lane, nhalf)
+                                        : row_dot_csr<KT, VT, LPR>(rowptr, colind, A, xp, row, valid, lane);
       if (valid && lane == 0) {
         const double v =
             (cmask && cmask[row]) ? 0.0 : (double)xp[row] + (double)invd[row] * ((double)b[row] - ax);
@@ -590,13 +620,14 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
   auto X = [&](int l) { return l == 0 ? (VT*)v.x0 : (VT*)a->lev[l].x; };
   auto W = [&](int l) { return l == 0 ? (VT*)v.tmp : (VT*)a->lev[l].x2; };
   auto mask = [&](int l) { return l == 0 ? v.cmask : nullptr; };
+  auto doff = [&](int l) { return (const int*)a->lev[l].d_dof_off; };
   const int lpr0 = v.lpr;
   for (int l = 0; l + 1 < nl; ++l) {  // down: residual of level l, aggregated into level l+1
     const AmgLevel& C = a->lev[l + 1];
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 0);
     dispatch_lpr(lpr0, [&](auto L) {
       k_amg_residual<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
-          rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l));
+          rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l), doff(l));
     });
     ++*launches;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 1);
@@ -618,7 +649,7 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     dispatch_lpr(lpr0, [&](auto L) {
       k_amg_smooth<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
           rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), (const VT*)F.invd, mask(l),
-          out, pcopy, part);
+          out, pcopy, part, doff(l));
     });
     ++*launches;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 1, 1);

@@ -25,60 +25,39 @@ struct ElemIdx {
   }
 };
 
-// Element computation.  Follows uvMatrixAssemblySSTREAM.m :168-455 for one
-// element: interpolation and clamps (:186-254), post-2025 flotation at the
-// integration points (:300-310), nodal-derivative sums (:332-347), drag and
-// viscosity (:351-353), tangent blocks including the Newton viscosity terms
-// (:362-425) and residual terms (:431-449).
-//
-// The Newton viscosity terms E11..E22 are written as the rank-one product
-// 2 h E P_I P_J with P_u = (2exx+eyy) dN/dx + exy dN/dy and
-// P_v = (2eyy+exx) dN/dy + exy dN/dx, which is the same expression as
-// :398-417 regrouped (E11 = h(4exx+2eyy) Deu dNI/dx + 2h exy Deu dNI/dy with
-// Deu = E P_u(J)).  The tangent is produced symmetric, which is what
-// (K+K.')/2 at :530-531 yields.
+// derivVector.m:96-109 at integration point ip
+template <int NOD>
+__device__ __forceinline__ void uv_deriv(const QuadTable& Q, int ip, const double (&xe)[NOD], const double (&ye)[NOD],
+                                         double (&Dx)[NOD], double (&Dy)[NOD], double& detJ) {
+  double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+#pragma unroll
+  for (int a = 0; a < NOD; ++a) {
+    J11 += xe[a] * Q.der[ip][0][a];
+    J12 += ye[a] * Q.der[ip][0][a];
+    J21 += xe[a] * Q.der[ip][1][a];
+    J22 += ye[a] * Q.der[ip][1][a];
+  }
+  detJ = J11 * J22 - J12 * J21;
+#pragma unroll
+  for (int a = 0; a < NOD; ++a) {
+    Dx[a] = (J22 * Q.der[ip][0][a] - J12 * Q.der[ip][1][a]) / detJ;
+    Dy[a] = (-J21 * Q.der[ip][0][a] + J11 * Q.der[ip][1][a]) / detJ;
+  }
+}
+
+// Contribution of integration point ip to the element tangent and residual
+// parts (accumulated into the outputs).
 template <int NOD, bool WITHK, typename KT>
-__device__ __forceinline__ void uv_element(const QuadTable& Q, const UvPhys& P, const SysScal& S,
-                                           const double (&xe)[NOD], const double (&ye)[NOD],
-                                           const double (&hn)[NOD], const double (&sn)[NOD],
-                                           const double (&un)[NOD], const double (&vn)[NOD],
-                                           const double (&Cn)[NOD], const double (&mn)[NOD],
-                                           const double (&An)[NOD], const double (&nn)[NOD],
-                                           const double (&Sn)[NOD], const double (&Bn)[NOD],
-                                           const double (&rn)[NOD], KT* Kuu, KT* Kvv, KT* Kuv,
-                                           double* Tx, double* Fx, double* Ty, double* Fy) {
+__device__ __forceinline__ void uv_ip(const QuadTable& Q, const UvPhys& P, const SysScal& S, int ip,
+                                      const double (&Dx)[NOD], const double (&Dy)[NOD], double detJ,
+                                      const double (&hn)[NOD], const double (&sn)[NOD], const double (&un)[NOD],
+                                      const double (&vn)[NOD], const double (&Cn)[NOD], const double (&mn)[NOD],
+                                      const double (&An)[NOD], const double (&nn)[NOD], const double (&Sn)[NOD],
+                                      const double (&Bn)[NOD], const double (&rn)[NOD], KT* Kuu, KT* Kvv, KT* Kuv,
+                                      double* Tx, double* Fx, double* Ty, double* Fy) {
   using I = ElemIdx<NOD>;
   const double rhow = S.rhow, g = S.g, ca = S.ca, sa = S.sa;
-#pragma unroll
-  for (int a = 0; a < NOD; ++a) { Tx[a] = 0; Fx[a] = 0; Ty[a] = 0; Fy[a] = 0; }
-  if (WITHK) {
-#pragma unroll
-    for (int i = 0; i < I::NS; ++i) { Kuu[i] = 0; Kvv[i] = 0; }
-#pragma unroll
-    for (int i = 0; i < NOD * NOD; ++i) Kuv[i] = 0;
-  }
-  double Dx[NOD], Dy[NOD], detJ = 0;
-  auto deriv = [&](int ip) {  // derivVector.m:96-109
-    double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
-#pragma unroll
-    for (int a = 0; a < NOD; ++a) {
-      J11 += xe[a] * Q.der[ip][0][a];
-      J12 += ye[a] * Q.der[ip][0][a];
-      J21 += xe[a] * Q.der[ip][1][a];
-      J22 += ye[a] * Q.der[ip][1][a];
-    }
-    detJ = J11 * J22 - J12 * J21;
-#pragma unroll
-    for (int a = 0; a < NOD; ++a) {
-      Dx[a] = (J22 * Q.der[ip][0][a] - J12 * Q.der[ip][1][a]) / detJ;
-      Dy[a] = (-J21 * Q.der[ip][0][a] + J11 * Q.der[ip][1][a]) / detJ;
-    }
-  };
-  if (NOD == 3) deriv(0);  // P1: constant over the element
-  const int nip = Q.nip;
-#pragma unroll 1
-  for (int ip = 0; ip < nip; ++ip) {
-    if (NOD != 3) deriv(ip);
+  {
     double N[NOD];
 #pragma unroll
     for (int a = 0; a < NOD; ++a) N[a] = Q.fun[ip][a];
@@ -196,7 +175,55 @@ __device__ __forceinline__ void uv_element(const QuadTable& Q, const UvPhys& P, 
 }
 
 template <int NOD, bool WITHK, typename KT>
-__global__ void __launch_bounds__(128) uv_patch_kernel(DevMesh M, QuadTable Q, UvPhys P, UvIn in, UvOut out) {
+__device__ __forceinline__ void uv_zero(KT* Kuu, KT* Kvv, KT* Kuv, double* Tx, double* Fx, double* Ty, double* Fy) {
+  using I = ElemIdx<NOD>;
+#pragma unroll
+  for (int a = 0; a < NOD; ++a) { Tx[a] = 0; Fx[a] = 0; Ty[a] = 0; Fy[a] = 0; }
+  if (WITHK) {
+#pragma unroll
+    for (int i = 0; i < I::NS; ++i) { Kuu[i] = 0; Kvv[i] = 0; }
+#pragma unroll
+    for (int i = 0; i < NOD * NOD; ++i) Kuv[i] = 0;
+  }
+}
+
+// Element computation.  Follows uvMatrixAssemblySSTREAM.m :168-455 for one
+// element: interpolation and clamps (:186-254), post-2025 flotation at the
+// integration points (:300-310), nodal-derivative sums (:332-347), drag and
+// viscosity (:351-353), tangent blocks including the Newton viscosity terms
+// (:362-425) and residual terms (:431-449).
+//
+// The Newton viscosity terms E11..E22 are written as the rank-one product
+// 2 h E P_I P_J with P_u = (2exx+eyy) dN/dx + exy dN/dy and
+// P_v = (2eyy+exx) dN/dy + exy dN/dx, which is the same expression as
+// :398-417 regrouped (E11 = h(4exx+2eyy) Deu dNI/dx + 2h exy Deu dNI/dy with
+// Deu = E P_u(J)).  The tangent is produced symmetric, which is what
+// (K+K.')/2 at :530-531 yields.
+template <int NOD, bool WITHK, typename KT>
+__device__ __forceinline__ void uv_element(const QuadTable& Q, const UvPhys& P, const SysScal& S,
+                                           const double (&xe)[NOD], const double (&ye)[NOD],
+                                           const double (&hn)[NOD], const double (&sn)[NOD],
+                                           const double (&un)[NOD], const double (&vn)[NOD],
+                                           const double (&Cn)[NOD], const double (&mn)[NOD],
+                                           const double (&An)[NOD], const double (&nn)[NOD],
+                                           const double (&Sn)[NOD], const double (&Bn)[NOD],
+                                           const double (&rn)[NOD], KT* Kuu, KT* Kvv, KT* Kuv,
+                                           double* Tx, double* Fx, double* Ty, double* Fy) {
+  uv_zero<NOD, WITHK, KT>(Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
+  double Dx[NOD], Dy[NOD], detJ = 0;
+  if (NOD == 3) uv_deriv<NOD>(Q, 0, xe, ye, Dx, Dy, detJ);  // P1: constant over the element
+#pragma unroll 1
+  for (int ip = 0; ip < Q.nip; ++ip) {
+    if (NOD != 3) uv_deriv<NOD>(Q, ip, xe, ye, Dx, Dy, detJ);
+    uv_ip<NOD, WITHK, KT>(Q, P, S, ip, Dx, Dy, detJ, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv, Kuv, Tx,
+                          Fx, Ty, Fy);
+  }
+}
+
+// P1 runs integration-point-parallel (at most 128 registers: two 256-thread or four
+// 128-thread blocks per SM); P2 keeps one element per thread in 128-thread blocks.
+template <int NOD, bool WITHK, typename KT>
+__global__ void __launch_bounds__(NOD == 3 ? 256 : 128, NOD == 3 ? 2 : 1) uv_patch_kernel(DevMesh M, QuadTable Q, UvPhys P, UvIn in, UvOut out) {
   using I = ElemIdx<NOD>;
   extern __shared__ __align__(16) unsigned char smem[];
   const int p = blockIdx.x;
@@ -212,10 +239,10 @@ __global__ void __launch_bounds__(128) uv_patch_kernel(DevMesh M, QuadTable Q, U
   const int voff = uoff + nn_s;
   const double gam = in.gamma ? in.gamma[s] : 0.0;
   const SysScal S = in.scal[s];
-  for (int t = threadIdx.x; t < ne; t += blockDim.x) {
-    const int e = __ldg(M.patch_elems + e0 + t);
-    double xe[NOD], ye[NOD], hn[NOD], sn[NOD], un[NOD], vn[NOD], Cn[NOD], mn[NOD], An[NOD], nn[NOD], Sn[NOD],
-        Bn[NOD], rn[NOD];
+  // nodal values of element e (u, v at X + gamma dX)
+  auto gather = [&](int e, double (&xe)[NOD], double (&ye)[NOD], double (&hn)[NOD], double (&sn)[NOD],
+                    double (&un)[NOD], double (&vn)[NOD], double (&Cn)[NOD], double (&mn)[NOD], double (&An)[NOD],
+                    double (&nn)[NOD], double (&Sn)[NOD], double (&Bn)[NOD], double (&rn)[NOD]) {
 #pragma unroll
     for (int a = 0; a < NOD; ++a) {
       const int gnode = __ldg(M.conn + (size_t)a * M.ne + e);
@@ -229,10 +256,9 @@ __global__ void __launch_bounds__(128) uv_patch_kernel(DevMesh M, QuadTable Q, U
       Sn[a] = __ldg(in.S + gnode); Bn[a] = __ldg(in.B + gnode);
       rn[a] = __ldg(in.rho + gnode);
     }
-    KT Kuu[I::NS], Kvv[I::NS], Kuv[NOD * NOD];
-    double Tx[NOD], Fx[NOD], Ty[NOD], Fy[NOD];
-    uv_element<NOD, WITHK, KT>(Q, P, S, xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv, Kuv, Tx, Fx,
-                               Ty, Fy);
+  };
+  auto store = [&](int t, const KT* Kuu, const KT* Kvv, const KT* Kuv, const double* Tx, const double* Fx,
+                   const double* Ty, const double* Fy) {
     if (WITHK) {
 #pragma unroll
       for (int i = 0; i < I::NS; ++i) { sK[i * E + t] = Kuu[i]; sK[(I::NS + i) * E + t] = Kvv[i]; }
@@ -245,6 +271,59 @@ __global__ void __launch_bounds__(128) uv_patch_kernel(DevMesh M, QuadTable Q, U
       sR[(1 * NOD + a) * E + t] = Fx[a];
       sR[(2 * NOD + a) * E + t] = Ty[a];
       sR[(3 * NOD + a) * E + t] = Fy[a];
+    }
+  };
+  if constexpr (NOD == 3) {
+    // P1: the integration points of an element on IPL lanes (one each), summed
+    // by a fixed-order butterfly; no loop-carried element state, so far fewer
+    // registers per thread than an element-per-thread loop.
+    constexpr int IPL = 8;
+    const int ip = threadIdx.x % IPL, grp = threadIdx.x / IPL, ngrp = blockDim.x / IPL;
+    for (int base = 0; base < ne; base += ngrp) {  // same trip count for every thread of the block
+      const int t = base + grp;
+      KT Kuu[I::NS], Kvv[I::NS], Kuv[NOD * NOD];
+      double Tx[NOD], Fx[NOD], Ty[NOD], Fy[NOD];
+      uv_zero<NOD, WITHK, KT>(Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
+      if (t < ne && ip < Q.nip) {
+        double xe[NOD], ye[NOD], hn[NOD], sn[NOD], un[NOD], vn[NOD], Cn[NOD], mn[NOD], An[NOD], nn[NOD], Sn[NOD],
+            Bn[NOD], rn[NOD];
+        gather(__ldg(M.patch_elems + e0 + t), xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn);
+        double Dx[NOD], Dy[NOD], detJ;
+        uv_deriv<NOD>(Q, 0, xe, ye, Dx, Dy, detJ);
+        uv_ip<NOD, WITHK, KT>(Q, P, S, ip, Dx, Dy, detJ, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv, Kuv,
+                              Tx, Fx, Ty, Fy);
+      }
+#pragma unroll
+      for (int o = IPL / 2; o > 0; o >>= 1) {
+        if (WITHK) {
+#pragma unroll
+          for (int i = 0; i < I::NS; ++i) {
+            Kuu[i] += __shfl_xor_sync(0xffffffffu, Kuu[i], o);
+            Kvv[i] += __shfl_xor_sync(0xffffffffu, Kvv[i], o);
+          }
+#pragma unroll
+          for (int i = 0; i < NOD * NOD; ++i) Kuv[i] += __shfl_xor_sync(0xffffffffu, Kuv[i], o);
+        }
+#pragma unroll
+        for (int a = 0; a < NOD; ++a) {
+          Tx[a] += __shfl_xor_sync(0xffffffffu, Tx[a], o);
+          Fx[a] += __shfl_xor_sync(0xffffffffu, Fx[a], o);
+          Ty[a] += __shfl_xor_sync(0xffffffffu, Ty[a], o);
+          Fy[a] += __shfl_xor_sync(0xffffffffu, Fy[a], o);
+        }
+      }
+      if (t < ne && ip == 0) store(t, Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
+    }
+  } else {
+    for (int t = threadIdx.x; t < ne; t += blockDim.x) {
+      double xe[NOD], ye[NOD], hn[NOD], sn[NOD], un[NOD], vn[NOD], Cn[NOD], mn[NOD], An[NOD], nn[NOD], Sn[NOD],
+          Bn[NOD], rn[NOD];
+      gather(__ldg(M.patch_elems + e0 + t), xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn);
+      KT Kuu[I::NS], Kvv[I::NS], Kuv[NOD * NOD];
+      double Tx[NOD], Fx[NOD], Ty[NOD], Fy[NOD];
+      uv_element<NOD, WITHK, KT>(Q, P, S, xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv, Kuv, Tx, Fx,
+                                 Ty, Fy);
+      store(t, Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
     }
   }
   __syncthreads();
@@ -309,23 +388,28 @@ size_t uv_patch_smem(int nod, bool withK, bool fp32, int E) {
 }
 
 template <int NOD, bool WITHK, typename KT>
-static cudaError_t launch_t(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out) {
+static cudaError_t launch_t(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, int threads) {
   size_t sm = uv_patch_smem(NOD, WITHK, sizeof(KT) == 4, m->dm.max_patch_elems);
   auto kern = uv_patch_kernel<NOD, WITHK, KT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  kern<<<m->dm.npatch, 128, sm, m->stream>>>(m->dm, quad_table(NOD), P, in, out);
+  // all of the unified L1/shared storage as shared memory: several patch blocks per SM
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
+  kern<<<m->dm.npatch, NOD == 3 ? threads : 128, sm, m->stream>>>(m->dm, quad_table(NOD), P, in, out);
   return cudaGetLastError();
 }
 
+// threads: CTA size of the P1 kernels (128 or 256; 0 = 256 with K, 128 residual-only)
 cudaError_t launch_uv_assembly(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, bool withK,
-                               bool fp32K) {
+                               bool fp32K, int threads) {
+  if (threads != 128 && threads != 256) threads = withK ? 256 : 128;
   if (m->nod == 3) {
-    if (!withK) return launch_t<3, false, double>(m, P, in, out);
-    return fp32K ? launch_t<3, true, float>(m, P, in, out) : launch_t<3, true, double>(m, P, in, out);
+    if (!withK) return launch_t<3, false, double>(m, P, in, out, threads);
+    return fp32K ? launch_t<3, true, float>(m, P, in, out, threads) : launch_t<3, true, double>(m, P, in, out, threads);
   }
-  if (!withK) return launch_t<6, false, double>(m, P, in, out);
-  return fp32K ? launch_t<6, true, float>(m, P, in, out) : launch_t<6, true, double>(m, P, in, out);
+  if (!withK) return launch_t<6, false, double>(m, P, in, out, 128);
+  return fp32K ? launch_t<6, true, float>(m, P, in, out, 128) : launch_t<6, true, double>(m, P, in, out, 128);
 }
 
 }  // namespace ua

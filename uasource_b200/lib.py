@@ -72,7 +72,7 @@ class ua_params(C.Structure):
         ("uvhAcceptableWorkOrForceTolerances", C.c_double * 2),
         ("krylov_rtol", C.c_double), ("krylov_maxit", C.c_int32), ("precision", C.c_int32),
         ("patch_nodes", C.c_int32), ("verbose", C.c_int32), ("profile", C.c_int32),
-        ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32), ("spmv_lanes", C.c_int32),
+        ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32), ("spmv_lanes", C.c_int32), ("asm_threads", C.c_int32),
     ]
 
 

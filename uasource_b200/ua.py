@@ -76,6 +76,7 @@ class CtrlVar:
     krylov_adaptive: int = 1
     krylov_precond: int = L.UA_PC_AMG
     spmv_lanes: int = 0
+    asm_threads: int = 0
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
