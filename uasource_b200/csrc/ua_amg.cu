@@ -52,6 +52,7 @@ struct AmgLevel {
   int *rowptr = nullptr, *colind = nullptr;
   int* dof_sys = nullptr;
   int* d_dof_off = nullptr;               // per-system dof offsets on the device
+  int* d_knz_off = nullptr;               // per-system non-zero offsets (uvh finest level)
   int *rb_start = nullptr, *rb_sys = nullptr;
   int nrb = 0;
   int* cmap = nullptr;                    // this level's dof -> next level's dof
@@ -71,6 +72,9 @@ struct Amg {
   void **d_lev_b = nullptr, **d_lev_x2 = nullptr, **d_lev_A = nullptr;
   int **d_lev_rowptr = nullptr, **d_lev_colind = nullptr, **d_lev_dofoff = nullptr;
   size_t bytes = 0;
+  // uvh handles: constraint mask and vectors of the velocity rows (2-dof layout)
+  unsigned char* uvh_mask = nullptr;
+  double *uvh_r = nullptr, *uvh_x0 = nullptr, *uvh_z = nullptr, *uvh_t = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -164,7 +168,7 @@ static void level_csr(AmgLevel& L, const std::vector<int>& gptr, const std::vect
 int amg_setup(ua_mesh* m) {
   if (m->amg) return UA_OK;
   if (m->amg_failed) return UA_ERR_INVALID;
-  if (m->ndof != 2) return set_error(UA_ERR_INVALID, "the AMG preconditioner serves the uv tangent");
+  if (m->ndof != 2 && m->ndof != 3) return set_error(UA_ERR_INVALID, "the AMG preconditioner needs uv or uvh dofs");
   const int nsys = m->dm.nsys;
   Amg* a = new Amg();
   a->nsys = nsys;
@@ -220,14 +224,29 @@ int amg_setup(ua_mesh* m) {
     L.node_off = g_off[l];
     std::vector<int> rowptr, colind, dof_sys;
     level_csr(L, g_ptr[l], g_col[l], nsys, rowptr, colind, dof_sys);
-    if (l == 0 && (L.ndof != m->ndof_total || L.nnz != m->nnz_total)) return fail("fine level does not match the handle");
+    if (l == 0 && m->ndof == 2 && (L.ndof != m->ndof_total || L.nnz != m->nnz_total))
+      return fail("fine level does not match the handle");
     std::vector<int> rb_start, rb_sys;
     for (int s = 0; s < nsys; ++s)
       for (int r = L.dof_off[s]; r < L.dof_off[s + 1]; r += kAmgRB) { rb_start.push_back(r); rb_sys.push_back(s); }
     rb_start.push_back(L.ndof);
     L.nrb = (int)rb_sys.size();
     L.invd = dalloc(m, a, sizeof(double) * (size_t)L.ndof, ok);
-    if (l > 0) {  // the fine level uses the handle's tangent structure and PCG vectors
+    if (l == 0 && m->ndof == 3) {
+      // uvh handle: the finest level is the velocity block, held apart from the 3-dof
+      // tangent (values extracted per Newton step), with its own rows and vectors
+      L.rb_start = upload(m, a, rb_start, ok);
+      L.rb_sys = upload(m, a, rb_sys, ok);
+      L.dof_sys = upload(m, a, dof_sys, ok);
+      L.rowptr = upload(m, a, rowptr, ok);
+      L.colind = upload(m, a, colind, ok);
+      L.d_knz_off = upload(m, a, L.knz_off, ok);
+      L.A = dalloc(m, a, sizeof(double) * (size_t)L.nnz, ok);
+      a->uvh_mask = (unsigned char*)dalloc(m, a, (size_t)L.ndof, ok);
+      for (double** v : {&a->uvh_r, &a->uvh_x0, &a->uvh_z, &a->uvh_t})
+        *v = (double*)dalloc(m, a, sizeof(double) * (size_t)L.ndof, ok);
+    }
+    if (l > 0) {  // the fine level of a uv handle uses the handle's tangent structure and PCG vectors
       L.rb_start = upload(m, a, rb_start, ok);
       L.rb_sys = upload(m, a, rb_sys, ok);
       L.dof_sys = upload(m, a, dof_sys, ok);
@@ -662,6 +681,75 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
 int amg_vcycle(ua_mesh* m, bool fp32, const AmgPcgView& v, long long* launches) {
   if (fp32) return vcycle_t<float, float>(m, v, launches);
   return vcycle_t<double, double>(m, v, launches);
+}
+
+// ---------------------------------------------------------------------------
+// uvh: block preconditioner, AMG on the velocity block
+// ---------------------------------------------------------------------------
+
+// 3-dof row (c, g) of a uvh tangent holds blocks b = u, v, h of deg(g)
+// entries; its u and v blocks are the velocity block's row (c, g), c < 2.
+// One thread per velocity row copies them, and the row's constraint mask.
+__global__ void k_uvh_extract(const DevMesh dm, int n2, const int* dof_sys2, const int* dof2_off, const int* knz2_off,
+                              const double* K3, const unsigned char* cmask3, double* K2, unsigned char* cmask2) {
+  const int i2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i2 >= n2) return;
+  const int s = dof_sys2[i2];
+  const int no = dm.sys_node_off[s], nn = dm.sys_node_off[s + 1] - no;
+  const int local = i2 - dof2_off[s], c = local / nn, gl = local - c * nn;
+  const int g = no + gl;
+  const int np0 = dm.nodeptr[g], deg = dm.nodeptr[g + 1] - np0, lp = np0 - dm.nodeptr[no];
+  const double* src = K3 + dm.sys_knz_off[s] + (size_t)c * 3 * dm.sys_nnzn[s] + 3 * (size_t)lp;
+  double* dst = K2 + knz2_off[s] + (size_t)c * 2 * dm.sys_nnzn[s] + 2 * (size_t)lp;
+  for (int k = 0; k < 2 * deg; ++k) dst[k] = src[k];
+  cmask2[i2] = cmask3[dm.sys_dof_off[s] + local];
+}
+
+// r2 = mask(p3 on the velocity rows), x0 = l1-Jacobi of r2 (pre-smoothing).
+__global__ void k_uvh_gather(const DevMesh dm, int n2, const int* dof_sys2, const int* dof2_off, const int* sel,
+                             const int* done, const unsigned char* cmask2, const double* p3, const double* invd2,
+                             double* r2, double* x0) {
+  const int i2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i2 >= n2) return;
+  const int s = dof_sys2[i2];
+  if (!sel[s] || done[s]) return;
+  const double v = cmask2[i2] ? 0.0 : p3[dm.sys_dof_off[s] + (i2 - dof2_off[s])];
+  r2[i2] = v;
+  x0[i2] = invd2[i2] * v;
+}
+
+__global__ void k_uvh_scatter(const DevMesh dm, int n2, const int* dof_sys2, const int* dof2_off, const int* sel,
+                              const int* done, const double* z2, double* out3) {
+  const int i2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i2 >= n2) return;
+  const int s = dof_sys2[i2];
+  if (!sel[s] || done[s]) return;
+  out3[dm.sys_dof_off[s] + (i2 - dof2_off[s])] = z2[i2];
+}
+
+int amg_numeric_uvh(ua_mesh* m, const double* K3, const unsigned char* cmask3, long long* launches) {
+  Amg* a = m->amg;
+  if (!a || m->ndof != 3) return set_error(UA_ERR_INVALID, "no uvh AMG hierarchy");
+  AmgLevel& F = a->lev[0];
+  k_uvh_extract<<<(F.ndof + 255) / 256, 256, 0, m->stream>>>(m->dm, F.ndof, F.dof_sys, F.d_dof_off, F.d_knz_off,
+                                                             K3, cmask3, (double*)F.A, a->uvh_mask), ++*launches;
+  return amg_numeric(m, F.rowptr, F.colind, F.A, false, a->uvh_mask, launches);
+}
+
+int amg_apply_uvh(ua_mesh* m, const double* p3, double* out3, const int* sel, const int* done, int lpr,
+                  long long* launches) {
+  Amg* a = m->amg;
+  AmgLevel& F = a->lev[0];
+  const int nb = (F.ndof + 255) / 256;
+  k_uvh_gather<<<nb, 256, 0, m->stream>>>(m->dm, F.ndof, F.dof_sys, F.d_dof_off, sel, done, a->uvh_mask, p3,
+                                          (const double*)F.invd, a->uvh_r, a->uvh_x0), ++*launches;
+  AmgPcgView v{F.rowptr, F.colind, F.A, a->uvh_r, a->uvh_x0, a->uvh_z, nullptr, nullptr, a->uvh_mask, sel, done,
+               F.rb_start, F.rb_sys, F.nrb, lpr, a->uvh_t};
+  int rc = vcycle_t<double, double>(m, v, launches);
+  if (rc) return rc;
+  k_uvh_scatter<<<nb, 256, 0, m->stream>>>(m->dm, F.ndof, F.dof_sys, F.d_dof_off, sel, done, a->uvh_z, out3),
+      ++*launches;
+  return UA_OK;
 }
 
 }  // namespace ua

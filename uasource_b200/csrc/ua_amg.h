@@ -41,6 +41,13 @@ const void* amg_invd0(const ua_mesh* m);
 // Numeric phase for a new tangent K0 (Galerkin products, smoother, coarsest inverses).
 int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
                 const unsigned char* cmask, long long* launches);
+// uvh handles: extract the velocity block of the 3-dof tangent K3 (and its
+// constraint mask) into the hierarchy's own finest level, then the numeric
+// phase (FP64).
+int amg_numeric_uvh(ua_mesh* m, const double* K3, const unsigned char* cmask3, long long* launches);
+// out3 = V-cycle(p3) on the velocity rows of 3-dof vectors (other rows untouched).
+int amg_apply_uvh(ua_mesh* m, const double* p3, double* out3, const int* sel, const int* done, int lpr,
+                  long long* launches);
 // One V(1,1) cycle.  The finest level runs as row-block kernels (residual,
 // aggregation, correction, smoothing); coarser levels use one thread per aggregate.
 int amg_vcycle(ua_mesh* m, bool fp32, const AmgPcgView& v, long long* launches);

@@ -63,7 +63,10 @@ struct Prof {
 };
 enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2, PK_AMGR = 3, PK_AMGP = 4, PK_COUNT = 5 };
 constexpr int kRedThreads = 256;
-enum { SV_RZ = 0, SV_PQ, SV_ALPHA, SV_BETA, SV_RR, SV_RR0, SV_TOL2, SV_NORM, SV_FF, SV_FD, SV_OMEGA, SV_COUNT };
+// per-system scalars; SV_RH = |rhat|^2, SV_RST = BiCGStab restart pending, SV_NRST = restarts so far
+enum { SV_RZ = 0, SV_PQ, SV_ALPHA, SV_BETA, SV_RR, SV_RR0, SV_TOL2, SV_NORM, SV_FF, SV_FD, SV_OMEGA, SV_RH, SV_RST,
+       SV_NRST, SV_COUNT };
+constexpr int kBicgMaxRestarts = 64;
 
 struct Work {
   int nsys = 0, nrb = 0, nc = 0;
@@ -1074,6 +1077,14 @@ static double forcing_term(const ua_params* p, double rForce) {
   return std::min(1e-2, std::max(p->krylov_rtol, 0.1 * std::sqrt(std::max(rForce, 0.0))));
 }
 
+// The uvh step always takes the line search (SSTREAM_TransientImplicit.m:418) and its cost
+// mixes momentum and mass-conservation rows, which loose directions stall: the uvh forcing
+// term stays at or below 1e-6 (1e-3 sqrt(rForce), clamped to [krylov_rtol, 1e-6]).
+static double forcing_term_uvh(const ua_params* p, double rForce) {
+  if (!p->krylov_adaptive || !(rForce == rForce)) return p->krylov_rtol;
+  return std::min(1e-6, std::max(p->krylov_rtol, 1e-3 * std::sqrt(std::max(rForce, 0.0))));
+}
+
 // uvResidualsCriteria.m:1-23
 static bool residual_criteria(const ua_params* p, double rForce, double rWork, int iteration, double gamma) {
   const double *a, *o;
@@ -1388,17 +1399,22 @@ __global__ void __launch_bounds__(256) k_bicg_init(const int* rb_start, const in
 }
 
 // p = r + beta (p - omega v); phat = invd p
+// p = r + beta (p - omega v), phat = invd p; after a breakdown (restart pending, beta = 0)
+// the shadow residual restarts from the current residual: rhat = r.
 __global__ void __launch_bounds__(256) k_bicg_p(const int* rb_start, const int* rb_sys, const int* sel,
                                                 const int* done, const double* sysv, int nsys, const double* r,
-                                                double* p, const double* vv, const double* invd, double* phat) {
+                                                double* p, const double* vv, const double* invd, double* phat,
+                                                double* rhat) {
   const int blk = blockIdx.x;
   const int s = rb_sys[blk];
   if (!sel[s] || done[s]) return;
   const double beta = sysv[SV_BETA * nsys + s], omega = sysv[SV_OMEGA * nsys + s];
+  const bool restart = sysv[SV_RST * nsys + s] != 0.0;
   for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) {
     const double pv = r[i] + beta * (p[i] - omega * vv[i]);
     p[i] = pv;
     phat[i] = invd[i] * pv;
+    if (restart) rhat[i] = r[i];
   }
 }
 
@@ -1454,11 +1470,15 @@ __global__ void k_bicg_reduce(int stage, const int* sys_rb_off, int nrb, const i
     sv[SV_ALPHA * nsys + s] = 1.0;
     sv[SV_OMEGA * nsys + s] = 1.0;
     sv[SV_BETA * nsys + s] = 0.0;  // first direction p = r
+    sv[SV_RH * nsys + s] = o[1];   // rhat = r
+    sv[SV_RST * nsys + s] = 0.0;
+    sv[SV_NRST * nsys + s] = 0.0;
     its[s] = 0;
     status[s] = 0;
     done[s] = (o[1] == 0.0) ? 1 : 0;
   } else if (stage == 1) {
     const double rv = o[0];
+    sv[SV_RST * nsys + s] = 0.0;  // every block of k_bicg_p has consumed a pending restart
     if (rv == 0.0 || !(rv == rv)) { status[s] = 1; done[s] = 1; sv[SV_ALPHA * nsys + s] = 0; return; }
     sv[SV_ALPHA * nsys + s] = sv[SV_RZ * nsys + s] / rv;
   } else if (stage == 2) {
@@ -1469,10 +1489,21 @@ __global__ void k_bicg_reduce(int stage, const int* sys_rb_off, int nrb, const i
     its[s] += 1;
     sv[SV_RR * nsys + s] = rr;
     const double omega = sv[SV_OMEGA * nsys + s];
-    sv[SV_BETA * nsys + s] = (rho_new / sv[SV_RZ * nsys + s]) * (sv[SV_ALPHA * nsys + s] / omega);
-    sv[SV_RZ * nsys + s] = rho_new;
-    if (rr <= sv[SV_TOL2 * nsys + s] * sv[SV_RR0 * nsys + s] || its[s] >= maxit || !(rr == rr)) done[s] = 1;
-    else if (omega == 0.0 || rho_new == 0.0) { status[s] = 1; done[s] = 1; }
+    if (rr <= sv[SV_TOL2 * nsys + s] * sv[SV_RR0 * nsys + s] || its[s] >= maxit || !(rr == rr)) {
+      done[s] = 1;
+    } else if (omega == 0.0 || fabs(rho_new) <= 1e-12 * sqrt(sv[SV_RH * nsys + s] * rr)) {
+      // breakdown (rhat nearly orthogonal to r, or a zero stabilisation step): restart from the
+      // current residual with rhat = r, p = r, a bounded number of times
+      if (sv[SV_NRST * nsys + s] >= kBicgMaxRestarts) { status[s] = 1; done[s] = 1; return; }
+      sv[SV_NRST * nsys + s] += 1.0;
+      sv[SV_RST * nsys + s] = 1.0;
+      sv[SV_BETA * nsys + s] = 0.0;
+      sv[SV_RZ * nsys + s] = rr;
+      sv[SV_RH * nsys + s] = rr;
+    } else {
+      sv[SV_BETA * nsys + s] = (rho_new / sv[SV_RZ * nsys + s]) * (sv[SV_ALPHA * nsys + s] / omega);
+      sv[SV_RZ * nsys + s] = rho_new;
+    }
   }
 }
 
@@ -1492,6 +1523,15 @@ static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out,
   double *vv = (double*)w->kq, *sv = (double*)w->ks, *shat = (double*)w->ksh, *t = (double*)w->kt;
   double* invd = (double*)w->invd;
   k_invdiag<KT, double><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, invd), ++g_launches;
+  // block preconditioner: the aggregation-AMG V-cycle of the velocity block on the u, v rows,
+  // point Jacobi on the h rows (the coupling blocks are left to the Krylov iteration)
+  bool amg = p->krylov_precond == UA_PC_AMG && m->ndof == 3 && !m->h_nodeptr.empty() && sizeof(KT) == 8;
+  if (amg && amg_setup(m) != UA_OK) amg = false;
+  if (amg) {
+    int rc = amg_numeric_uvh(m, (const double*)K, w->cmask, &g_launches);
+    if (rc) return rc;
+  }
+  const int lpr_uv = m->nod == 3 ? 1 : 2;
   k_zero_sel<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->dX), ++g_launches;
   if (w->nc)
     k_con_particular<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs,
@@ -1507,7 +1547,11 @@ static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out,
   while (true) {
     for (int k = 0; k < chunk; ++k) {
       k_bicg_p<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys, r, pp, vv,
-                                              invd, phat), ++g_launches;
+                                              invd, phat, rhat), ++g_launches;
+      if (amg) {
+        int rc = amg_apply_uvh(m, pp, phat, w->sel, w->done, lpr_uv, &g_launches);
+        if (rc) return rc;
+      }
       cudaEvent_t ev[2];
       prof_begin(m, PK_SPMV, ev);
       k_bicg_spmv<KT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr,
@@ -1517,6 +1561,10 @@ static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out,
                                                              w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
       k_bicg_s<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys, r, vv, invd,
                                               sv, shat), ++g_launches;
+      if (amg) {
+        int rc = amg_apply_uvh(m, sv, shat, w->sel, w->done, lpr_uv, &g_launches);
+        if (rc) return rc;
+      }
       k_bicg_spmv<KT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr,
                                                          w->colind, K, shat, w->cmask, t, sv, w->part), ++g_launches;
       k_bicg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
@@ -1691,7 +1739,7 @@ static int newton_run_uvh(ua_mesh* m, const ua_params* p, std::vector<ua_newton_
     t_asm += t1 - t0;
     for (int s = 0; s < nsys; ++s) its[s] = sel[s];
     std::vector<double> eta(nsys);
-    for (int s = 0; s < nsys; ++s) eta[s] = forcing_term(p, st[s].rForce == INFINITY ? 1.0 : st[s].rForce);
+    for (int s = 0; s < nsys; ++s) eta[s] = forcing_term_uvh(p, st[s].rForce == INFINITY ? 1.0 : st[s].rForce);
     if ((rc = bicgstab_t<double>(m, p, w->Kd, its.data(), eta.data()))) return rc;  // :136
     t_sol += now_ms() - t1;
     for (int s = 0; s < nsys; ++s) if (sel[s]) st[s].kits = its[s];
