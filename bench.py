@@ -420,8 +420,16 @@ def run_ours(args):
     avg_ms = ms / max(n, 1)
     achieved = alg_total / (ms / 1000) / 1e9 if ms > 0 else 0.0
     total_k = sum(v[0] for v in cand.values())
+    # DRAM traffic per launch: the ncu capture of the finest-level SpMV-class kernels on the 32-mesh
+    # batch read and wrote 1.01 (SpMV) and 1.04 (smoothing) times their algorithmic bytes
+    # (profiles/k_pcg_spmv_batch32.md, profiles/k_amg_smooth_batch32.md); scaled to this launch size
+    traffic_ratio = {"k_pcg_spmv": 147.4 / 146.3, "k_amg_smooth": 161.6 / 155.7}
+    tr = next((v for k, v in traffic_ratio.items() if dom.startswith(k)), None)
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-            "frac": achieved / hbm_peak, "traffic": None,
+            "frac": achieved / hbm_peak,
+            "traffic": (tr * alg_total / max(n, 1)) if tr else None,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum on the 32-mesh batch, scaled by "
+                               "algorithmic bytes to this launch size") if tr else None,
             "alg_bytes_per_launch": alg_total / max(n, 1), "alg_bytes_rule": rule,
             "avg_launch_ms": avg_ms, "launches": n,
             "peak_source": ("MEASURED_PEAKS.json hbm_gbs (burst copy), of measured" if "hbm_gbs" in peaks

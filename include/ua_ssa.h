@@ -51,6 +51,11 @@ extern "C" {
 #define UA_PC_JACOBI 0   /* point Jacobi */
 #define UA_PC_AMG    1   /* aggregation AMG V(1,1) cycle, l1-Jacobi smoother (default) */
 
+/* inner solvers of the unsymmetric uvh system (both constrained, preconditioned by AMG on the
+   velocity block and a block lower-triangular thickness step, or point Jacobi) */
+#define UA_KRYLOV_GMRES    0   /* restarted GMRES(m), right-preconditioned (default) */
+#define UA_KRYLOV_BICGSTAB 1   /* BiCGStab with restarts on breakdown */
+
 /* Assembly modes of uvMatrixAssembly (uvMatrixAssemblySSTREAM.m:17-28). */
 #define UA_ASM_R      0   /* CtrlVar.uvMatrixAssembly.Ronly=true */
 #define UA_ASM_RK     1   /* R and K */
@@ -121,6 +126,8 @@ typedef struct ua_params {
     int32_t spmv_lanes;        /* lanes per row of the uv PCG/AMG row products: 0 = by element type
                                   (1 for P1, 2 for P2), else 1, 2, 4, 8, 16 or 32 */
     int32_t asm_threads;       /* CTA size of the P1 uv assembly: 0 = default, else 128 or 256 */
+    int32_t uvh_krylov;        /* UA_KRYLOV_*: inner solver of the unsymmetric uvh system */
+    int32_t krylov_restart;    /* GMRES restart length m (uvh) */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

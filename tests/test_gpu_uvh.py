@@ -13,6 +13,7 @@ import scipy.sparse as sp
 import uasource_b200 as ua
 from oracle import ua_ref as R
 from uasource_b200 import synth
+from uasource_b200 import lib as L
 
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -52,14 +53,15 @@ def test_uvh_assembly_matches_golden(path):
     assert Kr is None and np.array_equal(Rr, Rg)
 
 
+@pytest.mark.parametrize("krylov", [L.UA_KRYLOV_GMRES, L.UA_KRYLOV_BICGSTAB], ids=["gmres", "bicgstab"])
 @pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p) for p in FIXTURES])
-def test_uvh_newton_matches_golden(path):
+def test_uvh_newton_matches_golden(path, krylov):
     z = np.load(path)
     mua = ua.CreateMUA(z["coordinates"], z["connectivity"], ndof=3)
     F0, F1 = _levels(z, False)
     bcs = ua.BCs(ubFixedNode=z["ubFixedNode"], ubFixedValue=z["ubFixedValue"], vbFixedNode=z["vbFixedNode"],
                  vbFixedValue=z["vbFixedValue"])
-    ctrl = ua.CtrlVar().set_force_tolerance(1e-20).set_uvh_force_tolerance(1e-20)
+    ctrl = ua.CtrlVar(uvh_krylov=krylov).set_force_tolerance(1e-20).set_uvh_force_tolerance(1e-20)
     Fo, lam, info = ua.uvh(ctrl, mua, F0, F1, bcs, float(z["dt"]))
     assert info.converged
     ref = np.concatenate([z["sol_ub"], z["sol_vb"], z["sol_h"]])
@@ -80,3 +82,25 @@ def test_uvh_zero_fields_matches_oracle():
     S1 = R.UvhState(z["state_h"], z["state_ub"], z["state_vb"], z["as_"], z["ab"])
     Ro, _ = R.uvh_matrix_assembly(R.Params(), m, Fo, S0, S1, float(z["dt"]), Ronly=True, ZeroFields=True)
     assert np.max(np.abs(Rg - Ro)) <= R_TOL * np.max(np.abs(Ro))
+
+
+def test_uvh_gmres_converges_on_a_larger_p2_mesh():
+    """The implicit step on a 101x51-vertex P2 mesh (10,000 elements), started from the
+    converged diagnostic state: restarted GMRES with the block preconditioner (AMG on the
+    velocity block, block lower-triangular thickness step) converges where BiCGStab broke
+    down, and the result satisfies the step to the requested force tolerance."""
+    P = synth.ice_stream_shelf(101, 51, nod=6, seed=0, transient=True)
+    bcs = ua.BCs.from_problem(P)
+    m2 = ua.CreateMUA(P.coordinates, P.connectivity)
+    Fo, _, _, _, iuv = ua.uv(ua.CtrlVar(precision=L.UA_PREC_MIXED, krylov_rtol=1e-6).set_force_tolerance(1e-20),
+                             m2, bcs, ua.Fields.from_problem(P))
+    assert iuv.converged
+    m3 = ua.CreateMUA(P.coordinates, P.connectivity, ndof=3)
+    F0 = ua.Fields.from_problem(P)
+    F0.ub, F0.vb = Fo.ub, Fo.vb
+    hb = ua.HBCs(ubFixedNode=bcs.ubFixedNode, ubFixedValue=bcs.ubFixedValue, vbFixedNode=bcs.vbFixedNode,
+                 vbFixedValue=bcs.vbFixedValue)
+    ctrl = ua.CtrlVar().set_force_tolerance(1e-20)
+    F1o, _, info = ua.uvh(ctrl, m3, F0, F0.copy(), hb, 0.1)
+    assert info.converged and info.rForce < 1e-15
+    assert np.all(np.isfinite(F1o.h)) and np.max(np.abs(F1o.h - P.h)) > 0

@@ -103,6 +103,11 @@ struct Work {
   double *h0 = nullptr, *u0 = nullptr, *v0 = nullptr, *as0 = nullptr, *ab0 = nullptr, *as1 = nullptr,
          *ab1 = nullptr, *dadh = nullptr;
   void *krh = nullptr, *ks = nullptr, *ksh = nullptr, *kt = nullptr;
+  // uvh GMRES(m): basis, work vectors, per-system coefficients
+  double *gm_V = nullptr, *gm_w = nullptr, *gm_z = nullptr, *gm_u = nullptr, *gm_part = nullptr;
+  double *gm_coef = nullptr, *gm_scal = nullptr;
+  int *gm_act = nullptr, *gm_ny = nullptr;
+  int gm_m = 0;
   // pinned host staging
   double* h_sysv = nullptr;
   int* h_int = nullptr;
@@ -1398,7 +1403,16 @@ __global__ void __launch_bounds__(256) k_bicg_init(const int* rb_start, const in
   block_partials<2>(v, part, nrb, blk);
 }
 
-// p = r + beta (p - omega v); phat = invd p
+// out = invd in (point-Jacobi preconditioner), selected unfinished systems
+__global__ void __launch_bounds__(256) k_scale_vec(const int* rb_start, const int* rb_sys, const int* sel,
+                                                   const int* done, const double* in, const double* invd,
+                                                   double* out) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) out[i] = invd[i] * in[i];
+}
+
 // p = r + beta (p - omega v), phat = invd p; after a breakdown (restart pending, beta = 0)
 // the shadow residual restarts from the current residual: rhat = r.
 __global__ void __launch_bounds__(256) k_bicg_p(const int* rb_start, const int* rb_sys, const int* sel,
@@ -1595,6 +1609,357 @@ static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out,
 // uvh driver: SSTREAM_TransientImplicit.m:6-717
 // ---------------------------------------------------------------------------
 
+// ---------------------------------------------------------------------------
+// Restarted GMRES(m) for the unsymmetric uvh system (replaces the direct
+// solve of solveKApe.m:104-107 like BiCGStab does), right-preconditioned, all
+// systems of the handle in lockstep with per-system Hessenberg matrices on the
+// host.  Classical Gram-Schmidt with one re-orthogonalisation pass.
+// ---------------------------------------------------------------------------
+
+// part[i*nrb + blk] = block partial of (w, V_i) for i < nv (grid: row blocks x nv)
+__global__ void __launch_bounds__(256) k_gm_dots(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
+                                                 const int* done, const double* w, const double* V, size_t ldv,
+                                                 double* part) {
+  const int blk = blockIdx.x, i = blockIdx.y;
+  const int s = rb_sys[blk];
+  double v[1] = {0};
+  if (sel[s] && !done[s]) {
+    const double* vi = V + (size_t)i * ldv;
+    for (int r = rb_start[blk] + threadIdx.x; r < rb_start[blk + 1]; r += blockDim.x) v[0] += w[r] * vi[r];
+  }
+  __shared__ double red[8];
+  double t = v[0];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sum = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) sum += red[k];
+    part[(size_t)i * nrb + blk] = sum;
+  }
+}
+
+// out[s*ld + i] = sum over the system's row blocks of part[i*nrb + b] (grid: systems x nv)
+__global__ void k_gm_reduce(const int* sys_rb_off, int nrb, const int* sel, const int* done, const double* part,
+                            double* out, int ld) {
+  const int s = blockIdx.x, i = blockIdx.y;
+  if (!sel[s] || done[s]) return;
+  double o[1];
+  sys_sum<1>(part + (size_t)i * nrb, nrb, sys_rb_off[s], sys_rb_off[s + 1], o);
+  if (threadIdx.x == 0) out[(size_t)s * ld + i] = o[0];
+}
+
+// w -= sum_i coef[s*ld + i] V_i (i < nv)
+__global__ void __launch_bounds__(256) k_gm_orth(const int* rb_start, const int* rb_sys, const int* sel,
+                                                 const int* done, double* w, const double* V, size_t ldv, int nv,
+                                                 const double* coef, int ld) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const double* c = coef + (size_t)s * ld;
+  for (int r = rb_start[blk] + threadIdx.x; r < rb_start[blk + 1]; r += blockDim.x) {
+    double acc = w[r];
+    for (int i = 0; i < nv; ++i) acc -= c[i] * V[(size_t)i * ldv + r];
+    w[r] = acc;
+  }
+}
+
+// dst = src * scale[s]
+__global__ void __launch_bounds__(256) k_gm_scale(const int* rb_start, const int* rb_sys, const int* sel,
+                                                  const int* done, const double* src, double* dst,
+                                                  const double* scale) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const double a = scale[s];
+  for (int r = rb_start[blk] + threadIdx.x; r < rb_start[blk + 1]; r += blockDim.x) dst[r] = src[r] * a;
+}
+
+// u = sum_i y[s*ld + i] V_i for i < ny[s]
+__global__ void __launch_bounds__(256) k_gm_combine(const int* rb_start, const int* rb_sys, const int* sel,
+                                                    const int* act, double* u, const double* V, size_t ldv,
+                                                    const double* y, const int* ny, int ld) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || !act[s]) return;
+  const double* c = y + (size_t)s * ld;
+  const int n = ny[s];
+  for (int r = rb_start[blk] + threadIdx.x; r < rb_start[blk + 1]; r += blockDim.x) {
+    double acc = 0;
+    for (int i = 0; i < n; ++i) acc += c[i] * V[(size_t)i * ldv + r];
+    u[r] = acc;
+  }
+}
+
+// x += z for systems with act[s]
+__global__ void __launch_bounds__(256) k_gm_axpy(const int* rb_start, const int* rb_sys, const int* sel,
+                                                 const int* act, double* x, const double* z) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || !act[s]) return;
+  for (int r = rb_start[blk] + threadIdx.x; r < rb_start[blk + 1]; r += blockDim.x) x[r] += z[r];
+}
+
+// r = mask(f - K x) and the block partial of r.r (systems with act[s])
+template <typename KT, int LPR>
+__global__ void __launch_bounds__(256) k_gm_resid(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
+                                                  const int* act, const int* rowptr, const int* colind, const KT* K,
+                                                  const double* x, const double* f, const unsigned char* cmask,
+                                                  double* r, double* part) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  double v[1] = {0};
+  if (sel[s] && act[s]) {
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread
+      const int row = row0 + grp;
+      const bool valid = row < re;
+      const double ax = row_dot<KT, double, LPR>(rowptr, colind, K, x, row, valid, lane);
+      if (valid && lane == 0) {
+        const double rv = cmask[row] ? 0.0 : f[row] - ax;
+        r[row] = rv;
+        v[0] += rv * rv;
+      }
+    }
+  }
+  block_partials<1>(v, part, nrb, blk);
+}
+
+// Thickness rows of the block lower-triangular preconditioner:
+// z_h = invd_h (p_h - K_hu z_u - K_hv z_v), the velocity part z already set
+// (row (2, g) of a uvh tangent: blocks u, v, h of deg entries each).
+__global__ void __launch_bounds__(256) k_uvh_hrows(const int* rb_start, const int* rb_sys, const int* sel,
+                                                   const int* done, const int* dof_off, const int* rowptr,
+                                                   const int* colind, const double* K, const double* invd,
+                                                   const unsigned char* cmask, const double* p, double* z) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const int nn = (dof_off[s + 1] - dof_off[s]) / 3, h0 = dof_off[s] + 2 * nn;
+  const int r0 = max(rb_start[blk], h0), r1 = rb_start[blk + 1];
+  for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+    if (cmask[row]) { z[row] = 0; continue; }
+    const int q0 = rowptr[row], deg = (rowptr[row + 1] - q0) / 3;
+    double acc = 0;
+    for (int q = q0; q < q0 + 2 * deg; ++q) acc += K[q] * z[colind[q]];
+    z[row] = invd[row] * (p[row] - acc);
+  }
+}
+
+struct GmSys {
+  std::vector<double> H, cs, sn, g;  // (m+1) x m column-major Hessenberg, rotations, rhs
+  double beta0 = 0, beta = 0, tol = 0;
+  int its = 0, j = 0;
+  bool active = false, cycle_done = false;
+};
+
+template <typename KT>
+static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, const double* eta) {
+  Work* w = m->work;
+  const int nsys = w->nsys, N = m->ndof_total;
+  const int mr = std::max(4, std::min(200, p->krylov_restart > 0 ? p->krylov_restart : 40));
+  const size_t ldv = (size_t)N;
+  const int ld = mr + 1;
+  // work space: basis V (mr+1 vectors), w, z, u; per-system coefficient arrays
+  if (!w->gm_V || w->gm_m != mr) {
+    w->gm_V = walloc<double>(m, (size_t)(mr + 1) * ldv);
+    w->gm_w = walloc<double>(m, ldv);
+    w->gm_z = walloc<double>(m, ldv);
+    w->gm_u = walloc<double>(m, ldv);
+    w->gm_part = walloc<double>(m, (size_t)(mr + 1) * w->nrb);
+    w->gm_coef = walloc<double>(m, (size_t)nsys * ld);
+    w->gm_scal = walloc<double>(m, (size_t)nsys * ld);
+    w->gm_act = walloc<int>(m, nsys);
+    w->gm_ny = walloc<int>(m, nsys);
+    if (!w->gm_V || !w->gm_w || !w->gm_z || !w->gm_u || !w->gm_part || !w->gm_coef || !w->gm_scal || !w->gm_act ||
+        !w->gm_ny)
+      return set_error(UA_ERR_OOM, "device allocation of the GMRES basis failed");
+    w->gm_m = mr;
+  }
+  double *V = w->gm_V, *wv = w->gm_w, *zv = w->gm_z, *uv = w->gm_u;
+  cudaStream_t st = m->stream;
+  double* invd = (double*)w->invd;
+  k_invdiag<KT, double><<<(N + 255) / 256, 256, 0, st>>>(N, K, w->diagpos, w->cmask, invd), ++g_launches;
+  bool amg = p->krylov_precond == UA_PC_AMG && m->ndof == 3 && !m->h_nodeptr.empty() && sizeof(KT) == 8;
+  if (amg && amg_setup(m) != UA_OK) amg = false;
+  if (amg) {
+    int rc = amg_numeric_uvh(m, (const double*)K, w->cmask, &g_launches);
+    if (rc) return rc;
+  }
+  const int lpr_uv = m->nod == 3 ? 1 : 2;
+  // preconditioner: velocity rows by the AMG V-cycle (else Jacobi), thickness rows by the
+  // block lower-triangular step
+  auto precond = [&](const double* in, double* out) -> int {
+    k_scale_vec<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, in, invd, out), ++g_launches;
+    if (amg) {
+      int rc = amg_apply_uvh(m, in, out, w->sel, w->done, lpr_uv, &g_launches);
+      if (rc) return rc;
+    }
+    if (m->ndof == 3)
+      k_uvh_hrows<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, m->dm.sys_dof_off, w->rowptr,
+                                          w->colind, (const double*)K, invd, w->cmask, in, out), ++g_launches;
+    return UA_OK;
+  };
+  auto spmv = [&](const double* x, double* y) {
+    k_bicg_spmv<KT, 16><<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr,
+                                                w->colind, K, x, w->cmask, y, nullptr, w->part), ++g_launches;
+  };
+  // host-side reduction results
+  std::vector<double> hco((size_t)nsys * ld), hco2((size_t)nsys * ld), hnrm((size_t)nsys * ld), hsc(nsys),
+      hy((size_t)nsys * ld);
+  std::vector<int> hact(nsys), hny(nsys), hdone(nsys);
+  auto reduce_to_host = [&](const double* part, int nv, std::vector<double>& dst) -> int {
+    k_gm_reduce<<<dim3(nsys, nv), kRedThreads, 0, st>>>(w->sys_rb_off, w->nrb, w->sel, w->done, part, w->gm_coef,
+                                                        ld), ++g_launches;
+    UA_CUDA_TRY(cudaMemcpyAsync(dst.data(), w->gm_coef, sizeof(double) * nsys * ld, cudaMemcpyDeviceToHost, st));
+    UA_CUDA_TRY(cudaStreamSynchronize(st));
+    return UA_OK;
+  };
+  // x0: zero plus the particular solution on the constrained dofs
+  k_zero_sel<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->dX), ++g_launches;
+  if (w->nc)
+    k_con_particular<<<(w->nc + 255) / 256, 256, 0, st>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs, w->X,
+                                                         w->dX, w->grhs), ++g_launches;
+  std::vector<GmSys> S(nsys);
+  for (int s = 0; s < nsys; ++s) {
+    S[s].active = its_out[s] != 0;
+    S[s].H.assign((size_t)ld * mr, 0.0);
+    S[s].cs.assign(mr, 0.0);
+    S[s].sn.assign(mr, 0.0);
+    S[s].g.assign(ld, 0.0);
+    S[s].tol = eta ? eta[s] : p->krylov_rtol;
+  }
+  auto upload_flags = [&]() -> int {
+    for (int s = 0; s < nsys; ++s) { hact[s] = S[s].active ? 1 : 0; hdone[s] = (S[s].active && !S[s].cycle_done) ? 0 : 1; }
+    UA_CUDA_TRY(cudaMemcpyAsync(w->gm_act, hact.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, st));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->done, hdone.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, st));
+    return UA_OK;
+  };
+  int total_cycles = 0;
+  const int max_cycles = std::max(1, p->krylov_maxit / mr + 1);
+  bool first = true;
+  while (true) {
+    // residual of the current iterate, v0 = r / |r|
+    for (int s = 0; s < nsys; ++s) S[s].cycle_done = false;
+    int rc = upload_flags();
+    if (rc) return rc;
+    dispatch_lpr(16, [&](auto L) {
+      k_gm_resid<KT, decltype(L)::value><<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->gm_act,
+                                                                  w->rowptr, w->colind, K, w->dX, w->frhs, w->cmask,
+                                                                  wv, w->gm_part);
+    });
+    ++g_launches;
+    if ((rc = reduce_to_host(w->gm_part, 1, hco))) return rc;
+    bool any = false;
+    for (int s = 0; s < nsys; ++s) {
+      GmSys& G = S[s];
+      if (!G.active) continue;
+      const double b = std::sqrt(std::max(hco[(size_t)s * ld], 0.0));
+      if (first) G.beta0 = b;
+      G.beta = b;
+      if (!(b == b) || b <= G.tol * G.beta0 || b == 0.0 || G.its >= p->krylov_maxit || total_cycles >= max_cycles) {
+        G.active = false;
+        continue;
+      }
+      std::fill(G.g.begin(), G.g.end(), 0.0);
+      G.g[0] = b;
+      G.j = 0;
+      hsc[s] = 1.0 / b;
+      any = true;
+    }
+    first = false;
+    if (!any) break;
+    if ((rc = upload_flags())) return rc;
+    UA_CUDA_TRY(cudaMemcpyAsync(w->gm_scal, hsc.data(), sizeof(double) * nsys, cudaMemcpyHostToDevice, st));
+    k_gm_scale<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, wv, V, w->gm_scal), ++g_launches;
+    // Arnoldi steps
+    for (int j = 0; j < mr; ++j) {
+      if ((rc = precond(V + (size_t)j * ldv, zv))) return rc;
+      spmv(zv, wv);
+      for (int pass = 0; pass < 2; ++pass) {
+        k_gm_dots<<<dim3(w->nrb, j + 1), 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, wv, V, ldv,
+                                                       w->gm_part), ++g_launches;
+        if ((rc = reduce_to_host(w->gm_part, j + 1, pass ? hco2 : hco))) return rc;
+        k_gm_orth<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, wv, V, ldv, j + 1, w->gm_coef,
+                                          ld), ++g_launches;
+      }
+      k_gm_dots<<<dim3(w->nrb, 1), 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, wv, wv, 0,
+                                                 w->gm_part), ++g_launches;
+      if ((rc = reduce_to_host(w->gm_part, 1, hnrm))) return rc;
+      bool more = false;
+      for (int s = 0; s < nsys; ++s) {
+        GmSys& G = S[s];
+        if (!G.active || G.cycle_done) continue;
+        double* h = &G.H[(size_t)j * ld];
+        for (int i = 0; i <= j; ++i) h[i] = hco[(size_t)s * ld + i] + hco2[(size_t)s * ld + i];
+        const double hn = std::sqrt(std::max(hnrm[(size_t)s * ld], 0.0));
+        h[j + 1] = hn;
+        for (int i = 0; i < j; ++i) {  // previous rotations
+          const double a = h[i], b = h[i + 1];
+          h[i] = G.cs[i] * a + G.sn[i] * b;
+          h[i + 1] = -G.sn[i] * a + G.cs[i] * b;
+        }
+        const double den = std::hypot(h[j], h[j + 1]);
+        G.cs[j] = den > 0 ? h[j] / den : 1.0;
+        G.sn[j] = den > 0 ? h[j + 1] / den : 0.0;
+        h[j] = den;
+        h[j + 1] = 0.0;
+        G.g[j + 1] = -G.sn[j] * G.g[j];
+        G.g[j] = G.cs[j] * G.g[j];
+        G.its++;
+        G.j = j + 1;
+        const double res = std::fabs(G.g[j + 1]);
+        if (res <= G.tol * G.beta0 || hn == 0.0 || !(res == res) || G.its >= p->krylov_maxit || j + 1 == mr) {
+          G.cycle_done = true;
+        } else {
+          more = true;
+          hsc[s] = 1.0 / hn;
+        }
+      }
+      if (!more) break;
+      if ((rc = upload_flags())) return rc;
+      UA_CUDA_TRY(cudaMemcpyAsync(w->gm_scal, hsc.data(), sizeof(double) * nsys, cudaMemcpyHostToDevice, st));
+      k_gm_scale<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, wv, V + (size_t)(j + 1) * ldv,
+                                         w->gm_scal), ++g_launches;
+    }
+    // x += M^-1 (V y), y from the triangular system of each active system
+    for (int s = 0; s < nsys; ++s) {
+      GmSys& G = S[s];
+      hny[s] = 0;
+      if (!G.active) continue;
+      const int k = G.j;
+      for (int i = k - 1; i >= 0; --i) {
+        double acc = G.g[i];
+        for (int c = i + 1; c < k; ++c) acc -= G.H[(size_t)c * ld + i] * hy[(size_t)s * ld + c];
+        const double d = G.H[(size_t)i * ld + i];
+        hy[(size_t)s * ld + i] = d != 0.0 ? acc / d : 0.0;
+      }
+      hny[s] = k;
+    }
+    for (int s = 0; s < nsys; ++s) S[s].cycle_done = false;
+    if ((rc = upload_flags())) return rc;
+    UA_CUDA_TRY(cudaMemcpyAsync(w->gm_scal, hy.data(), sizeof(double) * nsys * ld, cudaMemcpyHostToDevice, st));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->gm_ny, hny.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, st));
+    k_gm_combine<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->gm_act, uv, V, ldv, w->gm_scal,
+                                         w->gm_ny, ld), ++g_launches;
+    if ((rc = precond(uv, zv))) return rc;
+    k_gm_axpy<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->gm_act, w->dX, zv), ++g_launches;
+    ++total_cycles;
+  }
+  // restore selection semantics for the callers (done = finished)
+  for (int s = 0; s < nsys; ++s) hdone[s] = 1;
+  UA_CUDA_TRY(cudaMemcpyAsync(w->done, hdone.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, st));
+  if (w->nc)
+    k_con_multiplier<KT><<<(w->nc + 255) / 256, 256, 0, st>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->rowptr,
+                                                              w->colind, K, w->dX, w->frhs, w->dlam), ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
+  UA_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int s = 0; s < nsys; ++s) its_out[s] = its_out[s] ? S[s].its : 0;
+  return UA_OK;
+}
+
 static UvhPhys make_uvh_phys(const ua_params* p) {
   UvhPhys P;
   P.uv = make_phys(p);
@@ -1740,7 +2105,11 @@ static int newton_run_uvh(ua_mesh* m, const ua_params* p, std::vector<ua_newton_
     for (int s = 0; s < nsys; ++s) its[s] = sel[s];
     std::vector<double> eta(nsys);
     for (int s = 0; s < nsys; ++s) eta[s] = forcing_term_uvh(p, st[s].rForce == INFINITY ? 1.0 : st[s].rForce);
-    if ((rc = bicgstab_t<double>(m, p, w->Kd, its.data(), eta.data()))) return rc;  // :136
+    if (p->uvh_krylov == UA_KRYLOV_BICGSTAB) {
+      if ((rc = bicgstab_t<double>(m, p, w->Kd, its.data(), eta.data()))) return rc;  // :136
+    } else {
+      if ((rc = gmres_t<double>(m, p, w->Kd, its.data(), eta.data()))) return rc;
+    }
     t_sol += now_ms() - t1;
     for (int s = 0; s < nsys; ++s) if (sel[s]) st[s].kits = its[s];
     // r0 = func(0), r1 = func(1) (:155-156)
@@ -1865,6 +2234,7 @@ extern "C" void ua_params_default(ua_params* p) {
   std::memcpy(p->uvhAcceptableWorkOrForceTolerances, a2, sizeof a2);
   p->krylov_rtol = 1e-12; p->krylov_maxit = 20000; p->precision = UA_PREC_FP64;
   p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1; p->spmv_lanes = 0; p->asm_threads = 0;
+  p->uvh_krylov = UA_KRYLOV_GMRES; p->krylov_restart = 40;
   p->krylov_precond = UA_PC_AMG;
 }
 

@@ -27,6 +27,8 @@ UA_PREC_FP64 = 0
 UA_PREC_MIXED = 1
 UA_PC_JACOBI = 0
 UA_PC_AMG = 1
+UA_KRYLOV_GMRES = 0
+UA_KRYLOV_BICGSTAB = 1
 UA_ASM_R = 0
 UA_ASM_RK = 1
 UA_ASM_ZERO_R = 2
@@ -73,6 +75,7 @@ class ua_params(C.Structure):
         ("krylov_rtol", C.c_double), ("krylov_maxit", C.c_int32), ("precision", C.c_int32),
         ("patch_nodes", C.c_int32), ("verbose", C.c_int32), ("profile", C.c_int32),
         ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32), ("spmv_lanes", C.c_int32), ("asm_threads", C.c_int32),
+        ("uvh_krylov", C.c_int32), ("krylov_restart", C.c_int32),
     ]
 
 

@@ -77,6 +77,8 @@ class CtrlVar:
     krylov_precond: int = L.UA_PC_AMG
     spmv_lanes: int = 0
     asm_threads: int = 0
+    uvh_krylov: int = L.UA_KRYLOV_GMRES
+    krylov_restart: int = 40
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
