@@ -119,7 +119,7 @@ typedef struct ua_params {
     int32_t patch_nodes;       /* assembly patch size (0 = autotune) */
     int32_t verbose;           /* per-iteration log line to stderr */
     int32_t profile;           /* 1: time assembly and SpMV launches with CUDA events */
-    int32_t krylov_adaptive;   /* 1: inner tolerance eta_k = clamp(0.1*sqrt(rForce_k), krylov_rtol, 1e-2)
+    int32_t krylov_adaptive;   /* 1: inner tolerance eta_k = clamp(c*sqrt(rForce_k), krylov_rtol, max)
                                   (inexact Newton forcing term); 0: krylov_rtol every iteration */
     int32_t krylov_precond;    /* UA_PC_*: preconditioner of the uv inner PCG (the uvh BiCGStab uses
                                   point Jacobi) */
@@ -128,6 +128,7 @@ typedef struct ua_params {
     int32_t asm_threads;       /* CTA size of the P1 uv assembly: 0 = default, else 128 or 256 */
     int32_t uvh_krylov;        /* UA_KRYLOV_*: inner solver of the unsymmetric uvh system */
     int32_t krylov_restart;    /* GMRES restart length m (uvh) */
+    double krylov_eta_c, krylov_eta_max;  /* uv forcing term eta = clamp(c*sqrt(rForce), krylov_rtol, max) */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

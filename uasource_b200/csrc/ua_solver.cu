@@ -1075,11 +1075,14 @@ static int linear_solve(ua_mesh* m, const ua_params* p, std::vector<int>& its_ou
 }
 
 // Inner tolerance of Newton iteration with cost rForce: the forcing term
-// eta = 0.1*sqrt(rForce) (relative residual ~ ||[f;g]||/||fext0||), clamped to
-// [krylov_rtol, 1e-2]; krylov_rtol itself when adaptive tolerances are off.
+// eta = c*sqrt(rForce) (relative residual ~ ||[f;g]||/||fext0||), clamped to
+// [krylov_rtol, max] (defaults c = 0.5, max = 0.1, the fastest safe pair of a
+// sweep on B200); krylov_rtol itself when adaptive tolerances are off.
 static double forcing_term(const ua_params* p, double rForce) {
   if (!p->krylov_adaptive || !(rForce == rForce)) return p->krylov_rtol;
-  return std::min(1e-2, std::max(p->krylov_rtol, 0.1 * std::sqrt(std::max(rForce, 0.0))));
+  const double c = p->krylov_eta_c > 0 ? p->krylov_eta_c : 0.5;
+  const double hi = p->krylov_eta_max > 0 ? p->krylov_eta_max : 0.1;
+  return std::min(hi, std::max(p->krylov_rtol, c * std::sqrt(std::max(rForce, 0.0))));
 }
 
 // The uvh step always takes the line search (SSTREAM_TransientImplicit.m:418) and its cost
@@ -2235,6 +2238,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->krylov_rtol = 1e-12; p->krylov_maxit = 20000; p->precision = UA_PREC_FP64;
   p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1; p->spmv_lanes = 0; p->asm_threads = 0;
   p->uvh_krylov = UA_KRYLOV_GMRES; p->krylov_restart = 40;
+  p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1;
   p->krylov_precond = UA_PC_AMG;
 }
 

@@ -79,6 +79,8 @@ class CtrlVar:
     asm_threads: int = 0
     uvh_krylov: int = L.UA_KRYLOV_GMRES
     krylov_restart: int = 40
+    krylov_eta_c: float = 0.5
+    krylov_eta_max: float = 0.1
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
