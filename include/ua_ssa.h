@@ -129,6 +129,8 @@ typedef struct ua_params {
     int32_t uvh_krylov;        /* UA_KRYLOV_*: inner solver of the unsymmetric uvh system */
     int32_t krylov_restart;    /* GMRES restart length m (uvh) */
     double krylov_eta_c, krylov_eta_max;  /* uv forcing term eta = clamp(c*sqrt(rForce), krylov_rtol, max) */
+    int32_t precond_bf16;      /* mixed precision: 1 = the AMG V-cycle's finest-level passes read a BF16
+                                  copy of the tangent (the PCG operator stays FP32) */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

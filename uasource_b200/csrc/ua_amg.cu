@@ -22,6 +22,7 @@
 #include <cstring>
 #include <vector>
 #include <type_traits>
+#include <cuda_bf16.h>
 #include "ua_amg.h"
 
 namespace ua {
@@ -72,6 +73,7 @@ struct Amg {
   void **d_lev_b = nullptr, **d_lev_x2 = nullptr, **d_lev_A = nullptr;
   int **d_lev_rowptr = nullptr, **d_lev_colind = nullptr, **d_lev_dofoff = nullptr;
   size_t bytes = 0;
+  __nv_bfloat16* k0lo = nullptr;  // mixed precision: BF16 copy of the finest-level tangent
   // uvh handles: constraint mask and vectors of the velocity rows (2-dof layout)
   unsigned char* uvh_mask = nullptr;
   double *uvh_r = nullptr, *uvh_x0 = nullptr, *uvh_z = nullptr, *uvh_t = nullptr;
@@ -481,16 +483,40 @@ __device__ __forceinline__ double row_dot_uv(const int* rowptr, const int* colin
   return acc;
 }
 
-// Plain CSR row product (every index read); the form that is faster for FP32 values.
+__device__ __forceinline__ double to_d(double v) { return v; }
+__device__ __forceinline__ double to_d(float v) { return (double)v; }
+__device__ __forceinline__ double to_d(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
+
+// Plain CSR row product (every index read); the form that is faster for FP32 and BF16 values.
 template <typename KT, typename XT, int LPR>
 __device__ __forceinline__ double row_dot_csr(const int* rowptr, const int* colind, const KT* A, const XT* x, int row,
                                               bool valid, int lane) {
   double acc = 0;
-  if (valid)
-    for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) acc += (double)A[q] * (double)x[colind[q]];
+  if (valid) {
+    const int r1 = rowptr[row + 1];
+    int q = rowptr[row] + lane;
+    // four entries per step, loads first (more loads in flight), additions in entry order
+    for (; q + 3 * LPR < r1; q += 4 * LPR) {
+      const int c0 = colind[q], c1 = colind[q + LPR], c2 = colind[q + 2 * LPR], c3 = colind[q + 3 * LPR];
+      const double a0 = to_d(A[q]), a1 = to_d(A[q + LPR]), a2 = to_d(A[q + 2 * LPR]), a3 = to_d(A[q + 3 * LPR]);
+      const double x0 = (double)x[c0], x1 = (double)x[c1], x2 = (double)x[c2], x3 = (double)x[c3];
+      acc += a0 * x0;
+      acc += a1 * x1;
+      acc += a2 * x2;
+      acc += a3 * x3;
+    }
+    for (; q < r1; q += LPR) acc += to_d(A[q]) * (double)x[colind[q]];
+  }
 #pragma unroll
   for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
   return acc;
+}
+
+// BF16 copy of an FP32 tangent (the finest-level matrix of the mixed-precision
+// V-cycle's residual and smoothing passes)
+__global__ void k_to_bf16(long long n, const float* in, __nv_bfloat16* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16_rn(in[i]);
 }
 
 template <typename KT, typename VT, int LPR>
@@ -617,6 +643,18 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
   return UA_OK;
 }
 
+const void* amg_bf16_copy(ua_mesh* m, const float* K0, long long nnz, long long* launches) {
+  Amg* a = m->amg;
+  if (!a) return nullptr;
+  if (!a->k0lo) {
+    a->k0lo = (__nv_bfloat16*)dev_alloc(m, sizeof(__nv_bfloat16) * (size_t)std::max(nnz, 1LL));
+    if (!a->k0lo) return nullptr;
+    a->bytes += sizeof(__nv_bfloat16) * (size_t)nnz;
+  }
+  k_to_bf16<<<1184, 256, 0, m->stream>>>(nnz, K0, a->k0lo), ++*launches;
+  return a->k0lo;
+}
+
 int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
                 const unsigned char* cmask, long long* launches) {
   if (fp32) return numeric_t<float, float>(m, rowptr0, colind0, (const float*)K0, cmask, launches);
@@ -645,8 +683,13 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     const AmgLevel& C = a->lev[l + 1];
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 0);
     dispatch_lpr(lpr0, [&](auto L) {
-      k_amg_residual<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
-          rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l), doff(l));
+      if (l == 0 && v.K0lo)
+        k_amg_residual<__nv_bfloat16, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
+            rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
+            mask(l), W(l), doff(l));
+      else
+        k_amg_residual<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
+            rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l), doff(l));
     });
     ++*launches;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 1);
@@ -666,9 +709,14 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     double* part = l == 0 ? v.part_rz : nullptr;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 1, 0);
     dispatch_lpr(lpr0, [&](auto L) {
-      k_amg_smooth<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
-          rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), (const VT*)F.invd, mask(l),
-          out, pcopy, part, doff(l));
+      if (l == 0 && v.K0lo)
+        k_amg_smooth<__nv_bfloat16, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
+            rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
+            (const VT*)F.invd, mask(l), out, pcopy, part, doff(l));
+      else
+        k_amg_smooth<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
+            rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), (const VT*)F.invd,
+            mask(l), out, pcopy, part, doff(l));
     });
     ++*launches;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 1, 1);

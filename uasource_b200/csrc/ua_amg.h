@@ -28,6 +28,8 @@ struct AmgPcgView {
   // phase 0 before, 1 after)
   void (*mark)(void* ctx, int kind, int phase) = nullptr;
   void* mark_ctx = nullptr;
+  // optional BF16 copy of K0 for the finest-level residual and smoothing (mixed precision)
+  const void* K0lo = nullptr;
 };
 
 // Build the hierarchy of every system of the handle (host aggregation,
@@ -48,6 +50,9 @@ int amg_numeric_uvh(ua_mesh* m, const double* K3, const unsigned char* cmask3, l
 // out3 = V-cycle(p3) on the velocity rows of 3-dof vectors (other rows untouched).
 int amg_apply_uvh(ua_mesh* m, const double* p3, double* out3, const int* sel, const int* done, int lpr,
                   long long* launches);
+// Refresh the BF16 copy of an FP32 finest-level tangent (allocated on first use;
+// nullptr if that fails).
+const void* amg_bf16_copy(ua_mesh* m, const float* K0, long long nnz, long long* launches);
 // One V(1,1) cycle.  The finest level runs as row-block kernels (residual,
 // aggregation, correction, smoothing); coarser levels use one thread per aggregate.
 int amg_vcycle(ua_mesh* m, bool fp32, const AmgPcgView& v, long long* launches);

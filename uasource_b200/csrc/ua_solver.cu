@@ -115,12 +115,12 @@ struct Work {
   std::vector<int> h_sys_rb_off, h_sys_con_off;
   Prof prof;
   struct ServeState* serve = nullptr;
-  // replayable PCG chunks, index (fp32 ? 2 : 0) + (amg ? 1 : 0)
+  // replayable PCG chunks, index (fp32 ? 2 : 0) + (amg ? 1 : 0) + (BF16 V-cycle ? 4 : 0)
   bool no_graph = false;
-  cudaGraphExec_t pcg_exec[4] = {nullptr, nullptr, nullptr, nullptr};
-  long long pcg_exec_nodes[4] = {0, 0, 0, 0};
-  int pcg_exec_maxit[4] = {0, 0, 0, 0};
-  int pcg_exec_lpr[4] = {0, 0, 0, 0};
+  cudaGraphExec_t pcg_exec[8] = {};
+  long long pcg_exec_nodes[8] = {};
+  int pcg_exec_maxit[8] = {};
+  int pcg_exec_lpr[8] = {};
 };
 
 // Work of a timed launch: sum of the tangent non-zeros and dof rows of the
@@ -286,7 +286,19 @@ __device__ __forceinline__ double row_dot(const int* rowptr, const int* colind, 
   double acc = 0;
   if (valid) {
     const int r0 = rowptr[row], r1 = rowptr[row + 1];
-    for (int j = r0 + lane; j < r1; j += LPR) acc += (double)K[j] * (double)x[colind[j]];
+    int j = r0 + lane;
+    // four entries per step: indices and values first, then the gathers, so that each thread
+    // has several independent loads in flight; the additions keep the entry order
+    for (; j + 3 * LPR < r1; j += 4 * LPR) {
+      const int c0 = colind[j], c1 = colind[j + LPR], c2 = colind[j + 2 * LPR], c3 = colind[j + 3 * LPR];
+      const double a0 = (double)K[j], a1 = (double)K[j + LPR], a2 = (double)K[j + 2 * LPR], a3 = (double)K[j + 3 * LPR];
+      const double x0 = (double)x[c0], x1 = (double)x[c1], x2 = (double)x[c2], x3 = (double)x[c3];
+      acc += a0 * x0;
+      acc += a1 * x1;
+      acc += a2 * x2;
+      acc += a3 * x3;
+    }
+    for (; j < r1; j += LPR) acc += (double)K[j] * (double)x[colind[j]];
   }
 #pragma unroll
   for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
@@ -958,6 +970,10 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   AmgPcgView view{w->rowptr, w->colind, K, r, w->kx0, z, nullptr, w->part, w->cmask, w->sel, w->done,
                   w->rb_start, w->rb_sys, w->nrb, lpr, q};
   if (w->prof.on) { view.mark = prof_amg; view.mark_ctx = m; }
+  // mixed precision: the V-cycle's finest-level residual and smoothing read a BF16 copy of K (the
+  // l1 diagonal and the Galerkin products come from the FP32 values; the cycle stays symmetric and,
+  // with the l1 diagonal above half the row sums, positive definite)
+  if (amg && fp32 && p->precond_bf16) view.K0lo = amg_bf16_copy(m, (const float*)K, m->nnz_total, &g_launches);
   dispatch_lpr(lpr, [&](auto L) {
     if (uvlay)
       k_pcg_init<KT, VT, decltype(L)::value, true><<<w->nrb, 256, 0, m->stream>>>(
@@ -1015,7 +1031,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   // graph and replayed: every argument is a fixed device buffer of the handle, and systems that
   // have converged skip their rows on the device (done[s]), so a replay equals the launches.
   const bool graph = !w->no_graph && !p->profile;
-  const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0);
+  const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0) + (view.K0lo ? 4 : 0);
   if (graph && w->pcg_exec[gk] && (w->pcg_exec_maxit[gk] != p->krylov_maxit || w->pcg_exec_lpr[gk] != lpr)) {
     cudaGraphExecDestroy(w->pcg_exec[gk]);
     w->pcg_exec[gk] = nullptr;
@@ -2238,7 +2254,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->krylov_rtol = 1e-12; p->krylov_maxit = 20000; p->precision = UA_PREC_FP64;
   p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1; p->spmv_lanes = 0; p->asm_threads = 0;
   p->uvh_krylov = UA_KRYLOV_GMRES; p->krylov_restart = 40;
-  p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1;
+  p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
   p->krylov_precond = UA_PC_AMG;
 }
 

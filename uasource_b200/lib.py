@@ -76,7 +76,7 @@ class ua_params(C.Structure):
         ("patch_nodes", C.c_int32), ("verbose", C.c_int32), ("profile", C.c_int32),
         ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32), ("spmv_lanes", C.c_int32), ("asm_threads", C.c_int32),
         ("uvh_krylov", C.c_int32), ("krylov_restart", C.c_int32),
-        ("krylov_eta_c", C.c_double), ("krylov_eta_max", C.c_double),
+        ("krylov_eta_c", C.c_double), ("krylov_eta_max", C.c_double), ("precond_bf16", C.c_int32),
     ]
 
 

@@ -81,6 +81,7 @@ class CtrlVar:
     krylov_restart: int = 40
     krylov_eta_c: float = 0.5
     krylov_eta_max: float = 0.1
+    precond_bf16: int = 1
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
