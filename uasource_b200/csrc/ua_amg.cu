@@ -492,21 +492,8 @@ template <typename KT, typename XT, int LPR>
 __device__ __forceinline__ double row_dot_csr(const int* rowptr, const int* colind, const KT* A, const XT* x, int row,
                                               bool valid, int lane) {
   double acc = 0;
-  if (valid) {
-    const int r1 = rowptr[row + 1];
-    int q = rowptr[row] + lane;
-    // four entries per step, loads first (more loads in flight), additions in entry order
-    for (; q + 3 * LPR < r1; q += 4 * LPR) {
-      const int c0 = colind[q], c1 = colind[q + LPR], c2 = colind[q + 2 * LPR], c3 = colind[q + 3 * LPR];
-      const double a0 = to_d(A[q]), a1 = to_d(A[q + LPR]), a2 = to_d(A[q + 2 * LPR]), a3 = to_d(A[q + 3 * LPR]);
-      const double x0 = (double)x[c0], x1 = (double)x[c1], x2 = (double)x[c2], x3 = (double)x[c3];
-      acc += a0 * x0;
-      acc += a1 * x1;
-      acc += a2 * x2;
-      acc += a3 * x3;
-    }
-    for (; q < r1; q += LPR) acc += to_d(A[q]) * (double)x[colind[q]];
-  }
+  if (valid)
+    for (int q = rowptr[row] + lane; q < rowptr[row + 1]; q += LPR) acc += to_d(A[q]) * (double)x[colind[q]];
 #pragma unroll
   for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
   return acc;

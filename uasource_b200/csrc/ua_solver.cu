@@ -286,19 +286,7 @@ __device__ __forceinline__ double row_dot(const int* rowptr, const int* colind, 
   double acc = 0;
   if (valid) {
     const int r0 = rowptr[row], r1 = rowptr[row + 1];
-    int j = r0 + lane;
-    // four entries per step: indices and values first, then the gathers, so that each thread
-    // has several independent loads in flight; the additions keep the entry order
-    for (; j + 3 * LPR < r1; j += 4 * LPR) {
-      const int c0 = colind[j], c1 = colind[j + LPR], c2 = colind[j + 2 * LPR], c3 = colind[j + 3 * LPR];
-      const double a0 = (double)K[j], a1 = (double)K[j + LPR], a2 = (double)K[j + 2 * LPR], a3 = (double)K[j + 3 * LPR];
-      const double x0 = (double)x[c0], x1 = (double)x[c1], x2 = (double)x[c2], x3 = (double)x[c3];
-      acc += a0 * x0;
-      acc += a1 * x1;
-      acc += a2 * x2;
-      acc += a3 * x3;
-    }
-    for (; j < r1; j += LPR) acc += (double)K[j] * (double)x[colind[j]];
+    for (int j = r0 + lane; j < r1; j += LPR) acc += (double)K[j] * (double)x[colind[j]];
   }
 #pragma unroll
   for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
