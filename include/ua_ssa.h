@@ -131,6 +131,8 @@ typedef struct ua_params {
     double krylov_eta_c, krylov_eta_max;  /* uv forcing term eta = clamp(c*sqrt(rForce), krylov_rtol, max) */
     int32_t precond_bf16;      /* mixed precision: 1 = the AMG V-cycle's finest-level passes read a BF16
                                   copy of the tangent (the PCG operator stays FP32) */
+    int32_t amg_smoothed;      /* 1 = smoothed-aggregation prolongators (default), 0 = plain aggregation;
+                                  fixed by a handle's first AMG solve */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

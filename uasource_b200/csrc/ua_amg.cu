@@ -61,10 +61,20 @@ struct AmgLevel {
   void* A = nullptr;                      // coarse values (KT)
   void* invd = nullptr;                   // l1-Jacobi inverse row sums (VT)
   void *b = nullptr, *x = nullptr, *x2 = nullptr;  // rhs, pre-smoothed, post-smoothed (VT)
+  int* d_node_off = nullptr;              // per-system node offsets on the device
+  // smoothed aggregation, transfer from this level to the next (node-level lists, global ids):
+  // pn: fine node -> coarse nodes of its neighbours' aggregates (the prolongator's node pattern);
+  // apn: fine node -> coarse nodes of A P; ptn: coarse node -> (fine node, position in pn)
+  int *sa_agg = nullptr, *pn_ptr = nullptr, *pn_col = nullptr, *apn_ptr = nullptr, *apn_col = nullptr;
+  int *ptn_ptr = nullptr, *ptn_fine = nullptr, *ptn_k = nullptr;
+  int *pbase = nullptr, *pnnz = nullptr, *poff = nullptr, *apbase = nullptr, *apnnz = nullptr, *apoff = nullptr,
+      *ptbase = nullptr;
+  double *sa_p = nullptr, *sa_pt = nullptr, *sa_ap = nullptr;  // values: 4 per node-level entry
 };
 
 struct Amg {
   int nsys = 0, nlev = 0, maxdn = 0;
+  bool sa = false;            // smoothed aggregation (else plain)
   std::vector<AmgLevel> lev;  // lev[0] = the handle's own system
   std::vector<int> depth;     // per system: its coarsest level (>= 1)
   std::vector<int> h_dn, h_doff;
@@ -167,7 +177,7 @@ static void level_csr(AmgLevel& L, const std::vector<int>& gptr, const std::vect
   L.nnz = L.knz_off[nsys];
 }
 
-int amg_setup(ua_mesh* m) {
+int amg_setup(ua_mesh* m, bool smoothed) {
   if (m->amg) return UA_OK;
   if (m->amg_failed) return UA_ERR_INVALID;
   if (m->ndof != 2 && m->ndof != 3) return set_error(UA_ERR_INVALID, "the AMG preconditioner needs uv or uvh dofs");
@@ -177,6 +187,9 @@ int amg_setup(ua_mesh* m) {
   a->depth.assign(nsys, 0);
   // node graphs per level (global ids of the level)
   std::vector<std::vector<int>> g_off{m->h_node_off}, g_ptr{m->h_nodeptr}, g_col{m->h_nodecol}, g_agg;
+  // smoothed aggregation lists per transfer (index = fine level)
+  std::vector<std::vector<int>> g_pnp, g_pnc, g_apnp, g_apnc, g_ptnp, g_ptnf, g_ptnk;
+  a->sa = smoothed;
   std::vector<char> live(nsys, 1);
   auto fail = [&](const char* why) {
     delete a;
@@ -188,9 +201,14 @@ int amg_setup(ua_mesh* m) {
     const std::vector<int>& fp = g_ptr.back();
     const std::vector<int>& fc = g_col.back();
     std::vector<int> agg(no[nsys], -1), cno(nsys + 1, 0), cptr(1, 0), ccol;
+    std::vector<int> pnp(1, 0), pnc, apnp(1, 0), apnc, ptnp(1, 0), ptnf, ptnk;
     for (int s = 0; s < nsys; ++s) {
       const int n = no[s + 1] - no[s];
-      if (!live[s] || n == 0) { cno[s + 1] = cno[s]; continue; }
+      if (!live[s] || n == 0) {
+        cno[s + 1] = cno[s];
+        for (int i = 0; i < n; ++i) { pnp.push_back((int)pnc.size()); apnp.push_back((int)apnc.size()); }
+        continue;
+      }
       std::vector<int> lp(n + 1, 0), lc, la;
       for (int i = 0; i < n; ++i) {
         for (int k = fp[no[s] + i]; k < fp[no[s] + i + 1]; ++k) lc.push_back(fc[k] - no[s]);
@@ -200,12 +218,66 @@ int amg_setup(ua_mesh* m) {
       for (int i = 0; i < n; ++i) agg[no[s] + i] = cno[s] + la[i];
       cno[s + 1] = cno[s] + na;
       std::vector<std::vector<int>> adj(na);
-      for (int i = 0; i < n; ++i)
-        for (int k = lp[i]; k < lp[i + 1]; ++k) adj[la[i]].push_back(la[lc[k]]);
+      if (!smoothed) {
+        for (int i = 0; i < n; ++i)
+          for (int k = lp[i]; k < lp[i + 1]; ++k) adj[la[i]].push_back(la[lc[k]]);
+      } else {
+        // prolongator pattern: node i reaches the aggregates of its neighbours (P = (I - w D^-1 A) P0)
+        std::vector<int> lpn(n + 1, 0), lpc, stamp(na, -1);
+        for (int i = 0; i < n; ++i) {
+          const size_t b0 = lpc.size();
+          for (int k = lp[i]; k < lp[i + 1]; ++k) {
+            const int J = la[lc[k]];
+            if (stamp[J] != i) { stamp[J] = i; lpc.push_back(J); }
+          }
+          std::sort(lpc.begin() + b0, lpc.end());
+          lpn[i + 1] = (int)lpc.size();
+        }
+        // A P pattern: node i reaches the union of its neighbours' prolongator rows
+        std::vector<int> lapn(n + 1, 0), lapc;
+        std::fill(stamp.begin(), stamp.end(), -1);
+        for (int i = 0; i < n; ++i) {
+          const size_t b0 = lapc.size();
+          for (int k = lp[i]; k < lp[i + 1]; ++k) {
+            const int h = lc[k];
+            for (int t = lpn[h]; t < lpn[h + 1]; ++t)
+              if (stamp[lpc[t]] != i) { stamp[lpc[t]] = i; lapc.push_back(lpc[t]); }
+          }
+          std::sort(lapc.begin() + b0, lapc.end());
+          lapn[i + 1] = (int)lapc.size();
+        }
+        // transpose of the prolongator pattern, with each entry's position in its fine row
+        std::vector<int> ltp(na + 1, 0), ltf(lpc.size()), ltk(lpc.size());
+        for (int t = 0; t < (int)lpc.size(); ++t) ltp[lpc[t] + 1]++;
+        for (int J = 0; J < na; ++J) ltp[J + 1] += ltp[J];
+        {
+          std::vector<int> nx(ltp.begin(), ltp.end() - 1);
+          for (int i = 0; i < n; ++i)
+            for (int t = lpn[i]; t < lpn[i + 1]; ++t) { ltf[nx[lpc[t]]] = i; ltk[nx[lpc[t]]++] = t - lpn[i]; }
+        }
+        // coarse node graph of P' A P
+        std::fill(stamp.begin(), stamp.end(), -1);
+        for (int I = 0; I < na; ++I)
+          for (int u = ltp[I]; u < ltp[I + 1]; ++u) {
+            const int i = ltf[u];
+            for (int t = lapn[i]; t < lapn[i + 1]; ++t)
+              if (stamp[lapc[t]] != I) { stamp[lapc[t]] = I; adj[I].push_back(lapc[t]); }
+          }
+        for (int i = 0; i < n; ++i) {
+          for (int t = lpn[i]; t < lpn[i + 1]; ++t) pnc.push_back(cno[s] + lpc[t]);
+          pnp.push_back((int)pnc.size());
+          for (int t = lapn[i]; t < lapn[i + 1]; ++t) apnc.push_back(cno[s] + lapc[t]);
+          apnp.push_back((int)apnc.size());
+        }
+        for (int J = 0; J < na; ++J) {
+          for (int u = ltp[J]; u < ltp[J + 1]; ++u) { ptnf.push_back(no[s] + ltf[u]); ptnk.push_back(ltk[u]); }
+          ptnp.push_back((int)ptnf.size());
+        }
+      }
       for (int I = 0; I < na; ++I) {
         std::sort(adj[I].begin(), adj[I].end());
         adj[I].erase(std::unique(adj[I].begin(), adj[I].end()), adj[I].end());
-        if (2 * (int)adj[I].size() > kAmgMaxRow) return fail("coarse node degree above the row limit");
+        if (!smoothed && 2 * (int)adj[I].size() > kAmgMaxRow) return fail("coarse node degree above the row limit");
         for (int J : adj[I]) ccol.push_back(cno[s] + J);
         cptr.push_back((int)ccol.size());
       }
@@ -217,6 +289,8 @@ int amg_setup(ua_mesh* m) {
     g_off.push_back(cno);
     g_ptr.push_back(cptr);
     g_col.push_back(ccol);
+    g_pnp.push_back(pnp); g_pnc.push_back(pnc); g_apnp.push_back(apnp); g_apnc.push_back(apnc);
+    g_ptnp.push_back(ptnp); g_ptnf.push_back(ptnf); g_ptnk.push_back(ptnk);
   }
   a->nlev = (int)g_off.size();
   a->lev.resize(a->nlev);
@@ -298,6 +372,42 @@ int amg_setup(ua_mesh* m) {
   std::vector<void*> pb(a->nlev), px2(a->nlev), pA(a->nlev);
   std::vector<int*> prp(a->nlev), pci(a->nlev), pdo(a->nlev);
   for (int l = 0; l < a->nlev; ++l) {
+    a->lev[l].d_node_off = upload(m, a, a->lev[l].node_off, ok);
+    if (!a->lev[l].dof_sys) {  // a uv handle's finest level: rows -> system, for the smoothed transfer
+      std::vector<int> ds(a->lev[l].ndof);
+      for (int s = 0; s < nsys; ++s)
+        for (int d = a->lev[l].dof_off[s]; d < a->lev[l].dof_off[s + 1]; ++d) ds[d] = s;
+      a->lev[l].dof_sys = upload(m, a, ds, ok);
+    }
+    if (a->sa && l + 1 < a->nlev) {
+      AmgLevel& F = a->lev[l];
+      const AmgLevel& C = a->lev[l + 1];
+      F.sa_agg = upload(m, a, g_agg[l], ok);
+      F.pn_ptr = upload(m, a, g_pnp[l], ok);
+      F.pn_col = upload(m, a, g_pnc[l], ok);
+      F.apn_ptr = upload(m, a, g_apnp[l], ok);
+      F.apn_col = upload(m, a, g_apnc[l], ok);
+      F.ptn_ptr = upload(m, a, g_ptnp[l], ok);
+      F.ptn_fine = upload(m, a, g_ptnf[l], ok);
+      F.ptn_k = upload(m, a, g_ptnk[l], ok);
+      std::vector<int> pbase(nsys), pnnz(nsys), poff(nsys + 1, 0), apbase(nsys), apnnz(nsys), apoff(nsys + 1, 0),
+          ptbase(nsys);
+      for (int s = 0; s < nsys; ++s) {
+        pbase[s] = g_pnp[l][F.node_off[s]];
+        pnnz[s] = g_pnp[l][F.node_off[s + 1]] - pbase[s];
+        poff[s + 1] = poff[s] + 4 * pnnz[s];
+        apbase[s] = g_apnp[l][F.node_off[s]];
+        apnnz[s] = g_apnp[l][F.node_off[s + 1]] - apbase[s];
+        apoff[s + 1] = apoff[s] + 4 * apnnz[s];
+        ptbase[s] = g_ptnp[l][C.node_off[s]];
+      }
+      F.pbase = upload(m, a, pbase, ok); F.pnnz = upload(m, a, pnnz, ok); F.poff = upload(m, a, poff, ok);
+      F.apbase = upload(m, a, apbase, ok); F.apnnz = upload(m, a, apnnz, ok); F.apoff = upload(m, a, apoff, ok);
+      F.ptbase = upload(m, a, ptbase, ok);
+      F.sa_p = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
+      F.sa_pt = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
+      F.sa_ap = (double*)dalloc(m, a, sizeof(double) * (size_t)apoff[nsys], ok);
+    }
     pb[l] = a->lev[l].b;
     px2[l] = a->lev[l].x2;
     pA[l] = a->lev[l].A;
@@ -599,6 +709,199 @@ __global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const i
 }
 
 // ---------------------------------------------------------------------------
+// device: smoothed aggregation (P = (I - w D^-1 A) P0, coarse operator P' A P)
+// ---------------------------------------------------------------------------
+//
+// Values live on node-level lists with the tangent's layout rule: the entry of
+// dof row (c, g), column component c2 and list position k of system s sits at
+// off[s] + c*2*nnz[s] + 2*(ptr[g] - base[s]) + c2*deg(g) + k.  One thread owns
+// each output row and sums in a fixed order.
+
+constexpr double kSaOmega = 4.0 / 3.0;  // damping of the prolongator smoother (l1 diagonal: rho(D^-1 A) <= 1)
+
+__device__ __forceinline__ int sa_find(const int* list, int n, int key) {
+  for (int k = 0; k < n; ++k)
+    if (list[k] == key) return k;
+  return -1;
+}
+
+// dof row -> system, component, node (global) of a level
+__device__ __forceinline__ void sa_decode(int i, const int* dof_sys, const int* dof_off, const int* node_off, int& s,
+                                          int& c, int& g) {
+  s = dof_sys[i];
+  const int no = node_off[s], nn = node_off[s + 1] - no, loc = i - dof_off[s];
+  c = loc / nn;
+  g = no + (loc - c * nn);
+}
+
+// prolongator rows: P(i,:) = P0(i,:) - w invd_i A(i,:) P0 on unmasked rows and columns
+template <typename KT, typename VT>
+__global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int* node_off, const int* rowptr,
+                       const int* colind, const KT* A, const unsigned char* mask, const VT* invd, const int* agg,
+                       const int* pn_ptr, const int* pn_col, const int* pbase, const int* pnnz, const int* poff,
+                       double* P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  int s, c, g;
+  sa_decode(i, dof_sys, dof_off, node_off, s, c, g);
+  const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
+  double* row = P + poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]);
+  for (int t = 0; t < 2 * dP; ++t) row[t] = 0;
+  if (mask && mask[i]) return;
+  const int k0 = sa_find(pn_col + pr, dP, agg[g]);
+  if (k0 >= 0) row[c * dP + k0] = 1.0;
+  const double f = kSaOmega * (double)invd[i];
+  for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+    const int j = colind[q];
+    if (mask && mask[j]) continue;
+    int s2, c2, h;
+    sa_decode(j, dof_sys, dof_off, node_off, s2, c2, h);
+    const int k = sa_find(pn_col + pr, dP, agg[h]);
+    if (k >= 0) row[c2 * dP + k] -= f * (double)A[q];
+  }
+}
+
+// A P rows: AP(i,:) = sum over unmasked columns j of A(i,j) P(j,:)
+// one thread per (row, column block c3): the two blocks of a row are independent outputs
+template <typename KT>
+__global__ void k_sa_AP(int nf, const int* dof_sys, const int* dof_off, const int* node_off, const int* rowptr,
+                        const int* colind, const KT* A, const unsigned char* mask, const int* pn_ptr,
+                        const int* pn_col, const int* pbase, const int* pnnz, const int* poff, const double* P,
+                        const int* apn_ptr, const int* apn_col, const int* apbase, const int* apnnz, const int* apoff,
+                        double* AP) {
+  const int t2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t2 >= 2 * nf) return;
+  const int i = t2 >> 1, c3 = t2 & 1;
+  int s, c, g;
+  sa_decode(i, dof_sys, dof_off, node_off, s, c, g);
+  const int ar = apn_ptr[g], dA = apn_ptr[g + 1] - ar;
+  double* row = AP + apoff[s] + (size_t)c * 2 * apnnz[s] + 2 * (size_t)(ar - apbase[s]) + c3 * dA;
+  for (int t = 0; t < dA; ++t) row[t] = 0;
+  if (mask && mask[i]) return;
+  for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+    const int j = colind[q];
+    if (mask && mask[j]) continue;
+    const double a = (double)A[q];
+    int s2, c2, h;
+    sa_decode(j, dof_sys, dof_off, node_off, s2, c2, h);
+    const int pj = pn_ptr[h], dPj = pn_ptr[h + 1] - pj;
+    const double* prow = P + poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(pj - pbase[s]) + c3 * dPj;
+    int kk = 0;  // both lists are sorted: merge
+    for (int k = 0; k < dPj; ++k) {
+      const double w = prow[k];
+      const int J = pn_col[pj + k];
+      while (kk < dA && apn_col[ar + kk] < J) ++kk;
+      if (w != 0.0 && kk < dA && apn_col[ar + kk] == J) row[kk] += a * w;
+    }
+  }
+}
+
+// transpose values: P'(R = (c2, J), (c, u)) = P((c, fine node u of J), (c2, J))
+__global__ void k_sa_PT(int nc, const int* cdof_sys, const int* cdof_off, const int* cnode_off, const int* ptn_ptr,
+                        const int* ptn_fine, const int* ptn_k, const int* ptbase, const int* pn_ptr,
+                        const int* pbase, const int* pnnz, const int* poff, const double* P, double* PT) {
+  const int R = blockIdx.x * blockDim.x + threadIdx.x;
+  if (R >= nc) return;
+  int s, c2, J;
+  sa_decode(R, cdof_sys, cdof_off, cnode_off, s, c2, J);
+  const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
+  double* row = PT + poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
+  for (int c = 0; c < 2; ++c)
+    for (int u = 0; u < dT; ++u) {
+      const int g = ptn_fine[tr + u], pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
+      row[c * dT + u] = P[poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]) + c2 * dP + ptn_k[tr + u]];
+    }
+}
+
+// coarse operator rows: Ac(R,:) = sum over P'(R, i) AP(i,:), into the coarse level's CSR
+template <typename KT>
+__global__ void k_sa_Ac(int nc, const int* cdof_sys, const int* cdof_off, const int* cnode_off, const int* crowptr,
+                        const int* ccolind, const int* ptn_ptr, const int* ptn_fine, const int* ptbase,
+                        const int* pnnz, const int* poff, const double* PT, const int* apn_ptr, const int* apn_col,
+                        const int* apbase, const int* apnnz, const int* apoff, const double* AP, KT* Ac) {
+  const int t2 = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per (coarse row, column block c3)
+  if (t2 >= 2 * nc) return;
+  const int R = t2 >> 1, c3 = t2 & 1;
+  int s, c2, J;
+  sa_decode(R, cdof_sys, cdof_off, cnode_off, s, c2, J);
+  const int cr0 = crowptr[R], degc = (crowptr[R + 1] - cr0) >> 1;
+  KT* out = Ac + cr0 + c3 * degc;
+  for (int t = 0; t < degc; ++t) out[t] = (KT)0;
+  const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
+  const double* trow = PT + poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
+  const int cbase = cdof_off[s] - cnode_off[s];  // u-column dof of coarse node K: cbase + K
+  const int* ucol = ccolind + cr0;                // sorted u-block columns of the coarse row
+  for (int c = 0; c < 2; ++c)
+    for (int u = 0; u < dT; ++u) {
+      const double w = trow[c * dT + u];
+      if (w == 0.0) continue;
+      const int g = ptn_fine[tr + u], ar = apn_ptr[g], dA = apn_ptr[g + 1] - ar;
+      const double* arow = AP + apoff[s] + (size_t)c * 2 * apnnz[s] + 2 * (size_t)(ar - apbase[s]) + c3 * dA;
+      int pos = 0;  // both lists are sorted: merge
+      for (int kk = 0; kk < dA; ++kk) {
+        const int key = cbase + apn_col[ar + kk];
+        while (pos < degc && ucol[pos] < key) ++pos;
+        const double v = arow[kk];
+        if (v != 0.0 && pos < degc && ucol[pos] == key) out[pos] += (KT)(w * v);
+      }
+    }
+}
+
+// restriction b_c = P' res (coarse pre-smoothing x_c = invd b_c unless lc is the system's coarsest)
+// kSaRL lanes per coarse row (the row's 2*dT entries split over the lanes, then a lane sum)
+constexpr int kSaRL = 8;
+template <typename VT>
+__global__ void __launch_bounds__(256) k_sa_restrict(int nc, const int* cdof_sys, const int* cdof_off,
+                                                     const int* cnode_off, const int* depth, int lc, const int* sel,
+                                                     const int* done, const int* ptn_ptr, const int* ptn_fine,
+                                                     const int* ptbase, const int* pnnz, const int* poff,
+                                                     const double* PT, const int* fdof_off, const int* fnode_off,
+                                                     const VT* res, const VT* cinvd, VT* cb, VT* cx) {
+  const int R0 = (blockIdx.x * blockDim.x + threadIdx.x) / kSaRL, lane = threadIdx.x % kSaRL;
+  const bool valid = R0 < nc;
+  const int R = valid ? R0 : nc - 1;
+  int s, c2, J;
+  sa_decode(R, cdof_sys, cdof_off, cnode_off, s, c2, J);
+  const bool act = valid && sel[s] && !done[s];
+  double acc = 0;
+  if (act) {
+    const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
+    const double* trow = PT + poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
+    const int fno = fnode_off[s], fnn = fnode_off[s + 1] - fno, fd = fdof_off[s];
+    for (int t = lane; t < 2 * dT; t += kSaRL) {
+      const int c = t >= dT ? 1 : 0, u = t - c * dT;
+      acc += trow[t] * (double)res[fd + c * fnn + (ptn_fine[tr + u] - fno)];
+    }
+  }
+#pragma unroll
+  for (int o = kSaRL / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, kSaRL);
+  if (act && lane == 0) {
+    cb[R] = (VT)acc;
+    if (depth[s] > lc) cx[R] = (VT)((double)cinvd[R] * acc);
+  }
+}
+
+// prolongation x += P x_c on level l (systems deeper than l; masked rows have zero P rows)
+template <typename VT>
+__global__ void k_sa_prolong(int nf, const int* dof_sys, const int* dof_off, const int* node_off, const int* depth,
+                             int l, const int* sel, const int* done, const int* pn_ptr, const int* pn_col,
+                             const int* pbase, const int* pnnz, const int* poff, const double* P,
+                             const int* cdof_off, const int* cnode_off, const VT* xc, VT* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  int s, c, g;
+  sa_decode(i, dof_sys, dof_off, node_off, s, c, g);
+  if (!sel[s] || done[s] || depth[s] <= l) return;
+  const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
+  const double* row = P + poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]);
+  const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno, cd = cdof_off[s];
+  double acc = (double)x[i];
+  for (int c2 = 0; c2 < 2; ++c2)
+    for (int k = 0; k < dP; ++k) acc += row[c2 * dP + k] * (double)xc[cd + c2 * cnn + (pn_col[pr + k] - cno)];
+  x[i] = (VT)acc;
+}
+
+// ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
 
@@ -607,18 +910,45 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
                      long long* launches) {
   Amg* a = m->amg;
   cudaStream_t st = m->stream;
-  for (int l = 0; l + 1 < a->nlev; ++l) {
-    const AmgLevel& F = a->lev[l];
-    const AmgLevel& C = a->lev[l + 1];
-    k_amg_galerkin<KT><<<(C.ndof + 127) / 128, 128, 0, st>>>(
-        C.ndof, C.mptr, C.mlist, l == 0 ? rowptr0 : F.rowptr, l == 0 ? colind0 : F.colind,
-        l == 0 ? K0 : (const KT*)F.A, F.cmap, l == 0 ? cmask : nullptr, C.rowptr, C.colind, (KT*)C.A), ++*launches;
-  }
-  for (int l = 0; l < a->nlev; ++l) {
+  auto l1 = [&](int l) {
     const AmgLevel& L = a->lev[l];
     k_amg_l1<KT, VT><<<(L.ndof + 255) / 256, 256, 0, st>>>(
         L.ndof, l == 0 ? rowptr0 : L.rowptr, l == 0 ? colind0 : L.colind, l == 0 ? K0 : (const KT*)L.A,
         l == 0 ? cmask : nullptr, (VT*)L.invd), ++*launches;
+  };
+  if (a->sa) {
+    // per level: smoother diagonal, smoothed prolongator, A P, P' values, coarse operator
+    for (int l = 0; l + 1 < a->nlev; ++l) {
+      AmgLevel& F = a->lev[l];
+      AmgLevel& C = a->lev[l + 1];
+      const int* rp = l == 0 ? rowptr0 : F.rowptr;
+      const int* ci = l == 0 ? colind0 : F.colind;
+      const KT* A = l == 0 ? K0 : (const KT*)F.A;
+      const unsigned char* mk = l == 0 ? cmask : nullptr;
+      l1(l);
+      const int nbf = (F.ndof + 127) / 128, nbc = (C.ndof + 127) / 128;
+      k_sa_P<KT, VT><<<nbf, 128, 0, st>>>(F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk,
+                                          (const VT*)F.invd, F.sa_agg, F.pn_ptr, F.pn_col, F.pbase, F.pnnz, F.poff,
+                                          F.sa_p), ++*launches;
+      k_sa_AP<KT><<<(2 * F.ndof + 127) / 128, 128, 0, st>>>(F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr,
+                                       F.pn_col, F.pbase, F.pnnz, F.poff, F.sa_p, F.apn_ptr, F.apn_col, F.apbase,
+                                       F.apnnz, F.apoff, F.sa_ap), ++*launches;
+      k_sa_PT<<<nbc, 128, 0, st>>>(C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, F.ptn_ptr, F.ptn_fine, F.ptn_k,
+                                   F.ptbase, F.pn_ptr, F.pbase, F.pnnz, F.poff, F.sa_p, F.sa_pt), ++*launches;
+      k_sa_Ac<KT><<<(2 * C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr,
+                                       F.ptn_fine, F.ptbase, F.pnnz, F.poff, F.sa_pt, F.apn_ptr, F.apn_col, F.apbase,
+                                       F.apnnz, F.apoff, F.sa_ap, (KT*)C.A), ++*launches;
+    }
+    l1(a->nlev - 1);
+  } else {
+    for (int l = 0; l + 1 < a->nlev; ++l) {
+      const AmgLevel& F = a->lev[l];
+      const AmgLevel& C = a->lev[l + 1];
+      k_amg_galerkin<KT><<<(C.ndof + 127) / 128, 128, 0, st>>>(
+          C.ndof, C.mptr, C.mlist, l == 0 ? rowptr0 : F.rowptr, l == 0 ? colind0 : F.colind,
+          l == 0 ? K0 : (const KT*)F.A, F.cmap, l == 0 ? cmask : nullptr, C.rowptr, C.colind, (KT*)C.A), ++*launches;
+    }
+    for (int l = 0; l < a->nlev; ++l) l1(l);
   }
   const int sm = (int)(sizeof(double) * (size_t)a->maxdn * 2 * a->maxdn);
   UA_CUDA_TRY(cudaFuncSetAttribute(k_amg_dense_inverse<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
@@ -680,17 +1010,29 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     });
     ++*launches;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 1);
-    k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done,
-                                                           C.mptr, C.mlist, W(l), (const VT*)C.invd, (VT*)C.b,
-                                                           (VT*)C.x), ++*launches;
+    const AmgLevel& F = a->lev[l];
+    if (a->sa)
+      k_sa_restrict<VT><<<(int)(((long long)C.ndof * kSaRL + 255) / 256), 256, 0, st>>>(
+          C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, a->d_depth, l + 1, v.sel, v.done, F.ptn_ptr, F.ptn_fine,
+          F.ptbase, F.pnnz, F.poff, F.sa_pt, F.d_dof_off, F.d_node_off, W(l), (const VT*)C.invd, (VT*)C.b,
+          (VT*)C.x), ++*launches;
+    else
+      k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done,
+                                                             C.mptr, C.mlist, W(l), (const VT*)C.invd, (VT*)C.b,
+                                                             (VT*)C.x), ++*launches;
   }
   k_amg_dense_apply<VT><<<dim3(a->nsys, (a->maxdn + 31) / 32), 256, 0, st>>>(
       v.sel, v.done, a->d_depth, a->d_dn, a->d_doff, a->d_lev_dofoff, a->d_lev_b, a->d_lev_x2, a->dense), ++*launches;
   for (int l = nl - 2; l >= 0; --l) {  // up: correction from level l+1's post-smoothed x2, then smoothing
     const AmgLevel& F = a->lev[l];
     const AmgLevel& C = a->lev[l + 1];
-    k_amg_correct<VT><<<nrb(l), 256, 0, st>>>(rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, X(l),
-                                              (const VT*)C.x2, F.cmap, mask(l)), ++*launches;
+    if (a->sa)
+      k_sa_prolong<VT><<<(F.ndof + 255) / 256, 256, 0, st>>>(
+          F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, a->d_depth, l, v.sel, v.done, F.pn_ptr, F.pn_col, F.pbase,
+          F.pnnz, F.poff, F.sa_p, C.d_dof_off, C.d_node_off, (const VT*)C.x2, X(l)), ++*launches;
+    else
+      k_amg_correct<VT><<<nrb(l), 256, 0, st>>>(rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, X(l),
+                                                (const VT*)C.x2, F.cmap, mask(l)), ++*launches;
     VT* out = l == 0 ? (VT*)v.z : (VT*)F.x2;
     VT* pcopy = l == 0 ? (VT*)v.pcopy : nullptr;
     double* part = l == 0 ? v.part_rz : nullptr;

@@ -33,9 +33,10 @@ struct AmgPcgView {
 };
 
 // Build the hierarchy of every system of the handle (host aggregation,
-// device structures); no-op when built.  Returns UA_OK or an error code
+// device structures; smoothed = smoothed-aggregation prolongators, else
+// piecewise constant); no-op when built (the first call fixes the kind).  Returns UA_OK or an error code
 // (the handle then keeps point-Jacobi).
-int amg_setup(ua_mesh* m);
+int amg_setup(ua_mesh* m, bool smoothed);
 void amg_free(Amg* a);
 int amg_levels(const ua_mesh* m);
 // l1-Jacobi inverse row sums of the fine level (VT-typed, valid after amg_numeric)

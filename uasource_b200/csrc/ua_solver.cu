@@ -937,7 +937,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     w->kx0 = walloc<double>(m, N);
     if (!w->kx0) return set_error(UA_ERR_OOM, "device allocation of the AMG work vector failed");
   }
-  if (amg && amg_setup(m) != UA_OK) amg = false;  // shapes the hierarchy cannot take keep point Jacobi
+  if (amg && amg_setup(m, p->amg_smoothed != 0) != UA_OK) amg = false;  // shapes the hierarchy cannot take keep point Jacobi
   const bool fp32 = sizeof(KT) == 4;
   if (amg) {
     int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches);
@@ -1547,7 +1547,7 @@ static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out,
   // block preconditioner: the aggregation-AMG V-cycle of the velocity block on the u, v rows,
   // point Jacobi on the h rows (the coupling blocks are left to the Krylov iteration)
   bool amg = p->krylov_precond == UA_PC_AMG && m->ndof == 3 && !m->h_nodeptr.empty() && sizeof(KT) == 8;
-  if (amg && amg_setup(m) != UA_OK) amg = false;
+  if (amg && amg_setup(m, p->amg_smoothed != 0) != UA_OK) amg = false;
   if (amg) {
     int rc = amg_numeric_uvh(m, (const double*)K, w->cmask, &g_launches);
     if (rc) return rc;
@@ -1790,7 +1790,7 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
   double* invd = (double*)w->invd;
   k_invdiag<KT, double><<<(N + 255) / 256, 256, 0, st>>>(N, K, w->diagpos, w->cmask, invd), ++g_launches;
   bool amg = p->krylov_precond == UA_PC_AMG && m->ndof == 3 && !m->h_nodeptr.empty() && sizeof(KT) == 8;
-  if (amg && amg_setup(m) != UA_OK) amg = false;
+  if (amg && amg_setup(m, p->amg_smoothed != 0) != UA_OK) amg = false;
   if (amg) {
     int rc = amg_numeric_uvh(m, (const double*)K, w->cmask, &g_launches);
     if (rc) return rc;
@@ -2243,6 +2243,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1; p->spmv_lanes = 0; p->asm_threads = 0;
   p->uvh_krylov = UA_KRYLOV_GMRES; p->krylov_restart = 40;
   p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
+  p->amg_smoothed = 1;
   p->krylov_precond = UA_PC_AMG;
 }
 
