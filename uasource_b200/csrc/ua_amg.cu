@@ -29,6 +29,7 @@ namespace ua {
 
 constexpr int kAmgCoarseNodes = 48;   // a system stops coarsening at this many nodes
 constexpr int kAmgMaxRow = 32;        // longest coarse dof row (2 x coarse node degree)
+constexpr int kSaMaxDeg = 256;        // largest coarse node degree of a smoothed hierarchy (shared-memory rows)
 constexpr int kAmgMaxDense = 2 * kAmgCoarseNodes;
 constexpr int kAmgRB = 256;           // rows per row block of a coarse level
 
@@ -62,6 +63,7 @@ struct AmgLevel {
   void* invd = nullptr;                   // l1-Jacobi inverse row sums (VT)
   void *b = nullptr, *x = nullptr, *x2 = nullptr;  // rhs, pre-smoothed, post-smoothed (VT)
   int* d_node_off = nullptr;              // per-system node offsets on the device
+  int* node_sys = nullptr;                // node -> system (smoothed hierarchies)
   // smoothed aggregation, transfer from this level to the next (node-level lists, global ids):
   // pn: fine node -> coarse nodes of its neighbours' aggregates (the prolongator's node pattern);
   // apn: fine node -> coarse nodes of A P; ptn: coarse node -> (fine node, position in pn)
@@ -70,6 +72,7 @@ struct AmgLevel {
   int *pbase = nullptr, *pnnz = nullptr, *poff = nullptr, *apbase = nullptr, *apnnz = nullptr, *apoff = nullptr,
       *ptbase = nullptr;
   double *sa_p = nullptr, *sa_pt = nullptr, *sa_ap = nullptr;  // values: 4 per node-level entry
+  float *sa_plo = nullptr, *sa_ptlo = nullptr;  // FP32 copies of P and P' for the mixed-precision transfers
 };
 
 struct Amg {
@@ -177,10 +180,7 @@ static void level_csr(AmgLevel& L, const std::vector<int>& gptr, const std::vect
   L.nnz = L.knz_off[nsys];
 }
 
-int amg_setup(ua_mesh* m, bool smoothed) {
-  if (m->amg) return UA_OK;
-  if (m->amg_failed) return UA_ERR_INVALID;
-  if (m->ndof != 2 && m->ndof != 3) return set_error(UA_ERR_INVALID, "the AMG preconditioner needs uv or uvh dofs");
+static int amg_build(ua_mesh* m, bool smoothed) {
   const int nsys = m->dm.nsys;
   Amg* a = new Amg();
   a->nsys = nsys;
@@ -193,7 +193,6 @@ int amg_setup(ua_mesh* m, bool smoothed) {
   std::vector<char> live(nsys, 1);
   auto fail = [&](const char* why) {
     delete a;
-    m->amg_failed = true;
     return set_error(UA_ERR_INVALID, "AMG setup: %s", why);
   };
   while (std::find(live.begin(), live.end(), 1) != live.end()) {
@@ -278,6 +277,7 @@ int amg_setup(ua_mesh* m, bool smoothed) {
         std::sort(adj[I].begin(), adj[I].end());
         adj[I].erase(std::unique(adj[I].begin(), adj[I].end()), adj[I].end());
         if (!smoothed && 2 * (int)adj[I].size() > kAmgMaxRow) return fail("coarse node degree above the row limit");
+        if (smoothed && (int)adj[I].size() > kSaMaxDeg) return fail("smoothed coarse node degree above the limit");
         for (int J : adj[I]) ccol.push_back(cno[s] + J);
         cptr.push_back((int)ccol.size());
       }
@@ -373,6 +373,12 @@ int amg_setup(ua_mesh* m, bool smoothed) {
   std::vector<int*> prp(a->nlev), pci(a->nlev), pdo(a->nlev);
   for (int l = 0; l < a->nlev; ++l) {
     a->lev[l].d_node_off = upload(m, a, a->lev[l].node_off, ok);
+    if (a->sa) {
+      std::vector<int> ns(std::max(a->lev[l].node_off[nsys], 1), 0);
+      for (int s = 0; s < nsys; ++s)
+        for (int g = a->lev[l].node_off[s]; g < a->lev[l].node_off[s + 1]; ++g) ns[g] = s;
+      a->lev[l].node_sys = upload(m, a, ns, ok);
+    }
     if (!a->lev[l].dof_sys) {  // a uv handle's finest level: rows -> system, for the smoothed transfer
       std::vector<int> ds(a->lev[l].ndof);
       for (int s = 0; s < nsys; ++s)
@@ -407,6 +413,8 @@ int amg_setup(ua_mesh* m, bool smoothed) {
       F.sa_p = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
       F.sa_pt = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
       F.sa_ap = (double*)dalloc(m, a, sizeof(double) * (size_t)apoff[nsys], ok);
+      F.sa_plo = (float*)dalloc(m, a, sizeof(float) * (size_t)poff[nsys], ok);
+      F.sa_ptlo = (float*)dalloc(m, a, sizeof(float) * (size_t)poff[nsys], ok);
     }
     pb[l] = a->lev[l].b;
     px2[l] = a->lev[l].x2;
@@ -428,6 +436,18 @@ int amg_setup(ua_mesh* m, bool smoothed) {
   }
   m->amg = a;
   return UA_OK;
+}
+
+// smoothed aggregation first (when asked), plain aggregation if the smoothed hierarchy
+// exceeds its limits; a shape neither can take keeps point Jacobi for the handle's life
+int amg_setup(ua_mesh* m, bool smoothed) {
+  if (m->amg) return UA_OK;
+  if (m->amg_failed) return UA_ERR_INVALID;
+  if (m->ndof != 2 && m->ndof != 3) return set_error(UA_ERR_INVALID, "the AMG preconditioner needs uv or uvh dofs");
+  int rc = amg_build(m, smoothed);
+  if (rc == UA_ERR_INVALID && smoothed) rc = amg_build(m, false);
+  if (rc == UA_ERR_INVALID) m->amg_failed = true;
+  return rc;
 }
 
 void amg_free(Amg* a) { delete a; }
@@ -714,15 +734,18 @@ __global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const i
 //
 // Values live on node-level lists with the tangent's layout rule: the entry of
 // dof row (c, g), column component c2 and list position k of system s sits at
-// off[s] + c*2*nnz[s] + 2*(ptr[g] - base[s]) + c2*deg(g) + k.  One thread owns
-// each output row and sums in a fixed order.
+// off[s] + c*2*nnz[s] + 2*(ptr[g] - base[s]) + c2*deg(g) + k.  Every output
+// entry is summed in a fixed order (no atomics), so results are reproducible.
 
 constexpr double kSaOmega = 4.0 / 3.0;  // damping of the prolongator smoother (l1 diagonal: rho(D^-1 A) <= 1)
 
-__device__ __forceinline__ int sa_find(const int* list, int n, int key) {
-  for (int k = 0; k < n; ++k)
-    if (list[k] == key) return k;
-  return -1;
+__device__ __forceinline__ int sa_find(const int* list, int n, int key) {  // list sorted ascending
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (list[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return lo < n && list[lo] == key ? lo : -1;
 }
 
 // dof row -> system, component, node (global) of a level
@@ -761,144 +784,230 @@ __global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int
   }
 }
 
-// A P rows: AP(i,:) = sum over unmasked columns j of A(i,j) P(j,:)
-// one thread per (row, column block c3): the two blocks of a row are independent outputs
+// A P rows: AP(i,:) = sum over unmasked columns j of A(i,j) P(j,:), kSaGL lanes per fine node g.
+// Both rows (c = 0, 1) of the node share its neighbour list, so each neighbour h contributes
+// A((c,g),(c2,h)) P((c2,h),:) to four output blocks (c, c3) at once; the neighbours go in
+// order and the lanes take the entries of P(h,:), whose targets in the AP row are distinct:
+// a fixed summation order without atomics
+constexpr int kSaGL = 8;
 template <typename KT>
-__global__ void k_sa_AP(int nf, const int* dof_sys, const int* dof_off, const int* node_off, const int* rowptr,
-                        const int* colind, const KT* A, const unsigned char* mask, const int* pn_ptr,
-                        const int* pn_col, const int* pbase, const int* pnnz, const int* poff, const double* P,
-                        const int* apn_ptr, const int* apn_col, const int* apbase, const int* apnnz, const int* apoff,
-                        double* AP) {
-  const int t2 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t2 >= 2 * nf) return;
-  const int i = t2 >> 1, c3 = t2 & 1;
-  int s, c, g;
-  sa_decode(i, dof_sys, dof_off, node_off, s, c, g);
+__global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, const int* dof_off, const int* node_off,
+                                               const int* rowptr, const int* colind, const KT* A,
+                                               const unsigned char* mask, const int* pn_ptr, const int* pn_col,
+                                               const int* pbase, const int* pnnz, const int* poff, const double* P,
+                                               const int* apn_ptr, const int* apn_col, const int* apbase,
+                                               const int* apnnz, const int* apoff, double* AP) {
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) / kSaGL, lane = threadIdx.x % kSaGL;
+  if (g >= nfn) return;  // whole groups leave together
+  const unsigned gmask = ((1u << kSaGL) - 1u) << ((threadIdx.x & 31) & ~(kSaGL - 1));
+  const int s = node_sys[g];
+  const int no = node_off[s], nn = node_off[s + 1] - no, d0 = dof_off[s];
+  const int i0 = d0 + (g - no), i1 = i0 + nn;
   const int ar = apn_ptr[g], dA = apn_ptr[g + 1] - ar;
-  double* row = AP + apoff[s] + (size_t)c * 2 * apnnz[s] + 2 * (size_t)(ar - apbase[s]) + c3 * dA;
-  for (int t = 0; t < dA; ++t) row[t] = 0;
-  if (mask && mask[i]) return;
-  for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
-    const int j = colind[q];
-    if (mask && mask[j]) continue;
-    const double a = (double)A[q];
-    int s2, c2, h;
-    sa_decode(j, dof_sys, dof_off, node_off, s2, c2, h);
+  const int* acol = apn_col + ar;
+  const size_t ars = (size_t)2 * apnnz[s];  // AP row stride between c = 0 and c = 1
+  double* r0 = AP + apoff[s] + 2 * (size_t)(ar - apbase[s]);
+  for (int t = lane; t < 2 * dA; t += kSaGL) {
+    r0[t] = 0;
+    r0[ars + t] = 0;
+  }
+  const bool m0 = mask && mask[i0], m1 = mask && mask[i1];
+  if (m0 && m1) return;
+  const int q0 = rowptr[i0], q1 = rowptr[i1], deg = (rowptr[i0 + 1] - q0) >> 1;
+  const size_t prs = (size_t)2 * pnnz[s];  // P row stride between c2 = 0 and c2 = 1
+  for (int k = 0; k < deg; ++k) {
+    const int ju = colind[q0 + k], jv = ju + nn;  // u and v dofs of neighbour node h
+    const bool cu = mask && mask[ju], cv = mask && mask[jv];
+    const double a00 = (m0 || cu) ? 0.0 : (double)A[q0 + k], a01 = (m0 || cv) ? 0.0 : (double)A[q0 + deg + k];
+    const double a10 = (m1 || cu) ? 0.0 : (double)A[q1 + k], a11 = (m1 || cv) ? 0.0 : (double)A[q1 + deg + k];
+    if (a00 == 0.0 && a01 == 0.0 && a10 == 0.0 && a11 == 0.0) continue;  // uniform over the group
+    const int h = no + (ju - d0);
     const int pj = pn_ptr[h], dPj = pn_ptr[h + 1] - pj;
-    const double* prow = P + poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(pj - pbase[s]) + c3 * dPj;
-    int kk = 0;  // both lists are sorted: merge
-    for (int k = 0; k < dPj; ++k) {
-      const double w = prow[k];
-      const int J = pn_col[pj + k];
-      while (kk < dA && apn_col[ar + kk] < J) ++kk;
-      if (w != 0.0 && kk < dA && apn_col[ar + kk] == J) row[kk] += a * w;
+    const double* ph = P + poff[s] + 2 * (size_t)(pj - pbase[s]);
+    __syncwarp(gmask);  // the previous neighbour's updates are visible to the group
+    for (int t = lane; t < dPj; t += kSaGL) {
+      const int kk = sa_find(acol, dA, pn_col[pj + t]);
+      if (kk < 0) continue;
+#pragma unroll
+      for (int c3 = 0; c3 < 2; ++c3) {
+        const double p0 = ph[c3 * dPj + t], p1 = ph[prs + c3 * dPj + t];
+        r0[c3 * dA + kk] += a00 * p0 + a01 * p1;
+        r0[ars + c3 * dA + kk] += a10 * p0 + a11 * p1;
+      }
     }
   }
 }
 
-// transpose values: P'(R = (c2, J), (c, u)) = P((c, fine node u of J), (c2, J))
+// transpose values: P'(R = (c2, J), (c, u)) = P((c, fine node u of J), (c2, J)), and FP32 copies
+// of both (every P entry is the image of exactly one P' entry)
 __global__ void k_sa_PT(int nc, const int* cdof_sys, const int* cdof_off, const int* cnode_off, const int* ptn_ptr,
                         const int* ptn_fine, const int* ptn_k, const int* ptbase, const int* pn_ptr,
-                        const int* pbase, const int* pnnz, const int* poff, const double* P, double* PT) {
+                        const int* pbase, const int* pnnz, const int* poff, const double* P, double* PT, float* Plo,
+                        float* PTlo) {
   const int R = blockIdx.x * blockDim.x + threadIdx.x;
   if (R >= nc) return;
   int s, c2, J;
   sa_decode(R, cdof_sys, cdof_off, cnode_off, s, c2, J);
   const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
-  double* row = PT + poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
+  const size_t t0 = poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
   for (int c = 0; c < 2; ++c)
     for (int u = 0; u < dT; ++u) {
       const int g = ptn_fine[tr + u], pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
-      row[c * dT + u] = P[poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]) + c2 * dP + ptn_k[tr + u]];
+      const size_t pi = poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]) + c2 * dP + ptn_k[tr + u];
+      const double v = P[pi];
+      PT[t0 + c * dT + u] = v;
+      PTlo[t0 + c * dT + u] = (float)v;
+      Plo[pi] = (float)v;
     }
 }
 
-// coarse operator rows: Ac(R,:) = sum over P'(R, i) AP(i,:), into the coarse level's CSR
+// coarse operator rows: Ac((c2,J),:) = sum over P'((c2,J), (c,g)) AP((c,g),:), into the coarse
+// level's CSR.  One warp per coarse node J: its two rows share the column list (sorted, in
+// shared memory with the four blocks of FP64 sums) and the fine nodes g of P'(J,:).  The
+// lanes first load the fine-node data of 32 list entries; then the entries go in order, and
+// for each the lanes take the entries of AP(g,:), whose columns are distinct, so the targets
+// are distinct: a fixed summation order without atomics.
+constexpr int kSaAcWarps = 4;
 template <typename KT>
-__global__ void k_sa_Ac(int nc, const int* cdof_sys, const int* cdof_off, const int* cnode_off, const int* crowptr,
-                        const int* ccolind, const int* ptn_ptr, const int* ptn_fine, const int* ptbase,
-                        const int* pnnz, const int* poff, const double* PT, const int* apn_ptr, const int* apn_col,
-                        const int* apbase, const int* apnnz, const int* apoff, const double* AP, KT* Ac) {
-  const int t2 = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per (coarse row, column block c3)
-  if (t2 >= 2 * nc) return;
-  const int R = t2 >> 1, c3 = t2 & 1;
-  int s, c2, J;
-  sa_decode(R, cdof_sys, cdof_off, cnode_off, s, c2, J);
-  const int cr0 = crowptr[R], degc = (crowptr[R + 1] - cr0) >> 1;
-  KT* out = Ac + cr0 + c3 * degc;
-  for (int t = 0; t < degc; ++t) out[t] = (KT)0;
+__global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* cnode_sys, const int* cdof_off,
+                                                           const int* cnode_off, const int* crowptr,
+                                                           const int* ccolind, const int* ptn_ptr,
+                                                           const int* ptn_fine, const int* ptbase, const int* pnnz,
+                                                           const int* poff, const double* PT, const int* apn_ptr,
+                                                           const int* apn_col, const int* apbase, const int* apnnz,
+                                                           const int* apoff, const double* AP, KT* Ac) {
+  __shared__ int s_col[kSaAcWarps][kSaMaxDeg];
+  __shared__ double s_acc[kSaAcWarps][4 * kSaMaxDeg];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int J = blockIdx.x * kSaAcWarps + wid;
+  if (J >= ncn) return;  // whole warps leave together
+  const int s = cnode_sys[J];
+  const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno;
+  const int R0 = cdof_off[s] + (J - cno), R1 = R0 + cnn;
+  const int cr0 = crowptr[R0], cr1 = crowptr[R1], degc = min((crowptr[R0 + 1] - cr0) >> 1, kSaMaxDeg);
+  const int cbase = cdof_off[s] - cno;  // u-column dof of coarse node K: cbase + K
+  int* col = s_col[wid];
+  double* acc = s_acc[wid];  // block (c2, c3) at (2 c2 + c3) degc
+  for (int t = lane; t < degc; t += 32) {
+    col[t] = ccolind[cr0 + t] - cbase;
+    acc[t] = 0;
+    acc[degc + t] = 0;
+    acc[2 * degc + t] = 0;
+    acc[3 * degc + t] = 0;
+  }
   const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
-  const double* trow = PT + poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
-  const int cbase = cdof_off[s] - cnode_off[s];  // u-column dof of coarse node K: cbase + K
-  const int* ucol = ccolind + cr0;                // sorted u-block columns of the coarse row
-  for (int c = 0; c < 2; ++c)
-    for (int u = 0; u < dT; ++u) {
-      const double w = trow[c * dT + u];
-      if (w == 0.0) continue;
-      const int g = ptn_fine[tr + u], ar = apn_ptr[g], dA = apn_ptr[g + 1] - ar;
-      const double* arow = AP + apoff[s] + (size_t)c * 2 * apnnz[s] + 2 * (size_t)(ar - apbase[s]) + c3 * dA;
-      int pos = 0;  // both lists are sorted: merge
-      for (int kk = 0; kk < dA; ++kk) {
-        const int key = cbase + apn_col[ar + kk];
-        while (pos < degc && ucol[pos] < key) ++pos;
-        const double v = arow[kk];
-        if (v != 0.0 && pos < degc && ucol[pos] == key) out[pos] += (KT)(w * v);
+  const size_t prs = (size_t)2 * pnnz[s], ars = (size_t)2 * apnnz[s];
+  const double* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);  // P'((c2,J),(c,u)) = t0[c2 prs + c dT + u]
+  const double* apb = AP + apoff[s];
+  const int apb0 = apbase[s];
+  for (int u0 = 0; u0 < dT; u0 += 32) {
+    const int my = u0 + lane;
+    int g_ar = 0, g_dA = 0;
+    double w00 = 0, w01 = 0, w10 = 0, w11 = 0;
+    if (my < dT) {
+      const int g = ptn_fine[tr + my];
+      g_ar = apn_ptr[g];
+      g_dA = apn_ptr[g + 1] - g_ar;
+      w00 = t0[my];
+      w01 = t0[dT + my];
+      w10 = t0[prs + my];
+      w11 = t0[prs + dT + my];
+    }
+    const int nstep = min(32, dT - u0);
+    for (int e = 0; e < nstep; ++e) {
+      const int ar = __shfl_sync(0xffffffffu, g_ar, e), dA = __shfl_sync(0xffffffffu, g_dA, e);
+      const double v00 = __shfl_sync(0xffffffffu, w00, e), v01 = __shfl_sync(0xffffffffu, w01, e);
+      const double v10 = __shfl_sync(0xffffffffu, w10, e), v11 = __shfl_sync(0xffffffffu, w11, e);
+      const double* a0 = apb + 2 * (size_t)(ar - apb0);  // AP((c,g),(c3,kk)) = a0[c ars + c3 dA + kk]
+      __syncwarp();  // the previous entry's sums are visible to the warp
+      for (int kk = lane; kk < dA; kk += 32) {
+        const int pos = sa_find(col, degc, apn_col[ar + kk]);
+        if (pos < 0) continue;
+        const double x00 = a0[kk], x01 = a0[dA + kk], x10 = a0[ars + kk], x11 = a0[ars + dA + kk];
+        acc[pos] += v00 * x00 + v01 * x10;
+        acc[degc + pos] += v00 * x01 + v01 * x11;
+        acc[2 * degc + pos] += v10 * x00 + v11 * x10;
+        acc[3 * degc + pos] += v10 * x01 + v11 * x11;
       }
     }
+  }
+  __syncwarp();
+  for (int t = lane; t < 2 * degc; t += 32) {
+    Ac[cr0 + t] = (KT)acc[t];
+    Ac[cr1 + t] = (KT)acc[2 * degc + t];
+  }
 }
 
-// restriction b_c = P' res (coarse pre-smoothing x_c = invd b_c unless lc is the system's coarsest)
-// kSaRL lanes per coarse row (the row's 2*dT entries split over the lanes, then a lane sum)
+// restriction b_c = P' res (coarse pre-smoothing x_c = invd b_c unless lc is the system's coarsest),
+// kSaRL lanes per coarse node: both rows (c2 = 0, 1) of the node share the fine-node list and
+// the gathered residuals; a lane sum in a fixed order
 constexpr int kSaRL = 8;
 template <typename VT>
-__global__ void __launch_bounds__(256) k_sa_restrict(int nc, const int* cdof_sys, const int* cdof_off,
+__global__ void __launch_bounds__(256) k_sa_restrict(int ncn, const int* cnode_sys, const int* cdof_off,
                                                      const int* cnode_off, const int* depth, int lc, const int* sel,
                                                      const int* done, const int* ptn_ptr, const int* ptn_fine,
                                                      const int* ptbase, const int* pnnz, const int* poff,
-                                                     const double* PT, const int* fdof_off, const int* fnode_off,
+                                                     const VT* PT, const int* fdof_off, const int* fnode_off,
                                                      const VT* res, const VT* cinvd, VT* cb, VT* cx) {
-  const int R0 = (blockIdx.x * blockDim.x + threadIdx.x) / kSaRL, lane = threadIdx.x % kSaRL;
-  const bool valid = R0 < nc;
-  const int R = valid ? R0 : nc - 1;
-  int s, c2, J;
-  sa_decode(R, cdof_sys, cdof_off, cnode_off, s, c2, J);
+  const int J0 = (blockIdx.x * blockDim.x + threadIdx.x) / kSaRL, lane = threadIdx.x % kSaRL;
+  const bool valid = J0 < ncn;
+  const int J = valid ? J0 : ncn - 1;
+  const int s = cnode_sys[J];
   const bool act = valid && sel[s] && !done[s];
-  double acc = 0;
+  double a0 = 0, a1 = 0;
   if (act) {
     const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
-    const double* trow = PT + poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
+    const size_t rs = (size_t)2 * pnnz[s];  // P' row stride between c2 = 0 and c2 = 1
+    const VT* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);
     const int fno = fnode_off[s], fnn = fnode_off[s + 1] - fno, fd = fdof_off[s];
-    for (int t = lane; t < 2 * dT; t += kSaRL) {
-      const int c = t >= dT ? 1 : 0, u = t - c * dT;
-      acc += trow[t] * (double)res[fd + c * fnn + (ptn_fine[tr + u] - fno)];
+    for (int u = lane; u < dT; u += kSaRL) {
+      const int f = fd + (ptn_fine[tr + u] - fno);
+      const double r0 = (double)res[f], r1 = (double)res[f + fnn];
+      a0 += (double)t0[u] * r0 + (double)t0[dT + u] * r1;
+      a1 += (double)t0[rs + u] * r0 + (double)t0[rs + dT + u] * r1;
     }
   }
 #pragma unroll
-  for (int o = kSaRL / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, kSaRL);
+  for (int o = kSaRL / 2; o > 0; o >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, o, kSaRL);
+    a1 += __shfl_down_sync(0xffffffffu, a1, o, kSaRL);
+  }
   if (act && lane == 0) {
-    cb[R] = (VT)acc;
-    if (depth[s] > lc) cx[R] = (VT)((double)cinvd[R] * acc);
+    const int cno = cnode_off[s], R0 = cdof_off[s] + (J - cno), R1 = R0 + (cnode_off[s + 1] - cno);
+    cb[R0] = (VT)a0;
+    cb[R1] = (VT)a1;
+    if (depth[s] > lc) {
+      cx[R0] = (VT)((double)cinvd[R0] * a0);
+      cx[R1] = (VT)((double)cinvd[R1] * a1);
+    }
   }
 }
 
-// prolongation x += P x_c on level l (systems deeper than l; masked rows have zero P rows)
+// prolongation x += P x_c on level l (systems deeper than l; masked rows have zero P rows),
+// one thread per fine node: both rows share the coarse-node list and the gathered x_c
 template <typename VT>
-__global__ void k_sa_prolong(int nf, const int* dof_sys, const int* dof_off, const int* node_off, const int* depth,
+__global__ void k_sa_prolong(int nfn, const int* node_sys, const int* dof_off, const int* node_off, const int* depth,
                              int l, const int* sel, const int* done, const int* pn_ptr, const int* pn_col,
-                             const int* pbase, const int* pnnz, const int* poff, const double* P,
+                             const int* pbase, const int* pnnz, const int* poff, const VT* P,
                              const int* cdof_off, const int* cnode_off, const VT* xc, VT* x) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nf) return;
-  int s, c, g;
-  sa_decode(i, dof_sys, dof_off, node_off, s, c, g);
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nfn) return;
+  const int s = node_sys[g];
   if (!sel[s] || done[s] || depth[s] <= l) return;
   const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
-  const double* row = P + poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]);
+  const size_t rs = (size_t)2 * pnnz[s];  // P row stride between c = 0 and c = 1
+  const VT* p0 = P + poff[s] + 2 * (size_t)(pr - pbase[s]);
   const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno, cd = cdof_off[s];
-  double acc = (double)x[i];
-  for (int c2 = 0; c2 < 2; ++c2)
-    for (int k = 0; k < dP; ++k) acc += row[c2 * dP + k] * (double)xc[cd + c2 * cnn + (pn_col[pr + k] - cno)];
-  x[i] = (VT)acc;
+  const int no = node_off[s], i0 = dof_off[s] + (g - no), i1 = i0 + (node_off[s + 1] - no);
+  double a0 = (double)x[i0], a1 = (double)x[i1];
+  for (int k = 0; k < dP; ++k) {
+    const int K = cd + (pn_col[pr + k] - cno);
+    const double xu = (double)xc[K], xv = (double)xc[K + cnn];
+    a0 += (double)p0[k] * xu + (double)p0[dP + k] * xv;
+    a1 += (double)p0[rs + k] * xu + (double)p0[rs + dP + k] * xv;
+  }
+  x[i0] = (VT)a0;
+  x[i1] = (VT)a1;
 }
 
 // ---------------------------------------------------------------------------
@@ -930,12 +1039,13 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
       k_sa_P<KT, VT><<<nbf, 128, 0, st>>>(F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk,
                                           (const VT*)F.invd, F.sa_agg, F.pn_ptr, F.pn_col, F.pbase, F.pnnz, F.poff,
                                           F.sa_p), ++*launches;
-      k_sa_AP<KT><<<(2 * F.ndof + 127) / 128, 128, 0, st>>>(F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr,
+      k_sa_AP<KT><<<(int)(((long long)F.nn * kSaGL + 127) / 128), 128, 0, st>>>(F.nn, F.node_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr,
                                        F.pn_col, F.pbase, F.pnnz, F.poff, F.sa_p, F.apn_ptr, F.apn_col, F.apbase,
                                        F.apnnz, F.apoff, F.sa_ap), ++*launches;
       k_sa_PT<<<nbc, 128, 0, st>>>(C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, F.ptn_ptr, F.ptn_fine, F.ptn_k,
-                                   F.ptbase, F.pn_ptr, F.pbase, F.pnnz, F.poff, F.sa_p, F.sa_pt), ++*launches;
-      k_sa_Ac<KT><<<(2 * C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr,
+                                   F.ptbase, F.pn_ptr, F.pbase, F.pnnz, F.poff, F.sa_p, F.sa_pt, F.sa_plo,
+                                   F.sa_ptlo), ++*launches;
+      k_sa_Ac<KT><<<(C.nn + kSaAcWarps - 1) / kSaAcWarps, 32 * kSaAcWarps, 0, st>>>(C.nn, C.node_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr,
                                        F.ptn_fine, F.ptbase, F.pnnz, F.poff, F.sa_pt, F.apn_ptr, F.apn_col, F.apbase,
                                        F.apnnz, F.apoff, F.sa_ap, (KT*)C.A), ++*launches;
     }
@@ -978,6 +1088,13 @@ int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* 
   return numeric_t<double, double>(m, rowptr0, colind0, (const double*)K0, cmask, launches);
 }
 
+// the transfer values in the vector precision
+template <typename VT>
+static const VT* sa_vals(const double* v64, const float* v32) {
+  if constexpr (std::is_same<VT, float>::value) return v32;
+  else return v64;
+}
+
 template <typename KT, typename VT>
 static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
   Amg* a = m->amg;
@@ -1012,9 +1129,9 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 1);
     const AmgLevel& F = a->lev[l];
     if (a->sa)
-      k_sa_restrict<VT><<<(int)(((long long)C.ndof * kSaRL + 255) / 256), 256, 0, st>>>(
-          C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, a->d_depth, l + 1, v.sel, v.done, F.ptn_ptr, F.ptn_fine,
-          F.ptbase, F.pnnz, F.poff, F.sa_pt, F.d_dof_off, F.d_node_off, W(l), (const VT*)C.invd, (VT*)C.b,
+      k_sa_restrict<VT><<<(int)(((long long)C.nn * kSaRL + 255) / 256), 256, 0, st>>>(
+          C.nn, C.node_sys, C.d_dof_off, C.d_node_off, a->d_depth, l + 1, v.sel, v.done, F.ptn_ptr, F.ptn_fine,
+          F.ptbase, F.pnnz, F.poff, sa_vals<VT>(F.sa_pt, F.sa_ptlo), F.d_dof_off, F.d_node_off, W(l), (const VT*)C.invd, (VT*)C.b,
           (VT*)C.x), ++*launches;
     else
       k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done,
@@ -1027,9 +1144,9 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     const AmgLevel& F = a->lev[l];
     const AmgLevel& C = a->lev[l + 1];
     if (a->sa)
-      k_sa_prolong<VT><<<(F.ndof + 255) / 256, 256, 0, st>>>(
-          F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, a->d_depth, l, v.sel, v.done, F.pn_ptr, F.pn_col, F.pbase,
-          F.pnnz, F.poff, F.sa_p, C.d_dof_off, C.d_node_off, (const VT*)C.x2, X(l)), ++*launches;
+      k_sa_prolong<VT><<<(F.nn + 255) / 256, 256, 0, st>>>(
+          F.nn, F.node_sys, F.d_dof_off, F.d_node_off, a->d_depth, l, v.sel, v.done, F.pn_ptr, F.pn_col, F.pbase,
+          F.pnnz, F.poff, sa_vals<VT>(F.sa_p, F.sa_plo), C.d_dof_off, C.d_node_off, (const VT*)C.x2, X(l)), ++*launches;
     else
       k_amg_correct<VT><<<nrb(l), 256, 0, st>>>(rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, X(l),
                                                 (const VT*)C.x2, F.cmap, mask(l)), ++*launches;
