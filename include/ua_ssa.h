@@ -133,6 +133,9 @@ typedef struct ua_params {
                                   copy of the tangent (the PCG operator stays FP32) */
     int32_t amg_smoothed;      /* 1 = smoothed-aggregation prolongators (default), 0 = plain aggregation;
                                   fixed by a handle's first AMG solve */
+    int32_t krylov_full_grid;  /* 0 = the AMG-preconditioned PCG launches only the row and node blocks of
+                                  systems still iterating (device-compacted lists, default); 1 = every
+                                  block of the batch (same results) */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

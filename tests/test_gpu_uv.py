@@ -302,3 +302,23 @@ def test_graph_replay_equals_direct_launches(precision, rtol):
         assert info.converged
         out.append(np.concatenate([Fo.ub, Fo.vb]))
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+
+
+@pytest.mark.parametrize("precision,rtol", [(L.UA_PREC_FP64, 1e-12), (L.UA_PREC_MIXED, 1e-6)])
+def test_active_block_lists_equal_full_grid(precision, rtol):
+    """The PCG launched over the device-compacted lists of active row and node blocks gives
+    bit-identical results and iteration counts to launching every block of the batch (a
+    batch of uneven meshes, so systems converge at different iterations)."""
+    probs = [synth.ice_stream_shelf(21, 11, seed=0), synth.ice_stream_shelf(41, 21, seed=5),
+             synth.ice_stream_shelf(15, 8, seed=9), synth.ice_stream_shelf(31, 16, seed=2)]
+    batch = ua.CreateMUABatch([(P.coordinates, P.connectivity) for P in probs])
+    res = []
+    for full in (0, 1):
+        ctrl = ua.CtrlVar(precision=precision, krylov_rtol=rtol, krylov_full_grid=full).set_force_tolerance(1e-20)
+        out = ua.uv_batch(ctrl, batch, [ua.Fields.from_problem(P) for P in probs],
+                          [ua.BCs.from_problem(P) for P in probs])
+        assert all(o[2].converged for o in out)
+        res.append(([np.concatenate([o[0], o[1]]) for o in out], [o[2].krylov_its_total for o in out]))
+    assert len(set(res[0][1])) > 1  # the systems finish at different PCG iterations
+    assert res[0][1] == res[1][1]
+    assert all(np.array_equal(a, b) for a, b in zip(res[0][0], res[1][0]))

@@ -32,6 +32,8 @@ constexpr int kAmgMaxRow = 32;        // longest coarse dof row (2 x coarse node
 constexpr int kSaMaxDeg = 256;        // largest coarse node degree of a smoothed hierarchy (shared-memory rows)
 constexpr int kAmgMaxDense = 2 * kAmgCoarseNodes;
 constexpr int kAmgRB = 256;           // rows per row block of a coarse level
+constexpr int kSaRB = 128, kSaLPR = 2;
+constexpr int kAmgNB = 256;           // nodes per node block of the smoothed transfers  // smoothed hierarchies (longer coarse rows): rows per block, lanes per row
 
 // Calls f(std::integral_constant<int, LPR>) for the lanes-per-row value lpr (1, 2, 4, 8, 16 or 32).
 template <class F>
@@ -64,6 +66,11 @@ struct AmgLevel {
   void *b = nullptr, *x = nullptr, *x2 = nullptr;  // rhs, pre-smoothed, post-smoothed (VT)
   int* d_node_off = nullptr;              // per-system node offsets on the device
   int* node_sys = nullptr;                // node -> system (smoothed hierarchies)
+  std::vector<int> h_sys_rb_off;          // per-system prefix of the row blocks
+  // node blocks (kAmgNB nodes, never straddling two systems) for the smoothed transfers
+  int *nb_start = nullptr, *nb_sys = nullptr;
+  int nnb = 0;
+  std::vector<int> h_sys_nb_off;
   // smoothed aggregation, transfer from this level to the next (node-level lists, global ids):
   // pn: fine node -> coarse nodes of its neighbours' aggregates (the prolongator's node pattern);
   // apn: fine node -> coarse nodes of A P; ptn: coarse node -> (fine node, position in pn)
@@ -75,8 +82,24 @@ struct AmgLevel {
   float *sa_plo = nullptr, *sa_ptlo = nullptr;  // FP32 copies of P and P' for the mixed-precision transfers
 };
 
+// one active-block list to compact: blocks blk_off[s] .. blk_off[s+1] of every system s with
+// sel, !done and depth > lmin, in ascending order
+struct ActSpec {
+  const int* blk_off;
+  int lmin;
+  int* map;
+  int* cnt;
+};
+
 struct Amg {
   int nsys = 0, nlev = 0, maxdn = 0;
+  // active-block lists: rows[l] (level-l row blocks, depth > l; level 0 = the handle's blocks),
+  // fnodes[l] (level-l node blocks, depth > l), cnodes[l] (level-(l+1) node blocks, depth > l)
+  bool act_ready = false;
+  int nsm = 148;
+  std::vector<ActList> rows, fnodes, cnodes;
+  ActSpec* d_specs = nullptr;
+  int nspecs = 0;
   bool sa = false;            // smoothed aggregation (else plain)
   std::vector<AmgLevel> lev;  // lev[0] = the handle's own system
   std::vector<int> depth;     // per system: its coarsest level (>= 1)
@@ -303,8 +326,14 @@ static int amg_build(ua_mesh* m, bool smoothed) {
     if (l == 0 && m->ndof == 2 && (L.ndof != m->ndof_total || L.nnz != m->nnz_total))
       return fail("fine level does not match the handle");
     std::vector<int> rb_start, rb_sys;
-    for (int s = 0; s < nsys; ++s)
-      for (int r = L.dof_off[s]; r < L.dof_off[s + 1]; r += kAmgRB) { rb_start.push_back(r); rb_sys.push_back(s); }
+    L.h_sys_rb_off.assign(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) {
+      for (int r = L.dof_off[s]; r < L.dof_off[s + 1]; r += smoothed ? kSaRB : kAmgRB) {
+        rb_start.push_back(r);
+        rb_sys.push_back(s);
+      }
+      L.h_sys_rb_off[s + 1] = (int)rb_sys.size();
+    }
     rb_start.push_back(L.ndof);
     L.nrb = (int)rb_sys.size();
     L.invd = dalloc(m, a, sizeof(double) * (size_t)L.ndof, ok);
@@ -378,6 +407,20 @@ static int amg_build(ua_mesh* m, bool smoothed) {
       for (int s = 0; s < nsys; ++s)
         for (int g = a->lev[l].node_off[s]; g < a->lev[l].node_off[s + 1]; ++g) ns[g] = s;
       a->lev[l].node_sys = upload(m, a, ns, ok);
+      std::vector<int> nbs, nbsys;
+      AmgLevel& L = a->lev[l];
+      L.h_sys_nb_off.assign(nsys + 1, 0);
+      for (int s = 0; s < nsys; ++s) {
+        for (int g = L.node_off[s]; g < L.node_off[s + 1]; g += kAmgNB) {
+          nbs.push_back(g);
+          nbsys.push_back(s);
+        }
+        L.h_sys_nb_off[s + 1] = (int)nbsys.size();
+      }
+      nbs.push_back(L.node_off[nsys]);
+      L.nnb = (int)nbsys.size();
+      L.nb_start = upload(m, a, nbs, ok);
+      L.nb_sys = upload(m, a, nbsys, ok);
     }
     if (!a->lev[l].dof_sys) {  // a uv handle's finest level: rows -> system, for the smoothed transfer
       std::vector<int> ds(a->lev[l].ndof);
@@ -637,22 +680,26 @@ __global__ void k_to_bf16(long long n, const float* in, __nv_bfloat16* out) {
 }
 
 template <typename KT, typename VT, int LPR>
-__global__ void __launch_bounds__(256) k_amg_residual(const int* rb_start, const int* rb_sys, const int* sel,
-                                                      const int* done, const int* depth, int l, const int* rowptr,
-                                                      const int* colind, const KT* A, const VT* b, const VT* x,
-                                                      const unsigned char* cmask, VT* res, const int* dof_off) {
-  const int blk = blockIdx.x;
-  const int s = rb_sys[blk];
-  if (!sel[s] || done[s] || depth[s] <= l) return;
-  const int rs = rb_start[blk], re = rb_start[blk + 1];
-  const int nhalf = (dof_off[s + 1] - dof_off[s]) >> 1;
-  const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
-  for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
-    const int row = row0 + grp;
-    const bool valid = row < re;
-    const double ax = sizeof(KT) == 8 ? row_dot_uv<KT, VT, LPR>(rowptr, colind, A, x, row, valid, lane, nhalf)
-                                      : row_dot_csr<KT, VT, LPR>(rowptr, colind, A, x, row, valid, lane);
-    if (valid && lane == 0) res[row] = (VT)((cmask && cmask[row]) ? 0.0 : (double)b[row] - ax);
+__global__ void __launch_bounds__(256) k_amg_residual(const int* rb_start, const int* rb_sys, ActList act,
+                                                      const int* sel, const int* done, const int* depth, int l,
+                                                      const int* rowptr, const int* colind, const KT* A,
+                                                      const VT* b, const VT* x, const unsigned char* cmask, VT* res,
+                                                      const int* dof_off) {
+  const int nv = act.cnt ? *act.cnt : gridDim.x;  // list entries, else one block per CTA
+  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+    const int blk = act.map ? act.map[vb] : vb;
+    const int s = rb_sys[blk];
+    if (!sel[s] || done[s] || depth[s] <= l) continue;  // uniform over the block
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    const int nhalf = (dof_off[s + 1] - dof_off[s]) >> 1;
+    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
+      const int row = row0 + grp;
+      const bool valid = row < re;
+      const double ax = sizeof(KT) == 8 ? row_dot_uv<KT, VT, LPR>(rowptr, colind, A, x, row, valid, lane, nhalf)
+                                        : row_dot_csr<KT, VT, LPR>(rowptr, colind, A, x, row, valid, lane);
+      if (valid && lane == 0) res[row] = (VT)((cmask && cmask[row]) ? 0.0 : (double)b[row] - ax);
+    }
   }
 }
 
@@ -688,43 +735,47 @@ __global__ void __launch_bounds__(256) k_amg_correct(const int* rb_start, const 
 // for systems deeper than l; on the finest level pcopy (if set) receives a
 // copy and part the block partials of b.out.
 template <typename KT, typename VT, int LPR>
-__global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const int* rb_sys, const int* sel,
-                                                    const int* done, const int* depth, int l, const int* rowptr,
-                                                    const int* colind, const KT* A, const VT* b, const VT* xp,
-                                                    const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
-                                                    double* part, const int* dof_off) {
-  const int blk = blockIdx.x;
-  const int s = rb_sys[blk];
-  double rz = 0;
-  if (sel[s] && !done[s] && depth[s] > l) {
-    const int rs = rb_start[blk], re = rb_start[blk + 1];
-    const int nhalf = (dof_off[s + 1] - dof_off[s]) >> 1;
-    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
-    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
-      const int row = row0 + grp;
-      const bool valid = row < re;
-      const double ax = sizeof(KT) == 8 ? row_dot_uv<KT, VT, LPR>(rowptr, colind, A, xp, row, valid, lane, nhalf)
-                                        : row_dot_csr<KT, VT, LPR>(rowptr, colind, A, xp, row, valid, lane);
-      if (valid && lane == 0) {
-        const double v =
-            (cmask && cmask[row]) ? 0.0 : (double)xp[row] + (double)invd[row] * ((double)b[row] - ax);
-        out[row] = (VT)v;
-        if (pcopy) pcopy[row] = (VT)v;
-        rz += (double)b[row] * v;
+__global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const int* rb_sys, ActList act,
+                                                    const int* sel, const int* done, const int* depth, int l,
+                                                    const int* rowptr, const int* colind, const KT* A, const VT* b,
+                                                    const VT* xp, const VT* invd, const unsigned char* cmask, VT* out,
+                                                    VT* pcopy, double* part, const int* dof_off) {
+  __shared__ double red[8];
+  const int nv = act.cnt ? *act.cnt : gridDim.x;  // list entries, else one block per CTA
+  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+    const int blk = act.map ? act.map[vb] : vb;
+    const int s = rb_sys[blk];
+    double rz = 0;
+    if (sel[s] && !done[s] && depth[s] > l) {
+      const int rs = rb_start[blk], re = rb_start[blk + 1];
+      const int nhalf = (dof_off[s + 1] - dof_off[s]) >> 1;
+      const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+      for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread of the block
+        const int row = row0 + grp;
+        const bool valid = row < re;
+        const double ax = sizeof(KT) == 8 ? row_dot_uv<KT, VT, LPR>(rowptr, colind, A, xp, row, valid, lane, nhalf)
+                                          : row_dot_csr<KT, VT, LPR>(rowptr, colind, A, xp, row, valid, lane);
+        if (valid && lane == 0) {
+          const double v =
+              (cmask && cmask[row]) ? 0.0 : (double)xp[row] + (double)invd[row] * ((double)b[row] - ax);
+          out[row] = (VT)v;
+          if (pcopy) pcopy[row] = (VT)v;
+          rz += (double)b[row] * v;
+        }
       }
     }
-  }
-  if (!part) return;  // uniform per launch
-  __shared__ double red[8];
-  double t = rz;
+    if (!part) continue;  // uniform per launch
+    double t = rz;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double sum = 0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
-    part[blk] = sum;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
+      part[blk] = sum;
+    }
+    __syncthreads();  // red is rewritten by the next entry
   }
 }
 
@@ -943,71 +994,88 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
 // the gathered residuals; a lane sum in a fixed order
 constexpr int kSaRL = 8;
 template <typename VT>
-__global__ void __launch_bounds__(256) k_sa_restrict(int ncn, const int* cnode_sys, const int* cdof_off,
-                                                     const int* cnode_off, const int* depth, int lc, const int* sel,
-                                                     const int* done, const int* ptn_ptr, const int* ptn_fine,
-                                                     const int* ptbase, const int* pnnz, const int* poff,
-                                                     const VT* PT, const int* fdof_off, const int* fnode_off,
-                                                     const VT* res, const VT* cinvd, VT* cb, VT* cx) {
-  const int J0 = (blockIdx.x * blockDim.x + threadIdx.x) / kSaRL, lane = threadIdx.x % kSaRL;
-  const bool valid = J0 < ncn;
-  const int J = valid ? J0 : ncn - 1;
-  const int s = cnode_sys[J];
-  const bool act = valid && sel[s] && !done[s];
-  double a0 = 0, a1 = 0;
-  if (act) {
-    const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
+__global__ void __launch_bounds__(256) k_sa_restrict(const int* nb_start, const int* nb_sys, ActList act,
+                                                     const int* cdof_off, const int* cnode_off, const int* depth,
+                                                     int lc, const int* sel, const int* done, const int* ptn_ptr,
+                                                     const int* ptn_fine, const int* ptbase, const int* pnnz,
+                                                     const int* poff, const VT* PT, const int* fdof_off,
+                                                     const int* fnode_off, const VT* res, const VT* cinvd, VT* cb,
+                                                     VT* cx) {
+  const int sub = threadIdx.x / kSaRL, lane = threadIdx.x % kSaRL, nsub = blockDim.x / kSaRL;
+  const int nv = act.cnt ? *act.cnt : gridDim.x;  // list entries, else one node block per CTA
+  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+    const int b = act.map ? act.map[vb] : vb;
+    const int s = nb_sys[b];
+    if (!sel[s] || done[s]) continue;  // uniform over the block
+    const int n0 = nb_start[b], n1 = nb_start[b + 1];
+    const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno, cd = cdof_off[s];
     const size_t rs = (size_t)2 * pnnz[s];  // P' row stride between c2 = 0 and c2 = 1
-    const VT* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);
     const int fno = fnode_off[s], fnn = fnode_off[s + 1] - fno, fd = fdof_off[s];
-    for (int u = lane; u < dT; u += kSaRL) {
-      const int f = fd + (ptn_fine[tr + u] - fno);
-      const double r0 = (double)res[f], r1 = (double)res[f + fnn];
-      a0 += (double)t0[u] * r0 + (double)t0[dT + u] * r1;
-      a1 += (double)t0[rs + u] * r0 + (double)t0[rs + dT + u] * r1;
-    }
-  }
+    const bool presmooth = depth[s] > lc;
+    for (int J0 = n0; J0 < n1; J0 += nsub) {  // same trip count for every thread of the block
+      const int J = J0 + sub;
+      const bool valid = J < n1;
+      double a0 = 0, a1 = 0;
+      if (valid) {
+        const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
+        const VT* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);
+        for (int u = lane; u < dT; u += kSaRL) {
+          const int f = fd + (ptn_fine[tr + u] - fno);
+          const double r0 = (double)res[f], r1 = (double)res[f + fnn];
+          a0 += (double)t0[u] * r0 + (double)t0[dT + u] * r1;
+          a1 += (double)t0[rs + u] * r0 + (double)t0[rs + dT + u] * r1;
+        }
+      }
 #pragma unroll
-  for (int o = kSaRL / 2; o > 0; o >>= 1) {
-    a0 += __shfl_down_sync(0xffffffffu, a0, o, kSaRL);
-    a1 += __shfl_down_sync(0xffffffffu, a1, o, kSaRL);
-  }
-  if (act && lane == 0) {
-    const int cno = cnode_off[s], R0 = cdof_off[s] + (J - cno), R1 = R0 + (cnode_off[s + 1] - cno);
-    cb[R0] = (VT)a0;
-    cb[R1] = (VT)a1;
-    if (depth[s] > lc) {
-      cx[R0] = (VT)((double)cinvd[R0] * a0);
-      cx[R1] = (VT)((double)cinvd[R1] * a1);
+      for (int o = kSaRL / 2; o > 0; o >>= 1) {
+        a0 += __shfl_down_sync(0xffffffffu, a0, o, kSaRL);
+        a1 += __shfl_down_sync(0xffffffffu, a1, o, kSaRL);
+      }
+      if (valid && lane == 0) {
+        const int R0 = cd + (J - cno), R1 = R0 + cnn;
+        cb[R0] = (VT)a0;
+        cb[R1] = (VT)a1;
+        if (presmooth) {
+          cx[R0] = (VT)((double)cinvd[R0] * a0);
+          cx[R1] = (VT)((double)cinvd[R1] * a1);
+        }
+      }
     }
   }
 }
 
 // prolongation x += P x_c on level l (systems deeper than l; masked rows have zero P rows),
-// one thread per fine node: both rows share the coarse-node list and the gathered x_c
+// one thread per fine node of a node block: both rows share the coarse-node list and the gathered x_c
 template <typename VT>
-__global__ void k_sa_prolong(int nfn, const int* node_sys, const int* dof_off, const int* node_off, const int* depth,
-                             int l, const int* sel, const int* done, const int* pn_ptr, const int* pn_col,
-                             const int* pbase, const int* pnnz, const int* poff, const VT* P,
-                             const int* cdof_off, const int* cnode_off, const VT* xc, VT* x) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= nfn) return;
-  const int s = node_sys[g];
-  if (!sel[s] || done[s] || depth[s] <= l) return;
-  const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
-  const size_t rs = (size_t)2 * pnnz[s];  // P row stride between c = 0 and c = 1
-  const VT* p0 = P + poff[s] + 2 * (size_t)(pr - pbase[s]);
-  const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno, cd = cdof_off[s];
-  const int no = node_off[s], i0 = dof_off[s] + (g - no), i1 = i0 + (node_off[s + 1] - no);
-  double a0 = (double)x[i0], a1 = (double)x[i1];
-  for (int k = 0; k < dP; ++k) {
-    const int K = cd + (pn_col[pr + k] - cno);
-    const double xu = (double)xc[K], xv = (double)xc[K + cnn];
-    a0 += (double)p0[k] * xu + (double)p0[dP + k] * xv;
-    a1 += (double)p0[rs + k] * xu + (double)p0[rs + dP + k] * xv;
+__global__ void __launch_bounds__(256) k_sa_prolong(const int* nb_start, const int* nb_sys, ActList act,
+                                                    const int* dof_off, const int* node_off, const int* depth, int l,
+                                                    const int* sel, const int* done, const int* pn_ptr,
+                                                    const int* pn_col, const int* pbase, const int* pnnz,
+                                                    const int* poff, const VT* P, const int* cdof_off,
+                                                    const int* cnode_off, const VT* xc, VT* x) {
+  const int nv = act.cnt ? *act.cnt : gridDim.x;  // list entries, else one node block per CTA
+  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+    const int b = act.map ? act.map[vb] : vb;
+    const int s = nb_sys[b];
+    if (!sel[s] || done[s] || depth[s] <= l) continue;  // uniform over the block
+    const size_t rs = (size_t)2 * pnnz[s];  // P row stride between c = 0 and c = 1
+    const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno, cd = cdof_off[s];
+    const int no = node_off[s], nn = node_off[s + 1] - no, d0 = dof_off[s];
+    for (int g = nb_start[b] + threadIdx.x; g < nb_start[b + 1]; g += blockDim.x) {
+      const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
+      const VT* p0 = P + poff[s] + 2 * (size_t)(pr - pbase[s]);
+      const int i0 = d0 + (g - no), i1 = i0 + nn;
+      double a0 = (double)x[i0], a1 = (double)x[i1];
+      for (int k = 0; k < dP; ++k) {
+        const int K = cd + (pn_col[pr + k] - cno);
+        const double xu = (double)xc[K], xv = (double)xc[K + cnn];
+        a0 += (double)p0[k] * xu + (double)p0[dP + k] * xv;
+        a1 += (double)p0[rs + k] * xu + (double)p0[rs + dP + k] * xv;
+      }
+      x[i0] = (VT)a0;
+      x[i1] = (VT)a1;
+    }
   }
-  x[i0] = (VT)a0;
-  x[i1] = (VT)a1;
 }
 
 // ---------------------------------------------------------------------------
@@ -1112,27 +1180,31 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
   auto W = [&](int l) { return l == 0 ? (VT*)v.tmp : (VT*)a->lev[l].x2; };
   auto mask = [&](int l) { return l == 0 ? v.cmask : nullptr; };
   auto doff = [&](int l) { return (const int*)a->lev[l].d_dof_off; };
-  const int lpr0 = v.lpr;
+  const int lpr0 = v.lpr, lprc = a->sa ? kSaLPR : 1;  // lanes per row: finest level, coarse levels
+  // list-driven launches (the PCG of a uv handle): a grid of about one wave over the active blocks
+  const bool useact = v.act && a->act_ready;
+  auto rows_act = [&](int l) { return useact ? a->rows[l] : ActList{}; };
+  auto rows_grid = [&](int l) { return useact ? act_grid(nrb(l), a->nsm) : nrb(l); };
   for (int l = 0; l + 1 < nl; ++l) {  // down: residual of level l, aggregated into level l+1
     const AmgLevel& C = a->lev[l + 1];
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 0);
-    dispatch_lpr(lpr0, [&](auto L) {
+    dispatch_lpr(l == 0 ? lpr0 : lprc, [&](auto L) {
       if (l == 0 && v.K0lo)
-        k_amg_residual<__nv_bfloat16, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
-            rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
+        k_amg_residual<__nv_bfloat16, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
+            rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
             mask(l), W(l), doff(l));
       else
-        k_amg_residual<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
-            rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l), doff(l));
+        k_amg_residual<KT, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
+            rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l), doff(l));
     });
     ++*launches;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 1);
     const AmgLevel& F = a->lev[l];
     if (a->sa)
-      k_sa_restrict<VT><<<(int)(((long long)C.nn * kSaRL + 255) / 256), 256, 0, st>>>(
-          C.nn, C.node_sys, C.d_dof_off, C.d_node_off, a->d_depth, l + 1, v.sel, v.done, F.ptn_ptr, F.ptn_fine,
-          F.ptbase, F.pnnz, F.poff, sa_vals<VT>(F.sa_pt, F.sa_ptlo), F.d_dof_off, F.d_node_off, W(l), (const VT*)C.invd, (VT*)C.b,
-          (VT*)C.x), ++*launches;
+      k_sa_restrict<VT><<<useact ? act_grid(C.nnb, a->nsm) : C.nnb, 256, 0, st>>>(
+          C.nb_start, C.nb_sys, useact ? a->cnodes[l] : ActList{}, C.d_dof_off, C.d_node_off, a->d_depth, l + 1,
+          v.sel, v.done, F.ptn_ptr, F.ptn_fine, F.ptbase, F.pnnz, F.poff, sa_vals<VT>(F.sa_pt, F.sa_ptlo),
+          F.d_dof_off, F.d_node_off, W(l), (const VT*)C.invd, (VT*)C.b, (VT*)C.x), ++*launches;
     else
       k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done,
                                                              C.mptr, C.mlist, W(l), (const VT*)C.invd, (VT*)C.b,
@@ -1144,9 +1216,10 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     const AmgLevel& F = a->lev[l];
     const AmgLevel& C = a->lev[l + 1];
     if (a->sa)
-      k_sa_prolong<VT><<<(F.nn + 255) / 256, 256, 0, st>>>(
-          F.nn, F.node_sys, F.d_dof_off, F.d_node_off, a->d_depth, l, v.sel, v.done, F.pn_ptr, F.pn_col, F.pbase,
-          F.pnnz, F.poff, sa_vals<VT>(F.sa_p, F.sa_plo), C.d_dof_off, C.d_node_off, (const VT*)C.x2, X(l)), ++*launches;
+      k_sa_prolong<VT><<<useact ? act_grid(F.nnb, a->nsm) : F.nnb, 256, 0, st>>>(
+          F.nb_start, F.nb_sys, useact ? a->fnodes[l] : ActList{}, F.d_dof_off, F.d_node_off, a->d_depth, l,
+          v.sel, v.done, F.pn_ptr, F.pn_col, F.pbase, F.pnnz, F.poff, sa_vals<VT>(F.sa_p, F.sa_plo), C.d_dof_off,
+          C.d_node_off, (const VT*)C.x2, X(l)), ++*launches;
     else
       k_amg_correct<VT><<<nrb(l), 256, 0, st>>>(rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, X(l),
                                                 (const VT*)C.x2, F.cmap, mask(l)), ++*launches;
@@ -1154,14 +1227,14 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     VT* pcopy = l == 0 ? (VT*)v.pcopy : nullptr;
     double* part = l == 0 ? v.part_rz : nullptr;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 1, 0);
-    dispatch_lpr(lpr0, [&](auto L) {
+    dispatch_lpr(l == 0 ? lpr0 : lprc, [&](auto L) {
       if (l == 0 && v.K0lo)
-        k_amg_smooth<__nv_bfloat16, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
-            rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
+        k_amg_smooth<__nv_bfloat16, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
+            rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
             (const VT*)F.invd, mask(l), out, pcopy, part, doff(l));
       else
-        k_amg_smooth<KT, VT, decltype(L)::value><<<nrb(l), 256, 0, st>>>(
-            rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), (const VT*)F.invd,
+        k_amg_smooth<KT, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
+            rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), (const VT*)F.invd,
             mask(l), out, pcopy, part, doff(l));
     });
     ++*launches;
@@ -1245,5 +1318,105 @@ int amg_apply_uvh(ua_mesh* m, const double* p3, double* out3, const int* sel, co
       ++*launches;
   return UA_OK;
 }
+
+// ---------------------------------------------------------------------------
+// active-block lists
+// ---------------------------------------------------------------------------
+
+int act_grid(int nblocks, int nsm) { return std::max(1, std::min(nblocks, 8 * nsm)); }
+
+// exclusive block-wide scan of v (blockDim.x a multiple of 32, at most 1024); total = sum
+__device__ int block_excl_scan(int v, int* sh, int& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int t = lane < nw ? sh[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    sh[lane] = t;
+  }
+  __syncthreads();
+  const int pre = wid ? sh[wid - 1] : 0;
+  total = sh[nw - 1];
+  __syncthreads();  // sh is reused by the next call
+  return pre + x - v;
+}
+
+// one CTA per list: scan the systems in order, each active system writes its block ids
+__global__ void __launch_bounds__(1024) k_act_compact(const ActSpec* specs, int nsys, const int* sel,
+                                                      const int* done, const int* depth) {
+  __shared__ int sh[32];
+  const ActSpec sp = specs[blockIdx.x];
+  int base = 0;
+  for (int c0 = 0; c0 < nsys; c0 += blockDim.x) {  // same trip count for every thread
+    const int s = c0 + threadIdx.x;
+    int n = 0, b0 = 0;
+    if (s < nsys && sel[s] && !done[s] && depth[s] > sp.lmin) {
+      b0 = sp.blk_off[s];
+      n = sp.blk_off[s + 1] - b0;
+    }
+    int tot;
+    const int ex = block_excl_scan(n, sh, tot);
+    for (int k = 0; k < n; ++k) sp.map[base + ex + k] = b0 + k;
+    base += tot;
+  }
+  if (threadIdx.x == 0) *sp.cnt = base;
+}
+
+int amg_act_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
+  Amg* a = m->amg;
+  if (!a) return UA_ERR_INVALID;
+  if (a->act_ready) return UA_OK;
+  const int nsys = a->nsys;
+  if ((int)sys_rb_off0.size() != nsys + 1) return set_error(UA_ERR_INVALID, "active lists: row-block prefix size");
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&a->nsm, cudaDevAttrMultiProcessorCount, dev);
+  bool ok = true;
+  std::vector<ActSpec> specs;
+  auto make = [&](const std::vector<int>& off, int lmin) {
+    ActList L;
+    L.cap = off[nsys];
+    int* map = (int*)dalloc(m, a, sizeof(int) * (size_t)std::max(L.cap, 1), ok);
+    int* cnt = (int*)dalloc(m, a, sizeof(int), ok);
+    int* doff = upload(m, a, off, ok);
+    L.map = map;
+    L.cnt = cnt;
+    specs.push_back(ActSpec{doff, lmin, map, cnt});
+    return L;
+  };
+  const int nl = a->nlev;
+  a->rows.resize(std::max(nl - 1, 1));
+  a->fnodes.resize(std::max(nl - 1, 0));
+  a->cnodes.resize(std::max(nl - 1, 0));
+  a->rows[0] = make(sys_rb_off0, -1);  // the handle's Krylov rows: every active system
+  for (int l = 1; l + 1 < nl; ++l) a->rows[l] = make(a->lev[l].h_sys_rb_off, l);
+  if (a->sa)
+    for (int l = 0; l + 1 < nl; ++l) {
+      a->fnodes[l] = make(a->lev[l].h_sys_nb_off, l);
+      a->cnodes[l] = make(a->lev[l + 1].h_sys_nb_off, l);
+    }
+  a->d_specs = upload(m, a, specs, ok);
+  a->nspecs = (int)specs.size();
+  if (!ok) return set_error(UA_ERR_OOM, "active lists: device allocation failed");
+  a->act_ready = true;
+  return UA_OK;
+}
+
+void amg_act_compact(ua_mesh* m, const int* sel, const int* done, long long* launches) {
+  Amg* a = m->amg;
+  k_act_compact<<<a->nspecs, 1024, 0, m->stream>>>(a->d_specs, a->nsys, sel, done, a->d_depth), ++*launches;
+}
+
+ActList amg_act_rows0(const ua_mesh* m) { return m->amg && m->amg->act_ready ? m->amg->rows[0] : ActList{}; }
 
 }  // namespace ua

@@ -30,7 +30,27 @@ struct AmgPcgView {
   void* mark_ctx = nullptr;
   // optional BF16 copy of K0 for the finest-level residual and smoothing (mixed precision)
   const void* K0lo = nullptr;
+  // loop the row-block and node-block kernels over the active-block lists (amg_act_compact)
+  bool act = false;
 };
+
+// Active-block lists.  After every convergence check the row blocks (and, for the smoothed
+// transfers, the node blocks) of the systems still iterating are compacted on the device,
+// in ascending order; list-driven kernels run a grid of about one wave that loops over the
+// list, so converged systems of a batch cost no blocks.
+struct ActList {
+  const int* map = nullptr;  // list entry -> block id
+  const int* cnt = nullptr;  // number of entries (device scalar)
+  int cap = 0;               // blocks of the full structure
+};
+// Build the lists of a uv handle's hierarchy (level 0 uses the handle's row blocks,
+// sys_rb_off0 = per-system prefix of those blocks); no-op when built.
+int amg_act_init(ua_mesh* m, const std::vector<int>& sys_rb_off0);
+// Recompute every list from sel/done (one launch).
+void amg_act_compact(ua_mesh* m, const int* sel, const int* done, long long* launches);
+ActList amg_act_rows0(const ua_mesh* m);
+// grid of a list-driven kernel over at most nblocks blocks of 256 threads
+int act_grid(int nblocks, int nsm);
 
 // Build the hierarchy of every system of the handle (host aggregation,
 // device structures; smoothed = smoothed-aggregation prolongators, else

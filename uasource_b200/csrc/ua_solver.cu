@@ -115,12 +115,13 @@ struct Work {
   std::vector<int> h_sys_rb_off, h_sys_con_off;
   Prof prof;
   struct ServeState* serve = nullptr;
-  // replayable PCG chunks, index (fp32 ? 2 : 0) + (amg ? 1 : 0) + (BF16 V-cycle ? 4 : 0)
+  // replayable PCG chunks, index (fp32 ? 2 : 0) + (amg ? 1 : 0) + (BF16 V-cycle ? 4 : 0) + (active lists ? 8 : 0)
   bool no_graph = false;
-  cudaGraphExec_t pcg_exec[8] = {};
-  long long pcg_exec_nodes[8] = {};
-  int pcg_exec_maxit[8] = {};
-  int pcg_exec_lpr[8] = {};
+  cudaGraphExec_t pcg_exec[16] = {};
+  long long pcg_exec_nodes[16] = {};
+  int pcg_exec_maxit[16] = {};
+  int pcg_exec_lpr[16] = {};
+  int nsm = 148;  // SMs of the handle's device (grid of the list-driven kernels)
 };
 
 // Work of a timed launch: sum of the tangent non-zeros and dof rows of the
@@ -276,6 +277,7 @@ __device__ __forceinline__ void block_partials(double (&v)[NV], double* part, in
       part[j * nrb + blk] = t;
     }
   }
+  __syncthreads();  // red is rewritten by the next row block of a list-driven launch
 }
 
 // Row-block SpMV with LPR lanes per row: y = mask(K x) (or mask(f - K x) in init mode).
@@ -347,67 +349,78 @@ __global__ void __launch_bounds__(256) k_pcg_init(const int* rb_start, const int
 }
 
 // q = mask(K p); partial p.q
+// (list-driven when act.cnt is set: the CTAs loop over the active row blocks)
 template <typename KT, typename VT, int LPR, bool UV>
-__global__ void __launch_bounds__(256) k_pcg_spmv(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
-                                                  const int* done, const int* rowptr, const int* colind,
-                                                  const KT* K, const VT* p, const unsigned char* cmask, VT* q,
-                                                  double* part, const int* dof_off) {
-  const int blk = blockIdx.x;
-  const int s = rb_sys[blk];
-  double v[1] = {0};
-  if (sel[s] && !done[s]) {
-    const int rs = rb_start[blk], re = rb_start[blk + 1];
-    const int nhalf = UV ? (dof_off[s + 1] - dof_off[s]) >> 1 : 0;
-    const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
-    for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread
-      const int row = row0 + grp;
-      const bool valid = row < re;
-      double ax = UV ? row_dot_uv<KT, VT, LPR>(rowptr, colind, K, p, row, valid, lane, nhalf)
-                     : row_dot<KT, VT, LPR>(rowptr, colind, K, p, row, valid, lane);
-      if (valid && lane == 0) {
-        double qv = cmask[row] ? 0.0 : ax;
-        q[row] = (VT)qv;
-        v[0] += (double)p[row] * qv;
+__global__ void __launch_bounds__(256) k_pcg_spmv(const int* rb_start, const int* rb_sys, int nrb, ActList act,
+                                                  const int* sel, const int* done, const int* rowptr,
+                                                  const int* colind, const KT* K, const VT* p,
+                                                  const unsigned char* cmask, VT* q, double* part,
+                                                  const int* dof_off) {
+  const int nv = act.cnt ? *act.cnt : gridDim.x;
+  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+    const int blk = act.map ? act.map[vb] : vb;
+    const int s = rb_sys[blk];
+    double v[1] = {0};
+    if (sel[s] && !done[s]) {
+      const int rs = rb_start[blk], re = rb_start[blk + 1];
+      const int nhalf = UV ? (dof_off[s + 1] - dof_off[s]) >> 1 : 0;
+      const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR, ngrp = blockDim.x / LPR;
+      for (int row0 = rs; row0 < re; row0 += ngrp) {  // same trip count for every thread
+        const int row = row0 + grp;
+        const bool valid = row < re;
+        double ax = UV ? row_dot_uv<KT, VT, LPR>(rowptr, colind, K, p, row, valid, lane, nhalf)
+                       : row_dot<KT, VT, LPR>(rowptr, colind, K, p, row, valid, lane);
+        if (valid && lane == 0) {
+          double qv = cmask[row] ? 0.0 : ax;
+          q[row] = (VT)qv;
+          v[0] += (double)p[row] * qv;
+        }
       }
     }
+    block_partials<1>(v, part, nrb, blk);
   }
-  block_partials<1>(v, part, nrb, blk);
 }
 
 // x += alpha p; r -= alpha q; z = invd r; partials rz, rr
 template <typename VT>
-__global__ void __launch_bounds__(256) k_pcg_update1(const int* rb_start, const int* rb_sys, int nrb,
+__global__ void __launch_bounds__(256) k_pcg_update1(const int* rb_start, const int* rb_sys, int nrb, ActList act,
                                                      const int* sel, const int* done, const double* sysv,
                                                      int nsys, double* x, VT* r, VT* z, const VT* p, const VT* q,
                                                      const VT* invd, double* part) {
-  const int blk = blockIdx.x;
-  const int s = rb_sys[blk];
-  double v[2] = {0, 0};
-  if (sel[s] && !done[s]) {
-    const double alpha = sysv[SV_ALPHA * nsys + s];
-    const int rs = rb_start[blk], re = rb_start[blk + 1];
-    for (int i = rs + threadIdx.x; i < re; i += blockDim.x) {
-      x[i] += alpha * (double)p[i];
-      VT rr = (VT)((double)r[i] - alpha * (double)q[i]);
-      VT zz = (VT)((double)invd[i] * (double)rr);
-      r[i] = rr; z[i] = zz;
-      v[0] += (double)rr * (double)zz;
-      v[1] += (double)rr * (double)rr;
+  const int nv = act.cnt ? *act.cnt : gridDim.x;
+  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+    const int blk = act.map ? act.map[vb] : vb;
+    const int s = rb_sys[blk];
+    double v[2] = {0, 0};
+    if (sel[s] && !done[s]) {
+      const double alpha = sysv[SV_ALPHA * nsys + s];
+      const int rs = rb_start[blk], re = rb_start[blk + 1];
+      for (int i = rs + threadIdx.x; i < re; i += blockDim.x) {
+        x[i] += alpha * (double)p[i];
+        VT rr = (VT)((double)r[i] - alpha * (double)q[i]);
+        VT zz = (VT)((double)invd[i] * (double)rr);
+        r[i] = rr; z[i] = zz;
+        v[0] += (double)rr * (double)zz;
+        v[1] += (double)rr * (double)rr;
+      }
     }
+    block_partials<2>(v, part, nrb, blk);
   }
-  block_partials<2>(v, part, nrb, blk);
 }
 
 template <typename VT>
-__global__ void __launch_bounds__(256) k_pcg_update2(const int* rb_start, const int* rb_sys, const int* sel,
-                                                     const int* done, const double* sysv, int nsys, VT* p,
-                                                     const VT* z) {
-  const int blk = blockIdx.x;
-  const int s = rb_sys[blk];
-  if (!sel[s] || done[s]) return;
-  const double beta = sysv[SV_BETA * nsys + s];
-  const int rs = rb_start[blk], re = rb_start[blk + 1];
-  for (int i = rs + threadIdx.x; i < re; i += blockDim.x) p[i] = (VT)((double)z[i] + beta * (double)p[i]);
+__global__ void __launch_bounds__(256) k_pcg_update2(const int* rb_start, const int* rb_sys, ActList act,
+                                                     const int* sel, const int* done, const double* sysv, int nsys,
+                                                     VT* p, const VT* z) {
+  const int nv = act.cnt ? *act.cnt : gridDim.x;
+  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+    const int blk = act.map ? act.map[vb] : vb;
+    const int s = rb_sys[blk];
+    if (!sel[s] || done[s]) continue;  // uniform over the block
+    const double beta = sysv[SV_BETA * nsys + s];
+    const int rs = rb_start[blk], re = rb_start[blk + 1];
+    for (int i = rs + threadIdx.x; i < re; i += blockDim.x) p[i] = (VT)((double)z[i] + beta * (double)p[i]);
+  }
 }
 
 // Sum NV partial arrays of one system in a fixed order.
@@ -620,6 +633,7 @@ static int ensure_work(ua_mesh* m) {
   Work* w = new Work();
   const int nsys = m->dm.nsys, N = m->ndof_total, NN = m->nn_total;
   w->nsys = nsys;
+  cudaDeviceGetAttribute(&w->nsm, cudaDevAttrMultiProcessorCount, m->device);
   // row blocks
   std::vector<int> rb_start, rb_sys;
   w->h_sys_rb_off.assign(nsys + 1, 0);
@@ -962,6 +976,15 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   // l1 diagonal and the Galerkin products come from the FP32 values; the cycle stays symmetric and,
   // with the l1 diagonal above half the row sums, positive definite)
   if (amg && fp32 && p->precond_bf16) view.K0lo = amg_bf16_copy(m, (const float*)K, m->nnz_total, &g_launches);
+  // with AMG the finest-level Krylov kernels and the V-cycle loop over the row and node blocks of
+  // the systems still iterating (lists recompacted after every convergence check)
+  if (amg && !p->krylov_full_grid) {
+    int rc = amg_act_init(m, w->h_sys_rb_off);
+    if (rc) return rc;
+    view.act = true;
+  }
+  const ActList act0 = view.act ? amg_act_rows0(m) : ActList{};
+  const int grid0 = view.act ? act_grid(w->nrb, w->nsm) : w->nrb;
   dispatch_lpr(lpr, [&](auto L) {
     if (uvlay)
       k_pcg_init<KT, VT, decltype(L)::value, true><<<w->nrb, 256, 0, m->stream>>>(
@@ -976,6 +999,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   if (amg) {
     // done[] is reset by the stage-0 reduction below; the V-cycle must see every selected system
     UA_CUDA_TRY(cudaMemsetAsync(w->done, 0, w->nsys * sizeof(int), m->stream));
+    if (view.act) amg_act_compact(m, w->sel, w->done, &g_launches);
     view.pcopy = pp;
     int rc = amg_vcycle(m, fp32, view, &g_launches);
     if (rc) return rc;
@@ -983,6 +1007,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   }
   k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(0, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                         w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+  if (view.act) amg_act_compact(m, w->sel, w->done, &g_launches);
   UA_CUDA_TRY(cudaGetLastError());
   const int chunk = 16;
   // one PCG iteration for every selected, unfinished system
@@ -991,19 +1016,19 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     prof_begin(m, PK_SPMV, ev);
     dispatch_lpr(lpr, [&](auto L) {
       if (uvlay)
-        k_pcg_spmv<KT, VT, decltype(L)::value, true><<<w->nrb, 256, 0, m->stream>>>(
-            w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q, w->part,
+        k_pcg_spmv<KT, VT, decltype(L)::value, true><<<grid0, 256, 0, m->stream>>>(
+            w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q, w->part,
             m->dm.sys_dof_off);
       else
-        k_pcg_spmv<KT, VT, decltype(L)::value, false><<<w->nrb, 256, 0, m->stream>>>(
-            w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q, w->part,
+        k_pcg_spmv<KT, VT, decltype(L)::value, false><<<grid0, 256, 0, m->stream>>>(
+            w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q, w->part,
             nullptr);
     });
     ++g_launches;
     prof_end(m, ev);
     k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                           w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
-    k_pcg_update1<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->sysv,
+    k_pcg_update1<VT><<<grid0, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->sysv,
                                                      w->nsys, w->dX, r, zj, pp, q, invd, w->part), ++g_launches;
     if (amg) {
       int rc = amg_vcycle(m, fp32, view, &g_launches);
@@ -1011,15 +1036,16 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     }
     k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                           w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
-    k_pcg_update2<VT><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->done, w->sysv, w->nsys,
-                                                     pp, z), ++g_launches;
+    if (view.act) amg_act_compact(m, w->sel, w->done, &g_launches);
+    k_pcg_update2<VT><<<grid0, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, act0, w->sel, w->done, w->sysv,
+                                                     w->nsys, pp, z), ++g_launches;
     return UA_OK;
   };
   // A chunk of iterations is captured once per (handle, precision, preconditioner) as a CUDA
   // graph and replayed: every argument is a fixed device buffer of the handle, and systems that
   // have converged skip their rows on the device (done[s]), so a replay equals the launches.
   const bool graph = !w->no_graph && !p->profile;
-  const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0) + (view.K0lo ? 4 : 0);
+  const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0) + (view.K0lo ? 4 : 0) + (view.act ? 8 : 0);
   if (graph && w->pcg_exec[gk] && (w->pcg_exec_maxit[gk] != p->krylov_maxit || w->pcg_exec_lpr[gk] != lpr)) {
     cudaGraphExecDestroy(w->pcg_exec[gk]);
     w->pcg_exec[gk] = nullptr;
@@ -2244,6 +2270,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->uvh_krylov = UA_KRYLOV_GMRES; p->krylov_restart = 40;
   p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
   p->amg_smoothed = 1;
+  p->krylov_full_grid = 0;
   p->krylov_precond = UA_PC_AMG;
 }
 

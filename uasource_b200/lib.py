@@ -77,7 +77,7 @@ class ua_params(C.Structure):
         ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32), ("spmv_lanes", C.c_int32), ("asm_threads", C.c_int32),
         ("uvh_krylov", C.c_int32), ("krylov_restart", C.c_int32),
         ("krylov_eta_c", C.c_double), ("krylov_eta_max", C.c_double), ("precond_bf16", C.c_int32),
-        ("amg_smoothed", C.c_int32),
+        ("amg_smoothed", C.c_int32), ("krylov_full_grid", C.c_int32),
     ]
 
 

@@ -83,6 +83,7 @@ class CtrlVar:
     krylov_eta_max: float = 0.1
     precond_bf16: int = 1
     amg_smoothed: int = 1
+    krylov_full_grid: int = 0
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
