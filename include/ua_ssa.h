@@ -136,6 +136,8 @@ typedef struct ua_params {
     int32_t krylov_full_grid;  /* 0 = the AMG-preconditioned PCG launches only the row and node blocks of
                                   systems still iterating (device-compacted lists, default); 1 = every
                                   block of the batch (same results) */
+    int32_t uvh_h_sweeps;      /* uvh block preconditioner: l1-Jacobi sweeps on the thickness block K_hh
+                                  (0 = default 8) */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

@@ -105,6 +105,7 @@ struct Work {
   void *krh = nullptr, *ks = nullptr, *ksh = nullptr, *kt = nullptr;
   // uvh GMRES(m): basis, work vectors, per-system coefficients
   double *gm_V = nullptr, *gm_w = nullptr, *gm_z = nullptr, *gm_u = nullptr, *gm_part = nullptr;
+  double *gm_hb = nullptr, *gm_ht = nullptr, *gm_hl1 = nullptr;  // thickness-block sweeps: b_h, ping-pong, l1
   double *gm_coef = nullptr, *gm_scal = nullptr;
   int *gm_act = nullptr, *gm_ny = nullptr;
   int gm_m = 0;
@@ -1763,21 +1764,64 @@ __global__ void __launch_bounds__(256) k_gm_resid(const int* rb_start, const int
 // Thickness rows of the block lower-triangular preconditioner:
 // z_h = invd_h (p_h - K_hu z_u - K_hv z_v), the velocity part z already set
 // (row (2, g) of a uvh tangent: blocks u, v, h of deg entries each).
+// Thickness rows of the block lower-triangular preconditioner: b_h = p_h - K_hu z_u (z_u
+// already in z), then the first l1-Jacobi sweep zt_h = b_h / l1_h.  A row of the uvh tangent
+// holds three blocks of deg columns (u, v, h).
 __global__ void __launch_bounds__(256) k_uvh_hrows(const int* rb_start, const int* rb_sys, const int* sel,
                                                    const int* done, const int* dof_off, const int* rowptr,
-                                                   const int* colind, const double* K, const double* invd,
-                                                   const unsigned char* cmask, const double* p, double* z) {
+                                                   const int* colind, const double* K, const double* hl1,
+                                                   const unsigned char* cmask, const double* p, const double* z,
+                                                   double* bh, double* zt) {
   const int blk = blockIdx.x;
   const int s = rb_sys[blk];
   if (!sel[s] || done[s]) return;
   const int nn = (dof_off[s + 1] - dof_off[s]) / 3, h0 = dof_off[s] + 2 * nn;
   const int r0 = max(rb_start[blk], h0), r1 = rb_start[blk + 1];
   for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
-    if (cmask[row]) { z[row] = 0; continue; }
+    if (cmask[row]) { bh[row] = 0; zt[row] = 0; continue; }
     const int q0 = rowptr[row], deg = (rowptr[row + 1] - q0) / 3;
     double acc = 0;
     for (int q = q0; q < q0 + 2 * deg; ++q) acc += K[q] * z[colind[q]];
-    z[row] = invd[row] * (p[row] - acc);
+    const double b = p[row] - acc;
+    bh[row] = b;
+    zt[row] = b / hl1[row];
+  }
+}
+
+// l1 row sums of the thickness block K_hh (the h columns of the h rows)
+__global__ void __launch_bounds__(256) k_uvh_hl1(const int* rb_start, const int* rb_sys, const int* sel,
+                                                 const int* dof_off, const int* rowptr, const double* K,
+                                                 double* hl1) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s]) return;
+  const int nn = (dof_off[s + 1] - dof_off[s]) / 3, h0 = dof_off[s] + 2 * nn;
+  const int r0 = max(rb_start[blk], h0), r1 = rb_start[blk + 1];
+  for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+    const int q0 = rowptr[row], deg = (rowptr[row + 1] - q0) / 3;
+    double a = 0;
+    for (int q = q0 + 2 * deg; q < q0 + 3 * deg; ++q) a += fabs(K[q]);
+    hl1[row] = a > 0 ? a : 1.0;
+  }
+}
+
+// one l1-Jacobi sweep on the thickness block: zout_h = zin_h + (b_h - K_hh zin_h) / l1_h
+__global__ void __launch_bounds__(256) k_uvh_hsweep(const int* rb_start, const int* rb_sys, const int* sel,
+                                                    const int* done, const int* dof_off, const int* rowptr,
+                                                    const int* colind, const double* K, const double* hl1,
+                                                    const unsigned char* cmask, const double* bh,
+                                                    const double* zin, double* zout) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const int nn = (dof_off[s + 1] - dof_off[s]) / 3, h0 = dof_off[s] + 2 * nn;
+  const int r0 = max(rb_start[blk], h0), r1 = rb_start[blk + 1];
+  for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+    if (cmask[row]) { zout[row] = 0; continue; }
+    const int q0 = rowptr[row], deg = (rowptr[row + 1] - q0) / 3;
+    double acc = 0;
+    for (int q = q0 + 2 * deg; q < q0 + 3 * deg; ++q) acc += K[q] * zin[colind[q]];
+    zout[row] = zin[row] + (bh[row] - acc) / hl1[row];
   }
 }
 
@@ -1806,8 +1850,11 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
     w->gm_scal = walloc<double>(m, (size_t)nsys * ld);
     w->gm_act = walloc<int>(m, nsys);
     w->gm_ny = walloc<int>(m, nsys);
+    w->gm_hb = walloc<double>(m, ldv);
+    w->gm_ht = walloc<double>(m, ldv);
+    w->gm_hl1 = walloc<double>(m, ldv);
     if (!w->gm_V || !w->gm_w || !w->gm_z || !w->gm_u || !w->gm_part || !w->gm_coef || !w->gm_scal || !w->gm_act ||
-        !w->gm_ny)
+        !w->gm_ny || !w->gm_hb || !w->gm_ht || !w->gm_hl1)
       return set_error(UA_ERR_OOM, "device allocation of the GMRES basis failed");
     w->gm_m = mr;
   }
@@ -1822,17 +1869,34 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
     if (rc) return rc;
   }
   const int lpr_uv = m->nod == 3 ? 1 : 2;
-  // preconditioner: velocity rows by the AMG V-cycle (else Jacobi), thickness rows by the
-  // block lower-triangular step
+  // thickness block: l1-Jacobi sweeps on K_hh (the P2 consistent mass in K_hh is not diagonally
+  // dominant, so a plain Jacobi step is a poor inverse and a plain Jacobi iteration diverges)
+  const int hsw = p->uvh_h_sweeps > 0 ? p->uvh_h_sweeps : 8;
+  if (m->ndof == 3)
+    k_uvh_hl1<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, m->dm.sys_dof_off, w->rowptr,
+                                      (const double*)K, w->gm_hl1), ++g_launches;
+  // preconditioner: velocity rows by the AMG V-cycle (else Jacobi), thickness rows by the block
+  // lower-triangular step z_h = K_hh^-1 (r_h - K_hu z_u), K_hh^-1 by hsw l1-Jacobi sweeps from zero
   auto precond = [&](const double* in, double* out) -> int {
     k_scale_vec<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, in, invd, out), ++g_launches;
     if (amg) {
       int rc = amg_apply_uvh(m, in, out, w->sel, w->done, lpr_uv, &g_launches);
       if (rc) return rc;
     }
-    if (m->ndof == 3)
+    if (m->ndof == 3) {
+      // ping-pong between gm_ht and out so that the last sweep writes out (h rows only)
+      double* bufs[2] = {out, w->gm_ht};
+      int cur = (hsw - 1) % 2 == 0 ? 0 : 1;
       k_uvh_hrows<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, m->dm.sys_dof_off, w->rowptr,
-                                          w->colind, (const double*)K, invd, w->cmask, in, out), ++g_launches;
+                                          w->colind, (const double*)K, w->gm_hl1, w->cmask, in, out, w->gm_hb,
+                                          bufs[cur]), ++g_launches;
+      for (int k = 1; k < hsw; ++k) {
+        k_uvh_hsweep<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, m->dm.sys_dof_off,
+                                             w->rowptr, w->colind, (const double*)K, w->gm_hl1, w->cmask, w->gm_hb,
+                                             bufs[cur], bufs[1 - cur]), ++g_launches;
+        cur = 1 - cur;
+      }
+    }
     return UA_OK;
   };
   auto spmv = [&](const double* x, double* y) {
@@ -2271,6 +2335,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
   p->amg_smoothed = 1;
   p->krylov_full_grid = 0;
+  p->uvh_h_sweeps = 0;
   p->krylov_precond = UA_PC_AMG;
 }
 

@@ -84,6 +84,7 @@ class CtrlVar:
     precond_bf16: int = 1
     amg_smoothed: int = 1
     krylov_full_grid: int = 0
+    uvh_h_sweeps: int = 0
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
