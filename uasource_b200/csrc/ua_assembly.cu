@@ -76,10 +76,13 @@ __device__ __forceinline__ void uv_ip(const QuadTable& Q, const UvPhys& P, const
     if (Aint < P.AGlenmin) Aint = P.AGlenmin;  // :243
     const double Hint = Sint - Bint;
     const double hfint = rhow * Hint / rhoint;  // :300
-    const double Heint = heaviside_approx(P.kH, hint - hfint, P.Hh0);
-    const double HEint = heaviside_approx(P.kH, hfint - hint, P.Hh0);
-    const double deltaint = dirac_delta(P.kH, hint - hfint, P.Hh0);
-    const double Hposint = heaviside_approx(P.kH, Hint, P.Hh0) * Hint;
+    // flotation steps (:300-310): one expm1 per argument
+    const StepPulse fl = step_pulse(P.kH, hint - hfint, P.Hh0);
+    const double Heint = 0.5 + 0.5 * fl.t;
+    const double HEint = P.Hh0 == 0.0 ? 0.5 - 0.5 * fl.t : heaviside_approx(P.kH, hfint - hint, P.Hh0);
+    const double deltaint = fl.delta;
+    const double Hposint = (0.5 + 0.5 * step_pulse(P.kH, Hint, P.Hh0).t) * Hint;
+    const bool cube = S.cube != 0.0;  // n = m = 3 at every node of the system
     const double dint = HEint * rhoint * hint / rhow + Heint * Hposint;  // :310
     double dsdx = 0, dhdx = 0, dsdy = 0, dhdy = 0, exx = 0, eyy = 0, exy = 0;
 #pragma unroll
@@ -89,9 +92,9 @@ __device__ __forceinline__ void uv_ip(const QuadTable& Q, const UvPhys& P, const
       exx += Dx[a] * un[a]; eyy += Dy[a] * vn[a];
       exy += 0.5 * (Dx[a] * vn[a] + Dy[a] * un[a]);
     }
-    const Drag d = basal_drag_weertman(P, Heint, deltaint, uint, vint, Cint, mint);
+    const Drag d = basal_drag_weertman(P, Heint, deltaint, uint, vint, Cint, mint, cube);
     double eta, E;
-    effective_viscosity(P, Aint, nint, exx, eyy, exy, eta, E);
+    effective_viscosity(P, Aint, nint, exx, eyy, exy, eta, E, cube);
     const double dbdx = dsdx - dhdx, dbdy = dsdy - dhdy;
     const double detJw = detJ * Q.w[ip];
     if (WITHK) {

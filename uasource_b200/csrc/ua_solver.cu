@@ -244,6 +244,17 @@ __global__ void k_calc_bs(int nn, const int* node_sys, const SysScal* scal, doub
   s[g] = b + h[g];
 }
 
+// per-system flag n = m = 3 at every node (the assembly then takes reciprocal cube roots for the
+// powers): set, then cleared by any node with another exponent (every writer stores the same value)
+__global__ void k_cube_set(int nsys, SysScal* scal) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsys) scal[s].cube = 1.0;
+}
+__global__ void k_cube_check(int nn, const int* node_sys, const double* n, const double* m, SysScal* scal) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < nn && (n[g] != 3.0 || m[g] != 3.0)) scal[node_sys[g]].cube = 0.0;
+}
+
 template <typename KT, typename VT>
 __global__ void k_invdiag(int n, const KT* K, const int* diagpos, const unsigned char* cmask, VT* invd) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -747,9 +758,17 @@ static int upload_fields_sys(ua_mesh* m, const ua_fields& f, int s, SysScal& sc)
   return UA_OK;
 }
 
+static void set_cube_flags(ua_mesh* m) {
+  Work* w = m->work;
+  k_cube_set<<<(m->dm.nsys + 255) / 256, 256, 0, m->stream>>>(m->dm.nsys, w->scal), ++g_launches;
+  k_cube_check<<<(m->nn_total + 255) / 256, 256, 0, m->stream>>>(m->nn_total, m->dm.node_sys, w->n, w->m, w->scal),
+      ++g_launches;
+}
+
 static int finish_fields(ua_mesh* m, const ua_params* p, const std::vector<SysScal>& sc, int s0, int count) {
   Work* w = m->work;
   UA_CUDA_TRY(cudaMemcpyAsync(w->scal + s0, sc.data(), count * sizeof(SysScal), cudaMemcpyHostToDevice, m->stream));
+  set_cube_flags(m);
   k_calc_bs<<<(m->nn_total + 255) / 256, 256, 0, m->stream>>>(m->nn_total, m->dm.node_sys, w->scal, p->kH, p->Hh0,
                                                                w->h, w->S, w->B, w->rho, w->s), ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
@@ -2094,6 +2113,7 @@ static int upload_fields_uvh(ua_mesh* m, const ua_params* p, const ua_fields* F,
     sc[s].dt = f.dt;
   }
   UA_CUDA_TRY(cudaMemcpyAsync(w->scal, sc.data(), sc.size() * sizeof(SysScal), cudaMemcpyHostToDevice, m->stream));
+  set_cube_flags(m);
   (void)p;
   return UA_OK;
 }

@@ -158,11 +158,22 @@ __global__ void __launch_bounds__(NOD == 3 ? 512 : 320) uvh_patch_kernel(DevMesh
       const double Bint = itp(F_B), Sint = itp(F_S), rhoint = itp(F_RHO);
       const double Hint = Sint - Bint;
       const double hfint = rhow * Hint / rhoint;
-      const double Heint = heaviside_approx(P.kH, hint - hfint, P.Hh0);
-      const double HEint = heaviside_approx(P.kH, hfint - hint, P.Hh0);
-      const double deltaint = dirac_delta(P.kH, hint - hfint, P.Hh0);
-      const double Deltaint = dirac_delta(P.kH, hfint - hint, P.Hh0);
-      const double Hposint = heaviside_approx(P.kH, Hint, P.Hh0) * Hint;
+      // flotation steps and pulses: one expm1 per argument (for Hh0 = 0 the mirrored step is
+      // 1 - the step and the pulse is even)
+      const StepPulse fl = step_pulse(P.kH, hint - hfint, P.Hh0);
+      const double Heint = 0.5 + 0.5 * fl.t;
+      const double deltaint = fl.delta;
+      double HEint, Deltaint;
+      if (P.Hh0 == 0.0) {
+        HEint = 0.5 - 0.5 * fl.t;
+        Deltaint = fl.delta;
+      } else {
+        const StepPulse fm = step_pulse(P.kH, hfint - hint, P.Hh0);
+        HEint = 0.5 + 0.5 * fm.t;
+        Deltaint = fm.delta;
+      }
+      const double Hposint = (0.5 + 0.5 * step_pulse(P.kH, Hint, P.Hh0).t) * Hint;
+      const bool cube = S.cube != 0.0;  // n = m = 3 at every node of the system
       const double dint = HEint * rhoint * hint / rhow + Heint * Hposint;
       const double Dddhint = HEint * rhoint / rhow - Deltaint * hint * rhoint / rhow + deltaint * Hposint;
       // :132-148
@@ -172,8 +183,8 @@ __global__ void __launch_bounds__(NOD == 3 ? 512 : 320) uvh_patch_kernel(DevMesh
       const double exx = ddx(F_U1), eyy = ddy(F_V1);
       const double exy = 0.5 * (ddx(F_V1) + ddy(F_U1));
       double eta, Ev;
-      effective_viscosity(P.uv, Aint, nint, exx, eyy, exy, eta, Ev);  // :149
-      const Drag d = basal_drag_weertman(P.uv, Heint, deltaint, uint, vint, Cint, mint);  // :150
+      effective_viscosity(P.uv, Aint, nint, exx, eyy, exy, eta, Ev, cube);  // :149
+      const Drag d = basal_drag_weertman(P.uv, Heint, deltaint, uint, vint, Cint, mint, cube);  // :150
       const double speed0 = sqrt(u0int * u0int + v0int * v0int + P.SpeedZero * P.SpeedZero);  // :157
       const double tau0 = P.beta0 * supg_tau(P, speed0, lsupg, dt);                         // :158-159
       const double detJw = detJ * Q.w[ip];
