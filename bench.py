@@ -408,23 +408,40 @@ def run_ours(args):
         "k_pcg_spmv<float,float,1> (PCG SpMV + p.q)":
             (prof["spmv_ms"], prof["spmv_n"], 8 * wn["spmv"] + 13 * wr["spmv"],
              "8 B/nnz (value + column) + per row: 4 rowptr + 4 p + 4 q + 1 mask"),
-        "k_amg_residual<float,float,1> (finest-level residual of the pre-smoothed vector)":
-            (prof["amgR_ms"], prof["amgR_n"], 8 * wn["amgR"] + 17 * wr["amgR"],
-             "8 B/nnz + per row: 4 rowptr + 4 b + 4 x + 4 res + 1 mask"),
-        "k_amg_smooth<float,float,1> (finest-level l1-Jacobi post-smoothing + r.z)":
-            (prof["amgP_ms"], prof["amgP_n"], 8 * wn["amgP"] + 21 * wr["amgP"],
-             "8 B/nnz + per row: 4 rowptr + 4 b + 4 xp + 4 invd + 4 z + 1 mask"),
+        "k_amg_residual<bf16,float,1> (finest-level residual of the pre-smoothed vector, BF16 tangent copy)":
+            (prof["amgR_ms"], prof["amgR_n"], 6 * wn["amgR"] + 17 * wr["amgR"],
+             "6 B/nnz (BF16 value + column) + per row: 4 rowptr + 4 b + 4 x + 4 res + 1 mask"),
+        "k_amg_smooth<bf16,float,1> (finest-level l1-Jacobi post-smoothing + r.z, BF16 tangent copy)":
+            (prof["amgP_ms"], prof["amgP_n"], 6 * wn["amgP"] + 21 * wr["amgP"],
+             "6 B/nnz (BF16 value + column) + per row: 4 rowptr + 4 b + 4 xp + 4 invd + 4 z + 1 mask"),
     }
     dom = max(cand, key=lambda c: cand[c][0])
     ms, n, alg_total, rule = cand[dom]
     avg_ms = ms / max(n, 1)
     achieved = alg_total / (ms / 1000) / 1e9 if ms > 0 else 0.0
     total_k = sum(v[0] for v in cand.values())
-    # DRAM traffic per launch: the ncu capture of the finest-level SpMV-class kernels on the 32-mesh
-    # batch read and wrote 1.01 (SpMV) and 1.04 (smoothing) times their algorithmic bytes
-    # (profiles/k_pcg_spmv_batch32.md, profiles/k_amg_smooth_batch32.md); scaled to this launch size
-    traffic_ratio = {"k_pcg_spmv": 147.4 / 146.3, "k_amg_smooth": 161.6 / 155.7}
+    # DRAM traffic per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum of the first launch
+    # of each class on the 32-mesh batch (every system active) over its algorithmic bytes
+    # (profiles/launch_list_batch32_mixed.md and the per-kernel summaries beside it), scaled to this
+    # launch size
+    traffic_ratio = {"uv_patch_kernel<3,K": 193.88 / 145.44, "uv_patch_kernel<3,R": 130.97 / 79.95,
+                     "k_pcg_spmv": 147.55 / 146.31, "k_amg_residual": None, "k_amg_smooth": 123.96 / 122.99}
     tr = next((v for k, v in traffic_ratio.items() if dom.startswith(k)), None)
+    # The assembly classes are bound by FP64 issue, not HBM: their FP64 roofline beside the HBM one.
+    # Executed FP64 operations per P1 element (2 DFMA + DADD + DMUL, ncu instruction counts of the
+    # 32-mesh batch: 6.036e9 / 1,162,956 elements residual-only, 7.136e9 tangent+residual) over
+    # the measured launch time; peak 148 SMs x 64 DFMA/clock x 2 x 1965 MHz = 37.2 TFLOP/s (nominal,
+    # no measured FP64 figure in MEASURED_PEAKS.json).
+    fp64_peak = 148 * 64 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    fp64 = {}
+    for key, fpe in (("uv_patch_kernel<3,K,float> (tangent+residual assembly)", 6136.0),
+                     ("uv_patch_kernel<3,R> (residual-only assembly)", 5190.0)):
+        cms, cn, _, _ = cand[key]
+        cls_rows = wr["asmK" if "<3,K" in key else "asmR"]
+        if cms > 0:
+            tf = fpe * ele_per_row * cls_rows / (cms / 1000) / 1e12
+            fp64[key] = {"achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": tf / fp64_peak,
+                         "flops_per_element": fpe}
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak,
             "traffic": (tr * alg_total / max(n, 1)) if tr else None,
@@ -435,6 +452,7 @@ def run_ours(args):
             "peak_source": ("MEASURED_PEAKS.json hbm_gbs (burst copy), of measured" if "hbm_gbs" in peaks
                             else "fallback 6650 GB/s, of fallback"),
             "kernel_share_of_timed_classes": {c: v[0] / max(total_k, 1e-12) for c, v in cand.items()},
+            "fp64_assembly": fp64, "fp64_peak_source": "148 SMs x 64 DFMA/clock x 2 flops x max SM clock, of nominal",
             "classes_gbs": {c: (v[2] / (v[0] / 1000) / 1e9 if v[0] > 0 else None) for c, v in cand.items()}}
 
     cpu = None

@@ -33,7 +33,7 @@ constexpr int kSaMaxDeg = 256;        // largest coarse node degree of a smoothe
 constexpr int kAmgMaxDense = 2 * kAmgCoarseNodes;
 constexpr int kAmgRB = 256;           // rows per row block of a coarse level
 constexpr int kSaRB = 128, kSaLPR = 2;
-constexpr int kAmgNB = 256;           // nodes per node block of the smoothed transfers  // smoothed hierarchies (longer coarse rows): rows per block, lanes per row
+constexpr int kAmgNB = 32;            // nodes per node block of the smoothed transfers (one warp's worth)  // smoothed hierarchies (longer coarse rows): rows per block, lanes per row
 
 // Calls f(std::integral_constant<int, LPR>) for the lanes-per-row value lpr (1, 2, 4, 8, 16 or 32).
 template <class F>
@@ -1046,22 +1046,26 @@ __global__ void __launch_bounds__(256) k_sa_restrict(const int* nb_start, const 
 
 // prolongation x += P x_c on level l (systems deeper than l; masked rows have zero P rows),
 // one thread per fine node of a node block: both rows share the coarse-node list and the gathered x_c
+// (one warp per node block, kSaPW warps per CTA)
+constexpr int kSaPW = 8;
 template <typename VT>
-__global__ void __launch_bounds__(256) k_sa_prolong(const int* nb_start, const int* nb_sys, ActList act,
-                                                    const int* dof_off, const int* node_off, const int* depth, int l,
-                                                    const int* sel, const int* done, const int* pn_ptr,
-                                                    const int* pn_col, const int* pbase, const int* pnnz,
-                                                    const int* poff, const VT* P, const int* cdof_off,
-                                                    const int* cnode_off, const VT* xc, VT* x) {
-  const int nv = act.cnt ? *act.cnt : gridDim.x;  // list entries, else one node block per CTA
-  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+__global__ void __launch_bounds__(32 * kSaPW) k_sa_prolong(int nnb, const int* nb_start, const int* nb_sys,
+                                                           ActList act, const int* dof_off, const int* node_off,
+                                                           const int* depth, int l, const int* sel, const int* done,
+                                                           const int* pn_ptr, const int* pn_col, const int* pbase,
+                                                           const int* pnnz, const int* poff, const VT* P,
+                                                           const int* cdof_off, const int* cnode_off, const VT* xc,
+                                                           VT* x) {
+  const int nv = act.cnt ? *act.cnt : nnb;  // list entries, else every node block
+  const int lane = threadIdx.x & 31;
+  for (int vb = blockIdx.x * kSaPW + (threadIdx.x >> 5); vb < nv; vb += gridDim.x * kSaPW) {
     const int b = act.map ? act.map[vb] : vb;
     const int s = nb_sys[b];
-    if (!sel[s] || done[s] || depth[s] <= l) continue;  // uniform over the block
+    if (!sel[s] || done[s] || depth[s] <= l) continue;  // uniform over the warp
     const size_t rs = (size_t)2 * pnnz[s];  // P row stride between c = 0 and c = 1
     const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno, cd = cdof_off[s];
     const int no = node_off[s], nn = node_off[s + 1] - no, d0 = dof_off[s];
-    for (int g = nb_start[b] + threadIdx.x; g < nb_start[b + 1]; g += blockDim.x) {
+    for (int g = nb_start[b] + lane; g < nb_start[b + 1]; g += 32) {
       const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
       const VT* p0 = P + poff[s] + 2 * (size_t)(pr - pbase[s]);
       const int i0 = d0 + (g - no), i1 = i0 + nn;
@@ -1216,8 +1220,9 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     const AmgLevel& F = a->lev[l];
     const AmgLevel& C = a->lev[l + 1];
     if (a->sa)
-      k_sa_prolong<VT><<<useact ? act_grid(F.nnb, a->nsm) : F.nnb, 256, 0, st>>>(
-          F.nb_start, F.nb_sys, useact ? a->fnodes[l] : ActList{}, F.d_dof_off, F.d_node_off, a->d_depth, l,
+      k_sa_prolong<VT><<<useact ? act_grid((F.nnb + kSaPW - 1) / kSaPW, a->nsm) : (F.nnb + kSaPW - 1) / kSaPW,
+                         32 * kSaPW, 0, st>>>(
+          F.nnb, F.nb_start, F.nb_sys, useact ? a->fnodes[l] : ActList{}, F.d_dof_off, F.d_node_off, a->d_depth, l,
           v.sel, v.done, F.pn_ptr, F.pn_col, F.pbase, F.pnnz, F.poff, sa_vals<VT>(F.sa_p, F.sa_plo), C.d_dof_off,
           C.d_node_off, (const VT*)C.x2, X(l)), ++*launches;
     else
@@ -1352,11 +1357,14 @@ __device__ int block_excl_scan(int v, int* sh, int& total) {
   return pre + x - v;
 }
 
-// one CTA per list: scan the systems in order, each active system writes its block ids
+// one CTA per list: scan the systems in order (a chunk of blockDim.x systems at a time), then
+// one warp per active system writes its block ids, the lanes striding over them
 __global__ void __launch_bounds__(1024) k_act_compact(const ActSpec* specs, int nsys, const int* sel,
                                                       const int* done, const int* depth) {
   __shared__ int sh[32];
+  __shared__ int s_ex[1024], s_n[1024], s_b0[1024];
   const ActSpec sp = specs[blockIdx.x];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int base = 0;
   for (int c0 = 0; c0 < nsys; c0 += blockDim.x) {  // same trip count for every thread
     const int s = c0 + threadIdx.x;
@@ -1367,7 +1375,16 @@ __global__ void __launch_bounds__(1024) k_act_compact(const ActSpec* specs, int 
     }
     int tot;
     const int ex = block_excl_scan(n, sh, tot);
-    for (int k = 0; k < n; ++k) sp.map[base + ex + k] = b0 + k;
+    s_ex[threadIdx.x] = ex;
+    s_n[threadIdx.x] = n;
+    s_b0[threadIdx.x] = b0;
+    __syncthreads();
+    const int cn = min((int)blockDim.x, nsys - c0);
+    for (int t = wid; t < cn; t += nw) {
+      const int nt = s_n[t], et = base + s_ex[t], bt = s_b0[t];
+      for (int k = lane; k < nt; k += 32) sp.map[et + k] = bt + k;
+    }
+    __syncthreads();  // the shared arrays are rewritten by the next chunk
     base += tot;
   }
   if (threadIdx.x == 0) *sp.cnt = base;
