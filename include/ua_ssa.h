@@ -138,6 +138,9 @@ typedef struct ua_params {
                                   block of the batch (same results) */
     int32_t uvh_h_sweeps;      /* uvh block preconditioner: l1-Jacobi sweeps on the thickness block K_hh
                                   (0 = default 8) */
+    int32_t krylov_sell;       /* 1 = the AMG-preconditioned uv PCG runs its SpMV and the V-cycle's
+                                  finest-level passes on node-sliced (sliced ELL) copies of the tangent,
+                                  both rows of a node per thread (default); 0 = CSR row kernels */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */

@@ -322,3 +322,30 @@ def test_active_block_lists_equal_full_grid(precision, rtol):
     assert len(set(res[0][1])) > 1  # the systems finish at different PCG iterations
     assert res[0][1] == res[1][1]
     assert all(np.array_equal(a, b) for a, b in zip(res[0][0], res[1][0]))
+
+
+@pytest.mark.parametrize("precision,rtol,tol", [(L.UA_PREC_FP64, 1e-12, U_TOL_FP64), (L.UA_PREC_MIXED, 1e-6, U_TOL_MIXED)])
+def test_node_slices_agree_with_csr_kernels(precision, rtol, tol):
+    """The node-sliced (sliced ELL) SpMV and finest-level V-cycle passes, both rows of a node
+    per thread, give the CSR row kernels' solution within the form's tolerance on a batch of
+    uneven meshes (P1 and P2), and a batch solve equals each mesh solved alone bit for bit."""
+    probs = [synth.ice_stream_shelf(21, 11, seed=0), synth.ice_stream_shelf(41, 21, seed=5),
+             synth.ice_stream_shelf(15, 8, seed=9), synth.ice_stream_shelf(9, 6, nod=6, seed=0)]
+    res = {}
+    for sell in (1, 0):
+        ctrl = ua.CtrlVar(precision=precision, krylov_rtol=rtol, krylov_sell=sell).set_force_tolerance(1e-20)
+        out = []
+        for P in probs:
+            mua = ua.CreateMUA(P.coordinates, P.connectivity)
+            Fo, _, _, _, info = ua.uv(ctrl, mua, ua.BCs.from_problem(P), ua.Fields.from_problem(P))
+            assert info.converged
+            out.append(np.concatenate([Fo.ub, Fo.vb]))
+        res[sell] = out
+    for a, b in zip(res[1], res[0]):
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < tol
+    P2 = [p for p in probs if p.nod == 3]
+    batch = ua.CreateMUABatch([(P.coordinates, P.connectivity) for P in P2])
+    ctrl = ua.CtrlVar(precision=precision, krylov_rtol=rtol).set_force_tolerance(1e-20)
+    outb = ua.uv_batch(ctrl, batch, [ua.Fields.from_problem(P) for P in P2], [ua.BCs.from_problem(P) for P in P2])
+    for o, a in zip(outb, res[1][:len(P2)]):
+        assert np.array_equal(np.concatenate([o[0], o[1]]), a)

@@ -91,8 +91,35 @@ struct ActSpec {
   int* cnt;
 };
 
+// Finest-level node slices of a uv handle (sliced ELL over nodes).  A slice block is the set of
+// nodes of one u-row block of the handle's Krylov rows (at most kSellNodes nodes of one system);
+// inside it the nodes are ordered by decreasing degree and cut into slices of 32, one warp each.
+// Slice j holds width W_j = its largest degree; its slots are 32 * W_j, entry k of lane t at slot
+// off_j + 32 k + t.  Per slot: the u column (global u dof of the k-th neighbour; v column = u column
+// + the system's node count) and four values (blocks uu, uv, vu, vv at value offsets
+// 4 off_j + b 32 W_j + 32 k + t).  Padding slots hold zeros and the node's own column.  One column
+// index then serves four values, and a warp's loads of one k are contiguous.
+constexpr int kSellNodes = 256;  // nodes per slice block (= rows per row block)
+constexpr int kSellSlices = kSellNodes / 32;
+
+struct Sell {
+  bool ready = false, failed = false;
+  int nsb = 0;
+  long long slots = 0;
+  std::vector<int> h_sys_sb_off;  // per-system prefix of the slice blocks
+  int *sb_sys = nullptr, *sb_n0 = nullptr, *sb_cnt = nullptr, *sb_rbu = nullptr, *sb_rbv = nullptr;
+  int* perm = nullptr;             // [nn_total]: per block, its global node ids in slice order
+  long long* sl_off = nullptr;     // [nsb * kSellSlices + 1] slot offsets of the slices
+  int* cols = nullptr;             // [slots]
+  float* v32 = nullptr;            // [4 slots] FP32 values (mixed-precision PCG operator)
+  double* v64 = nullptr;           // [4 slots] FP64 values
+  __nv_bfloat16* vlo = nullptr;    // [4 slots] BF16 values (mixed-precision V-cycle)
+  ActList act;                     // slice blocks of the systems still iterating
+};
+
 struct Amg {
   int nsys = 0, nlev = 0, maxdn = 0;
+  Sell sell;
   // active-block lists: rows[l] (level-l row blocks, depth > l; level 0 = the handle's blocks),
   // fnodes[l] (level-l node blocks, depth > l), cnodes[l] (level-(l+1) node blocks, depth > l)
   bool act_ready = false;
@@ -780,6 +807,159 @@ __global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const i
 }
 
 // ---------------------------------------------------------------------------
+// device: finest-level node slices (both rows of a node per thread)
+// ---------------------------------------------------------------------------
+
+struct SellDev {
+  const int *sb_sys, *sb_n0, *sb_cnt, *sb_rbu, *sb_rbv, *perm;
+  const long long* sl_off;
+  const int* cols;
+  const int *dof_off, *node_off;  // per system
+};
+
+// The four values of a slot (blocks uu, uv, vu, vv) are adjacent, so a lane reads them with one
+// vector load: 8 bytes (BF16), 16 (FP32) or 32 (FP64, two loads).
+template <typename KT> struct Quad;
+template <> struct Quad<float> {
+  static __device__ __forceinline__ void get(const float* p, double (&e)[4]) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    e[0] = q.x; e[1] = q.y; e[2] = q.z; e[3] = q.w;
+  }
+};
+template <> struct Quad<double> {
+  static __device__ __forceinline__ void get(const double* p, double (&e)[4]) {
+    const double2 q0 = __ldg(reinterpret_cast<const double2*>(p)), q1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    e[0] = q0.x; e[1] = q0.y; e[2] = q1.x; e[3] = q1.y;
+  }
+};
+template <> struct Quad<__nv_bfloat16> {
+  static __device__ __forceinline__ void get(const __nv_bfloat16* p, double (&e)[4]) {
+    const uint2 q = __ldg(reinterpret_cast<const uint2*>(p));
+    // a BF16 value is the upper half of the FP32 value with the same bits
+    e[0] = __uint_as_float(q.x << 16); e[1] = __uint_as_float(q.x & 0xffff0000u);
+    e[2] = __uint_as_float(q.y << 16); e[3] = __uint_as_float(q.y & 0xffff0000u);
+  }
+};
+
+// Slice values (and, once per handle, the columns) from the tangent's CSR layout: row (c, g)
+// starts at knz_off[s] + 2 c nnzn[s] + 2 lp(g) and holds the u block then the v block of deg(g)
+// entries.  One CTA per slice block, one warp per slice, one lane per node; writes are contiguous.
+template <typename KT>
+__global__ void __launch_bounds__(256) k_sell_fill(SellDev S, const DevMesh dm, const KT* K, KT* vk,
+                                                   __nv_bfloat16* vlo, int* cols) {
+  const int sb = blockIdx.x;
+  const int w = threadIdx.x >> 5, t = threadIdx.x & 31, pos = w * 32 + t;
+  const int sl = sb * kSellSlices + w;
+  const long long o0 = S.sl_off[sl];
+  const int W = (int)((S.sl_off[sl + 1] - o0) >> 5);
+  if (W == 0) return;  // empty slice (warp-uniform)
+  const int s = S.sb_sys[sb];
+  const int no = dm.sys_node_off[s], d0 = dm.sys_dof_off[s];
+  const bool has = pos < S.sb_cnt[sb];
+  int g = no, np0 = 0, deg = 0;
+  if (has) {
+    g = S.perm[S.sb_n0[sb] + pos];
+    np0 = dm.nodeptr[g];
+    deg = dm.nodeptr[g + 1] - np0;
+  }
+  const long long lp = (long long)np0 - dm.nodeptr[no];
+  const long long bu = (long long)dm.sys_knz_off[s] + 2 * lp, bv = bu + 2LL * dm.sys_nnzn[s];
+  for (int k = 0; k < W; ++k) {
+    const bool in = has && k < deg;
+    const long long d = o0 + 32LL * k + t;
+    if (cols) cols[d] = d0 + (in ? dm.nodecol[np0 + k] : g) - no;
+    if (!K) continue;
+    KT e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+    if (in) { e0 = K[bu + k]; e1 = K[bu + deg + k]; e2 = K[bv + k]; e3 = K[bv + deg + k]; }
+    if (vk) { vk[4 * d] = e0; vk[4 * d + 1] = e1; vk[4 * d + 2] = e2; vk[4 * d + 3] = e3; }
+    if (vlo) {
+      vlo[4 * d] = __float2bfloat16_rn((float)e0); vlo[4 * d + 1] = __float2bfloat16_rn((float)e1);
+      vlo[4 * d + 2] = __float2bfloat16_rn((float)e2); vlo[4 * d + 3] = __float2bfloat16_rn((float)e3);
+    }
+  }
+}
+
+// Finest-level row products over the node slices, both rows (u, v) of a node per thread.
+//   MODE 0 (PCG SpMV):    out = mask(K x); partial x.out
+//   MODE 1 (AMG residual): out = mask(b - K x)                 (systems deeper than level 0)
+//   MODE 2 (AMG smoothing): out = mask(x + invd (b - K x)), pcopy = out; partial b.out
+// A block's partial goes to its u-row block, 0 to its v-row block.  List-driven when act.cnt is
+// set (the CTAs loop over the active slice blocks), else one slice block per CTA.
+template <typename KT, typename VT, int MODE>
+__global__ void __launch_bounds__(256) k_sell(SellDev S, int nsb, ActList act, const int* sel, const int* done,
+                                              const int* depth, const KT* vals, const VT* x, const VT* b,
+                                              const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
+                                              double* part) {
+  __shared__ double red[kSellSlices];
+  const int nv = act.cnt ? *act.cnt : nsb;
+  const int w = threadIdx.x >> 5, t = threadIdx.x & 31, pos = w * 32 + t;
+  for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
+    const int sb = act.map ? act.map[vb] : vb;
+    const int s = S.sb_sys[sb];
+    const bool live = sel[s] && !done[s] && (MODE == 0 || depth[s] > 0);
+    if (MODE == 1 && !live) continue;  // uniform over the block
+    double pv = 0;
+    if (live && pos < S.sb_cnt[sb]) {
+      const int sl = sb * kSellSlices + w;
+      const long long o0 = S.sl_off[sl];
+      const int W = (int)((S.sl_off[sl + 1] - o0) >> 5);
+      const int no = S.node_off[s], nn = S.node_off[s + 1] - no;
+      const int g = S.perm[S.sb_n0[sb] + pos];
+      const int ru = S.dof_off[s] + (g - no), rv = ru + nn;
+      // the node's own rows, loaded ahead of the row products
+      const bool mu = cmask && cmask[ru], mv = cmask && cmask[rv];
+      double xu0 = 0, xv0 = 0, bu0 = 0, bv0 = 0, du = 0, dv = 0;
+      if (MODE != 1) { xu0 = to_d(x[ru]); xv0 = to_d(x[rv]); }
+      if (MODE != 0) { bu0 = to_d(b[ru]); bv0 = to_d(b[rv]); }
+      if (MODE == 2) { du = to_d(invd[ru]); dv = to_d(invd[rv]); }
+      const int* cp = S.cols + o0 + t;
+      const KT* vp = vals + 4 * (o0 + t);
+      double au = 0, av = 0;
+#pragma unroll 3
+      for (int k = 0; k < W; ++k) {
+        const int j = __ldg(cp + 32 * k);
+        double e[4];
+        Quad<KT>::get(vp + 128 * k, e);
+        const double xu = to_d(x[j]), xv = to_d(x[j + nn]);
+        au = fma(e[0], xu, au);
+        au = fma(e[1], xv, au);
+        av = fma(e[2], xu, av);
+        av = fma(e[3], xv, av);
+      }
+      if (MODE == 0) {
+        const double qu = mu ? 0.0 : au, qv = mv ? 0.0 : av;
+        out[ru] = (VT)qu;
+        out[rv] = (VT)qv;
+        pv = xu0 * qu + xv0 * qv;
+      } else if (MODE == 1) {
+        out[ru] = (VT)(mu ? 0.0 : bu0 - au);
+        out[rv] = (VT)(mv ? 0.0 : bv0 - av);
+      } else {
+        const double zu = mu ? 0.0 : xu0 + du * (bu0 - au);
+        const double zv = mv ? 0.0 : xv0 + dv * (bv0 - av);
+        out[ru] = (VT)zu;
+        out[rv] = (VT)zv;
+        if (pcopy) { pcopy[ru] = (VT)zu; pcopy[rv] = (VT)zv; }
+        pv = bu0 * zu + bv0 * zv;
+      }
+    }
+    if (MODE == 1 || !part) continue;  // uniform per launch
+    double tw = pv;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tw += __shfl_down_sync(0xffffffffu, tw, o);
+    if (t == 0) red[w] = tw;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0;
+      for (int i = 0; i < kSellSlices; ++i) sum += red[i];
+      part[S.sb_rbu[sb]] = sum;
+      part[S.sb_rbv[sb]] = 0;
+    }
+    __syncthreads();  // red is rewritten by the next entry
+  }
+}
+
+// ---------------------------------------------------------------------------
 // device: smoothed aggregation (P = (I - w D^-1 A) P0, coarse operator P' A P)
 // ---------------------------------------------------------------------------
 //
@@ -1142,6 +1322,124 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
   return UA_OK;
 }
 
+static SellDev sell_dev(const ua_mesh* m, const Sell& S) {
+  return SellDev{S.sb_sys, S.sb_n0, S.sb_cnt, S.sb_rbu, S.sb_rbv, S.perm, S.sl_off, S.cols,
+                 m->dm.sys_dof_off, m->dm.sys_node_off};
+}
+
+int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
+  Amg* a = m->amg;
+  if (!a || m->ndof != 2 || m->h_nodeptr.empty()) return UA_ERR_INVALID;
+  Sell& S = a->sell;
+  if (S.ready) return UA_OK;
+  if (S.failed) return UA_ERR_INVALID;
+  const int nsys = a->nsys;
+  if ((int)sys_rb_off0.size() != nsys + 1) { S.failed = true; return UA_ERR_INVALID; }
+  std::vector<int> sb_sys, sb_n0, sb_cnt, sb_rbu, sb_rbv, perm(m->nn_total), idx;
+  std::vector<long long> sl_off(1, 0);
+  S.h_sys_sb_off.assign(nsys + 1, 0);
+  auto deg = [&](int g) { return m->h_nodeptr[g + 1] - m->h_nodeptr[g]; };
+  for (int s = 0; s < nsys; ++s) {
+    const int no = m->h_node_off[s], nn = m->h_node_off[s + 1] - no;
+    const int nbc = (nn + kSellNodes - 1) / kSellNodes;
+    // the handle's row blocks must be the u blocks then the v blocks of kSellNodes rows each
+    if (sys_rb_off0[s + 1] - sys_rb_off0[s] != 2 * nbc || 2 * nn != m->h_dof_off[s + 1] - m->h_dof_off[s]) {
+      S.failed = true;
+      return set_error(UA_ERR_INVALID, "node slices: row blocks of system %d do not split at the u/v boundary", s);
+    }
+    for (int i = 0; i < nbc; ++i) {
+      const int n0 = no + i * kSellNodes, cnt = std::min(kSellNodes, nn - i * kSellNodes);
+      idx.resize(cnt);
+      for (int k = 0; k < cnt; ++k) idx[k] = n0 + k;
+      std::stable_sort(idx.begin(), idx.end(), [&](int p, int q) { return deg(p) > deg(q); });
+      for (int k = 0; k < cnt; ++k) perm[n0 + k] = idx[k];
+      for (int j = 0; j < kSellSlices; ++j) {
+        int W = 0;
+        for (int k = j * 32; k < std::min(cnt, j * 32 + 32); ++k) W = std::max(W, deg(idx[k]));
+        sl_off.push_back(sl_off.back() + 32LL * W);
+      }
+      sb_sys.push_back(s);
+      sb_n0.push_back(n0);
+      sb_cnt.push_back(cnt);
+      sb_rbu.push_back(sys_rb_off0[s] + i);
+      sb_rbv.push_back(sys_rb_off0[s] + nbc + i);
+    }
+    S.h_sys_sb_off[s + 1] = (int)sb_sys.size();
+  }
+  bool ok = true;
+  S.nsb = (int)sb_sys.size();
+  S.slots = sl_off.back();
+  S.sb_sys = upload(m, a, sb_sys, ok);
+  S.sb_n0 = upload(m, a, sb_n0, ok);
+  S.sb_cnt = upload(m, a, sb_cnt, ok);
+  S.sb_rbu = upload(m, a, sb_rbu, ok);
+  S.sb_rbv = upload(m, a, sb_rbv, ok);
+  S.perm = upload(m, a, perm, ok);
+  S.sl_off = upload(m, a, sl_off, ok);
+  S.cols = (int*)dalloc(m, a, sizeof(int) * (size_t)S.slots, ok);
+  if (!ok) { S.failed = true; return set_error(UA_ERR_OOM, "node slices: device allocation failed"); }
+  if (S.nsb)
+    k_sell_fill<double><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, nullptr, nullptr, nullptr, S.cols);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { S.failed = true; return set_error(UA_ERR_CUDA, "node slices: %s", cudaGetErrorString(e)); }
+  S.ready = true;
+  return UA_OK;
+}
+
+int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* launches) {
+  Amg* a = m->amg;
+  if (!a || !a->sell.ready) return UA_ERR_INVALID;
+  Sell& S = a->sell;
+  bool ok = true;
+  const size_t nv = 4 * (size_t)S.slots;
+  if (fp32 && !S.v32) S.v32 = (float*)dalloc(m, a, sizeof(float) * nv, ok);
+  if (!fp32 && !S.v64) S.v64 = (double*)dalloc(m, a, sizeof(double) * nv, ok);
+  if (lo && !S.vlo) S.vlo = (__nv_bfloat16*)dalloc(m, a, sizeof(__nv_bfloat16) * nv, ok);
+  if (!ok) return set_error(UA_ERR_OOM, "node slices: device allocation of the values failed");
+  if (!S.nsb) return UA_OK;
+  if (fp32)
+    k_sell_fill<float><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, (const float*)K0, S.v32,
+                                                      lo ? S.vlo : nullptr, nullptr);
+  else
+    k_sell_fill<double><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, (const double*)K0, S.v64,
+                                                       lo ? S.vlo : nullptr, nullptr);
+  ++*launches;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "node slices: %s", cudaGetErrorString(e));
+  return UA_OK;
+}
+
+// Grid of a slice kernel: one slice block per CTA, or, list-driven, the CTAs resident at once
+// (per-instantiation occupancy, so that no partial second wave trails the list loop).
+template <typename KT, typename VT, int MODE>
+static int sell_grid(const Amg* a, bool listed) {
+  if (!listed) return a->sell.nsb;
+  static int occ = 0;
+  if (!occ && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sell<KT, VT, MODE>, 256, 0) != cudaSuccess ||
+               occ < 1))
+    occ = 1;
+  return std::max(1, std::min(a->sell.nsb, occ * a->nsm));
+}
+
+int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const int* sel, const int* done, const void* p,
+                  const unsigned char* cmask, void* q, double* part, long long* launches) {
+  Amg* a = m->amg;
+  const Sell& S = a->sell;
+  const bool useact = act && S.act.map;
+  const ActList L = useact ? S.act : ActList{};
+  if (!S.nsb) return UA_OK;
+  if (fp32)
+    k_sell<float, float, 0><<<sell_grid<float, float, 0>(a, useact), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v32,
+                                                         (const float*)p, nullptr, nullptr, cmask, (float*)q,
+                                                         nullptr, part);
+  else
+    k_sell<double, double, 0><<<sell_grid<double, double, 0>(a, useact), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v64,
+                                                           (const double*)p, nullptr, nullptr, cmask, (double*)q,
+                                                           nullptr, part);
+  ++*launches;
+  return UA_OK;
+}
+
 const void* amg_bf16_copy(ua_mesh* m, const float* K0, long long nnz, long long* launches) {
   Amg* a = m->amg;
   if (!a) return nullptr;
@@ -1165,6 +1463,30 @@ template <typename VT>
 static const VT* sa_vals(const double* v64, const float* v32) {
   if constexpr (std::is_same<VT, float>::value) return v32;
   else return v64;
+}
+
+// Finest-level residual (MODE 1: W = mask(r - K x0)) or smoothing (MODE 2: z = mask(x + invd (r - K x)),
+// pcopy, partials r.z) over the node slices, with BF16 values when v.sell_lo.
+template <typename KT, typename VT, int MODE>
+static void sell_pass(ua_mesh* m, const AmgPcgView& v, bool useact, const VT* invd, VT* out) {
+  Amg* a = m->amg;
+  const Sell& S = a->sell;
+  if (!S.nsb) return;
+  const bool la = useact && S.act.map;
+  const ActList L = la ? S.act : ActList{};
+  const VT* x = (const VT*)v.x0;
+  VT* pcopy = MODE == 2 ? (VT*)v.pcopy : nullptr;
+  double* part = MODE == 2 ? v.part_rz : nullptr;
+  const VT* b = (const VT*)v.r;
+  const KT* vk = nullptr;
+  if constexpr (std::is_same<KT, float>::value) vk = S.v32;
+  else vk = S.v64;
+  if (v.sell_lo)
+    k_sell<__nv_bfloat16, VT, MODE><<<sell_grid<__nv_bfloat16, VT, MODE>(a, la), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, v.sel, v.done, a->d_depth,
+                                                                 S.vlo, x, b, invd, v.cmask, out, pcopy, part);
+  else
+    k_sell<KT, VT, MODE><<<sell_grid<KT, VT, MODE>(a, la), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, v.sel, v.done, a->d_depth, vk, x, b,
+                                                      invd, v.cmask, out, pcopy, part);
 }
 
 template <typename KT, typename VT>
@@ -1192,6 +1514,9 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
   for (int l = 0; l + 1 < nl; ++l) {  // down: residual of level l, aggregated into level l+1
     const AmgLevel& C = a->lev[l + 1];
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 0);
+    if (l == 0 && v.sell)
+      sell_pass<KT, VT, 1>(m, v, useact, (const VT*)nullptr, W(0));
+    else
     dispatch_lpr(l == 0 ? lpr0 : lprc, [&](auto L) {
       if (l == 0 && v.K0lo)
         k_amg_residual<__nv_bfloat16, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
@@ -1232,6 +1557,9 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     VT* pcopy = l == 0 ? (VT*)v.pcopy : nullptr;
     double* part = l == 0 ? v.part_rz : nullptr;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 1, 0);
+    if (l == 0 && v.sell)
+      sell_pass<KT, VT, 2>(m, v, useact, (const VT*)F.invd, out);
+    else
     dispatch_lpr(l == 0 ? lpr0 : lprc, [&](auto L) {
       if (l == 0 && v.K0lo)
         k_amg_smooth<__nv_bfloat16, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
@@ -1422,6 +1750,7 @@ int amg_act_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
       a->fnodes[l] = make(a->lev[l].h_sys_nb_off, l);
       a->cnodes[l] = make(a->lev[l + 1].h_sys_nb_off, l);
     }
+  if (a->sell.ready) a->sell.act = make(a->sell.h_sys_sb_off, -1);  // node slice blocks: every active system
   a->d_specs = upload(m, a, specs, ok);
   a->nspecs = (int)specs.size();
   if (!ok) return set_error(UA_ERR_OOM, "active lists: device allocation failed");

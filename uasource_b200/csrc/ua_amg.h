@@ -32,6 +32,9 @@ struct AmgPcgView {
   const void* K0lo = nullptr;
   // loop the row-block and node-block kernels over the active-block lists (amg_act_compact)
   bool act = false;
+  // finest-level residual and smoothing over the node slices (amg_sell_fill done for this
+  // tangent); sell_lo: read their BF16 values
+  bool sell = false, sell_lo = false;
 };
 
 // Active-block lists.  After every convergence check the row blocks (and, for the smoothed
@@ -71,6 +74,16 @@ int amg_numeric_uvh(ua_mesh* m, const double* K3, const unsigned char* cmask3, l
 // out3 = V-cycle(p3) on the velocity rows of 3-dof vectors (other rows untouched).
 int amg_apply_uvh(ua_mesh* m, const double* p3, double* out3, const int* sel, const int* done, int lpr,
                   long long* launches);
+// Node slices of a uv handle's finest level (structure once per handle; call before
+// amg_act_init so that the slice blocks get an active list).  sys_rb_off0 is the handle's
+// per-system row-block prefix; its row blocks must split at the u/v boundary.  UA_OK, else an
+// error code and the CSR kernels stay in use.
+int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0);
+// Slice values of a new tangent K0 (KT = float if fp32, else double); lo: also the BF16 copy.
+int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* launches);
+// PCG SpMV over the node slices: q = mask(K p), partials p.q per u-row block (0 per v-row block).
+int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const int* sel, const int* done, const void* p,
+                  const unsigned char* cmask, void* q, double* part, long long* launches);
 // Refresh the BF16 copy of an FP32 finest-level tangent (allocated on first use;
 // nullptr if that fails).
 const void* amg_bf16_copy(ua_mesh* m, const float* K0, long long nnz, long long* launches);

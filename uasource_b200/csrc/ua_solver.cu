@@ -118,10 +118,10 @@ struct Work {
   struct ServeState* serve = nullptr;
   // replayable PCG chunks, index (fp32 ? 2 : 0) + (amg ? 1 : 0) + (BF16 V-cycle ? 4 : 0) + (active lists ? 8 : 0)
   bool no_graph = false;
-  cudaGraphExec_t pcg_exec[16] = {};
-  long long pcg_exec_nodes[16] = {};
-  int pcg_exec_maxit[16] = {};
-  int pcg_exec_lpr[16] = {};
+  cudaGraphExec_t pcg_exec[32] = {};
+  long long pcg_exec_nodes[32] = {};
+  int pcg_exec_maxit[32] = {};
+  int pcg_exec_lpr[32] = {};
   int nsm = 148;  // SMs of the handle's device (grid of the list-driven kernels)
 };
 
@@ -646,14 +646,18 @@ static int ensure_work(ua_mesh* m) {
   const int nsys = m->dm.nsys, N = m->ndof_total, NN = m->nn_total;
   w->nsys = nsys;
   cudaDeviceGetAttribute(&w->nsm, cudaDevAttrMultiProcessorCount, m->device);
-  // row blocks
+  // row blocks: per system and per dof component (u rows, v rows, ...), so that row block i
+  // of every component covers the same nodes (the node-sliced kernels write both rows of a node)
   std::vector<int> rb_start, rb_sys;
   w->h_sys_rb_off.assign(nsys + 1, 0);
   for (int s = 0; s < nsys; ++s) {
-    for (int r = m->h_dof_off[s]; r < m->h_dof_off[s + 1]; r += kRB) {
-      rb_start.push_back(r);
-      rb_sys.push_back(s);
-    }
+    const int d0 = m->h_dof_off[s], nd = m->h_dof_off[s + 1] - d0;
+    const int ncomp = (m->ndof > 1 && nd % m->ndof == 0) ? m->ndof : 1, nc = nd / ncomp;
+    for (int c = 0; c < ncomp; ++c)
+      for (int r = d0 + c * nc; r < d0 + (c + 1) * nc; r += kRB) {
+        rb_start.push_back(r);
+        rb_sys.push_back(s);
+      }
     w->h_sys_rb_off[s + 1] = (int)rb_start.size();
   }
   rb_start.push_back(N);
@@ -995,7 +999,17 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   // mixed precision: the V-cycle's finest-level residual and smoothing read a BF16 copy of K (the
   // l1 diagonal and the Galerkin products come from the FP32 values; the cycle stays symmetric and,
   // with the l1 diagonal above half the row sums, positive definite)
-  if (amg && fp32 && p->precond_bf16) view.K0lo = amg_bf16_copy(m, (const float*)K, m->nnz_total, &g_launches);
+  // node slices (default): the PCG SpMV and the V-cycle's finest-level passes read per-tangent
+  // sliced-ELL copies of K (FP32/FP64, plus BF16 for the mixed V-cycle) instead of the CSR
+  const bool sell = amg && p->krylov_sell && amg_sell_init(m, w->h_sys_rb_off) == UA_OK;
+  if (sell) {
+    int rc = amg_sell_fill(m, K, fp32, fp32 && p->precond_bf16, &g_launches);
+    if (rc) return rc;
+    view.sell = true;
+    view.sell_lo = fp32 && p->precond_bf16;
+  }
+  if (amg && fp32 && p->precond_bf16 && !sell)
+    view.K0lo = amg_bf16_copy(m, (const float*)K, m->nnz_total, &g_launches);
   // with AMG the finest-level Krylov kernels and the V-cycle loop over the row and node blocks of
   // the systems still iterating (lists recompacted after every convergence check)
   if (amg && !p->krylov_full_grid) {
@@ -1034,17 +1048,21 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   auto iteration = [&]() -> int {
     cudaEvent_t ev[2];
     prof_begin(m, PK_SPMV, ev);
-    dispatch_lpr(lpr, [&](auto L) {
-      if (uvlay)
-        k_pcg_spmv<KT, VT, decltype(L)::value, true><<<grid0, 256, 0, m->stream>>>(
-            w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q, w->part,
-            m->dm.sys_dof_off);
-      else
-        k_pcg_spmv<KT, VT, decltype(L)::value, false><<<grid0, 256, 0, m->stream>>>(
-            w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q, w->part,
-            nullptr);
-    });
-    ++g_launches;
+    if (view.sell)
+      amg_sell_spmv(m, fp32, view.act, w->sel, w->done, pp, w->cmask, q, w->part, &g_launches);
+    else {
+      dispatch_lpr(lpr, [&](auto L) {
+        if (uvlay)
+          k_pcg_spmv<KT, VT, decltype(L)::value, true><<<grid0, 256, 0, m->stream>>>(
+              w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q,
+              w->part, m->dm.sys_dof_off);
+        else
+          k_pcg_spmv<KT, VT, decltype(L)::value, false><<<grid0, 256, 0, m->stream>>>(
+              w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->rowptr, w->colind, K, pp, w->cmask, q,
+              w->part, nullptr);
+      });
+      ++g_launches;
+    }
     prof_end(m, ev);
     k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                           w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
@@ -1065,7 +1083,8 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   // graph and replayed: every argument is a fixed device buffer of the handle, and systems that
   // have converged skip their rows on the device (done[s]), so a replay equals the launches.
   const bool graph = !w->no_graph && !p->profile;
-  const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0) + (view.K0lo ? 4 : 0) + (view.act ? 8 : 0);
+  const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0) + (view.K0lo || view.sell_lo ? 4 : 0) + (view.act ? 8 : 0) +
+                 (view.sell ? 16 : 0);
   if (graph && w->pcg_exec[gk] && (w->pcg_exec_maxit[gk] != p->krylov_maxit || w->pcg_exec_lpr[gk] != lpr)) {
     cudaGraphExecDestroy(w->pcg_exec[gk]);
     w->pcg_exec[gk] = nullptr;
@@ -2356,6 +2375,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->amg_smoothed = 1;
   p->krylov_full_grid = 0;
   p->uvh_h_sweeps = 0;
+  p->krylov_sell = 1;
   p->krylov_precond = UA_PC_AMG;
 }
 

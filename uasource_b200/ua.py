@@ -85,6 +85,7 @@ class CtrlVar:
     amg_smoothed: int = 1
     krylov_full_grid: int = 0
     uvh_h_sweeps: int = 0
+    krylov_sell: int = 1
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
