@@ -405,15 +405,17 @@ def run_ours(args):
         "uv_patch_kernel<3,R> (residual-only assembly)":
             (prof["asmR_ms"], prof["asmR_n"], (12 * ele_per_row + 48 + 8) * wr["asmR"],
              "per row: 12*Ne/rows connectivity + 48 nodal fields + 8 R"),
-        "k_pcg_spmv<float,float,1> (PCG SpMV + p.q)":
-            (prof["spmv_ms"], prof["spmv_n"], 8 * wn["spmv"] + 13 * wr["spmv"],
-             "8 B/nnz (value + column) + per row: 4 rowptr + 4 p + 4 q + 1 mask"),
-        "k_amg_residual<bf16,float,1> (finest-level residual of the pre-smoothed vector, BF16 tangent copy)":
-            (prof["amgR_ms"], prof["amgR_n"], 6 * wn["amgR"] + 17 * wr["amgR"],
-             "6 B/nnz (BF16 value + column) + per row: 4 rowptr + 4 b + 4 x + 4 res + 1 mask"),
-        "k_amg_smooth<bf16,float,1> (finest-level l1-Jacobi post-smoothing + r.z, BF16 tangent copy)":
-            (prof["amgP_ms"], prof["amgP_n"], 6 * wn["amgP"] + 21 * wr["amgP"],
-             "6 B/nnz (BF16 value + column) + per row: 4 rowptr + 4 b + 4 xp + 4 invd + 4 z + 1 mask"),
+        # node-sliced tangent copies: four values per column index, so 1 B of index per non-zero;
+        # one 4-byte node id per node (2 B per row); padding slots are not algorithmic bytes
+        "k_sell<float,float,SpMV> (PCG SpMV + p.q, node slices)":
+            (prof["spmv_ms"], prof["spmv_n"], 5 * wn["spmv"] + 11 * wr["spmv"],
+             "5 B/nnz (FP32 value + 1/4 column) + per row: 2 node id + 4 p + 4 q + 1 mask"),
+        "k_sell<bf16,float,residual> (finest-level residual of the pre-smoothed vector, BF16 node slices)":
+            (prof["amgR_ms"], prof["amgR_n"], 3 * wn["amgR"] + 15 * wr["amgR"],
+             "3 B/nnz (BF16 value + 1/4 column) + per row: 2 node id + 4 b + 4 x + 4 res + 1 mask"),
+        "k_sell<bf16,float,smoothing> (finest-level l1-Jacobi post-smoothing + r.z, BF16 node slices)":
+            (prof["amgP_ms"], prof["amgP_n"], 3 * wn["amgP"] + 19 * wr["amgP"],
+             "3 B/nnz (BF16 value + 1/4 column) + per row: 2 node id + 4 b + 4 xp + 4 invd + 4 z + 1 mask"),
     }
     dom = max(cand, key=lambda c: cand[c][0])
     ms, n, alg_total, rule = cand[dom]
@@ -425,7 +427,8 @@ def run_ours(args):
     # (profiles/launch_list_batch32_mixed.md and the per-kernel summaries beside it), scaled to this
     # launch size
     traffic_ratio = {"uv_patch_kernel<3,K": 193.88 / 145.44, "uv_patch_kernel<3,R": 130.97 / 79.95,
-                     "k_pcg_spmv": 147.55 / 146.31, "k_amg_residual": None, "k_amg_smooth": 123.96 / 122.99}
+                     "k_sell<float,float,SpMV": None, "k_sell<bf16,float,residual": None,
+                     "k_sell<bf16,float,smoothing": None}
     tr = next((v for k, v in traffic_ratio.items() if dom.startswith(k)), None)
     # The assembly classes are bound by FP64 issue, not HBM: their FP64 roofline beside the HBM one.
     # Executed FP64 operations per P1 element (2 DFMA + DADD + DMUL, ncu instruction counts of the

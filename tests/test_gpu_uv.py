@@ -349,3 +349,21 @@ def test_node_slices_agree_with_csr_kernels(precision, rtol, tol):
     outb = ua.uv_batch(ctrl, batch, [ua.Fields.from_problem(P) for P in P2], [ua.BCs.from_problem(P) for P in P2])
     for o, a in zip(outb, res[1][:len(P2)]):
         assert np.array_equal(np.concatenate([o[0], o[1]]), a)
+
+
+@pytest.mark.parametrize("precision,rtol", [(L.UA_PREC_FP64, 1e-12), (L.UA_PREC_MIXED, 1e-6)])
+def test_tangent_assembled_ahead_matches_assembly_per_iteration(precision, rtol):
+    """With the tangent assembled ahead (K with R at the start iterate and at every full Newton
+    step, used when that point is accepted) the solve takes the same Newton iterations and ends
+    at the same solution as assembling K at the start of every iteration (the form used when
+    the caller reads the last tangent back)."""
+    for P in (synth.ice_stream_shelf(21, 11, seed=0), synth.ice_stream_shelf(41, 21, seed=5),
+              synth.ice_stream_shelf(9, 6, nod=6, seed=0)):
+        mua = ua.CreateMUA(P.coordinates, P.connectivity)
+        ctrl = ua.CtrlVar(precision=precision, krylov_rtol=rtol).set_force_tolerance(1e-20)
+        Fa, _, _, _, ia = ua.uv(ctrl, mua, ua.BCs.from_problem(P), ua.Fields.from_problem(P))
+        Fb, _, Kb, _, ib = ua.uv(ctrl, mua, ua.BCs.from_problem(P), ua.Fields.from_problem(P), return_K=True)
+        assert ia.converged and ib.converged and Kb is not None
+        assert ia.iterations == ib.iterations
+        a, b = np.concatenate([Fa.ub, Fa.vb]), np.concatenate([Fb.ub, Fb.vb])
+        assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(b)

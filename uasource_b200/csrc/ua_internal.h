@@ -118,6 +118,9 @@ struct ua_mesh {
   // aggregation AMG hierarchy of the uv tangent (built on first use)
   ua::Amg* amg = nullptr;
   bool amg_failed = false;
+  // the caller reads the tangent back after a Newton solve (ua_uv_newton with Kvals): the
+  // tangent must stay the one of the last Newton system, so no tangent is assembled ahead
+  bool keep_last_tangent = false;
 };
 
 namespace ua {

@@ -893,8 +893,11 @@ static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
   return UA_OK;
 }
 
+// The host staging buffers (pinned) are rewritten only after the stream has drained, so an
+// earlier asynchronous copy from them cannot pick up the new values.
 static int set_sel(ua_mesh* m, const std::vector<int>& sel) {
   Work* w = m->work;
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   for (int s = 0; s < w->nsys; ++s) w->h_int[s] = sel[s];
   UA_CUDA_TRY(cudaMemcpyAsync(w->sel, w->h_int, w->nsys * sizeof(int), cudaMemcpyHostToDevice, m->stream));
   return UA_OK;
@@ -902,6 +905,7 @@ static int set_sel(ua_mesh* m, const std::vector<int>& sel) {
 
 static int set_gamma(ua_mesh* m, const std::vector<double>& g) {
   Work* w = m->work;
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   for (int s = 0; s < w->nsys; ++s) w->h_gamma[s] = g[s];
   UA_CUDA_TRY(cudaMemcpyAsync(w->gamma, w->h_gamma, w->nsys * sizeof(double), cudaMemcpyHostToDevice, m->stream));
   return UA_OK;
@@ -928,10 +932,11 @@ static int assemble(ua_mesh* m, const ua_params* p, bool withK, bool useDir, con
 // CalcCostFunctionNR.m:14-41.  Result in sysv[SV_FF] (rForce) and sysv[SV_FD] (D2).
 // Cost function at X + gamma dX.  assembleR = false takes w->R as it stands:
 // the residual just assembled at X, which is the R-only assembly at gamma = 0.
-static int cost_eval(ua_mesh* m, const ua_params* p, bool useDir, bool assembleR = true) {
+// withK: assemble the tangent too (the next Newton system's, if this point is accepted).
+static int cost_eval(ua_mesh* m, const ua_params* p, bool useDir, bool assembleR = true, bool withK = false) {
   Work* w = m->work;
   if (assembleR) {
-    int rc = assemble(m, p, false, useDir, w->X, false);
+    int rc = assemble(m, p, withK, useDir, w->X, false);
     if (rc) return rc;
   }
   k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, w->dof_con, w->lam,
@@ -1179,6 +1184,9 @@ struct SysState {
   double r = 0, rForce = 0, rWork = 0, gamma = 1, ResidualReduction = 1e10;
   double r0 = 0, rForce0 = 0, rWork0 = 0, r1 = 0, rForce1 = 0, rWork1 = 0;
   int kits = 0;
+  // K and R in the work buffers are those of the current iterate (assembled ahead, at the
+  // cost evaluation that found the iterate), so the next Newton system needs no assembly
+  bool kfresh = false;
   // line search
   bool in_ls = false;
   BackTrack bt;
@@ -1196,6 +1204,16 @@ struct ServeState {
 
 static double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Tangent assembled ahead: the cost evaluations at the start iterate and at the full Newton
+// step (gamma = 1) assemble K with R.  When the point becomes the next iterate (the start, or a
+// full step accepted without backtracking) the next Newton system needs no assembly: K and R
+// at X_k + 1.0 dX_k are the ones an assembly at X_{k+1} gives, bit for bit.  Off when the
+// caller reads the last Newton system's tangent back, and for the modified Newton variant
+// (ModifiedNRuvIntervalCriterion > 1) that keeps old tangents.
+static bool tangent_ahead(const ua_mesh* m, const ua_params* p) {
+  return !m->keep_last_tangent && p->ModifiedNRuvIntervalCriterion <= 1;
 }
 
 // Start the Newton solve of the systems with run[s]=1 (SSTREAM2dNR2.m:100-156):
@@ -1226,10 +1244,12 @@ static int newton_init(ua_mesh* m, const ua_params* p, const std::vector<int>& r
   // initial cost (:149-152) with zero direction
   UA_CUDA_TRY(cudaMemsetAsync(w->dX, 0, m->ndof_total * sizeof(double), m->stream));
   if (w->nc) UA_CUDA_TRY(cudaMemsetAsync(w->dlam, 0, w->nc * sizeof(double), m->stream));
-  if ((rc = cost_eval(m, p, false))) return rc;
+  const bool ahead = tangent_ahead(m, p);
+  if ((rc = cost_eval(m, p, false, true, ahead))) return rc;
   for (int s = 0; s < nsys; ++s) {
     if (!run[s]) continue;
     st[s] = SysState();
+    st[s].kfresh = ahead;
     st[s].active = true;
     st[s].r = st[s].rForce = w->h_sysv[SV_FF * nsys + s];
     st[s].rWork = 0;
@@ -1269,7 +1289,22 @@ static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_rep
       if (st[s].active && (((st[s].iteration - 1) % std::max(1, p->ModifiedNRuvIntervalCriterion)) == 0 ||
                            st[s].ResidualReduction > p->ModifiedNRuvReductionCriterion))
         refreshK = true;
-    if ((rc = assemble(m, p, refreshK, false, w->X, false))) return rc;
+    const bool ahead = tangent_ahead(m, p);
+    std::vector<int> asel(nsys);
+    int n_asm = 0, n_fresh = 0;
+    for (int s = 0; s < nsys; ++s) {
+      asel[s] = sel[s] && !(ahead && st[s].kfresh);
+      n_asm += asel[s];
+      n_fresh += sel[s] && !asel[s];
+      st[s].kfresh = false;
+    }
+    if (n_fresh == 0) {
+      if ((rc = assemble(m, p, refreshK, false, w->X, false))) return rc;
+    } else if (n_asm > 0) {  // only the systems whose K and R were not assembled ahead
+      if ((rc = set_sel(m, asel))) return rc;
+      if ((rc = assemble(m, p, refreshK, false, w->X, false))) return rc;
+      if ((rc = set_sel(m, sel))) return rc;
+    }
     k_frhs<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->R, w->dof_con, w->lam, w->frhs), ++g_launches;
     UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
     double t1 = now_ms();
@@ -1296,11 +1331,11 @@ static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_rep
         S.iteration -= 1; S.converged = true; S.active = false; sel[s] = 0;
       }
     }
-    // gamma=1 (:288)
+    // gamma=1 (:288), with the tangent there when it is assembled ahead
     for (int s = 0; s < nsys; ++s) gam[s] = 1.0;
     if ((rc = set_sel(m, sel))) return rc;
     if ((rc = set_gamma(m, gam))) return rc;
-    if ((rc = cost_eval(m, p, true))) return rc;
+    if ((rc = cost_eval(m, p, true, true, ahead))) return rc;
     for (int s = 0; s < nsys; ++s) {
       if (!sel[s]) continue;
       SysState& S = st[s];
@@ -1309,6 +1344,7 @@ static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_rep
       S.rWork1 = D2 * D2;
       if (S.r1 / S.r0 < p->NewtonAcceptRatio) {  // :290-296
         S.in_ls = false;
+        S.kfresh = ahead;
         S.gamma = 1.0; S.r = S.r1; S.rForce = S.rForce1; S.rWork = S.rWork1; S.iarm = 0;
       } else {  // rLineminUa.m:57-135 (Newton-direction backtracking)
         S.in_ls = true;
@@ -2517,7 +2553,9 @@ extern "C" int ua_uv_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const 
   std::vector<ua_newton_report*> reps(1, rep);
   double* lam[1] = {lubvb};
   int nls[1] = {nl};
+  m->keep_last_tangent = Kvals != nullptr;
   int rc = newton_common(m, p, F, bcs, 1, reps, lam, nls);
+  m->keep_last_tangent = false;
   if (rc != UA_OK && rc != UA_ERR_NOT_CONVERGED) return rc;
   Work* w = m->work;
   if (R) UA_CUDA_TRY(cudaMemcpy(R, w->R, m->ndof_total * sizeof(double), cudaMemcpyDeviceToHost));
