@@ -885,8 +885,10 @@ __global__ void __launch_bounds__(256) k_sell_fill(SellDev S, const DevMesh dm, 
 //   MODE 2 (AMG smoothing): out = mask(x + invd (b - K x)), pcopy = out; partial b.out
 // A block's partial goes to its u-row block, 0 to its v-row block.  List-driven when act.cnt is
 // set (the CTAs loop over the active slice blocks), else one slice block per CTA.
+// FP32 vectors: at most 40 registers, six CTAs (48 warps) per SM for the gathers in flight;
+// FP64 vectors: the compiler's choice (48 registers, no spills).
 template <typename KT, typename VT, int MODE>
-__global__ void __launch_bounds__(256) k_sell(SellDev S, int nsb, ActList act, const int* sel, const int* done,
+__global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 6 : 0) k_sell(SellDev S, int nsb, ActList act, const int* sel, const int* done,
                                               const int* depth, const KT* vals, const VT* x, const VT* b,
                                               const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
                                               double* part) {

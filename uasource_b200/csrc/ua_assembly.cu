@@ -277,11 +277,22 @@ __global__ void __launch_bounds__(NOD == 3 ? 256 : 128, NOD == 3 ? 2 : 1) uv_pat
     }
   };
   if constexpr (NOD == 3) {
-    // P1: the integration points of an element on IPL lanes (one each), summed
-    // by a fixed-order butterfly; no loop-carried element state, so far fewer
-    // registers per thread than an element-per-thread loop.
-    constexpr int IPL = 8;
-    const int ip = threadIdx.x % IPL, grp = threadIdx.x / IPL, ngrp = blockDim.x / IPL;
+    // P1: the integration points of an element on the lanes of a group (one each), summed in
+    // a fixed order; no loop-carried element state, so far fewer registers per thread than an
+    // element-per-thread loop.  The 6-point (degree-4) rule runs in 6-lane groups, five per
+    // warp (lanes 30 and 31 idle: ip >= 6), so 30 of 32 lanes compute (the launch checks
+    // nip <= 6).
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int ip = lane < 30 ? lane % 6 : 6 + lane - 30;
+    const int grp = wid * 5 + min(lane / 6, 4);
+    const int ngrp = (int)(blockDim.x >> 5) * 5;
+    // fixed-order sum of a 6-lane group at its lane 0: ((v0 + v3) + (v1 + v4)) + (v2 + v5)
+    auto sum6 = [](auto v) {
+      v += __shfl_down_sync(0xffffffffu, v, 3);
+      const auto a = __shfl_down_sync(0xffffffffu, v, 1);
+      const auto b = __shfl_down_sync(0xffffffffu, v, 2);
+      return (v + a) + b;
+    };
     for (int base = 0; base < ne; base += ngrp) {  // same trip count for every thread of the block
       const int t = base + grp;
       KT Kuu[I::NS], Kvv[I::NS], Kuv[NOD * NOD];
@@ -296,24 +307,15 @@ __global__ void __launch_bounds__(NOD == 3 ? 256 : 128, NOD == 3 ? 2 : 1) uv_pat
         uv_ip<NOD, WITHK, KT>(Q, P, S, ip, Dx, Dy, detJ, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv, Kuv,
                               Tx, Fx, Ty, Fy);
       }
+      if (WITHK) {
 #pragma unroll
-      for (int o = IPL / 2; o > 0; o >>= 1) {
-        if (WITHK) {
+        for (int i = 0; i < I::NS; ++i) { Kuu[i] = sum6(Kuu[i]); Kvv[i] = sum6(Kvv[i]); }
 #pragma unroll
-          for (int i = 0; i < I::NS; ++i) {
-            Kuu[i] += __shfl_xor_sync(0xffffffffu, Kuu[i], o);
-            Kvv[i] += __shfl_xor_sync(0xffffffffu, Kvv[i], o);
-          }
+        for (int i = 0; i < NOD * NOD; ++i) Kuv[i] = sum6(Kuv[i]);
+      }
 #pragma unroll
-          for (int i = 0; i < NOD * NOD; ++i) Kuv[i] += __shfl_xor_sync(0xffffffffu, Kuv[i], o);
-        }
-#pragma unroll
-        for (int a = 0; a < NOD; ++a) {
-          Tx[a] += __shfl_xor_sync(0xffffffffu, Tx[a], o);
-          Fx[a] += __shfl_xor_sync(0xffffffffu, Fx[a], o);
-          Ty[a] += __shfl_xor_sync(0xffffffffu, Ty[a], o);
-          Fy[a] += __shfl_xor_sync(0xffffffffu, Fy[a], o);
-        }
+      for (int a = 0; a < NOD; ++a) {
+        Tx[a] = sum6(Tx[a]); Fx[a] = sum6(Fx[a]); Ty[a] = sum6(Ty[a]); Fy[a] = sum6(Fy[a]);
       }
       if (t < ne && ip == 0) store(t, Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
     }
@@ -392,6 +394,7 @@ size_t uv_patch_smem(int nod, bool withK, bool fp32, int E) {
 
 template <int NOD, bool WITHK, typename KT>
 static cudaError_t launch_t(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, int threads) {
+  if (NOD == 3 && quad_table(3).nip > 6) return cudaErrorInvalidConfiguration;  // 6-lane groups of the P1 kernel
   size_t sm = uv_patch_smem(NOD, WITHK, sizeof(KT) == 4, m->dm.max_patch_elems);
   auto kern = uv_patch_kernel<NOD, WITHK, KT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
