@@ -208,6 +208,29 @@ def test_nan_inputs_are_rejected():
     assert e.value.code == L.UA_ERR_NAN_INPUT
 
 
+def test_nan_inputs_are_rejected_in_a_batch():
+    """The NaN tests of a batch's host fields run on the device after the upload and report what
+    a scan on the host would: fields before velocities, the lowest system first; the handle then
+    solves clean inputs."""
+    probs = [synth.ice_stream_shelf(15, 8, seed=s) for s in (1, 2, 3)]
+    batch = ua.CreateMUABatch([(P.coordinates, P.connectivity) for P in probs])
+    bcs = [ua.BCs.from_problem(P) for P in probs]
+    Fs = [ua.Fields.from_problem(P) for P in probs]
+    Fs[2].h = Fs[2].h.copy(); Fs[2].h[4] = np.nan
+    Fs[1].C = Fs[1].C.copy(); Fs[1].C[7] = np.nan
+    Fs[0].ub = Fs[0].ub.copy(); Fs[0].ub[2] = np.nan
+    with pytest.raises(ua.UaError) as e:
+        ua.uv_batch(ua.CtrlVar(), batch, Fs, bcs)
+    assert e.value.code == L.UA_ERR_NAN_INPUT and "nan in C (system 1)" in str(e.value)
+    Fs = [ua.Fields.from_problem(P) for P in probs]
+    Fs[2].vb = Fs[2].vb.copy(); Fs[2].vb[0] = np.nan
+    with pytest.raises(ua.UaError) as e:
+        ua.uv_batch(ua.CtrlVar(), batch, Fs, bcs)
+    assert e.value.code == L.UA_ERR_NAN_INPUT and "uvMatrixAssembly:NaN" in str(e.value)
+    out = ua.uv_batch(ua.CtrlVar().set_force_tolerance(1e-20), batch, [ua.Fields.from_problem(P) for P in probs], bcs)
+    assert all(o[2].converged for o in out)
+
+
 def test_bad_mesh_is_rejected():
     coords = np.array([[0, 0], [1, 0], [2, 0.0]])
     with pytest.raises(ua.UaError) as e:

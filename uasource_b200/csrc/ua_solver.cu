@@ -112,6 +112,8 @@ struct Work {
   // pinned host staging
   double* h_sysv = nullptr;
   int* h_int = nullptr;
+  int* nan_first = nullptr;  // device NaN scan result (9 ints) and its pinned host copy
+  int* h_nan = nullptr;
   double* h_gamma = nullptr;
   std::vector<int> h_sys_rb_off, h_sys_con_off;
   Prof prof;
@@ -700,8 +702,11 @@ static int ensure_work(ua_mesh* m) {
   ok = ok && w->rowptr && w->colind && w->diagpos && w->scal && w->part && w->sysv && w->done && w->its &&
        w->status && w->sel && w->gamma && w->cmask && w->dof_con && w->rb_start && w->rb_sys && w->sys_rb_off;
   if (!ok) { delete w; return set_error(UA_ERR_OOM, "device allocation of work buffers failed"); }
+  w->nan_first = walloc<int>(m, 16);
+  if (!w->nan_first) { delete w; return set_error(UA_ERR_OOM, "device allocation of work buffers failed"); }
   if (cudaMallocHost(&w->h_sysv, SV_COUNT * sizeof(double) * nsys) != cudaSuccess ||
       cudaMallocHost(&w->h_int, 4 * sizeof(int) * (nsys + 1)) != cudaSuccess ||
+      cudaMallocHost(&w->h_nan, 16 * sizeof(int)) != cudaSuccess ||
       cudaMallocHost(&w->h_gamma, sizeof(double) * nsys) != cudaSuccess) {
     delete w;
     return set_error(UA_ERR_OOM, "pinned host allocation failed");
@@ -740,8 +745,42 @@ static bool any_nan(const double* v, int n) {
   return false;
 }
 
-// Nodal fields of system s (host or device pointers); SysScal staged in sc.
-static int upload_fields_sys(ua_mesh* m, const ua_fields& f, int s, SysScal& sc) {
+// NaN scan of uploaded arrays on the device (the reference's anynan tests, SSTREAM2dNR2.m:42-66):
+// per array k, first[k] = the lowest system with a NaN (node-indexed arrays map a node to its
+// system, dof-indexed ones search the system dof offsets).  first[] starts at INT_MAX.
+struct NanScan {
+  const double* a[10];
+  int len[10];
+  int dof[10];
+};
+
+__global__ void k_nan_scan(NanScan S, const int* node_sys, const int* sys_dof_off, int nsys, int* first) {
+  const int k = blockIdx.y;
+  const double* a = S.a[k];
+  const int n = S.len[k];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = a[i];
+    if (v != v) {
+      int sys = 0;
+      if (S.dof[k]) {
+        int lo = 0, hi = nsys - 1;  // largest sys with sys_dof_off[sys] <= i
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (sys_dof_off[mid] <= i) lo = mid; else hi = mid - 1;
+        }
+        sys = lo;
+      } else {
+        sys = node_sys[i];
+      }
+      atomicMin(first + k, sys);
+    }
+  }
+}
+
+// Nodal fields of system s (host or device pointers); SysScal staged in sc.  host_nan: scan host
+// arrays for NaN here (else the caller scans the uploaded fields on the device).
+static int upload_fields_sys(ua_mesh* m, const ua_fields& f, int s, SysScal& sc, bool host_nan = true,
+                             bool copy = true) {
   Work* w = m->work;
   const int no = m->h_node_off[s], nn = m->sys[s].nn;
   const double* src[] = {f.h, f.S, f.B, f.rho, f.AGlen, f.n, f.C, f.m};
@@ -751,9 +790,10 @@ static int upload_fields_sys(ua_mesh* m, const ua_fields& f, int s, SysScal& sc)
     if (!src[k]) return set_error(UA_ERR_INVALID, "system %d: null field pointer %s", s, names[k]);
     // SSTREAM2dNR2.m:42-65: NaN in C or A (warning + NaN solution in the
     // reference) and NaN in S, h, rho (error) all stop the solve here.
-    if (f.location == UA_HOST && any_nan(src[k], nn))
+    if (host_nan && f.location == UA_HOST && any_nan(src[k], nn))
       return set_error(UA_ERR_NAN_INPUT, "SSTREAM2dNR2: nan in %s (system %d)", names[k], s);
-    UA_CUDA_TRY(cudaMemcpyAsync(dst[k] + no, src[k], nn * sizeof(double),
+    if (copy)
+      UA_CUDA_TRY(cudaMemcpyAsync(dst[k] + no, src[k], nn * sizeof(double),
                                 f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                                 m->stream));
   }
@@ -779,22 +819,79 @@ static int finish_fields(ua_mesh* m, const ua_params* p, const std::vector<SysSc
   return UA_OK;
 }
 
-// Upload nodal fields of every system (host or device pointers) and compute s.
+// Upload nodal fields of every system (host or device pointers) and compute s.  The NaN tests
+// of host fields run on the device after the copies (device_nan_check).
 static int upload_fields(ua_mesh* m, const ua_params* p, const ua_fields* F, int nF) {
-  std::vector<SysScal> sc(m->dm.nsys);
-  for (int s = 0; s < m->dm.nsys; ++s) {
-    int rc = upload_fields_sys(m, F[nF == 1 ? 0 : s], s, sc[s]);
+  Work* w = m->work;
+  const int nsys = m->dm.nsys;
+  std::vector<SysScal> sc(nsys);
+  for (int s = 0; s < nsys; ++s) {
+    int rc = upload_fields_sys(m, F[nF == 1 ? 0 : s], s, sc[s], false, false);
     if (rc) return rc;
   }
-  return finish_fields(m, p, sc, 0, m->dm.nsys);
+  // one copy per run of systems whose arrays follow each other in memory (a batch passed as
+  // slices of one array per field), else one per system
+  double* dst[] = {w->h, w->S, w->B, w->rho, w->A, w->n, w->C, w->m};
+  auto src_of = [&](int s, int k) -> const double* {
+    const ua_fields& f = F[nF == 1 ? 0 : s];
+    const double* a[] = {f.h, f.S, f.B, f.rho, f.AGlen, f.n, f.C, f.m};
+    return a[k];
+  };
+  for (int k = 0; k < 8; ++k)
+    for (int s = 0; s < nsys;) {
+      const int loc = F[nF == 1 ? 0 : s].location;
+      const double* a = src_of(s, k);
+      size_t len = (size_t)m->sys[s].nn;
+      int e = s + 1;
+      while (e < nsys && F[nF == 1 ? 0 : e].location == loc && src_of(e, k) == a + len) len += m->sys[e++].nn;
+      UA_CUDA_TRY(cudaMemcpyAsync(dst[k] + m->h_node_off[s], a, len * sizeof(double),
+                                  loc == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, m->stream));
+      s = e;
+    }
+  return finish_fields(m, p, sc, 0, nsys);
 }
 
-// Velocities of system s into the dof vector X.
-static int upload_velocity_sys(ua_mesh* m, const ua_fields& f, int s) {
+// The NaN tests of upload_fields + upload_velocity on the device, over every system whose fields
+// came from host memory, with the host scan's errors and order: fields before velocities, then
+// the lowest system, then the field order h, S, B, rho, AGlen, n, C, m.
+static int device_nan_check(ua_mesh* m, const ua_fields* F, int nF) {
+  Work* w = m->work;
+  const int nsys = m->dm.nsys;
+  bool any_host = false;
+  for (int s = 0; s < nsys; ++s) any_host = any_host || F[nF == 1 ? 0 : s].location == UA_HOST;
+  if (!any_host) return UA_OK;
+  NanScan S{};
+  const double* arr[] = {w->h, w->S, w->B, w->rho, w->A, w->n, w->C, w->m, w->X};
+  const int na = 9;
+  for (int k = 0; k < na; ++k) {
+    S.a[k] = arr[k];
+    S.len[k] = k < 8 ? m->nn_total : m->ndof_total;
+    S.dof[k] = k == 8;
+  }
+  UA_CUDA_TRY(cudaMemsetAsync(w->nan_first, 0x7f, na * sizeof(int), m->stream));
+  k_nan_scan<<<dim3(296, na), 256, 0, m->stream>>>(S, m->dm.node_sys, m->dm.sys_dof_off, nsys, w->nan_first),
+      ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
+  int first[9];
+  UA_CUDA_TRY(cudaMemcpyAsync(w->h_nan, w->nan_first, na * sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  std::memcpy(first, w->h_nan, sizeof(first));
+  const char* names[] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
+  auto host_sys = [&](int s) { return s >= 0 && s < nsys && F[nF == 1 ? 0 : s].location == UA_HOST; };
+  int bs = nsys, bk = -1;
+  for (int k = 0; k < 8; ++k)
+    if (host_sys(first[k]) && first[k] < bs) { bs = first[k]; bk = k; }
+  if (bk >= 0) return set_error(UA_ERR_NAN_INPUT, "SSTREAM2dNR2: nan in %s (system %d)", names[bk], bs);
+  if (host_sys(first[8])) return set_error(UA_ERR_NAN_INPUT, "uvMatrixAssembly:NaN NaN in F.ub or F.vb");
+  return UA_OK;
+}
+
+// Velocities of system s into the dof vector X (host_nan as upload_fields_sys).
+static int upload_velocity_sys(ua_mesh* m, const ua_fields& f, int s, bool host_nan = true) {
   Work* w = m->work;
   const int d0 = m->h_dof_off[s], nn = m->sys[s].nn;
   if (!f.ub || !f.vb) return set_error(UA_ERR_INVALID, "null ub/vb");
-  if (f.location == UA_HOST && (any_nan(f.ub, nn) || any_nan(f.vb, nn)))
+  if (host_nan && f.location == UA_HOST && (any_nan(f.ub, nn) || any_nan(f.vb, nn)))
     return set_error(UA_ERR_NAN_INPUT, "uvMatrixAssembly:NaN NaN in F.ub or F.vb");
   auto kind = f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   UA_CUDA_TRY(cudaMemcpyAsync(w->X + d0, f.ub, nn * sizeof(double), kind, m->stream));
@@ -805,10 +902,10 @@ static int upload_velocity_sys(ua_mesh* m, const ua_fields& f, int s) {
 // Velocities of the fields into the dof vector X.
 static int upload_velocity(ua_mesh* m, const ua_fields* F, int nF) {
   for (int s = 0; s < m->dm.nsys; ++s) {
-    int rc = upload_velocity_sys(m, F[nF == 1 ? 0 : s], s);
+    int rc = upload_velocity_sys(m, F[nF == 1 ? 0 : s], s, false);
     if (rc) return rc;
   }
-  return UA_OK;
+  return device_nan_check(m, F, nF);
 }
 
 // BCs2MLC.m:19-25 + CreateLuv.m:28-76 + ScaleL.m for fixed-node BCs: one unit row
@@ -2608,6 +2705,7 @@ extern "C" void ua_mesh_destroy(ua_mesh* m) {
       if (e) cudaGraphExecDestroy(e);
     if (w->h_sysv) cudaFreeHost(w->h_sysv);
     if (w->h_int) cudaFreeHost(w->h_int);
+    if (w->h_nan) cudaFreeHost(w->h_nan);
     if (w->h_gamma) cudaFreeHost(w->h_gamma);
     delete w;
   }
@@ -2674,6 +2772,7 @@ extern "C" int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const 
     cudaStreamSynchronize(tmp.stream);
     if (w->h_sysv) cudaFreeHost(w->h_sysv);
     if (w->h_int) cudaFreeHost(w->h_int);
+    if (w->h_nan) cudaFreeHost(w->h_nan);
     if (w->h_gamma) cudaFreeHost(w->h_gamma);
     delete w;
     tmp.work = nullptr;
