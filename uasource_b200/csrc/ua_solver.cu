@@ -620,6 +620,15 @@ __global__ void k_lam_update(int nc, const int* con_sys, const int* sel, const d
   lam[c] += gamma[con_sys[c]] * dlam[c];
 }
 
+// Constraint masks: cmask[dof] = 1 and dof_con[dof] = c for every constraint c.
+__global__ void k_con_masks(int nc, const int* con_dof, unsigned char* cmask, int* dof_con) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const int d = con_dof[c];
+  cmask[d] = 1;
+  dof_con[d] = c;
+}
+
 __global__ void k_set_con_values(int nc, const int* con_dof, const int* con_sys, const int* sel,
                                  const double* con_rhs, double* X) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -979,13 +988,12 @@ static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
   }
   UA_CUDA_TRY(cudaMemcpyAsync(w->sys_con_off, sys_off.data(), (nsys + 1) * sizeof(int), cudaMemcpyHostToDevice,
                               m->stream));
-  // dof masks
-  std::vector<unsigned char> cmask(m->ndof_total, 0);
-  std::vector<int> dof_con(m->ndof_total, -1);
-  for (int c = 0; c < nc; ++c) { cmask[con_dof[c]] = 1; dof_con[con_dof[c]] = c; }
-  UA_CUDA_TRY(cudaMemcpyAsync(w->cmask, cmask.data(), cmask.size(), cudaMemcpyHostToDevice, m->stream));
-  UA_CUDA_TRY(cudaMemcpyAsync(w->dof_con, dof_con.data(), dof_con.size() * sizeof(int), cudaMemcpyHostToDevice,
-                              m->stream));
+  // dof masks, on the device: cmask = 0 and dof_con = -1 everywhere, then one thread per
+  // constraint (its dof is unique: repeated nodes were dropped above)
+  UA_CUDA_TRY(cudaMemsetAsync(w->cmask, 0, m->ndof_total, m->stream));
+  UA_CUDA_TRY(cudaMemsetAsync(w->dof_con, 0xff, m->ndof_total * sizeof(int), m->stream));
+  if (nc) k_con_masks<<<(nc + 255) / 256, 256, 0, m->stream>>>(nc, w->con_dof, w->cmask, w->dof_con), ++g_launches;
+  UA_CUDA_TRY(cudaGetLastError());
   UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   return UA_OK;
 }
