@@ -114,6 +114,8 @@ struct Sell {
   float* v32 = nullptr;            // [4 slots] FP32 values (mixed-precision PCG operator)
   double* v64 = nullptr;           // [4 slots] FP64 values
   __nv_bfloat16* vlo = nullptr;    // [4 slots] BF16 values (mixed-precision V-cycle)
+  double* spart = nullptr;         // [nsb * kSellSlices] per-slice partials (p.q, r.z)
+  int* sys_sl_off = nullptr;       // [nsys + 1] per-system slice prefix
   ActList act;                     // slice blocks of the systems still iterating
 };
 
@@ -883,7 +885,7 @@ __global__ void __launch_bounds__(256) k_sell_fill(SellDev S, const DevMesh dm, 
 //   MODE 0 (PCG SpMV):    out = mask(K x); partial x.out
 //   MODE 1 (AMG residual): out = mask(b - K x)                 (systems deeper than level 0)
 //   MODE 2 (AMG smoothing): out = mask(x + invd (b - K x)), pcopy = out; partial b.out
-// A block's partial goes to its u-row block, 0 to its v-row block.  List-driven when act.cnt is
+// The partials go per slice: part[slice block * kSellSlices + warp].  List-driven when act.cnt is
 // set (the CTAs loop over the active slice blocks), else one slice block per CTA.
 // FP32 vectors: at most 40 registers, six CTAs (48 warps) per SM for the gathers in flight;
 // FP64 vectors: the compiler's choice (48 registers, no spills).
@@ -892,7 +894,6 @@ __global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 6 : 0) k_sell(SellDev S
                                               const int* depth, const KT* vals, const VT* x, const VT* b,
                                               const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
                                               double* part) {
-  __shared__ double red[kSellSlices];
   const int nv = act.cnt ? *act.cnt : nsb;
   const int w = threadIdx.x >> 5, t = threadIdx.x & 31, pos = w * 32 + t;
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
@@ -946,18 +947,12 @@ __global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 6 : 0) k_sell(SellDev S
       }
     }
     if (MODE == 1 || !part) continue;  // uniform per launch
+    // one partial per slice (a fixed-order warp sum): no CTA barrier, so the warps of the short
+    // slices do not wait for the long ones
     double tw = pv;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) tw += __shfl_down_sync(0xffffffffu, tw, o);
-    if (t == 0) red[w] = tw;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double sum = 0;
-      for (int i = 0; i < kSellSlices; ++i) sum += red[i];
-      part[S.sb_rbu[sb]] = sum;
-      part[S.sb_rbv[sb]] = 0;
-    }
-    __syncthreads();  // red is rewritten by the next entry
+    if (t == 0) part[sb * kSellSlices + w] = tw;
   }
 }
 
@@ -1379,6 +1374,10 @@ int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
   S.perm = upload(m, a, perm, ok);
   S.sl_off = upload(m, a, sl_off, ok);
   S.cols = (int*)dalloc(m, a, sizeof(int) * (size_t)S.slots, ok);
+  S.spart = (double*)dalloc(m, a, sizeof(double) * kSellSlices * (size_t)std::max(S.nsb, 1), ok);
+  std::vector<int> sl_pre(nsys + 1);
+  for (int s = 0; s <= nsys; ++s) sl_pre[s] = kSellSlices * S.h_sys_sb_off[s];
+  S.sys_sl_off = upload(m, a, sl_pre, ok);
   if (!ok) { S.failed = true; return set_error(UA_ERR_OOM, "node slices: device allocation failed"); }
   if (S.nsb)
     k_sell_fill<double><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, nullptr, nullptr, nullptr, S.cols);
@@ -1423,8 +1422,13 @@ static int sell_grid(const Amg* a, bool listed) {
   return std::max(1, std::min(a->sell.nsb, occ * a->nsm));
 }
 
+void amg_sell_partials(const ua_mesh* m, const double** spart, const int** sys_sl_off) {
+  *spart = m->amg->sell.spart;
+  *sys_sl_off = m->amg->sell.sys_sl_off;
+}
+
 int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const int* sel, const int* done, const void* p,
-                  const unsigned char* cmask, void* q, double* part, long long* launches) {
+                  const unsigned char* cmask, void* q, long long* launches) {
   Amg* a = m->amg;
   const Sell& S = a->sell;
   const bool useact = act && S.act.map;
@@ -1433,11 +1437,11 @@ int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const int* sel, const int* do
   if (fp32)
     k_sell<float, float, 0><<<sell_grid<float, float, 0>(a, useact), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v32,
                                                          (const float*)p, nullptr, nullptr, cmask, (float*)q,
-                                                         nullptr, part);
+                                                         nullptr, S.spart);
   else
     k_sell<double, double, 0><<<sell_grid<double, double, 0>(a, useact), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v64,
                                                            (const double*)p, nullptr, nullptr, cmask, (double*)q,
-                                                           nullptr, part);
+                                                           nullptr, S.spart);
   ++*launches;
   return UA_OK;
 }
@@ -1478,7 +1482,7 @@ static void sell_pass(ua_mesh* m, const AmgPcgView& v, bool useact, const VT* in
   const ActList L = la ? S.act : ActList{};
   const VT* x = (const VT*)v.x0;
   VT* pcopy = MODE == 2 ? (VT*)v.pcopy : nullptr;
-  double* part = MODE == 2 ? v.part_rz : nullptr;
+  double* part = MODE == 2 ? S.spart : nullptr;
   const VT* b = (const VT*)v.r;
   const KT* vk = nullptr;
   if constexpr (std::is_same<KT, float>::value) vk = S.v32;

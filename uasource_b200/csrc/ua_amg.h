@@ -81,9 +81,12 @@ int amg_apply_uvh(ua_mesh* m, const double* p3, double* out3, const int* sel, co
 int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0);
 // Slice values of a new tangent K0 (KT = float if fp32, else double); lo: also the BF16 copy.
 int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* launches);
-// PCG SpMV over the node slices: q = mask(K p), partials p.q per u-row block (0 per v-row block).
+// Per-slice partials of the node-slice SpMV (p.q) and smoothing (r.z), and the per-system
+// slice prefix (the PCG reductions sum these instead of the row-block partials).
+void amg_sell_partials(const ua_mesh* m, const double** spart, const int** sys_sl_off);
+// PCG SpMV over the node slices: q = mask(K p), partials p.q per slice (amg_sell_partials).
 int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const int* sel, const int* done, const void* p,
-                  const unsigned char* cmask, void* q, double* part, long long* launches);
+                  const unsigned char* cmask, void* q, long long* launches);
 // Refresh the BF16 copy of an FP32 finest-level tangent (allocated on first use;
 // nullptr if that fails).
 const void* amg_bf16_copy(ua_mesh* m, const float* K0, long long nnz, long long* launches);

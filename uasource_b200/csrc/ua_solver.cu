@@ -461,14 +461,18 @@ __device__ __forceinline__ void sys_sum(const double* part, int nrb, int b0, int
 }
 
 // stage: 0 = init (rz, rr0), 1 = alpha (pq), 2 = beta (rz_new, rr)
+// spart (node slices): the p.q and r.z partials come per slice (sys_sl_off: per-system slice
+// prefix) instead of from part's first array; r.r stays in part's second array.
 __global__ void k_pcg_reduce(int stage, const int* sys_rb_off, int nrb, const int* sel, int* done, int* its,
-                             int* status, double* sysv, int nsys, const double* part, int maxit) {
+                             int* status, double* sysv, int nsys, const double* part, int maxit,
+                             const double* spart = nullptr, const int* sys_sl_off = nullptr) {
   const int s = blockIdx.x;
   if (!sel[s] || (stage > 0 && done[s])) return;
   const int b0 = sys_rb_off[s], b1 = sys_rb_off[s + 1];
   if (stage == 1) {
     double o[1];
-    sys_sum<1>(part, nrb, b0, b1, o);
+    if (spart) sys_sum<1>(spart, 0, sys_sl_off[s], sys_sl_off[s + 1], o);
+    else sys_sum<1>(part, nrb, b0, b1, o);
     if (threadIdx.x == 0) {
       const double pq = o[0];
       if (!(pq > 0)) {  // not positive definite on the free dofs, or breakdown
@@ -482,7 +486,16 @@ __global__ void k_pcg_reduce(int stage, const int* sys_rb_off, int nrb, const in
     return;
   }
   double o[2];
-  sys_sum<2>(part, nrb, b0, b1, o);
+  if (spart) {
+    double a[1], b[1];
+    sys_sum<1>(spart, 0, sys_sl_off[s], sys_sl_off[s + 1], a);
+    __syncthreads();  // sys_sum's shared array is rewritten by the next call
+    sys_sum<1>(part + nrb, 0, b0, b1, b);
+    o[0] = a[0];
+    o[1] = b[0];
+  } else {
+    sys_sum<2>(part, nrb, b0, b1, o);
+  }
   if (threadIdx.x != 0) return;
   if (stage == 0) {
     sysv[SV_RZ * nsys + s] = o[0];
@@ -1112,6 +1125,10 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   // node slices (default): the PCG SpMV and the V-cycle's finest-level passes read per-tangent
   // sliced-ELL copies of K (FP32/FP64, plus BF16 for the mixed V-cycle) instead of the CSR
   const bool sell = amg && p->krylov_sell && amg_sell_init(m, w->h_sys_rb_off) == UA_OK;
+  // with node slices the p.q and r.z partials are per slice
+  const double* spart = nullptr;
+  const int* sys_sl_off = nullptr;
+  if (sell) amg_sell_partials(m, &spart, &sys_sl_off);
   if (sell) {
     int rc = amg_sell_fill(m, K, fp32, fp32 && p->precond_bf16, &g_launches);
     if (rc) return rc;
@@ -1150,7 +1167,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     view.pcopy = nullptr;
   }
   k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(0, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
-                                                        w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+                                                        w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
   if (view.act) amg_act_compact(m, w->sel, w->done, &g_launches);
   UA_CUDA_TRY(cudaGetLastError());
   const int chunk = 16;
@@ -1159,7 +1176,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     cudaEvent_t ev[2];
     prof_begin(m, PK_SPMV, ev);
     if (view.sell)
-      amg_sell_spmv(m, fp32, view.act, w->sel, w->done, pp, w->cmask, q, w->part, &g_launches);
+      amg_sell_spmv(m, fp32, view.act, w->sel, w->done, pp, w->cmask, q, &g_launches);
     else {
       dispatch_lpr(lpr, [&](auto L) {
         if (uvlay)
@@ -1175,7 +1192,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     }
     prof_end(m, ev);
     k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
-                                                          w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+                                                          w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
     k_pcg_update1<VT><<<grid0, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->sysv,
                                                      w->nsys, w->dX, r, zj, pp, q, invd, w->part), ++g_launches;
     if (amg) {
@@ -1183,7 +1200,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
       if (rc) return rc;
     }
     k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
-                                                          w->status, w->sysv, w->nsys, w->part, p->krylov_maxit), ++g_launches;
+                                                          w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
     if (view.act) amg_act_compact(m, w->sel, w->done, &g_launches);
     k_pcg_update2<VT><<<grid0, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, act0, w->sel, w->done, w->sysv,
                                                      w->nsys, pp, z), ++g_launches;
