@@ -121,8 +121,9 @@ typedef struct ua_params {
     int32_t profile;           /* 1: time assembly and SpMV launches with CUDA events */
     int32_t krylov_adaptive;   /* 1: inner tolerance eta_k = clamp(c*sqrt(rForce_k), krylov_rtol, max)
                                   (inexact Newton forcing term); 0: krylov_rtol every iteration */
-    int32_t krylov_precond;    /* UA_PC_*: preconditioner of the uv inner PCG (the uvh BiCGStab uses
-                                  point Jacobi) */
+    int32_t krylov_precond;    /* UA_PC_*: preconditioner of the uv inner PCG; for uvh, UA_PC_AMG selects
+                                  the block preconditioner (AMG V-cycle on the velocity block, l1-Jacobi
+                                  sweeps on the thickness block) and UA_PC_JACOBI point Jacobi */
     int32_t spmv_lanes;        /* lanes per row of the uv PCG/AMG row products: 0 = by element type
                                   (1 for P1, 2 for P2), else 1, 2, 4, 8, 16 or 32 */
     int32_t asm_threads;       /* CTA size of the P1 uv assembly: 0 = default, else 128 or 256 */
@@ -267,7 +268,9 @@ int ua_uvh_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, int32_t 
 /* Implicit uvh step: SSTREAM_TransientImplicit.m:6-717 (via uvh.m:45 ->
  * uvh2D.m:20, no active-set thickness constraints).  F->ub, vb, h1: start
  * values in, solution out.  luvh: [l.ubvb; l.h] in/out (may be NULL).  The
- * inner solve is Jacobi-preconditioned BiCGStab on the constrained system. */
+ * inner solve on the constrained unsymmetric system is restarted GMRES(m)
+ * (m = krylov_restart) or BiCGStab (uvh_krylov), right-preconditioned by the
+ * block preconditioner selected with krylov_precond. */
 int ua_uvh_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs,
                   double* luvh, int32_t nl, ua_newton_report* rep);
 
@@ -317,7 +320,12 @@ int ua_solve_kape_symmetric(int32_t n, const int64_t* Arowptr, const int64_t* Ac
  * larger sizes return UA_ERR_INVALID.  The array is shared by all calls on a
  * device, so overlapping calls race; the first call on a device looks up the
  * array's address and should come before any stream capture.  Work runs on
- * cudaStreamPerThread and the call returns after it completes. */
+ * cudaStreamPerThread and the call returns after it completes; it is not
+ * ordered after work on the caller's streams, so every write to the inputs
+ * must be complete before the call (a stream or device synchronize).  The CSR
+ * of A is checked on the device before any product reads it: a column outside
+ * [0,n), a negative or decreasing row pointer or an empty matrix returns
+ * UA_ERR_INVALID.  Arowptr[n] must equal the length of Acol and Aval. */
 #define UA_NOALLOC_MAX_ROWS 131072
 #define UA_NOALLOC_MAX_CONSTRAINTS 16384
 int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr, const int32_t* Acol, const double* Aval,

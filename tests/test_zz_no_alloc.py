@@ -85,3 +85,20 @@ def test_noalloc_rejects_sizes_beyond_its_maximum():
                                              1e-12, 0, C.byref(its), 0)
     assert rc == L.UA_ERR_INVALID
     assert b"UA_NOALLOC_MAX_CONSTRAINTS" in lib.ua_last_error()
+
+
+def test_noalloc_rejects_a_malformed_csr():
+    """A column index outside [0, n) is reported as UA_ERR_INVALID before any product reads it."""
+    torch = pytest.importorskip("torch")
+    K, B, f, g, dofs, vals = _system()
+    bad = K.copy()
+    bad.indices = bad.indices.copy()
+    bad.indices[bad.indptr[5]] = K.shape[0] + 7  # one column past the end
+    with pytest.raises(L.UaError) as ei:
+        _noalloc(torch, bad, dofs, vals, f, g)
+    assert ei.value.code == L.UA_ERR_INVALID
+    assert "CSR" in str(ei.value)
+    # the entry point still works afterwards
+    x_ref, _, _ = ua.solveKApeSymmetric(K, B, f, g, rtol=1e-12)
+    x, _, _ = _noalloc(torch, K, dofs, vals, f, g)
+    assert np.linalg.norm(x - x_ref) <= RTOL * np.linalg.norm(x_ref)

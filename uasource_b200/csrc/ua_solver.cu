@@ -10,6 +10,7 @@
 // one-CTA-per-system kernel adds the partials in a fixed order, so a
 // system's result does not depend on which other systems share the launch.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -2899,19 +2900,32 @@ constexpr size_t kNaScratchBytes =
 static __device__ __align__(256) unsigned char g_na_scratch[kNaScratchBytes];
 
 constexpr int kNaMaxDevices = 64;
-static void* g_na_addr[kNaMaxDevices];
+// device address of g_na_scratch per device, looked up once; atomic because
+// host threads may make their first call on a device at the same time
+static std::atomic<void*> g_na_addr[kNaMaxDevices];
 
-// Clears the per-call state.  flags[0]: a free row has no diagonal entry;
+// Clears the per-call state and checks the caller's CSR (flags are zeroed by
+// the host before this launch).  flags[0]: a free row has no diagonal entry;
 // flags[1]: a dof is constrained twice (B*B' not diagonal); flags[2]: a
-// constraint entry is out of range or zero.
+// constraint entry is out of range or zero; flags[3]: the CSR of A is
+// malformed (a column outside [0,n), a negative or decreasing row pointer,
+// or no non-zero at all), so no later kernel may index with it.
 __global__ void k_na_setup(int n, const int* rowptr, const int* col, int* diagpos, unsigned char* cmask,
                            int* dof_con, double* X, int* rb_start, int* rb_sys, int nrb, int* sys_rb_off,
                            int* sys_con_off, int nl, int* sel, int* flags) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
     int dp = -1;
-    for (int j = rowptr[i]; j < rowptr[i + 1]; ++j)
-      if (col[j] == i) dp = j;
+    const int r0 = rowptr[i], r1 = rowptr[i + 1];
+    if (r0 < 0 || r1 < r0) {
+      atomicExch(&flags[3], 1);
+    } else {
+      for (int j = r0; j < r1; ++j) {
+        const int c = col[j];
+        if (c < 0 || c >= n) atomicExch(&flags[3], 1);
+        else if (c == i) dp = j;
+      }
+    }
     diagpos[i] = dp;
     cmask[i] = 0;
     dof_con[i] = -1;
@@ -2923,7 +2937,7 @@ __global__ void k_na_setup(int n, const int* rowptr, const int* col, int* diagpo
     sys_rb_off[0] = 0; sys_rb_off[1] = nrb;
     sys_con_off[0] = 0; sys_con_off[1] = nl;
     sel[0] = 1;
-    flags[0] = flags[1] = flags[2] = 0;
+    if (rowptr[n] <= rowptr[0]) atomicExch(&flags[3], 1);
   }
 }
 
@@ -2951,7 +2965,9 @@ __global__ void k_na_check_diag(int n, const unsigned char* cmask, int* diagpos,
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || diagpos[i] >= 0) return;
   if (!cmask[i]) atomicExch(&flags[0], 1);
-  diagpos[i] = rowptr[i] < rowptr[n] ? rowptr[i] : 0;  // constrained row: the value read is not used
+  // constrained row without entries: any valid index (the set-up rejects a CSR without non-zeros);
+  // the value read is not used
+  diagpos[i] = rowptr[i] < rowptr[n] ? rowptr[i] : rowptr[0];
 }
 
 __global__ void k_na_multiplier(int nl, const double* dlam, const double* Lval, double* y) {
@@ -2980,13 +2996,13 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
   }
   if (device < 0 || device >= ndev || device >= kNaMaxDevices) return set_error(UA_ERR_INVALID, "bad device ordinal %d", device);
   UA_CUDA_TRY(cudaSetDevice(device));
-  if (!g_na_addr[device]) {  // once per device, with that device current
-    void* a = nullptr;
-    UA_CUDA_TRY(cudaGetSymbolAddress(&a, g_na_scratch));
-    g_na_addr[device] = a;
+  void* na_base = g_na_addr[device].load(std::memory_order_acquire);
+  if (!na_base) {  // once per device, with that device current
+    UA_CUDA_TRY(cudaGetSymbolAddress(&na_base, g_na_scratch));
+    g_na_addr[device].store(na_base, std::memory_order_release);
   }
   // carve the scratch array
-  unsigned char* base = (unsigned char*)g_na_addr[device];
+  unsigned char* base = (unsigned char*)na_base;
   size_t off = 0;
   auto carve = [&](size_t bytes) {
     void* q = base + off;
@@ -3027,7 +3043,7 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
   w.done = small + 2 * kNaMaxRb + 6;
   w.its = small + 2 * kNaMaxRb + 7;
   w.status = small + 2 * kNaMaxRb + 8;
-  int* flags = small + 2 * kNaMaxRb + 9;       // 3
+  int* flags = small + 2 * kNaMaxRb + 9;       // 4
   w.part = dsmall; w.sysv = dsmall + 4 * kNaMaxRb;
   w.con_dof = con_i; w.con_sys = con_i + Cn;
   w.con_rhs = con_d; w.dlam = con_d + Cn; w.grhs = con_d + 2 * Cn;
@@ -3041,6 +3057,10 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
   view.work = &w;
   cudaStream_t st = view.stream;
   const int nb = (std::max(n, nrb + 1) + 255) / 256;
+  if (cudaMemsetAsync(flags, 0, 4 * sizeof(int), st) != cudaSuccess) {
+    view.work = nullptr;
+    return set_error(UA_ERR_CUDA, "no-alloc set-up failed");
+  }
   k_na_setup<<<nb, 256, 0, st>>>(n, Arowptr, Acol, w.diagpos, cmask, w.dof_con, w.X, w.rb_start, w.rb_sys, nrb,
                                  w.sys_rb_off, w.sys_con_off, nl, w.sel, flags);
   if (nl)
@@ -3048,14 +3068,18 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
                                                       w.con_rhs, flags);
   k_na_check_diag<<<(n + 255) / 256, 256, 0, st>>>(n, cmask, w.diagpos, Arowptr, flags);
   int rc = UA_OK;
-  int hf[3] = {0, 0, 0};
+  int hf[4] = {0, 0, 0, 0};
   if (cudaGetLastError() != cudaSuccess ||
       cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess) {
     view.work = nullptr;
     return set_error(UA_ERR_CUDA, "no-alloc set-up failed");
   }
-  if (hf[2]) rc = set_error(UA_ERR_INVALID, "constraint row with a dof out of range or a zero coefficient");
+  if (hf[3])
+    rc = set_error(UA_ERR_INVALID,
+                   "A's CSR is invalid: a column index outside [0,n), a negative or decreasing row pointer, "
+                   "or no non-zeros");
+  else if (hf[2]) rc = set_error(UA_ERR_INVALID, "constraint row with a dof out of range or a zero coefficient");
   else if (hf[1]) rc = set_error(UA_ERR_INVALID, "B*B' not diagonal (a dof constrained twice)");
   else if (hf[0]) rc = set_error(UA_ERR_INVALID, "a free row has no diagonal entry");
   if (rc == UA_OK) {
