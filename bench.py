@@ -24,13 +24,16 @@ Reported:
                 templates of 5k-500k elements, lognormal C perturbations, warm
                 starts; p50/p99 latency and solves/s
   roofline      the dominant kernel by measured device time (CUDA events)
-  cpu_baseline  the numpy restatement of the reference (oracle/ua_ref.py) on a
-                bounded sample, one core
+  cpu_baseline  the CPU restatement of the reference (oracle/ua_ref.py with its
+                element loop compiled, oracle/ua_ref_asm.cpp) on every host core over
+                16 meshes spanning the batch's size range; the GPU's FP64 and mixed
+                solutions of those meshes against the oracle's (rel_err_vs_oracle)
 
 Multi-GPU: independent replicas (whole meshes are the independent units; one
 solve of one mesh does not shard), one process per GPU, time = max over ranks.
-``--impl reference`` times the CPU restatement on the host cores (a process
-pool, one mesh per worker per step, size-stratified over the batch).
+``--impl reference`` times the CPU restatement on the host cores: step k of K
+solves the meshes of size rank k mod K, the K steps back to back on a process
+pool (one oracle process per core), so the timed steps solve the whole batch once.
 """
 from __future__ import annotations
 
@@ -46,6 +49,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BATCH = 256
+CPU_SAMPLE = 16  # meshes of the CPU baseline (one per size stratum) and of the error against the oracle
 METRIC = "uv Newton solves/s (batched, mixed FP32/FP64, <=1e-8 rel err vs FP64)"
 
 
@@ -56,11 +60,14 @@ def _workload(count):
 
 # ----------------------------------------------------------------------------- CPU reference arm
 
-def _oracle_solve(k, count):
-    """One full oracle solve of batch problem k (child process); returns (seconds, converged, Nele)."""
+def _oracle_solve(k, count, return_solution=False):
+    """One full oracle solve of batch problem k (child process): the numpy/scipy restatement with
+    its element loop in the compiled C++ restatement (one thread); returns
+    (seconds, converged, Nele, k, solution or None)."""
     sys.path.insert(0, ROOT)
     from oracle import ua_ref as R
     from uasource_b200 import synth
+    R.use_compiled_element_loop(True, 1)
     P = synth.batch_problem(k, count)
     mua = R.create_mua(P.coordinates, P.connectivity)
     p = R.Params()
@@ -70,7 +77,12 @@ def _oracle_solve(k, count):
                 vbFixedValue=P.vbFixedValue)
     t = time.perf_counter()
     res = R.uv(p, mua, bcs, F)
-    return time.perf_counter() - t, bool(res.converged), int(P.Nele)
+    dt = time.perf_counter() - t
+    sol = None
+    if return_solution:
+        import numpy as np
+        sol = np.concatenate([res.ub, res.vb])
+    return dt, bool(res.converged), int(P.Nele), int(k), sol
 
 
 def _oracle_solve_args(a):
@@ -89,71 +101,89 @@ def _stratified(count, n, offset):
     return [int(order[min(count - 1, int((j + offset) * count / n))]) for j in range(n)]
 
 
-def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
+def _host_cpu():
+    """Host core count and CPU model (from /proc/cpuinfo)."""
+    model = None
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return os.cpu_count() or 1, model
+
+
+def _pool(workers):
     import multiprocessing as mp
     for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[v] = "1"
+    return mp.get_context("spawn").Pool(workers)
+
+
+def run_reference(args):
+    """The reference's CPU algorithm on the host cores (the oracle port: MATLAB cannot run on
+    this machine).  Step k of K solves the meshes whose size rank is k modulo K, a stratified
+    1/K share of the batch; the K timed steps run back to back on a process pool with one
+    oracle process per core, largest meshes first, so together they solve each mesh of the
+    batch exactly once and the value is the batch throughput of the host."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
     count = args.batch
-    cores = os.cpu_count() or 1
-    workers = max(1, min(cores, 32))
+    cores, model = _host_cpu()
+    workers = max(1, min(cores, 64))
     order = _size_ranks(count)
-    ctx = mp.get_context("spawn")
-    res = []
-    with ctx.Pool(workers) as pool:
-        for _ in range(args.warmup):  # imports and page cache: the smallest mesh on every worker
+    K = max(1, args.steps)
+    steps = [[int(order[r]) for r in range(k, count, K)] for k in range(K)]
+    size_rank = {int(i): r for r, i in enumerate(order)}
+    tasks = sorted((i for st in steps for i in st), key=lambda i: -size_rank[i])
+    with _pool(workers) as pool:
+        for _ in range(args.warmup):  # imports, page cache, the compiled loop: the smallest mesh per worker
             pool.map(_oracle_solve_args, [(int(order[0]), count)] * workers)
         t0 = time.perf_counter()
-        for k in range(args.steps):
-            idx = _stratified(count, workers, (0.5 + 0.618034 * k) % 1.0)
-            res += pool.map(_oracle_solve_args, [(i, count) for i in idx])
+        res = list(pool.imap_unordered(_oracle_solve_args, [(i, count) for i in tasks]))
         el = time.perf_counter() - t0
-    solves = len(res)
-    value = solves / el
+    value = len(res) / el
     sizes = sorted(r[2] for r in res)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1000 * el / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": _workload(count), "l2": "n/a (CPU)"},
+        "config": {"workload": _workload(count), "l2": "n/a (CPU)",
+                   "step_rule": f"step k solves the meshes of size rank k mod {K} (stratified 1/{K} of the batch); "
+                                f"the {K} steps run back to back on the pool, largest first, covering the "
+                                f"{count} meshes once"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "port",
-                         "sample": f"per step {workers} meshes of the batch, one per size stratum "
-                                   f"({sizes[0]}-{sizes[-1]} elements over the run), one oracle "
-                                   f"(numpy/scipy restatement) process per core"},
+                         "nproc": cores, "cpu_model": model,
+                         "sample": f"all {len(res)} meshes of the batch ({sizes[0]}-{sizes[-1]} elements), one "
+                                   f"oracle process per core (numpy/scipy restatement, element loop in C++, "
+                                   f"SuperLU with UMFPACK's symmetric strategy)"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "converged": all(r[1] for r in res),
+        "converged": int(sum(r[1] for r in res)),
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def _cpu_baseline_single(count, max_seconds):
-    """Oracle on one core over a size-stratified sample until ~max_seconds of work.
-    Returns the sample's solves/s and an extrapolation to the whole batch
-    (per-solve time fitted as a*Nele^b over the sample, summed over all sizes)."""
-    import numpy as np
-    from uasource_b200 import synth
-    order = _size_ranks(count)
-    picks = [int(order[int(q * (count - 1))]) for q in (0.0, 0.125, 0.25, 0.375, 0.5, 0.625, 0.75)]
-    ts, ns = [], []
+def _cpu_baseline_pool(count, n):
+    """The oracle on every host core over a stratified sample of n meshes spanning the whole size
+    range (one per size stratum, the stratum's middle mesh); returns the line's cpu_baseline and
+    the oracle's solutions by batch index (for the GPU's error against the oracle)."""
+    cores, model = _host_cpu()
+    workers = max(1, min(cores, n))
+    picks = _stratified(count, n, 0.5)
     t0 = time.perf_counter()
-    for k in picks:
-        dt, ok, ne = _oracle_solve(k, count)
-        ts.append(dt); ns.append(ne)
-        if time.perf_counter() - t0 > max_seconds:
-            break
-    out = {"value": len(ts) / sum(ts), "unit": "solves/s", "cores": 1, "kind": "port",
-           "sample": f"{len(ts)} full oracle solves of batch meshes at size quantiles 0-{12.5 * (len(ts) - 1):.1f}% "
-                     f"({min(ns)}-{max(ns)} elements), single process"}
-    if len(ts) >= 2:
-        b, loga = np.polyfit(np.log(ns), np.log(ts), 1)
-        sizes = synth.batch_sizes(count)
-        t_all = float(np.sum(np.exp(loga) * sizes ** b))
-        out["extrapolated_batch_solves_per_s"] = count / t_all
-        out["extrapolation"] = f"t = {np.exp(loga):.3g}*Nele^{b:.3f} s fitted on the sample, summed over {count} sizes"
-    return out
+    with _pool(workers) as pool:
+        res = pool.map(_oracle_solve_args, [(i, count, True) for i in sorted(picks, key=lambda i: -i)])
+    el = time.perf_counter() - t0
+    ns = [r[2] for r in res]
+    out = {"value": len(res) / el, "unit": "solves/s", "cores": workers, "kind": "port", "nproc": cores,
+           "cpu_model": model,
+           "sample": f"{len(res)} full oracle solves, one per size stratum of the batch ({min(ns)}-{max(ns)} "
+                     f"elements), in parallel on {workers} processes; solves/s over the sample's wall time",
+           "core_seconds": sum(r[0] for r in res)}
+    return out, {r[3]: r[4] for r in res}
 
 
 # ----------------------------------------------------------------------------- GPU arm
@@ -166,12 +196,13 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = None
 
     def start(self):
+        import tempfile
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix=f"ua_clocks_gpu{self.index}_", suffix=".csv")
+            self.f = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
@@ -189,7 +220,10 @@ class ClockSampler:
         self.f.close()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in open(self.path):
+        with open(self.path) as fh:
+            rows = fh.readlines()
+        os.unlink(self.path)
+        for ln in rows:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -327,9 +361,13 @@ def run_ours(args):
     per_mx, outs_mx, clocks = timed(lambda: solve_batch(ctrlmx), args.steps, args.warmup, sampler)
     infos_mx = outs_mx[-1]
     errs = []
+    cpu_picks = set(_stratified(count, CPU_SAMPLE, 0.5))
+    u_mx = {}
     for s in range(count):
         u = torch.cat([ub[node_off[s]:node_off[s + 1]], vb[node_off[s]:node_off[s + 1]]]).cpu().numpy()
         errs.append(float(np.linalg.norm(u - u64[s]) / np.linalg.norm(u64[s])))
+        if s in cpu_picks:
+            u_mx[s] = u
     launches_mx = sum(o[0].gpu_launches for o in outs_mx)
 
     # batched FP64
@@ -423,9 +461,9 @@ def run_ours(args):
     avg_ms = ms / max(n, 1)
     achieved = alg_total / (ms / 1000) / 1e9 if ms > 0 else 0.0
     total_k = sum(v[0] for v in cand.values())
-    # DRAM traffic per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum of the first launch
-    # of each class on the 32-mesh batch (every system active) over its algorithmic bytes
-    # (profiles/launch_list_batch32_mixed.md and the per-kernel summaries beside it), scaled to this
+    # DRAM traffic per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum (MB) of the first
+    # launch of each class over its algorithmic bytes (MB), captured with
+    # `bench.py --batch 32 --legs mixed --steps 1 --warmup 1` (every system active), scaled to this
     # launch size
     traffic_ratio = {"uv_patch_kernel<3,K": 193.88 / 145.44, "uv_patch_kernel<3,R": 130.97 / 79.95,
                      "k_sell<float,float,SpMV": None, "k_sell<bf16,float,residual": None,
@@ -462,9 +500,18 @@ def run_ours(args):
             # coarse AMG levels, smoothed transfers, AMG set-up, vector updates and reductions)
             "timed_classes_share_of_device_time": total_k / max(float(prof_info.device_ms), 1e-12)}
 
-    cpu = None
+    cpu, vs_oracle = None, None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        cpu = _cpu_baseline_single(count, args.cpu_seconds)
+        cpu, u_ref = _cpu_baseline_pool(count, CPU_SAMPLE)
+        # the batched GPU solutions of the sampled meshes against the FP64 oracle's
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        e64 = [rel(u64[k], u_ref[k]) for k in sorted(u_ref)]
+        emx = [rel(u_mx[k], u_ref[k]) for k in sorted(u_ref)]
+        nes = [probs[k].Nele for k in sorted(u_ref)]
+        vs_oracle = {"meshes": len(e64), "elements": f"{min(nes)}-{max(nes)}",
+                     "fp64_batched_max": max(e64), "mixed_batched_max": max(emx),
+                     "mixed_batched_median": statistics.median(emx),
+                     "tolerance": {"fp64": 1e-10, "mixed": 1e-8}}
 
     if rank == 0:
         lat = sorted(per_mx)
@@ -482,19 +529,21 @@ def run_ours(args):
                        "newton_iterations_mean": float(np.mean(its)), "newton_iterations_max": int(max(its)),
                        "pcg_iterations_mean": float(np.mean(kits)), "converged": int(sum(i.converged for i in infos_mx))},
             "batch_latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "serving": serving,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": int(launches_mx),
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "cauchy_fallbacks": int(sum(i.cauchy_fallbacks for i in infos_mx) + sum(i.cauchy_fallbacks for i in infos64)),
             "rel_err_vs_fp64": {"max": max(errs), "median": statistics.median(errs)},
+            "rel_err_vs_oracle": vs_oracle,
             "plain_fp64": {"value": value_plain, "unit": "solves/s", "form": "one mesh at a time, all FP64",
                            "sample": f"{len(sample)} meshes, one per size stratum of the batch",
                            "ms_per_pass": t_plain},
             "batched_fp64": {"value": value_b64, "unit": "solves/s", "ms_per_step": t_b64 / len(per_b64),
                              "converged": int(sum(i.converged for i in infos64))},
             "mixed_batched_over_plain_fp64": value / value_plain,
-            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "serving": serving,
-            "roofline": roof,
-            "cpu_baseline": cpu,
-            "clocks": clocks,
-            "gpu_launches": int(launches_mx),
         }
         print(json.dumps(line), flush=True)
     mua.close()
@@ -654,7 +703,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--skip-serve", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=200.0)

@@ -193,6 +193,13 @@ typedef struct ua_newton_report {
     int32_t n_iter_records;     /* entries filled in iters (<= iters_capacity) */
     int32_t iters_capacity;
     ua_newton_iter* iters;      /* caller-owned, may be NULL */
+    /* Newton updates (SSTREAM2dNR2.m:367-369, SSTREAM_TransientImplicit.m:478-483): caller-owned,
+     * may be NULL.  Record k (the k-th entry of iters) receives the accepted update of that
+     * iteration, gamma*[du; dv; dl] for uv and gamma*[du; dv; dh; dl] for uvh (Úa dof order, then
+     * the Lagrange multipliers), at updates + k*update_stride.  update_stride >= ndof*Nnodes + nl,
+     * else the call returns UA_ERR_INVALID.  Filled for the first iters_capacity iterations. */
+    double* updates;
+    int64_t update_stride;
 } ua_newton_report;
 
 /* --------------------------------------------------------------------- */

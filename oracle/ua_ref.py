@@ -378,6 +378,41 @@ def basal_drag_weertman(p: Params, He, delta, ub, vb, C, m):
 # ---------------------------------------------------------------------------
 
 
+_COMPILED = {"lib": None, "threads": 1}
+
+
+def use_compiled_element_loop(enable=True, threads=1):
+    """Run uv_matrix_assembly's element loop in the C++ restatement (oracle/ua_ref_asm.cpp,
+    built by oracle/Makefile) on ``threads`` host threads, or back in numpy (the default)."""
+    import ctypes
+    import os
+    if not enable:
+        _COMPILED["lib"] = None
+        return
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libua_ref_asm.so")
+    lib = ctypes.CDLL(path)
+    lib.uvref_element_loop.restype = ctypes.c_int
+    _COMPILED["lib"] = lib
+    _COMPILED["threads"] = int(threads)
+
+
+def _compiled_element_loop(mua, funs, F, ub, vb, par, Ronly, K, T):
+    import ctypes
+    lib = _COMPILED["lib"]
+    c = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    keep = [np.ascontiguousarray(mua.connectivity, dtype=np.int64), c(mua.Deriv), c(mua.DetJ), c(mua.weights),
+            c(funs), c(F.h), c(F.s), c(ub), c(vb), c(F.C), c(F.m), c(F.AGlen), c(F.n), c(F.S), c(F.B), c(F.rho),
+            c(par)]
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+    outs = list(K) if K is not None else [None] * 4
+    outs += list(T)
+    rc = lib.uvref_element_loop(ctypes.c_int64(mua.Nele), ctypes.c_int(mua.nod), ctypes.c_int(mua.nip),
+                                *[ptr(a) for a in keep], ctypes.c_int(1 if Ronly else 0),
+                                ctypes.c_int(_COMPILED["threads"]), *[ptr(a) for a in outs])
+    if rc != 0:
+        raise RuntimeError("uvref_element_loop failed")
+
+
 def _matlab_sparse(I, J, V, m, n):
     """MATLAB ``sparse(I,J,V,m,n)``: sum duplicates, keep non-zeros only (CSC)."""
     A = sp.coo_matrix((V, (I, J)), shape=(m, n)).tocsc()
@@ -423,7 +458,13 @@ def uv_matrix_assembly(p: Params, mua: MUA, F: Fields, bcs: BCs = None, Ronly=Fa
     Tx = np.zeros((Nele, nod)); Ty = np.zeros((Nele, nod))
     Fx = np.zeros((Nele, nod)); Fy = np.zeros((Nele, nod))
 
-    for Iint in range(mua.nip):  # :168
+    if _COMPILED["lib"] is not None:  # the same element loop in C++ (oracle/ua_ref_asm.cpp)
+        par = np.array([p.kH, p.Hh0, p.SpeedZero, p.EpsZero, p.etaZero, p.Czero, p.Cmin, p.AGlenmin, Dvisk,
+                        F.rhow, g, ca, sa])
+        funs = np.array([shape_fun(nod, mua.points[i]) for i in range(mua.nip)])
+        _compiled_element_loop(mua, funs, F, ub, vb, par, Ronly, None if Ronly else (d1d1, d2d2, d1d2, d2d1),
+                               (Tx, Fx, Ty, Fy))
+    for Iint in (range(mua.nip) if _COMPILED["lib"] is None else ()):  # :168
         fun = shape_fun(nod, mua.points[Iint])
         Deriv = mua.Deriv[:, :, :, Iint]
         detJ = mua.DetJ[:, Iint]
@@ -580,6 +621,14 @@ def create_Luv(Nnodes, bcs: BCs):
 # ---------------------------------------------------------------------------
 
 
+def _splu(A):
+    """Sparse LU with UMFPACK's symmetric strategy, which MATLAB's ``decomposition`` applies to a
+    matrix of (nearly) symmetric pattern with a non-zero diagonal: a minimum-degree ordering of
+    A+A' and diagonal pivots unless an entry falls below 0.001 of its column's largest
+    (UMFPACK's default symmetric pivot tolerance)."""
+    return spla.splu(A, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.001, options=dict(SymmetricMode=True))
+
+
 def abfg_pre_eliminate(A, B, f, g):
     """ABfgPreEliminate.m:29-160 with SuperLU in place of MATLAB ``decomposition``."""
     A = sp.csc_matrix(A)
@@ -609,7 +658,7 @@ def abfg_pre_eliminate(A, B, f, g):
     # unsymmetric matrix with UMFPACK, which applies iterative refinement
     # (UMFPACK_IRSTEP, default 2 steps); SuperLU is used here with the same
     # number of refinement steps.
-    lu = spla.splu(Atilde)
+    lu = _splu(Atilde)
     x = lu.solve(btilde)
     for _ in range(2):
         x = x + lu.solve(btilde - Atilde @ x)
@@ -957,6 +1006,7 @@ class NewtonRecord:
     rForce: float
     rWork: float
     iarm: int
+    update: np.ndarray = None  # the accepted update [du; dv; (dh;) dl] (SSTREAM2dNR2.m:367-369)
 
 
 @dataclass
@@ -1061,7 +1111,7 @@ def sstream2dnr2(p: Params, mua: MUA, bcs: BCs, F: Fields, lubvb=None, solver=No
             iarm = ls.info.iarm
             bt_conv = ls.info.Converged
             cauchy += int(ls.needs_cauchy)
-        records.append(NewtonRecord(iteration, gamma, r0, r, rForce, rWork, iarm))
+        records.append(NewtonRecord(iteration, gamma, r0, r, rForce, rWork, iarm, np.concatenate([du, dv, dlu])))
         if verbose:
             print(f"NR-SSTREAM(uv):{iteration:3d}/{iarm:<2d} g={gamma:<14.7g} r/r0={r / r0:<14.7g} "
                   f"r0={r0:<14.7g} r={r:<14.7g} rForce={rForce:<14.7g} rWork={rWork:<14.7g}")
@@ -1427,7 +1477,8 @@ def sstream_transient_implicit(p: Params, mua: MUA, bcs: BCs, F: Fields, S0: Uvh
         S1.vb = S1.vb + gamma * dvb
         S1.h = S1.h + gamma * dh
         luvh = luvh + gamma * dl
-        records.append(NewtonRecord(iteration, gamma, r0, r, rForce, rWork, ls.info.iarm))
+        records.append(NewtonRecord(iteration, gamma, r0, r, rForce, rWork, ls.info.iarm,
+                                    np.concatenate([gamma * dub, gamma * dvb, gamma * dh, gamma * dl])))
         if verbose:
             print(f"NR-SSTREAM(uvh):{iteration:3d}/{ls.info.iarm:<2d} g={gamma:<14.7g} r/r0={r / r0:<14.7g} "
                   f"r0={r0:<14.7g} r={r:<14.7g} rForce={rForce:<14.7g} rWork={rWork:<14.7g}")

@@ -1381,6 +1381,64 @@ static int newton_init(ua_mesh* m, const ua_params* p, const std::vector<int>& r
   return UA_OK;
 }
 
+// Clears a report, keeping the caller-owned record and update buffers.
+static void reset_report(ua_newton_report* r) {
+  const int cap = r->iters_capacity;
+  ua_newton_iter* it = r->iters;
+  double* up = r->updates;
+  const int64_t stride = r->update_stride;
+  std::memset(r, 0, sizeof(*r));
+  r->iters_capacity = cap;
+  r->iters = it;
+  r->updates = up;
+  r->update_stride = stride;
+}
+
+// A caller-owned update buffer must hold ndof*Nnodes + nl doubles per record.
+static int check_update_stride(const ua_mesh* m, const std::vector<ua_newton_report*>& rep) {
+  const Work* w = m->work;
+  for (size_t s = 0; s < rep.size(); ++s) {
+    const ua_newton_report* r = rep[s];
+    if (!r || !r->updates) continue;
+    const int64_t need = (int64_t)(m->h_dof_off[s + 1] - m->h_dof_off[s]) +
+                         (w->h_sys_con_off[s + 1] - w->h_sys_con_off[s]);
+    if (r->update_stride < need)
+      return set_error(UA_ERR_INVALID, "update_stride %lld of system %d is below ndof*Nnodes + nl = %lld",
+                       (long long)r->update_stride, (int)s, (long long)need);
+  }
+  return UA_OK;
+}
+
+// Copies the accepted update gamma*[dX; dlam] of each system updated in this
+// iteration (sel[s]) into record n_iter_records-1 of its caller-owned buffer
+// (SSTREAM2dNR2.m:367-369).  The product by gamma is the one the update kernel
+// applies, so record and iterate agree bit for bit.
+static int record_updates(ua_mesh* m, const std::vector<ua_newton_report*>& rep, const std::vector<int>& sel,
+                          const std::vector<double>& gam) {
+  Work* w = m->work;
+  bool any = false;
+  for (size_t s = 0; s < rep.size(); ++s) {
+    ua_newton_report* r = rep[s];
+    if (!sel[s] || !r || !r->updates || r->n_iter_records <= 0 || r->n_iter_records > r->iters_capacity) continue;
+    double* dst = r->updates + (int64_t)(r->n_iter_records - 1) * r->update_stride;
+    const int d0 = m->h_dof_off[s], nd = m->h_dof_off[s + 1] - d0;
+    const int c0 = w->h_sys_con_off[s], nc = w->h_sys_con_off[s + 1] - c0;
+    UA_CUDA_TRY(cudaMemcpyAsync(dst, w->dX + d0, nd * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    if (nc) UA_CUDA_TRY(cudaMemcpyAsync(dst + nd, w->dlam + c0, nc * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    any = true;
+  }
+  if (!any) return UA_OK;
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  for (size_t s = 0; s < rep.size(); ++s) {
+    ua_newton_report* r = rep[s];
+    if (!sel[s] || !r || !r->updates || r->n_iter_records <= 0 || r->n_iter_records > r->iters_capacity) continue;
+    double* dst = r->updates + (int64_t)(r->n_iter_records - 1) * r->update_stride;
+    const int n = (m->h_dof_off[s + 1] - m->h_dof_off[s]) + (w->h_sys_con_off[s + 1] - w->h_sys_con_off[s]);
+    for (int i = 0; i < n; ++i) dst[i] = gam[s] * dst[i];
+  }
+  return UA_OK;
+}
+
 // One Newton iteration (SSTREAM2dNR2.m:157-392) of every active system.
 // *any is false when no system was active.
 static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_report*>& rep,
@@ -1545,6 +1603,7 @@ static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_rep
       k_lam_update<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_sys, w->sel, w->gamma, w->lam,
                                                                w->dlam), ++g_launches;
     UA_CUDA_TRY(cudaGetLastError());
+    if ((rc = record_updates(m, rep, sel, gam))) return rc;
   }
   return UA_OK;
 }
@@ -2485,6 +2544,7 @@ static int newton_run_uvh(ua_mesh* m, const ua_params* p, std::vector<ua_newton_
     if (w->nc)
       k_lam_update<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_sys, w->sel, w->gamma, w->lam, w->dlam), ++g_launches;
     UA_CUDA_TRY(cudaGetLastError());
+    if ((rc = record_updates(m, rep, sel, gam))) return rc;
   }
   for (int s = 0; s < nsys; ++s) {
     if (!rep[s]) continue;
@@ -2614,7 +2674,8 @@ static int newton_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_
                                   cudaMemcpyHostToDevice, m->stream));
   }
   for (auto r : rep)
-    if (r) { int cap = r->iters_capacity; ua_newton_iter* it = r->iters; std::memset(r, 0, sizeof(*r)); r->iters_capacity = cap; r->iters = it; }
+    if (r) reset_report(r);
+  if ((rc = check_update_stride(m, rep))) return rc;
   std::vector<SysState> st(nsys);
   std::vector<int> run(nsys, 1);
   if ((rc = newton_run(m, p, run, rep, st))) return rc;
@@ -3163,7 +3224,8 @@ static int uvh_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs
   if (luvh && nsys == 1 && nl == w->nc && nl > 0)
     UA_CUDA_TRY(cudaMemcpyAsync(w->lam, luvh, nl * sizeof(double), cudaMemcpyHostToDevice, m->stream));
   for (auto r : rep)
-    if (r) { int cap = r->iters_capacity; ua_newton_iter* it = r->iters; std::memset(r, 0, sizeof(*r)); r->iters_capacity = cap; r->iters = it; }
+    if (r) reset_report(r);
+  if ((rc = check_update_stride(m, rep))) return rc;
   std::vector<UvhSys> st(nsys);
   if ((rc = newton_run_uvh(m, p, rep, st))) return rc;
   for (int s = 0; s < nsys; ++s) {
@@ -3357,9 +3419,13 @@ extern "C" int ua_serve_result(ua_mesh* m, int32_t sys, double* ub, double* vb, 
   if (rep) {
     ua_newton_iter* it = rep->iters;
     int cap = rep->iters_capacity;
+    double* up = rep->updates;
+    const int64_t stride = rep->update_stride;
     *rep = w->serve->rep[sys];
     rep->iters = it;
     rep->iters_capacity = cap;
+    rep->updates = up;  // served solves keep no update records
+    rep->update_stride = stride;
     if (it) {
       int n = std::min(cap, w->serve->rep[sys].n_iter_records);
       for (int k = 0; k < n; ++k) it[k] = w->serve->recs[sys][k];

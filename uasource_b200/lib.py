@@ -116,7 +116,8 @@ class ua_newton_report(C.Structure):
                 ("kwork_nnz", C.c_double * 5), ("kwork_rows", C.c_double * 5),
                 ("gpu_launches", C.c_int32),
                 ("n_iter_records", C.c_int32), ("iters_capacity", C.c_int32),
-                ("iters", C.POINTER(ua_newton_iter))]
+                ("iters", C.POINTER(ua_newton_iter)),
+                ("updates", C.POINTER(C.c_double)), ("update_stride", C.c_int64)]
 
 
 # symbol -> (restype, argtypes); every function declared in include/ua_ssa.h

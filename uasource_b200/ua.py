@@ -376,9 +376,18 @@ class RunInfo:
     kernels: dict
     gpu_launches: int
     iters: list
+    updates: np.ndarray = None  # per iteration gamma*[du; dv; (dh;) dl] when requested
 
 
-def _report(rep, recs):
+def _updates_buffer(rep, cap, stride):
+    """Caller-owned buffer for the per-iteration Newton updates (SSTREAM2dNR2.m:367-369)."""
+    buf = np.full((cap, stride), np.nan)
+    rep.updates = buf.ctypes.data_as(C.POINTER(C.c_double))
+    rep.update_stride = stride
+    return buf
+
+
+def _report(rep, recs, updates=None):
     its = []
     for k in range(rep.n_iter_records):
         it = recs[k]
@@ -391,15 +400,17 @@ def _report(rep, recs):
                 work_rows=dict(zip(("asmK", "asmR", "spmv", "amgR", "amgP"), list(rep.kwork_rows))))
     return RunInfo(bool(rep.converged), rep.iterations, rep.backtrack_steps, rep.krylov_its_total,
                    rep.cauchy_fallbacks, bool(rep.retried), rep.r, rep.rForce, rep.rWork, rep.assembly_ms,
-                   rep.solve_ms, rep.total_ms, rep.device_ms, kern, rep.gpu_launches, its)
+                   rep.solve_ms, rep.total_ms, rep.device_ms, kern, rep.gpu_launches, its,
+                   None if updates is None else updates[:rep.n_iter_records].copy())
 
 
-def uv(ctrl: CtrlVar, mua: MUA, bcs: BCs, F: Fields, l=None, return_K=False):
+def uv(ctrl: CtrlVar, mua: MUA, bcs: BCs, F: Fields, l=None, return_K=False, return_updates=False):
     """uv.m:6 -> SSTREAM2dNR2.m:3-431 on the GPU (one mesh).
 
     Returns ``(F, l, Kuv, Ruv, RunInfo)``: F with the solved ub, vb, the
     Lagrange multipliers l.ubvb, and (if ``return_K``) the last tangent and
-    residual.
+    residual.  With ``return_updates`` RunInfo.updates holds, per Newton
+    iteration, the accepted update ``gamma*[du; dv; dl]`` (SSTREAM2dNR2.m:367-369).
     """
     lib = L.load()
     keep = _Keep()
@@ -414,6 +425,7 @@ def uv(ctrl: CtrlVar, mua: MUA, bcs: BCs, F: Fields, l=None, return_K=False):
     recs = (L.ua_newton_iter * ((ctrl.NRitmax + 2) * 2))()
     rep.iters = C.cast(recs, C.POINTER(L.ua_newton_iter))
     rep.iters_capacity = (ctrl.NRitmax + 2) * 2
+    upd = _updates_buffer(rep, rep.iters_capacity, 2 * Nn + nc.value) if return_updates else None
     Kv = np.zeros(mua.pattern()[1].size) if return_K else None
     Rv = np.zeros(2 * Nn) if return_K else None
     rc = lib.ua_uv_newton(mua.handle, C.byref(p), C.byref(cf), C.byref(cb), L.dptr(lam), len(lam), C.byref(rep),
@@ -422,7 +434,7 @@ def uv(ctrl: CtrlVar, mua: MUA, bcs: BCs, F: Fields, l=None, return_K=False):
     Fo = Fields(**{f.name: getattr(F, f.name) for f in dc_fields(F)})
     Fo.ub, Fo.vb = ub, vb
     K = _csr(mua, 0, Kv, False) if return_K else None
-    return Fo, lam, K, Rv, _report(rep, recs)
+    return Fo, lam, K, Rv, _report(rep, recs, upd)
 
 
 def uv_batch(ctrl: CtrlVar, mua: MUA, Fs, bcss):
@@ -531,12 +543,14 @@ class HBCs(BCs):
     hFixedValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
 
 
-def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None):
+def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None, return_updates=False):
     """uvh.m:5 -> uvh2D.m:20 -> SSTREAM_TransientImplicit.m:6-717 on the GPU.
 
     F0: state at t (h, ub, vb, as_, ab); F1: start values at t+dt and the
     time-independent fields.  Returns ``(F1, luvh, RunInfo)`` with F1.ub,
-    F1.vb, F1.h solved.
+    F1.vb, F1.h solved.  With ``return_updates`` RunInfo.updates holds the
+    per-iteration updates ``gamma*[du; dv; dh; dl]``
+    (SSTREAM_TransientImplicit.m:478-483).
     """
     lib = L.load()
     keep = _Keep()
@@ -555,11 +569,12 @@ def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None):
     recs = (L.ua_newton_iter * cap)()
     rep.iters = C.cast(recs, C.POINTER(L.ua_newton_iter))
     rep.iters_capacity = cap
+    upd = _updates_buffer(rep, cap, 3 * Nn + nc.value) if return_updates else None
     rc = lib.ua_uvh_newton(mua.handle, C.byref(p), C.byref(cf), C.byref(cb), L.dptr(lam), len(lam), C.byref(rep))
     L.check(rc, allow=(L.UA_ERR_NOT_CONVERGED,))
     Fo = F1.copy()
     Fo.ub, Fo.vb, Fo.h = ub, vb, h1
-    return Fo, lam, _report(rep, recs)
+    return Fo, lam, _report(rep, recs, upd)
 
 
 def solveKApeSymmetric(A, B, f, g, rtol=1e-12, maxit=0, device=0):
