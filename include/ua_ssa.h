@@ -56,6 +56,15 @@ extern "C" {
 #define UA_KRYLOV_GMRES    0   /* restarted GMRES(m), right-preconditioned (default) */
 #define UA_KRYLOV_BICGSTAB 1   /* BiCGStab with restarts on breakdown */
 
+/* CtrlVar.SlidingLaw (Ua2D_DefaultParameters.m:171-172, BasalDrag.m:184-272). */
+#define UA_SLIDING_WEERTMAN 0   /* "Weertman", "W" (default) */
+#define UA_SLIDING_BUDD     1   /* "Budd", "W-N0": uses F.q */
+#define UA_SLIDING_TSAI     2   /* "Tsai", "minCW-N0": uses F.muk */
+#define UA_SLIDING_COULOMB  3   /* "Coulomb", "C": uses F.muk */
+#define UA_SLIDING_CORNFORD 4   /* "Cornford", "rpCW-N0": uses F.muk */
+#define UA_SLIDING_UMBI     5   /* "Umbi", "rCW-N0": uses F.muk */
+#define UA_SLIDING_JOUGHIN  6   /* "Joughin", "rCW-V0": uses F.V0 */
+
 /* Assembly modes of uvMatrixAssembly (uvMatrixAssemblySSTREAM.m:17-28). */
 #define UA_ASM_R      0   /* CtrlVar.uvMatrixAssembly.Ronly=true */
 #define UA_ASM_RK     1   /* R and K */
@@ -142,6 +151,10 @@ typedef struct ua_params {
     int32_t krylov_sell;       /* 1 = the AMG-preconditioned uv PCG runs its SpMV and the V-cycle's
                                   finest-level passes on node-sliced (sliced ELL) copies of the tangent,
                                   both rows of a node per thread (default); 0 = CSR row kernels */
+    int32_t SlidingLaw;        /* UA_SLIDING_* (:171) */
+    double Nzero;              /* lower value of the effective pressure (:445) */
+    int32_t IncludeMelangeModelPhysics;  /* ocean and atmosphere drag on floating ice (BasalDrag.m:275-343);
+                                            needs F.uo, vo, Co, mo, ua, va, Ca, ma */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */
@@ -154,6 +167,11 @@ typedef struct ua_fields {
     const double *h0, *u0, *v0, *as0, *ab0, *as1, *ab1, *dadh;
     double *h1;                /* in: start thickness, out: solution */
     double dt;
+    /* sliding-law fields (UaFields.m; NULL where the law does not use them): Budd exponent q,
+       Coulomb friction coefficient muk, Joughin speed V0 */
+    const double *q, *muk, *V0;
+    /* melange: ocean velocity, drag and exponent; atmosphere the same (IncludeMelangeModelPhysics) */
+    const double *uo, *vo, *Co, *mo, *ua, *va, *Ca, *ma;
 } ua_fields;
 
 /* Boundary conditions (BCs2MLC.m, CreateLuv.m).  Index base as the mesh. */

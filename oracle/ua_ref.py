@@ -260,6 +260,9 @@ class Params:
     ModifiedNRuvhIntervalCriterion: int = 1        # :584
     ModifiedNRuvhReductionCriterion: float = 0.5   # :585
     NLtol: float = 1e-15             # BackTracking.m:125-127 default
+    SlidingLaw: str = "Weertman"     # :171
+    Nzero: float = 1e-20             # :445
+    IncludeMelangeModelPhysics: bool = False
 
     def set_force_tolerance(self, tol):
         """Set every force tolerance (desired and acceptable) to ``tol``."""
@@ -293,6 +296,19 @@ class Fields:
     ab: np.ndarray = None
     dasdh: np.ndarray = None
     dabdh: np.ndarray = None
+    # other sliding laws (BasalDrag.m): Budd exponent q, Coulomb friction muk, Joughin V0
+    q: np.ndarray = None
+    muk: np.ndarray = None
+    V0: np.ndarray = None
+    # melange / ocean and atmosphere drag (CtrlVar.IncludeMelangeModelPhysics)
+    uo: np.ndarray = None
+    vo: np.ndarray = None
+    Co: np.ndarray = None
+    mo: np.ndarray = None
+    ua: np.ndarray = None
+    va: np.ndarray = None
+    Ca: np.ndarray = None
+    ma: np.ndarray = None
 
     def copy(self):
         out = Fields(**{k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items()})
@@ -347,6 +363,151 @@ def effective_viscosity(p: Params, A, n, exx, eyy, exy):
     eta = 0.5 * A ** (-1.0 / n) * e ** ((1 - n) / n) + p.etaZero
     E = (1 - n) / (4 * n) * A ** (-1.0 / n) * e ** ((1 - 3 * n) / n)
     return eta, E
+
+
+def effective_pressure_n0(p, h, H, rho, rhow, g):
+    """N0 inside BasalDrag.m (zeroth-order hydrology): N = rho g max(h-hf, 0) + Nzero,
+    dN/dh = rho g where h > hf (else 0)."""
+    hf = rhow * H / rho
+    hf = np.where(hf < EPS, 0.0, hf)
+    Dh = h - hf
+    I = Dh < EPS
+    Dh = np.where(I, 0.0, Dh)
+    N = rho * g * Dh + p.Nzero
+    dNdh = np.where(I, 0.0, rho * g + 0 * Dh)
+    return N, dNdh
+
+
+def _isotropic(T_over_U, Bcoef, ub, vb):
+    """Drag of an isotropic law |tau| = T(U), tau = T(U) (u, v)/U with U = sqrt(u^2+v^2+u0^2):
+    tau_x = A u, d tau_x/du = A + B u^2, d tau_x/dv = B u v, d tau_y/dv = A + B v^2, where
+    A = T/U and B = (T' - T/U)/U^2."""
+    A, B = T_over_U, Bcoef
+    return A * ub, A * vb, A + B * ub * ub, B * ub * vb, B * ub * vb, A + B * vb * vb
+
+
+def basal_drag(p: Params, He, delta, h, H, rho, rhow, g, ub, vb, C, m, q=None, muk=None, V0=None, melange=None):
+    """BasalDrag.m:44-363 for CtrlVar.SlidingLaw (p.SlidingLaw) and the melange terms.
+
+    Weertman/W (:184-186, Weertman :410-446), Budd/W-N0 (:188-191, Budd :448-490), Coulomb/C
+    (:193-205, Coulomb :365-408), Tsai/minCW-N0 (:207-244: the smaller of the Weertman and
+    Coulomb stresses), Cornford/rpCW-N0 (:246-252, rpCWN0.m), Umbi/rCW-N0 (:254-263, rCWN0.m),
+    Joughin/rCW-V0 (:265-272, rCWV0.m).  The velocity derivatives of the last three follow from
+    their stresses |tau| = mu N W/((mu N)^m + W^m)^(1/m), mu N W/(mu N + W) and
+    W (U+V0)^(-1/m) with W = He (C+C0)^(-1/m) U^(1/m); their thickness derivatives are the
+    reference's expressions.  ``melange`` = (uo, vo, Co, mo, ua, va, Ca, ma) adds the ocean and
+    atmosphere drag on the floating part (:275-343).
+    Returns taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, dtauxdh, dtauydh.
+    """
+    law = p.SlidingLaw
+    delta = np.where(delta < 0, 0.0, delta)  # :48-49
+    He = np.where(He < 0, 0.0, He)
+    C0, u0 = p.Czero, p.SpeedZero
+    speed = np.sqrt(ub * ub + vb * vb + u0 ** 2)  # :71-77
+    Um = speed ** (1.0 / m - 1)
+    beta2 = (C + C0) ** (-1.0 / m) * Um
+    Dbeta2 = (1.0 / m - 1) * (C + C0) ** (-1.0 / m) * (ub ** 2 + vb ** 2 + u0 ** 2) ** ((1 - 3 * m) / (2 * m))
+    zero = 0 * ub
+
+    def weertman():
+        return (He * beta2 * ub, He * beta2 * vb, He * (beta2 + Dbeta2 * ub * ub), He * Dbeta2 * ub * vb,
+                He * Dbeta2 * ub * vb, He * (beta2 + Dbeta2 * vb * vb), delta * beta2 * ub, delta * beta2 * vb)
+
+    def coulomb(N, dNdh, Dh):  # Coulomb :365-408
+        Tau = muk * N
+        tx, ty = Tau * ub / speed, Tau * vb / speed
+        temp = speed ** 3
+        dxu = Tau * (1 / speed - ub ** 2 / temp)
+        dyv = Tau * (1 / speed - vb ** 2 / temp)
+        dxv = -Tau * ub * vb / temp
+        E = np.where(Dh < EPS, 0.0, muk * dNdh / speed)
+        return tx, ty, dxu, dxv, dxv, dyv, E * ub, E * vb
+
+    if law in ("Weertman", "W"):
+        out = weertman()
+    elif law in ("Budd", "W-N0"):  # Budd :448-490
+        N, dNdh = effective_pressure_n0(p, h, H, rho, rhow, g)
+        qm = q / m
+        Nqm = N ** qm
+        T = He * Nqm * beta2
+        E = delta * T + He * qm * N ** (qm - 1) * dNdh * beta2
+        out = (T * ub, T * vb, He * Nqm * (beta2 + Dbeta2 * ub * ub), He * Nqm * Dbeta2 * ub * vb,
+               He * Nqm * Dbeta2 * ub * vb, He * Nqm * (beta2 + Dbeta2 * vb * vb), E * ub, E * vb)
+    elif law in ("Coulomb", "C"):
+        N, dNdh = effective_pressure_n0(p, h, H, rho, rhow, g)
+        hf = rhow * H / rho
+        hf = np.where(hf < EPS, 0.0, hf)
+        Dh = h - hf
+        Dh = np.where(Dh < EPS, 0.0, Dh)
+        out = coulomb(N, dNdh, Dh)
+    elif law in ("Tsai", "minCW-N0"):
+        hf = rhow * H / rho
+        hf = np.where(hf < EPS, 0.0, hf)
+        Dh = h - hf
+        Dh = np.where(Dh < EPS, 0.0, Dh)
+        N, dNdh = effective_pressure_n0(p, h, H, rho, rhow, g)
+        W = weertman()
+        Cc = coulomb(N, dNdh, Dh)
+        isC = Cc[0] * Cc[0] + Cc[1] * Cc[1] < W[0] * W[0] + W[1] * W[1]
+        out = tuple(np.where(isC, c, w) for w, c in zip(W, Cc))
+        out = out[:4] + (out[3],) + out[5:]  # dtauydu = dtauxdv
+    elif law in ("Cornford", "rpCW-N0"):
+        N, dNdh = effective_pressure_n0(p, h, H, rho, rhow, g)
+        c = (C + C0) ** (-1.0 / m)
+        W = He * c * speed ** (1.0 / m)
+        muN = muk * N
+        S = muN ** m + W ** m
+        T_U = muN * He * c * speed ** (1.0 / m - 1) * S ** (-1.0 / m)
+        Tp = muN * (W / (m * speed)) * muN ** m * S ** (-1.0 / m - 1)
+        out = _isotropic(T_U, (Tp - T_U) / speed ** 2, ub, vb)
+        Wm = (c * speed ** (1.0 / m)) ** m
+        Eh = (2.0 ** (m + 1) * muN ** (m + 1) * delta * c * speed ** (1.0 / m - 1)
+              * (2.0 ** m * muN ** m + Wm) ** (-(m + 1) / m)
+              + muk * dNdh * He ** (m + 1) * c * speed ** (1.0 / m - 1) * Wm * S ** (-(m + 1) / m))
+        out = out + (Eh * ub, Eh * vb)
+    elif law in ("Umbi", "rCW-N0"):
+        N, dNdh = effective_pressure_n0(p, h, H, rho, rhow, g)
+        c1 = (C + C0) ** (1.0 / m)
+        muN = muk * N
+        den = muN * c1 + He * speed ** (1.0 / m)
+        T_U = muN * He * speed ** (1.0 / m - 1) / den
+        W = He * speed ** (1.0 / m) / c1
+        Tp = muN ** 2 * W / (m * speed * (muN + W) ** 2)
+        out = _isotropic(T_U, (Tp - T_U) / speed ** 2, ub, vb)
+        Eh = (muk * dNdh * He * speed ** (2.0 / m - 1) / den ** 2
+              + 4.0 * muk ** 2 * N ** 2 * delta * c1 * speed ** (1.0 / m - 1) / (2 * muN * c1 + speed ** (1.0 / m)) ** 2)
+        out = out + (Eh * ub, Eh * vb)
+    elif law in ("Joughin", "rCW-V0"):
+        c = (C + C0) ** (-1.0 / m)
+        T_U = He * c * (V0 + speed) ** (-1.0 / m) * speed ** (1.0 / m - 1)
+        Tp = T_U * speed * V0 / (m * speed * (speed + V0))
+        out = _isotropic(T_U, (Tp - T_U) / speed ** 2, ub, vb)
+        Eh = delta * c * (V0 + speed) ** (-1.0 / m) * speed ** (1.0 / m - 1)
+        out = out + (Eh * ub, Eh * vb)
+    else:
+        raise ValueError("BasalDrag:CaseNotFound")
+    out = [o + zero for o in out]
+    if melange is not None:  # :275-343
+        uo, vo, Co, mo, ua_, va_, Ca, ma = melange
+        for (uw, vw, Cw, mw) in ((uo, vo, Co, mo), (ua_, va_, Ca, ma)):
+            U, V = ub - uw, vb - vw
+            b2 = (Cw + C0) ** (-1.0 / mw) * np.sqrt(U * U + V * V + u0 ** 2) ** (1.0 / mw - 1)
+            Db2 = (1.0 / mw - 1) * (Cw + C0) ** (-1.0 / mw) * (U ** 2 + V ** 2 + u0 ** 2) ** ((1 - 3 * mw) / (2 * mw))
+            add = ((1 - He) * b2 * U, (1 - He) * b2 * V, (1 - He) * (b2 + Db2 * U * U), (1 - He) * (Db2 * U * V),
+                   (1 - He) * (Db2 * U * V), (1 - He) * (b2 + Db2 * V * V), -delta * b2 * U, -delta * b2 * V)
+            out = [a + b for a, b in zip(out, add)]
+    return tuple(out)
+
+
+def _drag_extras(p: Params, F: Fields, conn, fun):
+    """Integration-point values of the sliding-law fields (uvMatrixAssemblySSTREAM.m:210-254):
+    q, muk and V0 where the law uses them, and the melange fields when
+    CtrlVar.IncludeMelangeModelPhysics is on."""
+    at = lambda v: None if v is None else np.asarray(v, dtype=float)[conn] @ fun
+    out = {"q": at(F.q), "muk": at(F.muk), "V0": at(F.V0)}
+    if p.IncludeMelangeModelPhysics:
+        out["melange"] = tuple(at(getattr(F, k)) for k in ("uo", "vo", "Co", "mo", "ua", "va", "Ca", "ma"))
+    return out
 
 
 def basal_drag_weertman(p: Params, He, delta, ub, vb, C, m):
@@ -458,13 +619,15 @@ def uv_matrix_assembly(p: Params, mua: MUA, F: Fields, bcs: BCs = None, Ronly=Fa
     Tx = np.zeros((Nele, nod)); Ty = np.zeros((Nele, nod))
     Fx = np.zeros((Nele, nod)); Fy = np.zeros((Nele, nod))
 
-    if _COMPILED["lib"] is not None:  # the same element loop in C++ (oracle/ua_ref_asm.cpp)
+    compiled = (_COMPILED["lib"] is not None and p.SlidingLaw in ("Weertman", "W")
+                and not p.IncludeMelangeModelPhysics)
+    if compiled:  # the same element loop in C++ (oracle/ua_ref_asm.cpp), Weertman drag
         par = np.array([p.kH, p.Hh0, p.SpeedZero, p.EpsZero, p.etaZero, p.Czero, p.Cmin, p.AGlenmin, Dvisk,
                         F.rhow, g, ca, sa])
         funs = np.array([shape_fun(nod, mua.points[i]) for i in range(mua.nip)])
         _compiled_element_loop(mua, funs, F, ub, vb, par, Ronly, None if Ronly else (d1d1, d2d2, d1d2, d2d1),
                                (Tx, Fx, Ty, Fy))
-    for Iint in (range(mua.nip) if _COMPILED["lib"] is None else ()):  # :168
+    for Iint in (range(mua.nip) if not compiled else ()):  # :168
         fun = shape_fun(nod, mua.points[Iint])
         Deriv = mua.Deriv[:, :, :, Iint]
         detJ = mua.DetJ[:, Iint]
@@ -497,8 +660,9 @@ def uv_matrix_assembly(p: Params, mua: MUA, F: Fields, bcs: BCs = None, Ronly=Fa
             exx = exx + Deriv[:, 0, Inod] * ubnod[:, Inod]
             eyy = eyy + Deriv[:, 1, Inod] * vbnod[:, Inod]
             exy = exy + 0.5 * (Deriv[:, 0, Inod] * vbnod[:, Inod] + Deriv[:, 1, Inod] * ubnod[:, Inod])
-        taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, _, _ = basal_drag_weertman(
-            p, Heint, deltaint, uint, vint, Cint, mint)  # :351-352
+        taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, _, _ = basal_drag(
+            p, Heint, deltaint, hint, Hint, rhoint, F.rhow, g, uint, vint, Cint, mint,
+            **_drag_extras(p, F, conn, fun))  # :351-352
         etaint, Eint = effective_viscosity(p, AGlenint, nint, exx, eyy, exy)  # :353
         dbdx = dsdx - dhdx; dbdy = dsdy - dhdy  # :357
         detJw = detJ * mua.weights[Iint]  # :359
@@ -1256,8 +1420,9 @@ def uvh_matrix_assembly(p: Params, mua: MUA, F: Fields, S0: UvhState, S1: UvhSta
             exx = exx + Dx * unod[:, Inod]; eyy = eyy + Dy * vnod[:, Inod]
             exy = exy + 0.5 * (Dx * vnod[:, Inod] + Dy * unod[:, Inod])
         etaint, Eint = effective_viscosity(p, AGlenint, nint, exx, eyy, exy)  # :149
-        taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, dtauxdh, dtauydh = basal_drag_weertman(
-            p, Heint, deltaint, uint, vint, Cint, mint)  # :150-151
+        taux, tauy, dtauxdu, dtauxdv, dtauydu, dtauydv, dtauxdh, dtauydh = basal_drag(
+            p, Heint, deltaint, hint, Hint, rhoint, rhow, g, uint, vint, Cint, mint,
+            **_drag_extras(p, F, conn, fun))  # :150-151
         l = np.sqrt(2 * areas)  # :156
         speed0 = np.sqrt(u0int * u0int + v0int * v0int + p.SpeedZero ** 2)  # :157
         tau0 = p.SUPG_beta0 * supg_tau(p, speed0, l, dt)  # :158-159

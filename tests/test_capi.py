@@ -44,6 +44,8 @@ def test_params_default_matches_reference_defaults():
         a, b = getattr(p, name), getattr(cv, name)
         if isinstance(b, tuple):
             assert tuple(a) == b, name
+        elif name == "SlidingLaw":
+            assert a == L.SLIDING_LAWS[b], name
         else:
             assert a == b, name
 

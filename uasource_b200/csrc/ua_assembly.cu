@@ -49,6 +49,7 @@ __device__ __forceinline__ void uv_deriv(const QuadTable& Q, int ip, const doubl
 // parts (accumulated into the outputs).
 template <int NOD, bool WITHK, typename KT>
 __device__ __forceinline__ void uv_ip(const QuadTable& Q, const UvPhys& P, const SysScal& S, int ip,
+                                      const int (&gn)[NOD], const DragFields& DF,
                                       const double (&Dx)[NOD], const double (&Dy)[NOD], double detJ,
                                       const double (&hn)[NOD], const double (&sn)[NOD], const double (&un)[NOD],
                                       const double (&vn)[NOD], const double (&Cn)[NOD], const double (&mn)[NOD],
@@ -92,7 +93,10 @@ __device__ __forceinline__ void uv_ip(const QuadTable& Q, const UvPhys& P, const
       exx += Dx[a] * un[a]; eyy += Dy[a] * vn[a];
       exy += 0.5 * (Dx[a] * vn[a] + Dy[a] * un[a]);
     }
-    const Drag d = basal_drag_weertman(P, Heint, deltaint, uint, vint, Cint, mint, cube);
+    const Drag d = (P.law == UA_SLIDING_WEERTMAN && !P.melange)
+                       ? basal_drag_weertman(P, Heint, deltaint, uint, vint, Cint, mint, cube)
+                       : basal_drag_general(P, Heint, deltaint, hint, Hint, rhoint, rhow, g, uint, vint, Cint, mint,
+                                            drag_interp<NOD>(DF, gn, N));
     double eta, E;
     effective_viscosity(P, Aint, nint, exx, eyy, exy, eta, E, cube);
     const double dbdx = dsdx - dhdx, dbdy = dsdy - dhdy;
@@ -204,6 +208,7 @@ __device__ __forceinline__ void uv_zero(KT* Kuu, KT* Kvv, KT* Kuv, double* Tx, d
 // (K+K.')/2 at :530-531 yields.
 template <int NOD, bool WITHK, typename KT>
 __device__ __forceinline__ void uv_element(const QuadTable& Q, const UvPhys& P, const SysScal& S,
+                                           const int (&gn)[NOD], const DragFields& DF,
                                            const double (&xe)[NOD], const double (&ye)[NOD],
                                            const double (&hn)[NOD], const double (&sn)[NOD],
                                            const double (&un)[NOD], const double (&vn)[NOD],
@@ -218,120 +223,20 @@ __device__ __forceinline__ void uv_element(const QuadTable& Q, const UvPhys& P, 
 #pragma unroll 1
   for (int ip = 0; ip < Q.nip; ++ip) {
     if (NOD != 3) uv_deriv<NOD>(Q, ip, xe, ye, Dx, Dy, detJ);
-    uv_ip<NOD, WITHK, KT>(Q, P, S, ip, Dx, Dy, detJ, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv, Kuv, Tx,
-                          Fx, Ty, Fy);
+    uv_ip<NOD, WITHK, KT>(Q, P, S, ip, gn, DF, Dx, Dy, detJ, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv,
+                          Kuv, Tx, Fx, Ty, Fy);
   }
 }
 
-// P1 runs integration-point-parallel (at most 128 registers: two 256-thread or four
-// 128-thread blocks per SM); P2 keeps one element per thread in 128-thread blocks.
+// Phase 2 of the patch kernels: one thread per node-level non-zero of the
+// patch's rows sums the element contributions listed for it (increasing global
+// element order) and writes the four dof-level values; the same for the
+// residual on the diagonal entries.  No atomics: every matrix entry is produced
+// by exactly one thread, in a fixed order, whatever the patch partition.
 template <int NOD, bool WITHK, typename KT>
-__global__ void __launch_bounds__(NOD == 3 ? 256 : 128, NOD == 3 ? 2 : 1) uv_patch_kernel(DevMesh M, QuadTable Q, UvPhys P, UvIn in, UvOut out) {
+__device__ __forceinline__ void patch_scatter(const DevMesh& M, const UvOut& out, int p, int s, int uoff, int voff,
+                                              const KT* sK, const double* sR, int E) {
   using I = ElemIdx<NOD>;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int p = blockIdx.x;
-  const int s = M.patch_sys[p];
-  if (in.active && !in.active[s]) return;
-  const int E = M.max_patch_elems;
-  KT* sK = reinterpret_cast<KT*>(smem);
-  size_t koff = WITHK ? (((size_t)I::NKE * E * sizeof(KT) + 15) & ~(size_t)15) : 0;
-  double* sR = reinterpret_cast<double*>(smem + koff);
-  const int e0 = M.patch_elem_ptr[p], ne = M.patch_elem_ptr[p + 1] - e0;
-  const int uoff = M.sys_dof_off[s] - M.sys_node_off[s];
-  const int nn_s = M.sys_node_off[s + 1] - M.sys_node_off[s];
-  const int voff = uoff + nn_s;
-  const double gam = in.gamma ? in.gamma[s] : 0.0;
-  const SysScal S = in.scal[s];
-  // nodal values of element e (u, v at X + gamma dX)
-  auto gather = [&](int e, double (&xe)[NOD], double (&ye)[NOD], double (&hn)[NOD], double (&sn)[NOD],
-                    double (&un)[NOD], double (&vn)[NOD], double (&Cn)[NOD], double (&mn)[NOD], double (&An)[NOD],
-                    double (&nn)[NOD], double (&Sn)[NOD], double (&Bn)[NOD], double (&rn)[NOD]) {
-#pragma unroll
-    for (int a = 0; a < NOD; ++a) {
-      const int gnode = __ldg(M.conn + (size_t)a * M.ne + e);
-      xe[a] = __ldg(M.x + gnode); ye[a] = __ldg(M.y + gnode);
-      hn[a] = __ldg(in.h + gnode); sn[a] = __ldg(in.s + gnode);
-      double u = __ldg(in.X + uoff + gnode), v = __ldg(in.X + voff + gnode);
-      if (in.dX) { u += gam * __ldg(in.dX + uoff + gnode); v += gam * __ldg(in.dX + voff + gnode); }
-      un[a] = u; vn[a] = v;
-      Cn[a] = __ldg(in.C + gnode); mn[a] = __ldg(in.m + gnode);
-      An[a] = __ldg(in.A + gnode); nn[a] = __ldg(in.n + gnode);
-      Sn[a] = __ldg(in.S + gnode); Bn[a] = __ldg(in.B + gnode);
-      rn[a] = __ldg(in.rho + gnode);
-    }
-  };
-  auto store = [&](int t, const KT* Kuu, const KT* Kvv, const KT* Kuv, const double* Tx, const double* Fx,
-                   const double* Ty, const double* Fy) {
-    if (WITHK) {
-#pragma unroll
-      for (int i = 0; i < I::NS; ++i) { sK[i * E + t] = Kuu[i]; sK[(I::NS + i) * E + t] = Kvv[i]; }
-#pragma unroll
-      for (int i = 0; i < NOD * NOD; ++i) sK[(2 * I::NS + i) * E + t] = Kuv[i];
-    }
-#pragma unroll
-    for (int a = 0; a < NOD; ++a) {
-      sR[(0 * NOD + a) * E + t] = Tx[a];
-      sR[(1 * NOD + a) * E + t] = Fx[a];
-      sR[(2 * NOD + a) * E + t] = Ty[a];
-      sR[(3 * NOD + a) * E + t] = Fy[a];
-    }
-  };
-  if constexpr (NOD == 3) {
-    // P1: the integration points of an element on the lanes of a group (one each), summed in
-    // a fixed order; no loop-carried element state, so far fewer registers per thread than an
-    // element-per-thread loop.  The 6-point (degree-4) rule runs in 6-lane groups, five per
-    // warp (lanes 30 and 31 idle: ip >= 6), so 30 of 32 lanes compute (the launch checks
-    // nip <= 6).
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int ip = lane < 30 ? lane % 6 : 6 + lane - 30;
-    const int grp = wid * 5 + min(lane / 6, 4);
-    const int ngrp = (int)(blockDim.x >> 5) * 5;
-    // fixed-order sum of a 6-lane group at its lane 0: ((v0 + v3) + (v1 + v4)) + (v2 + v5)
-    auto sum6 = [](auto v) {
-      v += __shfl_down_sync(0xffffffffu, v, 3);
-      const auto a = __shfl_down_sync(0xffffffffu, v, 1);
-      const auto b = __shfl_down_sync(0xffffffffu, v, 2);
-      return (v + a) + b;
-    };
-    for (int base = 0; base < ne; base += ngrp) {  // same trip count for every thread of the block
-      const int t = base + grp;
-      KT Kuu[I::NS], Kvv[I::NS], Kuv[NOD * NOD];
-      double Tx[NOD], Fx[NOD], Ty[NOD], Fy[NOD];
-      uv_zero<NOD, WITHK, KT>(Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
-      if (t < ne && ip < Q.nip) {
-        double xe[NOD], ye[NOD], hn[NOD], sn[NOD], un[NOD], vn[NOD], Cn[NOD], mn[NOD], An[NOD], nn[NOD], Sn[NOD],
-            Bn[NOD], rn[NOD];
-        gather(__ldg(M.patch_elems + e0 + t), xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn);
-        double Dx[NOD], Dy[NOD], detJ;
-        uv_deriv<NOD>(Q, 0, xe, ye, Dx, Dy, detJ);
-        uv_ip<NOD, WITHK, KT>(Q, P, S, ip, Dx, Dy, detJ, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv, Kuv,
-                              Tx, Fx, Ty, Fy);
-      }
-      if (WITHK) {
-#pragma unroll
-        for (int i = 0; i < I::NS; ++i) { Kuu[i] = sum6(Kuu[i]); Kvv[i] = sum6(Kvv[i]); }
-#pragma unroll
-        for (int i = 0; i < NOD * NOD; ++i) Kuv[i] = sum6(Kuv[i]);
-      }
-#pragma unroll
-      for (int a = 0; a < NOD; ++a) {
-        Tx[a] = sum6(Tx[a]); Fx[a] = sum6(Fx[a]); Ty[a] = sum6(Ty[a]); Fy[a] = sum6(Fy[a]);
-      }
-      if (t < ne && ip == 0) store(t, Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
-    }
-  } else {
-    for (int t = threadIdx.x; t < ne; t += blockDim.x) {
-      double xe[NOD], ye[NOD], hn[NOD], sn[NOD], un[NOD], vn[NOD], Cn[NOD], mn[NOD], An[NOD], nn[NOD], Sn[NOD],
-          Bn[NOD], rn[NOD];
-      gather(__ldg(M.patch_elems + e0 + t), xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn);
-      KT Kuu[I::NS], Kvv[I::NS], Kuv[NOD * NOD];
-      double Tx[NOD], Fx[NOD], Ty[NOD], Fy[NOD];
-      uv_element<NOD, WITHK, KT>(Q, P, S, xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv, Kuv, Tx, Fx,
-                                 Ty, Fy);
-      store(t, Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
-    }
-  }
-  __syncthreads();
   const int pn0 = M.patch_node_ptr[p];
   const int nr = M.patch_node_ptr[p + 1] - pn0;
   if (WITHK) {
@@ -386,15 +291,359 @@ __global__ void __launch_bounds__(NOD == 3 ? 256 : 128, NOD == 3 ? 2 : 1) uv_pat
   }
 }
 
+// ---------------------------------------------------------------------------
+// P1 tangent and residual, re-derived for linear elements.
+//
+// On a 3-node triangle the basis gradients Dx, Dy, the strain rates exx, eyy,
+// exy and the slopes dbdx, dbdy are constant over the element
+// (uvMatrixAssemblySSTREAM.m:322-347 evaluate the same values at every
+// integration point).  The integration-point loop (:362-449) therefore
+// reduces to a handful of scalars per point, and
+//   Kuu_ab = S1 (4 Dx_a Dx_b + Dy_a Dy_b) + S2 Pu_a Pu_b + sum_ip cxu N_a N_b
+//   Kvv_ab = S1 (4 Dy_a Dy_b + Dx_a Dx_b) + S2 Pv_a Pv_b + sum_ip cyv N_a N_b
+//   Kuv_ab = S1 (2 Dx_a Dy_b + Dy_a Dx_b) + S2 Pu_a Pv_b + sum_ip cxv N_a N_b
+//   Tx_a = S1 ((4exx+2eyy) Dx_a + 2exy Dy_a) + sum_ip tx N_a,  Fx_a = P Dx_a + sum_ip fx N_a
+//   Ty_a = S1 ((4eyy+2exx) Dy_a + 2exy Dx_a) + sum_ip ty N_a,  Fy_a = P Dy_a + sum_ip fy N_a
+// with S1 = sum_ip h eta detJw, S2 = sum_ip 2 Dvisk h E detJw, P = sum_ip pp detJw,
+// Pu = (2exx+eyy) Dx + exy Dy, Pv = (2eyy+exx) Dy + exy Dx, and per point
+// tx = taux detJw, ty = tauy detJw, fx = (-g rr dbdx ca + rho g h sa) detJw,
+// fy = -g rr dbdy ca detJw, pp = g ca (rho h^2 - rhow d^2)/2, rr = rho h - rhow d,
+// and the drag derivatives cxu, cyv, cxv times detJw (BasalDrag.m:414-429).
+// The terms are the reference's, regrouped; the tangent is symmetric as
+// (K+K.')/2 makes it (:530-531).
+//
+// Mapping: six lanes per element, one integration point each (five elements per
+// warp, lanes 30-31 idle).  Each lane evaluates its point's physics and writes
+// its scalars to a per-warp scratch in shared memory; S1, S2 and P are summed
+// over the six lanes in a fixed order.  The six lanes of the element then form
+// the 21 tangent entries and 12 residual parts in six uniform steps, reading
+// the point scalars (same-address broadcasts) instead of reducing 33 values
+// across lanes.  The element tangents and residual parts go to shared memory
+// for the segmented sum of phase 2.
+// ---------------------------------------------------------------------------
+namespace p1 {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+// scratch slots per lane: residual scalars first, then the drag derivatives
+enum { TX = 0, TY = 1, FX = 2, FY = 3, CXU = 4, CYV = 5, CXV = 6, NSC = 7 };
+
+__device__ __forceinline__ double sel3(double a0, double a1, double a2, int i) {
+  return i == 0 ? a0 : (i == 1 ? a1 : a2);
+}
+
+// tanh z of z = k (x - x0), the argument of HeavisideApprox.m:86, from one expm1
+// (tanh z = sign(z) (1 - e^-2|z|) / (1 + e^-2|z|)); for |z| >= 20, tanh z rounds to
+// +-1 exactly in FP64, so the saturated value is returned without the transcendental.
+__device__ __forceinline__ double tanh_step(double k, double x, double x0) {
+  const double z = k * (x - x0);
+  if (fabs(z) >= 20.0) return z > 0 ? 1.0 : -1.0;
+  const double em = expm1(-2.0 * fabs(z));
+  return copysign(-em / (2.0 + em), z);
+}
+
+}  // namespace p1
+
+// GEN: any sliding law and the melange terms (basal_drag_general); else Weertman, with the
+// reciprocal-cube-root powers when n = m = 3 at every node of the system.
+template <bool WITHK, typename KT, bool GEN>
+__global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadTable Q, UvPhys P, UvIn in,
+                                                                 UvOut out) {
+  using I = ElemIdx<3>;
+  using namespace p1;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int p = blockIdx.x;
+  const int s = M.patch_sys[p];
+  if (in.active && !in.active[s]) return;
+  const int E = M.max_patch_elems;
+  KT* sK = reinterpret_cast<KT*>(smem);
+  const size_t koff = WITHK ? (((size_t)I::NKE * E * sizeof(KT) + 15) & ~(size_t)15) : 0;
+  double* sR = reinterpret_cast<double*>(smem + koff);  // 12 E
+  double* sN = sR + 12 * E;                              // N_a(ip) at [ip*3 + a], weights at [18 + ip]
+  double* scr = sN + 24;                                 // NSC x 32 per warp
+  const int e0 = M.patch_elem_ptr[p], ne = M.patch_elem_ptr[p + 1] - e0;
+  const int uoff = M.sys_dof_off[s] - M.sys_node_off[s];
+  const int nn_s = M.sys_node_off[s + 1] - M.sys_node_off[s];
+  const int voff = uoff + nn_s;
+  const double gam = in.gamma ? in.gamma[s] : 0.0;
+  const SysScal S = in.scal[s];
+  const bool cube = S.cube != 0.0;
+  if (threadIdx.x < 18) sN[threadIdx.x] = Q.fun[threadIdx.x / 3][threadIdx.x % 3];
+  else if (threadIdx.x < 24) sN[threadIdx.x] = Q.w[threadIdx.x - 18];
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int j = lane < 30 ? lane % 6 : lane - 30;  // integration point of this lane, and its output slot
+  const int grp = lane < 30 ? lane / 6 : 4;
+  const int g0 = grp * 6;                          // first lane of the element's group
+  double* ws = scr + wid * (NSC * 32);
+  const double N0 = sN[j * 3 + 0], N1 = sN[j * 3 + 1], N2 = sN[j * 3 + 2], wj = sN[18 + j];
+  const double rhow = S.rhow, g = S.g, ca = S.ca, sa = S.sa;
+  const int ngrp = kWarps * 5;
+
+  for (int base = 0; base < ne; base += ngrp) {  // same trip count for every thread of the block
+    const int t = base + wid * 5 + grp;
+    const bool valid = lane < 30 && t < ne;
+    const int e = __ldg(M.patch_elems + e0 + min(t, ne - 1));
+    const int n0 = __ldg(M.conn + e), n1 = __ldg(M.conn + (size_t)M.ne + e), n2 = __ldg(M.conn + 2 * (size_t)M.ne + e);
+    // element geometry (derivVector.m:96-109 with the constant P1 derivatives of the
+    // basis [xi, 1-xi-eta, eta]); one reciprocal of detJ
+    const double x0 = __ldg(M.x + n0), x1 = __ldg(M.x + n1), x2 = __ldg(M.x + n2);
+    const double y0 = __ldg(M.y + n0), y1 = __ldg(M.y + n1), y2 = __ldg(M.y + n2);
+    const double J11 = x0 - x1, J12 = y0 - y1, J21 = x2 - x1, J22 = y2 - y1;
+    const double detJ = J11 * J22 - J12 * J21;
+    const double rd = 1.0 / detJ;
+    const double Dx0 = J22 * rd, Dx1 = (J12 - J22) * rd, Dx2 = -J12 * rd;
+    const double Dy0 = -J21 * rd, Dy1 = (J21 - J11) * rd, Dy2 = J11 * rd;
+    // nodal values; velocities at X + gamma dX (CalcCostFunctionNR.m:14-16)
+    auto vel = [&](int nd, double& u, double& v) {
+      u = __ldg(in.X + uoff + nd);
+      v = __ldg(in.X + voff + nd);
+      if (in.dX) { u += gam * __ldg(in.dX + uoff + nd); v += gam * __ldg(in.dX + voff + nd); }
+    };
+    double u0, v0, u1, v1, u2, v2;
+    vel(n0, u0, v0); vel(n1, u1, v1); vel(n2, u2, v2);
+    const double h0 = __ldg(in.h + n0), h1 = __ldg(in.h + n1), h2 = __ldg(in.h + n2);
+    const double s0 = __ldg(in.s + n0), s1 = __ldg(in.s + n1), s2 = __ldg(in.s + n2);
+    // element constants (:322-347)
+    const double dsdx = (Dx0 * s0 + Dx1 * s1) + Dx2 * s2, dhdx = (Dx0 * h0 + Dx1 * h1) + Dx2 * h2;
+    const double dsdy = (Dy0 * s0 + Dy1 * s1) + Dy2 * s2, dhdy = (Dy0 * h0 + Dy1 * h1) + Dy2 * h2;
+    const double exx = (Dx0 * u0 + Dx1 * u1) + Dx2 * u2;
+    const double eyy = (Dy0 * v0 + Dy1 * v1) + Dy2 * v2;
+    const double exy = (0.5 * (Dx0 * v0 + Dy0 * u0) + 0.5 * (Dx1 * v1 + Dy1 * u1)) + 0.5 * (Dx2 * v2 + Dy2 * u2);
+    const double dbdx = dsdx - dhdx, dbdy = dsdy - dhdy;
+    const double e2 = P.EpsZero * P.EpsZero + exx * exx + eyy * eyy + exx * eyy + exy * exy;
+    // this lane's integration point: interpolation and clamps (:186-254)
+    const double hint = (h0 * N0 + h1 * N1) + h2 * N2;
+    const double uint = (u0 * N0 + u1 * N1) + u2 * N2;
+    const double vint = (v0 * N0 + v1 * N1) + v2 * N2;
+    auto interp = [&](const double* f) {
+      return (__ldg(f + n0) * N0 + __ldg(f + n1) * N1) + __ldg(f + n2) * N2;
+    };
+    double Cint = interp(in.C), Aint = interp(in.A);
+    if (Cint < P.Cmin) Cint = P.Cmin;        // :205
+    if (Aint < P.AGlenmin) Aint = P.AGlenmin;  // :243
+    const double Hint = interp(in.S) - interp(in.B);
+    const double rhoint = interp(in.rho);
+    // flotation at the integration point (:300-310)
+    const double hfint = rhow * Hint / rhoint;
+    const double tf = tanh_step(P.kH, hint - hfint, P.Hh0);
+    const double Heint = 0.5 + 0.5 * tf;
+    // H(hf - h): the mirror 0.5 - 0.5 tanh for x0 = 0 (tanh is odd)
+    const double HEint = P.Hh0 == 0.0 ? 0.5 - 0.5 * tf : 0.5 + 0.5 * tanh_step(P.kH, hfint - hint, P.Hh0);
+    const double Hposint = (0.5 + 0.5 * tanh_step(P.kH, Hint, P.Hh0)) * Hint;
+    const double dint = HEint * rhoint * hint / rhow + Heint * Hposint;
+    // drag (BasalDrag.m:54-77, :410-446): Weertman drag is identically zero on floating ice (He = 0)
+    double taux = 0, tauy = 0, dxu = 0, dyv = 0, dxv = 0;
+    if (GEN) {
+      const int gn[3] = {n0, n1, n2};
+      const double Nw[3] = {N0, N1, N2};
+      const Drag d = basal_drag_general(P, Heint, 0.0, hint, Hint, rhoint, rhow, g, uint, vint, Cint,
+                                        interp(in.m), drag_interp<3>(in.drag, gn, Nw));
+      taux = d.taux; tauy = d.tauy; dxu = d.dxu; dyv = d.dyv; dxv = d.dxv;
+    } else if (Heint > 0) {
+      const double sp2 = uint * uint + vint * vint + P.SpeedZero * P.SpeedZero;
+      double Cm, ps, cD;
+      if (cube) {
+        Cm = rcbrt(Cint + P.Czero); ps = rcbrt(sp2); cD = -2.0 / 3.0;
+      } else {
+        const double mint = interp(in.m);
+        Cm = pow(Cint + P.Czero, -1.0 / mint); ps = pow(sp2, (1.0 - mint) / (2.0 * mint)); cD = 1.0 / mint - 1.0;
+      }
+      const double beta2 = Cm * ps, Dbeta2 = cD * Cm * ps / sp2;
+      taux = Heint * beta2 * uint; tauy = Heint * beta2 * vint;
+      dxu = Heint * (beta2 + Dbeta2 * uint * uint);
+      dyv = Heint * (beta2 + Dbeta2 * vint * vint);
+      dxv = Heint * Dbeta2 * uint * vint;
+    }
+    // viscosity (EffectiveViscositySSTREAM.m:7-9)
+    double Am, pe, cE;
+    if (cube) {
+      Am = rcbrt(Aint); pe = rcbrt(e2); cE = -1.0 / 6.0;
+    } else {
+      const double nint = interp(in.n);
+      Am = pow(Aint, -1.0 / nint); pe = pow(sqrt(e2), (1.0 - nint) / nint); cE = (1.0 - nint) / (4.0 * nint);
+    }
+    const double eta = 0.5 * Am * pe + P.etaZero;
+    const double detJw = detJ * wj;
+    const double rr = rhoint * hint - rhow * dint;
+    double s_he = hint * eta * detJw;
+    double s_pp = 0.5 * g * ca * (rhoint * hint * hint - rhow * dint * dint) * detJw;
+    double s_hE = 0;
+    if (WITHK) s_hE = P.Dvisk * 2.0 * hint * (cE * Am * pe / e2) * detJw;
+    ws[TX * 32 + lane] = taux * detJw;
+    ws[TY * 32 + lane] = tauy * detJw;
+    ws[FX * 32 + lane] = (-g * rr * dbdx * ca + rhoint * g * hint * sa) * detJw;
+    ws[FY * 32 + lane] = (-g * rr * dbdy * ca) * detJw;
+    if (WITHK) {
+      ws[CXU * 32 + lane] = dxu * detJw;
+      ws[CYV * 32 + lane] = dyv * detJw;
+      ws[CXV * 32 + lane] = dxv * detJw;
+    }
+    // S1, S2, P over the element's six points, fixed order ((0+3)+(1+4))+(2+5), to every lane
+    auto sum6 = [&](double v) {
+      v += __shfl_down_sync(0xffffffffu, v, 3);
+      const double a = __shfl_down_sync(0xffffffffu, v, 1);
+      const double b = __shfl_down_sync(0xffffffffu, v, 2);
+      return __shfl_sync(0xffffffffu, (v + a) + b, g0);
+    };
+    const double S1 = sum6(s_he), Pp = sum6(s_pp);
+    const double S2 = WITHK ? sum6(s_hE) : 0.0;
+    __syncwarp();
+    // sum_ip sc(kind, ip) w(ip) for the element of this lane's group, ip in order
+    auto dot = [&](int kind, int a, int b, bool pair) {
+      const double* src = ws + kind * 32 + g0;
+      double acc = 0.0;
+#pragma unroll
+      for (int ip = 0; ip < 6; ++ip) {
+        const double w = pair ? sN[ip * 3 + a] * sN[ip * 3 + b] : sN[ip * 3 + a];
+        acc += src[ip] * w;
+      }
+      return acc;
+    };
+    if (valid) {
+      if (WITHK) {
+        const double Pu0 = (2 * exx + eyy) * Dx0 + exy * Dy0, Pu1 = (2 * exx + eyy) * Dx1 + exy * Dy1,
+                     Pu2 = (2 * exx + eyy) * Dx2 + exy * Dy2;
+        const double Pv0 = (2 * eyy + exx) * Dy0 + exy * Dx0, Pv1 = (2 * eyy + exx) * Dy1 + exy * Dx1,
+                     Pv2 = (2 * eyy + exx) * Dy2 + exy * Dx2;
+        // symmetric blocks: packed upper-triangle pair j (row-major: 00 01 02 11 12 22)
+        const int a = j < 3 ? 0 : (j < 5 ? 1 : 2);
+        const int b = j < 3 ? j : (j < 5 ? j - 2 : 2);
+        const double dxa = sel3(Dx0, Dx1, Dx2, a), dxb = sel3(Dx0, Dx1, Dx2, b);
+        const double dya = sel3(Dy0, Dy1, Dy2, a), dyb = sel3(Dy0, Dy1, Dy2, b);
+        const double kuu = S1 * (4 * dxa * dxb + dya * dyb) + S2 * (sel3(Pu0, Pu1, Pu2, a) * sel3(Pu0, Pu1, Pu2, b)) +
+                           dot(CXU, a, b, true);
+        const double kvv = S1 * (4 * dya * dyb + dxa * dxb) + S2 * (sel3(Pv0, Pv1, Pv2, a) * sel3(Pv0, Pv1, Pv2, b)) +
+                           dot(CYV, a, b, true);
+        sK[j * E + t] = (KT)kuu;
+        sK[(I::NS + j) * E + t] = (KT)kvv;
+        // uv block, full: entries (j/3, j%3) for j < 6, then (2, j) on lanes 0-2
+#pragma unroll
+        for (int step = 0; step < 2; ++step) {
+          const int q = step * 6 + j;
+          if (q < 9) {
+            const int ua = q / 3, ub = q % 3;
+            const double kuv = S1 * (2 * sel3(Dx0, Dx1, Dx2, ua) * sel3(Dy0, Dy1, Dy2, ub) +
+                                     sel3(Dy0, Dy1, Dy2, ua) * sel3(Dx0, Dx1, Dx2, ub)) +
+                               S2 * (sel3(Pu0, Pu1, Pu2, ua) * sel3(Pv0, Pv1, Pv2, ub)) + dot(CXV, ua, ub, true);
+            sK[(2 * I::NS + q) * E + t] = (KT)kuv;
+          }
+        }
+      }
+      // residual parts: lanes 0-2 the x rows of nodes 0-2, lanes 3-5 the y rows
+      const bool yrow = j >= 3;
+      const int a = yrow ? j - 3 : j;
+      const double da = sel3(Dx0, Dx1, Dx2, a), db = sel3(Dy0, Dy1, Dy2, a);
+      const double d1 = yrow ? db : da, d2 = yrow ? da : db;      // Dy, Dx for the y rows
+      const double e1 = yrow ? eyy : exx, e2_ = yrow ? exx : eyy;
+      const double T = S1 * ((4 * e1 + 2 * e2_) * d1 + 2 * exy * d2) + dot(yrow ? TY : TX, a, 0, false);
+      const double F = Pp * d1 + dot(yrow ? FY : FX, a, 0, false);
+      sR[((yrow ? 2 : 0) * 3 + a) * E + t] = T;
+      sR[((yrow ? 3 : 1) * 3 + a) * E + t] = F;
+    }
+    __syncwarp();  // the scratch is rewritten by the next element group
+  }
+  __syncthreads();
+  patch_scatter<3, WITHK, KT>(M, out, p, s, uoff, voff, sK, sR, E);
+}
+
+size_t uv_p1_smem(bool withK, bool fp32, int E) {
+  size_t k = withK ? (((size_t)ElemIdx<3>::NKE * E * (fp32 ? 4 : 8) + 15) & ~(size_t)15) : 0;
+  return k + (size_t)12 * E * 8 + 24 * 8 + (size_t)p1::kWarps * p1::NSC * 32 * 8;
+}
+
+// P2 (6-node elements): one element per thread in 128-thread blocks, the
+// integration points in a loop (the derivatives vary over the element).
+template <int NOD, bool WITHK, typename KT>
+__global__ void __launch_bounds__(128, 1) uv_patch_kernel(DevMesh M, QuadTable Q, UvPhys P, UvIn in, UvOut out) {
+  using I = ElemIdx<NOD>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int p = blockIdx.x;
+  const int s = M.patch_sys[p];
+  if (in.active && !in.active[s]) return;
+  const int E = M.max_patch_elems;
+  KT* sK = reinterpret_cast<KT*>(smem);
+  size_t koff = WITHK ? (((size_t)I::NKE * E * sizeof(KT) + 15) & ~(size_t)15) : 0;
+  double* sR = reinterpret_cast<double*>(smem + koff);
+  const int e0 = M.patch_elem_ptr[p], ne = M.patch_elem_ptr[p + 1] - e0;
+  const int uoff = M.sys_dof_off[s] - M.sys_node_off[s];
+  const int nn_s = M.sys_node_off[s + 1] - M.sys_node_off[s];
+  const int voff = uoff + nn_s;
+  const double gam = in.gamma ? in.gamma[s] : 0.0;
+  const SysScal S = in.scal[s];
+  // nodal values of element e (u, v at X + gamma dX)
+  auto gather = [&](int e, int (&gn)[NOD], double (&xe)[NOD], double (&ye)[NOD], double (&hn)[NOD],
+                    double (&sn)[NOD], double (&un)[NOD], double (&vn)[NOD], double (&Cn)[NOD], double (&mn)[NOD],
+                    double (&An)[NOD], double (&nn)[NOD], double (&Sn)[NOD], double (&Bn)[NOD], double (&rn)[NOD]) {
+#pragma unroll
+    for (int a = 0; a < NOD; ++a) {
+      const int gnode = __ldg(M.conn + (size_t)a * M.ne + e);
+      gn[a] = gnode;
+      xe[a] = __ldg(M.x + gnode); ye[a] = __ldg(M.y + gnode);
+      hn[a] = __ldg(in.h + gnode); sn[a] = __ldg(in.s + gnode);
+      double u = __ldg(in.X + uoff + gnode), v = __ldg(in.X + voff + gnode);
+      if (in.dX) { u += gam * __ldg(in.dX + uoff + gnode); v += gam * __ldg(in.dX + voff + gnode); }
+      un[a] = u; vn[a] = v;
+      Cn[a] = __ldg(in.C + gnode); mn[a] = __ldg(in.m + gnode);
+      An[a] = __ldg(in.A + gnode); nn[a] = __ldg(in.n + gnode);
+      Sn[a] = __ldg(in.S + gnode); Bn[a] = __ldg(in.B + gnode);
+      rn[a] = __ldg(in.rho + gnode);
+    }
+  };
+  auto store = [&](int t, const KT* Kuu, const KT* Kvv, const KT* Kuv, const double* Tx, const double* Fx,
+                   const double* Ty, const double* Fy) {
+    if (WITHK) {
+#pragma unroll
+      for (int i = 0; i < I::NS; ++i) { sK[i * E + t] = Kuu[i]; sK[(I::NS + i) * E + t] = Kvv[i]; }
+#pragma unroll
+      for (int i = 0; i < NOD * NOD; ++i) sK[(2 * I::NS + i) * E + t] = Kuv[i];
+    }
+#pragma unroll
+    for (int a = 0; a < NOD; ++a) {
+      sR[(0 * NOD + a) * E + t] = Tx[a];
+      sR[(1 * NOD + a) * E + t] = Fx[a];
+      sR[(2 * NOD + a) * E + t] = Ty[a];
+      sR[(3 * NOD + a) * E + t] = Fy[a];
+    }
+  };
+  for (int t = threadIdx.x; t < ne; t += blockDim.x) {
+    int gn[NOD];
+    double xe[NOD], ye[NOD], hn[NOD], sn[NOD], un[NOD], vn[NOD], Cn[NOD], mn[NOD], An[NOD], nn[NOD], Sn[NOD],
+        Bn[NOD], rn[NOD];
+    gather(__ldg(M.patch_elems + e0 + t), gn, xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn);
+    KT Kuu[I::NS], Kvv[I::NS], Kuv[NOD * NOD];
+    double Tx[NOD], Fx[NOD], Ty[NOD], Fy[NOD];
+    uv_element<NOD, WITHK, KT>(Q, P, S, gn, in.drag, xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv,
+                               Kuv, Tx, Fx, Ty, Fy);
+    store(t, Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
+  }
+  __syncthreads();
+  patch_scatter<NOD, WITHK, KT>(M, out, p, s, uoff, voff, sK, sR, E);
+}
+
 size_t uv_patch_smem(int nod, bool withK, bool fp32, int E) {
   int NS = nod * (nod + 1) / 2, NKE = 2 * NS + nod * nod;
   size_t k = withK ? (((size_t)NKE * E * (fp32 ? 4 : 8) + 15) & ~(size_t)15) : 0;
   return k + (size_t)4 * nod * E * 8;
 }
 
+template <bool WITHK, typename KT>
+static cudaError_t launch_p1(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out) {
+  if (quad_table(3).nip != 6) return cudaErrorInvalidConfiguration;  // six lanes, one point each
+  size_t sm = uv_p1_smem(WITHK, sizeof(KT) == 4, m->dm.max_patch_elems);
+  const bool gen = P.law != UA_SLIDING_WEERTMAN || P.melange;
+  auto kern = gen ? uv_p1_kernel<WITHK, KT, true> : uv_p1_kernel<WITHK, KT, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
+  kern<<<m->dm.npatch, p1::kThreads, sm, m->stream>>>(m->dm, quad_table(3), P, in, out);
+  return cudaGetLastError();
+}
+
 template <int NOD, bool WITHK, typename KT>
 static cudaError_t launch_t(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, int threads) {
-  if (NOD == 3 && quad_table(3).nip > 6) return cudaErrorInvalidConfiguration;  // 6-lane groups of the P1 kernel
   size_t sm = uv_patch_smem(NOD, WITHK, sizeof(KT) == 4, m->dm.max_patch_elems);
   auto kern = uv_patch_kernel<NOD, WITHK, KT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -409,10 +658,10 @@ static cudaError_t launch_t(const ua_mesh* m, const UvPhys& P, const UvIn& in, c
 // threads: CTA size of the P1 kernels (128 or 256; 0 = 256 with K, 128 residual-only)
 cudaError_t launch_uv_assembly(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, bool withK,
                                bool fp32K, int threads) {
-  if (threads != 128 && threads != 256) threads = withK ? 256 : 128;
+  (void)threads;
   if (m->nod == 3) {
-    if (!withK) return launch_t<3, false, double>(m, P, in, out, threads);
-    return fp32K ? launch_t<3, true, float>(m, P, in, out, threads) : launch_t<3, true, double>(m, P, in, out, threads);
+    if (!withK) return launch_p1<false, double>(m, P, in, out);
+    return fp32K ? launch_p1<true, float>(m, P, in, out) : launch_p1<true, double>(m, P, in, out);
   }
   if (!withK) return launch_t<6, false, double>(m, P, in, out, 128);
   return fp32K ? launch_t<6, true, float>(m, P, in, out, 128) : launch_t<6, true, double>(m, P, in, out, 128);

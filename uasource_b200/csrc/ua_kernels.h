@@ -15,6 +15,7 @@ struct UvIn {
   const double* gamma;    // [nsys], may be null
   const SysScal* scal;    // [nsys]
   const int* active;      // [nsys], may be null (all active)
+  DragFields drag;        // sliding-law and melange fields (null unless the law reads them)
 };
 
 struct UvOut {
@@ -35,6 +36,7 @@ struct UvhIn {
   const SysScal* scal;
   const int* active;
   int zero_fields;        // uvhMatrixAssembly.m:9-15
+  DragFields drag;        // sliding-law and melange fields (null unless the law reads them)
 };
 
 struct UvhPhys {

@@ -1,11 +1,28 @@
 // Device restatement of the SSA constitutive, drag and flotation functions.
 #pragma once
 #include <cuda_runtime.h>
+#include "../../include/ua_ssa.h"
 
 namespace ua {
 
 struct UvPhys {            // CtrlVar subset used inside the element loop
   double kH, Hh0, SpeedZero, EpsZero, etaZero, Czero, Cmin, AGlenmin, Dvisk;
+  double Nzero;            // CtrlVar.Nzero (effective pressure floor)
+  int law;                 // CtrlVar.SlidingLaw (UA_SLIDING_*)
+  int melange;             // CtrlVar.IncludeMelangeModelPhysics
+};
+
+// Integration-point values of the fields the other sliding laws and the melange
+// terms read (uvMatrixAssemblySSTREAM.m:210-254); unused ones are zero.
+struct DragIp {
+  double q, muk, V0;
+  double uo, vo, Co, mo, ua, va, Ca, ma;
+};
+
+// Nodal arrays of those fields (global node index; null when the law does not use them).
+struct DragFields {
+  const double *q, *muk, *V0;
+  const double* mel[8];  // uo, vo, Co, mo, ua, va, Ca, ma
 };
 
 struct SysScal {           // per-system F scalars
@@ -91,6 +108,156 @@ __device__ __forceinline__ Drag basal_drag_weertman(const UvPhys& P, double He, 
   d.dxh = delta * beta2 * u;
   d.dyh = delta * beta2 * v;
   return d;
+}
+
+// N0 of BasalDrag.m (zeroth-order hydrology): N = rho g max(h - hf, 0) + Nzero with
+// hf = rhow H / rho (values below eps taken as 0), dN/dh = rho g where h > hf.
+__device__ __forceinline__ void effective_pressure_n0(const UvPhys& P, double h, double H, double rho, double rhow,
+                                                      double g, double& N, double& dNdh, double& Dh) {
+  const double eps = 2.220446049250313e-16;
+  double hf = rhow * H / rho;
+  if (hf < eps) hf = 0.0;
+  Dh = h - hf;
+  const bool dry = Dh < eps;
+  if (dry) Dh = 0.0;
+  N = rho * g * Dh + P.Nzero;
+  dNdh = dry ? 0.0 : rho * g;
+}
+
+// An isotropic law |tau| = T(U) with tau = T (u, v) / U: A = T/U, B = (T' - T/U)/U^2 give
+// tau_x = A u, d tau_x/du = A + B u^2, d tau_x/dv = B u v, d tau_y/dv = A + B v^2.
+__device__ __forceinline__ void isotropic_drag(double A, double B, double u, double v, Drag& d) {
+  d.taux = A * u; d.tauy = A * v;
+  d.dxu = A + B * u * u; d.dyv = A + B * v * v; d.dxv = B * u * v;
+}
+
+// BasalDrag.m:44-363 for every CtrlVar.SlidingLaw, plus the melange terms (:275-343).
+// Weertman, Budd and Coulomb follow the reference's expressions (:410-490, :365-408);
+// Tsai takes the smaller of the Weertman and Coulomb stresses pointwise (:207-244).
+// Cornford (rpCWN0.m), Umbi (rCWN0.m) and Joughin (rCWV0.m) are written through their
+// stresses |tau| = mu N W / ((mu N)^m + W^m)^(1/m), mu N W / (mu N + W) and
+// W (U + V0)^(-1/m), W = He (C + C0)^(-1/m) U^(1/m), and their velocity derivatives
+// (isotropic_drag); their thickness derivatives are the reference's expressions, which
+// evaluate the Heaviside factor of the delta term at 1/2.
+__device__ inline Drag basal_drag_general(const UvPhys& P, double He, double delta, double h, double H,
+                                          double rho, double rhow, double g, double u, double v, double C,
+                                          double m, const DragIp& x) {
+  const double eps = 2.220446049250313e-16;
+  if (delta < 0) delta = 0;
+  if (He < 0) He = 0;
+  const double C0 = P.Czero, u0 = P.SpeedZero;
+  const double sp2 = u * u + v * v + u0 * u0;
+  const double speed = sqrt(sp2);
+  const double cm = pow(C + C0, -1.0 / m);
+  const double beta2 = cm * pow(speed, 1.0 / m - 1);
+  const double Dbeta2 = (1.0 / m - 1) * cm * pow(sp2, (1 - 3 * m) / (2 * m));
+  Drag d{};
+  auto weertman = [&](Drag& r) {
+    r.taux = He * beta2 * u; r.tauy = He * beta2 * v;
+    r.dxu = He * (beta2 + Dbeta2 * u * u); r.dyv = He * (beta2 + Dbeta2 * v * v); r.dxv = He * Dbeta2 * u * v;
+    r.dxh = delta * beta2 * u; r.dyh = delta * beta2 * v;
+  };
+  auto coulomb = [&](Drag& r, double N, double dNdh, double Dh) {
+    const double Tau = x.muk * N;
+    r.taux = Tau * u / speed; r.tauy = Tau * v / speed;
+    const double temp = speed * speed * speed;
+    r.dxu = Tau * (1 / speed - u * u / temp); r.dyv = Tau * (1 / speed - v * v / temp);
+    r.dxv = -Tau * u * v / temp;
+    const double E = Dh < eps ? 0.0 : x.muk * dNdh / speed;
+    r.dxh = E * u; r.dyh = E * v;
+  };
+  double N = 0, dNdh = 0, Dh = 0;
+  if (P.law != UA_SLIDING_WEERTMAN && P.law != UA_SLIDING_JOUGHIN)
+    effective_pressure_n0(P, h, H, rho, rhow, g, N, dNdh, Dh);
+  switch (P.law) {
+    case UA_SLIDING_BUDD: {
+      const double qm = x.q / m, Nqm = pow(N, qm);
+      const double T = He * Nqm * beta2;
+      const double E = delta * T + He * qm * pow(N, qm - 1) * dNdh * beta2;
+      d.taux = T * u; d.tauy = T * v;
+      d.dxu = He * Nqm * (beta2 + Dbeta2 * u * u); d.dyv = He * Nqm * (beta2 + Dbeta2 * v * v);
+      d.dxv = He * Nqm * Dbeta2 * u * v;
+      d.dxh = E * u; d.dyh = E * v;
+      break;
+    }
+    case UA_SLIDING_COULOMB:
+      coulomb(d, N, dNdh, Dh);
+      break;
+    case UA_SLIDING_TSAI: {
+      Drag w{}, c{};
+      weertman(w);
+      coulomb(c, N, dNdh, Dh);
+      d = (c.taux * c.taux + c.tauy * c.tauy < w.taux * w.taux + w.tauy * w.tauy) ? c : w;
+      break;
+    }
+    case UA_SLIDING_CORNFORD: {
+      const double muN = x.muk * N, cu = cm * pow(speed, 1.0 / m);
+      const double W = He * cu, S = pow(muN, m) + pow(W, m);
+      const double TU = muN * He * cm * pow(speed, 1.0 / m - 1) * pow(S, -1.0 / m);
+      const double Tp = muN * (W / (m * speed)) * pow(muN, m) * pow(S, -1.0 / m - 1);
+      isotropic_drag(TU, (Tp - TU) / sp2, u, v, d);
+      const double Wm = pow(cu, m), us = cm * pow(speed, 1.0 / m - 1);
+      const double E = pow(2.0, m + 1) * pow(muN, m + 1) * delta * us * pow(pow(2.0, m) * pow(muN, m) + Wm, -(m + 1) / m) +
+                       x.muk * dNdh * pow(He, m + 1) * us * Wm * pow(S, -(m + 1) / m);
+      d.dxh = E * u; d.dyh = E * v;
+      break;
+    }
+    case UA_SLIDING_UMBI: {
+      const double c1 = pow(C + C0, 1.0 / m), muN = x.muk * N, sm = pow(speed, 1.0 / m);
+      const double den = muN * c1 + He * sm;
+      const double TU = muN * He * pow(speed, 1.0 / m - 1) / den;
+      const double W = He * sm / c1;
+      const double Tp = muN * muN * W / (m * speed * (muN + W) * (muN + W));
+      isotropic_drag(TU, (Tp - TU) / sp2, u, v, d);
+      const double den2 = 2 * muN * c1 + sm;
+      const double E = x.muk * dNdh * He * pow(speed, 2.0 / m - 1) / (den * den) +
+                       4.0 * x.muk * x.muk * N * N * delta * c1 * pow(speed, 1.0 / m - 1) / (den2 * den2);
+      d.dxh = E * u; d.dyh = E * v;
+      break;
+    }
+    case UA_SLIDING_JOUGHIN: {
+      const double us = cm * pow(x.V0 + speed, -1.0 / m) * pow(speed, 1.0 / m - 1);
+      const double TU = He * us;
+      const double Tp = TU * x.V0 / (m * (speed + x.V0));
+      isotropic_drag(TU, (Tp - TU) / sp2, u, v, d);
+      d.dxh = delta * us * u; d.dyh = delta * us * v;
+      break;
+    }
+    default:
+      weertman(d);
+  }
+  if (P.melange) {  // ocean and atmosphere drag on the floating part
+    const double w0[2][4] = {{x.uo, x.vo, x.Co, x.mo}, {x.ua, x.va, x.Ca, x.ma}};
+    for (int k = 0; k < 2; ++k) {
+      const double U = u - w0[k][0], V = v - w0[k][1], Cw = w0[k][2], mw = w0[k][3];
+      const double s2 = U * U + V * V + u0 * u0;
+      const double cw = pow(Cw + C0, -1.0 / mw);
+      const double b2 = cw * pow(sqrt(s2), 1.0 / mw - 1);
+      const double Db2 = (1.0 / mw - 1) * cw * pow(s2, (1 - 3 * mw) / (2 * mw));
+      d.taux += (1 - He) * b2 * U; d.tauy += (1 - He) * b2 * V;
+      d.dxu += (1 - He) * (b2 + Db2 * U * U); d.dyv += (1 - He) * (b2 + Db2 * V * V);
+      d.dxv += (1 - He) * (Db2 * U * V);
+      d.dxh += -delta * b2 * U; d.dyh += -delta * b2 * V;
+    }
+  }
+  return d;
+}
+
+// Interpolated sliding-law fields at an integration point (nodal values times N).
+template <int NOD>
+__device__ __forceinline__ DragIp drag_interp(const DragFields& F, const int (&gn)[NOD], const double* N) {
+  DragIp x{};
+  auto at = [&](const double* f) {
+    double r = 0.0;
+    if (f)
+#pragma unroll
+      for (int a = 0; a < NOD; ++a) r += __ldg(f + gn[a]) * N[a];
+    return r;
+  };
+  x.q = at(F.q); x.muk = at(F.muk); x.V0 = at(F.V0);
+  x.uo = at(F.mel[0]); x.vo = at(F.mel[1]); x.Co = at(F.mel[2]); x.mo = at(F.mel[3]);
+  x.ua = at(F.mel[4]); x.va = at(F.mel[5]); x.Ca = at(F.mel[6]); x.ma = at(F.mel[7]);
+  return x;
 }
 
 }  // namespace ua

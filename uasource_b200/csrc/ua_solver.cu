@@ -78,6 +78,10 @@ struct Work {
   // nodal fields
   double *h, *s, *S, *B, *rho, *A, *n, *C, *m;
   SysScal* scal;
+  // sliding-law and melange fields (q, muk, V0, uo, vo, Co, mo, ua, va, Ca, ma): buffers allocated
+  // on first use, dragf[k] = dragbuf[k] while the configured law reads field k, else null
+  double* dragbuf[11] = {};
+  const double* dragf[11] = {};
   // dof vectors
   double *X, *X0, *dX, *R, *frhs, *Tint, *Fext;
   double* Kd = nullptr;
@@ -759,7 +763,49 @@ static UvPhys make_phys(const ua_params* p) {
   P.kH = p->kH; P.Hh0 = p->Hh0; P.SpeedZero = p->SpeedZero; P.EpsZero = p->EpsZero; P.etaZero = p->etaZero;
   P.Czero = p->Czero; P.Cmin = p->Cmin; P.AGlenmin = p->AGlenmin;
   P.Dvisk = p->Picard ? 0.0 : p->NRviscosity;  // uvMatrixAssemblySSTREAM.m:67-71
+  P.Nzero = p->Nzero;
+  P.law = p->SlidingLaw;
+  P.melange = p->IncludeMelangeModelPhysics != 0;
   return P;
+}
+
+// The sliding-law and melange fields the configured law reads (BasalDrag.m), copied to the
+// device for every system; the others stay null.  A law whose fields are missing is refused.
+static int upload_drag_fields(ua_mesh* m, const ua_params* p, const ua_fields* F, int nF) {
+  Work* w = m->work;
+  if (p->SlidingLaw < UA_SLIDING_WEERTMAN || p->SlidingLaw > UA_SLIDING_JOUGHIN)
+    return set_error(UA_ERR_INVALID, "BasalDrag:CaseNotFound unknown SlidingLaw %d", p->SlidingLaw);
+  const int law = p->SlidingLaw;
+  bool need[11] = {};
+  need[0] = law == UA_SLIDING_BUDD;
+  need[1] = law == UA_SLIDING_TSAI || law == UA_SLIDING_COULOMB || law == UA_SLIDING_CORNFORD ||
+            law == UA_SLIDING_UMBI;
+  need[2] = law == UA_SLIDING_JOUGHIN;
+  for (int k = 3; k < 11; ++k) need[k] = p->IncludeMelangeModelPhysics != 0;
+  const char* names[11] = {"q", "muk", "V0", "uo", "vo", "Co", "mo", "ua", "va", "Ca", "ma"};
+  for (int k = 0; k < 11; ++k) {
+    w->dragf[k] = nullptr;
+    if (!need[k]) continue;
+    if (!w->dragbuf[k]) w->dragbuf[k] = walloc<double>(m, (size_t)m->nn_total);
+    if (!w->dragbuf[k]) return set_error(UA_ERR_OOM, "device allocation of F.%s failed", names[k]);
+    for (int s = 0; s < m->dm.nsys; ++s) {
+      const ua_fields& f = F[nF == 1 ? 0 : s];
+      const double* src[11] = {f.q, f.muk, f.V0, f.uo, f.vo, f.Co, f.mo, f.ua, f.va, f.Ca, f.ma};
+      if (!src[k]) return set_error(UA_ERR_INVALID, "system %d: the sliding law needs F.%s", s, names[k]);
+      UA_CUDA_TRY(cudaMemcpyAsync(w->dragbuf[k] + m->h_node_off[s], src[k], m->sys[s].nn * sizeof(double),
+                                  f.location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                  m->stream));
+    }
+    w->dragf[k] = w->dragbuf[k];
+  }
+  return UA_OK;
+}
+
+static DragFields drag_fields(const Work* w) {
+  DragFields D{};
+  D.q = w->dragf[0]; D.muk = w->dragf[1]; D.V0 = w->dragf[2];
+  for (int k = 0; k < 8; ++k) D.mel[k] = w->dragf[3 + k];
+  return D;
 }
 
 static bool any_nan(const double* v, int n) {
@@ -871,6 +917,7 @@ static int upload_fields(ua_mesh* m, const ua_params* p, const ua_fields* F, int
                                   loc == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, m->stream));
       s = e;
     }
+  if (int rc = upload_drag_fields(m, p, F, nF)) return rc;
   return finish_fields(m, p, sc, 0, nsys);
 }
 
@@ -1035,6 +1082,7 @@ static int assemble(ua_mesh* m, const ua_params* p, bool withK, bool useDir, con
   Work* w = m->work;
   UvIn in{w->h, w->s, w->S, w->B, w->rho, w->A, w->n, w->C, w->m, X, useDir ? w->dX : nullptr,
           useDir ? w->gamma : nullptr, w->scal, w->sel};
+  in.drag = drag_fields(w);
   bool fp32 = p->precision == UA_PREC_MIXED;
   UvOut out{w->R, withK ? (fp32 ? (void*)w->Kf : (void*)w->Kd) : nullptr, parts ? w->Tint : nullptr,
             parts ? w->Fext : nullptr};
@@ -2351,14 +2399,14 @@ static int upload_fields_uvh(ua_mesh* m, const ua_params* p, const ua_fields* F,
   }
   UA_CUDA_TRY(cudaMemcpyAsync(w->scal, sc.data(), sc.size() * sizeof(SysScal), cudaMemcpyHostToDevice, m->stream));
   set_cube_flags(m);
-  (void)p;
-  return UA_OK;
+  return upload_drag_fields(m, p, F, nF);
 }
 
 static int assemble_uvh(ua_mesh* m, const ua_params* p, bool withK, bool useDir, bool zero, bool parts) {
   Work* w = m->work;
   UvhIn in{w->S, w->B, w->rho, w->A, w->n, w->C, w->m, w->h0, w->u0, w->v0, w->as0, w->ab0, w->as1, w->ab1,
            w->dadh, w->X, useDir ? w->dX : nullptr, useDir ? w->gamma : nullptr, w->scal, w->sel, zero ? 1 : 0};
+  in.drag = drag_fields(w);
   UvOut out{w->R, withK ? (void*)w->Kd : nullptr, parts ? w->Tint : nullptr, parts ? w->Fext : nullptr};
   cudaEvent_t ev[2];
   prof_begin(m, withK ? PK_ASMK : PK_ASMR, ev);
@@ -2596,6 +2644,9 @@ extern "C" void ua_params_default(ua_params* p) {
   p->uvh_h_sweeps = 0;
   p->krylov_sell = 1;
   p->krylov_precond = UA_PC_AMG;
+  p->SlidingLaw = UA_SLIDING_WEERTMAN;  // :171
+  p->Nzero = 1e-20;                     // :445
+  p->IncludeMelangeModelPhysics = 0;
 }
 
 extern "C" int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs, int32_t mode,

@@ -184,7 +184,17 @@ __global__ void __launch_bounds__(NOD == 3 ? 512 : 320) uvh_patch_kernel(DevMesh
       const double exy = 0.5 * (ddx(F_V1) + ddy(F_U1));
       double eta, Ev;
       effective_viscosity(P.uv, Aint, nint, exx, eyy, exy, eta, Ev, cube);  // :149
-      const Drag d = basal_drag_weertman(P.uv, Heint, deltaint, uint, vint, Cint, mint, cube);  // :150
+      Drag d;  // :150
+      if (P.uv.law == UA_SLIDING_WEERTMAN && !P.uv.melange) {
+        d = basal_drag_weertman(P.uv, Heint, deltaint, uint, vint, Cint, mint, cube);
+      } else {
+        int gn[NOD];
+        const int e = __ldg(M.patch_elems + e0 + el);
+#pragma unroll
+        for (int a = 0; a < NOD; ++a) gn[a] = __ldg(M.conn + (size_t)a * M.ne + e);
+        d = basal_drag_general(P.uv, Heint, deltaint, hint, Hint, rhoint, rhow, g, uint, vint, Cint, mint,
+                               drag_interp<NOD>(in.drag, gn, N));
+      }
       const double speed0 = sqrt(u0int * u0int + v0int * v0int + P.SpeedZero * P.SpeedZero);  // :157
       const double tau0 = P.beta0 * supg_tau(P, speed0, lsupg, dt);                         // :158-159
       const double detJw = detJ * Q.w[ip];

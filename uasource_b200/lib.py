@@ -24,6 +24,11 @@ UA_ERR_KRYLOV = -8
 UA_ERR_NO_DEVICE = -9
 
 UA_PREC_FP64 = 0
+UA_SLIDING_WEERTMAN, UA_SLIDING_BUDD, UA_SLIDING_TSAI, UA_SLIDING_COULOMB = 0, 1, 2, 3
+UA_SLIDING_CORNFORD, UA_SLIDING_UMBI, UA_SLIDING_JOUGHIN = 4, 5, 6
+# CtrlVar.SlidingLaw names (Ua2D_DefaultParameters.m:172) -> UA_SLIDING_*
+SLIDING_LAWS = {"Weertman": 0, "W": 0, "Budd": 1, "W-N0": 1, "Tsai": 2, "minCW-N0": 2, "Coulomb": 3, "C": 3,
+                "Cornford": 4, "rpCW-N0": 4, "Umbi": 5, "rCW-N0": 5, "Joughin": 6, "rCW-V0": 6}
 UA_PREC_MIXED = 1
 UA_PC_JACOBI = 0
 UA_PC_AMG = 1
@@ -79,6 +84,7 @@ class ua_params(C.Structure):
         ("krylov_eta_c", C.c_double), ("krylov_eta_max", C.c_double), ("precond_bf16", C.c_int32),
         ("amg_smoothed", C.c_int32), ("krylov_full_grid", C.c_int32),
         ("uvh_h_sweeps", C.c_int32), ("krylov_sell", C.c_int32),
+        ("SlidingLaw", C.c_int32), ("Nzero", C.c_double), ("IncludeMelangeModelPhysics", C.c_int32),
     ]
 
 
@@ -88,7 +94,10 @@ class ua_fields(C.Structure):
                 ("m", _dp), ("ub", _dp), ("vb", _dp),
                 ("rhow", C.c_double), ("g", C.c_double), ("alpha", C.c_double),
                 ("h0", _dp), ("u0", _dp), ("v0", _dp), ("as0", _dp), ("ab0", _dp), ("as1", _dp), ("ab1", _dp),
-                ("dadh", _dp), ("h1", _dp), ("dt", C.c_double)]
+                ("dadh", _dp), ("h1", _dp), ("dt", C.c_double),
+                ("q", _dp), ("muk", _dp), ("V0", _dp),
+                ("uo", _dp), ("vo", _dp), ("Co", _dp), ("mo", _dp), ("ua", _dp), ("va", _dp), ("Ca", _dp),
+                ("ma", _dp)]
 
 
 class ua_bcs(C.Structure):

@@ -86,6 +86,9 @@ class CtrlVar:
     krylov_full_grid: int = 0
     uvh_h_sweeps: int = 0
     krylov_sell: int = 1
+    SlidingLaw: str = "Weertman"          # any name of L.SLIDING_LAWS
+    Nzero: float = 1e-20
+    IncludeMelangeModelPhysics: int = 0
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
@@ -108,6 +111,10 @@ class CtrlVar:
             if isinstance(v, tuple):
                 arr = getattr(p, f.name)
                 arr[0], arr[1] = float(v[0]), float(v[1])
+            elif f.name == "SlidingLaw":
+                if v not in L.SLIDING_LAWS:
+                    raise ValueError(f"BasalDrag:CaseNotFound what sliding law? ({v!r})")
+                p.SlidingLaw = L.SLIDING_LAWS[v]
             else:
                 setattr(p, f.name, v)
         return p
@@ -132,6 +139,17 @@ class Fields:
     as_: np.ndarray = None      # surface mass balance F.as (transient solves)
     ab: np.ndarray = None       # basal mass balance F.ab
     dadh: np.ndarray = None     # d(as+ab)/dh (MassBalanceGeometryFeedback=3), None = 0
+    q: np.ndarray = None        # Budd sliding-law exponent
+    muk: np.ndarray = None      # Coulomb friction coefficient (Tsai, Coulomb, Cornford, Umbi)
+    V0: np.ndarray = None       # Joughin speed scale
+    uo: np.ndarray = None       # melange: ocean velocity, drag coefficient and exponent
+    vo: np.ndarray = None
+    Co: np.ndarray = None
+    mo: np.ndarray = None
+    ua: np.ndarray = None       # melange: atmosphere velocity, drag coefficient and exponent
+    va: np.ndarray = None
+    Ca: np.ndarray = None
+    ma: np.ndarray = None
 
     @staticmethod
     def from_problem(P):
@@ -206,6 +224,10 @@ def _c_fields(F: Fields, keep: _Keep, Nn: int):
     cf.ub = L.dptr(ub)
     cf.vb = L.dptr(vb)
     cf.rhow, cf.g, cf.alpha = float(F.rhow), float(F.g), float(F.alpha)
+    for name in ("q", "muk", "V0", "uo", "vo", "Co", "mo", "ua", "va", "Ca", "ma"):
+        v = getattr(F, name)
+        if v is not None:
+            setattr(cf, name, keep.d(full(v)))
     return cf, ub, vb
 
 
