@@ -324,6 +324,15 @@ int ua_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
 /* Number of rows of the constraint matrix L built from bcs (CreateLuv.m). */
 int ua_constraint_count(const ua_mesh* m, const ua_bcs* bcs, int32_t ndof, int32_t* nc);
 
+/* The constraint matrix L and right-hand side c of the fixed-node BCs of a single-mesh handle
+ * (AssembleLuvSSTREAM.m:2-40 -> BCs2MLC.m:19-29, CreateLuv.m:28-76, ScaleL.m:28-33; createLh.m
+ * for fixed h on an ndof=3 handle): row k has its one non-zero L(k, dof[k]) = val[k] (0-based
+ * dof in Úa order) and c(k) = rhs[k].  Rows in the order of the Lagrange multipliers: fixed u
+ * nodes increasing, then fixed v nodes, then fixed h nodes as given.  This is the L that
+ * SSTREAM2dNR2.m:3 returns as Lubvb.  Arrays may be NULL to query *nc only. */
+int ua_constraint_matrix(const ua_mesh* m, const ua_bcs* bcs, int32_t* nc, int32_t* dof, double* val,
+                         double* rhs);
+
 /* solveKApeSymmetric (solveKApeSymmetric.m:71-113) -> ABfgPreEliminate
  * (ABfgPreEliminate.m:29-160) for an SPD block A given in CSR on the host:
  * [A L'; L 0][x;y] = [f;g] with L given in CSR (nl rows, at most one non-zero

@@ -1,11 +1,12 @@
 /*
- * [ub,vb,lubvb,Kuv,Ruv,info] = SSTREAM2dNR2_mex(CtrlVar,MUA,BCs,F,l)
+ * [ub,vb,lubvb,Kuv,Ruv,info,Lubvb] = SSTREAM2dNR2_mex(CtrlVar,MUA,BCs,F,l)
  *
  * Drop-in for the Newton solve SSTREAM2dNR2.m:3 (called from uv.m:104),
  * including the reset-and-retry of uv.m:107-112.  `l` is the l.ubvb vector
  * (may be []).  `info` is a struct with the RunInfo.Forward fields
- * uvConverged, uvIterations, uvResidual, uvBackTrackSteps and the
- * per-iteration record of the NR-SSTREAM(uv) log line (SSTREAM2dNR2.m:386).
+ * uvConverged, uvIterations, uvResidual, uvBackTrackSteps, rForce and rWork.
+ * Lubvb is the constraint matrix L of the BCs (nc x 2Nn sparse), the
+ * reference's last output.
  */
 #include "ua_mex_common.h"
 
@@ -22,6 +23,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     double *ub, *vb, *lam, *K = NULL, *R = NULL, *own[8];
     const char* names[8] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
     const double* src[8];
+    double* own_drag[11];
     int k, rc;
 
     if (nrhs < 4) mexErrMsgIdAndTxt("Ua:mex:nargin", "SSTREAM2dNR2_mex(CtrlVar,MUA,BCs,F,l)");
@@ -34,6 +36,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     for (k = 0; k < 8; ++k) src[k] = ua_mex_nodal(F, names[k], nn, &own[k]);
     f.h = src[0]; f.S = src[1]; f.B = src[2]; f.rho = src[3];
     f.AGlen = src[4]; f.n = src[5]; f.C = src[6]; f.m = src[7];
+    ua_mex_drag_fields(F, nn, &f, own_drag);
     plhs[0] = mxCreateDoubleMatrix(nn, 1, mxREAL);
     plhs[1] = mxCreateDoubleMatrix(nn, 1, mxREAL);
     ub = mxGetPr(plhs[0]); vb = mxGetPr(plhs[1]);
@@ -57,6 +60,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     }
     rc = ua_uv_newton(m, &p, &f, &b, lam, nc, &rep, K, R);
     for (k = 0; k < 8; ++k) if (own[k]) mxFree(own[k]);
+    for (k = 0; k < 11; ++k) if (own_drag[k]) mxFree(own_drag[k]);
     if (rc != UA_OK && rc != UA_ERR_NOT_CONVERGED) ua_mex_fail(rc);
     if (nlhs > 2) {
         plhs[2] = mxCreateDoubleMatrix(nc, 1, mxREAL);
@@ -75,6 +79,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         mxSetField(s, 0, "rWork", mxCreateDoubleScalar(rep.rWork));
         plhs[5] = s;
     }
+    if (nlhs > 6) plhs[6] = ua_mex_constraint_L(m, &b, 2 * nn);
     mxFree(lam);
     if (K) mxFree(K);
     if (R) mxFree(R);

@@ -22,6 +22,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     double *ub, *vb, *h, *lam, *own[14];
     const char* names[8] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
     const double* src[8];
+    double* own_drag[11];
     int k, rc;
 
     if (nrhs < 5) mexErrMsgIdAndTxt("Ua:mex:nargin", "SSTREAM_TransientImplicit_mex(CtrlVar,MUA,BCs1,F0,F1,l1)");
@@ -36,6 +37,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     for (k = 0; k < 8; ++k) src[k] = ua_mex_nodal(F1, names[k], nn, &own[k]);
     f.h = src[0]; f.S = src[1]; f.B = src[2]; f.rho = src[3];
     f.AGlen = src[4]; f.n = src[5]; f.C = src[6]; f.m = src[7];
+    ua_mex_drag_fields(F1, nn, &f, own_drag);
     plhs[0] = mxCreateDoubleMatrix(nn, 1, mxREAL);
     plhs[1] = mxCreateDoubleMatrix(nn, 1, mxREAL);
     plhs[2] = mxCreateDoubleMatrix(nn, 1, mxREAL);
@@ -65,6 +67,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     rep.iters_capacity = 256;
     rc = ua_uvh_newton(m, &p, &f, &b, lam, nc, &rep);
     for (k = 0; k < 14; ++k) if (own[k]) mxFree(own[k]);
+    for (k = 0; k < 11; ++k) if (own_drag[k]) mxFree(own_drag[k]);
     if (rc != UA_OK && rc != UA_ERR_NOT_CONVERGED) ua_mex_fail(rc);
     if (nlhs > 3) {
         plhs[3] = mxCreateDoubleMatrix(nc, 1, mxREAL);

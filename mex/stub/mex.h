@@ -31,6 +31,9 @@ mxArray* mxCreateSparse(mwSize m, mwSize n, mwSize nzmax, mxComplexity c);
 mxArray* mxCreateDoubleMatrix(mwSize m, mwSize n, mxComplexity c);
 mxArray* mxCreateDoubleScalar(double v);
 mxArray* mxCreateStructMatrix(mwSize m, mwSize n, int nfields, const char** names);
+mxArray* mxCreateString(const char* s);
+void mxDestroyArray(mxArray* a);
+int mxIsSparse(const mxArray* a);
 void* mxMalloc(size_t n);
 void* mxCalloc(size_t n, size_t size);
 void mxFree(void* p);

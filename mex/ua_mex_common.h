@@ -43,6 +43,14 @@ static uint64_t ua_mex_hash(const void* p, size_t n, uint64_t h) {
     return h;
 }
 
+static void ua_mex_fail(int rc) {
+    const char* id = "Ua:mex:Error";
+    if (rc == UA_ERR_NAN_INPUT) id = "uvMatrixAssembly:NaN";
+    else if (rc == UA_ERR_NO_DEVICE) id = "Ua:mex:NoDevice";
+    else if (rc == UA_ERR_OOM) id = "Ua:mex:OutOfMemory";
+    mexErrMsgIdAndTxt(id, "%s", ua_last_error());
+}
+
 static const mxArray* ua_mex_field(const mxArray* s, const char* name, int required) {
     const mxArray* f = (s && mxIsStruct(s)) ? mxGetField(s, 0, name) : NULL;
     if (!f && required) mexErrMsgIdAndTxt("Ua:mex:MissingField", "missing field %s", name);
@@ -139,6 +147,29 @@ static void ua_mex_params(const mxArray* C, ua_params* p) {
             }
         }
     }
+    /* CtrlVar.SlidingLaw as a char array (a MATLAB string object is not readable through the C
+     * API: pass char(CtrlVar.SlidingLaw), or the numeric GPUSlidingLaw = UA_SLIDING_*) */
+    {
+        static const char* laws[14] = {"Weertman", "W", "Budd", "W-N0", "Tsai", "minCW-N0", "Coulomb", "C",
+                                       "Cornford", "rpCW-N0", "Umbi", "rCW-N0", "Joughin", "rCW-V0"};
+        static const int codes[14] = {UA_SLIDING_WEERTMAN, UA_SLIDING_WEERTMAN, UA_SLIDING_BUDD, UA_SLIDING_BUDD,
+                                      UA_SLIDING_TSAI, UA_SLIDING_TSAI, UA_SLIDING_COULOMB, UA_SLIDING_COULOMB,
+                                      UA_SLIDING_CORNFORD, UA_SLIDING_CORNFORD, UA_SLIDING_UMBI, UA_SLIDING_UMBI,
+                                      UA_SLIDING_JOUGHIN, UA_SLIDING_JOUGHIN};
+        const mxArray* t = ua_mex_field(C, "SlidingLaw", 0);
+        if (t && mxIsChar(t)) {
+            char* name = mxArrayToString(t);
+            int k, found = 0;
+            for (k = 0; name && k < 14; ++k)
+                if (!strcmp(name, laws[k])) { p->SlidingLaw = codes[k]; found = 1; }
+            if (name) mxFree(name);
+            if (!found) mexErrMsgIdAndTxt("BasalDrag:CaseNotFound", "what sliding law?");
+        }
+        p->SlidingLaw = (int32_t)ua_mex_scalar(C, "GPUSlidingLaw", p->SlidingLaw);
+    }
+    p->Nzero = ua_mex_scalar(C, "Nzero", p->Nzero);
+    p->IncludeMelangeModelPhysics =
+        (int32_t)ua_mex_scalar(C, "IncludeMelangeModelPhysics", p->IncludeMelangeModelPhysics);
     /* the GPU form selected by a CtrlVar.UseGPU-style switch (0=FP64, 1=mixed) */
     p->precision = (int32_t)ua_mex_scalar(C, "GPUPrecision", p->precision);
     p->krylov_rtol = ua_mex_scalar(C, "GPUKrylovTol", p->krylov_rtol);
@@ -206,6 +237,53 @@ static const double* ua_mex_nodal(const mxArray* F, const char* name, size_t nn,
     return NULL;
 }
 
+/* The sliding-law and melange fields of F present and non-empty (F.q, F.muk, F.V0, F.uo, F.vo,
+ * F.Co, F.mo, F.ua, F.va, F.Ca, F.ma); scalars are expanded.  own[11] receives the expanded
+ * copies (free them with mxFree). */
+static void ua_mex_drag_fields(const mxArray* F, size_t nn, ua_fields* f, double** own) {
+    static const char* names[11] = {"q", "muk", "V0", "uo", "vo", "Co", "mo", "ua", "va", "Ca", "ma"};
+    const double** dst[11];
+    int k;
+    dst[0] = &f->q; dst[1] = &f->muk; dst[2] = &f->V0; dst[3] = &f->uo; dst[4] = &f->vo; dst[5] = &f->Co;
+    dst[6] = &f->mo; dst[7] = &f->ua; dst[8] = &f->va; dst[9] = &f->Ca; dst[10] = &f->ma;
+    for (k = 0; k < 11; ++k) {
+        const mxArray* a = ua_mex_field(F, names[k], 0);
+        own[k] = NULL;
+        *dst[k] = NULL;
+        if (a && !mxIsEmpty(a)) *dst[k] = ua_mex_nodal(F, names[k], nn, &own[k]);
+    }
+}
+
+/* The constraint matrix L (nc x ncols sparse, one unit entry per row; ScaleL.m) of the BCs b, as
+ * AssembleLuvSSTREAM.m / AssembleLuvhSSTREAM.m build it, via ua_constraint_matrix. */
+static mxArray* ua_mex_constraint_L(ua_mesh* m, const ua_bcs* b, int32_t ncols) {
+    int32_t nc = 0, k;
+    int32_t* dof;
+    double* val;
+    mwIndex *jc, *ir, *cnt;
+    double* pr;
+    mxArray* L;
+    int rc = ua_constraint_matrix(m, b, &nc, NULL, NULL, NULL);
+    if (rc != UA_OK) ua_mex_fail(rc);
+    dof = (int32_t*)mxMalloc((nc > 0 ? nc : 1) * sizeof(int32_t));
+    val = (double*)mxMalloc((nc > 0 ? nc : 1) * sizeof(double));
+    rc = ua_constraint_matrix(m, b, &nc, dof, val, NULL);
+    if (rc != UA_OK) ua_mex_fail(rc);
+    L = mxCreateSparse(nc, ncols, nc > 0 ? nc : 1, mxREAL);
+    jc = mxGetJc(L); ir = mxGetIr(L); pr = mxGetPr(L);
+    cnt = (mwIndex*)mxCalloc(ncols + 1, sizeof(mwIndex));
+    for (k = 0; k < nc; ++k) cnt[dof[k] + 1]++;
+    for (k = 0; k < ncols; ++k) cnt[k + 1] += cnt[k];
+    for (k = 0; k <= ncols; ++k) jc[k] = cnt[k];
+    for (k = 0; k < nc; ++k) {  /* rows in increasing order, so each column's rows come out sorted */
+        ir[cnt[dof[k]]] = (mwIndex)k;
+        pr[cnt[dof[k]]] = val[k];
+        cnt[dof[k]]++;
+    }
+    mxFree(cnt); mxFree(dof); mxFree(val);
+    return L;
+}
+
 /* dadh of uvhMatrixAssembly.m:152-158: F1.dasdh + F1.dabdh when
  * CtrlVar.MassBalanceGeometryFeedback is 3, else none (NULL = zero). */
 static const double* ua_mex_dadh(const mxArray* C, const mxArray* F1, size_t nn, double** owned) {
@@ -257,14 +335,6 @@ static void ua_mex_bcs(const mxArray* B, ua_bcs* b) {
     b->hfixed_node = ua_mex_nodes(B, "hFixedNode", &b->n_hfixed);
     b->hfixed_value = ua_mex_values(B, "hFixedValue");
     for (i = 0; i < b->n_hfixed; ++i) ((int32_t*)b->hfixed_node)[i] -= 1;
-}
-
-static void ua_mex_fail(int rc) {
-    const char* id = "Ua:mex:Error";
-    if (rc == UA_ERR_NAN_INPUT) id = "uvMatrixAssembly:NaN";
-    else if (rc == UA_ERR_NO_DEVICE) id = "Ua:mex:NoDevice";
-    else if (rc == UA_ERR_OOM) id = "Ua:mex:OutOfMemory";
-    mexErrMsgIdAndTxt(id, "%s", ua_last_error());
 }
 
 /* CSR values on the structural pattern -> MATLAB sparse (CSC, sorted rows, no

@@ -21,6 +21,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     double *R, *K = NULL, *T = NULL, *Fx = NULL, *own[8];
     const char* names[8] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
     const double* src[8];
+    double* own_drag[11];
     int k;
 
     if (nrhs != 4) mexErrMsgIdAndTxt("Ua:mex:nargin", "uvMatrixAssemblySSTREAM_mex(CtrlVar,MUA,F,BCs)");
@@ -40,6 +41,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     for (k = 0; k < 8; ++k) src[k] = ua_mex_nodal(F, names[k], nn, &own[k]);
     f.h = src[0]; f.S = src[1]; f.B = src[2]; f.rho = src[3];
     f.AGlen = src[4]; f.n = src[5]; f.C = src[6]; f.m = src[7];
+    ua_mex_drag_fields(F, nn, &f, own_drag);
     f.ub = mxGetPr(ua_mex_field(F, "ub", 1));
     f.vb = mxGetPr(ua_mex_field(F, "vb", 1));
     f.rhow = ua_mex_scalar(F, "rhow", 1030.0);
@@ -56,6 +58,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     }
     rc = ua_uv_assemble(m, &p, &f, &b, mode, R, K, T, Fx);
     for (k = 0; k < 8; ++k) if (own[k]) mxFree(own[k]);
+    for (k = 0; k < 11; ++k) if (own_drag[k]) mxFree(own_drag[k]);
     if (rc != UA_OK) ua_mex_fail(rc);
     plhs[0] = ua_mex_sparse_vector(neq, R);
     if (nlhs > 1) plhs[1] = K ? ua_mex_sparse(m, neq, K) : mxCreateDoubleMatrix(0, 0, mxREAL);

@@ -21,6 +21,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     int32_t nn, neq;
     int64_t nnz = 0;
     double *R, *K = NULL, *own[14];
+    double* own_drag[11];
     const char* names[8] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
     const double* src[8];
 
@@ -41,6 +42,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     for (k = 0; k < 8; ++k) src[k] = ua_mex_nodal(F1, names[k], nn, &own[k]);
     f.h = src[0]; f.S = src[1]; f.B = src[2]; f.rho = src[3];
     f.AGlen = src[4]; f.n = src[5]; f.C = src[6]; f.m = src[7];
+    ua_mex_drag_fields(F1, nn, &f, own_drag);
     f.ub = mxGetPr(ua_mex_field(F1, "ub", 1));
     f.vb = mxGetPr(ua_mex_field(F1, "vb", 1));
     f.h1 = (double*)src[0];
@@ -64,6 +66,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     }
     rc = ua_uvh_assemble(m, &p, &f, mode, R, K, NULL, NULL);
     for (k = 0; k < 14; ++k) if (own[k]) mxFree(own[k]);
+    for (k = 0; k < 11; ++k) if (own_drag[k]) mxFree(own_drag[k]);
     if (rc != UA_OK) ua_mex_fail(rc);
     plhs[0] = ua_mex_sparse_vector(neq, R);
     if (nlhs > 1) plhs[1] = K ? ua_mex_sparse_unsym(m, neq, K) : mxCreateDoubleMatrix(0, 0, mxREAL);

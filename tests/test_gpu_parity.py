@@ -189,10 +189,11 @@ def test_c0_newton_trajectory_and_updates_match_oracle(c0):
 def test_update_buffer_stride_is_checked(c0):
     P, _, mua_g, _ = c0
     import ctypes as C
+    from uasource_b200 import ua as host
     lib = L.load()
-    keep = ua._Keep()
-    cf, _, _ = ua._c_fields(ua.Fields.from_problem(P), keep, P.Nnodes)
-    cb = ua._c_bcs(ua.BCs.from_problem(P), keep)
+    keep = host._Keep()
+    cf, _, _ = host._c_fields(ua.Fields.from_problem(P), keep, P.Nnodes)
+    cb = host._c_bcs(ua.BCs.from_problem(P), keep)
     p = ua.CtrlVar().set_force_tolerance(1e-20).to_c()
     rep = L.ua_newton_report()
     buf = np.zeros((4, 10))

@@ -980,11 +980,14 @@ static int upload_velocity(ua_mesh* m, const ua_fields* F, int nF) {
 
 // BCs2MLC.m:19-25 + CreateLuv.m:28-76 + ScaleL.m for fixed-node BCs: one unit row
 // per unique fixed node (first occurrence's value), u rows then v rows.
-static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
-  Work* w = m->work;
+// The constraint rows of the fixed-node BCs, host side: per system the u rows by increasing
+// node, then the v rows, then (ndof 3) the h rows in the given order; each row has one unit
+// entry at con_dof (global dof) and right-hand side rhs (first occurrence of a repeated node).
+static int constraint_rows(const ua_mesh* m, const ua_bcs* bcs, int nB, std::vector<int>& con_dof,
+                           std::vector<int>& con_sys, std::vector<double>& rhs, std::vector<int>& sys_off) {
   const int nsys = m->dm.nsys;
-  std::vector<int> con_dof, con_sys, sys_off(nsys + 1, 0);
-  std::vector<double> rhs;
+  con_dof.clear(); con_sys.clear(); rhs.clear();
+  sys_off.assign(nsys + 1, 0);
   for (int s = 0; s < nsys; ++s) {
     const ua_bcs* b = bcs ? &bcs[nB == 1 ? 0 : s] : nullptr;
     if (b && (b->n_utied > 0 || b->n_vtied > 0))
@@ -1027,6 +1030,15 @@ static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
     }
     sys_off[s + 1] = (int)con_dof.size();
   }
+  return UA_OK;
+}
+
+static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
+  Work* w = m->work;
+  const int nsys = m->dm.nsys;
+  std::vector<int> con_dof, con_sys, sys_off;
+  std::vector<double> rhs;
+  if (int rc = constraint_rows(m, bcs, nB, con_dof, con_sys, rhs, sys_off)) return rc;
   const int nc = (int)con_dof.size();
   if (nc > w->nc || !w->con_dof) {
     int cap = std::max(nc, 1);
@@ -2829,6 +2841,22 @@ extern "C" int ua_constraint_count(const ua_mesh* m, const ua_bcs* bcs, int32_t 
     if (ndof == 3) n += bcs->n_hfixed;
   }
   *nc = n;
+  return UA_OK;
+}
+
+extern "C" int ua_constraint_matrix(const ua_mesh* m, const ua_bcs* bcs, int32_t* nc, int32_t* dof, double* val,
+                                    double* rhs) {
+  if (!m || !nc) return set_error(UA_ERR_INVALID, "ua_constraint_matrix: null argument");
+  if (m->dm.nsys != 1) return set_error(UA_ERR_INVALID, "ua_constraint_matrix takes a single-mesh handle");
+  std::vector<int> cd, cs, off;
+  std::vector<double> r;
+  if (int rc = constraint_rows(m, bcs, 1, cd, cs, r, off)) return rc;
+  *nc = (int32_t)cd.size();
+  for (size_t k = 0; k < cd.size(); ++k) {
+    if (dof) dof[k] = cd[k];
+    if (val) val[k] = 1.0;  // one unit entry per row: ScaleL.m leaves it 1
+    if (rhs) rhs[k] = r[k];
+  }
   return UA_OK;
 }
 

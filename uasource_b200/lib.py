@@ -161,6 +161,7 @@ SIGNATURES = {
     "ua_serve_result": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, C.POINTER(ua_newton_report)]),
     "ua_mem_info": (C.c_int, [C.c_int32, _lp, _lp]),
     "ua_constraint_count": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), C.c_int32, _ip]),
+    "ua_constraint_matrix": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), _ip, _ip, _dp, _dp]),
     "ua_solve_kape_symmetric": (C.c_int, [C.c_int32, _lp, _lp, _dp, C.c_int32, _lp, _lp, _dp, _dp, _dp, _dp, _dp,
                                           C.c_double, C.c_int32, _ip, C.c_int32]),
     "ua_solve_kape_symmetric_noalloc": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
