@@ -26,7 +26,7 @@ static ua_mesh* g_meshes[2] = {NULL, NULL};
 static uint64_t g_mesh_keys[2] = {0, 0};
 static int g_locked = 0;
 
-static void ua_mex_cleanup(void) {
+static inline void ua_mex_cleanup(void) {
     int k;
     for (k = 0; k < 2; ++k) {
         if (g_meshes[k]) ua_mesh_destroy(g_meshes[k]);
@@ -36,14 +36,14 @@ static void ua_mex_cleanup(void) {
 }
 
 /* FNV-1a over the raw bytes of the mesh arrays: detects a changed MUA. */
-static uint64_t ua_mex_hash(const void* p, size_t n, uint64_t h) {
+static inline uint64_t ua_mex_hash(const void* p, size_t n, uint64_t h) {
     const unsigned char* b = (const unsigned char*)p;
     size_t i;
     for (i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ULL;
     return h;
 }
 
-static void ua_mex_fail(int rc) {
+static inline void ua_mex_fail(int rc) {
     const char* id = "Ua:mex:Error";
     if (rc == UA_ERR_NAN_INPUT) id = "uvMatrixAssembly:NaN";
     else if (rc == UA_ERR_NO_DEVICE) id = "Ua:mex:NoDevice";
@@ -51,20 +51,20 @@ static void ua_mex_fail(int rc) {
     mexErrMsgIdAndTxt(id, "%s", ua_last_error());
 }
 
-static const mxArray* ua_mex_field(const mxArray* s, const char* name, int required) {
+static inline const mxArray* ua_mex_field(const mxArray* s, const char* name, int required) {
     const mxArray* f = (s && mxIsStruct(s)) ? mxGetField(s, 0, name) : NULL;
     if (!f && required) mexErrMsgIdAndTxt("Ua:mex:MissingField", "missing field %s", name);
     return f;
 }
 
-static double ua_mex_scalar(const mxArray* s, const char* name, double dflt) {
+static inline double ua_mex_scalar(const mxArray* s, const char* name, double dflt) {
     const mxArray* f = ua_mex_field(s, name, 0);
     if (!f || mxIsEmpty(f)) return dflt;
     return mxGetScalar(f);
 }
 
 /* CtrlVar -> ua_params (fields named as in Ua2D_DefaultParameters.m). */
-static void ua_mex_params(const mxArray* C, ua_params* p) {
+static inline void ua_mex_params(const mxArray* C, ua_params* p) {
     const mxArray* f;
     ua_params_default(p);
     p->kH = ua_mex_scalar(C, "kH", p->kH);
@@ -179,7 +179,7 @@ static void ua_mex_params(const mxArray* C, ua_params* p) {
 
 /* MUA -> cached device mesh with ndof dofs per node (2: uv, 3: uvh), rebuilt
  * when coordinates/connectivity change. */
-static ua_mesh* ua_mex_mesh_ndof(const mxArray* MUA, int ndof) {
+static inline ua_mesh* ua_mex_mesh_ndof(const mxArray* MUA, int ndof) {
     const mxArray* co = ua_mex_field(MUA, "coordinates", 1);
     const mxArray* cn = ua_mex_field(MUA, "connectivity", 1);
     size_t nn = mxGetM(co), ne = mxGetM(cn), nod = mxGetN(cn), i;
@@ -220,10 +220,10 @@ static ua_mesh* ua_mex_mesh_ndof(const mxArray* MUA, int ndof) {
     return g_meshes[slot];
 }
 
-static ua_mesh* ua_mex_mesh(const mxArray* MUA) { return ua_mex_mesh_ndof(MUA, 2); }
+static inline ua_mesh* ua_mex_mesh(const mxArray* MUA) { return ua_mex_mesh_ndof(MUA, 2); }
 
 /* A nodal field: Nn-vector, or a scalar expanded as uv.m:34-40 does for m and n. */
-static const double* ua_mex_nodal(const mxArray* F, const char* name, size_t nn, double** owned) {
+static inline const double* ua_mex_nodal(const mxArray* F, const char* name, size_t nn, double** owned) {
     const mxArray* f = ua_mex_field(F, name, 1);
     size_t k = mxGetNumberOfElements(f), i;
     *owned = NULL;
@@ -240,7 +240,7 @@ static const double* ua_mex_nodal(const mxArray* F, const char* name, size_t nn,
 /* The sliding-law and melange fields of F present and non-empty (F.q, F.muk, F.V0, F.uo, F.vo,
  * F.Co, F.mo, F.ua, F.va, F.Ca, F.ma); scalars are expanded.  own[11] receives the expanded
  * copies (free them with mxFree). */
-static void ua_mex_drag_fields(const mxArray* F, size_t nn, ua_fields* f, double** own) {
+static inline void ua_mex_drag_fields(const mxArray* F, size_t nn, ua_fields* f, double** own) {
     static const char* names[11] = {"q", "muk", "V0", "uo", "vo", "Co", "mo", "ua", "va", "Ca", "ma"};
     const double** dst[11];
     int k;
@@ -256,7 +256,7 @@ static void ua_mex_drag_fields(const mxArray* F, size_t nn, ua_fields* f, double
 
 /* The constraint matrix L (nc x ncols sparse, one unit entry per row; ScaleL.m) of the BCs b, as
  * AssembleLuvSSTREAM.m / AssembleLuvhSSTREAM.m build it, via ua_constraint_matrix. */
-static mxArray* ua_mex_constraint_L(ua_mesh* m, const ua_bcs* b, int32_t ncols) {
+static inline mxArray* ua_mex_constraint_L(ua_mesh* m, const ua_bcs* b, int32_t ncols) {
     int32_t nc = 0, k;
     int32_t* dof;
     double* val;
@@ -286,7 +286,7 @@ static mxArray* ua_mex_constraint_L(ua_mesh* m, const ua_bcs* b, int32_t ncols) 
 
 /* dadh of uvhMatrixAssembly.m:152-158: F1.dasdh + F1.dabdh when
  * CtrlVar.MassBalanceGeometryFeedback is 3, else none (NULL = zero). */
-static const double* ua_mex_dadh(const mxArray* C, const mxArray* F1, size_t nn, double** owned) {
+static inline const double* ua_mex_dadh(const mxArray* C, const mxArray* F1, size_t nn, double** owned) {
     const mxArray *a = ua_mex_field(F1, "dasdh", 0), *b = ua_mex_field(F1, "dabdh", 0);
     size_t i;
     *owned = NULL;
@@ -298,7 +298,7 @@ static const double* ua_mex_dadh(const mxArray* C, const mxArray* F1, size_t nn,
 }
 
 /* BCs node lists (double, 1-based) -> int32 arrays owned by the caller. */
-static int32_t* ua_mex_nodes(const mxArray* B, const char* name, int32_t* n) {
+static inline int32_t* ua_mex_nodes(const mxArray* B, const char* name, int32_t* n) {
     const mxArray* f = ua_mex_field(B, name, 0);
     size_t k = f ? mxGetNumberOfElements(f) : 0, i;
     int32_t* out;
@@ -309,14 +309,14 @@ static int32_t* ua_mex_nodes(const mxArray* B, const char* name, int32_t* n) {
     return out;
 }
 
-static const double* ua_mex_values(const mxArray* B, const char* name) {
+static inline const double* ua_mex_values(const mxArray* B, const char* name) {
     const mxArray* f = ua_mex_field(B, name, 0);
     return (f && !mxIsEmpty(f)) ? mxGetPr(f) : NULL;
 }
 
 /* The mesh's 1-based BC lists.  The library takes 0-based indices for
  * index_base handles created from MATLAB too, so shift here. */
-static void ua_mex_bcs(const mxArray* B, ua_bcs* b) {
+static inline void ua_mex_bcs(const mxArray* B, ua_bcs* b) {
     int32_t i;
     memset(b, 0, sizeof(*b));
     if (!B || !mxIsStruct(B)) return;
@@ -340,7 +340,7 @@ static void ua_mex_bcs(const mxArray* B, ua_bcs* b) {
 /* CSR values on the structural pattern -> MATLAB sparse (CSC, sorted rows, no
  * explicit zeros).  The uv pattern and values are symmetric, so the CSR arrays
  * are read as CSC. */
-static mxArray* ua_mex_sparse(ua_mesh* m, int32_t n, const double* vals) {
+static inline mxArray* ua_mex_sparse(ua_mesh* m, int32_t n, const double* vals) {
     int64_t nnz = 0, j, k, out = 0;
     int64_t *rp, *ci;
     mxArray* S;
@@ -367,7 +367,7 @@ static mxArray* ua_mex_sparse(ua_mesh* m, int32_t n, const double* vals) {
 /* CSR values of an unsymmetric tangent (uvh) on the structural pattern ->
  * MATLAB sparse: a column-count pass, then the transpose (CSC, sorted rows,
  * no explicit zeros). */
-static mxArray* ua_mex_sparse_unsym(ua_mesh* m, int32_t n, const double* vals) {
+static inline mxArray* ua_mex_sparse_unsym(ua_mesh* m, int32_t n, const double* vals) {
     int64_t nnz = 0, i, k, out = 0;
     int64_t *rp, *ci;
     mwIndex *jc, *ir, *next;
@@ -394,7 +394,7 @@ static mxArray* ua_mex_sparse_unsym(ua_mesh* m, int32_t n, const double* vals) {
 }
 
 /* A dense vector as an n x 1 sparse (MATLAB's Tint-Fext is sparse-typed). */
-static mxArray* ua_mex_sparse_vector(int32_t n, const double* v) {
+static inline mxArray* ua_mex_sparse_vector(int32_t n, const double* v) {
     int32_t i, nz = 0;
     mxArray* S;
     mwIndex *jc, *ir;

@@ -74,7 +74,7 @@ static mxArray* alloc_array(int kind, size_t m, size_t n) {
 mxArray* mxCreateDoubleMatrix(mwSize m, mwSize n, mxComplexity c) {
     mxArray* a = alloc_array(K_DOUBLE, m, n);
     (void)c;
-    a->pr = (double*)calloc(m * n ? m * n : 1, sizeof(double));
+    a->pr = (double*)calloc((m * n) > 0 ? m * n : 1, sizeof(double));
     return a;
 }
 
