@@ -318,6 +318,32 @@ int ua_serve_begin(ua_mesh* m, const ua_params* p, int32_t count, const int32_t*
 int ua_serve_step(ua_mesh* m, const ua_params* p, int32_t* finished, int32_t* nactive);
 int ua_serve_result(ua_mesh* m, int32_t sys, double* ub, double* vb, ua_newton_report* rep);
 
+/* Velocity data of the misfit (Meas in Misfit.m:38-66 with CtrlVar.Inverse.Measurements "-uv-"):
+ * measured surface velocities and their standard errors uErr = sqrt(diag(Meas.usCov)),
+ * vErr = sqrt(diag(Meas.vsCov)); Nnodes each, in the memory space of the fields (ua_fields.location). */
+typedef struct ua_measurements {
+    const double *us, *vs, *usErr, *vsErr;
+} ua_measurements;
+
+#define UA_ADJ_LOGC      1   /* gradient with respect to log10(C) (CtrlVar.Inverse.InvertFor "-logC-") */
+#define UA_ADJ_PREMUL_M  2   /* CtrlVar.Inverse.AdjointGradientPreMultiplier "M": (M/Area)\dIdC */
+
+/* Adjoint gradient of the velocity misfit with respect to C at the solved state F->ub, F->vb of
+ * a single-mesh uv handle (Misfit.m:38-260, the adjoint branch for "-uv-" data; dIdCq.m:1-163;
+ * ApplyAdjointGradientPreMultiplier.m; MassMatrix2D1dof.m):
+ *   I = (r_u' M r_u + r_v' M r_v)/2/Area with r = (u - us)./uErr and M the consistent mass matrix;
+ *   [K L'; L 0][lambda; mu] = [dI/d(u,v); c] with K the uv tangent at the state and L, c the
+ *   adjoint BCs (solveKApeSymmetric; here the constrained AMG-PCG to p->krylov_rtol);
+ *   dIdC_I = int dFuvdC (u lambda_u + v lambda_v) N_I (BasalDrag.m:80-160 for the sliding law),
+ *   then log(10) C .* dIdC (UA_ADJ_LOGC) and (M/Area)\dIdC (UA_ADJ_PREMUL_M).
+ * Outputs are caller-owned host arrays, each may be NULL: I, dIduv (2Nn), lambda (2Nn, the
+ * adjoint velocities [uAdjoint; vAdjoint]), dIdC (Nn); krylov_its the PCG iterations.  Runs in
+ * FP64 whatever p->precision says.  The Coulomb law has no C-gradient in the reference and is
+ * refused with UA_ERR_INVALID. */
+int ua_uv_adjoint_dIdC(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs_adjoint,
+                       const ua_measurements* meas, int32_t flags, double* I, double* dIduv, double* lambda,
+                       double* dIdC, int32_t* krylov_its);
+
 /* Free and total device memory (admission by free HBM). */
 int ua_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
 

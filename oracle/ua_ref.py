@@ -1648,3 +1648,145 @@ def sstream_transient_implicit(p: Params, mua: MUA, bcs: BCs, F: Fields, S0: Uvh
             print(f"NR-SSTREAM(uvh):{iteration:3d}/{ls.info.iarm:<2d} g={gamma:<14.7g} r/r0={r / r0:<14.7g} "
                   f"r0={r0:<14.7g} r={r:<14.7g} rForce={rForce:<14.7g} rWork={rWork:<14.7g}")
     return UvhResult(S1.ub, S1.vb, S1.h, luvh, converged, iteration, records)
+
+
+# ---------------------------------------------------------------------------
+# Adjoint gradient of the velocity misfit with respect to C — Misfit.m ("-uv-", adjoint branch),
+# dIdCq.m, BasalDrag.m (dFuvdClambda), MassMatrix2D1dof.m, ApplyAdjointGradientPreMultiplier.m
+# ---------------------------------------------------------------------------
+
+
+def mass_matrix(mua: MUA):
+    """MassMatrix2D1dof.m: consistent mass matrix, symmetrised as (M+M.')/2."""
+    Nele, nod = mua.Nele, mua.nod
+    d1d1 = np.zeros((Nele, nod, nod))
+    for Iint in range(mua.nip):
+        fun = shape_fun(nod, mua.points[Iint])
+        detJw = mua.DetJ[:, Iint] * mua.weights[Iint]
+        for I in range(nod):
+            for J in range(nod):
+                d1d1[:, I, J] += fun[J] * fun[I] * detJw
+    conn = mua.connectivity
+    Ii = np.concatenate([conn[:, I] for I in range(nod) for J in range(nod)])
+    Jj = np.concatenate([conn[:, J] for I in range(nod) for J in range(nod)])
+    Xv = np.concatenate([d1d1[:, I, J] for I in range(nod) for J in range(nod)])
+    M = _matlab_sparse(Ii, Jj, Xv, mua.Nnodes, mua.Nnodes)
+    return ((M + M.T) / 2).tocsc()
+
+
+def mesh_area(mua: MUA):
+    """CreateMUA.m:97-98: total area, the sum of the element areas (TriAreaFE.m)."""
+    return float(np.sum(tri_area_fe(mua.coordinates, mua.connectivity)))
+
+
+def misfit_uv(mua: MUA, F: Fields, us, vs, usErr, vsErr, M=None):
+    """Misfit.m:38-131 with CtrlVar.Inverse.Measurements "-uv-" (ud = vd = 0 for SSTREAM):
+    residuals (u - us)/uErr, I = (r_u' M r_u + r_v' M r_v)/2/Area and dI/d(u,v) = [M r_u ./ uErr;
+    M r_v ./ vErr]/Area.  Returns (I, dIduv)."""
+    if M is None:
+        M = mass_matrix(mua)
+    A = mesh_area(mua)
+    ru = (F.ub - us) / usErr
+    rv = (F.vb - vs) / vsErr
+    duIdu = (M @ ru) / usErr / A
+    dvIdv = (M @ rv) / vsErr / A
+    I = float(ru @ (M @ ru) + rv @ (M @ rv)) / 2 / A
+    return I, np.concatenate([duIdu, dvIdv])
+
+
+def dFuvdC(p: Params, He, h, H, rho, rhow, g, u, v, C, m, q=None, muk=None, V0=None):
+    """BasalDrag.m:80-160 (CtrlVar.Inverse.dFuvdClambda): the derivative of the drag magnitude over
+    speed with respect to C, per sliding law.  The Coulomb law has none (the reference stops)."""
+    law = p.SlidingLaw
+    He = np.where(He < 0, 0.0, He)
+    C0, u0 = p.Czero, p.SpeedZero
+    speed = np.sqrt(u * u + v * v + u0 ** 2)
+    Um = speed ** (1.0 / m - 1)
+    if law in ("Weertman", "W"):
+        return He * (1.0 / m) * (C + C0) ** (-1.0 / m - 1) * Um
+    if law in ("Budd", "W-N0"):
+        hf = rhow * H / rho
+        hf = np.where(hf < EPS, 0.0, hf)
+        Dh = h - hf
+        Dh = np.where(Dh < EPS, 0.0, Dh)
+        N = rho * g * Dh
+        Nqm = N ** (q / m)
+        return He * Nqm * (1.0 / m) * (C + C0) ** (-1.0 / m - 1) * Um
+    if law in ("Cornford", "rpCW-N0"):
+        N, _ = effective_pressure_n0(p, h, H, rho, rhow, g)
+        U = speed
+        return (U ** (1.0 / m - 1) * muk ** (m + 1) * N ** (m + 1) * He
+                * (muk ** m * N ** m + U * (He * (C + C0) ** (-1.0 / m)) ** m) ** (-1.0 / m - 1)
+                * (C + C0) ** (-1.0 / m - 1)) / m
+    if law in ("Umbi", "rCW-N0"):
+        N, _ = effective_pressure_n0(p, h, H, rho, rhow, g)
+        U = speed
+        return (U ** (1.0 / m) * muk ** 2 * N ** 2 * He / (U ** (1.0 / m) * He + muk * N * (C + C0) ** (1.0 / m)) ** 2
+                * (C + C0) ** (1.0 / m - 1)) / (U * m)
+    if law in ("Tsai", "minCW-N0"):
+        out = He * (1.0 / m) * (C + C0) ** (-1.0 / m - 1) * Um
+        N, dNdh = effective_pressure_n0(p, h, H, rho, rhow, g)
+        beta2 = (C + C0) ** (-1.0 / m) * Um
+        tW2 = (He * beta2 * u) ** 2 + (He * beta2 * v) ** 2
+        Tau = muk * N
+        tC2 = (Tau * u / speed) ** 2 + (Tau * v / speed) ** 2
+        return np.where(tC2 < tW2, 0.0, out)
+    if law in ("Joughin", "rCW-V0"):
+        U = speed
+        return (U ** (1.0 / m - 1) * He * (U + V0) ** (-1.0 / m) * (C + C0) ** (-1.0 / m - 1)) / m
+    raise ValueError("BasalDrag:InvalidCase inversion for C with this sliding law is not implemented")
+
+
+def dIdCq(p: Params, mua: MUA, F: Fields, uAdjoint, vAdjoint):
+    """dIdCq.m:1-163 (before the logC scaling and the pre-multiplier): the nodal integral
+    int dFuvdC (u uAdj + v vAdj) N_I, with He from the interpolated nodal flotation thickness."""
+    conn = mua.connectivity
+    G = lambda a: np.asarray(a, dtype=float)[conn]
+    hnod, unod, vnod, Cnod, mnod = G(F.h), G(F.ub), G(F.vb), G(F.C), G(F.m)
+    qnod = G(F.q) if (p.SlidingLaw in ("Budd", "W-N0") and F.q is not None) else mnod * 0
+    muknod = G(F.muk) if F.muk is not None else mnod * 0
+    V0nod = G(F.V0) if F.V0 is not None else mnod * 0
+    Bnod, Snod, rhonod = G(F.B), G(F.S), G(F.rho)
+    hfnod = F.rhow * (Snod - Bnod) / rhonod
+    uAn, vAn = G(uAdjoint), G(vAdjoint)
+    T = np.zeros((mua.Nele, mua.nod))
+    for Iint in range(mua.nip):
+        fun = shape_fun(mua.nod, mua.points[Iint])
+        detJ = mua.DetJ[:, Iint]
+        hint, uint, vint = hnod @ fun, unod @ fun, vnod @ fun
+        Cint = Cnod @ fun
+        Cint = np.where(Cint < p.Cmin, p.Cmin, Cint)
+        mint, qint, mukint, V0int = mnod @ fun, qnod @ fun, muknod @ fun, V0nod @ fun
+        Bint, Sint = Bnod @ fun, Snod @ fun
+        Hint = Sint - Bint
+        rhoint = rhonod @ fun
+        uAi, vAi = uAn @ fun, vAn @ fun
+        hfint = hfnod @ fun
+        Heint = heaviside_approx(p.kH, hint - hfint, p.Hh0)
+        Ctemp = dFuvdC(p, Heint, hint, Hint, rhoint, F.rhow, F.g, uint, vint, Cint, mint, qint, mukint, V0int)
+        detJw = detJ * mua.weights[Iint]
+        for I in range(mua.nod):
+            T[:, I] += Ctemp * (uint * uAi + vint * vAi) * fun[I] * detJw
+    return np.bincount(conn.ravel(order="F"), weights=T.ravel(order="F"), minlength=mua.Nnodes)
+
+
+def adjoint_gradient_C(p: Params, mua: MUA, F: Fields, bcs_adjoint: BCs, us, vs, usErr, vsErr, logC=True,
+                       premultiplier="M"):
+    """The adjoint gradient of the "-uv-" misfit with respect to C at the solved state F
+    (Misfit.m:160-260): the last Newton tangent K at (ub, vb), the adjoint system
+    [K L'; L 0][lambda; mu] = [dI/duv; 0] with L of the adjoint BCs (solveKApeSymmetric),
+    dIdCq at lambda, log(10) C dIdC for "logC" (dIdCq.m:153-156), and (M/Area)\\dIdC for the
+    pre-multiplier "M" (ApplyAdjointGradientPreMultiplier.m).  Returns (I, dIduv, lambda, dIdC)."""
+    Fp = prepare_fields(p, F)
+    _, K = uv_matrix_assembly(p, mua, Fp)
+    M = mass_matrix(mua)
+    I, dIduv = misfit_uv(mua, Fp, us, vs, usErr, vsErr, M)
+    L, c = create_Luv(mua.Nnodes, bcs_adjoint)
+    lam, _ = abfg_pre_eliminate(K, L, dIduv, np.zeros(0 if c is None else c.size))
+    N = mua.Nnodes
+    g = dIdCq(p, mua, Fp, lam[:N], lam[N:2 * N])
+    if logC:
+        g = math.log(10) * Fp.C * g
+    if premultiplier == "M":
+        g = spla.spsolve((M / mesh_area(mua)).tocsc(), g)
+    return I, dIduv, lam, g

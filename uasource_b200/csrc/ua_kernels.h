@@ -45,6 +45,30 @@ struct UvhPhys {
   int tau_kind;           // 0 taus, 1 taut, 2 tau1, 3 tau2
 };
 
+// Inputs of the adjoint gradient assembly (dIdCq.m): nodal fields, the state and the adjoint
+// velocities, all indexed by global node (q, muk, V0 null where the law does not use them).
+struct AdjIn {
+  const double *h, *S, *B, *rho, *C, *m, *q, *muk, *V0;
+  const double *u, *v;
+  const double *uA, *vA;
+  double rhow, g;
+};
+
+cudaError_t adj_mass_matrix(const ua_mesh* m, double* Mval);
+cudaError_t adj_dIdC(const ua_mesh* m, const UvPhys& P, const AdjIn& in, double* out);
+cudaError_t adj_node_spmv(const ua_mesh* m, const int* nodeptr, const int* nodecol, const double* A,
+                          const double* x, double* y);
+cudaError_t adj_misfit(const ua_mesh* m, const double* u, const double* v, const double* us, const double* vs,
+                       const double* ue, const double* ve, double* ru, double* rv);
+cudaError_t adj_misfit_grad(const ua_mesh* m, const double* Mru, const double* Mrv, const double* ue,
+                            const double* ve, double area, double* f);
+cudaError_t adj_logc(const ua_mesh* m, const double* C, double* g);
+cudaError_t adj_dot(cudaStream_t st, int n, const double* a, const double* b, double* part, double* out, int slot);
+int adj_cg(const ua_mesh* m, const int* nodeptr, const int* nodecol, const double* A, const double* b, double* x,
+           double rtol, int maxit, double* work, double* h_sc);
+cudaError_t adj_scale(const ua_mesh* m, double s, double* x);
+constexpr int kAdjDotBlocks = 256;  // block partials of the adjoint's dot products
+
 size_t uv_patch_smem(int nod, bool withK, bool fp32, int E);
 size_t uvh_patch_smem(int nod, bool withK, bool fp32, int E);
 int uvh_fields_per_node();

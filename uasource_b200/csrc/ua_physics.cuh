@@ -243,6 +243,53 @@ __device__ inline Drag basal_drag_general(const UvPhys& P, double He, double del
   return d;
 }
 
+// BasalDrag.m:80-160 (CtrlVar.Inverse.dFuvdClambda): the derivative with respect to C of the drag
+// magnitude over speed, per sliding law, as the adjoint gradient dIdCq.m uses it.  Budd takes
+// N = rho g max(h - hf, 0) without Nzero (:120-126); Tsai is the Weertman term where the Weertman
+// stress is the smaller one and 0 where Coulomb applies (:137-147).  Coulomb has none (the host
+// refuses it).
+__device__ inline double dFuvdC(const UvPhys& P, double He, double h, double H, double rho, double rhow, double g,
+                                double u, double v, double C, double m, double q, double muk, double V0) {
+  const double eps = 2.220446049250313e-16;
+  if (He < 0) He = 0;
+  const double C0 = P.Czero, u0 = P.SpeedZero;
+  const double speed = sqrt(u * u + v * v + u0 * u0);
+  const double Um = pow(speed, 1.0 / m - 1);
+  double N = 0, dNdh = 0, Dh = 0;
+  switch (P.law) {
+    case UA_SLIDING_BUDD: {
+      double hf = rhow * H / rho;
+      if (hf < eps) hf = 0;
+      double D = h - hf;
+      if (D < eps) D = 0;
+      const double Nb = rho * g * D;
+      return He * pow(Nb, q / m) * (1.0 / m) * pow(C + C0, -1.0 / m - 1) * Um;
+    }
+    case UA_SLIDING_CORNFORD:
+      effective_pressure_n0(P, h, H, rho, rhow, g, N, dNdh, Dh);
+      return (pow(speed, 1.0 / m - 1) * pow(muk, m + 1) * pow(N, m + 1) * He *
+              pow(pow(muk, m) * pow(N, m) + speed * pow(He * pow(C + C0, -1.0 / m), m), -1.0 / m - 1) *
+              pow(C + C0, -1.0 / m - 1)) / m;
+    case UA_SLIDING_UMBI: {
+      effective_pressure_n0(P, h, H, rho, rhow, g, N, dNdh, Dh);
+      const double den = pow(speed, 1.0 / m) * He + muk * N * pow(C + C0, 1.0 / m);
+      return (pow(speed, 1.0 / m) * muk * muk * N * N * He / (den * den) * pow(C + C0, 1.0 / m - 1)) / (speed * m);
+    }
+    case UA_SLIDING_TSAI: {
+      effective_pressure_n0(P, h, H, rho, rhow, g, N, dNdh, Dh);
+      const double beta2 = pow(C + C0, -1.0 / m) * Um;
+      const double tw2 = (He * beta2 * u) * (He * beta2 * u) + (He * beta2 * v) * (He * beta2 * v);
+      const double Tau = muk * N;
+      const double tc2 = (Tau * u / speed) * (Tau * u / speed) + (Tau * v / speed) * (Tau * v / speed);
+      return tc2 < tw2 ? 0.0 : He * (1.0 / m) * pow(C + C0, -1.0 / m - 1) * Um;
+    }
+    case UA_SLIDING_JOUGHIN:
+      return (pow(speed, 1.0 / m - 1) * He * pow(speed + V0, -1.0 / m) * pow(C + C0, -1.0 / m - 1)) / m;
+    default:
+      return He * (1.0 / m) * pow(C + C0, -1.0 / m - 1) * Um;
+  }
+}
+
 // Interpolated sliding-law fields at an integration point (nodal values times N).
 template <int NOD>
 __device__ __forceinline__ DragIp drag_interp(const DragFields& F, const int (&gn)[NOD], const double* N) {

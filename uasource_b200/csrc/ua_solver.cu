@@ -82,6 +82,9 @@ struct Work {
   // on first use, dragf[k] = dragbuf[k] while the configured law reads field k, else null
   double* dragbuf[11] = {};
   const double* dragf[11] = {};
+  // adjoint gradient work (mass matrix values, measurements, misfit and CG vectors)
+  double* adj_buf = nullptr;
+  size_t adj_cap = 0;
   // dof vectors
   double *X, *X0, *dX, *R, *frhs, *Tint, *Fext;
   double* Kd = nullptr;
@@ -3243,6 +3246,116 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
   }
   view.work = nullptr;
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint gradient of the velocity misfit with respect to C (Misfit.m adjoint
+// branch with "-uv-" data, dIdCq.m, ApplyAdjointGradientPreMultiplier.m).
+// ---------------------------------------------------------------------------
+extern "C" int ua_uv_adjoint_dIdC(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs_adjoint,
+                                  const ua_measurements* meas, int32_t flags, double* I, double* dIduv,
+                                  double* lambda, double* dIdC, int32_t* krylov_its) {
+  if (!m || !p || !F || !meas) return set_error(UA_ERR_INVALID, "ua_uv_adjoint_dIdC: null argument");
+  if (m->ndof != 2 || m->dm.nsys != 1)
+    return set_error(UA_ERR_INVALID, "ua_uv_adjoint_dIdC takes a single-mesh uv (ndof=2) handle");
+  if (!meas->us || !meas->vs || !meas->usErr || !meas->vsErr)
+    return set_error(UA_ERR_INVALID, "Misfit:us Meas.us, Meas.vs and their errors are required for -uv- data");
+  if (p->SlidingLaw == UA_SLIDING_COULOMB)
+    return set_error(UA_ERR_INVALID, "BasalDrag:InvalidCase inversion for C with the Coulomb sliding law is not "
+                                     "implemented");
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  ua_params q = *p;  // the adjoint runs in FP64 at a fixed inner tolerance
+  q.precision = UA_PREC_FP64;
+  q.krylov_adaptive = 0;
+  int rc;
+  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_K(m, UA_PREC_FP64))) return rc;
+  if ((rc = upload_fields(m, &q, F, 1))) return rc;
+  if ((rc = upload_velocity(m, F, 1))) return rc;
+  if ((rc = build_constraints(m, bcs_adjoint, 1))) return rc;
+  Work* w = m->work;
+  const int nn = m->nn_total, N = m->ndof_total;
+  const size_t nnzn = m->h_nodeptr.empty() ? 0 : (size_t)m->h_nodeptr.back();
+  const size_t need = nnzn + 18 * (size_t)nn + 2 * (size_t)N + kAdjDotBlocks + 16;
+  if (w->adj_cap < need) {
+    w->adj_buf = walloc<double>(m, need);
+    if (!w->adj_buf) return set_error(UA_ERR_OOM, "device allocation of the adjoint work failed");
+    w->adj_cap = need;
+  }
+  double* Mval = w->adj_buf;
+  double *us = Mval + nnzn, *vs = us + nn, *ue = vs + nn, *ve = ue + nn;
+  double *ru = ve + nn, *rv = ru + nn, *Mru = rv + nn, *Mrv = Mru + nn, *gv = Mrv + nn, *gout = gv + nn;
+  double* cgw = gout + nn;       // 6 nn + kAdjDotBlocks + 8
+  double* xsave = cgw + 6 * (size_t)nn + kAdjDotBlocks + 8;  // N
+  double* sc = cgw + 6 * (size_t)nn + kAdjDotBlocks;        // dot results (slots used here: 0, 1)
+  const double* src[4] = {meas->us, meas->vs, meas->usErr, meas->vsErr};
+  double* dst[4] = {us, vs, ue, ve};
+  for (int k = 0; k < 4; ++k)
+    UA_CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], nn * sizeof(double),
+                                F->location == UA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                m->stream));
+  // total area (CreateMUA.m:97-98): TriAreaFE over the corner nodes
+  double area = 0.0;
+  {
+    const HostSystem& hs = m->sys[0];
+    const int c1 = m->nod == 3 ? 1 : 2, c2 = m->nod == 3 ? 2 : 4;
+    for (int e = 0; e < hs.ne; ++e) {
+      const int a = hs.conn[e], b = hs.conn[(size_t)c1 * hs.ne + e], c = hs.conn[(size_t)c2 * hs.ne + e];
+      area += 0.5 * std::fabs((hs.x[a] - hs.x[c]) * (hs.y[b] - hs.y[a]) - (hs.x[a] - hs.x[b]) * (hs.y[c] - hs.y[a]));
+    }
+  }
+  // K at the state (the last Newton tangent the reference reuses as dfuv)
+  std::vector<int> sel(1, 1);
+  if ((rc = set_sel(m, sel))) return rc;
+  if ((rc = assemble(m, &q, true, false, w->X, false))) return rc;
+  // misfit and its gradient (Misfit.m:56-63, :117-120)
+  UA_CUDA_TRY(adj_mass_matrix(m, Mval));
+  UA_CUDA_TRY(adj_misfit(m, w->X, w->X + nn, us, vs, ue, ve, ru, rv));
+  UA_CUDA_TRY(adj_node_spmv(m, m->dm.nodeptr, m->dm.nodecol, Mval, ru, Mru));
+  UA_CUDA_TRY(adj_node_spmv(m, m->dm.nodeptr, m->dm.nodecol, Mval, rv, Mrv));
+  UA_CUDA_TRY(adj_dot(m->stream, nn, ru, Mru, cgw + 6 * (size_t)nn, sc, 0));
+  UA_CUDA_TRY(adj_dot(m->stream, nn, rv, Mrv, cgw + 6 * (size_t)nn, sc, 1));
+  UA_CUDA_TRY(adj_misfit_grad(m, Mru, Mrv, ue, ve, area, w->frhs));
+  g_launches += 8;
+  double hs2[2];
+  UA_CUDA_TRY(cudaMemcpyAsync(hs2, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  // adjoint solve [K L'; L 0][lambda; mu] = [dI/duv; c] (Misfit.m:182-187): the constrained PCG
+  // takes dX_c = c - X_c on the constrained dofs, so X is parked at zero for the solve
+  UA_CUDA_TRY(cudaMemcpyAsync(xsave, w->X, N * sizeof(double), cudaMemcpyDeviceToDevice, m->stream));
+  UA_CUDA_TRY(cudaMemsetAsync(w->X, 0, N * sizeof(double), m->stream));
+  std::vector<int> its(1, 1);
+  rc = pcg_t<double, double>(m, &q, w->Kd, its.data(), nullptr);
+  UA_CUDA_TRY(cudaMemcpyAsync(w->X, xsave, N * sizeof(double), cudaMemcpyDeviceToDevice, m->stream));
+  if (rc) return rc;
+  int status = 0;
+  UA_CUDA_TRY(cudaMemcpyAsync(&status, w->status, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  if (status) return set_error(UA_ERR_KRYLOV, "adjoint PCG breakdown: K is not positive definite on the free dofs");
+  if (krylov_its) *krylov_its = its[0];
+  if (I) *I = (hs2[0] + hs2[1]) / 2 / area;
+  // dIdCq.m: the gradient assembly at (u, v, lambda)
+  AdjIn in{w->h, w->S, w->B, w->rho, w->C, w->m, w->dragf[0], w->dragf[1], w->dragf[2],
+           w->X, w->X + nn, w->dX, w->dX + nn, F->rhow, F->g};
+  UA_CUDA_TRY(adj_dIdC(m, make_phys(&q), in, gv));
+  ++g_launches;
+  if (flags & UA_ADJ_LOGC) {
+    UA_CUDA_TRY(adj_logc(m, w->C, gv));
+    ++g_launches;
+  }
+  double* g = gv;
+  if (flags & UA_ADJ_PREMUL_M) {  // (M/Area)\dIdC = Area (M\dIdC)
+    double hsc[1];
+    const int cits = adj_cg(m, m->dm.nodeptr, m->dm.nodecol, Mval, gv, gout, 1e-14, 20 * 1000, cgw, hsc);
+    if (cits == -2) return set_error(UA_ERR_CUDA, "mass-matrix solve failed");
+    if (cits == -1) return set_error(UA_ERR_KRYLOV, "mass-matrix CG reached its iteration cap");
+    UA_CUDA_TRY(adj_scale(m, area, gout));
+    g = gout;
+  }
+  if (dIduv) UA_CUDA_TRY(cudaMemcpyAsync(dIduv, w->frhs, N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (lambda) UA_CUDA_TRY(cudaMemcpyAsync(lambda, w->dX, N * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if (dIdC) UA_CUDA_TRY(cudaMemcpyAsync(dIdC, g, nn * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return UA_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -24,6 +24,7 @@ UA_ERR_KRYLOV = -8
 UA_ERR_NO_DEVICE = -9
 
 UA_PREC_FP64 = 0
+UA_ADJ_LOGC, UA_ADJ_PREMUL_M = 1, 2
 UA_SLIDING_WEERTMAN, UA_SLIDING_BUDD, UA_SLIDING_TSAI, UA_SLIDING_COULOMB = 0, 1, 2, 3
 UA_SLIDING_CORNFORD, UA_SLIDING_UMBI, UA_SLIDING_JOUGHIN = 4, 5, 6
 # CtrlVar.SlidingLaw names (Ua2D_DefaultParameters.m:172) -> UA_SLIDING_*
@@ -100,6 +101,10 @@ class ua_fields(C.Structure):
                 ("ma", _dp)]
 
 
+class ua_measurements(C.Structure):
+    _fields_ = [("us", _dp), ("vs", _dp), ("usErr", _dp), ("vsErr", _dp)]
+
+
 class ua_bcs(C.Structure):
     _fields_ = [("n_ufixed", C.c_int32), ("ufixed_node", _ip), ("ufixed_value", _dp),
                 ("n_vfixed", C.c_int32), ("vfixed_node", _ip), ("vfixed_value", _dp),
@@ -162,6 +167,8 @@ SIGNATURES = {
     "ua_mem_info": (C.c_int, [C.c_int32, _lp, _lp]),
     "ua_constraint_count": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), C.c_int32, _ip]),
     "ua_constraint_matrix": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), _ip, _ip, _dp, _dp]),
+    "ua_uv_adjoint_dIdC": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),
+                                     C.POINTER(ua_measurements), C.c_int32, _dp, _dp, _dp, _dp, _ip]),
     "ua_solve_kape_symmetric": (C.c_int, [C.c_int32, _lp, _lp, _dp, C.c_int32, _lp, _lp, _dp, _dp, _dp, _dp, _dp,
                                           C.c_double, C.c_int32, _ip, C.c_int32]),
     "ua_solve_kape_symmetric_noalloc": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,

@@ -599,6 +599,31 @@ def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None, r
     return Fo, lam, _report(rep, recs, upd)
 
 
+def adjoint_gradient_C(ctrl: CtrlVar, mua: MUA, F: Fields, bcs_adjoint: BCs, us, vs, usErr, vsErr, logC=True,
+                       premultiplier="M"):
+    """Adjoint gradient of the "-uv-" velocity misfit with respect to C at the solved state F
+    (Misfit.m adjoint branch -> solveKApeSymmetric -> dIdCq.m -> ApplyAdjointGradientPreMultiplier.m)
+    on the GPU.  ``logC``: the gradient with respect to log10(C); ``premultiplier`` "M" or "I"
+    (CtrlVar.Inverse.AdjointGradientPreMultiplier).  Returns (I, dIduv, lambda, dIdC, krylov_its)
+    with lambda = [uAdjoint; vAdjoint]."""
+    if premultiplier not in ("M", "I"):
+        raise ValueError("AdjointGradientPreMultiplier must be 'M' or 'I'")
+    lib = L.load()
+    keep = _Keep()
+    Nn = mua.Nnodes()
+    cf, _, _ = _c_fields(F, keep, Nn)
+    cb = _c_bcs(bcs_adjoint, keep)
+    p = ctrl.to_c()
+    ms = L.ua_measurements(keep.d(us), keep.d(vs), keep.d(usErr), keep.d(vsErr))
+    flags = (L.UA_ADJ_LOGC if logC else 0) | (L.UA_ADJ_PREMUL_M if premultiplier == "M" else 0)
+    I = C.c_double()
+    its = C.c_int32()
+    dIduv = np.zeros(2 * Nn); lam = np.zeros(2 * Nn); g = np.zeros(Nn)
+    L.check(lib.ua_uv_adjoint_dIdC(mua.handle, C.byref(p), C.byref(cf), C.byref(cb), C.byref(ms), flags,
+                                   C.byref(I), L.dptr(dIduv), L.dptr(lam), L.dptr(g), C.byref(its)))
+    return I.value, dIduv, lam, g, its.value
+
+
 def solveKApeSymmetric(A, B, f, g, rtol=1e-12, maxit=0, device=0):
     """solveKApeSymmetric.m -> ABfgPreEliminate.m for SPD A and selection-type B.
 
