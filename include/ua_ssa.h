@@ -155,6 +155,12 @@ typedef struct ua_params {
     double Nzero;              /* lower value of the effective pressure (:445) */
     int32_t IncludeMelangeModelPhysics;  /* ocean and atmosphere drag on floating ice (BasalDrag.m:275-343);
                                             needs F.uo, vo, Co, mo, ua, va, Ca, ma */
+    /* active-set minimum-thickness constraints of the implicit uvh step (uvh.m:64-212) */
+    int32_t ThicknessConstraints;        /* :1478 (1 = active-set method, the default) */
+    double ThickMin;                     /* :1469 */
+    int32_t ThicknessConstraintsItMax;   /* :1479 */
+    int32_t MaxNumberOfNewlyIntroducedActiveThicknessConstraints;  /* :1500 */
+    int32_t MinNumberOfNewlyIntroducedActiveThicknessConstraints;  /* :1502 */
 } ua_params;
 
 /* Nodal fields F (UaFields.m).  Scalars rhow, g, alpha are F.rhow, F.g, F.alpha. */
@@ -181,6 +187,8 @@ typedef struct ua_bcs {
     int32_t n_utied;  const int32_t* utied_a; const int32_t* utied_b;
     int32_t n_vtied;  const int32_t* vtied_a; const int32_t* vtied_b;
     int32_t n_hfixed; const int32_t* hfixed_node; const double* hfixed_value;
+    int32_t n_hpos; const int32_t* hpos_node;  /* BCs.hPosNode: the active minimum-thickness set on entry
+                                                  (the previous step's, may be empty) */
 } ua_bcs;
 
 /* One Newton iteration (the SSTREAM2dNR2.m:386-387 log line). */
@@ -218,6 +226,13 @@ typedef struct ua_newton_report {
      * else the call returns UA_ERR_INVALID.  Filled for the first iters_capacity iterations. */
     double* updates;
     int64_t update_stride;
+    /* uvh active set (RunInfo.Forward.uvhActiveSet*, uvh.m:205-207) */
+    int32_t active_set_iterations;   /* uvhActiveSetIterations */
+    int32_t active_set_cyclical;     /* uvhActiveSetCyclical */
+    int32_t active_set_converged;    /* ActiveSetConverged (0 when ThicknessConstraintsItMax was reached) */
+    int32_t n_hpos;                  /* uvhActiveSetConstraints: the size of the final active set */
+    int32_t hpos_capacity;           /* capacity of hpos_node */
+    int32_t* hpos_node;              /* caller-owned, may be NULL: the final BCs1.hPosNode (0-based) */
 } ua_newton_report;
 
 /* --------------------------------------------------------------------- */
@@ -290,8 +305,15 @@ int ua_uv_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fields, const 
 int ua_uvh_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, int32_t mode,
                     double* R, double* Kvals, double* Tint, double* Fext);
 
-/* Implicit uvh step: SSTREAM_TransientImplicit.m:6-717 (via uvh.m:45 ->
- * uvh2D.m:20, no active-set thickness constraints).  F->ub, vb, h1: start
+/* Implicit uvh step: uvh.m:5-222 -> uvh2D.m:20 -> SSTREAM_TransientImplicit.m:6-717.  With
+ * p->ThicknessConstraints the step runs inside the active-set loop of uvh.m:64-212
+ * (ActiveSetInitialisation.m, ActiveSetUpdate.m): nodes with h < ThickMin are fixed at ThickMin,
+ * constraints whose mass-flux reaction -Reactions.h/(rho dt) is negative are released
+ * (CalculateReactions.m: Reactions.h = M \ Lh' l.h), until the set is unchanged, cyclical or
+ * ThicknessConstraintsItMax iterations have run; bcs->hpos_node is the set on entry and
+ * rep->hpos_node receives the final one.  A step that does not converge is reported as
+ * UA_ERR_NOT_CONVERGED (the reference's time-step reduction of uvh2NotConvergent.m is the
+ * caller's).  F->ub, vb, h1: start
  * values in, solution out.  luvh: [l.ubvb; l.h] in/out (may be NULL).  The
  * inner solve on the constrained unsymmetric system is restarted GMRES(m)
  * (m = krylov_restart) or BiCGStab (uvh_krylov), right-preconditioned by the

@@ -257,6 +257,11 @@ class Params:
     uvhExitBackTrackingStepLength: float = 1e-3                    # :502
     uvhAcceptableWorkAndForceTolerances: tuple = (math.inf, 1e-6)  # :504
     uvhAcceptableWorkOrForceTolerances: tuple = (1.0, 1e-8)        # :505
+    ThicknessConstraints: int = 1                  # :1478 (active-set method)
+    ThickMin: float = 1.0                          # :1469
+    ThicknessConstraintsItMax: int = 10            # :1479
+    MaxNumberOfNewlyIntroducedActiveThicknessConstraints: int = 1000  # :1500
+    MinNumberOfNewlyIntroducedActiveThicknessConstraints: int = 0     # :1502
     ModifiedNRuvhIntervalCriterion: int = 1        # :584
     ModifiedNRuvhReductionCriterion: float = 0.5   # :585
     NLtol: float = 1e-15             # BackTracking.m:125-127 default
@@ -1790,3 +1795,113 @@ def adjoint_gradient_C(p: Params, mua: MUA, F: Fields, bcs_adjoint: BCs, us, vs,
     if premultiplier == "M":
         g = spla.spsolve((M / mesh_area(mua)).tocsc(), g)
     return I, dIduv, lam, g
+
+
+# ---------------------------------------------------------------------------
+# uvh active-set thickness constraints — uvh.m:64-212, ActiveSetInitialisation.m,
+# ActiveSetUpdate.m, CalculateReactions.m
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class ActiveSetResult:
+    res: UvhResult
+    hPosNode: np.ndarray
+    iterations: int
+    cyclical: bool
+    converged: bool
+
+
+def _setdiff(a, b):
+    """MATLAB setdiff: the sorted unique values of a that are not in b."""
+    return np.setdiff1d(np.asarray(a, dtype=np.int64), np.asarray(b, dtype=np.int64))
+
+
+def uvh_active_set(p: Params, mua: MUA, bcs: BCs, F: Fields, S0: UvhState, S1: UvhState, dt, hPosNode=None,
+                   solver=None):
+    """uvh.m:64-212: the implicit step with the active set of minimum-thickness constraints.
+
+    hPos constraints fix h = ThickMin at their nodes (rows appended after the fixed-h rows,
+    createLh.m).  After each solve, constraints whose mass-flux reaction
+    ah = -Reactions.h/(rho dt) is negative are released (Reactions.h = M^-1 Lh' l.h,
+    CalculateReactions.m) and nodes with h < ThickMin are activated (at most
+    MaxNumberOfNewlyIntroducedActiveThicknessConstraints, the thinnest ones); the loop ends when
+    the set is unchanged, cyclical, or after ThicknessConstraintsItMax iterations.
+    """
+    hfixed = np.asarray(bcs.hFixedNode, dtype=np.int64)
+    hfixv = np.asarray(bcs.hFixedValue, dtype=float)
+    tmin = p.ThickMin
+    S1 = S1.copy()
+    # ActiveSetInitialisation.m
+    hpos = _setdiff([] if hPosNode is None else hPosNode, hfixed)
+    last_active = hpos.copy()
+    if np.min(S1.h) > 1.1 * tmin:
+        hpos = np.zeros(0, np.int64)
+    if hpos.size == 0:
+        hpos = _setdiff(np.flatnonzero(S1.h < tmin), hfixed)
+    deact = _setdiff(last_active, hpos)
+    act = _setdiff(hpos, last_active)
+    if (deact.size or act.size) and deact.size < p.MinNumberOfNewlyIntroducedActiveThicknessConstraints \
+            and act.size < p.MinNumberOfNewlyIntroducedActiveThicknessConstraints:
+        hpos, act, deact = last_active, np.zeros(0, np.int64), np.zeros(0, np.int64)
+    last_released, last_activated = deact, act
+    M = mass_matrix(mua)
+    it = 1
+    cyclical = False
+    as_converged = True
+    while True:
+        S1.h = S1.h.copy()
+        S1.h[hpos] = tmin
+        b = BCs(ubFixedNode=bcs.ubFixedNode, ubFixedValue=bcs.ubFixedValue, vbFixedNode=bcs.vbFixedNode,
+                vbFixedValue=bcs.vbFixedValue, hFixedNode=np.concatenate([hfixed, hpos]),
+                hFixedValue=np.concatenate([hfixv, np.full(hpos.size, tmin)]))
+        res = sstream_transient_implicit(p, mua, b, F, S0, S1, dt, solver=solver)
+        if not res.converged:
+            return ActiveSetResult(res, hpos, it, cyclical, False)
+        S1 = UvhState(res.h.copy(), res.ub, res.vb, S1.as_, S1.ab)
+        if np.any(S1.h[hpos] < tmin):
+            S1.h[hpos] = tmin
+        # ActiveSetUpdate.m
+        hpos = _setdiff(hpos, hfixed)
+        last_set = hpos.copy()
+        nuv = res.luvh.size - hfixed.size - last_set.size
+        lh = res.luvh[nuv:]
+        if hpos.size:
+            rhs = np.zeros(mua.Nnodes)
+            np.add.at(rhs, np.concatenate([hfixed, last_set]), lh)  # Lh' l.h (unit rows)
+            Rh = spla.spsolve(M.tocsc(), rhs)
+            ah = (-Rh / (F.rho * dt))[hpos]
+            isneg = ah < -0.0 * tmin / dt
+            newinactive = np.flatnonzero(isneg)
+            hpos = hpos[~isneg]
+        else:
+            newinactive = np.zeros(0, np.int64)
+        released = last_set[newinactive]
+        new_active = np.flatnonzero(S1.h < tmin)
+        new_active = _setdiff(_setdiff(_setdiff(new_active, hfixed), hpos), released)
+        if new_active.size > p.MaxNumberOfNewlyIntroducedActiveThicknessConstraints:
+            order = np.argsort(S1.h, kind="stable")
+            new_active = order[:p.MaxNumberOfNewlyIntroducedActiveThicknessConstraints]
+        if new_active.size:
+            hpos = np.concatenate([hpos, new_active])
+        deact = _setdiff(last_set, hpos)
+        act = _setdiff(hpos, last_set)
+        cyclical = False
+        if act.size or deact.size:
+            if np.setxor1d(act, last_released).size == 0 and np.setxor1d(deact, last_activated).size == 0:
+                cyclical = True
+        if cyclical:
+            hpos = np.concatenate([hpos, deact])
+        if (deact.size or act.size) and deact.size < p.MinNumberOfNewlyIntroducedActiveThicknessConstraints \
+                and act.size < p.MinNumberOfNewlyIntroducedActiveThicknessConstraints:
+            hpos, act, deact = last_set, np.zeros(0, np.int64), np.zeros(0, np.int64)
+        modified = np.setxor1d(hpos, last_set).size > 0
+        last_released, last_activated = deact, act
+        it += 1
+        if not modified or cyclical:
+            break
+        if it > p.ThicknessConstraintsItMax:
+            as_converged = False
+            break
+    res = UvhResult(S1.ub, S1.vb, S1.h, res.luvh, res.converged, res.iterations, res.records)
+    return ActiveSetResult(res, hpos, it - 1, cyclical, as_converged)

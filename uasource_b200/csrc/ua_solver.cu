@@ -10,6 +10,7 @@
 // one-CTA-per-system kernel adds the partials in a fixed order, so a
 // system's result does not depend on which other systems share the launch.
 #include <algorithm>
+#include <iterator>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -1450,11 +1451,15 @@ static void reset_report(ua_newton_report* r) {
   ua_newton_iter* it = r->iters;
   double* up = r->updates;
   const int64_t stride = r->update_stride;
+  int32_t* hp = r->hpos_node;
+  const int hcap = r->hpos_capacity;
   std::memset(r, 0, sizeof(*r));
   r->iters_capacity = cap;
   r->iters = it;
   r->updates = up;
   r->update_stride = stride;
+  r->hpos_node = hp;
+  r->hpos_capacity = hcap;
 }
 
 // A caller-owned update buffer must hold ndof*Nnodes + nl doubles per record.
@@ -2662,6 +2667,11 @@ extern "C" void ua_params_default(ua_params* p) {
   p->SlidingLaw = UA_SLIDING_WEERTMAN;  // :171
   p->Nzero = 1e-20;                     // :445
   p->IncludeMelangeModelPhysics = 0;
+  p->ThicknessConstraints = 1;          // :1478
+  p->ThickMin = 1.0;                    // :1469
+  p->ThicknessConstraintsItMax = 10;    // :1479
+  p->MaxNumberOfNewlyIntroducedActiveThicknessConstraints = 1000;  // :1500
+  p->MinNumberOfNewlyIntroducedActiveThicknessConstraints = 0;     // :1502
 }
 
 extern "C" int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs, int32_t mode,
@@ -3248,6 +3258,16 @@ extern "C" int ua_solve_kape_symmetric_noalloc(int32_t n, const int32_t* Arowptr
   return rc;
 }
 
+// Device work of the adjoint gradient and of the active-set reactions (mass matrix, vectors).
+static int ensure_adj_buf(ua_mesh* m, size_t need) {
+  Work* w = m->work;
+  if (w->adj_cap >= need) return UA_OK;
+  w->adj_buf = walloc<double>(m, need);
+  if (!w->adj_buf) return set_error(UA_ERR_OOM, "device allocation of the adjoint work failed");
+  w->adj_cap = need;
+  return UA_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint gradient of the velocity misfit with respect to C (Misfit.m adjoint
 // branch with "-uv-" data, dIdCq.m, ApplyAdjointGradientPreMultiplier.m).
@@ -3277,11 +3297,7 @@ extern "C" int ua_uv_adjoint_dIdC(ua_mesh* m, const ua_params* p, const ua_field
   const int nn = m->nn_total, N = m->ndof_total;
   const size_t nnzn = m->h_nodeptr.empty() ? 0 : (size_t)m->h_nodeptr.back();
   const size_t need = nnzn + 18 * (size_t)nn + 2 * (size_t)N + kAdjDotBlocks + 16;
-  if (w->adj_cap < need) {
-    w->adj_buf = walloc<double>(m, need);
-    if (!w->adj_buf) return set_error(UA_ERR_OOM, "device allocation of the adjoint work failed");
-    w->adj_cap = need;
-  }
+  if ((rc = ensure_adj_buf(m, need))) return rc;
   double* Mval = w->adj_buf;
   double *us = Mval + nnzn, *vs = us + nn, *ue = vs + nn, *ve = ue + nn;
   double *ru = ve + nn, *rv = ru + nn, *Mru = rv + nn, *Mrv = Mru + nn, *gv = Mrv + nn, *gout = gv + nn;
@@ -3450,10 +3466,168 @@ static int uvh_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs
   return all_conv ? UA_OK : UA_ERR_NOT_CONVERGED;
 }
 
+// Sorted-set helpers with MATLAB's setdiff/setxor semantics (sorted unique results).
+static std::vector<int> sorted_unique(std::vector<int> a) {
+  std::sort(a.begin(), a.end());
+  a.erase(std::unique(a.begin(), a.end()), a.end());
+  return a;
+}
+static std::vector<int> set_diff(const std::vector<int>& a, const std::vector<int>& b) {
+  std::vector<int> A = sorted_unique(a), B = sorted_unique(b), out;
+  std::set_difference(A.begin(), A.end(), B.begin(), B.end(), std::back_inserter(out));
+  return out;
+}
+static std::vector<int> set_xor(const std::vector<int>& a, const std::vector<int>& b) {
+  std::vector<int> A = sorted_unique(a), B = sorted_unique(b), out;
+  std::set_symmetric_difference(A.begin(), A.end(), B.begin(), B.end(), std::back_inserter(out));
+  return out;
+}
+
+// uvh.m:64-212: the implicit step inside the active-set loop of minimum-thickness constraints
+// (ActiveSetInitialisation.m, ActiveSetUpdate.m, CalculateReactions.m).  Host orchestration of
+// device solves; the sets follow MATLAB's sorted setdiff, and the reactions pair the h
+// multipliers with the re-sorted active set as CalculateReactions does.
+static int uvh_active_set(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs, ua_newton_report* rep,
+                          double* luvh, int32_t nl) {
+  if (F->location != UA_HOST) return set_error(UA_ERR_INVALID, "the uvh active set takes host fields");
+  if (!F->ub || !F->vb || !F->h1 || !F->rho) return set_error(UA_ERR_INVALID, "ua_uvh_newton: null field");
+  const int nn = m->sys[0].nn;
+  const double tmin = p->ThickMin, dt = F->dt;
+  std::vector<double> ub(F->ub, F->ub + nn), vb(F->vb, F->vb + nn), h(F->h1, F->h1 + nn), rho(F->rho, F->rho + nn);
+  std::vector<int> hfixed;
+  std::vector<double> hfixv;
+  for (int i = 0; bcs && i < bcs->n_hfixed; ++i) {
+    hfixed.push_back(bcs->hfixed_node[i]);
+    hfixv.push_back(bcs->hfixed_value ? bcs->hfixed_value[i] : 0.0);
+  }
+  std::vector<int> hpos_in;
+  for (int i = 0; bcs && i < bcs->n_hpos; ++i) {
+    const int k = bcs->hpos_node[i];
+    if (k < 0 || k >= nn) return set_error(UA_ERR_INVALID, "hPosNode index %d out of range", k);
+    hpos_in.push_back(k);
+  }
+  const int minnew = p->MinNumberOfNewlyIntroducedActiveThicknessConstraints;
+  // ActiveSetInitialisation.m
+  std::vector<int> hpos = set_diff(hpos_in, hfixed);
+  const std::vector<int> last_active0 = hpos;
+  if (*std::min_element(h.begin(), h.end()) > 1.1 * tmin) hpos.clear();
+  if (hpos.empty()) {
+    std::vector<int> thin;
+    for (int i = 0; i < nn; ++i)
+      if (h[i] < tmin) thin.push_back(i);
+    hpos = set_diff(thin, hfixed);
+  }
+  std::vector<int> deact = set_diff(last_active0, hpos), act = set_diff(hpos, last_active0);
+  if ((!deact.empty() || !act.empty()) && (int)deact.size() < minnew && (int)act.size() < minnew) {
+    hpos = last_active0; deact.clear(); act.clear();
+  }
+  std::vector<int> last_released = deact, last_activated = act;
+  // the consistent mass matrix for the reactions (MassMatrix2D1dof.m)
+  int rc;
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  if ((rc = ensure_work(m))) return rc;
+  const size_t nnzn = (size_t)m->h_nodeptr.back();
+  if ((rc = ensure_adj_buf(m, nnzn + 9 * (size_t)nn + kAdjDotBlocks + 16))) return rc;
+  double* Mval = m->work->adj_buf;
+  double *d_rhs = Mval + nnzn, *d_r = d_rhs + nn, *cgw = d_r + nn;
+  UA_CUDA_TRY(adj_mass_matrix(m, Mval));
+  int it = 1, max_newton = 0, kits = 0;
+  bool cyclical = false, as_conv = true;
+  std::vector<double> lam;
+  ua_fields f = *F;
+  f.ub = ub.data(); f.vb = vb.data(); f.h1 = h.data();
+  int solve_rc = UA_OK;
+  while (true) {
+    for (int k : hpos) h[k] = tmin;
+    std::vector<int> hf2 = hfixed;
+    std::vector<double> hv2 = hfixv;
+    for (int k : hpos) { hf2.push_back(k); hv2.push_back(tmin); }
+    ua_bcs b2{};
+    if (bcs) b2 = *bcs;
+    b2.n_hfixed = (int32_t)hf2.size(); b2.hfixed_node = hf2.data(); b2.hfixed_value = hv2.data();
+    b2.n_hpos = 0; b2.hpos_node = nullptr;
+    int32_t nc = 0;
+    if ((rc = ua_constraint_count(m, &b2, 3, &nc))) return rc;
+    lam.assign(std::max(nc, 1), 0.0);
+    std::vector<ua_newton_report*> reps(1, rep);
+    solve_rc = uvh_common(m, p, &f, &b2, 1, reps, lam.data(), nc);
+    if (rep) { max_newton = std::max(max_newton, rep->iterations); kits += rep->krylov_its_total; }
+    if (solve_rc == UA_ERR_NOT_CONVERGED) break;
+    if (solve_rc) return solve_rc;
+    for (int k : hpos)
+      if (h[k] < tmin) h[k] = tmin;
+    // ActiveSetUpdate.m
+    hpos = set_diff(hpos, hfixed);
+    const std::vector<int> last_set = hpos;
+    const int nuv = nc - (int)hf2.size();
+    std::vector<int> released;
+    if (!hpos.empty()) {
+      std::vector<double> rhs(nn, 0.0), r(nn, 0.0);
+      for (size_t k = 0; k < hfixed.size(); ++k) rhs[hfixed[k]] += lam[nuv + k];
+      for (size_t k = 0; k < last_set.size(); ++k) rhs[last_set[k]] += lam[nuv + hfixed.size() + k];
+      UA_CUDA_TRY(cudaMemcpyAsync(d_rhs, rhs.data(), nn * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+      double hsc[1];
+      const int cits = adj_cg(m, m->dm.nodeptr, m->dm.nodecol, Mval, d_rhs, d_r, 1e-14, 20000, cgw, hsc);
+      if (cits < 0) return set_error(UA_ERR_KRYLOV, "mass-matrix solve of the thickness reactions failed");
+      UA_CUDA_TRY(cudaMemcpyAsync(r.data(), d_r, nn * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+      UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+      std::vector<int> keep;
+      for (int k : hpos) {
+        const double ah = -r[k] / (rho[k] * dt);
+        if (ah < -0.0 * tmin / dt) released.push_back(k);
+        else keep.push_back(k);
+      }
+      hpos = keep;
+    }
+    std::vector<int> thin;
+    for (int i = 0; i < nn; ++i)
+      if (h[i] < tmin) thin.push_back(i);
+    std::vector<int> newact = set_diff(set_diff(set_diff(thin, hfixed), hpos), released);
+    const int maxnew = p->MaxNumberOfNewlyIntroducedActiveThicknessConstraints;
+    if ((int)newact.size() > maxnew) {
+      std::vector<int> order(nn);
+      for (int i = 0; i < nn; ++i) order[i] = i;
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h[a] < h[b]; });
+      newact.assign(order.begin(), order.begin() + maxnew);
+    }
+    hpos.insert(hpos.end(), newact.begin(), newact.end());
+    deact = set_diff(last_set, hpos);
+    act = set_diff(hpos, last_set);
+    cyclical = (!act.empty() || !deact.empty()) && set_xor(act, last_released).empty() &&
+               set_xor(deact, last_activated).empty();
+    if (cyclical) hpos.insert(hpos.end(), deact.begin(), deact.end());
+    if ((!deact.empty() || !act.empty()) && (int)deact.size() < minnew && (int)act.size() < minnew) {
+      hpos = last_set; deact.clear(); act.clear();
+    }
+    const bool modified = !set_xor(hpos, last_set).empty();
+    last_released = deact;
+    last_activated = act;
+    ++it;
+    if (!modified || cyclical) break;
+    if (it > p->ThicknessConstraintsItMax) { as_conv = false; break; }
+  }
+  std::memcpy(F->ub, ub.data(), nn * sizeof(double));
+  std::memcpy(F->vb, vb.data(), nn * sizeof(double));
+  std::memcpy(F->h1, h.data(), nn * sizeof(double));
+  if (luvh && nl == (int)lam.size()) std::memcpy(luvh, lam.data(), nl * sizeof(double));
+  if (rep) {
+    rep->iterations = max_newton;  // uvh.m:89-90: the largest Newton count of the active-set iterations
+    rep->krylov_its_total = kits;
+    rep->active_set_iterations = it - 1;
+    rep->active_set_cyclical = cyclical ? 1 : 0;
+    rep->active_set_converged = as_conv ? 1 : 0;
+    rep->n_hpos = (int32_t)hpos.size();
+    if (rep->hpos_node)
+      for (int k = 0; k < (int)hpos.size() && k < rep->hpos_capacity; ++k) rep->hpos_node[k] = hpos[k];
+  }
+  return solve_rc;
+}
+
 extern "C" int ua_uvh_newton(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs, double* luvh,
                              int32_t nl, ua_newton_report* rep) {
   if (!m || !p || !F) return set_error(UA_ERR_INVALID, "ua_uvh_newton: null argument");
   if (m->dm.nsys != 1) return set_error(UA_ERR_INVALID, "ua_uvh_newton takes a single-mesh handle");
+  if (p->ThicknessConstraints) return uvh_active_set(m, p, F, bcs, rep, luvh, nl);
   std::vector<ua_newton_report*> reps(1, rep);
   return uvh_common(m, p, F, bcs, 1, reps, luvh, nl);
 }

@@ -86,6 +86,9 @@ class ua_params(C.Structure):
         ("amg_smoothed", C.c_int32), ("krylov_full_grid", C.c_int32),
         ("uvh_h_sweeps", C.c_int32), ("krylov_sell", C.c_int32),
         ("SlidingLaw", C.c_int32), ("Nzero", C.c_double), ("IncludeMelangeModelPhysics", C.c_int32),
+        ("ThicknessConstraints", C.c_int32), ("ThickMin", C.c_double), ("ThicknessConstraintsItMax", C.c_int32),
+        ("MaxNumberOfNewlyIntroducedActiveThicknessConstraints", C.c_int32),
+        ("MinNumberOfNewlyIntroducedActiveThicknessConstraints", C.c_int32),
     ]
 
 
@@ -110,7 +113,8 @@ class ua_bcs(C.Structure):
                 ("n_vfixed", C.c_int32), ("vfixed_node", _ip), ("vfixed_value", _dp),
                 ("n_utied", C.c_int32), ("utied_a", _ip), ("utied_b", _ip),
                 ("n_vtied", C.c_int32), ("vtied_a", _ip), ("vtied_b", _ip),
-                ("n_hfixed", C.c_int32), ("hfixed_node", _ip), ("hfixed_value", _dp)]
+                ("n_hfixed", C.c_int32), ("hfixed_node", _ip), ("hfixed_value", _dp),
+                ("n_hpos", C.c_int32), ("hpos_node", _ip)]
 
 
 class ua_newton_iter(C.Structure):
@@ -131,7 +135,10 @@ class ua_newton_report(C.Structure):
                 ("gpu_launches", C.c_int32),
                 ("n_iter_records", C.c_int32), ("iters_capacity", C.c_int32),
                 ("iters", C.POINTER(ua_newton_iter)),
-                ("updates", C.POINTER(C.c_double)), ("update_stride", C.c_int64)]
+                ("updates", C.POINTER(C.c_double)), ("update_stride", C.c_int64),
+                ("active_set_iterations", C.c_int32), ("active_set_cyclical", C.c_int32),
+                ("active_set_converged", C.c_int32), ("n_hpos", C.c_int32), ("hpos_capacity", C.c_int32),
+                ("hpos_node", _ip)]
 
 
 # symbol -> (restype, argtypes); every function declared in include/ua_ssa.h

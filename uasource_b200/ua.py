@@ -89,6 +89,11 @@ class CtrlVar:
     SlidingLaw: str = "Weertman"          # any name of L.SLIDING_LAWS
     Nzero: float = 1e-20
     IncludeMelangeModelPhysics: int = 0
+    ThicknessConstraints: int = 1         # uvh active set (uvh.m:64-212)
+    ThickMin: float = 1.0
+    ThicknessConstraintsItMax: int = 10
+    MaxNumberOfNewlyIntroducedActiveThicknessConstraints: int = 1000
+    MinNumberOfNewlyIntroducedActiveThicknessConstraints: int = 0
 
     def set_force_tolerance(self, tol):
         """Set every uv force tolerance (desired and acceptable) to ``tol`` (rForce < tol)."""
@@ -399,6 +404,7 @@ class RunInfo:
     gpu_launches: int
     iters: list
     updates: np.ndarray = None  # per iteration gamma*[du; dv; (dh;) dl] when requested
+    active_set: dict = None     # uvh: iterations, cyclical, converged, hPosNode (the final active set)
 
 
 def _updates_buffer(rep, cap, stride):
@@ -560,9 +566,11 @@ def uvhAssembly(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, dt, Ronly=False
 
 @dataclass
 class HBCs(BCs):
-    """Velocity and thickness boundary conditions (0-based node indices)."""
+    """Velocity and thickness boundary conditions (0-based node indices); hPosNode is the active
+    minimum-thickness set carried from the previous step (BCs1.hPosNode)."""
     hFixedNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     hFixedValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    hPosNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
 
 
 def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None, return_updates=False):
@@ -582,6 +590,9 @@ def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None, r
     hn = getattr(bcs, "hFixedNode", None) if bcs is not None else None
     if hn is not None and len(hn):
         cb.n_hfixed = len(hn); cb.hfixed_node = keep.i(hn); cb.hfixed_value = keep.d(bcs.hFixedValue)
+    hp = getattr(bcs, "hPosNode", None) if bcs is not None else None
+    if hp is not None and len(hp):
+        cb.n_hpos = len(hp); cb.hpos_node = keep.i(hp)
     p = ctrl.to_c()
     nc = C.c_int32()
     L.check(lib.ua_constraint_count(mua.handle, C.byref(cb), 3, C.byref(nc)))
@@ -592,11 +603,19 @@ def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None, r
     rep.iters = C.cast(recs, C.POINTER(L.ua_newton_iter))
     rep.iters_capacity = cap
     upd = _updates_buffer(rep, cap, 3 * Nn + nc.value) if return_updates else None
+    hpos_out = np.zeros(Nn, np.int32)
+    rep.hpos_node = L.iptr(hpos_out)
+    rep.hpos_capacity = Nn
     rc = lib.ua_uvh_newton(mua.handle, C.byref(p), C.byref(cf), C.byref(cb), L.dptr(lam), len(lam), C.byref(rep))
     L.check(rc, allow=(L.UA_ERR_NOT_CONVERGED,))
     Fo = F1.copy()
     Fo.ub, Fo.vb, Fo.h = ub, vb, h1
-    return Fo, lam, _report(rep, recs, upd)
+    info = _report(rep, recs, upd)
+    if ctrl.ThicknessConstraints:
+        info.active_set = dict(iterations=rep.active_set_iterations, cyclical=bool(rep.active_set_cyclical),
+                               converged=bool(rep.active_set_converged),
+                               hPosNode=hpos_out[:rep.n_hpos].copy())
+    return Fo, lam, info
 
 
 def adjoint_gradient_C(ctrl: CtrlVar, mua: MUA, F: Fields, bcs_adjoint: BCs, us, vs, usErr, vsErr, logC=True,
