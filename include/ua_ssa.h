@@ -180,7 +180,11 @@ typedef struct ua_fields {
     const double *uo, *vo, *Co, *mo, *ua, *va, *Ca, *ma;
 } ua_fields;
 
-/* Boundary conditions (BCs2MLC.m, CreateLuv.m).  Index base as the mesh. */
+/* Boundary conditions (BCs2MLC.m, CreateLuv.m).  Index base as the mesh.  Fixed nodes, ties
+ * (u_A - u_B = 0) and fixed normal velocities become rows of L scaled to unit length (ScaleL.m);
+ * the rows must have disjoint support (every dof in at most one constraint), as
+ * ABfgPreEliminate.m requires, else UA_ERR_INVALID.  Ties and normal velocities are taken by the
+ * uv solves with the AMG preconditioner. */
 typedef struct ua_bcs {
     int32_t n_ufixed; const int32_t* ufixed_node; const double* ufixed_value;
     int32_t n_vfixed; const int32_t* vfixed_node; const double* vfixed_value;
@@ -189,6 +193,9 @@ typedef struct ua_bcs {
     int32_t n_hfixed; const int32_t* hfixed_node; const double* hfixed_value;
     int32_t n_hpos; const int32_t* hpos_node;  /* BCs.hPosNode: the active minimum-thickness set on entry
                                                   (the previous step's, may be empty) */
+    /* BCs.ubvbFixedNormalNode/Value: Nx u + Ny v = -value with the boundary's nodal normals
+       (CreateLuv.m:62-72, CalcEdgeAndNodalNormals.m; uv solves) */
+    int32_t n_normal; const int32_t* normal_node; const double* normal_value;
 } ua_bcs;
 
 /* One Newton iteration (the SSTREAM2dNR2.m:386-387 log line). */
@@ -372,12 +379,15 @@ int ua_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
 /* Number of rows of the constraint matrix L built from bcs (CreateLuv.m). */
 int ua_constraint_count(const ua_mesh* m, const ua_bcs* bcs, int32_t ndof, int32_t* nc);
 
-/* The constraint matrix L and right-hand side c of the fixed-node BCs of a single-mesh handle
+/* The constraint matrix L and right-hand side c of the BCs of a single-mesh handle
  * (AssembleLuvSSTREAM.m:2-40 -> BCs2MLC.m:19-29, CreateLuv.m:28-76, ScaleL.m:28-33; createLh.m
- * for fixed h on an ndof=3 handle): row k has its one non-zero L(k, dof[k]) = val[k] (0-based
- * dof in Úa order) and c(k) = rhs[k].  Rows in the order of the Lagrange multipliers: fixed u
- * nodes increasing, then fixed v nodes, then fixed h nodes as given.  This is the L that
- * SSTREAM2dNR2.m:3 returns as Lubvb.  Arrays may be NULL to query *nc only. */
+ * for fixed h on an ndof=3 handle).  Row k has at most two non-zeros: L(k, dof[2k]) = val[2k]
+ * and, for ties and normal velocities, L(k, dof[2k+1]) = val[2k+1] (dof[2k+1] = -1 and
+ * val[2k+1] = 0 for a one-entry row); dofs are 0-based in Úa order, rows scaled to unit length,
+ * c(k) = rhs[k].  Rows in the order of the Lagrange multipliers: u ties, v ties, fixed u nodes
+ * increasing, fixed v nodes, fixed normal velocities, fixed h nodes as given.  This is the L that
+ * SSTREAM2dNR2.m:3 returns as Lubvb.  dof and val hold 2*nc entries; arrays may be NULL to
+ * query *nc only. */
 int ua_constraint_matrix(const ua_mesh* m, const ua_bcs* bcs, int32_t* nc, int32_t* dof, double* val,
                          double* rhs);
 

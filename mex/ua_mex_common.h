@@ -254,10 +254,11 @@ static inline void ua_mex_drag_fields(const mxArray* F, size_t nn, ua_fields* f,
     }
 }
 
-/* The constraint matrix L (nc x ncols sparse, one unit entry per row; ScaleL.m) of the BCs b, as
- * AssembleLuvSSTREAM.m / AssembleLuvhSSTREAM.m build it, via ua_constraint_matrix. */
+/* The constraint matrix L (nc x ncols sparse, one or two entries per row, rows of unit length;
+ * ScaleL.m) of the BCs b, as AssembleLuvSSTREAM.m / AssembleLuvhSSTREAM.m build it, via
+ * ua_constraint_matrix. */
 static inline mxArray* ua_mex_constraint_L(ua_mesh* m, const ua_bcs* b, int32_t ncols) {
-    int32_t nc = 0, k;
+    int32_t nc = 0, k, e;
     int32_t* dof;
     double* val;
     mwIndex *jc, *ir, *cnt;
@@ -265,20 +266,22 @@ static inline mxArray* ua_mex_constraint_L(ua_mesh* m, const ua_bcs* b, int32_t 
     mxArray* L;
     int rc = ua_constraint_matrix(m, b, &nc, NULL, NULL, NULL);
     if (rc != UA_OK) ua_mex_fail(rc);
-    dof = (int32_t*)mxMalloc((nc > 0 ? nc : 1) * sizeof(int32_t));
-    val = (double*)mxMalloc((nc > 0 ? nc : 1) * sizeof(double));
+    dof = (int32_t*)mxMalloc((nc > 0 ? 2 * nc : 2) * sizeof(int32_t));
+    val = (double*)mxMalloc((nc > 0 ? 2 * nc : 2) * sizeof(double));
     rc = ua_constraint_matrix(m, b, &nc, dof, val, NULL);
     if (rc != UA_OK) ua_mex_fail(rc);
-    L = mxCreateSparse(nc, ncols, nc > 0 ? nc : 1, mxREAL);
+    L = mxCreateSparse(nc, ncols, nc > 0 ? 2 * nc : 1, mxREAL);
     jc = mxGetJc(L); ir = mxGetIr(L); pr = mxGetPr(L);
     cnt = (mwIndex*)mxCalloc(ncols + 1, sizeof(mwIndex));
-    for (k = 0; k < nc; ++k) cnt[dof[k] + 1]++;
+    for (e = 0; e < 2 * nc; ++e)
+        if (dof[e] >= 0) cnt[dof[e] + 1]++;
     for (k = 0; k < ncols; ++k) cnt[k + 1] += cnt[k];
     for (k = 0; k <= ncols; ++k) jc[k] = cnt[k];
-    for (k = 0; k < nc; ++k) {  /* rows in increasing order, so each column's rows come out sorted */
-        ir[cnt[dof[k]]] = (mwIndex)k;
-        pr[cnt[dof[k]]] = val[k];
-        cnt[dof[k]]++;
+    for (e = 0; e < 2 * nc; ++e) {  /* rows in increasing order, so each column's rows come out sorted */
+        if (dof[e] < 0) continue;
+        ir[cnt[dof[e]]] = (mwIndex)(e / 2);
+        pr[cnt[dof[e]]] = val[e];
+        cnt[dof[e]]++;
     }
     mxFree(cnt); mxFree(dof); mxFree(val);
     return L;
@@ -309,31 +312,41 @@ static inline int32_t* ua_mex_nodes(const mxArray* B, const char* name, int32_t*
     return out;
 }
 
-static inline const double* ua_mex_values(const mxArray* B, const char* name) {
+/* The values that go with n nodes: NULL (all zero) when the field is missing or empty, else
+ * exactly n of them. */
+static inline const double* ua_mex_values(const mxArray* B, const char* name, int32_t n) {
     const mxArray* f = ua_mex_field(B, name, 0);
-    return (f && !mxIsEmpty(f)) ? mxGetPr(f) : NULL;
+    if (!f || mxIsEmpty(f)) return NULL;
+    if ((int64_t)mxGetNumberOfElements(f) != n)
+        mexErrMsgIdAndTxt("Ua:mex:BCs", "%s has %d entries for %d nodes", name, (int)mxGetNumberOfElements(f), n);
+    return mxGetPr(f);
 }
 
 /* The mesh's 1-based BC lists.  The library takes 0-based indices for
  * index_base handles created from MATLAB too, so shift here. */
 static inline void ua_mex_bcs(const mxArray* B, ua_bcs* b) {
-    int32_t i;
+    int32_t i, n_ub = 0, n_vb = 0;
     memset(b, 0, sizeof(*b));
     if (!B || !mxIsStruct(B)) return;
     b->ufixed_node = ua_mex_nodes(B, "ubFixedNode", &b->n_ufixed);
-    b->ufixed_value = ua_mex_values(B, "ubFixedValue");
+    b->ufixed_value = ua_mex_values(B, "ubFixedValue", b->n_ufixed);
     b->vfixed_node = ua_mex_nodes(B, "vbFixedNode", &b->n_vfixed);
-    b->vfixed_value = ua_mex_values(B, "vbFixedValue");
+    b->vfixed_value = ua_mex_values(B, "vbFixedValue", b->n_vfixed);
     b->utied_a = ua_mex_nodes(B, "ubTiedNodeA", &b->n_utied);
-    b->utied_b = ua_mex_nodes(B, "ubTiedNodeB", &b->n_utied);
+    b->utied_b = ua_mex_nodes(B, "ubTiedNodeB", &n_ub);
     b->vtied_a = ua_mex_nodes(B, "vbTiedNodeA", &b->n_vtied);
-    b->vtied_b = ua_mex_nodes(B, "vbTiedNodeB", &b->n_vtied);
+    b->vtied_b = ua_mex_nodes(B, "vbTiedNodeB", &n_vb);
+    if (n_ub != b->n_utied || n_vb != b->n_vtied)  /* CreateLuv.m pairs A(k) with B(k) */
+        mexErrMsgIdAndTxt("Ua:mex:BCs", "ubTiedNodeA/B and vbTiedNodeA/B must have equal lengths");
     for (i = 0; i < b->n_ufixed; ++i) ((int32_t*)b->ufixed_node)[i] -= 1;
     for (i = 0; i < b->n_vfixed; ++i) ((int32_t*)b->vfixed_node)[i] -= 1;
     for (i = 0; i < b->n_utied; ++i) { ((int32_t*)b->utied_a)[i] -= 1; ((int32_t*)b->utied_b)[i] -= 1; }
     for (i = 0; i < b->n_vtied; ++i) { ((int32_t*)b->vtied_a)[i] -= 1; ((int32_t*)b->vtied_b)[i] -= 1; }
     b->hfixed_node = ua_mex_nodes(B, "hFixedNode", &b->n_hfixed);
-    b->hfixed_value = ua_mex_values(B, "hFixedValue");
+    b->hfixed_value = ua_mex_values(B, "hFixedValue", b->n_hfixed);
+    b->normal_node = ua_mex_nodes(B, "ubvbFixedNormalNode", &b->n_normal);
+    b->normal_value = ua_mex_values(B, "ubvbFixedNormalValue", b->n_normal);
+    for (i = 0; i < b->n_normal; ++i) ((int32_t*)b->normal_node)[i] -= 1;
     for (i = 0; i < b->n_hfixed; ++i) ((int32_t*)b->hfixed_node)[i] -= 1;
 }
 

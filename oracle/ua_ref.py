@@ -333,6 +333,8 @@ class BCs:
     vbTiedNodeB: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     hFixedNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     hFixedValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    ubvbFixedNormalNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    ubvbFixedNormalValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
 
 
 # ---------------------------------------------------------------------------
@@ -760,8 +762,55 @@ def structural_pattern(mua: MUA, ndof: int):
 # ---------------------------------------------------------------------------
 
 
-def create_Luv(Nnodes, bcs: BCs):
-    """BCs2MLC.m:19-29 + CreateLuv.m:28-76 + ScaleL.m:28-33 (ties, then fixed u, fixed v)."""
+def boundary_edges(connectivity, Nnodes):
+    """The boundary edges of the mesh (FindBoundary.m: the element edges that belong to one
+    element), each as [start, (mid,) end] in its element's node order."""
+    nod = connectivity.shape[1]
+    corners = [0, 1, 2] if nod == 3 else [0, 2, 4]
+    edges = []
+    for k in range(3):
+        a = connectivity[:, corners[k]]
+        b = connectivity[:, corners[(k + 1) % 3]]
+        if nod == 6:
+            edges.append(np.stack([a, connectivity[:, corners[k] + 1], b], axis=1))
+        else:
+            edges.append(np.stack([a, b], axis=1))
+    E = np.concatenate(edges)
+    key = np.minimum(E[:, 0], E[:, -1]) * Nnodes + np.maximum(E[:, 0], E[:, -1])
+    _, inv, cnt = np.unique(key, return_inverse=True, return_counts=True)
+    return E[cnt[inv] == 1]
+
+
+def nodal_normals(coordinates, connectivity):
+    """CalcEdgeAndNodalNormals.m:9-40: unit edge normals (-dy, dx)/l of the boundary edges and the
+    nodal normals (start node: the edge's normal, end node: plus the edge's normal, P2 mid node:
+    the mean of its two sub-edges), normalised.  Returns (Nx, Ny) over all nodes."""
+    Nn = coordinates.shape[0]
+    E = boundary_edges(connectivity, Nn)
+    nsub = E.shape[1] - 1
+    x, y = coordinates[:, 0], coordinates[:, 1]
+    nx = np.zeros((E.shape[0], nsub)); ny = np.zeros((E.shape[0], nsub))
+    for I in range(nsub):
+        dx = x[E[:, I + 1]] - x[E[:, I]]
+        dy = y[E[:, I + 1]] - y[E[:, I]]
+        l = np.sqrt(dy * dy + dx * dx)
+        nx[:, I] = -dy / l
+        ny[:, I] = dx / l
+    Nx = np.zeros(Nn); Ny = np.zeros(Nn)
+    Nx[E[:, 0]] = nx[:, 0]; Ny[E[:, 0]] = ny[:, 0]
+    Nx[E[:, -1]] = Nx[E[:, -1]] + nx[:, nsub - 1]
+    Ny[E[:, -1]] = Ny[E[:, -1]] + ny[:, nsub - 1]
+    for I in range(1, nsub):
+        Nx[E[:, I]] = Nx[E[:, I]] + (nx[:, I - 1] + nx[:, I]) / 2
+        Ny[E[:, I]] = Ny[E[:, I]] + (ny[:, I - 1] + ny[:, I]) / 2
+    with np.errstate(invalid="ignore", divide="ignore"):
+        l = np.sqrt(Nx * Nx + Ny * Ny)
+        return Nx / l, Ny / l
+
+
+def create_Luv(Nnodes, bcs: BCs, mua: MUA = None):
+    """BCs2MLC.m:19-29 + CreateLuv.m:28-76 + ScaleL.m:28-33 (u ties, v ties, fixed u, fixed v,
+    fixed normal velocities Nx u + Ny v = -value with the nodal normals of the mesh)."""
     ufn, ui = np.unique(bcs.ubFixedNode, return_index=True)
     ufv = np.asarray(bcs.ubFixedValue, dtype=float)[ui]
     vfn, vi = np.unique(bcs.vbFixedNode, return_index=True)
@@ -776,6 +825,10 @@ def create_Luv(Nnodes, bcs: BCs):
         ia.append(JJ); ib.append(nI); xv.append(1.0); b.append(val); JJ += 1
     for nI, val in zip(vfn, vfv):
         ia.append(JJ); ib.append(nI + Nnodes); xv.append(1.0); b.append(val); JJ += 1
+    if len(bcs.ubvbFixedNormalNode):
+        Nx, Ny = nodal_normals(mua.coordinates, mua.connectivity)
+        for nI, val in zip(bcs.ubvbFixedNormalNode, bcs.ubvbFixedNormalValue):
+            ia += [JJ, JJ]; ib += [nI, nI + Nnodes]; xv += [Nx[nI], Ny[nI]]; b.append(-val); JJ += 1
     if JJ == 0:
         return None, None
     L = _matlab_sparse(np.array(ia), np.array(ib), np.array(xv), JJ, 2 * Nnodes).tocsr()
@@ -1213,7 +1266,7 @@ def sstream2dnr2(p: Params, mua: MUA, bcs: BCs, F: Fields, lubvb=None, solver=No
         solver = abfg_pre_eliminate
     F = F.copy()
     Nn = mua.Nnodes
-    L, cuv = create_Luv(Nn, bcs)  # :32
+    L, cuv = create_Luv(Nn, bcs, mua)  # :32
     nc = 0 if cuv is None else cuv.shape[0]
     if lubvb is None or lubvb.shape[0] != nc:
         lubvb = np.zeros(nc)
@@ -1519,10 +1572,10 @@ def uvh_matrix_assembly(p: Params, mua: MUA, F: Fields, S0: UvhState, S1: UvhSta
     return R, K
 
 
-def create_Luvh(Nnodes, bcs: BCs):
+def create_Luvh(Nnodes, bcs: BCs, mua: MUA = None):
     """AssembleLuvhSSTREAM.m:5-72 with BCs2MLC.m (Luv as create_Luv; Lh from
     createLh.m: ties, then fixed h nodes in the given order), rows scaled by ScaleL."""
-    Luv, cuv = create_Luv(Nnodes, bcs)
+    Luv, cuv = create_Luv(Nnodes, bcs, mua)
     hn = np.asarray(bcs.hFixedNode, dtype=np.int64)
     if hn.size:
         Lh = _matlab_sparse(np.arange(hn.size), hn, np.ones(hn.size), hn.size, Nnodes).tocsr()
@@ -1589,7 +1642,7 @@ def sstream_transient_implicit(p: Params, mua: MUA, bcs: BCs, F: Fields, S0: Uvh
         solver = abfg_pre_eliminate
     Nn = mua.Nnodes
     S1 = S1.copy()
-    L, cuvh = create_Luvh(Nn, bcs)  # :35
+    L, cuvh = create_Luvh(Nn, bcs, mua)  # :35
     nc = 0 if cuvh is None else cuvh.size
     luvh = np.zeros(nc) if luvh is None or len(luvh) != nc else luvh.copy()
     dl = np.zeros(nc)
@@ -1786,7 +1839,7 @@ def adjoint_gradient_C(p: Params, mua: MUA, F: Fields, bcs_adjoint: BCs, us, vs,
     _, K = uv_matrix_assembly(p, mua, Fp)
     M = mass_matrix(mua)
     I, dIduv = misfit_uv(mua, Fp, us, vs, usErr, vsErr, M)
-    L, c = create_Luv(mua.Nnodes, bcs_adjoint)
+    L, c = create_Luv(mua.Nnodes, bcs_adjoint, mua)
     lam, _ = abfg_pre_eliminate(K, L, dIduv, np.zeros(0 if c is None else c.size))
     N = mua.Nnodes
     g = dIdCq(p, mua, Fp, lam[:N], lam[N:2 * N])

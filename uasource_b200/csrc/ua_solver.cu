@@ -10,6 +10,7 @@
 // one-CTA-per-system kernel adds the partials in a fixed order, so a
 // system's result does not depend on which other systems share the launch.
 #include <algorithm>
+#include <array>
 #include <iterator>
 #include <atomic>
 #include <chrono>
@@ -86,6 +87,13 @@ struct Work {
   // adjoint gradient work (mass matrix values, measurements, misfit and CG vectors)
   double* adj_buf = nullptr;
   size_t adj_cap = 0;
+  // two-entry constraint rows (ties, normal velocities): second dof and the scaled coefficients of
+  // every row (dof2 = -1 for one-entry rows), the list of two-entry rows and its length
+  int* con_dof2 = nullptr;
+  double *con_v1 = nullptr, *con_v2 = nullptr;
+  int* pair_rows = nullptr;
+  int npair = 0;
+  size_t pair_cap = 0;
   // dof vectors
   double *X, *X0, *dX, *R, *frhs, *Tint, *Fext;
   double* Kd = nullptr;
@@ -135,6 +143,17 @@ struct Work {
   int pcg_exec_lpr[32] = {};
   int nsm = 148;  // SMs of the handle's device (grid of the list-driven kernels)
 };
+
+// Two-entry constraint rows (ties, normal velocities): the second dof and the scaled coefficients
+// of every row; all null when every row has one unit entry (a dof selection).
+struct ConPairs {
+  const int* dof2;
+  const double *v1, *v2;
+};
+
+static ConPairs con_pairs(const Work* w) {
+  return w->npair ? ConPairs{w->con_dof2, w->con_v1, w->con_v2} : ConPairs{nullptr, nullptr, nullptr};
+}
 
 // Work of a timed launch: sum of the tangent non-zeros and dof rows of the
 // systems it processes (selected; for Krylov kernels also not yet converged).
@@ -525,37 +544,95 @@ __global__ void k_pcg_reduce(int stage, const int* sys_rb_off, int nrb, const in
 
 // Constraint rows of the Newton system (mask form):
 // dX[dof_c] = grhs_c = c_c - X[dof_c] (particular solution x_p = L' g).
+__device__ __forceinline__ bool con_is_pair(const ConPairs& cp, int c) { return cp.dof2 && cp.dof2[c] >= 0; }
+// coefficient of row c at dof i (1 for a one-entry row)
+__device__ __forceinline__ double con_coef(const ConPairs& cp, const int* con_dof, int c, int i) {
+  if (!con_is_pair(cp, c)) return 1.0;
+  return con_dof[c] == i ? cp.v1[c] : cp.v2[c];
+}
+
+// Particular solution of B dX = g - B X (ABfgPreEliminate.m:63 with unit rows): a one-entry row
+// sets its dof, a two-entry row b puts b (g - b'X) on its pair.
 __global__ void k_con_particular(int nc, const int* con_dof, const int* con_sys, const int* sel,
-                                 const double* con_rhs, const double* X, double* dX, double* grhs) {
+                                 const double* con_rhs, const double* X, double* dX, double* grhs, ConPairs cp) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc || !sel[con_sys[c]]) return;
   const int d = con_dof[c];
+  if (con_is_pair(cp, c)) {
+    const int d2 = cp.dof2[c];
+    const double t = con_rhs[c] - (cp.v1[c] * X[d] + cp.v2[c] * X[d2]);
+    grhs[c] = t;
+    dX[d] = cp.v1[c] * t;
+    dX[d2] = cp.v2[c] * t;
+    return;
+  }
   const double gv = con_rhs[c] - X[d];
   grhs[c] = gv;
   dX[d] = gv;
+}
+
+// z <- (I - b b') z on the two-entry rows (their dofs are free; rows have disjoint support).
+template <typename VT>
+__global__ void k_pair_project(int npair, const int* pair_rows, const int* con_dof, const int* con_sys,
+                               const int* sel, const int* done, ConPairs cp, VT* z) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npair) return;
+  const int c = pair_rows[k];
+  const int s = con_sys[c];
+  if (!sel[s] || (done && done[s])) return;
+  const int a = con_dof[c], b = cp.dof2[c];
+  const double t = cp.v1[c] * (double)z[a] + cp.v2[c] * (double)z[b];
+  z[a] = (VT)((double)z[a] - cp.v1[c] * t);
+  z[b] = (VT)((double)z[b] - cp.v2[c] * t);
+}
+
+// The first residual projected, and the l1-Jacobi pre-smoothed vector of the V-cycle refreshed on
+// the projected entries (x0 = D^-1 r is diagonal).
+template <typename VT>
+__global__ void k_pair_project_r0(int npair, const int* pair_rows, const int* con_dof, const int* con_sys,
+                                  const int* sel, ConPairs cp, VT* r, VT* x0, const VT* invd) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npair) return;
+  const int c = pair_rows[k];
+  if (!sel[con_sys[c]]) return;
+  const int a = con_dof[c], b = cp.dof2[c];
+  const double t = cp.v1[c] * (double)r[a] + cp.v2[c] * (double)r[b];
+  r[a] = (VT)((double)r[a] - cp.v1[c] * t);
+  r[b] = (VT)((double)r[b] - cp.v2[c] * t);
+  if (x0) {
+    x0[a] = (VT)((double)invd[a] * (double)r[a]);
+    x0[b] = (VT)((double)invd[b] * (double)r[b]);
+  }
 }
 
 // dl_c = (frhs - K dX)[dof_c]  (ABfgPreEliminate.m:138 with B a selection)
 template <typename KT>
 __global__ void k_con_multiplier(int nc, const int* con_dof, const int* con_sys, const int* sel, const int* rowptr,
                                  const int* colind, const KT* K, const double* dX, const double* frhs,
-                                 double* dlam) {
+                                 double* dlam, ConPairs cp) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc || !sel[con_sys[c]]) return;
+  auto row_res = [&](int d) {
+    double acc = 0;
+    for (int j = rowptr[d]; j < rowptr[d + 1]; ++j) acc += (double)K[j] * dX[colind[j]];
+    return frhs[d] - acc;
+  };
   const int d = con_dof[c];
-  double acc = 0;
-  for (int j = rowptr[d]; j < rowptr[d + 1]; ++j) acc += (double)K[j] * dX[colind[j]];
-  dlam[c] = frhs[d] - acc;
+  if (con_is_pair(cp, c)) {  // y = b'(f - K x) (ABfgPreEliminate.m:138)
+    dlam[c] = cp.v1[c] * row_res(d) + cp.v2[c] * row_res(cp.dof2[c]);
+    return;
+  }
+  dlam[c] = row_res(d);
 }
 
 // frhs = -R - L' l  (SSTREAM2dNR2.m:235)
 __global__ void k_frhs(const int* rb_start, const int* rb_sys, const int* sel, const double* R, const int* dof_con,
-                       const double* lam, double* frhs) {
+                       const double* lam, double* frhs, const int* con_dof, ConPairs cp) {
   const int blk = blockIdx.x;
   if (!sel[rb_sys[blk]]) return;
   for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) {
     const int c = dof_con[i];
-    frhs[i] = -R[i] - (c >= 0 ? lam[c] : 0.0);
+    frhs[i] = -R[i] - (c >= 0 ? con_coef(cp, con_dof, c, i) * lam[c] : 0.0);
   }
 }
 
@@ -564,7 +641,7 @@ __global__ void k_frhs(const int* rb_start, const int* rb_sys, const int* sel, c
 __global__ void __launch_bounds__(256) k_cost_rows(const int* rb_start, const int* rb_sys, int nrb, const int* sel,
                                                    const double* R, const int* dof_con, const double* lam,
                                                    const double* dlam, const double* gamma, const double* dX,
-                                                   double* part) {
+                                                   double* part, const int* con_dof, ConPairs cp) {
   const int blk = blockIdx.x;
   const int s = rb_sys[blk];
   double v[2] = {0, 0};
@@ -573,7 +650,7 @@ __global__ void __launch_bounds__(256) k_cost_rows(const int* rb_start, const in
     for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) {
       const int c = dof_con ? dof_con[i] : -1;
       double f = -R[i];
-      if (c >= 0) f -= lam[c] + gm * dlam[c];
+      if (c >= 0) f -= con_coef(cp, con_dof, c, i) * (lam[c] + gm * dlam[c]);
       v[0] += f * f;
       if (dX) v[1] += f * dX[i];
     }
@@ -586,7 +663,7 @@ __global__ void __launch_bounds__(256) k_cost_rows(const int* rb_start, const in
 __global__ void k_cost_reduce(const int* sys_rb_off, int nrb, const int* sel, const double* part, int nsys,
                               double* sysv, const int* sys_con_off, const int* con_dof, const double* con_rhs,
                               const double* X, const double* dX, const double* dlam, const double* gamma,
-                              int write_norm) {
+                              int write_norm, ConPairs cp) {
   const int s = blockIdx.x;
   if (!sel[s]) return;
   double o[2];
@@ -598,7 +675,11 @@ __global__ void k_cost_reduce(const int* sys_rb_off, int nrb, const int* sel, co
     const double gm = gamma ? gamma[s] : 0.0;
     for (int c = sys_con_off[s] + threadIdx.x; c < sys_con_off[s + 1]; c += blockDim.x) {
       const int d = con_dof[c];
-      const double xv = X[d] + (dX ? gm * dX[d] : 0.0);
+      double xv = X[d] + (dX ? gm * dX[d] : 0.0);
+      if (con_is_pair(cp, c)) {  // g = c - L X on a two-entry row
+        const int d2 = cp.dof2[c];
+        xv = cp.v1[c] * xv + cp.v2[c] * (X[d2] + (dX ? gm * dX[d2] : 0.0));
+      }
       const double gv = con_rhs[c] - xv;
       gg += gv * gv;
       if (dlam) gd += gv * dlam[c];
@@ -643,18 +724,24 @@ __global__ void k_lam_update(int nc, const int* con_sys, const int* sel, const d
 }
 
 // Constraint masks: cmask[dof] = 1 and dof_con[dof] = c for every constraint c.
-__global__ void k_con_masks(int nc, const int* con_dof, unsigned char* cmask, int* dof_con) {
+__global__ void k_con_masks(int nc, const int* con_dof, ConPairs cp, unsigned char* cmask, int* dof_con) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   const int d = con_dof[c];
-  cmask[d] = 1;
   dof_con[d] = c;
+  if (con_is_pair(cp, c)) {  // both dofs stay free: the Krylov iteration projects them
+    dof_con[cp.dof2[c]] = c;
+    return;
+  }
+  cmask[d] = 1;
 }
 
+// Fixed values into the iterate (SSTREAM2dNR2.m:101-104); two-entry rows are left to the Newton
+// update, as the reference sets only fixed nodes.
 __global__ void k_set_con_values(int nc, const int* con_dof, const int* con_sys, const int* sel,
-                                 const double* con_rhs, double* X) {
+                                 const double* con_rhs, double* X, ConPairs cp) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < nc && (!sel || sel[con_sys[c]])) X[con_dof[c]] = con_rhs[c];
+  if (c < nc && (!sel || sel[con_sys[c]]) && !con_is_pair(cp, c)) X[con_dof[c]] = con_rhs[c];
 }
 
 __global__ void k_zero_sel(const int* rb_start, const int* rb_sys, const int* sel, double* v) {
@@ -984,19 +1071,93 @@ static int upload_velocity(ua_mesh* m, const ua_fields* F, int nF) {
 
 // BCs2MLC.m:19-25 + CreateLuv.m:28-76 + ScaleL.m for fixed-node BCs: one unit row
 // per unique fixed node (first occurrence's value), u rows then v rows.
-// The constraint rows of the fixed-node BCs, host side: per system the u rows by increasing
-// node, then the v rows, then (ndof 3) the h rows in the given order; each row has one unit
-// entry at con_dof (global dof) and right-hand side rhs (first occurrence of a repeated node).
+// Nodal normals of the boundary (CalcEdgeAndNodalNormals.m): the boundary edges are the element
+// edges that belong to one element, each traversed in its element's node order; an edge A->B has
+// the unit normal (-dy, dx)/l, a boundary node gets the normal of the edge starting at it plus that
+// of the edge ending at it (a P2 mid-edge node the mean of its two sub-edges), normalised.
+static void nodal_normals(const HostSystem& hs, int nod, std::vector<double>& Nx, std::vector<double>& Ny) {
+  const int ne = hs.ne;
+  const int cl[3] = {0, nod == 3 ? 1 : 2, nod == 3 ? 2 : 4};
+  std::vector<std::array<int, 3>> edges;  // (start corner, mid or -1, end corner)
+  std::vector<std::pair<long long, int>> key;
+  for (int e = 0; e < ne; ++e)
+    for (int k = 0; k < 3; ++k) {
+      const int a = hs.conn[(size_t)cl[k] * ne + e], b = hs.conn[(size_t)cl[(k + 1) % 3] * ne + e];
+      const int mid = nod == 6 ? hs.conn[(size_t)(cl[k] + 1) * ne + e] : -1;
+      key.push_back({(long long)std::min(a, b) * hs.nn + std::max(a, b), (int)edges.size()});
+      edges.push_back({a, mid, b});
+    }
+  std::sort(key.begin(), key.end());
+  Nx.assign(hs.nn, 0.0); Ny.assign(hs.nn, 0.0);
+  std::vector<int> bnd;
+  for (size_t i = 0; i < key.size(); ++i) {
+    const bool dup = (i > 0 && key[i].first == key[i - 1].first) ||
+                     (i + 1 < key.size() && key[i].first == key[i + 1].first);
+    if (!dup) bnd.push_back(key[i].second);
+  }
+  std::sort(bnd.begin(), bnd.end());
+  auto unit_normal = [&](int a, int b, double& nx, double& ny) {
+    const double dx = hs.x[b] - hs.x[a], dy = hs.y[b] - hs.y[a];
+    nx = -dy; ny = dx;
+    const double l = std::sqrt(nx * nx + ny * ny);
+    nx = nx / l; ny = ny / l;
+  };
+  for (int ei : bnd) {  // start nodes: assignment
+    const auto& E = edges[ei];
+    double nx, ny;
+    unit_normal(E[0], E[1] >= 0 ? E[1] : E[2], nx, ny);
+    Nx[E[0]] = nx; Ny[E[0]] = ny;
+  }
+  for (int ei : bnd) {  // end nodes and mid nodes: sums
+    const auto& E = edges[ei];
+    double nx2, ny2;
+    unit_normal(E[1] >= 0 ? E[1] : E[0], E[2], nx2, ny2);
+    Nx[E[2]] = Nx[E[2]] + nx2; Ny[E[2]] = Ny[E[2]] + ny2;
+    if (E[1] >= 0) {
+      double nx1, ny1;
+      unit_normal(E[0], E[1], nx1, ny1);
+      Nx[E[1]] = Nx[E[1]] + (nx1 + nx2) / 2; Ny[E[1]] = Ny[E[1]] + (ny1 + ny2) / 2;
+    }
+  }
+  for (int i = 0; i < hs.nn; ++i) {
+    const double l = std::sqrt(Nx[i] * Nx[i] + Ny[i] * Ny[i]);
+    Nx[i] = Nx[i] / l; Ny[i] = Ny[i] / l;
+  }
+}
+
+// The constraint rows of the BCs, host side (BCs2MLC.m:19-29, CreateLuv.m:28-76, ScaleL.m:28-33,
+// createLh.m): per system the u ties, the v ties, the fixed u nodes (increasing, first occurrence
+// of a repeated node), the fixed v nodes, the fixed-normal-velocity nodes, then (ndof 3) the fixed
+// h nodes as given.  Row c has the entry con_v1[c] at dof con_dof[c] and, for ties and normal
+// rows, con_v2[c] at con_dof2[c] (else -1), all scaled to a unit row like the right-hand side.
+// The rows must have disjoint support (B B' diagonal, ABfgPreEliminate.m:35).
 static int constraint_rows(const ua_mesh* m, const ua_bcs* bcs, int nB, std::vector<int>& con_dof,
-                           std::vector<int>& con_sys, std::vector<double>& rhs, std::vector<int>& sys_off) {
+                           std::vector<int>& con_sys, std::vector<double>& rhs, std::vector<int>& sys_off,
+                           std::vector<int>* con_dof2 = nullptr, std::vector<double>* con_v1 = nullptr,
+                           std::vector<double>* con_v2 = nullptr) {
   const int nsys = m->dm.nsys;
   con_dof.clear(); con_sys.clear(); rhs.clear();
+  std::vector<int> d2;
+  std::vector<double> v1, v2;
   sys_off.assign(nsys + 1, 0);
   for (int s = 0; s < nsys; ++s) {
     const ua_bcs* b = bcs ? &bcs[nB == 1 ? 0 : s] : nullptr;
-    if (b && (b->n_utied > 0 || b->n_vtied > 0))
-      return set_error(UA_ERR_INVALID, "tied-node constraints are not supported by the device solver");
     const int nn = m->sys[s].nn, d0 = m->h_dof_off[s];
+    auto push = [&](int da, double a, int db, double bval, double r) {
+      const double scale = 1.0 / std::sqrt(a * a + (db >= 0 ? bval * bval : 0.0));  // ScaleL.m:28-33
+      con_dof.push_back(da); d2.push_back(db); v1.push_back(a * scale); v2.push_back(db >= 0 ? bval * scale : 0.0);
+      con_sys.push_back(s); rhs.push_back(r * scale);
+    };
+    for (int comp = 0; b && comp < 2; ++comp) {  // ties (CreateLuv.m:35-48)
+      const int n = comp == 0 ? b->n_utied : b->n_vtied;
+      const int* A = comp == 0 ? b->utied_a : b->vtied_a;
+      const int* B = comp == 0 ? b->utied_b : b->vtied_b;
+      for (int i = 0; i < n; ++i) {
+        if (A[i] < 0 || A[i] >= nn || B[i] < 0 || B[i] >= nn || A[i] == B[i])
+          return set_error(UA_ERR_INVALID, "system %d: tied node index out of range or tied to itself", s);
+        push(d0 + comp * nn + A[i], 1.0, d0 + comp * nn + B[i], -1.0, 0.0);
+      }
+    }
     const int base = 0;  // indices are 0-based at this layer
     for (int comp = 0; b && comp < 2; ++comp) {
       int n = comp == 0 ? b->n_ufixed : b->n_vfixed;
@@ -1013,9 +1174,20 @@ static int constraint_rows(const ua_mesh* m, const ua_bcs* bcs, int nB, std::vec
         if (i > 0 && idx[i].first == idx[i - 1].first) continue;  // unique, first occurrence
         double v = vals ? vals[idx[i].second] : 0.0;
         if (v != v) return set_error(UA_ERR_NAN_INPUT, "nan in fixed value");
-        con_dof.push_back(d0 + comp * nn + idx[i].first);
-        con_sys.push_back(s);
-        rhs.push_back(v);
+        push(d0 + comp * nn + idx[i].first, 1.0, -1, 0.0, v);
+      }
+    }
+    if (b && b->n_normal > 0) {  // fixed normal velocity (CreateLuv.m:62-72): Nx u + Ny v = -value
+      std::vector<double> Nx, Ny;
+      nodal_normals(m->sys[s], m->nod, Nx, Ny);
+      for (int i = 0; i < b->n_normal; ++i) {
+        const int nd = b->normal_node[i];
+        if (nd < 0 || nd >= nn) return set_error(UA_ERR_INVALID, "system %d: normal-velocity node out of range", s);
+        if (!std::isfinite(Nx[nd]) || !std::isfinite(Ny[nd]) || Nx[nd] * Nx[nd] + Ny[nd] * Ny[nd] < 0.25)
+          return set_error(UA_ERR_INVALID, "system %d: normal-velocity node %d is not on the mesh boundary", s, nd);
+        const double v = b->normal_value ? b->normal_value[i] : 0.0;
+        if (v != v) return set_error(UA_ERR_NAN_INPUT, "nan in fixed normal velocity");
+        push(d0 + nd, Nx[nd], d0 + nn + nd, Ny[nd], -v);
       }
     }
     if (b && m->ndof == 3 && b->n_hfixed > 0) {  // createLh.m: fixed h nodes in the given order
@@ -1027,23 +1199,56 @@ static int constraint_rows(const ua_mesh* m, const ua_bcs* bcs, int nB, std::vec
         seen[nd] = 1;
         double v = b->hfixed_value ? b->hfixed_value[i] : 0.0;
         if (v != v) return set_error(UA_ERR_NAN_INPUT, "nan in fixed h value");
-        con_dof.push_back(d0 + 2 * nn + nd);
-        con_sys.push_back(s);
-        rhs.push_back(v);
+        push(d0 + 2 * nn + nd, 1.0, -1, 0.0, v);
       }
     }
     sys_off[s + 1] = (int)con_dof.size();
   }
+  // disjoint support: every dof in at most one row
+  {
+    std::vector<int> all(con_dof);
+    for (int d : d2)
+      if (d >= 0) all.push_back(d);
+    std::sort(all.begin(), all.end());
+    for (size_t i = 1; i < all.size(); ++i)
+      if (all[i] == all[i - 1])
+        return set_error(UA_ERR_INVALID, "ABfgPreEliminate:B B*B^T not diagonal (dof %d is in two constraints)",
+                         all[i]);
+  }
+  if (con_dof2) *con_dof2 = d2;
+  if (con_v1) *con_v1 = v1;
+  if (con_v2) *con_v2 = v2;
   return UA_OK;
 }
 
 static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
   Work* w = m->work;
   const int nsys = m->dm.nsys;
-  std::vector<int> con_dof, con_sys, sys_off;
-  std::vector<double> rhs;
-  if (int rc = constraint_rows(m, bcs, nB, con_dof, con_sys, rhs, sys_off)) return rc;
+  std::vector<int> con_dof, con_sys, sys_off, con_dof2;
+  std::vector<double> rhs, con_v1, con_v2;
+  if (int rc = constraint_rows(m, bcs, nB, con_dof, con_sys, rhs, sys_off, &con_dof2, &con_v1, &con_v2)) return rc;
   const int nc = (int)con_dof.size();
+  // two-entry rows (ties, normal velocities): their coefficients and the list of those rows
+  std::vector<int> pairs;
+  for (int c = 0; c < nc; ++c)
+    if (con_dof2[c] >= 0) pairs.push_back(c);
+  w->npair = (int)pairs.size();
+  if (w->npair) {
+    if ((size_t)nc > w->pair_cap) {
+      w->con_dof2 = walloc<int>(m, nc);
+      w->con_v1 = walloc<double>(m, nc);
+      w->con_v2 = walloc<double>(m, nc);
+      w->pair_rows = walloc<int>(m, nc);
+      if (!w->con_dof2 || !w->con_v1 || !w->con_v2 || !w->pair_rows)
+        return set_error(UA_ERR_OOM, "constraint allocation failed");
+      w->pair_cap = nc;
+    }
+    UA_CUDA_TRY(cudaMemcpyAsync(w->con_dof2, con_dof2.data(), nc * sizeof(int), cudaMemcpyHostToDevice, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->con_v1, con_v1.data(), nc * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->con_v2, con_v2.data(), nc * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(w->pair_rows, pairs.data(), w->npair * sizeof(int), cudaMemcpyHostToDevice,
+                                m->stream));
+  }
   if (nc > w->nc || !w->con_dof) {
     int cap = std::max(nc, 1);
     w->con_dof = walloc<int>(m, cap);
@@ -1069,7 +1274,9 @@ static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
   // constraint (its dof is unique: repeated nodes were dropped above)
   UA_CUDA_TRY(cudaMemsetAsync(w->cmask, 0, m->ndof_total, m->stream));
   UA_CUDA_TRY(cudaMemsetAsync(w->dof_con, 0xff, m->ndof_total * sizeof(int), m->stream));
-  if (nc) k_con_masks<<<(nc + 255) / 256, 256, 0, m->stream>>>(nc, w->con_dof, w->cmask, w->dof_con), ++g_launches;
+  if (nc)
+    k_con_masks<<<(nc + 255) / 256, 256, 0, m->stream>>>(nc, w->con_dof, con_pairs(w), w->cmask, w->dof_con),
+        ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
   UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   return UA_OK;
@@ -1123,11 +1330,11 @@ static int cost_eval(ua_mesh* m, const ua_params* p, bool useDir, bool assembleR
     if (rc) return rc;
   }
   k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, w->dof_con, w->lam,
-                                             w->dlam, useDir ? w->gamma : nullptr, w->dX, w->part), ++g_launches;
+                                             w->dlam, useDir ? w->gamma : nullptr, w->dX, w->part, w->con_dof, con_pairs(w)), ++g_launches;
   k_cost_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, w->nsys, w->sysv,
                                                          w->sys_con_off, w->con_dof, w->con_rhs, w->X,
                                                          useDir ? w->dX : nullptr, w->dlam,
-                                                         useDir ? w->gamma : nullptr, 0), ++g_launches;
+                                                         useDir ? w->gamma : nullptr, 0, con_pairs(w)), ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
   UA_CUDA_TRY(cudaMemcpyAsync(w->h_sysv, w->sysv, SV_COUNT * w->nsys * sizeof(double), cudaMemcpyDeviceToHost,
                               m->stream));
@@ -1175,7 +1382,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   k_zero_sel<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->dX), ++g_launches;
   if (w->nc)
     k_con_particular<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs,
-                                                                 w->X, w->dX, w->grhs), ++g_launches;
+                                                                 w->X, w->dX, w->grhs, con_pairs(w)), ++g_launches;
   VT *r = (VT*)w->kr, *z = (VT*)w->kz, *pp = (VT*)w->kp, *q = (VT*)w->kq;
   // with AMG the Jacobi-type kernels write the l1 pre-smoothed vector x0 and the V-cycle writes z (and r.z)
   const VT* invd = amg ? (const VT*)amg_invd0(m) : (const VT*)w->invd;
@@ -1222,6 +1429,16 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
           pp, w->part, nullptr);
   });
   ++g_launches;
+  // two-entry constraint rows (ties, normal velocities): the iteration runs in the range of the
+  // projector I - B'B on their pairs; the fused p.q and r.z partials stay exact because p and r
+  // stay in that range
+  const ConPairs cp = con_pairs(w);
+  const int npb = (w->npair + 255) / 256;
+  if (w->npair && !amg)
+    return set_error(UA_ERR_INVALID, "tied and normal-velocity constraints need the AMG preconditioner");
+  if (w->npair)
+    k_pair_project_r0<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel, cp, r,
+                                                      zj, invd), ++g_launches;
   if (amg) {
     // done[] is reset by the stage-0 reduction below; the V-cycle must see every selected system
     UA_CUDA_TRY(cudaMemsetAsync(w->done, 0, w->nsys * sizeof(int), m->stream));
@@ -1230,6 +1447,12 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     int rc = amg_vcycle(m, fp32, view, &g_launches);
     if (rc) return rc;
     view.pcopy = nullptr;
+    if (w->npair) {
+      k_pair_project<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
+                                                     nullptr, cp, z), ++g_launches;
+      k_pair_project<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
+                                                     nullptr, cp, pp), ++g_launches;
+    }
   }
   k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(0, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                         w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
@@ -1258,11 +1481,17 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     prof_end(m, ev);
     k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                           w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
+    if (w->npair)
+      k_pair_project<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
+                                                     w->done, cp, q), ++g_launches;
     k_pcg_update1<VT><<<grid0, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->sysv,
                                                      w->nsys, w->dX, r, zj, pp, q, invd, w->part), ++g_launches;
     if (amg) {
       int rc = amg_vcycle(m, fp32, view, &g_launches);
       if (rc) return rc;
+      if (w->npair)
+        k_pair_project<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
+                                                       w->done, cp, z), ++g_launches;
     }
     k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                           w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
@@ -1274,7 +1503,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   // A chunk of iterations is captured once per (handle, precision, preconditioner) as a CUDA
   // graph and replayed: every argument is a fixed device buffer of the handle, and systems that
   // have converged skip their rows on the device (done[s]), so a replay equals the launches.
-  const bool graph = !w->no_graph && !p->profile;
+  const bool graph = !w->no_graph && !p->profile && w->npair == 0;
   const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0) + (view.K0lo || view.sell_lo ? 4 : 0) + (view.act ? 8 : 0) +
                  (view.sell ? 16 : 0);
   if (graph && w->pcg_exec[gk] && (w->pcg_exec_maxit[gk] != p->krylov_maxit || w->pcg_exec_lpr[gk] != lpr)) {
@@ -1320,7 +1549,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   if (w->nc)
     k_con_multiplier<KT><<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel,
                                                                      w->rowptr, w->colind, K, w->dX, w->frhs,
-                                                                     w->dlam), ++g_launches;
+                                                                     w->dlam, con_pairs(w)), ++g_launches;
   UA_CUDA_TRY(cudaMemcpyAsync(w->h_int, w->its, w->nsys * sizeof(int), cudaMemcpyDeviceToHost, m->stream));
   UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   for (int s = 0; s < w->nsys; ++s) its_out[s] = its_out[s] ? w->h_int[s] : 0;
@@ -1415,17 +1644,17 @@ static int newton_init(ua_mesh* m, const ua_params* p, const std::vector<int>& r
   if ((rc = set_sel(m, run))) return rc;
   if (w->nc) {
     k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel,
-                                                                 w->con_rhs, w->X), ++g_launches;
+                                                                 w->con_rhs, w->X, con_pairs(w)), ++g_launches;
     k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel,
-                                                                 w->con_rhs, w->X0), ++g_launches;
+                                                                 w->con_rhs, w->X0, con_pairs(w)), ++g_launches;
   }
   {
     if ((rc = assemble(m, p, false, false, w->X0, false))) return rc;
     k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, nullptr, nullptr,
-                                               nullptr, nullptr, nullptr, w->part), ++g_launches;
+                                               nullptr, nullptr, nullptr, w->part, nullptr, ConPairs{}), ++g_launches;
     k_cost_reduce<<<nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, nsys, w->sysv,
                                                        nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                                       nullptr, 1), ++g_launches;
+                                                       nullptr, 1, con_pairs(w)), ++g_launches;
     UA_CUDA_TRY(cudaGetLastError());
   }
   // initial cost (:149-152) with zero direction
@@ -1554,7 +1783,7 @@ static int newton_step(ua_mesh* m, const ua_params* p, std::vector<ua_newton_rep
       if ((rc = assemble(m, p, refreshK, false, w->X, false))) return rc;
       if ((rc = set_sel(m, sel))) return rc;
     }
-    k_frhs<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->R, w->dof_con, w->lam, w->frhs), ++g_launches;
+    k_frhs<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->R, w->dof_con, w->lam, w->frhs, w->con_dof, con_pairs(w)), ++g_launches;
     UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
     double t1 = now_ms();
     t_asm += t1 - t0;
@@ -1885,6 +2114,9 @@ static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out,
   Work* w = m->work;
   const int N = m->ndof_total;
   const int lpr = 16;
+  if (w->npair)
+    return set_error(UA_ERR_INVALID, "tied nodes and fixed normal velocities need the GMRES uvh solver "
+                                     "(uvh_krylov = UA_KRYLOV_GMRES)");
   for (int s = 0; s < w->nsys; ++s) {
     const double e = eta ? eta[s] : p->krylov_rtol;
     w->h_sysv[s] = e * e;
@@ -1907,7 +2139,7 @@ static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out,
   k_zero_sel<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->dX), ++g_launches;
   if (w->nc)
     k_con_particular<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs,
-                                                                 w->X, w->dX, w->grhs), ++g_launches;
+                                                                 w->X, w->dX, w->grhs, con_pairs(w)), ++g_launches;
   k_bicg_init<KT, 16><<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->rowptr, w->colind, K,
                                                      w->dX, w->frhs, w->cmask, r, rhat, pp, vv, w->part), ++g_launches;
   k_bicg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(0, w->sys_rb_off, w->nrb, w->sel, w->done, w->its, w->status,
@@ -1956,7 +2188,7 @@ static int bicgstab_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out,
   }
   if (w->nc)
     k_con_multiplier<KT><<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->rowptr,
-                                                                     w->colind, K, w->dX, w->frhs, w->dlam), ++g_launches;
+                                                                     w->colind, K, w->dX, w->frhs, w->dlam, con_pairs(w)), ++g_launches;
   UA_CUDA_TRY(cudaMemcpyAsync(w->h_int, w->its, w->nsys * sizeof(int), cudaMemcpyDeviceToHost, m->stream));
   UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   for (int s = 0; s < w->nsys; ++s) its_out[s] = its_out[s] ? w->h_int[s] : 0;
@@ -2227,6 +2459,15 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
     k_bicg_spmv<KT, 16><<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, w->rowptr,
                                                 w->colind, K, x, w->cmask, y, nullptr, w->part), ++g_launches;
   };
+  // Two-entry constraint rows (ties, normal velocities): the Krylov space is kept in the range of
+  // I - B'B by projecting the residual, every preconditioned vector and every product, so GMRES
+  // solves the projected system (P K P) x = P f on it.
+  const int npb = (w->npair + 255) / 256;
+  auto project = [&](double* v) {
+    if (w->npair)
+      k_pair_project<double><<<npb, 256, 0, st>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel, w->done,
+                                                  con_pairs(w), v), ++g_launches;
+  };
   // host-side reduction results
   std::vector<double> hco((size_t)nsys * ld), hco2((size_t)nsys * ld), hnrm((size_t)nsys * ld), hsc(nsys),
       hy((size_t)nsys * ld);
@@ -2242,7 +2483,7 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
   k_zero_sel<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->dX), ++g_launches;
   if (w->nc)
     k_con_particular<<<(w->nc + 255) / 256, 256, 0, st>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs, w->X,
-                                                         w->dX, w->grhs), ++g_launches;
+                                                         w->dX, w->grhs, con_pairs(w)), ++g_launches;
   std::vector<GmSys> S(nsys);
   for (int s = 0; s < nsys; ++s) {
     S[s].active = its_out[s] != 0;
@@ -2272,6 +2513,11 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
                                                                   wv, w->gm_part);
     });
     ++g_launches;
+    if (w->npair) {  // project the residual before its norm is taken
+      project(wv);
+      k_gm_dots<<<dim3(w->nrb, 1), 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, wv, wv, 0,
+                                                 w->gm_part), ++g_launches;
+    }
     if ((rc = reduce_to_host(w->gm_part, 1, hco))) return rc;
     bool any = false;
     for (int s = 0; s < nsys; ++s) {
@@ -2298,7 +2544,9 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
     // Arnoldi steps
     for (int j = 0; j < mr; ++j) {
       if ((rc = precond(V + (size_t)j * ldv, zv))) return rc;
+      project(zv);
       spmv(zv, wv);
+      project(wv);
       for (int pass = 0; pass < 2; ++pass) {
         k_gm_dots<<<dim3(w->nrb, j + 1), 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, wv, V, ldv,
                                                        w->gm_part), ++g_launches;
@@ -2366,6 +2614,7 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
     k_gm_combine<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->gm_act, uv, V, ldv, w->gm_scal,
                                          w->gm_ny, ld), ++g_launches;
     if ((rc = precond(uv, zv))) return rc;
+    project(zv);
     k_gm_axpy<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->gm_act, w->dX, zv), ++g_launches;
     ++total_cycles;
   }
@@ -2374,7 +2623,7 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
   UA_CUDA_TRY(cudaMemcpyAsync(w->done, hdone.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, st));
   if (w->nc)
     k_con_multiplier<KT><<<(w->nc + 255) / 256, 256, 0, st>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->rowptr,
-                                                              w->colind, K, w->dX, w->frhs, w->dlam), ++g_launches;
+                                                              w->colind, K, w->dX, w->frhs, w->dlam, con_pairs(w)), ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
   UA_CUDA_TRY(cudaStreamSynchronize(st));
   for (int s = 0; s < nsys; ++s) its_out[s] = its_out[s] ? S[s].its : 0;
@@ -2447,10 +2696,10 @@ static int cost_eval_uvh(ua_mesh* m, const ua_params* p, bool assembleR = true) 
     if (rc) return rc;
   }
   k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, w->dof_con, w->lam,
-                                             w->dlam, w->gamma, w->dX, w->part), ++g_launches;
+                                             w->dlam, w->gamma, w->dX, w->part, w->con_dof, con_pairs(w)), ++g_launches;
   k_cost_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, w->nsys, w->sysv,
                                                          w->sys_con_off, w->con_dof, w->con_rhs, w->X, w->dX, w->dlam,
-                                                         w->gamma, 0), ++g_launches;
+                                                         w->gamma, 0, con_pairs(w)), ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
   UA_CUDA_TRY(cudaMemcpyAsync(w->h_sysv, w->sysv, SV_COUNT * w->nsys * sizeof(double), cudaMemcpyDeviceToHost,
                               m->stream));
@@ -2489,13 +2738,13 @@ static int newton_run_uvh(ua_mesh* m, const ua_params* p, std::vector<ua_newton_
   // uvhMakeInitialIterateFeasible (:37-41)
   if (w->nc)
     k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel, w->con_rhs,
-                                                                 w->X), ++g_launches;
+                                                                 w->X, con_pairs(w)), ++g_launches;
   // Fext0 at ZeroFields (:53-56); the normalisation of CalcCostFunctionNRuvh
   if ((rc = assemble_uvh(m, p, false, false, true, false))) return rc;
   k_cost_rows<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->R, nullptr, nullptr, nullptr,
-                                             nullptr, nullptr, w->part), ++g_launches;
+                                             nullptr, nullptr, w->part, nullptr, ConPairs{}), ++g_launches;
   k_cost_reduce<<<nsys, kRedThreads, 0, m->stream>>>(w->sys_rb_off, w->nrb, w->sel, w->part, nsys, w->sysv, nullptr,
-                                                     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 1), ++g_launches;
+                                                     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 1, con_pairs(w)), ++g_launches;
   UA_CUDA_TRY(cudaGetLastError());
   for (int s = 0; s < nsys; ++s) { st[s] = UvhSys(); st[s].active = true; }
   while (true) {
@@ -2520,7 +2769,7 @@ static int newton_run_uvh(ua_mesh* m, const ua_params* p, std::vector<ua_newton_
     if ((rc = set_sel(m, sel))) return rc;
     double t0 = now_ms();
     if ((rc = assemble_uvh(m, p, true, false, false, false))) return rc;  // :127
-    k_frhs<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->R, w->dof_con, w->lam, w->frhs), ++g_launches;
+    k_frhs<<<w->nrb, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->sel, w->R, w->dof_con, w->lam, w->frhs, w->con_dof, con_pairs(w)), ++g_launches;
     UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
     double t1 = now_ms();
     t_asm += t1 - t0;
@@ -2693,7 +2942,7 @@ extern "C" int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F
     UA_CUDA_TRY(cudaMemsetAsync(w->X, 0, m->ndof_total * sizeof(double), m->stream));
     if (w->nc)
       k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, nullptr,
-                                                                   w->con_rhs, w->X), ++g_launches;
+                                                                   w->con_rhs, w->X, con_pairs(w)), ++g_launches;
   }
   std::vector<int> sel(1, 1);
   if ((rc = set_sel(m, sel))) return rc;
@@ -2850,7 +3099,7 @@ extern "C" int ua_constraint_count(const ua_mesh* m, const ua_bcs* bcs, int32_t 
       std::sort(v.begin(), v.end());
       n += (int)(std::unique(v.begin(), v.end()) - v.begin());
     }
-    n += bcs->n_utied + bcs->n_vtied;
+    n += bcs->n_utied + bcs->n_vtied + bcs->n_normal;
     if (ndof == 3) n += bcs->n_hfixed;
   }
   *nc = n;
@@ -2861,13 +3110,13 @@ extern "C" int ua_constraint_matrix(const ua_mesh* m, const ua_bcs* bcs, int32_t
                                     double* rhs) {
   if (!m || !nc) return set_error(UA_ERR_INVALID, "ua_constraint_matrix: null argument");
   if (m->dm.nsys != 1) return set_error(UA_ERR_INVALID, "ua_constraint_matrix takes a single-mesh handle");
-  std::vector<int> cd, cs, off;
-  std::vector<double> r;
-  if (int rc = constraint_rows(m, bcs, 1, cd, cs, r, off)) return rc;
+  std::vector<int> cd, cs, off, cd2;
+  std::vector<double> r, v1, v2;
+  if (int rc = constraint_rows(m, bcs, 1, cd, cs, r, off, &cd2, &v1, &v2)) return rc;
   *nc = (int32_t)cd.size();
   for (size_t k = 0; k < cd.size(); ++k) {
-    if (dof) dof[k] = cd[k];
-    if (val) val[k] = 1.0;  // one unit entry per row: ScaleL.m leaves it 1
+    if (dof) { dof[2 * k] = cd[k]; dof[2 * k + 1] = cd2[k]; }
+    if (val) { val[2 * k] = v1[k]; val[2 * k + 1] = v2[k]; }
     if (rhs) rhs[k] = r[k];
   }
   return UA_OK;

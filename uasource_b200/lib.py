@@ -114,7 +114,8 @@ class ua_bcs(C.Structure):
                 ("n_utied", C.c_int32), ("utied_a", _ip), ("utied_b", _ip),
                 ("n_vtied", C.c_int32), ("vtied_a", _ip), ("vtied_b", _ip),
                 ("n_hfixed", C.c_int32), ("hfixed_node", _ip), ("hfixed_value", _dp),
-                ("n_hpos", C.c_int32), ("hpos_node", _ip)]
+                ("n_hpos", C.c_int32), ("hpos_node", _ip),
+                ("n_normal", C.c_int32), ("normal_node", _ip), ("normal_value", _dp)]
 
 
 class ua_newton_iter(C.Structure):

@@ -177,6 +177,8 @@ class BCs:
     ubTiedNodeB: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     vbTiedNodeA: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     vbTiedNodeB: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    ubvbFixedNormalNode: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    ubvbFixedNormalValue: np.ndarray = field(default_factory=lambda: np.zeros(0))
 
     @staticmethod
     def from_problem(P):
@@ -244,6 +246,15 @@ def _c_bcs(B: BCs, keep: _Keep):
     cb.n_vfixed = len(B.vbFixedNode); cb.vfixed_node = keep.i(B.vbFixedNode); cb.vfixed_value = keep.d(B.vbFixedValue)
     cb.n_utied = len(B.ubTiedNodeA); cb.utied_a = keep.i(B.ubTiedNodeA); cb.utied_b = keep.i(B.ubTiedNodeB)
     cb.n_vtied = len(B.vbTiedNodeA); cb.vtied_a = keep.i(B.vbTiedNodeA); cb.vtied_b = keep.i(B.vbTiedNodeB)
+    if len(B.ubvbFixedNormalNode):
+        cb.n_normal = len(B.ubvbFixedNormalNode); cb.normal_node = keep.i(B.ubvbFixedNormalNode)
+        cb.normal_value = keep.d(B.ubvbFixedNormalValue)
+    hn = getattr(B, "hFixedNode", None)
+    if hn is not None and len(hn):
+        cb.n_hfixed = len(hn); cb.hfixed_node = keep.i(hn); cb.hfixed_value = keep.d(B.hFixedValue)
+    hp = getattr(B, "hPosNode", None)
+    if hp is not None and len(hp):
+        cb.n_hpos = len(hp); cb.hpos_node = keep.i(hp)
     return cb
 
 
@@ -587,12 +598,6 @@ def uvh(ctrl: CtrlVar, mua: MUA, F0: Fields, F1: Fields, bcs: BCs, dt, l=None, r
     Nn = mua.Nnodes()
     cf, ub, vb, h1 = _c_fields_uvh(F0, F1, dt, keep, Nn)
     cb = _c_bcs(bcs, keep)
-    hn = getattr(bcs, "hFixedNode", None) if bcs is not None else None
-    if hn is not None and len(hn):
-        cb.n_hfixed = len(hn); cb.hfixed_node = keep.i(hn); cb.hfixed_value = keep.d(bcs.hFixedValue)
-    hp = getattr(bcs, "hPosNode", None) if bcs is not None else None
-    if hp is not None and len(hp):
-        cb.n_hpos = len(hp); cb.hpos_node = keep.i(hp)
     p = ctrl.to_c()
     nc = C.c_int32()
     L.check(lib.ua_constraint_count(mua.handle, C.byref(cb), 3, C.byref(nc)))
@@ -641,6 +646,28 @@ def adjoint_gradient_C(ctrl: CtrlVar, mua: MUA, F: Fields, bcs_adjoint: BCs, us,
     L.check(lib.ua_uv_adjoint_dIdC(mua.handle, C.byref(p), C.byref(cf), C.byref(cb), C.byref(ms), flags,
                                    C.byref(I), L.dptr(dIduv), L.dptr(lam), L.dptr(g), C.byref(its)))
     return I.value, dIduv, lam, g, its.value
+
+
+def constraint_matrix(mua: MUA, bcs: BCs):
+    """The constraint matrix L and right-hand side c of ``bcs`` on a single-mesh handle, as the
+    solvers impose them (BCs2MLC.m -> CreateLuv.m, createLh.m for fixed h on an ndof=3 handle,
+    ScaleL.m): rows u ties, v ties, fixed u, fixed v, fixed normal velocities, fixed h, each scaled
+    to unit length.  Returns (L as a scipy CSR matrix of ndof*Nnodes columns, c)."""
+    import scipy.sparse as sp
+    lib = L.load()
+    keep = _Keep()
+    cb = _c_bcs(bcs, keep)
+    nc = C.c_int32()
+    L.check(lib.ua_constraint_matrix(mua.handle, C.byref(cb), C.byref(nc), None, None, None))
+    n = nc.value
+    dof = np.zeros(2 * n, np.int32)
+    val = np.zeros(2 * n)
+    rhs = np.zeros(n)
+    L.check(lib.ua_constraint_matrix(mua.handle, C.byref(cb), C.byref(nc), L.iptr(dof), L.dptr(val), L.dptr(rhs)))
+    rows = np.repeat(np.arange(n), 2)
+    keep_ = dof >= 0
+    Lm = sp.csr_matrix((val[keep_], (rows[keep_], dof[keep_])), shape=(n, mua.ndof * mua.Nnodes()))
+    return Lm, rhs
 
 
 def solveKApeSymmetric(A, B, f, g, rtol=1e-12, maxit=0, device=0):
