@@ -1,12 +1,15 @@
 /*
  * [ub,vb,h,luvh,info] = SSTREAM_TransientImplicit_mex(CtrlVar,MUA,BCs1,F0,F1,l1)
  *
- * Drop-in for the implicit uvh Newton step SSTREAM_TransientImplicit.m:6-717
- * (called through uvh.m:45 -> uvh2D.m:20; without the active-set thickness
- * constraints of uvh.m:72-212).  F0: state at t; F1: start values at t+dt and
- * the time-independent fields; CtrlVar.dt the time step.  l1 is [l.ubvb; l.h]
- * (may be []).  info carries uvhConverged, uvhIterations, the last residual
- * and backtracking steps.
+ * Drop-in for the implicit uvh step uvh.m:5-222 -> uvh2D.m:20 ->
+ * SSTREAM_TransientImplicit.m:6-717, with the minimum-thickness active set of
+ * uvh.m:64-212 when CtrlVar.ThicknessConstraints is 1 (BCs1.hPosNode, 1-based,
+ * the set carried from the previous step).  F0: state at t; F1: start values at
+ * t+dt and the time-independent fields; CtrlVar.dt the time step.  l1 is
+ * [l.ubvb; l.h] (may be []).  info carries uvhConverged, uvhIterations, the last
+ * residual and backtracking steps, and with the active set hPosNode (the final
+ * set, 1-based: BCs1.hPosNode for the next step), activeSetIterations,
+ * activeSetConverged and activeSetCyclical.
  */
 #include "ua_mex_common.h"
 
@@ -20,6 +23,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     ua_newton_iter recs[256];
     int32_t nn, nc = 0;
     double *ub, *vb, *h, *lam, *own[14];
+    int32_t* hpos;
     const char* names[8] = {"h", "S", "B", "rho", "AGlen", "n", "C", "m"};
     const double* src[8];
     double* own_drag[11];
@@ -65,6 +69,9 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     memset(&rep, 0, sizeof(rep));
     rep.iters = recs;
     rep.iters_capacity = 256;
+    hpos = (int32_t*)mxCalloc(nn > 0 ? nn : 1, sizeof(int32_t));
+    rep.hpos_node = hpos;
+    rep.hpos_capacity = nn;
     rc = ua_uvh_newton(m, &p, &f, &b, lam, nc, &rep);
     for (k = 0; k < 14; ++k) if (own[k]) mxFree(own[k]);
     for (k = 0; k < 11; ++k) if (own_drag[k]) mxFree(own_drag[k]);
@@ -74,15 +81,25 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         if (nc) memcpy(mxGetPr(plhs[3]), lam, nc * sizeof(double));
     }
     if (nlhs > 4) {
-        const char* fn[6] = {"uvhConverged", "uvhIterations", "uvhResidual", "uvhBackTrackSteps", "rForce", "rWork"};
-        mxArray* s = mxCreateStructMatrix(1, 1, 6, fn);
+        const char* fn[10] = {"uvhConverged", "uvhIterations", "uvhResidual", "uvhBackTrackSteps", "rForce", "rWork",
+                              "hPosNode", "activeSetIterations", "activeSetConverged", "activeSetCyclical"};
+        mxArray* s = mxCreateStructMatrix(1, 1, p.ThicknessConstraints ? 10 : 6, fn);
         mxSetField(s, 0, "uvhConverged", mxCreateDoubleScalar(rep.converged));
         mxSetField(s, 0, "uvhIterations", mxCreateDoubleScalar(rep.iterations));
         mxSetField(s, 0, "uvhResidual", mxCreateDoubleScalar(rep.r));
         mxSetField(s, 0, "uvhBackTrackSteps", mxCreateDoubleScalar(rep.backtrack_steps));
         mxSetField(s, 0, "rForce", mxCreateDoubleScalar(rep.rForce));
         mxSetField(s, 0, "rWork", mxCreateDoubleScalar(rep.rWork));
+        if (p.ThicknessConstraints) {
+            mxArray* hp = mxCreateDoubleMatrix(rep.n_hpos, 1, mxREAL);
+            for (k = 0; k < rep.n_hpos; ++k) mxGetPr(hp)[k] = (double)hpos[k] + 1.0;
+            mxSetField(s, 0, "hPosNode", hp);
+            mxSetField(s, 0, "activeSetIterations", mxCreateDoubleScalar(rep.active_set_iterations));
+            mxSetField(s, 0, "activeSetConverged", mxCreateDoubleScalar(rep.active_set_converged));
+            mxSetField(s, 0, "activeSetCyclical", mxCreateDoubleScalar(rep.active_set_cyclical));
+        }
         plhs[4] = s;
     }
+    mxFree(hpos);
     mxFree(lam);
 }

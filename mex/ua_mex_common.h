@@ -168,6 +168,14 @@ static inline void ua_mex_params(const mxArray* C, ua_params* p) {
         p->SlidingLaw = (int32_t)ua_mex_scalar(C, "GPUSlidingLaw", p->SlidingLaw);
     }
     p->Nzero = ua_mex_scalar(C, "Nzero", p->Nzero);
+    /* the minimum-thickness active set of uvh.m:64-212 (Ua2D_DefaultParameters.m:1479-1500) */
+    p->ThicknessConstraints = (int32_t)ua_mex_scalar(C, "ThicknessConstraints", p->ThicknessConstraints);
+    p->ThickMin = ua_mex_scalar(C, "ThickMin", p->ThickMin);
+    p->ThicknessConstraintsItMax = (int32_t)ua_mex_scalar(C, "ThicknessConstraintsItMax", p->ThicknessConstraintsItMax);
+    p->MaxNumberOfNewlyIntroducedActiveThicknessConstraints = (int32_t)ua_mex_scalar(
+        C, "MaxNumberOfNewlyIntroducedActiveThicknessConstraints", p->MaxNumberOfNewlyIntroducedActiveThicknessConstraints);
+    p->MinNumberOfNewlyIntroducedActiveThicknessConstraints = (int32_t)ua_mex_scalar(
+        C, "MinNumberOfNewlyIntroducedActiveThicknessConstraints", p->MinNumberOfNewlyIntroducedActiveThicknessConstraints);
     p->IncludeMelangeModelPhysics =
         (int32_t)ua_mex_scalar(C, "IncludeMelangeModelPhysics", p->IncludeMelangeModelPhysics);
     /* the GPU form selected by a CtrlVar.UseGPU-style switch (0=FP64, 1=mixed) */
@@ -348,6 +356,8 @@ static inline void ua_mex_bcs(const mxArray* B, ua_bcs* b) {
     b->normal_value = ua_mex_values(B, "ubvbFixedNormalValue", b->n_normal);
     for (i = 0; i < b->n_normal; ++i) ((int32_t*)b->normal_node)[i] -= 1;
     for (i = 0; i < b->n_hfixed; ++i) ((int32_t*)b->hfixed_node)[i] -= 1;
+    b->hpos_node = ua_mex_nodes(B, "hPosNode", &b->n_hpos);  /* the active set carried from the last step */
+    for (i = 0; i < b->n_hpos; ++i) ((int32_t*)b->hpos_node)[i] -= 1;
 }
 
 /* CSR values on the structural pattern -> MATLAB sparse (CSC, sorted rows, no

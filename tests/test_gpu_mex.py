@@ -225,6 +225,44 @@ def test_newton_gateway(gateways):
     assert sp.issparse(K) and K.shape == (2 * P.Nnodes, 2 * P.Nnodes) and sp.issparse(Rv)
 
 
+def test_newton_gateway_with_ties_and_normals(gateways):
+    """BCs.ubTiedNodeA/B and ubvbFixedNormalNode/Value through the gateway: the solution and the
+    two-entry rows of L (CreateLuv.m:28-76, ScaleL.m) as the oracle has them."""
+    from tests.constraint_cases import front_nodes, problem, tie_nodes
+    g = gateways["SSTREAM2dNR2_mex"]
+    P = problem(21, 11, 3, np.pi / 6)
+    bottom, top = tie_nodes(P)
+    fr = front_nodes(P)
+    kw = dict(ubTiedNodeA=bottom[:-1], ubTiedNodeB=top[:-1], ubvbFixedNormalNode=fr,
+              ubvbFixedNormalValue=np.zeros(fr.size))
+    b = _bcs(P)
+    b.update({"ubTiedNodeA": kw["ubTiedNodeA"] + 1.0, "ubTiedNodeB": kw["ubTiedNodeB"] + 1.0,
+              "ubvbFixedNormalNode": fr + 1.0, "ubvbFixedNormalValue": np.zeros(fr.size)})
+    ctrl = {"uvDesiredWorkAndForceTolerances": [np.inf, 1e-20], "uvDesiredWorkOrForceTolerances": [np.inf, 1e-20]}
+    ub, vb, lam, K, Rv, info, L = g(7, g.struct(ctrl), _mua(g, P), g.struct(b), g.struct(_F(P)),
+                                    g.double(np.zeros((0, 0))))
+    p = R.Params()
+    p.set_force_tolerance(1e-20)
+    ref = R.uv(p, R.create_mua(P.coordinates, P.connectivity),
+               R.BCs(ubFixedNode=P.ubFixedNode, ubFixedValue=P.ubFixedValue, vbFixedNode=P.vbFixedNode,
+                     vbFixedValue=P.vbFixedValue, **kw),
+               R.Fields(h=P.h, S=P.S, B=P.B, rho=P.rho, AGlen=P.AGlen, n=P.n, C=P.C, m=P.m, ub=P.ub, vb=P.vb))
+    u = np.concatenate([ub.ravel(), vb.ravel()]); u_ref = np.concatenate([ref.ub, ref.vb])
+    assert info["uvConverged"][0, 0] == 1
+    assert np.linalg.norm(u - u_ref) <= U_TOL * np.linalg.norm(u_ref)
+    _csc_equal(L, sp.csc_matrix(ref.L), 1e-15)
+
+
+def test_gateway_refuses_unequal_tie_lists(gateways):
+    g = gateways["SSTREAM2dNR2_mex"]
+    P = synth.ice_stream_shelf(9, 6, nod=3, seed=0)
+    b = _bcs(P)
+    b.update({"ubTiedNodeA": np.array([2.0, 3.0]), "ubTiedNodeB": np.array([5.0])})
+    with pytest.raises(RuntimeError) as ei:
+        g(7, g.struct({}), _mua(g, P), g.struct(b), g.struct(_F(P)), g.double(np.zeros((0, 0))))
+    assert str(ei.value).startswith("Ua:mex:BCs")
+
+
 def _uvh_fixture():
     import glob
     path = sorted(glob.glob(os.path.join(HERE, "golden", "uvh_P2_*.npz")))[0]
@@ -266,3 +304,34 @@ def test_uvh_newton_gateway(gateways):
     got = np.concatenate([ub.ravel(), vb.ravel(), h.ravel()])
     ref = np.concatenate([z["sol_ub"], z["sol_vb"], z["sol_h"]])
     assert np.linalg.norm(got - ref) <= U_TOL * np.linalg.norm(ref)
+
+
+def test_uvh_newton_gateway_active_set(gateways):
+    """CtrlVar.ThicknessConstraints through the gateway: the final BCs1.hPosNode (1-based) and
+    the step match the oracle's active-set loop (uvh.m:64-212)."""
+    from tests.active_set_cases import thin_patch_problem
+    g = gateways["SSTREAM_TransientImplicit_mex"]
+    P, h, as_ = thin_patch_problem()
+    p = R.Params()
+    p.set_force_tolerance(1e-20)
+    p.uvhDesiredWorkAndForceTolerances = (np.inf, 1e-20)
+    p.uvhDesiredWorkOrForceTolerances = (np.inf, 1e-20)
+    mo = R.create_mua(P.coordinates, P.connectivity)
+    Fo = R.Fields(h=h, S=P.S, B=P.B, rho=P.rho, AGlen=P.AGlen, n=P.n, C=P.C, m=P.m, ub=P.ub, vb=P.vb)
+    bo = R.BCs(ubFixedNode=P.ubFixedNode, ubFixedValue=P.ubFixedValue, vbFixedNode=P.vbFixedNode,
+               vbFixedValue=P.vbFixedValue)
+    uv = R.uv(p, mo, bo, Fo)
+    S0 = R.UvhState(h.copy(), uv.ub.copy(), uv.vb.copy(), as_.copy(), P.ab.copy())
+    ref = R.uvh_active_set(p, mo, bo, Fo, S0, S0.copy(), 0.1)
+    assert ref.converged and ref.hPosNode.size > 0
+    F = _F(P, uv.ub, uv.vb, {"h": h, "as": as_, "ab": P.ab})
+    ctrl = {"dt": 0.1, "ThicknessConstraints": 1.0, "ThickMin": 1.0,
+            "uvhDesiredWorkAndForceTolerances": [np.inf, 1e-20], "uvhDesiredWorkOrForceTolerances": [np.inf, 1e-20]}
+    ub, vb, hh, lam, info = g(5, g.struct(ctrl), _mua(g, P), g.struct(_bcs(P)), g.struct(F), g.struct(dict(F)),
+                              g.double(np.zeros((0, 0))))
+    assert info["uvhConverged"][0, 0] == 1 and info["activeSetConverged"][0, 0] == 1
+    assert info["activeSetIterations"][0, 0] == ref.iterations
+    assert np.array_equal(info["hPosNode"].ravel().astype(np.int64) - 1, ref.hPosNode)
+    got = np.concatenate([ub.ravel(), vb.ravel(), hh.ravel()])
+    want = np.concatenate([ref.res.ub, ref.res.vb, ref.res.h])
+    assert np.linalg.norm(got - want) <= U_TOL * np.linalg.norm(want)
