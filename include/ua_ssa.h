@@ -125,7 +125,9 @@ typedef struct ua_params {
     double krylov_rtol;        /* relative residual of the preconditioned solve */
     int32_t krylov_maxit;
     int32_t precision;         /* UA_PREC_* */
-    int32_t patch_nodes;       /* assembly patch size (0 = autotune) */
+    int32_t patch_nodes;       /* nodes per assembly patch (one CTA each): 0 = the schedule ua_autotune chose
+                                  for this device, element type and dof count, else the default shape
+                                  (clamp(Nnodes/600, 16, 128) per system); > 0 = that many */
     int32_t verbose;           /* per-iteration log line to stderr */
     int32_t profile;           /* 1: time assembly and SpMV launches with CUDA events */
     int32_t krylov_adaptive;   /* 1: inner tolerance eta_k = clamp(c*sqrt(rForce_k), krylov_rtol, max)
@@ -135,7 +137,8 @@ typedef struct ua_params {
                                   sweeps on the thickness block) and UA_PC_JACOBI point Jacobi */
     int32_t spmv_lanes;        /* lanes per row of the uv PCG/AMG row products: 0 = by element type
                                   (1 for P1, 2 for P2), else 1, 2, 4, 8, 16 or 32 */
-    int32_t asm_threads;       /* CTA size of the P1 uv assembly: 0 = default, else 128 or 256 */
+    int32_t asm_threads;       /* CTA size of the P1 uv assembly: 0 = the tuned one (ua_autotune), else 256;
+                                  or 128 or 256 */
     int32_t uvh_krylov;        /* UA_KRYLOV_*: inner solver of the unsymmetric uvh system */
     int32_t krylov_restart;    /* GMRES restart length m (uvh) */
     double krylov_eta_c, krylov_eta_max;  /* uv forcing term eta = clamp(c*sqrt(rForce), krylov_rtol, max) */
@@ -250,7 +253,7 @@ const char* ua_last_error(void);
 int ua_device_count(void);
 
 /* ABI check for foreign bindings: sizes (bytes) of ua_mesh_desc, ua_params,
- * ua_fields, ua_bcs, ua_newton_iter, ua_newton_report, in that order (n <= 6).
+ * ua_fields, ua_bcs, ua_newton_iter, ua_newton_report, ua_tune_report, in that order (n <= 7).
  * No counterpart in the reference; it needs no GPU. */
 int ua_struct_sizes(int64_t* sizes, int32_t n);
 
@@ -289,6 +292,23 @@ int ua_mesh_flipped(const ua_mesh* m, int32_t* nflipped);
  * (uvMatrixAssemblySSTREAM.m:530-531); NULL for mode R. Tint/Fext optional. */
 int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_bcs* bcs,
                    int32_t mode, double* R, double* Kvals, double* Tint, double* Fext);
+
+/* Assembly autotuner.  Times the tangent+residual uv assembly of the handle's systems at the
+ * fields F (nF = 1 or one per system) for each candidate schedule, reps launches each: patch
+ * shapes pn = clamp(nn/div, 16, cap) nodes per patch (div = 0: cap nodes) and, for P1, CTAs of
+ * 256 or 128 threads.  The fastest becomes the handle's schedule and the process-wide tuned
+ * schedule of (device, nod, ndof), which handles then use when patch_nodes and asm_threads are 0.
+ * K and R are bit-identical under every schedule.  Needs an ndof=2 handle. */
+#define UA_TUNE_MAX 16
+typedef struct {
+    int32_t n_candidates;
+    int32_t div[UA_TUNE_MAX], cap[UA_TUNE_MAX], threads[UA_TUNE_MAX];
+    double ms[UA_TUNE_MAX];    /* mean time of one assembly launch per candidate */
+    int32_t chosen;            /* index of the fastest */
+    double default_ms;         /* candidate 0: the default schedule */
+} ua_tune_report;
+int ua_autotune(ua_mesh* m, const ua_params* p, const ua_fields* F, int32_t nF, int32_t reps,
+                ua_tune_report* rep);
 
 /* Whole uv Newton solve: SSTREAM2dNR2.m:3-431 with the reset-and-retry of
  * uv.m:107-112.  F->ub/F->vb: start values in, solution out.  lubvb: Lagrange

@@ -28,10 +28,10 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layout_matches_binding():
     lib = L.load()
-    sizes = np.zeros(6, np.int64)
-    assert lib.ua_struct_sizes(L.lptr(sizes), 6) == 0
+    sizes = np.zeros(7, np.int64)
+    assert lib.ua_struct_sizes(L.lptr(sizes), 7) == 0
     ours = [C.sizeof(t) for t in (L.ua_mesh_desc, L.ua_params, L.ua_fields, L.ua_bcs, L.ua_newton_iter,
-                                  L.ua_newton_report)]
+                                  L.ua_newton_report, L.ua_tune_report)]
     assert list(sizes) == ours
 
 

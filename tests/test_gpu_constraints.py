@@ -31,9 +31,11 @@ def _bc_kw(P, kind):
                 ubvbFixedNormalValue=np.zeros(fr.size))
 
 
-def _fixed(P):
-    return dict(ubFixedNode=P.ubFixedNode, ubFixedValue=P.ubFixedValue, vbFixedNode=P.vbFixedNode,
-                vbFixedValue=P.vbFixedValue)
+def _fixed(P, v_free=()):
+    """The problem's fixed u and v nodes, without v at the nodes in v_free (whose v is tied)."""
+    keep = ~np.isin(P.vbFixedNode, np.asarray(v_free, dtype=np.int64))
+    return dict(ubFixedNode=P.ubFixedNode, ubFixedValue=P.ubFixedValue, vbFixedNode=P.vbFixedNode[keep],
+                vbFixedValue=np.asarray(P.vbFixedValue)[keep])
 
 
 def test_constraint_matrix_matches_oracle():
@@ -42,9 +44,10 @@ def test_constraint_matrix_matches_oracle():
     fr = front_nodes(P)
     kw = dict(ubTiedNodeA=bottom, ubTiedNodeB=top, vbTiedNodeA=bottom[:2], vbTiedNodeB=top[:2],
               ubvbFixedNormalNode=fr, ubvbFixedNormalValue=np.linspace(1.0, 2.0, fr.size))
-    Lr, cr = R.create_Luv(P.Nnodes, R.BCs(**_fixed(P), **kw), R.create_mua(P.coordinates, P.connectivity))
+    fx = _fixed(P, v_free=np.concatenate([bottom[:2], top[:2]]))
+    Lr, cr = R.create_Luv(P.Nnodes, R.BCs(**fx, **kw), R.create_mua(P.coordinates, P.connectivity))
     mua = ua.CreateMUA(P.coordinates, P.connectivity)
-    Lg, cg = ua.constraint_matrix(mua, ua.BCs(**_fixed(P), **kw))
+    Lg, cg = ua.constraint_matrix(mua, ua.BCs(**fx, **kw))
     assert Lg.shape == Lr.shape
     assert np.max(np.abs((Lg - Lr).toarray())) <= 1e-15
     assert np.max(np.abs(cg - cr)) <= 1e-15 * np.max(np.abs(cr))

@@ -62,7 +62,8 @@ class Gateway:
         m, n = a.shape
         p = self.lib.mxCreateDoubleMatrix(m, n, 0)
         if m * n:
-            C.memmove(self.lib.mxGetPr(p), np.asfortranarray(a).ctypes.data, 8 * m * n)
+            af = np.asfortranarray(a)  # held until the copy is done: a temporary could be freed first
+            C.memmove(self.lib.mxGetPr(p), af.ctypes.data, 8 * m * n)
         return p
 
     def struct(self, d):

@@ -9,7 +9,7 @@ import scipy.sparse as sp
 import uasource_b200 as ua
 from oracle import ua_ref as R
 from uasource_b200 import synth
-from tests.sliding_cases import LAWS, law_inputs
+from tests.sliding_cases import LAWS, law_inputs, soften_C
 
 pytestmark = pytest.mark.gpu
 K_TOL = 1e-12
@@ -24,7 +24,7 @@ def _row_rel(Kg, Kr):
 
 
 def _inputs(law, nod, nx, ny, transient=False):
-    P = synth.ice_stream_shelf(nx, ny, nod=nod, seed=5, transient=transient)
+    P = soften_C(synth.ice_stream_shelf(nx, ny, nod=nod, seed=5, transient=transient))
     name, mel, extra = law_inputs(law, P.Nnodes, seed=2)
     p = R.Params()
     p.SlidingLaw = name

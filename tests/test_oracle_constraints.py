@@ -35,12 +35,15 @@ def test_constraint_rows_in_multiplier_order():
     bottom, top = tie_nodes(P)
     fr = front_nodes(P)
     vals = np.linspace(1.0, 2.0, fr.size)
-    bcs = R.BCs(ubFixedNode=P.ubFixedNode, ubFixedValue=P.ubFixedValue, vbFixedNode=P.vbFixedNode,
-                vbFixedValue=P.vbFixedValue, ubTiedNodeA=bottom, ubTiedNodeB=top,
+    keep = ~np.isin(P.vbFixedNode, np.concatenate([bottom[:2], top[:2]]))  # v tied there instead
+    bcs = R.BCs(ubFixedNode=P.ubFixedNode, ubFixedValue=P.ubFixedValue, vbFixedNode=P.vbFixedNode[keep],
+                vbFixedValue=np.asarray(P.vbFixedValue)[keep], ubTiedNodeA=bottom, ubTiedNodeB=top,
                 vbTiedNodeA=bottom[:2], vbTiedNodeB=top[:2], ubvbFixedNormalNode=fr, ubvbFixedNormalValue=vals)
     mua = R.create_mua(P.coordinates, P.connectivity)
     L, c = R.create_Luv(Nn, bcs, mua)
-    nu, nv = np.unique(P.ubFixedNode).size, np.unique(P.vbFixedNode).size
+    Ld_ = L.toarray()
+    assert np.all(np.count_nonzero(Ld_, axis=0) <= 1)  # disjoint support: B B' diagonal
+    nu, nv = np.unique(P.ubFixedNode).size, np.unique(P.vbFixedNode[keep]).size
     assert L.shape == (bottom.size + 2 + nu + nv + fr.size, 2 * Nn)
     Ld = L.toarray()
     assert np.allclose(np.sum(Ld * Ld, axis=1), 1.0, rtol=0, atol=1e-15)  # ScaleL: unit rows

@@ -6,5 +6,5 @@ interface on top of it.
 """
 from .ua import (CtrlVar, Fields, BCs, HBCs, MUA, CreateMUA, CreateMUABatch, uvMatrixAssembly, uv, uv_batch,  # noqa: F401,E501
                  uv_resident, uv_batch_resident, uvhAssembly, uvh,
-                 solveKApeSymmetric, adjoint_gradient_C, constraint_matrix, RunInfo)
+                 solveKApeSymmetric, adjoint_gradient_C, constraint_matrix, autotune, RunInfo)
 from .lib import UaError  # noqa: F401

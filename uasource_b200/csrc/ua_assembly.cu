@@ -239,7 +239,7 @@ __device__ __forceinline__ void patch_scatter(const DevMesh& M, const UvOut& out
   using I = ElemIdx<NOD>;
   const int pn0 = M.patch_node_ptr[p];
   const int nr = M.patch_node_ptr[p + 1] - pn0;
-  if (WITHK) {
+  if (WITHK && out.K) {
     const int q0 = M.patch_q_ptr[p], q1 = M.patch_q_ptr[p + 1];
     const int nbase = M.nodeptr[M.sys_node_off[s]];
     const int nnzn = M.sys_nnzn[s];
@@ -323,8 +323,7 @@ __device__ __forceinline__ void patch_scatter(const DevMesh& M, const UvOut& out
 // ---------------------------------------------------------------------------
 namespace p1 {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
+constexpr int kThreads = 256;  // the largest CTA (launch bounds); 128 also runs (asm_threads)
 // scratch slots per lane: residual scalars first, then the drag derivatives
 enum { TX = 0, TY = 1, FX = 2, FY = 3, CXU = 4, CYV = 5, CXV = 6, NSC = 7 };
 
@@ -356,6 +355,9 @@ __global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadT
   const int s = M.patch_sys[p];
   if (in.active && !in.active[s]) return;
   const int E = M.max_patch_elems;
+  // residual-only calls run the same instantiation as the tangent calls of their precision with
+  // out.K null, so both compute R with the same instructions (bit-identical R)
+  const bool kw = WITHK && out.K != nullptr;
   KT* sK = reinterpret_cast<KT*>(smem);
   const size_t koff = WITHK ? (((size_t)I::NKE * E * sizeof(KT) + 15) & ~(size_t)15) : 0;
   double* sR = reinterpret_cast<double*>(smem + koff);  // 12 E
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadT
   double* ws = scr + wid * (NSC * 32);
   const double N0 = sN[j * 3 + 0], N1 = sN[j * 3 + 1], N2 = sN[j * 3 + 2], wj = sN[18 + j];
   const double rhow = S.rhow, g = S.g, ca = S.ca, sa = S.sa;
-  const int ngrp = kWarps * 5;
+  const int ngrp = (blockDim.x >> 5) * 5;  // five elements per warp
 
   for (int base = 0; base < ne; base += ngrp) {  // same trip count for every thread of the block
     const int t = base + wid * 5 + grp;
@@ -470,12 +472,12 @@ __global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadT
     double s_he = hint * eta * detJw;
     double s_pp = 0.5 * g * ca * (rhoint * hint * hint - rhow * dint * dint) * detJw;
     double s_hE = 0;
-    if (WITHK) s_hE = P.Dvisk * 2.0 * hint * (cE * Am * pe / e2) * detJw;
+    if (kw) s_hE = P.Dvisk * 2.0 * hint * (cE * Am * pe / e2) * detJw;
     ws[TX * 32 + lane] = taux * detJw;
     ws[TY * 32 + lane] = tauy * detJw;
     ws[FX * 32 + lane] = (-g * rr * dbdx * ca + rhoint * g * hint * sa) * detJw;
     ws[FY * 32 + lane] = (-g * rr * dbdy * ca) * detJw;
-    if (WITHK) {
+    if (kw) {
       ws[CXU * 32 + lane] = dxu * detJw;
       ws[CYV * 32 + lane] = dyv * detJw;
       ws[CXV * 32 + lane] = dxv * detJw;
@@ -488,7 +490,7 @@ __global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadT
       return __shfl_sync(0xffffffffu, (v + a) + b, g0);
     };
     const double S1 = sum6(s_he), Pp = sum6(s_pp);
-    const double S2 = WITHK ? sum6(s_hE) : 0.0;
+    const double S2 = kw ? sum6(s_hE) : 0.0;
     __syncwarp();
     // sum_ip sc(kind, ip) w(ip) for the element of this lane's group, ip in order
     auto dot = [&](int kind, int a, int b, bool pair) {
@@ -502,7 +504,7 @@ __global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadT
       return acc;
     };
     if (valid) {
-      if (WITHK) {
+      if (kw) {
         const double Pu0 = (2 * exx + eyy) * Dx0 + exy * Dy0, Pu1 = (2 * exx + eyy) * Dx1 + exy * Dy1,
                      Pu2 = (2 * exx + eyy) * Dx2 + exy * Dy2;
         const double Pv0 = (2 * eyy + exx) * Dy0 + exy * Dx0, Pv1 = (2 * eyy + exx) * Dy1 + exy * Dx1,
@@ -548,9 +550,9 @@ __global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadT
   patch_scatter<3, WITHK, KT>(M, out, p, s, uoff, voff, sK, sR, E);
 }
 
-size_t uv_p1_smem(bool withK, bool fp32, int E) {
+size_t uv_p1_smem(bool withK, bool fp32, int E, int threads) {
   size_t k = withK ? (((size_t)ElemIdx<3>::NKE * E * (fp32 ? 4 : 8) + 15) & ~(size_t)15) : 0;
-  return k + (size_t)12 * E * 8 + 24 * 8 + (size_t)p1::kWarps * p1::NSC * 32 * 8;
+  return k + (size_t)12 * E * 8 + 24 * 8 + (size_t)(threads / 32) * p1::NSC * 32 * 8;
 }
 
 // P2 (6-node elements): one element per thread in 128-thread blocks, the
@@ -629,16 +631,17 @@ size_t uv_patch_smem(int nod, bool withK, bool fp32, int E) {
 }
 
 template <bool WITHK, typename KT>
-static cudaError_t launch_p1(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out) {
+static cudaError_t launch_p1(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, int threads) {
   if (quad_table(3).nip != 6) return cudaErrorInvalidConfiguration;  // six lanes, one point each
-  size_t sm = uv_p1_smem(WITHK, sizeof(KT) == 4, m->dm.max_patch_elems);
+  if (threads != 128 && threads != 256) return cudaErrorInvalidConfiguration;
+  size_t sm = uv_p1_smem(WITHK, sizeof(KT) == 4, m->dm.max_patch_elems, threads);
   const bool gen = P.law != UA_SLIDING_WEERTMAN || P.melange;
   auto kern = gen ? uv_p1_kernel<WITHK, KT, true> : uv_p1_kernel<WITHK, KT, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
-  kern<<<m->dm.npatch, p1::kThreads, sm, m->stream>>>(m->dm, quad_table(3), P, in, out);
+  kern<<<m->dm.npatch, threads, sm, m->stream>>>(m->dm, quad_table(3), P, in, out);
   return cudaGetLastError();
 }
 
@@ -655,13 +658,14 @@ static cudaError_t launch_t(const ua_mesh* m, const UvPhys& P, const UvIn& in, c
   return cudaGetLastError();
 }
 
-// threads: CTA size of the P1 kernels (128 or 256; 0 = 256 with K, 128 residual-only)
+// threads: CTA size of the P1 kernel (128 or 256; 0 = 256)
 cudaError_t launch_uv_assembly(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, bool withK,
                                bool fp32K, int threads) {
-  (void)threads;
-  if (m->nod == 3) {
-    if (!withK) return launch_p1<false, double>(m, P, in, out);
-    return fp32K ? launch_p1<true, float>(m, P, in, out) : launch_p1<true, double>(m, P, in, out);
+  if (m->nod == 3) {  // residual-only: the tangent instantiation of the precision with out.K null
+    UvOut o = out;
+    if (!withK) o.K = nullptr;
+    const int t = threads > 0 ? threads : p1::kThreads;
+    return fp32K ? launch_p1<true, float>(m, P, in, o, t) : launch_p1<true, double>(m, P, in, o, t);
   }
   if (!withK) return launch_t<6, false, double>(m, P, in, out, 128);
   return fp32K ? launch_t<6, true, float>(m, P, in, out, 128) : launch_t<6, true, double>(m, P, in, out, 128);

@@ -67,9 +67,10 @@ extern "C" int ua_mesh_flipped(const ua_mesh* m, int32_t* nflipped) {
 }
 
 extern "C" int ua_struct_sizes(int64_t* sizes, int32_t n) {
-  const int64_t all[6] = {(int64_t)sizeof(ua_mesh_desc), (int64_t)sizeof(ua_params), (int64_t)sizeof(ua_fields),
-                          (int64_t)sizeof(ua_bcs), (int64_t)sizeof(ua_newton_iter), (int64_t)sizeof(ua_newton_report)};
-  if (!sizes || n < 0 || n > 6) return ua::set_error(UA_ERR_INVALID, "ua_struct_sizes: bad arguments");
+  const int64_t all[7] = {(int64_t)sizeof(ua_mesh_desc), (int64_t)sizeof(ua_params), (int64_t)sizeof(ua_fields),
+                          (int64_t)sizeof(ua_bcs), (int64_t)sizeof(ua_newton_iter), (int64_t)sizeof(ua_newton_report),
+                          (int64_t)sizeof(ua_tune_report)};
+  if (!sizes || n < 0 || n > 7) return ua::set_error(UA_ERR_INVALID, "ua_struct_sizes: bad arguments");
   for (int i = 0; i < n; ++i) sizes[i] = all[i];
   return UA_OK;
 }

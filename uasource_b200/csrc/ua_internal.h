@@ -69,6 +69,22 @@ struct DevMesh {
   int max_patch_elems;
 };
 
+// Patch shape: the nodes of a system of nn nodes are cut, in Morton order, into patches of
+// pn = clamp(nn / div, 16, cap) nodes (and at most the shared-memory element budget), so that
+// a small mesh still gives enough patches to fill the SMs and a large one gets patches of cap
+// nodes.  div = 0 means pn = cap for every system.
+struct PatchShape {
+  int div = 600;
+  int cap = 128;
+};
+
+// The assembly schedule ua_autotune picks per (device, element type, dofs per node): the patch
+// shape and the CTA size of the P1 kernel (128 or 256 threads).
+struct AsmTuning {
+  PatchShape shape;
+  int threads = 256;
+};
+
 // Host-side mirror plus ownership of device buffers.
 struct DeviceBuffer {
   void* ptr = nullptr;
@@ -121,12 +137,21 @@ struct ua_mesh {
   // the caller reads the tangent back after a Newton solve (ua_uv_newton with Kvals): the
   // tangent must stay the one of the last Newton system, so no tangent is assembled ahead
   bool keep_last_tangent = false;
+  // the shape of the current patch plan and the CTA size of the P1 assembly
+  ua::PatchShape patch_shape;
+  int asm_threads = 256;
 };
 
 namespace ua {
 // allocation helpers (record ownership in the mesh)
 void* dev_alloc(ua_mesh* m, size_t bytes);
+void dev_free(ua_mesh* m, const void* p);
 void dev_free_all(ua_mesh* m);
+// rebuilds the patch plan of a handle with another shape (the results do not depend on it)
+int rebuild_patches(ua_mesh* m, PatchShape shape);
+// the process-wide tuning for (device, nod, ndof), set by ua_autotune; the default if none
+AsmTuning tuned_assembly(int device, int nod, int ndof, bool* tuned = nullptr);
+void set_tuned_assembly(int device, int nod, int ndof, AsmTuning t);
 int set_error(int code, const char* fmt, ...);
 const QuadTable& quad_table(int nod);
 }  // namespace ua

@@ -5,7 +5,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 #include "ua_internal.h"
 
 namespace ua {
@@ -32,6 +35,17 @@ void* dev_alloc(ua_mesh* m, size_t bytes) {
   m->owned.push_back({p, bytes});
   m->device_bytes += bytes;
   return p;
+}
+
+void dev_free(ua_mesh* m, const void* p) {
+  if (!p) return;
+  for (size_t i = 0; i < m->owned.size(); ++i)
+    if (m->owned[i].ptr == p) {
+      cudaFree(m->owned[i].ptr);
+      m->device_bytes -= m->owned[i].bytes;
+      m->owned.erase(m->owned.begin() + i);
+      return;
+    }
 }
 
 void dev_free_all(ua_mesh* m) {
@@ -138,6 +152,202 @@ static int upload_vec(ua_mesh* m, const std::vector<T>& v, const T** d) {
   return rc;
 }
 
+// Shared-memory bytes of one element in the assembly kernel (symmetric uu/vv
+// blocks, full uv block, and Tx,Fx,Ty,Fy) for ndof=2; for ndof=3 nine full blocks
+// and six residual parts.
+static size_t elem_smem_bytes(int nod, int ndof) {
+  if (ndof == 2) return (size_t)(nod * (nod + 1) + nod * nod + 4 * nod) * sizeof(double);
+  return (size_t)(9 * nod * nod + 6 * nod + 19 * nod) * sizeof(double);  // + staged nodal fields
+}
+
+// Largest element count per patch: shared memory of the assembly kernel and,
+// for the uvh kernel (one thread per element node), its block size.
+static int max_patch_elements(int nod, int ndof) {
+  const size_t budget = ndof == 2 ? 160 * 1024 : 200 * 1024;
+  int e = (int)std::min<size_t>(1023, budget / elem_smem_bytes(nod, ndof));
+  if (ndof == 3) e = std::min(e, (nod == 3 ? 512 : 320) / nod);
+  return e;
+}
+
+// Node -> element lists (each sorted by global element id).
+static void node_elements(int nod, int NN, int NE, const std::vector<int>& conn, std::vector<int>& n2e_ptr,
+                          std::vector<int>& n2e) {
+  n2e_ptr.assign(NN + 1, 0);
+  for (int a = 0; a < nod; ++a)
+    for (int e = 0; e < NE; ++e) n2e_ptr[conn[(size_t)a * NE + e] + 1]++;
+  for (int i = 0; i < NN; ++i) n2e_ptr[i + 1] += n2e_ptr[i];
+  n2e.resize(n2e_ptr[NN]);
+  std::vector<int> fill(n2e_ptr.begin(), n2e_ptr.end() - 1);
+  for (int e = 0; e < NE; ++e)  // increasing e => each list sorted; an element lists a node once
+    for (int a = 0; a < nod; ++a) n2e[fill[conn[(size_t)a * NE + e]]++] = e;
+}
+
+// Global (batch) connectivity and coordinates of a handle from its per-system copies.
+static void global_arrays(const ua_mesh* m, std::vector<int>& conn, std::vector<double>& X, std::vector<double>& Y,
+                          std::vector<int>* node_sys) {
+  const int nod = m->nod, nsys = (int)m->sys.size();
+  const int NN = m->h_node_off[nsys], NE = m->h_elem_off[nsys];
+  conn.assign((size_t)nod * NE, 0);
+  X.assign(NN, 0.0); Y.assign(NN, 0.0);
+  if (node_sys) node_sys->assign(NN, 0);
+  for (int s = 0; s < nsys; ++s) {
+    const HostSystem& hs = m->sys[s];
+    int no = m->h_node_off[s], eo = m->h_elem_off[s];
+    for (int i = 0; i < hs.nn; ++i) {
+      X[no + i] = hs.x[i]; Y[no + i] = hs.y[i];
+      if (node_sys) (*node_sys)[no + i] = s;
+    }
+    for (int a = 0; a < nod; ++a)
+      for (int e = 0; e < hs.ne; ++e) conn[(size_t)a * NE + eo + e] = no + hs.conn[(size_t)a * hs.ne + e];
+  }
+}
+
+// The symbolic scatter plan: node patches with their element lists and, per node-level
+// non-zero of a patch row, the packed contribution list (element-local id, local row node,
+// local column node) in increasing global element order.  The contributions of a non-zero
+// are the same whatever the patches, so K and R do not depend on the shape.
+struct PatchPlan {
+  std::vector<int> patch_sys, patch_node_ptr{0}, patch_nodes, patch_elem_ptr{0}, patch_elems;
+  std::vector<int> patch_q_ptr{0}, pq_cptr{0}, prow_diag;
+  std::vector<uint32_t> pq_rk;
+  std::vector<uint16_t> contrib;
+  int max_elems = 0;
+};
+
+static int build_patch_plan(const ua_mesh* m, const std::vector<int>& conn, const std::vector<double>& X,
+                            const std::vector<double>& Y, const std::vector<int>& n2e_ptr, const std::vector<int>& n2e,
+                            PatchShape shape, PatchPlan& P) {
+  const int nod = m->nod, nsys = (int)m->sys.size();
+  const int NE = m->h_elem_off[nsys];
+  const std::vector<int>& nodeptr = m->h_nodeptr;
+  const std::vector<int>& nodecol = m->h_nodecol;
+  const int emax = max_patch_elements(nod, m->ndof);
+  std::vector<int> mark(NE, -1), elocal(NE, -1);
+  for (int s = 0; s < nsys; ++s) {
+    int no = m->h_node_off[s], nn = m->sys[s].nn;
+    double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+    for (int i = 0; i < nn; ++i) {
+      xmin = std::min(xmin, X[no + i]); xmax = std::max(xmax, X[no + i]);
+      ymin = std::min(ymin, Y[no + i]); ymax = std::max(ymax, Y[no + i]);
+    }
+    double span = std::max(xmax - xmin, ymax - ymin);
+    if (!(span > 0)) span = 1;
+    std::vector<std::pair<uint32_t, int>> key(nn);
+    for (int i = 0; i < nn; ++i) {
+      uint32_t qx = (uint32_t)std::min(65535.0, std::floor((X[no + i] - xmin) / span * 65535.0));
+      uint32_t qy = (uint32_t)std::min(65535.0, std::floor((Y[no + i] - ymin) / span * 65535.0));
+      key[i] = {spread16(qx) | (spread16(qy) << 1), no + i};
+    }
+    std::stable_sort(key.begin(), key.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    const int pn = shape.div > 0 ? std::max(16, std::min(shape.cap, nn / shape.div)) : std::max(1, shape.cap);
+    size_t idx = 0;
+    while (idx < key.size()) {
+      std::vector<int> nodes, elems;
+      int stamp = (int)P.patch_sys.size();
+      while (idx < key.size() && (int)nodes.size() < pn) {
+        int g = key[idx].second;
+        int add = 0;
+        for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t) add += (mark[n2e[t]] != stamp);
+        if (!nodes.empty() && (int)elems.size() + add > emax) break;
+        if ((int)elems.size() + add > emax) return set_error(UA_ERR_BAD_MESH, "node %d touches too many elements", g);
+        nodes.push_back(g);
+        for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t)
+          if (mark[n2e[t]] != stamp) { mark[n2e[t]] = stamp; elems.push_back(n2e[t]); }
+        ++idx;
+      }
+      std::sort(elems.begin(), elems.end());
+      for (int i = 0; i < (int)elems.size(); ++i) elocal[elems[i]] = i;
+      P.patch_sys.push_back(s);
+      for (int r = 0; r < (int)nodes.size(); ++r) {
+        int g = nodes[r];
+        int deg = nodeptr[g + 1] - nodeptr[g];
+        for (int k = 0; k < deg; ++k) {
+          int j = nodecol[nodeptr[g] + k];
+          if (j == g) P.prow_diag.push_back((int)P.pq_rk.size());
+          P.pq_rk.push_back(((uint32_t)r << 16) | (uint32_t)k);
+          for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t) {  // sorted global element order
+            int e = n2e[t];
+            int a = -1, b = -1;
+            for (int c = 0; c < nod; ++c) {
+              int v = conn[(size_t)c * NE + e];
+              if (v == g) a = c;
+              if (v == j) b = c;
+            }
+            if (b >= 0) P.contrib.push_back(pack_contrib(elocal[e], a, b));
+          }
+          P.pq_cptr.push_back((int)P.contrib.size());
+        }
+      }
+      P.patch_nodes.insert(P.patch_nodes.end(), nodes.begin(), nodes.end());
+      P.patch_node_ptr.push_back((int)P.patch_nodes.size());
+      P.patch_elems.insert(P.patch_elems.end(), elems.begin(), elems.end());
+      P.patch_elem_ptr.push_back((int)P.patch_elems.size());
+      P.patch_q_ptr.push_back((int)P.pq_rk.size());
+      P.max_elems = std::max(P.max_elems, (int)elems.size());
+    }
+  }
+  return UA_OK;
+}
+
+// Uploads a plan into the handle, releasing the buffers of the plan it replaces.
+static int install_patch_plan(ua_mesh* m, const PatchPlan& P) {
+  DevMesh& dm = m->dm;
+  const void* old[10] = {dm.patch_sys, dm.patch_node_ptr, dm.patch_nodes, dm.patch_elem_ptr, dm.patch_elems,
+                         dm.patch_q_ptr, dm.pq_rk, dm.pq_cptr, dm.contrib, dm.prow_diag};
+  if (m->stream) UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  for (const void* q : old) dev_free(m, q);
+  int rc;
+  if ((rc = upload_vec(m, P.patch_sys, &dm.patch_sys))) return rc;
+  if ((rc = upload_vec(m, P.patch_node_ptr, &dm.patch_node_ptr))) return rc;
+  if ((rc = upload_vec(m, P.patch_nodes, &dm.patch_nodes))) return rc;
+  if ((rc = upload_vec(m, P.patch_elem_ptr, &dm.patch_elem_ptr))) return rc;
+  if ((rc = upload_vec(m, P.patch_elems, &dm.patch_elems))) return rc;
+  if ((rc = upload_vec(m, P.patch_q_ptr, &dm.patch_q_ptr))) return rc;
+  if ((rc = upload_vec(m, P.pq_rk, &dm.pq_rk))) return rc;
+  if ((rc = upload_vec(m, P.pq_cptr, &dm.pq_cptr))) return rc;
+  if ((rc = upload_vec(m, P.contrib, &dm.contrib))) return rc;
+  if ((rc = upload_vec(m, P.prow_diag, &dm.prow_diag))) return rc;
+  dm.npatch = (int)P.patch_sys.size();
+  dm.max_patch_elems = P.max_elems;
+  return UA_OK;
+}
+
+namespace ua {
+
+int rebuild_patches(ua_mesh* m, PatchShape shape) {
+  if (shape.cap < 1 || shape.cap > 1024 || shape.div < 0)
+    return set_error(UA_ERR_INVALID, "patch shape (div %d, cap %d) out of range", shape.div, shape.cap);
+  if (m->patch_shape.div == shape.div && m->patch_shape.cap == shape.cap) return UA_OK;
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  std::vector<int> conn, n2e_ptr, n2e;
+  std::vector<double> X, Y;
+  global_arrays(m, conn, X, Y, nullptr);
+  node_elements(m->nod, m->nn_total, m->ne_total, conn, n2e_ptr, n2e);
+  PatchPlan plan;
+  int rc = build_patch_plan(m, conn, X, Y, n2e_ptr, n2e, shape, plan);
+  if (rc) return rc;
+  if ((rc = install_patch_plan(m, plan))) return rc;
+  m->patch_shape = shape;
+  return UA_OK;
+}
+
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, AsmTuning> g_tuned;
+
+AsmTuning tuned_assembly(int device, int nod, int ndof, bool* tuned) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find({device, nod, ndof});
+  if (tuned) *tuned = it != g_tuned.end();
+  return it == g_tuned.end() ? AsmTuning{} : it->second;
+}
+
+void set_tuned_assembly(int device, int nod, int ndof, AsmTuning t) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[{device, nod, ndof}] = t;
+}
+
+}  // namespace ua
+
 // detJ at the element centroid as derivVector.m:96-100 (for the orientation test of
 // TestAndCorrectForInsideOutElements.m).
 static double centroid_detJ(int nod, const double* xe, const double* ye) {
@@ -161,23 +371,6 @@ static void flip(int nod, int* l) {
     int t[6] = {l[0], l[5], l[4], l[3], l[2], l[1]};
     for (int a = 0; a < 6; ++a) l[a] = t[a];
   }
-}
-
-// Shared-memory bytes of one element in the assembly kernel (symmetric uu/vv
-// blocks, full uv block, and Tx,Fx,Ty,Fy) for ndof=2; for ndof=3 nine full blocks
-// and six residual parts.
-static size_t elem_smem_bytes(int nod, int ndof) {
-  if (ndof == 2) return (size_t)(nod * (nod + 1) + nod * nod + 4 * nod) * sizeof(double);
-  return (size_t)(9 * nod * nod + 6 * nod + 19 * nod) * sizeof(double);  // + staged nodal fields
-}
-
-// Largest element count per patch: shared memory of the assembly kernel and,
-// for the uvh kernel (one thread per element node), its block size.
-static int max_patch_elements(int nod, int ndof) {
-  const size_t budget = ndof == 2 ? 160 * 1024 : 200 * 1024;
-  int e = (int)std::min<size_t>(1023, budget / elem_smem_bytes(nod, ndof));
-  if (ndof == 3) e = std::min(e, (nod == 3 ? 512 : 320) / nod);
-  return e;
 }
 
 extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, int32_t ndof, int32_t device,
@@ -239,32 +432,12 @@ extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, in
   }
   int NN = m->h_node_off[nsys], NE = m->h_elem_off[nsys];
   m->nn_total = NN; m->ne_total = NE;
-  std::vector<int> conn((size_t)nod * NE);
-  std::vector<double> X(NN), Y(NN);
-  std::vector<int> node_sys(NN);
-  for (int s = 0; s < nsys; ++s) {
-    const HostSystem& hs = m->sys[s];
-    int no = m->h_node_off[s], eo = m->h_elem_off[s];
-    for (int i = 0; i < hs.nn; ++i) { X[no + i] = hs.x[i]; Y[no + i] = hs.y[i]; node_sys[no + i] = s; }
-    for (int a = 0; a < nod; ++a)
-      for (int e = 0; e < hs.ne; ++e) conn[(size_t)a * NE + eo + e] = no + hs.conn[(size_t)a * hs.ne + e];
-  }
+  std::vector<int> conn, node_sys;
+  std::vector<double> X, Y;
+  global_arrays(m, conn, X, Y, &node_sys);
   // ---- node -> element CSR -------------------------------------------------------
-  std::vector<int> n2e_ptr(NN + 1, 0), n2e;
-  for (int a = 0; a < nod; ++a)
-    for (int e = 0; e < NE; ++e) n2e_ptr[conn[(size_t)a * NE + e] + 1]++;
-  for (int i = 0; i < NN; ++i) n2e_ptr[i + 1] += n2e_ptr[i];
-  n2e.resize(n2e_ptr[NN]);
-  {
-    std::vector<int> fill(n2e_ptr.begin(), n2e_ptr.end() - 1);
-    for (int e = 0; e < NE; ++e)       // increasing e => each list sorted
-      for (int a = 0; a < nod; ++a) {
-        int g = conn[(size_t)a * NE + e];
-        // an element lists a node once, so no duplicate within a list
-        n2e[fill[g]++] = e;
-      }
-    for (int g = 0; g < NN; ++g) std::sort(n2e.begin() + n2e_ptr[g], n2e.begin() + n2e_ptr[g + 1]);
-  }
+  std::vector<int> n2e_ptr, n2e;
+  node_elements(nod, NN, NE, conn, n2e_ptr, n2e);
   for (int g = 0; g < NN; ++g)
     if (n2e_ptr[g + 1] == n2e_ptr[g]) { delete m; return set_error(UA_ERR_BAD_MESH, "node %d belongs to no element", g); }
   // ---- node-level adjacency (sorted, includes self) ------------------------------
@@ -302,83 +475,20 @@ extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, in
   m->ndof_total = m->h_dof_off[nsys];
   m->nnz_total = knz;
   // ---- patches (Morton-ordered node groups within each system) --------------------
-  const int emax = max_patch_elements(nod, ndof);
-  std::vector<int> patch_sys, patch_node_ptr(1, 0), patch_nodes, patch_elem_ptr(1, 0), patch_elems;
-  std::vector<int> patch_q_ptr(1, 0), pq_cptr(1, 0), prow_diag;
-  std::vector<uint32_t> pq_rk;
-  std::vector<uint16_t> contrib;
-  std::vector<int> mark(NE, -1);
-  std::vector<int> elocal(NE, -1);
-  for (int s = 0; s < nsys; ++s) {
-    int no = m->h_node_off[s], nn = m->sys[s].nn;
-    double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
-    for (int i = 0; i < nn; ++i) {
-      xmin = std::min(xmin, X[no + i]); xmax = std::max(xmax, X[no + i]);
-      ymin = std::min(ymin, Y[no + i]); ymax = std::max(ymax, Y[no + i]);
-    }
-    double span = std::max(xmax - xmin, ymax - ymin);
-    if (!(span > 0)) span = 1;
-    std::vector<std::pair<uint32_t, int>> key(nn);
-    for (int i = 0; i < nn; ++i) {
-      uint32_t qx = (uint32_t)std::min(65535.0, std::floor((X[no + i] - xmin) / span * 65535.0));
-      uint32_t qy = (uint32_t)std::min(65535.0, std::floor((Y[no + i] - ymin) / span * 65535.0));
-      key[i] = {spread16(qx) | (spread16(qy) << 1), no + i};
-    }
-    std::stable_sort(key.begin(), key.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    // patch size: enough patches to fill 148 SMs several times, at most 128 nodes
-    int pn = std::max(16, std::min(128, nn / 600));
-    size_t idx = 0;
-    while (idx < key.size()) {
-      std::vector<int> nodes, elems;
-      int stamp = (int)patch_sys.size();
-      while (idx < key.size() && (int)nodes.size() < pn) {
-        int g = key[idx].second;
-        int add = 0;
-        for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t) add += (mark[n2e[t]] != stamp);
-        if (!nodes.empty() && (int)elems.size() + add > emax) break;
-        if ((int)elems.size() + add > emax) { delete m; return set_error(UA_ERR_BAD_MESH, "node %d touches too many elements", g); }
-        nodes.push_back(g);
-        for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t)
-          if (mark[n2e[t]] != stamp) { mark[n2e[t]] = stamp; elems.push_back(n2e[t]); }
-        ++idx;
-      }
-      std::sort(elems.begin(), elems.end());
-      for (int i = 0; i < (int)elems.size(); ++i) elocal[elems[i]] = i;
-      patch_sys.push_back(s);
-      // rows of this patch
-      for (int r = 0; r < (int)nodes.size(); ++r) {
-        int g = nodes[r];
-        int deg = nodeptr[g + 1] - nodeptr[g];
-        for (int k = 0; k < deg; ++k) {
-          int j = nodecol[nodeptr[g] + k];
-          if (j == g) prow_diag.push_back((int)pq_rk.size());
-          pq_rk.push_back(((uint32_t)r << 16) | (uint32_t)k);
-          for (int t = n2e_ptr[g]; t < n2e_ptr[g + 1]; ++t) {  // sorted global element order
-            int e = n2e[t];
-            int a = -1, b = -1;
-            for (int c = 0; c < nod; ++c) {
-              int v = conn[(size_t)c * NE + e];
-              if (v == g) a = c;
-              if (v == j) b = c;
-            }
-            if (b >= 0) contrib.push_back(pack_contrib(elocal[e], a, b));
-          }
-          pq_cptr.push_back((int)contrib.size());
-        }
-      }
-      patch_nodes.insert(patch_nodes.end(), nodes.begin(), nodes.end());
-      patch_node_ptr.push_back((int)patch_nodes.size());
-      patch_elems.insert(patch_elems.end(), elems.begin(), elems.end());
-      patch_elem_ptr.push_back((int)patch_elems.size());
-      patch_q_ptr.push_back((int)pq_rk.size());
-      m->dm.max_patch_elems = std::max(m->dm.max_patch_elems, (int)elems.size());
-    }
+  {
+    const AsmTuning t = tuned_assembly(device, nod, ndof);
+    m->patch_shape = t.shape;
+    m->asm_threads = t.threads;
+  }
+  PatchPlan plan;
+  {
+    int prc = build_patch_plan(m, conn, X, Y, n2e_ptr, n2e, m->patch_shape, plan);
+    if (prc) { delete m; return prc; }
   }
   // ---- upload ----------------------------------------------------------------------
   UA_CUDA_TRY(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
   DevMesh& dm = m->dm;
   dm.nsys = nsys; dm.nn = NN; dm.ne = NE; dm.nod = nod; dm.nip = m->nip; dm.ndof = ndof;
-  dm.npatch = (int)patch_sys.size();
   int rc = UA_OK;
   std::vector<int> knz_off(m->h_knz_off.begin(), m->h_knz_off.end());
   if ((rc = upload_vec(m, conn, &dm.conn))) goto fail;
@@ -391,16 +501,7 @@ extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, in
   if ((rc = upload_vec(m, m->h_dof_off, &dm.sys_dof_off))) goto fail;
   if ((rc = upload_vec(m, knz_off, &dm.sys_knz_off))) goto fail;
   if ((rc = upload_vec(m, m->h_nnzn, &dm.sys_nnzn))) goto fail;
-  if ((rc = upload_vec(m, patch_sys, &dm.patch_sys))) goto fail;
-  if ((rc = upload_vec(m, patch_node_ptr, &dm.patch_node_ptr))) goto fail;
-  if ((rc = upload_vec(m, patch_nodes, &dm.patch_nodes))) goto fail;
-  if ((rc = upload_vec(m, patch_elem_ptr, &dm.patch_elem_ptr))) goto fail;
-  if ((rc = upload_vec(m, patch_elems, &dm.patch_elems))) goto fail;
-  if ((rc = upload_vec(m, patch_q_ptr, &dm.patch_q_ptr))) goto fail;
-  if ((rc = upload_vec(m, pq_rk, &dm.pq_rk))) goto fail;
-  if ((rc = upload_vec(m, pq_cptr, &dm.pq_cptr))) goto fail;
-  if ((rc = upload_vec(m, contrib, &dm.contrib))) goto fail;
-  if ((rc = upload_vec(m, prow_diag, &dm.prow_diag))) goto fail;
+  if ((rc = install_patch_plan(m, plan))) goto fail;
   *out = m;
   return UA_OK;
 fail:

@@ -759,7 +759,22 @@ static T* walloc(ua_mesh* m, size_t n) {
   return (T*)dev_alloc(m, n * sizeof(T));
 }
 
-static int ensure_work(ua_mesh* m) {
+// The patch plan the parameters ask for: patch_nodes > 0 cuts every system into patches of that
+// many nodes; 0 takes the shape tuned for this device, element type and dof count by
+// ua_autotune, or the default.  K and R do not depend on the plan.
+static int ensure_plan(ua_mesh* m, const ua_params* p) {
+  if (!p) return UA_OK;
+  if (p->patch_nodes < 0 || p->patch_nodes > 1024)
+    return set_error(UA_ERR_INVALID, "patch_nodes must be 0 (tuned or default) or 1..1024");
+  if (p->asm_threads != 0 && p->asm_threads != 128 && p->asm_threads != 256)
+    return set_error(UA_ERR_INVALID, "asm_threads must be 0 (tuned or default), 128 or 256");
+  const AsmTuning t = tuned_assembly(m->device, m->nod, m->ndof);
+  m->asm_threads = p->asm_threads > 0 ? p->asm_threads : t.threads;
+  return rebuild_patches(m, p->patch_nodes > 0 ? PatchShape{0, p->patch_nodes} : t.shape);
+}
+
+static int ensure_work(ua_mesh* m, const ua_params* p) {
+  if (int rc = ensure_plan(m, p)) return rc;
   if (m->work) return UA_OK;
   UA_CUDA_TRY(cudaSetDevice(m->device));
   Work* w = new Work();
@@ -1311,7 +1326,7 @@ static int assemble(ua_mesh* m, const ua_params* p, bool withK, bool useDir, con
             parts ? w->Fext : nullptr};
   cudaEvent_t ev[2];
   prof_begin(m, withK ? PK_ASMK : PK_ASMR, ev);
-  cudaError_t e = launch_uv_assembly(m, make_phys(p), in, out, withK, fp32, p->asm_threads);
+  cudaError_t e = launch_uv_assembly(m, make_phys(p), in, out, withK, fp32, m->asm_threads);
   prof_end(m, ev);
   ++g_launches;
   if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "uv assembly launch: %s", cudaGetErrorString(e));
@@ -2931,7 +2946,7 @@ extern "C" int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F
   if (mode != UA_ASM_R && mode != UA_ASM_RK && mode != UA_ASM_ZERO_R) return set_error(UA_ERR_INVALID, "bad mode");
   UA_CUDA_TRY(cudaSetDevice(m->device));
   int rc;
-  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_work(m, p))) return rc;
   Work* w = m->work;
   bool withK = mode == UA_ASM_RK;
   if (withK && (rc = ensure_K(m, p->precision))) return rc;
@@ -2965,13 +2980,84 @@ extern "C" int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F
   return UA_OK;
 }
 
+// The assembly autotuner: times the tangent+residual assembly (the dominant kernel of the uv
+// Newton solve) of this handle's systems at the given fields for each candidate schedule (patch
+// shape x CTA size), keeps the fastest for the handle and records it as the tuned schedule of
+// this device, element type and dof count, which every handle then takes with patch_nodes = 0
+// and asm_threads = 0.  The schedules change where the element work runs, not what is summed in
+// which order, so K and R are the same under every one of them.
+extern "C" int ua_autotune(ua_mesh* m, const ua_params* p, const ua_fields* F, int32_t nF, int32_t reps,
+                           ua_tune_report* rep) {
+  if (!m || !p || !F || !rep) return set_error(UA_ERR_INVALID, "ua_autotune: null argument");
+  if (m->ndof != 2) return set_error(UA_ERR_INVALID, "ua_autotune tunes the uv assembly (ndof=2 handle)");
+  if (nF != 1 && nF != m->dm.nsys) return set_error(UA_ERR_INVALID, "ua_autotune: nF must be 1 or the system count");
+  if (reps < 1) reps = 3;
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  int rc;
+  if ((rc = ensure_work(m, nullptr))) return rc;
+  Work* w = m->work;
+  if ((rc = ensure_K(m, p->precision))) return rc;
+  if ((rc = upload_fields(m, p, F, nF))) return rc;
+  if ((rc = upload_velocity(m, F, nF))) return rc;
+  std::vector<int> sel(w->nsys, 1);
+  if ((rc = set_sel(m, sel))) return rc;
+  ua_params q = *p;
+  q.profile = 0;
+  // candidates: the default shape first; P2 elements run 128-thread CTAs only
+  const PatchShape shapes[] = {{600, 128}, {300, 128}, {150, 128}, {1200, 128}, {300, 64}, {150, 64}, {0, 48}};
+  const int nthr = m->nod == 3 ? 2 : 1;
+  const int thr[2] = {256, 128};
+  std::memset(rep, 0, sizeof(*rep));
+  const PatchShape keep_shape = m->patch_shape;
+  const int keep_threads = m->asm_threads;
+  cudaEvent_t e0, e1;
+  UA_CUDA_TRY(cudaEventCreate(&e0));
+  UA_CUDA_TRY(cudaEventCreate(&e1));
+  int best = -1;
+  for (const PatchShape& sh : shapes) {
+    if ((rc = rebuild_patches(m, sh))) break;
+    for (int ti = 0; ti < nthr && rep->n_candidates < UA_TUNE_MAX; ++ti) {
+      m->asm_threads = thr[ti];
+      if ((rc = assemble(m, &q, true, false, w->X, false))) break;  // warm-up
+      UA_CUDA_TRY(cudaEventRecord(e0, m->stream));
+      for (int r = 0; r < reps && !rc; ++r) rc = assemble(m, &q, true, false, w->X, false);
+      if (rc) break;
+      UA_CUDA_TRY(cudaEventRecord(e1, m->stream));
+      UA_CUDA_TRY(cudaEventSynchronize(e1));
+      float ms = 0;
+      UA_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      const int k = rep->n_candidates++;
+      rep->div[k] = sh.div; rep->cap[k] = sh.cap; rep->threads[k] = thr[ti];
+      rep->ms[k] = ms / reps;
+      if (best < 0 || rep->ms[k] < rep->ms[best]) best = k;
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc || best < 0) {  // leave the handle as it was
+    m->asm_threads = keep_threads;
+    int rc2 = rebuild_patches(m, keep_shape);
+    return rc ? rc : (rc2 ? rc2 : set_error(UA_ERR_INVALID, "ua_autotune: no candidate ran"));
+  }
+  AsmTuning t;
+  t.shape = PatchShape{rep->div[best], rep->cap[best]};
+  t.threads = rep->threads[best];
+  if ((rc = rebuild_patches(m, t.shape))) return rc;
+  m->asm_threads = t.threads;
+  set_tuned_assembly(m->device, m->nod, m->ndof, t);
+  rep->chosen = best;
+  rep->default_ms = rep->ms[0];
+  return UA_OK;
+}
+
 static int newton_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs* bcs, int nF,
                          std::vector<ua_newton_report*>& rep, double** lam_io, const int* nl_io) {
   if (m->ndof != 2) return set_error(UA_ERR_INVALID, "uv Newton needs a ndof=2 mesh handle");
   UA_CUDA_TRY(cudaSetDevice(m->device));
   int rc;
   double t0 = now_ms();
-  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_work(m, p))) return rc;
   if ((rc = ensure_K(m, p->precision))) return rc;
   if ((rc = upload_fields(m, p, F, nF))) return rc;
   if ((rc = upload_velocity(m, F, nF))) return rc;
@@ -3537,7 +3623,7 @@ extern "C" int ua_uv_adjoint_dIdC(ua_mesh* m, const ua_params* p, const ua_field
   q.precision = UA_PREC_FP64;
   q.krylov_adaptive = 0;
   int rc;
-  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_work(m, p))) return rc;
   if ((rc = ensure_K(m, UA_PREC_FP64))) return rc;
   if ((rc = upload_fields(m, &q, F, 1))) return rc;
   if ((rc = upload_velocity(m, F, 1))) return rc;
@@ -3634,7 +3720,7 @@ extern "C" int ua_uvh_assemble(ua_mesh* m, const ua_params* p, const ua_fields* 
   if (mode != UA_ASM_R && mode != UA_ASM_RK && mode != UA_ASM_ZERO_R) return set_error(UA_ERR_INVALID, "bad mode");
   UA_CUDA_TRY(cudaSetDevice(m->device));
   int rc;
-  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_work(m, p))) return rc;
   Work* w = m->work;
   const bool withK = mode == UA_ASM_RK;
   if (withK && (rc = ensure_K(m, UA_PREC_FP64))) return rc;
@@ -3659,7 +3745,7 @@ static int uvh_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_bcs
   UA_CUDA_TRY(cudaSetDevice(m->device));
   int rc;
   double t0 = now_ms();
-  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_work(m, p))) return rc;
   if ((rc = ensure_K(m, UA_PREC_FP64))) return rc;
   if ((rc = upload_fields_uvh(m, p, F, nF))) return rc;
   if ((rc = build_constraints(m, bcs, nF))) return rc;
@@ -3774,7 +3860,7 @@ static int uvh_active_set(ua_mesh* m, const ua_params* p, ua_fields* F, const ua
   // the consistent mass matrix for the reactions (MassMatrix2D1dof.m)
   int rc;
   UA_CUDA_TRY(cudaSetDevice(m->device));
-  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_work(m, p))) return rc;
   const size_t nnzn = (size_t)m->h_nodeptr.back();
   if ((rc = ensure_adj_buf(m, nnzn + 9 * (size_t)nn + kAdjDotBlocks + 16))) return rc;
   double* Mval = m->work->adj_buf;
@@ -3904,7 +3990,7 @@ extern "C" int ua_serve_setup(ua_mesh* m, const ua_params* p, const ua_bcs* bcs)
   if (m->ndof != 2) return set_error(UA_ERR_INVALID, "serving runs the uv solve (ndof=2 handle)");
   UA_CUDA_TRY(cudaSetDevice(m->device));
   int rc;
-  if ((rc = ensure_work(m))) return rc;
+  if ((rc = ensure_work(m, p))) return rc;
   if ((rc = ensure_K(m, p->precision))) return rc;
   if ((rc = build_constraints(m, bcs, m->dm.nsys))) return rc;
   Work* w = m->work;

@@ -142,6 +142,15 @@ class ua_newton_report(C.Structure):
                 ("hpos_node", _ip)]
 
 
+UA_TUNE_MAX = 16
+
+
+class ua_tune_report(C.Structure):
+    _fields_ = [("n_candidates", C.c_int32), ("div", C.c_int32 * UA_TUNE_MAX), ("cap", C.c_int32 * UA_TUNE_MAX),
+                ("threads", C.c_int32 * UA_TUNE_MAX), ("ms", C.c_double * UA_TUNE_MAX), ("chosen", C.c_int32),
+                ("default_ms", C.c_double)]
+
+
 # symbol -> (restype, argtypes); every function declared in include/ua_ssa.h
 SIGNATURES = {
     "ua_version": (C.c_char_p, []),
@@ -175,6 +184,8 @@ SIGNATURES = {
     "ua_mem_info": (C.c_int, [C.c_int32, _lp, _lp]),
     "ua_constraint_count": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), C.c_int32, _ip]),
     "ua_constraint_matrix": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), _ip, _ip, _dp, _dp]),
+    "ua_autotune": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.c_int32, C.c_int32,
+                              C.POINTER(ua_tune_report)]),
     "ua_uv_adjoint_dIdC": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),
                                      C.POINTER(ua_measurements), C.c_int32, _dp, _dp, _dp, _dp, _ip]),
     "ua_solve_kape_symmetric": (C.c_int, [C.c_int32, _lp, _lp, _dp, C.c_int32, _lp, _lp, _dp, _dp, _dp, _dp, _dp,

@@ -648,6 +648,30 @@ def adjoint_gradient_C(ctrl: CtrlVar, mua: MUA, F: Fields, bcs_adjoint: BCs, us,
     return I.value, dIduv, lam, g, its.value
 
 
+def autotune(ctrl: CtrlVar, mua: MUA, F, reps=3):
+    """Tunes the assembly schedule of a uv handle (patch shape and P1 CTA size) at the fields F
+    (one Fields for every system, or a list with one per system) and makes the fastest the
+    process-wide schedule for this device, element type and dof count (used by every handle with
+    ``patch_nodes = 0`` and ``asm_threads = 0``).  Returns a dict with the candidates, their mean
+    launch times (ms), the chosen one and the default schedule's time.  Results do not depend on
+    the schedule."""
+    lib = L.load()
+    keep = _Keep()
+    Fs = F if isinstance(F, (list, tuple)) else [F]
+    cfs = (L.ua_fields * len(Fs))()
+    for k, Fk in enumerate(Fs):
+        Nn = mua.Nnodes(k) if len(Fs) > 1 else mua.Nnodes()
+        cf, _, _ = _c_fields(Fk, keep, Nn)
+        cfs[k] = cf
+    p = ctrl.to_c()
+    rep = L.ua_tune_report()
+    L.check(lib.ua_autotune(mua.handle, C.byref(p), cfs, len(Fs), reps, C.byref(rep)))
+    n = rep.n_candidates
+    cands = [dict(div=rep.div[i], cap=rep.cap[i], threads=rep.threads[i], ms=rep.ms[i]) for i in range(n)]
+    return dict(candidates=cands, chosen=cands[rep.chosen], default_ms=rep.default_ms,
+                gain=rep.default_ms / cands[rep.chosen]["ms"])
+
+
 def constraint_matrix(mua: MUA, bcs: BCs):
     """The constraint matrix L and right-hand side c of ``bcs`` on a single-mesh handle, as the
     solvers impose them (BCs2MLC.m -> CreateLuv.m, createLh.m for fixed h on an ndof=3 handle,
