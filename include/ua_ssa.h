@@ -361,11 +361,14 @@ int ua_uvh_newton_batch(ua_mesh* m, const ua_params* p, ua_fields* fields, const
  *                    F[k] (start velocities = warm start).
  *   ua_serve_step  : one Newton iteration of every active slot; finished[i]=1
  *                    for slots whose solve ended in this step; *nactive = busy slots.
- *   ua_serve_result: solution and report of a finished slot. */
+ *   ua_serve_result: solution and report of a finished slot.
+ *   ua_serve_cancel: between steps, drop active slots sys[k] from the iteration (they are free
+ *                    again; the other slots' results are unchanged bit for bit). */
 int ua_serve_setup(ua_mesh* m, const ua_params* p, const ua_bcs* bcs);
 int ua_serve_begin(ua_mesh* m, const ua_params* p, int32_t count, const int32_t* sys, const ua_fields* F);
 int ua_serve_step(ua_mesh* m, const ua_params* p, int32_t* finished, int32_t* nactive);
 int ua_serve_result(ua_mesh* m, int32_t sys, double* ub, double* vb, ua_newton_report* rep);
+int ua_serve_cancel(ua_mesh* m, int32_t count, const int32_t* sys);
 
 /* Velocity data of the misfit (Meas in Misfit.m:38-66 with CtrlVar.Inverse.Measurements "-uv-"):
  * measured surface velocities and their standard errors uErr = sqrt(diag(Meas.usCov)),

@@ -70,3 +70,76 @@ def test_mixed_served_within_tolerance_of_plain_fp64():
         assert np.linalg.norm(u - u64) <= 1e-8 * np.linalg.norm(u64)
         mua.close()
     srv.close()
+
+
+def _solve_alone(ctrl, P, C):
+    mua = ua.CreateMUA(P.coordinates, P.connectivity)
+    F = ua.Fields.from_problem(P)
+    F.C = C
+    Fo, _, _, _, info = ua.uv(ctrl, mua, ua.BCs.from_problem(P), F)
+    mua.close()
+    return Fo, info
+
+
+def test_cancel_leaves_the_other_slots_bit_identical():
+    """A request cancelled from another thread between steps (one active, one still queued)
+    frees its slot; every other request's result is the one it gets alone, bit for bit."""
+    import threading
+    tpl = _templates()
+    ctrl = ua.CtrlVar(precision=L.UA_PREC_MIXED, krylov_rtol=1e-6).set_force_tolerance(1e-20)
+    srv = SsaServer(tpl, ctrl, replicas=1)
+    reqs = _requests(tpl, 7, seed=12)
+    for i, r in enumerate(reqs):
+        r.arrival = 0.0 if i < 3 else 10.0  # the last four wait in the queue (offline run)
+    cancelled = {1, 5}
+
+    def on_step(step, server):
+        if step == 2:  # from a host thread, as a client would
+            t = threading.Thread(target=lambda: [server.cancel(rid) for rid in cancelled])
+            t.start()
+            t.join()
+
+    srv.run(reqs, realtime=False, on_step=on_step)
+    for r in reqs:
+        if r.rid in cancelled:
+            assert r.status == "cancelled" and r.info is None
+            continue
+        assert r.status == "done" and r.info.converged
+        Fo, info = _solve_alone(ctrl, tpl[r.template], r.C)
+        assert np.array_equal(Fo.ub, r.ub) and np.array_equal(Fo.vb, r.vb)
+        assert info.iterations == r.info.iterations
+    srv.close()
+
+
+def test_own_mesh_request_is_admitted_by_its_memory_estimate():
+    """A mesh that is not a template is admitted on its device-memory estimate, solved with the
+    resident slots in the same loop, and gives the result it gets alone."""
+    tpl = _templates()
+    ctrl = ua.CtrlVar(precision=L.UA_PREC_FP64, krylov_rtol=1e-12).set_force_tolerance(1e-20)
+    srv = SsaServer(tpl, ctrl, replicas=1)
+    reqs = _requests(tpl, 3, seed=3)
+    P = synth.ice_stream_shelf(27, 14, seed=31)
+    rng = np.random.default_rng(5)
+    own = Request(rid=99, template=None, problem=P, C=perturbed_C(P, rng), ub0=np.zeros(P.Nnodes),
+                  vb0=np.zeros(P.Nnodes))
+    stats = srv.run(reqs + [own], realtime=False)
+    assert stats.completed == 4 and stats.max_active == 4
+    assert own.status == "done" and own.info.converged
+    assert 0 < own.estimate_bytes < srv.free_bytes()
+    Fo, info = _solve_alone(ctrl, P, own.C)
+    assert np.array_equal(Fo.ub, own.ub) and np.array_equal(Fo.vb, own.vb)
+    srv.close()
+
+
+def test_own_mesh_request_is_refused_when_its_estimate_exceeds_free_hbm():
+    tpl = _templates()
+    ctrl = ua.CtrlVar(precision=L.UA_PREC_MIXED, krylov_rtol=1e-6).set_force_tolerance(1e-20)
+    srv = SsaServer(tpl, ctrl, replicas=1)
+    P = synth.ice_stream_shelf(21, 11, seed=32)
+    own = Request(rid=7, template=None, problem=P, C=P.C, ub0=np.zeros(P.Nnodes), vb0=np.zeros(P.Nnodes))
+    srv.reserve_bytes = srv.free_bytes()  # nothing left for a new handle
+    reqs = _requests(tpl, 2, seed=8)
+    stats = srv.run(reqs + [own], realtime=False)
+    assert own.status == "refused" and own.error == L.UA_ERR_OOM and own.info is None
+    assert stats.completed == 2 and all(r.status == "done" for r in reqs)
+    srv.close()

@@ -4108,6 +4108,26 @@ extern "C" int ua_serve_step(ua_mesh* m, const ua_params* p, int32_t* finished, 
   return UA_OK;
 }
 
+// Cancels active slots between steps: they leave the Newton iteration at once and are free for
+// new requests.  The other slots' arithmetic does not see them (per-system reductions and line
+// searches), so their results stay bit-identical.  A slot that is not busy is ignored.
+extern "C" int ua_serve_cancel(ua_mesh* m, int32_t count, const int32_t* sys) {
+  if (!m || !m->work || !m->work->serve) return set_error(UA_ERR_INVALID, "ua_serve_cancel: not set up");
+  if (count < 0 || (count > 0 && !sys)) return set_error(UA_ERR_INVALID, "ua_serve_cancel: bad arguments");
+  ServeState& S = *m->work->serve;
+  for (int k = 0; k < count; ++k) {
+    const int s = sys[k];
+    if (s < 0 || s >= (int)S.busy.size()) return set_error(UA_ERR_INVALID, "slot %d out of range", s);
+    if (!S.busy[s]) continue;
+    S.busy[s] = 0;
+    S.st[s].active = false;
+    S.st[s].converged = false;
+    S.st[s].in_ls = false;
+    S.st[s].kfresh = false;
+  }
+  return UA_OK;
+}
+
 extern "C" int ua_serve_result(ua_mesh* m, int32_t sys, double* ub, double* vb, ua_newton_report* rep) {
   if (!m || !m->work || !m->work->serve) return set_error(UA_ERR_INVALID, "ua_serve_result: not set up");
   if (sys < 0 || sys >= m->work->nsys) return set_error(UA_ERR_INVALID, "slot %d out of range", sys);

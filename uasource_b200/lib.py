@@ -184,6 +184,7 @@ SIGNATURES = {
     "ua_mem_info": (C.c_int, [C.c_int32, _lp, _lp]),
     "ua_constraint_count": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), C.c_int32, _ip]),
     "ua_constraint_matrix": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), _ip, _ip, _dp, _dp]),
+    "ua_serve_cancel": (C.c_int, [C.c_void_p, C.c_int32, _ip]),
     "ua_autotune": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.c_int32, C.c_int32,
                               C.POINTER(ua_tune_report)]),
     "ua_uv_adjoint_dIdC": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),

@@ -10,11 +10,21 @@ between Newton iterations, while the other slots keep iterating
 while others are on the GPU overlaps on the device.  Each slot's arithmetic
 is independent of the other slots (per-system reductions and line searches),
 so a result is the same alone and in the mix.
+
+A request may also carry a mesh that is not a template (``problem``).  It is
+admitted by its own device-memory estimate (bytes per node measured on the
+resident template set, times its node count, with a margin) against the free
+HBM less a reserve: admitted, it gets a handle of its own that is stepped with
+the resident slots and released when it finishes; refused, it ends with status
+"refused" and ``UA_ERR_OOM``.  ``cancel(rid)`` may be called from any thread:
+between two Newton iterations a queued request is dropped and an active one
+leaves its slot (``ua_serve_cancel``), without touching the other slots.
 """
 from __future__ import annotations
 
 import collections
 import ctypes as C
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -32,6 +42,7 @@ class Request:
     ub0: np.ndarray               # warm start
     vb0: np.ndarray
     arrival: float = 0.0          # seconds after the start of the run
+    problem: object = None        # a mesh that is not a template (template is then None)
     # filled by the server
     admitted: float = None
     finished: float = None
@@ -39,6 +50,9 @@ class Request:
     ub: np.ndarray = None
     vb: np.ndarray = None
     info: object = None
+    status: str = None            # "done", "cancelled" or "refused"
+    error: int = 0                # UA_ERR_OOM for a request refused by its memory estimate
+    estimate_bytes: int = None
 
     @property
     def latency(self):
@@ -62,10 +76,15 @@ class ServeStats:
 class SsaServer:
     """Resident templates x replicas slots on one device."""
 
-    def __init__(self, templates, ctrl: CtrlVar, device=0, replicas=None, hbm_fraction=0.5, max_replicas=8):
+    def __init__(self, templates, ctrl: CtrlVar, device=0, replicas=None, hbm_fraction=0.5, max_replicas=8,
+                 reserve_bytes=1 << 30, margin=1.25):
         self.templates = list(templates)
         self.ctrl = ctrl
         self.device = device
+        self.reserve_bytes = int(reserve_bytes)
+        self.margin = float(margin)
+        self._cancel = set()
+        self._lock = threading.Lock()
         lib = L.load()
         if replicas is None:
             replicas = self._replicas_from_hbm(hbm_fraction, max_replicas)
@@ -87,6 +106,25 @@ class SsaServer:
         self.free = collections.defaultdict(collections.deque)
         for s, k in enumerate(self.slot_template):
             self.free[k].append(s)
+        # device bytes per node of a resident, set-up slot: the memory model of admission
+        self.bytes_per_node = self.mua.device_bytes() / max(1, sum(self.templates[k].Nnodes
+                                                                   for k in self.slot_template))
+
+    # -- admission of a mesh that is not a template, by its memory estimate --------------
+    def estimate_bytes(self, P):
+        """Device bytes a handle for problem P is expected to take (set up for serving)."""
+        return int(self.margin * self.bytes_per_node * P.Nnodes)
+
+    def free_bytes(self):
+        free = C.c_int64()
+        total = C.c_int64()
+        L.check(L.load().ua_mem_info(self.device, C.byref(free), C.byref(total)))
+        return free.value
+
+    def cancel(self, rid):
+        """Cancels request rid (queued or active); safe from any thread, applied between steps."""
+        with self._lock:
+            self._cancel.add(rid)
 
     # -- admission by free HBM ---------------------------------------------------------
     def _replicas_from_hbm(self, fraction, max_replicas):
@@ -113,7 +151,7 @@ class SsaServer:
         return len(self.slot_template)
 
     def _fields(self, req: Request, keep: _Keep):
-        P = self.templates[req.template]
+        P = self.templates[req.template] if req.problem is None else req.problem
         F = Fields.from_problem(P)
         F.C = req.C
         F.ub = req.ub0
@@ -121,30 +159,97 @@ class SsaServer:
         cf, _, _ = _c_fields(F, keep, P.Nnodes)
         return cf
 
-    def run(self, requests, realtime=True, sleep=time.sleep):
+    def _result(self, mua, slot, r, P, tnow):
+        lib = L.load()
+        r.ub = np.zeros(P.Nnodes)
+        r.vb = np.zeros(P.Nnodes)
+        rep = L.ua_newton_report()
+        cap = 2 * (self.ctrl.NRitmax + 2)
+        recs = (L.ua_newton_iter * cap)()
+        rep.iters = C.cast(recs, C.POINTER(L.ua_newton_iter))
+        rep.iters_capacity = cap
+        L.check(lib.ua_serve_result(mua.handle, int(slot), L.dptr(r.ub), L.dptr(r.vb), C.byref(rep)))
+        r.info = _report(rep, recs)
+        r.finished = tnow
+        r.status = "done"
+
+    def _admit_own(self, r, now):
+        """A request with its own mesh: admitted on its memory estimate into a handle of its own,
+        else refused with UA_ERR_OOM.  Returns the handle or None."""
+        lib = L.load()
+        P = r.problem
+        r.estimate_bytes = self.estimate_bytes(P)
+        if r.estimate_bytes > self.free_bytes() - self.reserve_bytes:
+            r.status, r.error, r.admitted, r.finished = "refused", L.UA_ERR_OOM, now, now
+            return None
+        mua = MUA([(P.coordinates, P.connectivity)], ndof=2, device=self.device)
+        keep = _Keep()
+        cbs = (L.ua_bcs * 1)()
+        cbs[0] = _c_bcs(BCs.from_problem(P), keep)
+        L.check(lib.ua_serve_setup(mua.handle, C.byref(self._p), cbs))
+        cfs = (L.ua_fields * 1)()
+        cfs[0] = self._fields(r, keep)
+        sys_ids = np.zeros(1, np.int32)
+        L.check(lib.ua_serve_begin(mua.handle, C.byref(self._p), 1, L.iptr(sys_ids), cfs))
+        r.slot, r.admitted = 0, now
+        return mua
+
+    def run(self, requests, realtime=True, sleep=time.sleep, on_step=None):
         """Serve `requests` (sorted by arrival time).  With realtime=False the
-        arrivals are taken as already due when the loop reaches them (offline batch)."""
+        arrivals are taken as already due when the loop reaches them (offline batch).
+        on_step(step, server), if given, runs after every step (for instance to cancel)."""
         lib = L.load()
         queue = collections.deque(sorted(requests, key=lambda r: r.arrival))
         pending = collections.deque()
         active = {}
+        own = {}  # rid -> (handle, request): requests with their own mesh
         nslots = self.nslots
         finished = np.zeros(nslots, np.int32)
+        fin1 = np.zeros(1, np.int32)
         nact = C.c_int32()
         t0 = time.perf_counter()
         steps = 0
         max_active = 0
         done = []
-        while queue or pending or active:
+        while queue or pending or active or own:
             now = time.perf_counter() - t0
             while queue and (queue[0].arrival <= now or not realtime):
                 pending.append(queue.popleft())
-            # admit arrived requests into free slots of their template (FIFO per template)
+            # cancellations (from any thread): queued requests are dropped, active ones leave
+            with self._lock:
+                cancel, self._cancel = self._cancel, set()
+            if cancel:
+                for dq in (queue, pending):
+                    for r in [x for x in dq if x.rid in cancel]:
+                        dq.remove(r)
+                        r.status, r.finished = "cancelled", now
+                        done.append(r)
+                slots = [s for s, r in active.items() if r.rid in cancel]
+                if slots:
+                    L.check(lib.ua_serve_cancel(self.mua.handle, len(slots), L.iptr(np.array(slots, np.int32))))
+                    for s in slots:
+                        r = active.pop(s)
+                        r.status, r.finished = "cancelled", now
+                        self.free[r.template].append(s)
+                        done.append(r)
+                for rid in [x for x in own if x in cancel]:
+                    mua, r = own.pop(rid)
+                    mua.close()
+                    r.status, r.finished = "cancelled", now
+                    done.append(r)
+            # admit arrived requests into free slots of their template (FIFO per template); a
+            # request with its own mesh by its memory estimate
             admit, keep = [], _Keep()
             still = collections.deque()
             while pending:
                 r = pending.popleft()
-                if self.free[r.template]:
+                if r.problem is not None:
+                    h = self._admit_own(r, now)
+                    if h is None:
+                        done.append(r)
+                    else:
+                        own[r.rid] = (h, r)
+                elif self.free[r.template]:
                     r.slot = self.free[r.template].popleft()
                     r.admitted = now
                     admit.append(r)
@@ -159,34 +264,36 @@ class SsaServer:
                 L.check(lib.ua_serve_begin(self.mua.handle, C.byref(self._p), len(admit), L.iptr(sys_ids), cfs))
                 for r in admit:
                     active[r.slot] = r
-            if not active:
+            if not active and not own:
                 if queue and realtime:
                     sleep(max(0.0, queue[0].arrival - (time.perf_counter() - t0)))
                 continue
-            max_active = max(max_active, len(active))
-            L.check(lib.ua_serve_step(self.mua.handle, C.byref(self._p), L.iptr(finished), C.byref(nact)))
+            max_active = max(max_active, len(active) + len(own))
+            if active:
+                L.check(lib.ua_serve_step(self.mua.handle, C.byref(self._p), L.iptr(finished), C.byref(nact)))
+            for rid, (h, r) in list(own.items()):
+                L.check(lib.ua_serve_step(h.handle, C.byref(self._p), L.iptr(fin1), C.byref(nact)))
+                if fin1[0]:
+                    self._result(h, 0, r, r.problem, time.perf_counter() - t0)
+                    h.close()
+                    del own[rid]
+                    done.append(r)
             steps += 1
             tnow = time.perf_counter() - t0
-            for s in np.flatnonzero(finished):
-                r = active.pop(int(s))
-                P = self.templates[r.template]
-                r.ub = np.zeros(P.Nnodes)
-                r.vb = np.zeros(P.Nnodes)
-                rep = L.ua_newton_report()
-                cap = 2 * (self.ctrl.NRitmax + 2)
-                recs = (L.ua_newton_iter * cap)()
-                rep.iters = C.cast(recs, C.POINTER(L.ua_newton_iter))
-                rep.iters_capacity = cap
-                L.check(lib.ua_serve_result(self.mua.handle, int(s), L.dptr(r.ub), L.dptr(r.vb), C.byref(rep)))
-                r.info = _report(rep, recs)
-                r.finished = tnow
-                self.free[r.template].append(int(s))
-                done.append(r)
+            if active:
+                for s in np.flatnonzero(finished):
+                    r = active.pop(int(s))
+                    self._result(self.mua, s, r, self.templates[r.template], tnow)
+                    self.free[r.template].append(int(s))
+                    done.append(r)
+            if on_step is not None:
+                on_step(steps, self)
         makespan = time.perf_counter() - t0
-        lat = sorted(1000 * r.latency for r in done)
-        q = [1000 * (r.admitted - r.arrival) for r in done]
+        served = [r for r in done if r.status == "done"]
+        lat = sorted(1000 * r.latency for r in served)
+        q = [1000 * (r.admitted - r.arrival) for r in served]
         pct = lambda a, f: a[min(len(a) - 1, int(f * len(a)))] if a else float("nan")
-        return ServeStats(len(done), makespan, len(done) / makespan if makespan > 0 else float("nan"),
+        return ServeStats(len(served), makespan, len(served) / makespan if makespan > 0 else float("nan"),
                           pct(lat, 0.5), pct(lat, 0.99), float(np.mean(q)) if q else float("nan"), nslots, steps,
                           max_active, lat)
 
