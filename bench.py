@@ -419,6 +419,11 @@ def run_ours(args):
     if not args.skip_serve:
         serving = _serve_leg(args, ua, L, synth, np, local)
 
+    # P2 legs: the implicit uvh step and the mixed uv solve against the oracle
+    p2 = None
+    if not args.skip_p2 and rank == 0 and world == 1:
+        p2 = _p2_legs(args, ua, L, synth, np)
+
     t_mx = max_over_ranks(sum(per_mx))
     t_b64 = max_over_ranks(sum(per_b64))
     t_plain = max_over_ranks(sum(per_plain))
@@ -553,6 +558,7 @@ def run_ours(args):
             "batched_fp64": {"value": value_b64, "unit": "solves/s", "ms_per_step": t_b64 / len(per_b64),
                              "converged": int(sum(i.converged for i in infos64))},
             "mixed_batched_over_plain_fp64": value / value_plain,
+            "p2": p2,
             "autotune": None if tune is None else {
                 "chosen": tune["chosen"], "default_ms": tune["default_ms"], "tuned_ms": tune["chosen"]["ms"],
                 "gain": tune["gain"], "candidates": len(tune["candidates"]),
@@ -612,6 +618,80 @@ def _serve_leg(args, ua, L, synth, np, device):
             "mean_queue_ms": st.mean_queue_ms, "slots": st.slots, "max_active": st.max_active,
             "makespan_s": st.makespan_s, "converged": int(sum(bool(r.info.converged) for r in reqs)),
             "rel_err_vs_fp64_max": max(errs) if errs else None, "checked": len(errs)}
+
+
+def _oracle_p2(nx, ny):
+    """Oracle uv solve of the nx x ny-vertex P2 ice stream/shelf mesh (seed 0; child process):
+    (seconds, converged, solution [ub; vb])."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from oracle import ua_ref as R
+    from uasource_b200 import synth
+    R.use_compiled_element_loop(True, 1)
+    P = synth.ice_stream_shelf(nx, ny, nod=6, seed=0)
+    p = R.Params()
+    p.set_force_tolerance(1e-20)
+    F = R.Fields(h=P.h, S=P.S, B=P.B, rho=P.rho, AGlen=P.AGlen, n=P.n, C=P.C, m=P.m, ub=P.ub, vb=P.vb)
+    bcs = R.BCs(ubFixedNode=P.ubFixedNode, ubFixedValue=P.ubFixedValue, vbFixedNode=P.vbFixedNode,
+                vbFixedValue=P.vbFixedValue)
+    t = time.perf_counter()
+    res = R.uv(p, R.create_mua(P.coordinates, P.connectivity), bcs, F)
+    return time.perf_counter() - t, bool(res.converged), np.concatenate([res.ub, res.vb])
+
+
+P2_UV = (101, 51)     # 10,000 P2 elements: the largest P2 uv mesh of the oracle leg
+P2_UVH = (201, 101)   # 40,000 P2 elements: the implicit-step leg
+
+
+def _p2_legs(args, ua, L, synth, np):
+    """P2 forms of the path beside the batched headline: the FP64 implicit uvh step (dt = 0.1 a,
+    from the converged diagnostic state) on a 40k-element P2 mesh, and the uv solve on a
+    10k-element P2 mesh in mixed and plain FP64, each against the FP64 oracle's solution."""
+    with _pool(1) as pool:
+        job = pool.apply_async(_oracle_p2, P2_UV)
+        out = {}
+        # uv, mixed vs FP64, against the oracle
+        P = synth.ice_stream_shelf(*P2_UV, nod=6, seed=0)
+        mua = ua.CreateMUA(P.coordinates, P.connectivity)
+        bcs = ua.BCs.from_problem(P)
+        sol = {}
+        for name, prec, rtol in (("fp64", L.UA_PREC_FP64, 1e-12), ("mixed", L.UA_PREC_MIXED, 1e-6)):
+            ctrl = ua.CtrlVar(precision=prec, krylov_rtol=rtol).set_force_tolerance(1e-20)
+            per, res = _timed_calls(lambda: ua.uv(ctrl, mua, bcs, ua.Fields.from_problem(P)), 2, 1)
+            Fo, _, _, _, info = res
+            sol[name] = (np.concatenate([Fo.ub, Fo.vb]), info, 1000 * len(per) / sum(per))
+        mua.close()
+        # uvh step
+        Pt = synth.ice_stream_shelf(*P2_UVH, nod=6, seed=0, transient=True)
+        bt = ua.BCs.from_problem(Pt)
+        m2 = ua.CreateMUA(Pt.coordinates, Pt.connectivity)
+        Fd, _, _, _, _ = ua.uv(ua.CtrlVar(precision=L.UA_PREC_MIXED, krylov_rtol=1e-6).set_force_tolerance(1e-20),
+                               m2, bt, ua.Fields.from_problem(Pt))
+        m2.close()
+        m3 = ua.CreateMUA(Pt.coordinates, Pt.connectivity, ndof=3)
+        F0 = ua.Fields.from_problem(Pt)
+        F0.ub, F0.vb = Fd.ub, Fd.vb
+        hb = ua.HBCs(ubFixedNode=bt.ubFixedNode, ubFixedValue=bt.ubFixedValue, vbFixedNode=bt.vbFixedNode,
+                     vbFixedValue=bt.vbFixedValue)
+        ctrl = ua.CtrlVar().set_force_tolerance(1e-20)
+        per, res = _timed_calls(lambda: ua.uvh(ctrl, m3, F0, F0.copy(), hb, 0.1), 2, 1)
+        info = res[2]
+        m3.close()
+        out["uvh_step"] = {"mesh": f"P2 {P2_UVH[0]}x{P2_UVH[1]} vertices, {Pt.Nele} elements, {Pt.Nnodes} nodes",
+                           "form": "plain FP64, GMRES with the block preconditioner", "dt_a": 0.1,
+                           "steps_per_s": 1000 * len(per) / sum(per), "ms_per_step": sum(per) / len(per),
+                           "newton_iterations": info.iterations, "krylov_iterations": info.krylov_its_total,
+                           "converged": bool(info.converged)}
+        t_or, conv, u_ref = job.get()
+    rel = lambda a: float(np.linalg.norm(a - u_ref) / np.linalg.norm(u_ref))
+    out["uv_vs_oracle"] = {"mesh": f"P2 {P2_UV[0]}x{P2_UV[1]} vertices, {P.Nele} elements, {P.Nnodes} nodes",
+                           "oracle_converged": conv, "oracle_s": t_or,
+                           "fp64": {"solves_per_s": sol["fp64"][2], "rel_err": rel(sol["fp64"][0]),
+                                    "newton_iterations": sol["fp64"][1].iterations},
+                           "mixed": {"solves_per_s": sol["mixed"][2], "rel_err": rel(sol["mixed"][0]),
+                                     "newton_iterations": sol["mixed"][1].iterations},
+                           "tolerance": {"fp64": 1e-10, "mixed": 1e-8}}
+    return out
 
 
 def _big_p2_problem(transient):
@@ -718,6 +798,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-serve", action="store_true")
+    ap.add_argument("--skip-p2", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-templates", type=int, default=16)

@@ -396,6 +396,13 @@ int ua_uv_adjoint_dIdC(ua_mesh* m, const ua_params* p, const ua_fields* F, const
                        const ua_measurements* meas, int32_t flags, double* I, double* dIduv, double* lambda,
                        double* dIdC, int32_t* krylov_its);
 
+/* The bounds-checked debug build (libuassa_debug.so, `make debug`): every kernel that gathers
+ * through the connectivity, the patch element lists, the contribution lists or the node-slice
+ * columns checks the index against its range; the first violation is recorded (site: 1 patch
+ * element id, 2 element node id, 3 contribution element, 4 tangent index, 5 residual row, 6 node-
+ * slice column) and the access is skipped.  enabled = 0 in the release build. */
+int ua_debug_bounds(const ua_mesh* m, int32_t* enabled, int32_t* site, int64_t* index);
+
 /* Free and total device memory (admission by free HBM). */
 int ua_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
 

@@ -817,6 +817,7 @@ struct SellDev {
   const long long* sl_off;
   const int* cols;
   const int *dof_off, *node_off;  // per system
+  unsigned long long* dbg;        // first bounds violation (debug build)
 };
 
 // The four values of a slot (blocks uu, uv, vu, vv) are adjacent, so a lane reads them with one
@@ -920,7 +921,10 @@ __global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 6 : 0) k_sell(SellDev S
       double au = 0, av = 0;
 #pragma unroll 3
       for (int k = 0; k < W; ++k) {
-        const int j = __ldg(cp + 32 * k);
+        int j = __ldg(cp + 32 * k);
+        bool okj = true;
+        UA_CHECK_INDEX(S.dbg, j, S.dof_off[s], S.dof_off[s] + nn, BS_SELL_COL, okj);
+        (void)okj;
         double e[4];
         Quad<KT>::get(vp + 128 * k, e);
         const double xu = to_d(x[j]), xv = to_d(x[j + nn]);
@@ -1321,7 +1325,7 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
 
 static SellDev sell_dev(const ua_mesh* m, const Sell& S) {
   return SellDev{S.sb_sys, S.sb_n0, S.sb_cnt, S.sb_rbu, S.sb_rbv, S.perm, S.sl_off, S.cols,
-                 m->dm.sys_dof_off, m->dm.sys_node_off};
+                 m->dm.sys_dof_off, m->dm.sys_node_off, m->dm.dbg};
 }
 
 int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {

@@ -239,6 +239,8 @@ __device__ __forceinline__ void patch_scatter(const DevMesh& M, const UvOut& out
   using I = ElemIdx<NOD>;
   const int pn0 = M.patch_node_ptr[p];
   const int nr = M.patch_node_ptr[p + 1] - pn0;
+  const int nep = M.patch_elem_ptr[p + 1] - M.patch_elem_ptr[p];  // elements of this patch
+  (void)nep;
   if (WITHK && out.K) {
     const int q0 = M.patch_q_ptr[p], q1 = M.patch_q_ptr[p + 1];
     const int nbase = M.nodeptr[M.sys_node_off[s]];
@@ -255,15 +257,23 @@ __device__ __forceinline__ void patch_scatter(const DevMesh& M, const UvOut& out
       const int c1 = __ldg(M.pq_cptr + t + 1);
       for (int c = __ldg(M.pq_cptr + t); c < c1; ++c) {
         const uint16_t code = __ldg(M.contrib + c);
-        const int el = code >> 6, a = (code >> 3) & 7, b = code & 7;
+        int el = code >> 6;
+        const int a = (code >> 3) & 7, b = code & 7;
+        bool ok = true;
+        UA_CHECK_INDEX(M.dbg, el, 0, nep, BS_CONTRIB_ELEM, ok);
+        if (!ok) continue;
         const int sy = I::sym(a, b);
         uu += sK[sy * E + el];
         vv += sK[(I::NS + sy) * E + el];
         uv += sK[(2 * I::NS + a * NOD + b) * E + el];
         vu += sK[(2 * I::NS + b * NOD + a) * E + el];
       }
-      const size_t b0 = (size_t)kbase + 2 * (size_t)lp;
-      const size_t b1 = (size_t)kbase + 2 * (size_t)nnzn + 2 * (size_t)lp;
+      size_t b0 = (size_t)kbase + 2 * (size_t)lp;
+      size_t b1 = (size_t)kbase + 2 * (size_t)nnzn + 2 * (size_t)lp;
+      bool okk = true;
+      UA_CHECK_INDEX(M.dbg, b0, (size_t)kbase, (size_t)M.sys_knz_off[s + 1] - deg - k, BS_K_INDEX, okk);
+      UA_CHECK_INDEX(M.dbg, b1, (size_t)kbase, (size_t)M.sys_knz_off[s + 1] - deg - k, BS_K_INDEX, okk);
+      if (!okk) continue;
       KT* Ko = reinterpret_cast<KT*>(out.K);
       Ko[b0 + k] = uu;
       Ko[b0 + deg + k] = uv;
@@ -272,13 +282,20 @@ __device__ __forceinline__ void patch_scatter(const DevMesh& M, const UvOut& out
     }
   }
   for (int r = threadIdx.x; r < nr; r += blockDim.x) {
-    const int g = __ldg(M.patch_nodes + pn0 + r);
+    int g = __ldg(M.patch_nodes + pn0 + r);
+    bool okr = true;
+    UA_CHECK_INDEX(M.dbg, g, M.sys_node_off[s], M.sys_node_off[s + 1], BS_R_INDEX, okr);
+    if (!okr) continue;
     const int t = __ldg(M.prow_diag + pn0 + r);
     double tx = 0, fx = 0, ty = 0, fy = 0;
     const int c1 = __ldg(M.pq_cptr + t + 1);
     for (int c = __ldg(M.pq_cptr + t); c < c1; ++c) {
       const uint16_t code = __ldg(M.contrib + c);
-      const int el = code >> 6, a = (code >> 3) & 7;
+      int el = code >> 6;
+      const int a = (code >> 3) & 7;
+      bool ok = true;
+      UA_CHECK_INDEX(M.dbg, el, 0, nep, BS_CONTRIB_ELEM, ok);
+      if (!ok) continue;
       tx += sR[(0 * NOD + a) * E + el];
       fx += sR[(1 * NOD + a) * E + el];
       ty += sR[(2 * NOD + a) * E + el];
@@ -385,9 +402,14 @@ __global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadT
 
   for (int base = 0; base < ne; base += ngrp) {  // same trip count for every thread of the block
     const int t = base + wid * 5 + grp;
-    const bool valid = lane < 30 && t < ne;
-    const int e = __ldg(M.patch_elems + e0 + min(t, ne - 1));
-    const int n0 = __ldg(M.conn + e), n1 = __ldg(M.conn + (size_t)M.ne + e), n2 = __ldg(M.conn + 2 * (size_t)M.ne + e);
+    bool inb = true;
+    int e = __ldg(M.patch_elems + e0 + min(t, ne - 1));
+    UA_CHECK_INDEX(M.dbg, e, 0, M.ne, BS_PATCH_ELEM, inb);
+    int n0 = __ldg(M.conn + e), n1 = __ldg(M.conn + (size_t)M.ne + e), n2 = __ldg(M.conn + 2 * (size_t)M.ne + e);
+    UA_CHECK_INDEX(M.dbg, n0, 0, M.nn, BS_ELEM_NODE, inb);
+    UA_CHECK_INDEX(M.dbg, n1, 0, M.nn, BS_ELEM_NODE, inb);
+    UA_CHECK_INDEX(M.dbg, n2, 0, M.nn, BS_ELEM_NODE, inb);
+    const bool valid = lane < 30 && t < ne && inb;
     // element geometry (derivVector.m:96-109 with the constant P1 derivatives of the
     // basis [xi, 1-xi-eta, eta]); one reciprocal of detJ
     const double x0 = __ldg(M.x + n0), x1 = __ldg(M.x + n1), x2 = __ldg(M.x + n2);
@@ -580,7 +602,10 @@ __global__ void __launch_bounds__(128, 1) uv_patch_kernel(DevMesh M, QuadTable Q
                     double (&An)[NOD], double (&nn)[NOD], double (&Sn)[NOD], double (&Bn)[NOD], double (&rn)[NOD]) {
 #pragma unroll
     for (int a = 0; a < NOD; ++a) {
-      const int gnode = __ldg(M.conn + (size_t)a * M.ne + e);
+      int gnode = __ldg(M.conn + (size_t)a * M.ne + e);
+      bool okn = true;
+      UA_CHECK_INDEX(M.dbg, gnode, 0, M.nn, BS_ELEM_NODE, okn);
+      (void)okn;
       gn[a] = gnode;
       xe[a] = __ldg(M.x + gnode); ye[a] = __ldg(M.y + gnode);
       hn[a] = __ldg(in.h + gnode); sn[a] = __ldg(in.s + gnode);

@@ -33,6 +33,33 @@ __host__ __device__ inline uint16_t pack_contrib(int el, int a, int b) {
   return (uint16_t)((el << 6) | (a << 3) | b);
 }
 
+// Bounds checks of the debug build (`make debug`, -DUA_BOUNDS_CHECK): an index outside [lo, hi)
+// records the check site and the index in the handle's flag (the first one wins), is replaced by
+// lo and marks the access invalid (ok = false), so nothing is read or written out of range.  The
+// release build compiles them out.
+#ifdef UA_BOUNDS_CHECK
+__device__ inline bool in_bounds(unsigned long long* dbg, long long i, long long lo, long long hi, int site) {
+  if (i >= lo && i < hi) return true;
+  if (dbg) atomicCAS(dbg, 0ULL, ((unsigned long long)(site & 0xffff) << 48) | ((unsigned long long)i & 0xffffffffffffULL));
+  return false;
+}
+#define UA_CHECK_INDEX(dbg, i, lo, hi, site, ok)                                               \
+  do {                                                                                         \
+    if (!ua::in_bounds((dbg), (long long)(i), (long long)(lo), (long long)(hi), (site))) {     \
+      (i) = (lo);                                                                              \
+      (ok) = false;                                                                            \
+    }                                                                                          \
+  } while (0)
+#else
+#define UA_CHECK_INDEX(dbg, i, lo, hi, site, ok) \
+  do {                                          \
+  } while (0)
+#endif
+// check sites (bits 48-63 of the recorded flag)
+enum BoundsSite {
+  BS_PATCH_ELEM = 1, BS_ELEM_NODE = 2, BS_CONTRIB_ELEM = 3, BS_K_INDEX = 4, BS_R_INDEX = 5, BS_SELL_COL = 6
+};
+
 struct QuadTable {
   int nip;
   double w[kMaxNip];
@@ -67,6 +94,7 @@ struct DevMesh {
   const uint16_t* contrib;
   const int* prow_diag;       // per patch row (aligned with patch_nodes): pq index of diagonal
   int max_patch_elems;
+  unsigned long long* dbg;    // first bounds violation (debug build; null otherwise)
 };
 
 // Patch shape: the nodes of a system of nn nodes are cut, in Morton order, into patches of

@@ -502,6 +502,14 @@ extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, in
   if ((rc = upload_vec(m, knz_off, &dm.sys_knz_off))) goto fail;
   if ((rc = upload_vec(m, m->h_nnzn, &dm.sys_nnzn))) goto fail;
   if ((rc = install_patch_plan(m, plan))) goto fail;
+#ifdef UA_BOUNDS_CHECK
+  {
+    const std::vector<unsigned long long> zero(1, 0ULL);
+    if ((rc = upload_vec(m, zero, (const unsigned long long**)&dm.dbg))) goto fail;
+  }
+#else
+  dm.dbg = nullptr;
+#endif
   *out = m;
   return UA_OK;
 fail:
@@ -509,4 +517,23 @@ fail:
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   return rc;
+}
+
+// The first bounds violation a kernel of this handle recorded (bounds-checked build only).
+extern "C" int ua_debug_bounds(const ua_mesh* m, int32_t* enabled, int32_t* site, int64_t* index) {
+  if (!m || !enabled || !site || !index) return set_error(UA_ERR_INVALID, "ua_debug_bounds: null argument");
+  *site = 0;
+  *index = 0;
+#ifdef UA_BOUNDS_CHECK
+  *enabled = 1;
+  unsigned long long v = 0;
+  UA_CUDA_TRY(cudaSetDevice(m->device));
+  UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  UA_CUDA_TRY(cudaMemcpy(&v, m->dm.dbg, sizeof(v), cudaMemcpyDeviceToHost));
+  *site = (int32_t)(v >> 48);
+  *index = (int64_t)(v & 0xffffffffffffULL);
+#else
+  *enabled = 0;
+#endif
+  return UA_OK;
 }

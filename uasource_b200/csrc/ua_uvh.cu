@@ -64,8 +64,12 @@ __global__ void __launch_bounds__(NOD == 3 ? 512 : 320) uvh_patch_kernel(DevMesh
   // stage the nodal fields (one thread per element node)
   for (int t = threadIdx.x; t < ne * NOD; t += blockDim.x) {
     const int el = t / NOD, a = t % NOD;
-    const int e = __ldg(M.patch_elems + e0 + el);
-    const int gn = __ldg(M.conn + (size_t)a * M.ne + e);
+    bool inb = true;
+    int e = __ldg(M.patch_elems + e0 + el);
+    UA_CHECK_INDEX(M.dbg, e, 0, M.ne, BS_PATCH_ELEM, inb);
+    int gn = __ldg(M.conn + (size_t)a * M.ne + e);
+    UA_CHECK_INDEX(M.dbg, gn, 0, M.nn, BS_ELEM_NODE, inb);
+    (void)inb;
     double h1 = in.X[hoff + gn], u1 = in.X[uoff + gn], v1 = in.X[voff + gn];
     if (in.dX) { h1 += gam * in.dX[hoff + gn]; u1 += gam * in.dX[uoff + gn]; v1 += gam * in.dX[voff + gn]; }
     const double h0 = __ldg(in.h0 + gn);
@@ -281,10 +285,21 @@ __global__ void __launch_bounds__(NOD == 3 ? 512 : 320) uvh_patch_kernel(DevMesh
       const int cend = __ldg(M.pq_cptr + q + 1);
       for (int c = __ldg(M.pq_cptr + q); c < cend; ++c) {
         const uint16_t code = __ldg(M.contrib + c);
-        const int ce = code >> 6, a = (code >> 3) & 7, b = code & 7;
+        int ce = code >> 6;
+        const int a = (code >> 3) & 7, b = code & 7;
+        bool ok = true;
+        UA_CHECK_INDEX(M.dbg, ce, 0, ne, BS_CONTRIB_ELEM, ok);
+        if (!ok) continue;
         const KT* src = sK + (size_t)(a * 9 * NOD + b) * E + ce;
 #pragma unroll
         for (int i = 0; i < 9; ++i) v[i] += src[(size_t)i * NOD * E];
+      }
+      {
+        size_t last = (size_t)kbase + 6 * (size_t)nnzn + 3 * (size_t)lp + 2 * (size_t)deg + k;  // largest index
+        bool okk = true;
+        UA_CHECK_INDEX(M.dbg, last, (size_t)kbase, (size_t)M.sys_knz_off[s + 1], BS_K_INDEX, okk);
+        (void)last;
+        if (!okk) continue;
       }
 #pragma unroll
       for (int cr = 0; cr < 3; ++cr) {
@@ -295,13 +310,20 @@ __global__ void __launch_bounds__(NOD == 3 ? 512 : 320) uvh_patch_kernel(DevMesh
     }
   }
   for (int r = threadIdx.x; r < nr; r += blockDim.x) {
-    const int gnd = __ldg(M.patch_nodes + pn0 + r);
+    int gnd = __ldg(M.patch_nodes + pn0 + r);
+    bool okr = true;
+    UA_CHECK_INDEX(M.dbg, gnd, M.sys_node_off[s], M.sys_node_off[s + 1], BS_R_INDEX, okr);
+    if (!okr) continue;
     const int q = __ldg(M.prow_diag + pn0 + r);
     double acc[6] = {0, 0, 0, 0, 0, 0};
     const int cend = __ldg(M.pq_cptr + q + 1);
     for (int c = __ldg(M.pq_cptr + q); c < cend; ++c) {
       const uint16_t code = __ldg(M.contrib + c);
-      const int ce = code >> 6, a = (code >> 3) & 7;
+      int ce = code >> 6;
+      const int a = (code >> 3) & 7;
+      bool ok = true;
+      UA_CHECK_INDEX(M.dbg, ce, 0, ne, BS_CONTRIB_ELEM, ok);
+      if (!ok) continue;
 #pragma unroll
       for (int i = 0; i < 6; ++i) acc[i] += sR[(i * NOD + a) * E + ce];
     }

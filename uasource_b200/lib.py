@@ -10,7 +10,8 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libuassa.so")
+# UASOURCE_B200_LIBRARY selects another build of the library (the bounds-checked libuassa_debug.so)
+LIB_PATH = os.environ.get("UASOURCE_B200_LIBRARY") or os.path.join(_HERE, "libuassa.so")
 
 UA_OK = 0
 UA_ERR_INVALID = -1
@@ -185,6 +186,7 @@ SIGNATURES = {
     "ua_constraint_count": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), C.c_int32, _ip]),
     "ua_constraint_matrix": (C.c_int, [C.c_void_p, C.POINTER(ua_bcs), _ip, _ip, _dp, _dp]),
     "ua_serve_cancel": (C.c_int, [C.c_void_p, C.c_int32, _ip]),
+    "ua_debug_bounds": (C.c_int, [C.c_void_p, _ip, _ip, _lp]),
     "ua_autotune": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.c_int32, C.c_int32,
                               C.POINTER(ua_tune_report)]),
     "ua_uv_adjoint_dIdC": (C.c_int, [C.c_void_p, C.POINTER(ua_params), C.POINTER(ua_fields), C.POINTER(ua_bcs),
