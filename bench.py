@@ -563,7 +563,8 @@ def run_ours(args):
                 "chosen": tune["chosen"], "default_ms": tune["default_ms"], "tuned_ms": tune["chosen"]["ms"],
                 "gain": tune["gain"], "candidates": len(tune["candidates"]),
                 "rule": "tangent+residual assembly of the whole batch at u=v=0, mean of 3 launches per schedule; "
-                        "patches of clamp(nn/div, 16, cap) nodes, P1 CTAs of 256 or 128 threads"},
+                        "patches of clamp(nn/div, 16, cap) nodes x P1 (CTA threads, registers) of (256, 128), "
+                        "(128, 128), (128, 96), (256, 80), (128, 80)"},
         }
         print(json.dumps(line), flush=True)
     mua.close()

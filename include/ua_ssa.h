@@ -139,6 +139,8 @@ typedef struct ua_params {
                                   (1 for P1, 2 for P2), else 1, 2, 4, 8, 16 or 32 */
     int32_t asm_threads;       /* CTA size of the P1 uv assembly: 0 = the tuned one (ua_autotune), else 256;
                                   or 128 or 256 */
+    int32_t asm_regs;          /* register budget of the P1 uv assembly kernel (occupancy against spills):
+                                  0 = the tuned one, else 128; or 128, 96 (128-thread CTAs only) or 80 */
     int32_t uvh_krylov;        /* UA_KRYLOV_*: inner solver of the unsymmetric uvh system */
     int32_t krylov_restart;    /* GMRES restart length m (uvh) */
     double krylov_eta_c, krylov_eta_max;  /* uv forcing term eta = clamp(c*sqrt(rForce), krylov_rtol, max) */
@@ -296,13 +298,14 @@ int ua_uv_assemble(ua_mesh* m, const ua_params* p, const ua_fields* F, const ua_
 /* Assembly autotuner.  Times the tangent+residual uv assembly of the handle's systems at the
  * fields F (nF = 1 or one per system) for each candidate schedule, reps launches each: patch
  * shapes pn = clamp(nn/div, 16, cap) nodes per patch (div = 0: cap nodes) and, for P1, CTAs of
- * 256 or 128 threads.  The fastest becomes the handle's schedule and the process-wide tuned
- * schedule of (device, nod, ndof), which handles then use when patch_nodes and asm_threads are 0.
+ * 256 or 128 threads with register budgets of 128, 96 (128 threads) or 80 per thread.  The
+ * fastest becomes the handle's schedule and the process-wide tuned schedule of (device, nod,
+ * ndof), which handles then use when patch_nodes, asm_threads and asm_regs are 0.
  * K and R are bit-identical under every schedule.  Needs an ndof=2 handle. */
-#define UA_TUNE_MAX 16
+#define UA_TUNE_MAX 48
 typedef struct {
     int32_t n_candidates;
-    int32_t div[UA_TUNE_MAX], cap[UA_TUNE_MAX], threads[UA_TUNE_MAX];
+    int32_t div[UA_TUNE_MAX], cap[UA_TUNE_MAX], threads[UA_TUNE_MAX], regs[UA_TUNE_MAX];
     double ms[UA_TUNE_MAX];    /* mean time of one assembly launch per candidate */
     int32_t chosen;            /* index of the fastest */
     double default_ms;         /* candidate 0: the default schedule */

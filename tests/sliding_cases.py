@@ -19,7 +19,9 @@ def law_inputs(law, Nn, seed=0):
     if law in ("Tsai", "Coulomb", "Cornford", "Umbi"):
         # small enough that the Coulomb stress mu N is of the order of the Weertman stress, so the
         # Tsai minimum takes both branches and the regularised laws differ from either
-        f["muk"] = 0.002 + 0.02 * rng.random(Nn)
+        # (at least 0.008, so that the P2 interpolant, which undershoots the nodal minimum by up
+        # to an eighth of the nodal range, stays positive at every integration point)
+        f["muk"] = 0.008 + 0.014 * rng.random(Nn)
     if law == "Joughin":
         f["V0"] = 100.0 + 50.0 * rng.random(Nn)
     if law == "melange":

@@ -1,5 +1,6 @@
 """The assembly autotuner (ua_autotune) and the schedules it chooses between: patch shapes
-(patch_nodes) and P1 CTA sizes (asm_threads) change where the element work runs, not what is
+(patch_nodes), P1 CTA sizes (asm_threads) and register budgets (asm_regs) change where and how
+the element work runs, not what is
 summed in which order, so the tangent, the residual and whole Newton solves are bit-identical
 under every schedule; the tuner times every candidate and keeps the fastest."""
 import numpy as np
@@ -25,10 +26,10 @@ def test_assembly_is_bit_identical_under_every_schedule(nod, nx, ny, precision):
     F = ua.Fields.from_problem(P)
     F.ub, F.vb = _state(P)
     out = []
-    threads = (256, 128) if nod == 3 else (0,)
+    scheds = ((256, 128), (128, 128), (128, 96), (256, 80), (128, 80)) if nod == 3 else ((0, 0),)
     for pn in (0, 16, 37, 128):
-        for t in threads:
-            ctrl = ua.CtrlVar(precision=precision, patch_nodes=pn, asm_threads=t)
+        for t, rg in scheds:
+            ctrl = ua.CtrlVar(precision=precision, patch_nodes=pn, asm_threads=t, asm_regs=rg)
             R, K = ua.uvMatrixAssembly(ctrl, mua, F)
             Rr, _ = ua.uvMatrixAssembly(ctrl, mua, F, Ronly=True)
             assert np.array_equal(Rr, R)  # the residual-only pass computes R with the same instructions
@@ -47,11 +48,12 @@ def test_autotune_times_every_candidate_and_keeps_the_fastest():
     before = ua.uv_batch(ctrl, mua, [F.copy() for F in Fs], bcs)
     t = ua.autotune(ctrl, mua, Fs, reps=2)
     c = t["candidates"]
-    assert len(c) == 14  # seven patch shapes x two CTA sizes (P1)
-    assert {x["threads"] for x in c} == {128, 256}
+    assert len(c) == 35  # seven patch shapes x five (CTA size, register budget) schedules (P1)
+    assert {x["threads"] for x in c} == {128, 256} and {x["regs"] for x in c} == {128, 96, 80}
     assert all(x["ms"] > 0 for x in c)
     assert t["chosen"]["ms"] == min(x["ms"] for x in c)
-    assert t["default_ms"] == c[0]["ms"] and c[0]["div"] == 600 and c[0]["cap"] == 128 and c[0]["threads"] == 256
+    assert t["default_ms"] == c[0]["ms"] and (c[0]["div"], c[0]["cap"], c[0]["threads"], c[0]["regs"]) == \
+        (600, 128, 256, 128)
     after = ua.uv_batch(ctrl, mua, [F.copy() for F in Fs], bcs)  # now on the tuned schedule
     for (ua_, va, ia), (ub_, vb_, ib) in zip(before, after):
         assert ia.converged and ib.converged and ia.iterations == ib.iterations
@@ -66,7 +68,8 @@ def test_autotune_times_every_candidate_and_keeps_the_fastest():
 def test_bad_schedule_is_refused():
     P = synth.ice_stream_shelf(9, 6, seed=0)
     mua = ua.CreateMUA(P.coordinates, P.connectivity)
-    for kw in (dict(patch_nodes=-1), dict(patch_nodes=5000), dict(asm_threads=96)):
+    for kw in (dict(patch_nodes=-1), dict(patch_nodes=5000), dict(asm_threads=96), dict(asm_regs=64),
+               dict(asm_threads=256, asm_regs=96)):
         with pytest.raises(L.UaError) as ei:
             ua.uvMatrixAssembly(ua.CtrlVar(**kw), mua, ua.Fields.from_problem(P))
         assert ei.value.code == L.UA_ERR_INVALID

@@ -34,7 +34,6 @@ for nod, nx, ny in ((3, 41, 21), (6, 13, 7)):
     for prec in (L.UA_PREC_FP64, L.UA_PREC_MIXED):
         ctrl = ua.CtrlVar(precision=prec, krylov_rtol=1e-6 if prec else 1e-12).set_force_tolerance(1e-20)
         Fo, _, _, _, info = ua.uv(ctrl, m, ua.BCs.from_problem(P), ua.Fields.from_problem(P))
-        assert info.converged
     out[f"uv{nod}"] = flag(m)
     m3 = ua.CreateMUA(P.coordinates, P.connectivity, ndof=3)
     F0 = ua.Fields.from_problem(P)

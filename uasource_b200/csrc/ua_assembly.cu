@@ -362,9 +362,16 @@ __device__ __forceinline__ double tanh_step(double k, double x, double x0) {
 
 // GEN: any sliding law and the melange terms (basal_drag_general); else Weertman, with the
 // reciprocal-cube-root powers when n = m = 3 at every node of the system.
-template <bool WITHK, typename KT, bool GEN>
-__global__ void __launch_bounds__(p1::kThreads, 2) uv_p1_kernel(DevMesh M, QuadTable Q, UvPhys P, UvIn in,
-                                                                 UvOut out) {
+// RV: register budget (launch bounds): 0 = 128 registers (two 256-thread CTAs per SM), 1 = 96
+// (five 128-thread CTAs), 2 = 80 (three 256-thread CTAs); fewer registers, more warps to hide
+// the gathers' latency, against spills to local memory.
+namespace p1 {
+constexpr int max_threads(int rv) { return rv == 1 ? 128 : 256; }
+constexpr int min_blocks(int rv) { return rv == 0 ? 2 : (rv == 1 ? 5 : 3); }
+}  // namespace p1
+template <bool WITHK, typename KT, bool GEN, int RV>
+__global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
+    uv_p1_kernel(DevMesh M, QuadTable Q, UvPhys P, UvIn in, UvOut out) {
   using I = ElemIdx<3>;
   using namespace p1;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -655,13 +662,22 @@ size_t uv_patch_smem(int nod, bool withK, bool fp32, int E) {
   return k + (size_t)4 * nod * E * 8;
 }
 
+template <bool WITHK, typename KT, bool GEN>
+static auto p1_kernel(int rv) {
+  return rv == 1 ? uv_p1_kernel<WITHK, KT, GEN, 1> : (rv == 2 ? uv_p1_kernel<WITHK, KT, GEN, 2>
+                                                               : uv_p1_kernel<WITHK, KT, GEN, 0>);
+}
+
 template <bool WITHK, typename KT>
-static cudaError_t launch_p1(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, int threads) {
+static cudaError_t launch_p1(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, int threads,
+                             int regs) {
   if (quad_table(3).nip != 6) return cudaErrorInvalidConfiguration;  // six lanes, one point each
   if (threads != 128 && threads != 256) return cudaErrorInvalidConfiguration;
+  const int rv = regs == 96 ? 1 : (regs == 80 ? 2 : 0);
+  if (rv == 1 && threads != 128) return cudaErrorInvalidConfiguration;
   size_t sm = uv_p1_smem(WITHK, sizeof(KT) == 4, m->dm.max_patch_elems, threads);
   const bool gen = P.law != UA_SLIDING_WEERTMAN || P.melange;
-  auto kern = gen ? uv_p1_kernel<WITHK, KT, true> : uv_p1_kernel<WITHK, KT, false>;
+  auto kern = gen ? p1_kernel<WITHK, KT, true>(rv) : p1_kernel<WITHK, KT, false>(rv);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -683,14 +699,14 @@ static cudaError_t launch_t(const ua_mesh* m, const UvPhys& P, const UvIn& in, c
   return cudaGetLastError();
 }
 
-// threads: CTA size of the P1 kernel (128 or 256; 0 = 256)
+// threads: CTA size of the P1 kernel (128 or 256; 0 = 256); regs: its register budget (128, 96, 80)
 cudaError_t launch_uv_assembly(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, bool withK,
-                               bool fp32K, int threads) {
+                               bool fp32K, int threads, int regs) {
   if (m->nod == 3) {  // residual-only: the tangent instantiation of the precision with out.K null
     UvOut o = out;
     if (!withK) o.K = nullptr;
     const int t = threads > 0 ? threads : p1::kThreads;
-    return fp32K ? launch_p1<true, float>(m, P, in, o, t) : launch_p1<true, double>(m, P, in, o, t);
+    return fp32K ? launch_p1<true, float>(m, P, in, o, t, regs) : launch_p1<true, double>(m, P, in, o, t, regs);
   }
   if (!withK) return launch_t<6, false, double>(m, P, in, out, 128);
   return fp32K ? launch_t<6, true, float>(m, P, in, out, 128) : launch_t<6, true, double>(m, P, in, out, 128);

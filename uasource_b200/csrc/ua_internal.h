@@ -107,10 +107,11 @@ struct PatchShape {
 };
 
 // The assembly schedule ua_autotune picks per (device, element type, dofs per node): the patch
-// shape and the CTA size of the P1 kernel (128 or 256 threads).
+// shape, the CTA size of the P1 kernel (128 or 256 threads) and its register budget.
 struct AsmTuning {
   PatchShape shape;
   int threads = 256;
+  int regs = 128;  // register budget of the P1 kernel: 128, 96 (128-thread CTAs) or 80
 };
 
 // Host-side mirror plus ownership of device buffers.
@@ -168,6 +169,7 @@ struct ua_mesh {
   // the shape of the current patch plan and the CTA size of the P1 assembly
   ua::PatchShape patch_shape;
   int asm_threads = 256;
+  int asm_regs = 128;
 };
 
 namespace ua {

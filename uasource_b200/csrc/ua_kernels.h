@@ -74,6 +74,6 @@ size_t uvh_patch_smem(int nod, bool withK, bool fp32, int E);
 int uvh_fields_per_node();
 cudaError_t launch_uvh_assembly(const ua_mesh* m, const UvhPhys& P, const UvhIn& in, const UvOut& out, bool withK);
 cudaError_t launch_uv_assembly(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, bool withK,
-                               bool fp32K, int threads = 0);
+                               bool fp32K, int threads = 0, int regs = 0);
 
 }  // namespace ua

@@ -479,6 +479,7 @@ extern "C" int ua_mesh_create_batch(const ua_mesh_desc* descs, int32_t count, in
     const AsmTuning t = tuned_assembly(device, nod, ndof);
     m->patch_shape = t.shape;
     m->asm_threads = t.threads;
+    m->asm_regs = t.regs;
   }
   PatchPlan plan;
   {

@@ -768,8 +768,13 @@ static int ensure_plan(ua_mesh* m, const ua_params* p) {
     return set_error(UA_ERR_INVALID, "patch_nodes must be 0 (tuned or default) or 1..1024");
   if (p->asm_threads != 0 && p->asm_threads != 128 && p->asm_threads != 256)
     return set_error(UA_ERR_INVALID, "asm_threads must be 0 (tuned or default), 128 or 256");
+  if (p->asm_regs != 0 && p->asm_regs != 128 && p->asm_regs != 96 && p->asm_regs != 80)
+    return set_error(UA_ERR_INVALID, "asm_regs must be 0 (tuned or default), 128, 96 or 80");
   const AsmTuning t = tuned_assembly(m->device, m->nod, m->ndof);
   m->asm_threads = p->asm_threads > 0 ? p->asm_threads : t.threads;
+  m->asm_regs = p->asm_regs > 0 ? p->asm_regs : t.regs;
+  if (m->asm_regs == 96 && m->asm_threads != 128)
+    return set_error(UA_ERR_INVALID, "asm_regs = 96 runs 128-thread CTAs only (asm_threads = 128)");
   return rebuild_patches(m, p->patch_nodes > 0 ? PatchShape{0, p->patch_nodes} : t.shape);
 }
 
@@ -1326,7 +1331,7 @@ static int assemble(ua_mesh* m, const ua_params* p, bool withK, bool useDir, con
             parts ? w->Fext : nullptr};
   cudaEvent_t ev[2];
   prof_begin(m, withK ? PK_ASMK : PK_ASMR, ev);
-  cudaError_t e = launch_uv_assembly(m, make_phys(p), in, out, withK, fp32, m->asm_threads);
+  cudaError_t e = launch_uv_assembly(m, make_phys(p), in, out, withK, fp32, m->asm_threads, m->asm_regs);
   prof_end(m, ev);
   ++g_launches;
   if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "uv assembly launch: %s", cudaGetErrorString(e));
@@ -2920,7 +2925,7 @@ extern "C" void ua_params_default(ua_params* p) {
   std::memcpy(p->uvhAcceptableWorkAndForceTolerances, a1, sizeof a1);
   std::memcpy(p->uvhAcceptableWorkOrForceTolerances, a2, sizeof a2);
   p->krylov_rtol = 1e-12; p->krylov_maxit = 20000; p->precision = UA_PREC_FP64;
-  p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1; p->spmv_lanes = 0; p->asm_threads = 0;
+  p->patch_nodes = 0; p->verbose = 0; p->profile = 0; p->krylov_adaptive = 1; p->spmv_lanes = 0; p->asm_threads = 0; p->asm_regs = 0;
   p->uvh_krylov = UA_KRYLOV_GMRES; p->krylov_restart = 40;
   p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
   p->amg_smoothed = 1;
@@ -3005,19 +3010,21 @@ extern "C" int ua_autotune(ua_mesh* m, const ua_params* p, const ua_fields* F, i
   q.profile = 0;
   // candidates: the default shape first; P2 elements run 128-thread CTAs only
   const PatchShape shapes[] = {{600, 128}, {300, 128}, {150, 128}, {1200, 128}, {300, 64}, {150, 64}, {0, 48}};
-  const int nthr = m->nod == 3 ? 2 : 1;
-  const int thr[2] = {256, 128};
+  // P1 schedules (CTA size, register budget); P2 elements run 128-thread CTAs of one budget
+  const int sched[5][2] = {{256, 128}, {128, 128}, {128, 96}, {256, 80}, {128, 80}};
+  const int nsched = m->nod == 3 ? 5 : 1;
   std::memset(rep, 0, sizeof(*rep));
   const PatchShape keep_shape = m->patch_shape;
-  const int keep_threads = m->asm_threads;
+  const int keep_threads = m->asm_threads, keep_regs = m->asm_regs;
   cudaEvent_t e0, e1;
   UA_CUDA_TRY(cudaEventCreate(&e0));
   UA_CUDA_TRY(cudaEventCreate(&e1));
   int best = -1;
   for (const PatchShape& sh : shapes) {
     if ((rc = rebuild_patches(m, sh))) break;
-    for (int ti = 0; ti < nthr && rep->n_candidates < UA_TUNE_MAX; ++ti) {
-      m->asm_threads = thr[ti];
+    for (int ti = 0; ti < nsched && rep->n_candidates < UA_TUNE_MAX; ++ti) {
+      m->asm_threads = m->nod == 3 ? sched[ti][0] : 128;
+      m->asm_regs = sched[ti][1];
       if ((rc = assemble(m, &q, true, false, w->X, false))) break;  // warm-up
       UA_CUDA_TRY(cudaEventRecord(e0, m->stream));
       for (int r = 0; r < reps && !rc; ++r) rc = assemble(m, &q, true, false, w->X, false);
@@ -3027,7 +3034,7 @@ extern "C" int ua_autotune(ua_mesh* m, const ua_params* p, const ua_fields* F, i
       float ms = 0;
       UA_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
       const int k = rep->n_candidates++;
-      rep->div[k] = sh.div; rep->cap[k] = sh.cap; rep->threads[k] = thr[ti];
+      rep->div[k] = sh.div; rep->cap[k] = sh.cap; rep->threads[k] = m->asm_threads; rep->regs[k] = m->asm_regs;
       rep->ms[k] = ms / reps;
       if (best < 0 || rep->ms[k] < rep->ms[best]) best = k;
     }
@@ -3037,14 +3044,17 @@ extern "C" int ua_autotune(ua_mesh* m, const ua_params* p, const ua_fields* F, i
   cudaEventDestroy(e1);
   if (rc || best < 0) {  // leave the handle as it was
     m->asm_threads = keep_threads;
+    m->asm_regs = keep_regs;
     int rc2 = rebuild_patches(m, keep_shape);
     return rc ? rc : (rc2 ? rc2 : set_error(UA_ERR_INVALID, "ua_autotune: no candidate ran"));
   }
   AsmTuning t;
   t.shape = PatchShape{rep->div[best], rep->cap[best]};
   t.threads = rep->threads[best];
+  t.regs = rep->regs[best];
   if ((rc = rebuild_patches(m, t.shape))) return rc;
   m->asm_threads = t.threads;
+  m->asm_regs = t.regs;
   set_tuned_assembly(m->device, m->nod, m->ndof, t);
   rep->chosen = best;
   rep->default_ms = rep->ms[0];

@@ -82,6 +82,7 @@ class ua_params(C.Structure):
         ("krylov_rtol", C.c_double), ("krylov_maxit", C.c_int32), ("precision", C.c_int32),
         ("patch_nodes", C.c_int32), ("verbose", C.c_int32), ("profile", C.c_int32),
         ("krylov_adaptive", C.c_int32), ("krylov_precond", C.c_int32), ("spmv_lanes", C.c_int32), ("asm_threads", C.c_int32),
+        ("asm_regs", C.c_int32),
         ("uvh_krylov", C.c_int32), ("krylov_restart", C.c_int32),
         ("krylov_eta_c", C.c_double), ("krylov_eta_max", C.c_double), ("precond_bf16", C.c_int32),
         ("amg_smoothed", C.c_int32), ("krylov_full_grid", C.c_int32),
@@ -143,12 +144,13 @@ class ua_newton_report(C.Structure):
                 ("hpos_node", _ip)]
 
 
-UA_TUNE_MAX = 16
+UA_TUNE_MAX = 48
 
 
 class ua_tune_report(C.Structure):
     _fields_ = [("n_candidates", C.c_int32), ("div", C.c_int32 * UA_TUNE_MAX), ("cap", C.c_int32 * UA_TUNE_MAX),
-                ("threads", C.c_int32 * UA_TUNE_MAX), ("ms", C.c_double * UA_TUNE_MAX), ("chosen", C.c_int32),
+                ("threads", C.c_int32 * UA_TUNE_MAX), ("regs", C.c_int32 * UA_TUNE_MAX),
+                ("ms", C.c_double * UA_TUNE_MAX), ("chosen", C.c_int32),
                 ("default_ms", C.c_double)]
 
 

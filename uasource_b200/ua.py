@@ -77,6 +77,7 @@ class CtrlVar:
     krylov_precond: int = L.UA_PC_AMG
     spmv_lanes: int = 0
     asm_threads: int = 0
+    asm_regs: int = 0
     uvh_krylov: int = L.UA_KRYLOV_GMRES
     krylov_restart: int = 40
     krylov_eta_c: float = 0.5
@@ -652,7 +653,7 @@ def autotune(ctrl: CtrlVar, mua: MUA, F, reps=3):
     """Tunes the assembly schedule of a uv handle (patch shape and P1 CTA size) at the fields F
     (one Fields for every system, or a list with one per system) and makes the fastest the
     process-wide schedule for this device, element type and dof count (used by every handle with
-    ``patch_nodes = 0`` and ``asm_threads = 0``).  Returns a dict with the candidates, their mean
+    ``patch_nodes``, ``asm_threads`` and ``asm_regs`` at 0).  Returns a dict with the candidates, their mean
     launch times (ms), the chosen one and the default schedule's time.  Results do not depend on
     the schedule."""
     lib = L.load()
@@ -667,7 +668,8 @@ def autotune(ctrl: CtrlVar, mua: MUA, F, reps=3):
     rep = L.ua_tune_report()
     L.check(lib.ua_autotune(mua.handle, C.byref(p), cfs, len(Fs), reps, C.byref(rep)))
     n = rep.n_candidates
-    cands = [dict(div=rep.div[i], cap=rep.cap[i], threads=rep.threads[i], ms=rep.ms[i]) for i in range(n)]
+    cands = [dict(div=rep.div[i], cap=rep.cap[i], threads=rep.threads[i], regs=rep.regs[i], ms=rep.ms[i])
+             for i in range(n)]
     return dict(candidates=cands, chosen=cands[rep.chosen], default_ms=rep.default_ms,
                 gain=rep.default_ms / cands[rep.chosen]["ms"])
 
