@@ -151,9 +151,6 @@ typedef struct ua_params {
     int32_t krylov_full_grid;  /* 0 = the AMG-preconditioned PCG launches only the row and node blocks of
                                   systems still iterating (device-compacted lists, default); 1 = every
                                   block of the batch (same results) */
-    int32_t krylov_fused_reduce; /* 1 = the node-slice PCG sums p.q and r.z in the last CTA of each system
-                                  of the kernels that write them (default); 0 = separate reduction
-                                  kernels (same results) */
     int32_t uvh_h_sweeps;      /* uvh block preconditioner: l1-Jacobi sweeps on the thickness block K_hh
                                   (0 = default 8) */
     int32_t krylov_sell;       /* 1 = the AMG-preconditioned uv PCG runs its SpMV and the V-cycle's

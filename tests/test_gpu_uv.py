@@ -390,24 +390,3 @@ def test_tangent_assembled_ahead_matches_assembly_per_iteration(precision, rtol)
         assert ia.iterations == ib.iterations
         a, b = np.concatenate([Fa.ub, Fa.vb]), np.concatenate([Fb.ub, Fb.vb])
         assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(b)
-
-
-@pytest.mark.parametrize("precision,rtol", [(L.UA_PREC_FP64, 1e-12), (L.UA_PREC_MIXED, 1e-6)])
-@pytest.mark.parametrize("full_grid", [0, 1], ids=["lists", "full"])
-def test_fused_reductions_equal_the_reduction_kernel(precision, rtol, full_grid):
-    """The PCG's p.q and r.z sums finished in the last CTA of each system of the node-slice
-    kernels give bit-identical iterates, iteration counts and solutions to the separate reduction
-    kernel, for a batch of uneven meshes (systems finish at different iterations)."""
-    probs = [synth.ice_stream_shelf(41, 21, seed=0), synth.ice_stream_shelf(15, 8, seed=5),
-             synth.ice_stream_shelf(61, 31, seed=9)]
-    mua = ua.CreateMUABatch([(P.coordinates, P.connectivity) for P in probs])
-    out = []
-    for fused in (1, 0, 1):
-        ctrl = ua.CtrlVar(precision=precision, krylov_rtol=rtol, krylov_fused_reduce=fused,
-                          krylov_full_grid=full_grid).set_force_tolerance(1e-20)
-        res = ua.uv_batch(ctrl, mua, [ua.Fields.from_problem(P) for P in probs], [ua.BCs.from_problem(P) for P in probs])
-        assert all(i.converged for _, _, i in res)
-        out.append([(np.concatenate([u, v]), i.iterations, i.krylov_its_total) for u, v, i in res])
-    for k in (1, 2):
-        for (ua_, na, ka), (ub_, nb, kb) in zip(out[0], out[k]):
-            assert np.array_equal(ua_, ub_) and na == nb and ka == kb

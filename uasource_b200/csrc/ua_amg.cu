@@ -894,7 +894,7 @@ template <typename KT, typename VT, int MODE>
 __global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 6 : 0) k_sell(SellDev S, int nsb, ActList act, const int* sel, const int* done,
                                               const int* depth, const KT* vals, const VT* x, const VT* b,
                                               const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
-                                              double* part, PcgFuse fuse) {
+                                              double* part) {
   const int nv = act.cnt ? *act.cnt : nsb;
   const int w = threadIdx.x >> 5, t = threadIdx.x & 31, pos = w * 32 + t;
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
@@ -957,7 +957,6 @@ __global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 6 : 0) k_sell(SellDev S
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) tw += __shfl_down_sync(0xffffffffu, tw, o);
     if (t == 0) part[sb * kSellSlices + w] = tw;
-    if (fuse.stage) pcg_fused_tail(fuse, S.sb_sys[sb], kSellSlices, part);  // uniform per launch
   }
 }
 
@@ -1432,7 +1431,7 @@ void amg_sell_partials(const ua_mesh* m, const double** spart, const int** sys_s
   *sys_sl_off = m->amg->sell.sys_sl_off;
 }
 
-int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const PcgFuse& fuse, const int* sel, const int* done, const void* p,
+int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const int* sel, const int* done, const void* p,
                   const unsigned char* cmask, void* q, long long* launches) {
   Amg* a = m->amg;
   const Sell& S = a->sell;
@@ -1442,11 +1441,11 @@ int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const PcgFuse& fuse, const in
   if (fp32)
     k_sell<float, float, 0><<<sell_grid<float, float, 0>(a, useact), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v32,
                                                          (const float*)p, nullptr, nullptr, cmask, (float*)q,
-                                                         nullptr, S.spart, fuse);
+                                                         nullptr, S.spart);
   else
     k_sell<double, double, 0><<<sell_grid<double, double, 0>(a, useact), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v64,
                                                            (const double*)p, nullptr, nullptr, cmask, (double*)q,
-                                                           nullptr, S.spart, fuse);
+                                                           nullptr, S.spart);
   ++*launches;
   return UA_OK;
 }
@@ -1488,17 +1487,16 @@ static void sell_pass(ua_mesh* m, const AmgPcgView& v, bool useact, const VT* in
   const VT* x = (const VT*)v.x0;
   VT* pcopy = MODE == 2 ? (VT*)v.pcopy : nullptr;
   double* part = MODE == 2 ? S.spart : nullptr;
-  const PcgFuse fuse = MODE == 2 && part ? v.fuse : PcgFuse{};
   const VT* b = (const VT*)v.r;
   const KT* vk = nullptr;
   if constexpr (std::is_same<KT, float>::value) vk = S.v32;
   else vk = S.v64;
   if (v.sell_lo)
     k_sell<__nv_bfloat16, VT, MODE><<<sell_grid<__nv_bfloat16, VT, MODE>(a, la), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, v.sel, v.done, a->d_depth,
-                                                                 S.vlo, x, b, invd, v.cmask, out, pcopy, part, fuse);
+                                                                 S.vlo, x, b, invd, v.cmask, out, pcopy, part);
   else
     k_sell<KT, VT, MODE><<<sell_grid<KT, VT, MODE>(a, la), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, v.sel, v.done, a->d_depth, vk, x, b,
-                                                      invd, v.cmask, out, pcopy, part, fuse);
+                                                      invd, v.cmask, out, pcopy, part);
 }
 
 template <typename KT, typename VT>

@@ -1,7 +1,6 @@
 // Aggregation AMG preconditioner of the uv tangent (internal interface).
 #pragma once
 #include "ua_internal.h"
-#include "ua_pcg_reduce.cuh"
 
 namespace ua {
 
@@ -36,9 +35,6 @@ struct AmgPcgView {
   // finest-level residual and smoothing over the node slices (amg_sell_fill done for this
   // tangent); sell_lo: read their BF16 values
   bool sell = false, sell_lo = false;
-  // the PCG's stage-2 reduction (r.z, r.r) finished in the finest-level smoothing's last CTA of
-  // each system (stage 2), else off
-  PcgFuse fuse;
 };
 
 // Active-block lists.  After every convergence check the row blocks (and, for the smoothed
@@ -89,7 +85,7 @@ int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* lau
 // slice prefix (the PCG reductions sum these instead of the row-block partials).
 void amg_sell_partials(const ua_mesh* m, const double** spart, const int** sys_sl_off);
 // PCG SpMV over the node slices: q = mask(K p), partials p.q per slice (amg_sell_partials).
-int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const PcgFuse& fuse, const int* sel, const int* done, const void* p,
+int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const int* sel, const int* done, const void* p,
                   const unsigned char* cmask, void* q, long long* launches);
 // Refresh the BF16 copy of an FP32 finest-level tangent (allocated on first use;
 // nullptr if that fails).

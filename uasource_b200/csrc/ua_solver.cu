@@ -19,7 +19,6 @@
 #include <cstring>
 #include <vector>
 #include "ua_internal.h"
-#include "ua_pcg_reduce.cuh"
 #include "ua_kernels.h"
 #include <type_traits>
 #include "ua_linesearch.h"
@@ -66,6 +65,10 @@ struct Prof {
   int act_cap = 0;
 };
 enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2, PK_AMGR = 3, PK_AMGP = 4, PK_COUNT = 5 };
+constexpr int kRedThreads = 256;
+// per-system scalars; SV_RH = |rhat|^2, SV_RST = BiCGStab restart pending, SV_NRST = restarts so far
+enum { SV_RZ = 0, SV_PQ, SV_ALPHA, SV_BETA, SV_RR, SV_RR0, SV_TOL2, SV_NORM, SV_FF, SV_FD, SV_OMEGA, SV_RH, SV_RST,
+       SV_NRST, SV_COUNT };
 constexpr int kBicgMaxRestarts = 64;
 
 struct Work {
@@ -89,7 +92,6 @@ struct Work {
   int* con_dof2 = nullptr;
   double *con_v1 = nullptr, *con_v2 = nullptr;
   int* pair_rows = nullptr;
-  int* fuse_cnt = nullptr;  // per system: slice blocks done in the running fused-reduction kernel (0 between)
   int npair = 0;
   size_t pair_cap = 0;
   // dof vectors
@@ -134,12 +136,11 @@ struct Work {
   Prof prof;
   struct ServeState* serve = nullptr;
   // replayable PCG chunks, index (fp32 ? 2 : 0) + (amg ? 1 : 0) + (BF16 V-cycle ? 4 : 0) + (active lists ? 8 : 0)
-  // + (node slices ? 16 : 0) + (fused reductions ? 32 : 0)
   bool no_graph = false;
-  cudaGraphExec_t pcg_exec[64] = {};
-  long long pcg_exec_nodes[64] = {};
-  int pcg_exec_maxit[64] = {};
-  int pcg_exec_lpr[64] = {};
+  cudaGraphExec_t pcg_exec[32] = {};
+  long long pcg_exec_nodes[32] = {};
+  int pcg_exec_maxit[32] = {};
+  int pcg_exec_lpr[32] = {};
   int nsm = 148;  // SMs of the handle's device (grid of the list-driven kernels)
 };
 
@@ -464,6 +465,28 @@ __global__ void __launch_bounds__(256) k_pcg_update2(const int* rb_start, const 
   }
 }
 
+// Sum NV partial arrays of one system in a fixed order.
+template <int NV>
+__device__ __forceinline__ void sys_sum(const double* part, int nrb, int b0, int b1, double (&out)[NV]) {
+  __shared__ double red[NV][kRedThreads];
+  double acc[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) acc[j] = 0;
+  for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] += part[j * nrb + b];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) red[j][threadIdx.x] = acc[j];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+#pragma unroll
+      for (int j = 0; j < NV; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + st];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < NV; ++j) out[j] = red[j][0];
+}
 
 // stage: 0 = init (rz, rr0), 1 = alpha (pq), 2 = beta (rz_new, rr)
 // spart (node slices): the p.q and r.z partials come per slice (sys_sl_off: per-system slice
@@ -478,7 +501,16 @@ __global__ void k_pcg_reduce(int stage, const int* sys_rb_off, int nrb, const in
     double o[1];
     if (spart) sys_sum<1>(spart, 0, sys_sl_off[s], sys_sl_off[s + 1], o);
     else sys_sum<1>(part, nrb, b0, b1, o);
-    if (threadIdx.x == 0) pcg_stage1(s, o[0], sysv, nsys, status, done);
+    if (threadIdx.x == 0) {
+      const double pq = o[0];
+      if (!(pq > 0)) {  // not positive definite on the free dofs, or breakdown
+        status[s] = 1;
+        done[s] = 1;
+        sysv[SV_ALPHA * nsys + s] = 0;
+      } else {
+        sysv[SV_ALPHA * nsys + s] = sysv[SV_RZ * nsys + s] / pq;
+      }
+    }
     return;
   }
   double o[2];
@@ -502,7 +534,12 @@ __global__ void k_pcg_reduce(int stage, const int* sys_rb_off, int nrb, const in
     done[s] = (o[1] == 0.0) ? 1 : 0;
     return;
   }
-  pcg_stage2(s, o[0], o[1], sysv, nsys, its, done, maxit);
+  const double rz_new = o[0], rr = o[1];
+  its[s] += 1;
+  sysv[SV_RR * nsys + s] = rr;
+  sysv[SV_BETA * nsys + s] = rz_new / sysv[SV_RZ * nsys + s];
+  sysv[SV_RZ * nsys + s] = rz_new;
+  if (rr <= sysv[SV_TOL2 * nsys + s] * sysv[SV_RR0 * nsys + s] || its[s] >= maxit || !(rr == rr)) done[s] = 1;
 }
 
 // Constraint rows of the Newton system (mask form):
@@ -796,16 +833,13 @@ static int ensure_work(ua_mesh* m, const ua_params* p) {
   w->done = walloc<int>(m, nsys);
   w->its = walloc<int>(m, nsys);
   w->status = walloc<int>(m, nsys);
-  w->fuse_cnt = walloc<int>(m, nsys);
   w->sel = walloc<int>(m, nsys);
   w->gamma = walloc<double>(m, nsys);
   w->cmask = walloc<unsigned char>(m, N);
   w->dof_con = walloc<int>(m, N);
   ok = ok && w->rowptr && w->colind && w->diagpos && w->scal && w->part && w->sysv && w->done && w->its &&
-       w->status && w->fuse_cnt && w->sel && w->gamma && w->cmask && w->dof_con && w->rb_start && w->rb_sys &&
-       w->sys_rb_off;
+       w->status && w->sel && w->gamma && w->cmask && w->dof_con && w->rb_start && w->rb_sys && w->sys_rb_off;
   if (!ok) { delete w; return set_error(UA_ERR_OOM, "device allocation of work buffers failed"); }
-  UA_CUDA_TRY(cudaMemsetAsync(w->fuse_cnt, 0, nsys * sizeof(int), m->stream));
   w->nan_first = walloc<int>(m, 16);
   if (!w->nan_first) { delete w; return set_error(UA_ERR_OOM, "device allocation of work buffers failed"); }
   if (cudaMallocHost(&w->h_sysv, SV_COUNT * sizeof(double) * nsys) != cudaSuccess ||
@@ -1444,25 +1478,13 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
                                                         w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
   if (view.act) amg_act_compact(m, w->sel, w->done, &g_launches);
   UA_CUDA_TRY(cudaGetLastError());
-  // the stage-1 and stage-2 sums in the last CTA of each system of the node-slice SpMV and the
-  // V-cycle's finest-level smoothing (same order, same bits as the reduction kernel)
-  const bool fused = view.sell && spart && p->krylov_fused_reduce != 0;
-  PcgFuse fz;
-  if (fused) {
-    fz.cnt = w->fuse_cnt; fz.sys_sl_off = sys_sl_off; fz.rb_part = w->part; fz.nrb = w->nrb;
-    fz.sys_rb_off = w->sys_rb_off; fz.sel = w->sel; fz.done = w->done; fz.status = w->status; fz.its = w->its;
-    fz.sysv = w->sysv; fz.nsys = w->nsys; fz.maxit = p->krylov_maxit;
-  }
-  PcgFuse fz1 = fz, fz2 = fz;
-  if (fused) { fz1.stage = 1; fz2.stage = 2; }
-  view.fuse = fz2;
   const int chunk = 16;
   // one PCG iteration for every selected, unfinished system
   auto iteration = [&]() -> int {
     cudaEvent_t ev[2];
     prof_begin(m, PK_SPMV, ev);
     if (view.sell)
-      amg_sell_spmv(m, fp32, view.act, fz1, w->sel, w->done, pp, w->cmask, q, &g_launches);
+      amg_sell_spmv(m, fp32, view.act, w->sel, w->done, pp, w->cmask, q, &g_launches);
     else {
       dispatch_lpr(lpr, [&](auto L) {
         if (uvlay)
@@ -1477,9 +1499,8 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
       ++g_launches;
     }
     prof_end(m, ev);
-    if (!fused)
-      k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
-                                                            w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
+    k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                          w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
     if (w->npair)
       k_pair_project<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
                                                      w->done, cp, q), ++g_launches;
@@ -1492,9 +1513,8 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
         k_pair_project<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
                                                        w->done, cp, z), ++g_launches;
     }
-    if (!fused)
-      k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
-                                                            w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
+    k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+                                                          w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
     if (view.act) amg_act_compact(m, w->sel, w->done, &g_launches);
     k_pcg_update2<VT><<<grid0, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, act0, w->sel, w->done, w->sysv,
                                                      w->nsys, pp, z), ++g_launches;
@@ -1505,7 +1525,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   // have converged skip their rows on the device (done[s]), so a replay equals the launches.
   const bool graph = !w->no_graph && !p->profile && w->npair == 0;
   const int gk = (fp32 ? 2 : 0) + (amg ? 1 : 0) + (view.K0lo || view.sell_lo ? 4 : 0) + (view.act ? 8 : 0) +
-                 (view.sell ? 16 : 0) + (fused ? 32 : 0);
+                 (view.sell ? 16 : 0);
   if (graph && w->pcg_exec[gk] && (w->pcg_exec_maxit[gk] != p->krylov_maxit || w->pcg_exec_lpr[gk] != lpr)) {
     cudaGraphExecDestroy(w->pcg_exec[gk]);
     w->pcg_exec[gk] = nullptr;
@@ -2910,7 +2930,6 @@ extern "C" void ua_params_default(ua_params* p) {
   p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
   p->amg_smoothed = 1;
   p->krylov_full_grid = 0;
-  p->krylov_fused_reduce = 1;
   p->uvh_h_sweeps = 0;
   p->krylov_sell = 1;
   p->krylov_precond = UA_PC_AMG;
