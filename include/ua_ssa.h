@@ -151,6 +151,10 @@ typedef struct ua_params {
     int32_t krylov_full_grid;  /* 0 = the AMG-preconditioned PCG launches only the row and node blocks of
                                   systems still iterating (device-compacted lists, default); 1 = every
                                   block of the batch (same results) */
+    int32_t amg_P_refresh;     /* smoothed aggregation: recompute each system's prolongators P on the
+                                  first Newton step of its solve and then every amg_P_refresh-th step
+                                  (1 = every step, default); the coarse operators P'KP always use the
+                                  current tangent */
     int32_t uvh_h_sweeps;      /* uvh block preconditioner: l1-Jacobi sweeps on the thickness block K_hh
                                   (0 = default 8) */
     int32_t krylov_sell;       /* 1 = the AMG-preconditioned uv PCG runs its SpMV and the V-cycle's

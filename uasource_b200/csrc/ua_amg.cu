@@ -142,6 +142,10 @@ struct Amg {
   // uvh handles: constraint mask and vectors of the velocity rows (2-dof layout)
   unsigned char* uvh_mask = nullptr;
   double *uvh_r = nullptr, *uvh_x0 = nullptr, *uvh_z = nullptr, *uvh_t = nullptr;
+  // per system: numeric set-ups since its solve started (prolongator refresh), and the systems
+  // whose prolongators the current set-up recomputes
+  std::vector<int> p_age, h_prefresh;
+  int* d_prefresh = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -565,9 +569,10 @@ __global__ void k_amg_galerkin(int ncd, const int* mptr, const int* mlist, const
 // l1-Jacobi: invd_i = 1 / sum_j |a_ij| over unmasked columns (0 on masked or empty rows)
 template <typename KT, typename VT>
 __global__ void k_amg_l1(int n, const int* rowptr, const int* colind, const KT* A, const unsigned char* cmask,
-                         VT* invd) {
+                         VT* invd, const int* dof_sys, const int* sel) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (sel && !sel[dof_sys[i]]) return;  // systems not in this Newton step keep their values
   double s = 0;
   if (!(cmask && cmask[i]))
     for (int q = rowptr[i]; q < rowptr[i + 1]; ++q)
@@ -587,12 +592,12 @@ template <typename KT>
 __global__ void __launch_bounds__(256) k_amg_dense_inverse(const int* depth, const int* dn_arr, const int* doff,
                                                            int* const* lev_rowptr, int* const* lev_colind,
                                                            void* const* lev_A, int* const* lev_dofoff,
-                                                           double* dense) {
+                                                           double* dense, const int* sel) {
   extern __shared__ double M[];
   __shared__ double fac[kAmgMaxDense];
   const int s = blockIdx.x;
   const int n = dn_arr[s];
-  if (n == 0) return;
+  if (n == 0 || (sel && !sel[s])) return;
   const int l = depth[s];
   const int* rp = lev_rowptr[l];
   const int* ci = lev_colind[l];
@@ -849,7 +854,7 @@ template <> struct Quad<__nv_bfloat16> {
 // entries.  One CTA per slice block, one warp per slice, one lane per node; writes are contiguous.
 template <typename KT>
 __global__ void __launch_bounds__(256) k_sell_fill(SellDev S, const DevMesh dm, const KT* K, KT* vk,
-                                                   __nv_bfloat16* vlo, int* cols) {
+                                                   __nv_bfloat16* vlo, int* cols, const int* sel) {
   const int sb = blockIdx.x;
   const int w = threadIdx.x >> 5, t = threadIdx.x & 31, pos = w * 32 + t;
   const int sl = sb * kSellSlices + w;
@@ -857,6 +862,7 @@ __global__ void __launch_bounds__(256) k_sell_fill(SellDev S, const DevMesh dm, 
   const int W = (int)((S.sl_off[sl + 1] - o0) >> 5);
   if (W == 0) return;  // empty slice (warp-uniform)
   const int s = S.sb_sys[sb];
+  if (sel && K && !sel[s]) return;  // values of the systems of this Newton step only
   const int no = dm.sys_node_off[s], d0 = dm.sys_dof_off[s];
   const bool has = pos < S.sb_cnt[sb];
   int g = no, np0 = 0, deg = 0;
@@ -994,11 +1000,12 @@ template <typename KT, typename VT>
 __global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int* node_off, const int* rowptr,
                        const int* colind, const KT* A, const unsigned char* mask, const VT* invd, const int* agg,
                        const int* pn_ptr, const int* pn_col, const int* pbase, const int* pnnz, const int* poff,
-                       double* P) {
+                       double* P, const int* sel) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nf) return;
   int s, c, g;
   sa_decode(i, dof_sys, dof_off, node_off, s, c, g);
+  if (sel && !sel[s]) return;
   const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
   double* row = P + poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]);
   for (int t = 0; t < 2 * dP; ++t) row[t] = 0;
@@ -1028,11 +1035,12 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
                                                const unsigned char* mask, const int* pn_ptr, const int* pn_col,
                                                const int* pbase, const int* pnnz, const int* poff, const double* P,
                                                const int* apn_ptr, const int* apn_col, const int* apbase,
-                                               const int* apnnz, const int* apoff, double* AP) {
+                                               const int* apnnz, const int* apoff, double* AP, const int* sel) {
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) / kSaGL, lane = threadIdx.x % kSaGL;
   if (g >= nfn) return;  // whole groups leave together
   const unsigned gmask = ((1u << kSaGL) - 1u) << ((threadIdx.x & 31) & ~(kSaGL - 1));
   const int s = node_sys[g];
+  if (sel && !sel[s]) return;  // whole groups
   const int no = node_off[s], nn = node_off[s + 1] - no, d0 = dof_off[s];
   const int i0 = d0 + (g - no), i1 = i0 + nn;
   const int ar = apn_ptr[g], dA = apn_ptr[g + 1] - ar;
@@ -1075,11 +1083,12 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
 __global__ void k_sa_PT(int nc, const int* cdof_sys, const int* cdof_off, const int* cnode_off, const int* ptn_ptr,
                         const int* ptn_fine, const int* ptn_k, const int* ptbase, const int* pn_ptr,
                         const int* pbase, const int* pnnz, const int* poff, const double* P, double* PT, float* Plo,
-                        float* PTlo) {
+                        float* PTlo, const int* sel) {
   const int R = blockIdx.x * blockDim.x + threadIdx.x;
   if (R >= nc) return;
   int s, c2, J;
   sa_decode(R, cdof_sys, cdof_off, cnode_off, s, c2, J);
+  if (sel && !sel[s]) return;
   const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
   const size_t t0 = poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
   for (int c = 0; c < 2; ++c)
@@ -1107,13 +1116,14 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
                                                            const int* ptn_fine, const int* ptbase, const int* pnnz,
                                                            const int* poff, const double* PT, const int* apn_ptr,
                                                            const int* apn_col, const int* apbase, const int* apnnz,
-                                                           const int* apoff, const double* AP, KT* Ac) {
+                                                           const int* apoff, const double* AP, KT* Ac, const int* sel) {
   __shared__ int s_col[kSaAcWarps][kSaMaxDeg];
   __shared__ double s_acc[kSaAcWarps][4 * kSaMaxDeg];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int J = blockIdx.x * kSaAcWarps + wid;
   if (J >= ncn) return;  // whole warps leave together
   const int s = cnode_sys[J];
+  if (sel && !sel[s]) return;  // whole warps
   const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno;
   const int R0 = cdof_off[s] + (J - cno), R1 = R0 + cnn;
   const int cr0 = crowptr[R0], cr1 = crowptr[R1], degc = min((crowptr[R0 + 1] - cr0) >> 1, kSaMaxDeg);
@@ -1269,14 +1279,14 @@ __global__ void __launch_bounds__(32 * kSaPW) k_sa_prolong(int nnb, const int* n
 
 template <typename KT, typename VT>
 static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const KT* K0, const unsigned char* cmask,
-                     long long* launches) {
+                     const int* sel, const int* psel, long long* launches) {
   Amg* a = m->amg;
   cudaStream_t st = m->stream;
   auto l1 = [&](int l) {
     const AmgLevel& L = a->lev[l];
     k_amg_l1<KT, VT><<<(L.ndof + 255) / 256, 256, 0, st>>>(
         L.ndof, l == 0 ? rowptr0 : L.rowptr, l == 0 ? colind0 : L.colind, l == 0 ? K0 : (const KT*)L.A,
-        l == 0 ? cmask : nullptr, (VT*)L.invd), ++*launches;
+        l == 0 ? cmask : nullptr, (VT*)L.invd, L.dof_sys, sel), ++*launches;
   };
   if (a->sa) {
     // per level: smoother diagonal, smoothed prolongator, A P, P' values, coarse operator
@@ -1291,16 +1301,16 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
       const int nbf = (F.ndof + 127) / 128, nbc = (C.ndof + 127) / 128;
       k_sa_P<KT, VT><<<nbf, 128, 0, st>>>(F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk,
                                           (const VT*)F.invd, F.sa_agg, F.pn_ptr, F.pn_col, F.pbase, F.pnnz, F.poff,
-                                          F.sa_p), ++*launches;
+                                          F.sa_p, psel), ++*launches;
       k_sa_AP<KT><<<(int)(((long long)F.nn * kSaGL + 127) / 128), 128, 0, st>>>(F.nn, F.node_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr,
                                        F.pn_col, F.pbase, F.pnnz, F.poff, F.sa_p, F.apn_ptr, F.apn_col, F.apbase,
-                                       F.apnnz, F.apoff, F.sa_ap), ++*launches;
+                                       F.apnnz, F.apoff, F.sa_ap, sel), ++*launches;
       k_sa_PT<<<nbc, 128, 0, st>>>(C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, F.ptn_ptr, F.ptn_fine, F.ptn_k,
                                    F.ptbase, F.pn_ptr, F.pbase, F.pnnz, F.poff, F.sa_p, F.sa_pt, F.sa_plo,
-                                   F.sa_ptlo), ++*launches;
+                                   F.sa_ptlo, psel), ++*launches;
       k_sa_Ac<KT><<<(C.nn + kSaAcWarps - 1) / kSaAcWarps, 32 * kSaAcWarps, 0, st>>>(C.nn, C.node_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr,
                                        F.ptn_fine, F.ptbase, F.pnnz, F.poff, F.sa_pt, F.apn_ptr, F.apn_col, F.apbase,
-                                       F.apnnz, F.apoff, F.sa_ap, (KT*)C.A), ++*launches;
+                                       F.apnnz, F.apoff, F.sa_ap, (KT*)C.A, sel), ++*launches;
     }
     l1(a->nlev - 1);
   } else {
@@ -1316,7 +1326,7 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
   const int sm = (int)(sizeof(double) * (size_t)a->maxdn * 2 * a->maxdn);
   UA_CUDA_TRY(cudaFuncSetAttribute(k_amg_dense_inverse<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   k_amg_dense_inverse<KT><<<a->nsys, 256, sm, st>>>(a->d_depth, a->d_dn, a->d_doff, a->d_lev_rowptr,
-                                                     a->d_lev_colind, a->d_lev_A, a->d_lev_dofoff, a->dense),
+                                                     a->d_lev_colind, a->d_lev_A, a->d_lev_dofoff, a->dense, sel),
       ++*launches;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "AMG numeric phase: %s", cudaGetErrorString(e));
@@ -1384,14 +1394,15 @@ int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
   S.sys_sl_off = upload(m, a, sl_pre, ok);
   if (!ok) { S.failed = true; return set_error(UA_ERR_OOM, "node slices: device allocation failed"); }
   if (S.nsb)
-    k_sell_fill<double><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, nullptr, nullptr, nullptr, S.cols);
+    k_sell_fill<double><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, nullptr, nullptr, nullptr, S.cols,
+                                                       nullptr);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { S.failed = true; return set_error(UA_ERR_CUDA, "node slices: %s", cudaGetErrorString(e)); }
   S.ready = true;
   return UA_OK;
 }
 
-int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* launches) {
+int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* launches, const int* sel) {
   Amg* a = m->amg;
   if (!a || !a->sell.ready) return UA_ERR_INVALID;
   Sell& S = a->sell;
@@ -1404,10 +1415,10 @@ int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* lau
   if (!S.nsb) return UA_OK;
   if (fp32)
     k_sell_fill<float><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, (const float*)K0, S.v32,
-                                                      lo ? S.vlo : nullptr, nullptr);
+                                                      lo ? S.vlo : nullptr, nullptr, sel);
   else
     k_sell_fill<double><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, (const double*)K0, S.v64,
-                                                       lo ? S.vlo : nullptr, nullptr);
+                                                       lo ? S.vlo : nullptr, nullptr, sel);
   ++*launches;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "node slices: %s", cudaGetErrorString(e));
@@ -1463,9 +1474,39 @@ const void* amg_bf16_copy(ua_mesh* m, const float* K0, long long nnz, long long*
 }
 
 int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
-                const unsigned char* cmask, long long* launches) {
-  if (fp32) return numeric_t<float, float>(m, rowptr0, colind0, (const float*)K0, cmask, launches);
-  return numeric_t<double, double>(m, rowptr0, colind0, (const double*)K0, cmask, launches);
+                const unsigned char* cmask, long long* launches, const int* sel, const std::vector<int>* h_sel,
+                int p_refresh) {
+  // prolongators: recomputed for the selected systems on the first set-up of their solve and then
+  // every p_refresh-th one (all of them when no host selection is given)
+  Amg* a = m->amg;
+  const int* psel = sel;
+  if (a && a->sa && h_sel && p_refresh > 1) {
+    const int ns = a->nsys;
+    if ((int)a->p_age.size() != ns) a->p_age.assign(ns, 0);
+    a->h_prefresh.assign(ns, 0);
+    for (int s = 0; s < ns; ++s) {
+      if (!(*h_sel)[s]) continue;
+      a->h_prefresh[s] = a->p_age[s] % p_refresh == 0 ? 1 : 0;
+      a->p_age[s] += 1;
+    }
+    bool ok = true;
+    if (!a->d_prefresh) a->d_prefresh = (int*)dalloc(m, a, sizeof(int) * ns, ok);
+    if (!ok) return set_error(UA_ERR_OOM, "AMG: device allocation failed");
+    UA_CUDA_TRY(cudaMemcpyAsync(a->d_prefresh, a->h_prefresh.data(), sizeof(int) * ns, cudaMemcpyHostToDevice,
+                                m->stream));
+    UA_CUDA_TRY(cudaStreamSynchronize(m->stream));  // h_prefresh is rewritten by the next set-up
+    psel = a->d_prefresh;
+  }
+  if (fp32) return numeric_t<float, float>(m, rowptr0, colind0, (const float*)K0, cmask, sel, psel, launches);
+  return numeric_t<double, double>(m, rowptr0, colind0, (const double*)K0, cmask, sel, psel, launches);
+}
+
+void amg_restart_P(ua_mesh* m, const std::vector<int>& run) {
+  Amg* a = m->amg;
+  if (!a) return;
+  if ((int)a->p_age.size() != a->nsys) a->p_age.assign(a->nsys, 0);
+  for (int s = 0; s < a->nsys && s < (int)run.size(); ++s)
+    if (run[s]) a->p_age[s] = 0;
 }
 
 // the transfer values in the vector precision

@@ -65,8 +65,14 @@ int amg_levels(const ua_mesh* m);
 // l1-Jacobi inverse row sums of the fine level (VT-typed, valid after amg_numeric)
 const void* amg_invd0(const ua_mesh* m);
 // Numeric phase for a new tangent K0 (Galerkin products, smoother, coarsest inverses).
+// sel (device): the systems of this Newton step (others keep their hierarchies); h_sel (host copy)
+// and p_refresh > 1: each system's prolongators are recomputed on the first set-up of its solve
+// (amg_restart_P) and then every p_refresh-th set-up, the coarse operators every time.
 int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
-                const unsigned char* cmask, long long* launches);
+                const unsigned char* cmask, long long* launches, const int* sel = nullptr,
+                const std::vector<int>* h_sel = nullptr, int p_refresh = 1);
+// the systems of `run` start a solve: their next set-up recomputes the prolongators
+void amg_restart_P(ua_mesh* m, const std::vector<int>& run);
 // uvh handles: extract the velocity block of the 3-dof tangent K3 (and its
 // constraint mask) into the hierarchy's own finest level, then the numeric
 // phase (FP64).
@@ -80,7 +86,7 @@ int amg_apply_uvh(ua_mesh* m, const double* p3, double* out3, const int* sel, co
 // error code and the CSR kernels stay in use.
 int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0);
 // Slice values of a new tangent K0 (KT = float if fp32, else double); lo: also the BF16 copy.
-int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* launches);
+int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* launches, const int* sel = nullptr);
 // Per-slice partials of the node-slice SpMV (p.q) and smoothing (r.z), and the per-system
 // slice prefix (the PCG reductions sum these instead of the row-block partials).
 void amg_sell_partials(const ua_mesh* m, const double** spart, const int** sys_sl_off);

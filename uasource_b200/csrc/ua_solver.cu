@@ -92,6 +92,7 @@ struct Work {
   int* con_dof2 = nullptr;
   double *con_v1 = nullptr, *con_v2 = nullptr;
   int* pair_rows = nullptr;
+  std::vector<int> h_sel;  // host copy of sel (set_sel)
   int npair = 0;
   size_t pair_cap = 0;
   // dof vectors
@@ -1307,6 +1308,7 @@ static int build_constraints(ua_mesh* m, const ua_bcs* bcs, int nB) {
 static int set_sel(ua_mesh* m, const std::vector<int>& sel) {
   Work* w = m->work;
   UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  w->h_sel.assign(sel.begin(), sel.begin() + w->nsys);
   for (int s = 0; s < w->nsys; ++s) w->h_int[s] = sel[s];
   UA_CUDA_TRY(cudaMemcpyAsync(w->sel, w->h_int, w->nsys * sizeof(int), cudaMemcpyHostToDevice, m->stream));
   return UA_OK;
@@ -1393,7 +1395,9 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   if (amg && amg_setup(m, p->amg_smoothed != 0) != UA_OK) amg = false;  // shapes the hierarchy cannot take keep point Jacobi
   const bool fp32 = sizeof(KT) == 4;
   if (amg) {
-    int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches);
+    // the systems of this Newton step only (the others' hierarchies are not read)
+    int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches, w->sel, &w->h_sel,
+                         p->amg_P_refresh);
     if (rc) return rc;
   } else {
     k_invdiag<KT, VT><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, (VT*)w->invd), ++g_launches;
@@ -1422,7 +1426,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   const int* sys_sl_off = nullptr;
   if (sell) amg_sell_partials(m, &spart, &sys_sl_off);
   if (sell) {
-    int rc = amg_sell_fill(m, K, fp32, fp32 && p->precond_bf16, &g_launches);
+    int rc = amg_sell_fill(m, K, fp32, fp32 && p->precond_bf16, &g_launches, w->sel);
     if (rc) return rc;
     view.sell = true;
     view.sell_lo = fp32 && p->precond_bf16;
@@ -1662,6 +1666,7 @@ static int newton_init(ua_mesh* m, const ua_params* p, const std::vector<int>& r
   // make the iterate feasible (:101-104) and compute fext0 at ZeroFields (:122-124)
   UA_CUDA_TRY(cudaMemsetAsync(w->X0, 0, m->ndof_total * sizeof(double), m->stream));
   if ((rc = set_sel(m, run))) return rc;
+  amg_restart_P(m, run);  // a new solve: its first AMG set-up recomputes the prolongators
   if (w->nc) {
     k_set_con_values<<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel,
                                                                  w->con_rhs, w->X, con_pairs(w)), ++g_launches;
@@ -2930,6 +2935,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
   p->amg_smoothed = 1;
   p->krylov_full_grid = 0;
+  p->amg_P_refresh = 1;
   p->uvh_h_sweeps = 0;
   p->krylov_sell = 1;
   p->krylov_precond = UA_PC_AMG;

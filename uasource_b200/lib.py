@@ -86,6 +86,7 @@ class ua_params(C.Structure):
         ("uvh_krylov", C.c_int32), ("krylov_restart", C.c_int32),
         ("krylov_eta_c", C.c_double), ("krylov_eta_max", C.c_double), ("precond_bf16", C.c_int32),
         ("amg_smoothed", C.c_int32), ("krylov_full_grid", C.c_int32),
+        ("amg_P_refresh", C.c_int32),
         ("uvh_h_sweeps", C.c_int32), ("krylov_sell", C.c_int32),
         ("SlidingLaw", C.c_int32), ("Nzero", C.c_double), ("IncludeMelangeModelPhysics", C.c_int32),
         ("ThicknessConstraints", C.c_int32), ("ThickMin", C.c_double), ("ThicknessConstraintsItMax", C.c_int32),
