@@ -153,7 +153,7 @@ typedef struct ua_params {
                                   block of the batch (same results) */
     int32_t amg_P_refresh;     /* smoothed aggregation: recompute each system's prolongators P on the
                                   first Newton step of its solve and then every amg_P_refresh-th step
-                                  (1 = every step, default); the coarse operators P'KP always use the
+                                  (default 4; 1 = every step); the coarse operators P'KP always use the
                                   current tangent */
     int32_t uvh_h_sweeps;      /* uvh block preconditioner: l1-Jacobi sweeps on the thickness block K_hh
                                   (0 = default 8) */

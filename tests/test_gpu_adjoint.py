@@ -5,7 +5,7 @@ oracle, through the C-ABI (ua_uv_adjoint_dIdC).
 The misfit I and its gradient dI/d(u,v) come from the mass matrix and the data
 alone (within 1e-12); the adjoint velocities lambda solve the constrained tangent
 system iteratively here and directly in the oracle, so lambda satisfies the oracle's
-adjoint system to a backward error of 1e-10, and lambda and the gradient dIdC are
+adjoint system to a componentwise backward error of 1e-10, and lambda and the gradient dIdC are
 compared within 1e-9 relative L2 with the inner tolerance at 1e-14.  The coarse P2
 case (9 x 6 vertices) has a tangent of condition number about 1e11 (drag of order
 1e15 next to the u = 0 inflow boundary), so any two solves of it agree only to about
@@ -82,7 +82,9 @@ def test_adjoint_gradient_matches_oracle(nod, nx, ny, law, logC, prem):
     fixed = np.unique(Lm.nonzero()[1])
     free = np.setdiff1d(np.arange(2 * P.Nnodes), fixed)
     r = (K @ lam - dIduv_ref)[free]
-    assert np.linalg.norm(r) <= TOL_BACKWARD * np.linalg.norm(dIduv_ref[free])
+    # componentwise (Oettli-Prager): rows next to the u = 0 inflow carry drag of order 1e15
+    scale = (abs(K) @ np.abs(lam) + np.abs(dIduv_ref))[free]
+    assert np.max(np.abs(r) / scale) <= TOL_BACKWARD
     assert np.max(np.abs(lam[fixed])) <= 1e-12 * np.max(np.abs(lam))
     tol = TOL_ADJ_ILL if nod == 6 else TOL_ADJ
     assert _rel(lam, lam_ref) <= tol

@@ -390,3 +390,28 @@ def test_tangent_assembled_ahead_matches_assembly_per_iteration(precision, rtol)
         assert ia.iterations == ib.iterations
         a, b = np.concatenate([Fa.ub, Fa.vb]), np.concatenate([Fb.ub, Fb.vb])
         assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("refresh", [1, 2, 100])
+def test_prolongator_refresh_interval(refresh):
+    """Prolongators kept over Newton steps (the coarse operators recomputed from each tangent):
+    the solve converges to the same solution within the tolerance of the inner solve, FP64 and
+    mixed, and a batch equals each mesh alone bit for bit with the interval in use."""
+    probs = [synth.ice_stream_shelf(41, 21, seed=1), synth.ice_stream_shelf(21, 11, seed=6)]
+    ref = []
+    for P in probs:
+        c = ua.CtrlVar(amg_P_refresh=1).set_force_tolerance(1e-20)
+        Fo, _, _, _, info = ua.uv(c, ua.CreateMUA(P.coordinates, P.connectivity), ua.BCs.from_problem(P),
+                                  ua.Fields.from_problem(P))
+        ref.append(np.concatenate([Fo.ub, Fo.vb]))
+    for prec, tol in ((L.UA_PREC_FP64, 1e-10), (L.UA_PREC_MIXED, 1e-8)):
+        ctrl = ua.CtrlVar(precision=prec, krylov_rtol=1e-12 if prec == L.UA_PREC_FP64 else 1e-6,
+                          amg_P_refresh=refresh).set_force_tolerance(1e-20)
+        mb = ua.CreateMUABatch([(P.coordinates, P.connectivity) for P in probs])
+        batch = ua.uv_batch(ctrl, mb, [ua.Fields.from_problem(P) for P in probs], [ua.BCs.from_problem(P) for P in probs])
+        for k, P in enumerate(probs):
+            Fo, _, _, _, info = ua.uv(ctrl, ua.CreateMUA(P.coordinates, P.connectivity), ua.BCs.from_problem(P),
+                                      ua.Fields.from_problem(P))
+            u = np.concatenate([Fo.ub, Fo.vb])
+            assert info.converged and np.linalg.norm(u - ref[k]) <= tol * np.linalg.norm(ref[k])
+            assert np.array_equal(batch[k][0], Fo.ub) and np.array_equal(batch[k][1], Fo.vb)

@@ -1027,8 +1027,11 @@ __global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int
 // Both rows (c = 0, 1) of the node share its neighbour list, so each neighbour h contributes
 // A((c,g),(c2,h)) P((c2,h),:) to four output blocks (c, c3) at once; the neighbours go in
 // order and the lanes take the entries of P(h,:), whose targets in the AP row are distinct:
-// a fixed summation order without atomics
+// a fixed summation order without atomics.  A row of at most kSaApSm coarse columns is summed in
+// shared memory (its column list there too, for the searches) and written once; longer rows are
+// summed in place in global memory, in the same order.
 constexpr int kSaGL = 8;
+constexpr int kSaApSm = 64;
 template <typename KT>
 __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, const int* dof_off, const int* node_off,
                                                const int* rowptr, const int* colind, const KT* A,
@@ -1036,6 +1039,9 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
                                                const int* pbase, const int* pnnz, const int* poff, const double* P,
                                                const int* apn_ptr, const int* apn_col, const int* apbase,
                                                const int* apnnz, const int* apoff, double* AP, const int* sel) {
+  __shared__ double s_acc[128 / kSaGL][4 * kSaApSm];
+  __shared__ int s_col[128 / kSaGL][kSaApSm];
+  const int gi = threadIdx.x / kSaGL;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) / kSaGL, lane = threadIdx.x % kSaGL;
   if (g >= nfn) return;  // whole groups leave together
   const unsigned gmask = ((1u << kSaGL) - 1u) << ((threadIdx.x & 31) & ~(kSaGL - 1));
@@ -1044,36 +1050,51 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
   const int no = node_off[s], nn = node_off[s + 1] - no, d0 = dof_off[s];
   const int i0 = d0 + (g - no), i1 = i0 + nn;
   const int ar = apn_ptr[g], dA = apn_ptr[g + 1] - ar;
-  const int* acol = apn_col + ar;
   const size_t ars = (size_t)2 * apnnz[s];  // AP row stride between c = 0 and c = 1
   double* r0 = AP + apoff[s] + 2 * (size_t)(ar - apbase[s]);
+  const bool sm = dA <= kSaApSm;  // uniform over the group
+  double* o0 = sm ? s_acc[gi] : r0;
+  const size_t o1 = sm ? (size_t)2 * dA : ars;  // offset of row c = 1
+  const int* acol = apn_col + ar;
+  if (sm) {
+    for (int t = lane; t < dA; t += kSaGL) s_col[gi][t] = acol[t];
+    acol = s_col[gi];
+  }
   for (int t = lane; t < 2 * dA; t += kSaGL) {
-    r0[t] = 0;
-    r0[ars + t] = 0;
+    o0[t] = 0;
+    o0[o1 + t] = 0;
   }
   const bool m0 = mask && mask[i0], m1 = mask && mask[i1];
-  if (m0 && m1) return;
-  const int q0 = rowptr[i0], q1 = rowptr[i1], deg = (rowptr[i0 + 1] - q0) >> 1;
-  const size_t prs = (size_t)2 * pnnz[s];  // P row stride between c2 = 0 and c2 = 1
-  for (int k = 0; k < deg; ++k) {
-    const int ju = colind[q0 + k], jv = ju + nn;  // u and v dofs of neighbour node h
-    const bool cu = mask && mask[ju], cv = mask && mask[jv];
-    const double a00 = (m0 || cu) ? 0.0 : (double)A[q0 + k], a01 = (m0 || cv) ? 0.0 : (double)A[q0 + deg + k];
-    const double a10 = (m1 || cu) ? 0.0 : (double)A[q1 + k], a11 = (m1 || cv) ? 0.0 : (double)A[q1 + deg + k];
-    if (a00 == 0.0 && a01 == 0.0 && a10 == 0.0 && a11 == 0.0) continue;  // uniform over the group
-    const int h = no + (ju - d0);
-    const int pj = pn_ptr[h], dPj = pn_ptr[h + 1] - pj;
-    const double* ph = P + poff[s] + 2 * (size_t)(pj - pbase[s]);
-    __syncwarp(gmask);  // the previous neighbour's updates are visible to the group
-    for (int t = lane; t < dPj; t += kSaGL) {
-      const int kk = sa_find(acol, dA, pn_col[pj + t]);
-      if (kk < 0) continue;
+  if (!(m0 && m1)) {
+    const int q0 = rowptr[i0], q1 = rowptr[i1], deg = (rowptr[i0 + 1] - q0) >> 1;
+    const size_t prs = (size_t)2 * pnnz[s];  // P row stride between c2 = 0 and c2 = 1
+    for (int k = 0; k < deg; ++k) {
+      const int ju = colind[q0 + k], jv = ju + nn;  // u and v dofs of neighbour node h
+      const bool cu = mask && mask[ju], cv = mask && mask[jv];
+      const double a00 = (m0 || cu) ? 0.0 : (double)A[q0 + k], a01 = (m0 || cv) ? 0.0 : (double)A[q0 + deg + k];
+      const double a10 = (m1 || cu) ? 0.0 : (double)A[q1 + k], a11 = (m1 || cv) ? 0.0 : (double)A[q1 + deg + k];
+      if (a00 == 0.0 && a01 == 0.0 && a10 == 0.0 && a11 == 0.0) continue;  // uniform over the group
+      const int h = no + (ju - d0);
+      const int pj = pn_ptr[h], dPj = pn_ptr[h + 1] - pj;
+      const double* ph = P + poff[s] + 2 * (size_t)(pj - pbase[s]);
+      __syncwarp(gmask);  // the previous neighbour's updates (and the zeroed rows) are visible to the group
+      for (int t = lane; t < dPj; t += kSaGL) {
+        const int kk = sa_find(acol, dA, pn_col[pj + t]);
+        if (kk < 0) continue;
 #pragma unroll
-      for (int c3 = 0; c3 < 2; ++c3) {
-        const double p0 = ph[c3 * dPj + t], p1 = ph[prs + c3 * dPj + t];
-        r0[c3 * dA + kk] += a00 * p0 + a01 * p1;
-        r0[ars + c3 * dA + kk] += a10 * p0 + a11 * p1;
+        for (int c3 = 0; c3 < 2; ++c3) {
+          const double p0 = ph[c3 * dPj + t], p1 = ph[prs + c3 * dPj + t];
+          o0[c3 * dA + kk] += a00 * p0 + a01 * p1;
+          o0[o1 + c3 * dA + kk] += a10 * p0 + a11 * p1;
+        }
       }
+    }
+  }
+  if (sm) {  // one write of the two rows
+    __syncwarp(gmask);
+    for (int t = lane; t < 2 * dA; t += kSaGL) {
+      r0[t] = o0[t];
+      r0[ars + t] = o0[o1 + t];
     }
   }
 }

@@ -2935,7 +2935,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
   p->amg_smoothed = 1;
   p->krylov_full_grid = 0;
-  p->amg_P_refresh = 1;
+  p->amg_P_refresh = 4;
   p->uvh_h_sweeps = 0;
   p->krylov_sell = 1;
   p->krylov_precond = UA_PC_AMG;
