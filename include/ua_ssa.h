@@ -153,8 +153,9 @@ typedef struct ua_params {
                                   block of the batch (same results) */
     int32_t amg_P_refresh;     /* smoothed aggregation: recompute each system's prolongators P on the
                                   first Newton step of its solve and then every amg_P_refresh-th step
-                                  (default 4; 1 = every step); the coarse operators P'KP always use the
-                                  current tangent */
+                                  (0 = by precision: every step in FP64, every fourth in the mixed form;
+                                  1 = every step); the coarse operators P'KP always use the current
+                                  tangent */
     int32_t uvh_h_sweeps;      /* uvh block preconditioner: l1-Jacobi sweeps on the thickness block K_hh
                                   (0 = default 8) */
     int32_t krylov_sell;       /* 1 = the AMG-preconditioned uv PCG runs its SpMV and the V-cycle's

@@ -51,6 +51,7 @@ static void dispatch_lpr(int lpr, F&& f) {
 struct AmgLevel {
   int nn = 0, ndof = 0;
   long long nnz = 0;
+  int ap_maxrow = 0;  // longest A P row (coarse columns) of the level
   std::vector<int> node_off, dof_off, knz_off, nnzn;  // per system (0-sized when the system has no such level)
   // dof-level CSR of a coarse level, same layout rule as the finest level
   int *rowptr = nullptr, *colind = nullptr;
@@ -486,6 +487,9 @@ static int amg_build(ua_mesh* m, bool smoothed) {
       F.pbase = upload(m, a, pbase, ok); F.pnnz = upload(m, a, pnnz, ok); F.poff = upload(m, a, poff, ok);
       F.apbase = upload(m, a, apbase, ok); F.apnnz = upload(m, a, apnnz, ok); F.apoff = upload(m, a, apoff, ok);
       F.ptbase = upload(m, a, ptbase, ok);
+      F.ap_maxrow = 0;
+      for (size_t i = 0; i + 1 < g_apnp[l].size(); ++i)
+        F.ap_maxrow = std::max(F.ap_maxrow, g_apnp[l][i + 1] - g_apnp[l][i]);
       F.sa_p = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
       F.sa_pt = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
       F.sa_ap = (double*)dalloc(m, a, sizeof(double) * (size_t)apoff[nsys], ok);
@@ -996,30 +1000,32 @@ __device__ __forceinline__ void sa_decode(int i, const int* dof_sys, const int* 
 }
 
 // prolongator rows: P(i,:) = P0(i,:) - w invd_i A(i,:) P0 on unmasked rows and columns
-template <typename KT, typename VT>
+// ST: the type the set-up stores and sums P, A P and P' in (FP32 for the mixed-precision form,
+// whose V-cycle transfers read FP32 values, else FP64)
+template <typename KT, typename VT, typename ST>
 __global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int* node_off, const int* rowptr,
                        const int* colind, const KT* A, const unsigned char* mask, const VT* invd, const int* agg,
                        const int* pn_ptr, const int* pn_col, const int* pbase, const int* pnnz, const int* poff,
-                       double* P, const int* sel) {
+                       ST* P, const int* sel) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nf) return;
   int s, c, g;
   sa_decode(i, dof_sys, dof_off, node_off, s, c, g);
   if (sel && !sel[s]) return;
   const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
-  double* row = P + poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]);
+  ST* row = P + poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]);
   for (int t = 0; t < 2 * dP; ++t) row[t] = 0;
   if (mask && mask[i]) return;
   const int k0 = sa_find(pn_col + pr, dP, agg[g]);
-  if (k0 >= 0) row[c * dP + k0] = 1.0;
-  const double f = kSaOmega * (double)invd[i];
+  if (k0 >= 0) row[c * dP + k0] = 1;
+  const ST f = (ST)(kSaOmega * (double)invd[i]);
   for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
     const int j = colind[q];
     if (mask && mask[j]) continue;
     int s2, c2, h;
     sa_decode(j, dof_sys, dof_off, node_off, s2, c2, h);
     const int k = sa_find(pn_col + pr, dP, agg[h]);
-    if (k >= 0) row[c2 * dP + k] -= f * (double)A[q];
+    if (k >= 0) row[c2 * dP + k] -= f * (ST)A[q];
   }
 }
 
@@ -1031,17 +1037,21 @@ __global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int
 // shared memory (its column list there too, for the searches) and written once; longer rows are
 // summed in place in global memory, in the same order.
 constexpr int kSaGL = 8;
-constexpr int kSaApSm = 64;
-template <typename KT>
+constexpr int kSaApSm = 64;  // longest row summed in shared memory
+// dynamic shared memory: per group of kSaGL lanes 4 * ms sums and ms columns (ms = 0: none)
+template <typename ST>
+size_t sa_ap_smem(int ms) { return (size_t)(128 / kSaGL) * ms * (4 * sizeof(ST) + sizeof(int)); }
+template <typename KT, typename ST>
 __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, const int* dof_off, const int* node_off,
                                                const int* rowptr, const int* colind, const KT* A,
                                                const unsigned char* mask, const int* pn_ptr, const int* pn_col,
-                                               const int* pbase, const int* pnnz, const int* poff, const double* P,
+                                               const int* pbase, const int* pnnz, const int* poff, const ST* P,
                                                const int* apn_ptr, const int* apn_col, const int* apbase,
-                                               const int* apnnz, const int* apoff, double* AP, const int* sel) {
-  __shared__ double s_acc[128 / kSaGL][4 * kSaApSm];
-  __shared__ int s_col[128 / kSaGL][kSaApSm];
+                                               const int* apnnz, const int* apoff, ST* AP, const int* sel, int ms) {
+  extern __shared__ __align__(16) unsigned char sa_smem[];
   const int gi = threadIdx.x / kSaGL;
+  ST* g_acc = reinterpret_cast<ST*>(sa_smem) + (size_t)gi * 4 * ms;
+  int* g_col = reinterpret_cast<int*>(reinterpret_cast<ST*>(sa_smem) + (size_t)(128 / kSaGL) * 4 * ms) + gi * ms;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) / kSaGL, lane = threadIdx.x % kSaGL;
   if (g >= nfn) return;  // whole groups leave together
   const unsigned gmask = ((1u << kSaGL) - 1u) << ((threadIdx.x & 31) & ~(kSaGL - 1));
@@ -1051,14 +1061,14 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
   const int i0 = d0 + (g - no), i1 = i0 + nn;
   const int ar = apn_ptr[g], dA = apn_ptr[g + 1] - ar;
   const size_t ars = (size_t)2 * apnnz[s];  // AP row stride between c = 0 and c = 1
-  double* r0 = AP + apoff[s] + 2 * (size_t)(ar - apbase[s]);
-  const bool sm = dA <= kSaApSm;  // uniform over the group
-  double* o0 = sm ? s_acc[gi] : r0;
+  ST* r0 = AP + apoff[s] + 2 * (size_t)(ar - apbase[s]);
+  const bool sm = dA <= ms;  // uniform over the group
+  ST* o0 = sm ? g_acc : r0;
   const size_t o1 = sm ? (size_t)2 * dA : ars;  // offset of row c = 1
   const int* acol = apn_col + ar;
   if (sm) {
-    for (int t = lane; t < dA; t += kSaGL) s_col[gi][t] = acol[t];
-    acol = s_col[gi];
+    for (int t = lane; t < dA; t += kSaGL) g_col[t] = acol[t];
+    acol = g_col;
   }
   for (int t = lane; t < 2 * dA; t += kSaGL) {
     o0[t] = 0;
@@ -1071,19 +1081,19 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
     for (int k = 0; k < deg; ++k) {
       const int ju = colind[q0 + k], jv = ju + nn;  // u and v dofs of neighbour node h
       const bool cu = mask && mask[ju], cv = mask && mask[jv];
-      const double a00 = (m0 || cu) ? 0.0 : (double)A[q0 + k], a01 = (m0 || cv) ? 0.0 : (double)A[q0 + deg + k];
-      const double a10 = (m1 || cu) ? 0.0 : (double)A[q1 + k], a11 = (m1 || cv) ? 0.0 : (double)A[q1 + deg + k];
-      if (a00 == 0.0 && a01 == 0.0 && a10 == 0.0 && a11 == 0.0) continue;  // uniform over the group
+      const ST a00 = (m0 || cu) ? ST(0) : (ST)A[q0 + k], a01 = (m0 || cv) ? ST(0) : (ST)A[q0 + deg + k];
+      const ST a10 = (m1 || cu) ? ST(0) : (ST)A[q1 + k], a11 = (m1 || cv) ? ST(0) : (ST)A[q1 + deg + k];
+      if (a00 == ST(0) && a01 == ST(0) && a10 == ST(0) && a11 == ST(0)) continue;  // uniform over the group
       const int h = no + (ju - d0);
       const int pj = pn_ptr[h], dPj = pn_ptr[h + 1] - pj;
-      const double* ph = P + poff[s] + 2 * (size_t)(pj - pbase[s]);
+      const ST* ph = P + poff[s] + 2 * (size_t)(pj - pbase[s]);
       __syncwarp(gmask);  // the previous neighbour's updates (and the zeroed rows) are visible to the group
       for (int t = lane; t < dPj; t += kSaGL) {
         const int kk = sa_find(acol, dA, pn_col[pj + t]);
         if (kk < 0) continue;
 #pragma unroll
         for (int c3 = 0; c3 < 2; ++c3) {
-          const double p0 = ph[c3 * dPj + t], p1 = ph[prs + c3 * dPj + t];
+          const ST p0 = ph[c3 * dPj + t], p1 = ph[prs + c3 * dPj + t];
           o0[c3 * dA + kk] += a00 * p0 + a01 * p1;
           o0[o1 + c3 * dA + kk] += a10 * p0 + a11 * p1;
         }
@@ -1101,9 +1111,10 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
 
 // transpose values: P'(R = (c2, J), (c, u)) = P((c, fine node u of J), (c2, J)), and FP32 copies
 // of both (every P entry is the image of exactly one P' entry)
+template <typename ST>
 __global__ void k_sa_PT(int nc, const int* cdof_sys, const int* cdof_off, const int* cnode_off, const int* ptn_ptr,
                         const int* ptn_fine, const int* ptn_k, const int* ptbase, const int* pn_ptr,
-                        const int* pbase, const int* pnnz, const int* poff, const double* P, double* PT, float* Plo,
+                        const int* pbase, const int* pnnz, const int* poff, const ST* P, ST* PT, float* Plo,
                         float* PTlo, const int* sel) {
   const int R = blockIdx.x * blockDim.x + threadIdx.x;
   if (R >= nc) return;
@@ -1116,10 +1127,10 @@ __global__ void k_sa_PT(int nc, const int* cdof_sys, const int* cdof_off, const 
     for (int u = 0; u < dT; ++u) {
       const int g = ptn_fine[tr + u], pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
       const size_t pi = poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]) + c2 * dP + ptn_k[tr + u];
-      const double v = P[pi];
+      const ST v = P[pi];
       PT[t0 + c * dT + u] = v;
-      PTlo[t0 + c * dT + u] = (float)v;
-      Plo[pi] = (float)v;
+      if (PTlo) PTlo[t0 + c * dT + u] = (float)v;  // FP32 copies for the transfers of a FP64 set-up
+      if (Plo) Plo[pi] = (float)v;
     }
 }
 
@@ -1130,14 +1141,14 @@ __global__ void k_sa_PT(int nc, const int* cdof_sys, const int* cdof_off, const 
 // for each the lanes take the entries of AP(g,:), whose columns are distinct, so the targets
 // are distinct: a fixed summation order without atomics.
 constexpr int kSaAcWarps = 4;
-template <typename KT>
+template <typename KT, typename ST>
 __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* cnode_sys, const int* cdof_off,
                                                            const int* cnode_off, const int* crowptr,
                                                            const int* ccolind, const int* ptn_ptr,
                                                            const int* ptn_fine, const int* ptbase, const int* pnnz,
-                                                           const int* poff, const double* PT, const int* apn_ptr,
+                                                           const int* poff, const ST* PT, const int* apn_ptr,
                                                            const int* apn_col, const int* apbase, const int* apnnz,
-                                                           const int* apoff, const double* AP, KT* Ac, const int* sel) {
+                                                           const int* apoff, const ST* AP, KT* Ac, const int* sel) {
   __shared__ int s_col[kSaAcWarps][kSaMaxDeg];
   __shared__ double s_acc[kSaAcWarps][4 * kSaMaxDeg];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1160,8 +1171,8 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
   }
   const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
   const size_t prs = (size_t)2 * pnnz[s], ars = (size_t)2 * apnnz[s];
-  const double* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);  // P'((c2,J),(c,u)) = t0[c2 prs + c dT + u]
-  const double* apb = AP + apoff[s];
+  const ST* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);  // P'((c2,J),(c,u)) = t0[c2 prs + c dT + u]
+  const ST* apb = AP + apoff[s];
   const int apb0 = apbase[s];
   for (int u0 = 0; u0 < dT; u0 += 32) {
     const int my = u0 + lane;
@@ -1181,12 +1192,13 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
       const int ar = __shfl_sync(0xffffffffu, g_ar, e), dA = __shfl_sync(0xffffffffu, g_dA, e);
       const double v00 = __shfl_sync(0xffffffffu, w00, e), v01 = __shfl_sync(0xffffffffu, w01, e);
       const double v10 = __shfl_sync(0xffffffffu, w10, e), v11 = __shfl_sync(0xffffffffu, w11, e);
-      const double* a0 = apb + 2 * (size_t)(ar - apb0);  // AP((c,g),(c3,kk)) = a0[c ars + c3 dA + kk]
+      const ST* a0 = apb + 2 * (size_t)(ar - apb0);  // AP((c,g),(c3,kk)) = a0[c ars + c3 dA + kk]
       __syncwarp();  // the previous entry's sums are visible to the warp
       for (int kk = lane; kk < dA; kk += 32) {
         const int pos = sa_find(col, degc, apn_col[ar + kk]);
         if (pos < 0) continue;
-        const double x00 = a0[kk], x01 = a0[dA + kk], x10 = a0[ars + kk], x11 = a0[ars + dA + kk];
+        const double x00 = (double)a0[kk], x01 = (double)a0[dA + kk], x10 = (double)a0[ars + kk],
+                     x11 = (double)a0[ars + dA + kk];
         acc[pos] += v00 * x00 + v01 * x10;
         acc[degc + pos] += v00 * x01 + v01 * x11;
         acc[2 * degc + pos] += v10 * x00 + v11 * x10;
@@ -1320,18 +1332,26 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
       const unsigned char* mk = l == 0 ? cmask : nullptr;
       l1(l);
       const int nbf = (F.ndof + 127) / 128, nbc = (C.ndof + 127) / 128;
-      k_sa_P<KT, VT><<<nbf, 128, 0, st>>>(F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk,
-                                          (const VT*)F.invd, F.sa_agg, F.pn_ptr, F.pn_col, F.pbase, F.pnnz, F.poff,
-                                          F.sa_p, psel), ++*launches;
-      k_sa_AP<KT><<<(int)(((long long)F.nn * kSaGL + 127) / 128), 128, 0, st>>>(F.nn, F.node_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr,
-                                       F.pn_col, F.pbase, F.pnnz, F.poff, F.sa_p, F.apn_ptr, F.apn_col, F.apbase,
-                                       F.apnnz, F.apoff, F.sa_ap, sel), ++*launches;
-      k_sa_PT<<<nbc, 128, 0, st>>>(C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, F.ptn_ptr, F.ptn_fine, F.ptn_k,
-                                   F.ptbase, F.pn_ptr, F.pbase, F.pnnz, F.poff, F.sa_p, F.sa_pt, F.sa_plo,
-                                   F.sa_ptlo, psel), ++*launches;
-      k_sa_Ac<KT><<<(C.nn + kSaAcWarps - 1) / kSaAcWarps, 32 * kSaAcWarps, 0, st>>>(C.nn, C.node_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr,
-                                       F.ptn_fine, F.ptbase, F.pnnz, F.poff, F.sa_pt, F.apn_ptr, F.apn_col, F.apbase,
-                                       F.apnnz, F.apoff, F.sa_ap, (KT*)C.A, sel), ++*launches;
+      // the mixed form sets up in FP32 into the arrays its transfers read (sa_plo, sa_ptlo); the
+      // FP64 form in FP64, with FP32 copies
+      using ST = typename std::conditional<sizeof(KT) == 4, float, double>::type;
+      ST* Pv = sizeof(KT) == 4 ? (ST*)F.sa_plo : (ST*)F.sa_p;
+      ST* PTv = sizeof(KT) == 4 ? (ST*)F.sa_ptlo : (ST*)F.sa_pt;
+      ST* APv = (ST*)F.sa_ap;
+      k_sa_P<KT, VT, ST><<<nbf, 128, 0, st>>>(F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk,
+                                              (const VT*)F.invd, F.sa_agg, F.pn_ptr, F.pn_col, F.pbase, F.pnnz,
+                                              F.poff, Pv, psel), ++*launches;
+      const int ms = F.ap_maxrow <= kSaApSm ? F.ap_maxrow : 0;  // rows summed in shared memory
+      k_sa_AP<KT, ST><<<(int)(((long long)F.nn * kSaGL + 127) / 128), 128, sa_ap_smem<ST>(ms), st>>>(F.nn, F.node_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr,
+                                       F.pn_col, F.pbase, F.pnnz, F.poff, Pv, F.apn_ptr, F.apn_col, F.apbase,
+                                       F.apnnz, F.apoff, APv, sel, ms), ++*launches;
+      k_sa_PT<ST><<<nbc, 128, 0, st>>>(C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, F.ptn_ptr, F.ptn_fine, F.ptn_k,
+                                       F.ptbase, F.pn_ptr, F.pbase, F.pnnz, F.poff, Pv, PTv,
+                                       sizeof(KT) == 4 ? nullptr : F.sa_plo, sizeof(KT) == 4 ? nullptr : F.sa_ptlo,
+                                       psel), ++*launches;
+      k_sa_Ac<KT, ST><<<(C.nn + kSaAcWarps - 1) / kSaAcWarps, 32 * kSaAcWarps, 0, st>>>(C.nn, C.node_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr,
+                                       F.ptn_fine, F.ptbase, F.pnnz, F.poff, PTv, F.apn_ptr, F.apn_col, F.apbase,
+                                       F.apnnz, F.apoff, APv, (KT*)C.A, sel), ++*launches;
     }
     l1(a->nlev - 1);
   } else {

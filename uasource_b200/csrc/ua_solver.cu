@@ -1396,8 +1396,10 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   const bool fp32 = sizeof(KT) == 4;
   if (amg) {
     // the systems of this Newton step only (the others' hierarchies are not read)
-    int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches, w->sel, &w->h_sel,
-                         p->amg_P_refresh);
+    // prolongator refresh: every Newton step in FP64 (the Newton trajectory of the reference's
+    // direct solves), every fourth in the mixed form, unless set
+    const int prefresh = p->amg_P_refresh > 0 ? p->amg_P_refresh : (fp32 ? 4 : 1);
+    int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches, w->sel, &w->h_sel, prefresh);
     if (rc) return rc;
   } else {
     k_invdiag<KT, VT><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, (VT*)w->invd), ++g_launches;
@@ -2935,7 +2937,7 @@ extern "C" void ua_params_default(ua_params* p) {
   p->krylov_eta_c = 0.5; p->krylov_eta_max = 0.1; p->precond_bf16 = 1;
   p->amg_smoothed = 1;
   p->krylov_full_grid = 0;
-  p->amg_P_refresh = 4;
+  p->amg_P_refresh = 0;
   p->uvh_h_sweeps = 0;
   p->krylov_sell = 1;
   p->krylov_precond = UA_PC_AMG;

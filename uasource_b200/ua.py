@@ -85,7 +85,7 @@ class CtrlVar:
     precond_bf16: int = 1
     amg_smoothed: int = 1
     krylov_full_grid: int = 0
-    amg_P_refresh: int = 4
+    amg_P_refresh: int = 0
     uvh_h_sweeps: int = 0
     krylov_sell: int = 1
     SlidingLaw: str = "Weertman"          # any name of L.SLIDING_LAWS
