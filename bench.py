@@ -450,10 +450,10 @@ def run_ours(args):
     ele_per_row = Ne / rows
     # per class: (ms, launches, algorithmic bytes summed over the launches, bytes per non-zero / row)
     cand = {
-        "uv_patch_kernel<3,K,float> (tangent+residual assembly)":
+        "uv_p1_kernel<K,float> (tangent+residual assembly)":
             (prof["asmK_ms"], prof["asmK_n"], 4 * wn["asmK"] + (12 * ele_per_row + 48 + 8) * wr["asmK"],
              "4 B/nnz (K write) + per row: 12*Ne/rows connectivity + 48 nodal fields + 8 R"),
-        "uv_patch_kernel<3,R> (residual-only assembly)":
+        "uv_p1_kernel<K off> (residual-only assembly)":
             (prof["asmR_ms"], prof["asmR_n"], (12 * ele_per_row + 48 + 8) * wr["asmR"],
              "per row: 12*Ne/rows connectivity + 48 nodal fields + 8 R"),
         # node-sliced tangent copies: four values per column index, so 1 B of index per non-zero;
@@ -477,21 +477,20 @@ def run_ours(args):
     # launch of each class over its algorithmic bytes (MB), captured with
     # `bench.py --batch 32 --legs mixed --steps 1 --warmup 1` (every system active), scaled to this
     # launch size
-    traffic_ratio = {"uv_patch_kernel<3,K": 193.88 / 145.44, "uv_patch_kernel<3,R": 130.97 / 79.95,
+    traffic_ratio = {"uv_p1_kernel<K,": (133.05 + 48.05) / 145.44, "uv_p1_kernel<K off": None,
                      "k_sell<float,float,SpMV": None, "k_sell<bf16,float,residual": None,
                      "k_sell<bf16,float,smoothing": None}
     tr = next((v for k, v in traffic_ratio.items() if dom.startswith(k)), None)
-    # The assembly classes are bound by FP64 issue, not HBM: their FP64 roofline beside the HBM one.
-    # Executed FP64 operations per P1 element (2 DFMA + DADD + DMUL, ncu instruction counts of the
-    # 32-mesh batch: 6.036e9 / 1,162,956 elements residual-only, 7.136e9 tangent+residual) over
-    # the measured launch time; peak 148 SMs x 64 DFMA/clock x 2 x 1965 MHz = 37.2 TFLOP/s (nominal,
-    # no measured FP64 figure in MEASURED_PEAKS.json).
+    # The assembly is bound by latency and FP64 issue, not HBM: its FP64 roofline beside the HBM one.
+    # Executed FP64 operations per P1 element of the tangent+residual pass (2 DFMA + DADD + DMUL,
+    # ncu per-cycle instruction sums x cycles of the 32-mesh batch: 4.82e9 over 1,162,956 elements,
+    # patch halos included) over the measured launch time; peak 148 SMs x 64 DFMA/clock x 2 x 1965
+    # MHz = 37.2 TFLOP/s (nominal, no measured FP64 figure in MEASURED_PEAKS.json).
     fp64_peak = 148 * 64 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
     fp64 = {}
-    for key, fpe in (("uv_patch_kernel<3,K,float> (tangent+residual assembly)", 6136.0),
-                     ("uv_patch_kernel<3,R> (residual-only assembly)", 5190.0)):
+    for key, fpe in (("uv_p1_kernel<K,float> (tangent+residual assembly)", 4146.0),):
         cms, cn, _, _ = cand[key]
-        cls_rows = wr["asmK" if "<3,K" in key else "asmR"]
+        cls_rows = wr["asmK"]
         if cms > 0:
             tf = fpe * ele_per_row * cls_rows / (cms / 1000) / 1e12
             fp64[key] = {"achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": tf / fp64_peak,
