@@ -343,6 +343,8 @@ namespace p1 {
 constexpr int kThreads = 256;  // the largest CTA (launch bounds); 128 also runs (asm_threads)
 // scratch slots per lane: residual scalars first, then the drag derivatives
 enum { TX = 0, TY = 1, FX = 2, FY = 3, CXU = 4, CYV = 5, CXV = 6, NSC = 7 };
+// staged fields of a patch's element nodes
+enum { ND_X = 0, ND_Y, ND_U, ND_V, ND_H, ND_S, ND_C, ND_A, ND_SS, ND_B, ND_RHO, ND_M, ND_N, ND_COUNT };
 
 __device__ __forceinline__ double sel3(double a0, double a1, double a2, int i) {
   return i == 0 ? a0 : (i == 1 ? a1 : a2);
@@ -387,6 +389,8 @@ __global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
   double* sR = reinterpret_cast<double*>(smem + koff);  // 12 E
   double* sN = sR + 12 * E;                              // N_a(ip) at [ip*3 + a], weights at [18 + ip]
   double* scr = sN + 24;                                 // NSC x 32 per warp
+  double* nd = scr + (blockDim.x >> 5) * (NSC * 32);     // staged node fields [ND_COUNT][MH]
+  const int MH = M.max_patch_hnodes;
   const int e0 = M.patch_elem_ptr[p], ne = M.patch_elem_ptr[p + 1] - e0;
   const int uoff = M.sys_dof_off[s] - M.sys_node_off[s];
   const int nn_s = M.sys_node_off[s + 1] - M.sys_node_off[s];
@@ -396,6 +400,24 @@ __global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
   const bool cube = S.cube != 0.0;
   if (threadIdx.x < 18) sN[threadIdx.x] = Q.fun[threadIdx.x / 3][threadIdx.x % 3];
   else if (threadIdx.x < 24) sN[threadIdx.x] = Q.w[threadIdx.x - 18];
+  // stage the fields of the patch's element nodes: every load of the element loop then comes
+  // from shared memory, and the gathers of the whole patch are in flight together
+  const int hb0 = M.patch_hnode_ptr[p], nh = M.patch_hnode_ptr[p + 1] - hb0;
+  for (int t = threadIdx.x; t < nh; t += blockDim.x) {
+    int gn = __ldg(M.patch_hnodes + hb0 + t);
+    bool okn = true;
+    UA_CHECK_INDEX(M.dbg, gn, M.sys_node_off[s], M.sys_node_off[s + 1], BS_ELEM_NODE, okn);
+    (void)okn;
+    double u = __ldg(in.X + uoff + gn), v = __ldg(in.X + voff + gn);  // at X + gamma dX (CalcCostFunctionNR.m:14-16)
+    if (in.dX) { u += gam * __ldg(in.dX + uoff + gn); v += gam * __ldg(in.dX + voff + gn); }
+    nd[ND_X * MH + t] = __ldg(M.x + gn); nd[ND_Y * MH + t] = __ldg(M.y + gn);
+    nd[ND_U * MH + t] = u; nd[ND_V * MH + t] = v;
+    nd[ND_H * MH + t] = __ldg(in.h + gn); nd[ND_S * MH + t] = __ldg(in.s + gn);
+    nd[ND_C * MH + t] = __ldg(in.C + gn); nd[ND_A * MH + t] = __ldg(in.A + gn);
+    nd[ND_SS * MH + t] = __ldg(in.S + gn); nd[ND_B * MH + t] = __ldg(in.B + gn);
+    nd[ND_RHO * MH + t] = __ldg(in.rho + gn); nd[ND_M * MH + t] = __ldg(in.m + gn);
+    nd[ND_N * MH + t] = cube ? 3.0 : __ldg(in.n + gn);
+  }
   __syncthreads();
 
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -410,32 +432,28 @@ __global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
   for (int base = 0; base < ne; base += ngrp) {  // same trip count for every thread of the block
     const int t = base + wid * 5 + grp;
     bool inb = true;
-    int e = __ldg(M.patch_elems + e0 + min(t, ne - 1));
-    UA_CHECK_INDEX(M.dbg, e, 0, M.ne, BS_PATCH_ELEM, inb);
-    int n0 = __ldg(M.conn + e), n1 = __ldg(M.conn + (size_t)M.ne + e), n2 = __ldg(M.conn + 2 * (size_t)M.ne + e);
-    UA_CHECK_INDEX(M.dbg, n0, 0, M.nn, BS_ELEM_NODE, inb);
-    UA_CHECK_INDEX(M.dbg, n1, 0, M.nn, BS_ELEM_NODE, inb);
-    UA_CHECK_INDEX(M.dbg, n2, 0, M.nn, BS_ELEM_NODE, inb);
+    // the element's nodes as indices into the staged fields
+    const size_t eln = (size_t)(e0 + min(t, ne - 1)) * 3;
+    int n0 = __ldg(M.patch_elnodes + eln), n1 = __ldg(M.patch_elnodes + eln + 1), n2 = __ldg(M.patch_elnodes + eln + 2);
+    UA_CHECK_INDEX(M.dbg, n0, 0, nh, BS_ELEM_NODE, inb);
+    UA_CHECK_INDEX(M.dbg, n1, 0, nh, BS_ELEM_NODE, inb);
+    UA_CHECK_INDEX(M.dbg, n2, 0, nh, BS_ELEM_NODE, inb);
     const bool valid = lane < 30 && t < ne && inb;
+    auto nf = [&](int f, int l) { return nd[f * MH + l]; };
     // element geometry (derivVector.m:96-109 with the constant P1 derivatives of the
     // basis [xi, 1-xi-eta, eta]); one reciprocal of detJ
-    const double x0 = __ldg(M.x + n0), x1 = __ldg(M.x + n1), x2 = __ldg(M.x + n2);
-    const double y0 = __ldg(M.y + n0), y1 = __ldg(M.y + n1), y2 = __ldg(M.y + n2);
+    const double x0 = nf(ND_X, n0), x1 = nf(ND_X, n1), x2 = nf(ND_X, n2);
+    const double y0 = nf(ND_Y, n0), y1 = nf(ND_Y, n1), y2 = nf(ND_Y, n2);
     const double J11 = x0 - x1, J12 = y0 - y1, J21 = x2 - x1, J22 = y2 - y1;
     const double detJ = J11 * J22 - J12 * J21;
     const double rd = 1.0 / detJ;
     const double Dx0 = J22 * rd, Dx1 = (J12 - J22) * rd, Dx2 = -J12 * rd;
     const double Dy0 = -J21 * rd, Dy1 = (J21 - J11) * rd, Dy2 = J11 * rd;
-    // nodal values; velocities at X + gamma dX (CalcCostFunctionNR.m:14-16)
-    auto vel = [&](int nd, double& u, double& v) {
-      u = __ldg(in.X + uoff + nd);
-      v = __ldg(in.X + voff + nd);
-      if (in.dX) { u += gam * __ldg(in.dX + uoff + nd); v += gam * __ldg(in.dX + voff + nd); }
-    };
-    double u0, v0, u1, v1, u2, v2;
-    vel(n0, u0, v0); vel(n1, u1, v1); vel(n2, u2, v2);
-    const double h0 = __ldg(in.h + n0), h1 = __ldg(in.h + n1), h2 = __ldg(in.h + n2);
-    const double s0 = __ldg(in.s + n0), s1 = __ldg(in.s + n1), s2 = __ldg(in.s + n2);
+    // nodal values (velocities staged at X + gamma dX)
+    const double u0 = nf(ND_U, n0), u1 = nf(ND_U, n1), u2 = nf(ND_U, n2);
+    const double v0 = nf(ND_V, n0), v1 = nf(ND_V, n1), v2 = nf(ND_V, n2);
+    const double h0 = nf(ND_H, n0), h1 = nf(ND_H, n1), h2 = nf(ND_H, n2);
+    const double s0 = nf(ND_S, n0), s1 = nf(ND_S, n1), s2 = nf(ND_S, n2);
     // element constants (:322-347)
     const double dsdx = (Dx0 * s0 + Dx1 * s1) + Dx2 * s2, dhdx = (Dx0 * h0 + Dx1 * h1) + Dx2 * h2;
     const double dsdy = (Dy0 * s0 + Dy1 * s1) + Dy2 * s2, dhdy = (Dy0 * h0 + Dy1 * h1) + Dy2 * h2;
@@ -448,14 +466,12 @@ __global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
     const double hint = (h0 * N0 + h1 * N1) + h2 * N2;
     const double uint = (u0 * N0 + u1 * N1) + u2 * N2;
     const double vint = (v0 * N0 + v1 * N1) + v2 * N2;
-    auto interp = [&](const double* f) {
-      return (__ldg(f + n0) * N0 + __ldg(f + n1) * N1) + __ldg(f + n2) * N2;
-    };
-    double Cint = interp(in.C), Aint = interp(in.A);
+    auto interp = [&](int f) { return (nf(f, n0) * N0 + nf(f, n1) * N1) + nf(f, n2) * N2; };
+    double Cint = interp(ND_C), Aint = interp(ND_A);
     if (Cint < P.Cmin) Cint = P.Cmin;        // :205
     if (Aint < P.AGlenmin) Aint = P.AGlenmin;  // :243
-    const double Hint = interp(in.S) - interp(in.B);
-    const double rhoint = interp(in.rho);
+    const double Hint = interp(ND_SS) - interp(ND_B);
+    const double rhoint = interp(ND_RHO);
     // flotation at the integration point (:300-310)
     const double hfint = rhow * Hint / rhoint;
     const double tf = tanh_step(P.kH, hint - hfint, P.Hh0);
@@ -467,10 +483,11 @@ __global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
     // drag (BasalDrag.m:54-77, :410-446): Weertman drag is identically zero on floating ice (He = 0)
     double taux = 0, tauy = 0, dxu = 0, dyv = 0, dxv = 0;
     if (GEN) {
-      const int gn[3] = {n0, n1, n2};
+      const int gn[3] = {__ldg(M.patch_hnodes + hb0 + n0), __ldg(M.patch_hnodes + hb0 + n1),
+                         __ldg(M.patch_hnodes + hb0 + n2)};
       const double Nw[3] = {N0, N1, N2};
       const Drag d = basal_drag_general(P, Heint, 0.0, hint, Hint, rhoint, rhow, g, uint, vint, Cint,
-                                        interp(in.m), drag_interp<3>(in.drag, gn, Nw));
+                                        interp(ND_M), drag_interp<3>(in.drag, gn, Nw));
       taux = d.taux; tauy = d.tauy; dxu = d.dxu; dyv = d.dyv; dxv = d.dxv;
     } else if (Heint > 0) {
       const double sp2 = uint * uint + vint * vint + P.SpeedZero * P.SpeedZero;
@@ -478,7 +495,7 @@ __global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
       if (cube) {
         Cm = rcbrt(Cint + P.Czero); ps = rcbrt(sp2); cD = -2.0 / 3.0;
       } else {
-        const double mint = interp(in.m);
+        const double mint = interp(ND_M);
         Cm = pow(Cint + P.Czero, -1.0 / mint); ps = pow(sp2, (1.0 - mint) / (2.0 * mint)); cD = 1.0 / mint - 1.0;
       }
       const double beta2 = Cm * ps, Dbeta2 = cD * Cm * ps / sp2;
@@ -492,7 +509,7 @@ __global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
     if (cube) {
       Am = rcbrt(Aint); pe = rcbrt(e2); cE = -1.0 / 6.0;
     } else {
-      const double nint = interp(in.n);
+      const double nint = interp(ND_N);
       Am = pow(Aint, -1.0 / nint); pe = pow(sqrt(e2), (1.0 - nint) / nint); cE = (1.0 - nint) / (4.0 * nint);
     }
     const double eta = 0.5 * Am * pe + P.etaZero;
@@ -579,9 +596,10 @@ __global__ void __launch_bounds__(p1::max_threads(RV), p1::min_blocks(RV))
   patch_scatter<3, WITHK, KT>(M, out, p, s, uoff, voff, sK, sR, E);
 }
 
-size_t uv_p1_smem(bool withK, bool fp32, int E, int threads) {
+size_t uv_p1_smem(bool withK, bool fp32, int E, int threads, int MH) {
   size_t k = withK ? (((size_t)ElemIdx<3>::NKE * E * (fp32 ? 4 : 8) + 15) & ~(size_t)15) : 0;
-  return k + (size_t)12 * E * 8 + 24 * 8 + (size_t)(threads / 32) * p1::NSC * 32 * 8;
+  return k + (size_t)12 * E * 8 + 24 * 8 + (size_t)(threads / 32) * p1::NSC * 32 * 8 +
+         (size_t)p1::ND_COUNT * MH * 8;
 }
 
 // P2 (6-node elements): one element per thread in 128-thread blocks, the
@@ -675,7 +693,7 @@ static cudaError_t launch_p1(const ua_mesh* m, const UvPhys& P, const UvIn& in, 
   if (threads != 128 && threads != 256) return cudaErrorInvalidConfiguration;
   const int rv = regs == 96 ? 1 : (regs == 80 ? 2 : 0);
   if (rv == 1 && threads != 128) return cudaErrorInvalidConfiguration;
-  size_t sm = uv_p1_smem(WITHK, sizeof(KT) == 4, m->dm.max_patch_elems, threads);
+  size_t sm = uv_p1_smem(WITHK, sizeof(KT) == 4, m->dm.max_patch_elems, threads, m->dm.max_patch_hnodes);
   const bool gen = P.law != UA_SLIDING_WEERTMAN || P.melange;
   auto kern = gen ? p1_kernel<WITHK, KT, true>(rv) : p1_kernel<WITHK, KT, false>(rv);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -94,6 +94,12 @@ struct DevMesh {
   const uint16_t* contrib;
   const int* prow_diag;       // per patch row (aligned with patch_nodes): pq index of diagonal
   int max_patch_elems;
+  // the nodes of each patch's elements (its rows and their halo), sorted, and per patch element
+  // the patch-local index of each of its nodes (element-local order), for staging node data
+  const int* patch_hnode_ptr; // [npatch+1]
+  const int* patch_hnodes;    // global node ids
+  const uint16_t* patch_elnodes;  // [patch element][nod], aligned with patch_elems
+  int max_patch_hnodes;
   unsigned long long* dbg;    // first bounds violation (debug build; null otherwise)
 };
 

@@ -211,7 +211,9 @@ struct PatchPlan {
   std::vector<int> patch_q_ptr{0}, pq_cptr{0}, prow_diag;
   std::vector<uint32_t> pq_rk;
   std::vector<uint16_t> contrib;
-  int max_elems = 0;
+  std::vector<int> hnode_ptr{0}, hnodes;
+  std::vector<uint16_t> elnodes;
+  int max_elems = 0, max_hnodes = 0;
 };
 
 static int build_patch_plan(const ua_mesh* m, const std::vector<int>& conn, const std::vector<double>& X,
@@ -278,6 +280,24 @@ static int build_patch_plan(const ua_mesh* m, const std::vector<int>& conn, cons
           P.pq_cptr.push_back((int)P.contrib.size());
         }
       }
+      // the nodes of the patch's elements, sorted, and each element's nodes as indices into them
+      {
+        std::vector<int> hn;
+        hn.reserve(elems.size() * nod);
+        for (int e : elems)
+          for (int c = 0; c < nod; ++c) hn.push_back(conn[(size_t)c * NE + e]);
+        std::sort(hn.begin(), hn.end());
+        hn.erase(std::unique(hn.begin(), hn.end()), hn.end());
+        if (hn.size() > 65535) return set_error(UA_ERR_BAD_MESH, "patch with more than 65535 element nodes");
+        for (int e : elems)
+          for (int c = 0; c < nod; ++c) {
+            const int v = conn[(size_t)c * NE + e];
+            P.elnodes.push_back((uint16_t)(std::lower_bound(hn.begin(), hn.end(), v) - hn.begin()));
+          }
+        P.hnodes.insert(P.hnodes.end(), hn.begin(), hn.end());
+        P.hnode_ptr.push_back((int)P.hnodes.size());
+        P.max_hnodes = std::max(P.max_hnodes, (int)hn.size());
+      }
       P.patch_nodes.insert(P.patch_nodes.end(), nodes.begin(), nodes.end());
       P.patch_node_ptr.push_back((int)P.patch_nodes.size());
       P.patch_elems.insert(P.patch_elems.end(), elems.begin(), elems.end());
@@ -292,8 +312,9 @@ static int build_patch_plan(const ua_mesh* m, const std::vector<int>& conn, cons
 // Uploads a plan into the handle, releasing the buffers of the plan it replaces.
 static int install_patch_plan(ua_mesh* m, const PatchPlan& P) {
   DevMesh& dm = m->dm;
-  const void* old[10] = {dm.patch_sys, dm.patch_node_ptr, dm.patch_nodes, dm.patch_elem_ptr, dm.patch_elems,
-                         dm.patch_q_ptr, dm.pq_rk, dm.pq_cptr, dm.contrib, dm.prow_diag};
+  const void* old[13] = {dm.patch_sys, dm.patch_node_ptr, dm.patch_nodes, dm.patch_elem_ptr, dm.patch_elems,
+                         dm.patch_q_ptr, dm.pq_rk, dm.pq_cptr, dm.contrib, dm.prow_diag,
+                         dm.patch_hnode_ptr, dm.patch_hnodes, dm.patch_elnodes};
   if (m->stream) UA_CUDA_TRY(cudaStreamSynchronize(m->stream));
   for (const void* q : old) dev_free(m, q);
   int rc;
@@ -307,8 +328,12 @@ static int install_patch_plan(ua_mesh* m, const PatchPlan& P) {
   if ((rc = upload_vec(m, P.pq_cptr, &dm.pq_cptr))) return rc;
   if ((rc = upload_vec(m, P.contrib, &dm.contrib))) return rc;
   if ((rc = upload_vec(m, P.prow_diag, &dm.prow_diag))) return rc;
+  if ((rc = upload_vec(m, P.hnode_ptr, &dm.patch_hnode_ptr))) return rc;
+  if ((rc = upload_vec(m, P.hnodes, &dm.patch_hnodes))) return rc;
+  if ((rc = upload_vec(m, P.elnodes, &dm.patch_elnodes))) return rc;
   dm.npatch = (int)P.patch_sys.size();
   dm.max_patch_elems = P.max_elems;
+  dm.max_patch_hnodes = P.max_hnodes;
   return UA_OK;
 }
 
