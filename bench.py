@@ -807,7 +807,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default assembly schedule")
     ap.add_argument("--batch", type=int, default=BATCH, help="meshes per step (default 256)")
     # the 1M-element P2 workloads (their own JSON line; the headline line is the batched one)
-    ap.add_argument("--workload", default="batch", choices=["batch", "uv1m", "uvh1m"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "uv1m", "uvh1m", "p2"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -815,6 +815,13 @@ def main():
         return run_uv1m(args)
     if args.workload == "uvh1m":
         return run_uvh1m(args)
+    if args.workload == "p2":  # the P2 legs alone (their own line; bounded cases for profiling)
+        import numpy as np
+        import uasource_b200 as ua
+        from uasource_b200 import lib as L
+        from uasource_b200 import synth
+        print(json.dumps({"workload": "p2", "p2": _p2_legs(args, ua, L, synth, np)}), flush=True)
+        return 0
     return run_ours(args)
 
 
