@@ -147,6 +147,14 @@ struct Amg {
   // whose prolongators the current set-up recomputes
   std::vector<int> p_age, h_prefresh;
   int* d_prefresh = nullptr;
+  // the numeric set-up of a Newton step captured as one CUDA graph per (precision, selection
+  // kind) and replayed: every argument is a fixed device buffer of the handle
+  cudaGraphExec_t setup_exec[8] = {};
+  long long setup_nodes[8] = {};
+  ~Amg() {
+    for (auto& e : setup_exec)
+      if (e) cudaGraphExecDestroy(e);
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -1364,8 +1372,7 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
     }
     for (int l = 0; l < a->nlev; ++l) l1(l);
   }
-  const int sm = (int)(sizeof(double) * (size_t)a->maxdn * 2 * a->maxdn);
-  UA_CUDA_TRY(cudaFuncSetAttribute(k_amg_dense_inverse<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  const int sm = (int)(sizeof(double) * (size_t)a->maxdn * 2 * a->maxdn);  // attribute set by the caller
   k_amg_dense_inverse<KT><<<a->nsys, 256, sm, st>>>(a->d_depth, a->d_dn, a->d_doff, a->d_lev_rowptr,
                                                      a->d_lev_colind, a->d_lev_A, a->d_lev_dofoff, a->dense, sel),
       ++*launches;
@@ -1516,7 +1523,7 @@ const void* amg_bf16_copy(ua_mesh* m, const float* K0, long long nnz, long long*
 
 int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
                 const unsigned char* cmask, long long* launches, const int* sel, const std::vector<int>* h_sel,
-                int p_refresh) {
+                int p_refresh, bool graph) {
   // prolongators: recomputed for the selected systems on the first set-up of their solve and then
   // every p_refresh-th one (all of them when no host selection is given)
   Amg* a = m->amg;
@@ -1538,8 +1545,35 @@ int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* 
     UA_CUDA_TRY(cudaStreamSynchronize(m->stream));  // h_prefresh is rewritten by the next set-up
     psel = a->d_prefresh;
   }
-  if (fp32) return numeric_t<float, float>(m, rowptr0, colind0, (const float*)K0, cmask, sel, psel, launches);
-  return numeric_t<double, double>(m, rowptr0, colind0, (const double*)K0, cmask, sel, psel, launches);
+  const int sm = (int)(sizeof(double) * (size_t)a->maxdn * 2 * a->maxdn);
+  if (fp32)
+    UA_CUDA_TRY(cudaFuncSetAttribute(k_amg_dense_inverse<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  else
+    UA_CUDA_TRY(cudaFuncSetAttribute(k_amg_dense_inverse<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  auto run = [&](long long* l) {
+    return fp32 ? numeric_t<float, float>(m, rowptr0, colind0, (const float*)K0, cmask, sel, psel, l)
+                : numeric_t<double, double>(m, rowptr0, colind0, (const double*)K0, cmask, sel, psel, l);
+  };
+  if (!graph) return run(launches);
+  // one captured graph per kind of call (FP32/FP64 values, prolongator selection, handle's
+  // selection), replayed at every later Newton step
+  const int key = (fp32 ? 1 : 0) + (psel == a->d_prefresh && psel ? 2 : 0) + (sel ? 4 : 0);
+  if (!a->setup_exec[key]) {
+    long long n = 0;
+    cudaGraph_t gr = nullptr;
+    UA_CUDA_TRY(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = run(&n);
+    cudaError_t ce = cudaStreamEndCapture(m->stream, &gr);
+    if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+    if (ce != cudaSuccess) return set_error(UA_ERR_CUDA, "AMG set-up graph capture: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&a->setup_exec[key], gr, 0);
+    cudaGraphDestroy(gr);
+    if (ce != cudaSuccess) return set_error(UA_ERR_CUDA, "AMG set-up graph: %s", cudaGetErrorString(ce));
+    a->setup_nodes[key] = n;
+  }
+  UA_CUDA_TRY(cudaGraphLaunch(a->setup_exec[key], m->stream));
+  *launches += a->setup_nodes[key];
+  return UA_OK;
 }
 
 void amg_restart_P(ua_mesh* m, const std::vector<int>& run) {

@@ -68,9 +68,10 @@ const void* amg_invd0(const ua_mesh* m);
 // sel (device): the systems of this Newton step (others keep their hierarchies); h_sel (host copy)
 // and p_refresh > 1: each system's prolongators are recomputed on the first set-up of its solve
 // (amg_restart_P) and then every p_refresh-th set-up, the coarse operators every time.
+// graph: run the set-up's launches as a captured CUDA graph (captured once per kind of call).
 int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* K0, bool fp32,
                 const unsigned char* cmask, long long* launches, const int* sel = nullptr,
-                const std::vector<int>* h_sel = nullptr, int p_refresh = 1);
+                const std::vector<int>* h_sel = nullptr, int p_refresh = 1, bool graph = false);
 // the systems of `run` start a solve: their next set-up recomputes the prolongators
 void amg_restart_P(ua_mesh* m, const std::vector<int>& run);
 // uvh handles: extract the velocity block of the 3-dof tangent K3 (and its

@@ -1399,7 +1399,8 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     // prolongator refresh: every Newton step in FP64 (the Newton trajectory of the reference's
     // direct solves), every fourth in the mixed form, unless set
     const int prefresh = p->amg_P_refresh > 0 ? p->amg_P_refresh : (fp32 ? 4 : 1);
-    int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches, w->sel, &w->h_sel, prefresh);
+    int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches, w->sel, &w->h_sel, prefresh,
+                         !w->no_graph && !p->profile);
     if (rc) return rc;
   } else {
     k_invdiag<KT, VT><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, (VT*)w->invd), ++g_launches;
