@@ -47,7 +47,7 @@ __device__ __forceinline__ void uv_deriv(const QuadTable& Q, int ip, const doubl
 
 // Contribution of integration point ip to the element tangent and residual
 // parts (accumulated into the outputs).
-template <int NOD, bool WITHK, typename KT>
+template <int NOD, bool WITHK, typename KT, bool GEN>
 __device__ __forceinline__ void uv_ip(const QuadTable& Q, const UvPhys& P, const SysScal& S, int ip,
                                       const int (&gn)[NOD], const DragFields& DF,
                                       const double (&Dx)[NOD], const double (&Dy)[NOD], double detJ,
@@ -93,10 +93,11 @@ __device__ __forceinline__ void uv_ip(const QuadTable& Q, const UvPhys& P, const
       exx += Dx[a] * un[a]; eyy += Dy[a] * vn[a];
       exy += 0.5 * (Dx[a] * vn[a] + Dy[a] * un[a]);
     }
-    const Drag d = (P.law == UA_SLIDING_WEERTMAN && !P.melange)
-                       ? basal_drag_weertman(P, Heint, deltaint, uint, vint, Cint, mint, cube)
-                       : basal_drag_general(P, Heint, deltaint, hint, Hint, rhoint, rhow, g, uint, vint, Cint, mint,
-                                            drag_interp<NOD>(DF, gn, N));
+    // GEN: any sliding law and the melange terms; else Weertman (the general code stays out of
+    // the Weertman build, whose registers it would crowd)
+    const Drag d = !GEN ? basal_drag_weertman(P, Heint, deltaint, uint, vint, Cint, mint, cube)
+                        : basal_drag_general(P, Heint, deltaint, hint, Hint, rhoint, rhow, g, uint, vint, Cint, mint,
+                                             drag_interp<NOD>(DF, gn, N));
     double eta, E;
     effective_viscosity(P, Aint, nint, exx, eyy, exy, eta, E, cube);
     const double dbdx = dsdx - dhdx, dbdy = dsdy - dhdy;
@@ -206,7 +207,7 @@ __device__ __forceinline__ void uv_zero(KT* Kuu, KT* Kvv, KT* Kuv, double* Tx, d
 // :398-417 regrouped (E11 = h(4exx+2eyy) Deu dNI/dx + 2h exy Deu dNI/dy with
 // Deu = E P_u(J)).  The tangent is produced symmetric, which is what
 // (K+K.')/2 at :530-531 yields.
-template <int NOD, bool WITHK, typename KT>
+template <int NOD, bool WITHK, typename KT, bool GEN>
 __device__ __forceinline__ void uv_element(const QuadTable& Q, const UvPhys& P, const SysScal& S,
                                            const int (&gn)[NOD], const DragFields& DF,
                                            const double (&xe)[NOD], const double (&ye)[NOD],
@@ -223,7 +224,7 @@ __device__ __forceinline__ void uv_element(const QuadTable& Q, const UvPhys& P, 
 #pragma unroll 1
   for (int ip = 0; ip < Q.nip; ++ip) {
     if (NOD != 3) uv_deriv<NOD>(Q, ip, xe, ye, Dx, Dy, detJ);
-    uv_ip<NOD, WITHK, KT>(Q, P, S, ip, gn, DF, Dx, Dy, detJ, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv,
+    uv_ip<NOD, WITHK, KT, GEN>(Q, P, S, ip, gn, DF, Dx, Dy, detJ, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv,
                           Kuv, Tx, Fx, Ty, Fy);
   }
 }
@@ -604,7 +605,7 @@ size_t uv_p1_smem(bool withK, bool fp32, int E, int threads, int MH) {
 
 // P2 (6-node elements): one element per thread in 128-thread blocks, the
 // integration points in a loop (the derivatives vary over the element).
-template <int NOD, bool WITHK, typename KT>
+template <int NOD, bool WITHK, typename KT, bool GEN>
 __global__ void __launch_bounds__(128, 1) uv_patch_kernel(DevMesh M, QuadTable Q, UvPhys P, UvIn in, UvOut out) {
   using I = ElemIdx<NOD>;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -666,7 +667,7 @@ __global__ void __launch_bounds__(128, 1) uv_patch_kernel(DevMesh M, QuadTable Q
     gather(__ldg(M.patch_elems + e0 + t), gn, xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn);
     KT Kuu[I::NS], Kvv[I::NS], Kuv[NOD * NOD];
     double Tx[NOD], Fx[NOD], Ty[NOD], Fy[NOD];
-    uv_element<NOD, WITHK, KT>(Q, P, S, gn, in.drag, xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv,
+    uv_element<NOD, WITHK, KT, GEN>(Q, P, S, gn, in.drag, xe, ye, hn, sn, un, vn, Cn, mn, An, nn, Sn, Bn, rn, Kuu, Kvv,
                                Kuv, Tx, Fx, Ty, Fy);
     store(t, Kuu, Kvv, Kuv, Tx, Fx, Ty, Fy);
   }
@@ -707,7 +708,8 @@ static cudaError_t launch_p1(const ua_mesh* m, const UvPhys& P, const UvIn& in, 
 template <int NOD, bool WITHK, typename KT>
 static cudaError_t launch_t(const ua_mesh* m, const UvPhys& P, const UvIn& in, const UvOut& out, int threads) {
   size_t sm = uv_patch_smem(NOD, WITHK, sizeof(KT) == 4, m->dm.max_patch_elems);
-  auto kern = uv_patch_kernel<NOD, WITHK, KT>;
+  const bool gen = P.law != UA_SLIDING_WEERTMAN || P.melange;
+  auto kern = gen ? uv_patch_kernel<NOD, WITHK, KT, true> : uv_patch_kernel<NOD, WITHK, KT, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   // all of the unified L1/shared storage as shared memory: several patch blocks per SM
