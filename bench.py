@@ -731,7 +731,10 @@ def run_uv1m(args):
         per, out = _timed_calls(lambda: ua.uv(ctrl, mua, bcs, ua.Fields.from_problem(P)), args.steps,
                                 max(1, min(args.warmup, 1)))
         Fo, _, _, _, info = out
-        res[name] = (per, np.concatenate([Fo.ub, Fo.vb]), info)
+        # one more solve with per-class launch timing (not part of the timed steps)
+        prof = ua.uv(ua.CtrlVar(precision=prec, krylov_rtol=rtol, profile=1).set_force_tolerance(1e-20), mua, bcs,
+                     ua.Fields.from_problem(P))[4]
+        res[name] = (per, np.concatenate([Fo.ub, Fo.vb]), info, {"kernels": prof.kernels, "device_ms": prof.device_ms})
     u64 = res["fp64"][1]
     err = float(np.linalg.norm(res["mixed"][1] - u64) / np.linalg.norm(u64))
     v_mx = 1000 * len(res["mixed"][0]) / sum(res["mixed"][0])
@@ -744,9 +747,9 @@ def run_uv1m(args):
                                    f"{P.Nnodes} nodes, seed 0, rForce<1e-20"},
             "plain_fp64": {"value": v_64, "unit": "solves/s",
                            "newton_iterations": res["fp64"][2].iterations,
-                           "pcg_iterations": res["fp64"][2].krylov_its_total},
+                           "pcg_iterations": res["fp64"][2].krylov_its_total, "profiled": res["fp64"][3]},
             "mixed": {"newton_iterations": res["mixed"][2].iterations,
-                      "pcg_iterations": res["mixed"][2].krylov_its_total},
+                      "pcg_iterations": res["mixed"][2].krylov_its_total, "profiled": res["mixed"][3]},
             "rel_err_mixed_vs_fp64": err, "mixed_over_plain": v_mx / v_64}
     print(json.dumps(line), flush=True)
     mua.close()

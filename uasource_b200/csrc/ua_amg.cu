@@ -52,6 +52,7 @@ struct AmgLevel {
   int nn = 0, ndof = 0;
   long long nnz = 0;
   int ap_maxrow = 0;  // longest A P row (coarse columns) of the level
+  int ac_maxdeg = 0;  // largest node degree of the next (coarse) level
   std::vector<int> node_off, dof_off, knz_off, nnzn;  // per system (0-sized when the system has no such level)
   // dof-level CSR of a coarse level, same layout rule as the finest level
   int *rowptr = nullptr, *colind = nullptr;
@@ -498,6 +499,9 @@ static int amg_build(ua_mesh* m, bool smoothed) {
       F.ap_maxrow = 0;
       for (size_t i = 0; i + 1 < g_apnp[l].size(); ++i)
         F.ap_maxrow = std::max(F.ap_maxrow, g_apnp[l][i + 1] - g_apnp[l][i]);
+      F.ac_maxdeg = 0;
+      for (size_t I = 0; I + 1 < g_ptr[l + 1].size(); ++I)
+        F.ac_maxdeg = std::max(F.ac_maxdeg, g_ptr[l + 1][I + 1] - g_ptr[l + 1][I]);
       F.sa_p = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
       F.sa_pt = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
       F.sa_ap = (double*)dalloc(m, a, sizeof(double) * (size_t)apoff[nsys], ok);
@@ -1039,16 +1043,20 @@ __global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int
 
 // A P rows: AP(i,:) = sum over unmasked columns j of A(i,j) P(j,:), kSaGL lanes per fine node g.
 // Both rows (c = 0, 1) of the node share its neighbour list, so each neighbour h contributes
-// A((c,g),(c2,h)) P((c2,h),:) to four output blocks (c, c3) at once; the neighbours go in
-// order and the lanes take the entries of P(h,:), whose targets in the AP row are distinct:
-// a fixed summation order without atomics.  A row of at most kSaApSm coarse columns is summed in
-// shared memory (its column list there too, for the searches) and written once; longer rows are
-// summed in place in global memory, in the same order.
+// A((c,g),(c2,h)) P((c2,h),:) to four output blocks (c, c3) at once.  The lanes first load the
+// data of up to kSaGL neighbours (column, the four A entries, the row of P(h,:)); the neighbours
+// then go in order.  A row of at most kSaApSm coarse columns is summed in shared memory (its
+// column list there too, for the searches): the lanes split into kSaApG groups of kSaGL / kSaApG,
+// group q takes the neighbours q, q + kSaApG, ... into its own copy of the row, its lanes the
+// entries of P(h,:), whose targets in the AP row are distinct, and the copies are added in group
+// order at the one write.  Longer rows are summed in place in global memory by all kSaGL lanes,
+// neighbour after neighbour.  Either way a fixed summation order without atomics.
 constexpr int kSaGL = 8;
+constexpr int kSaApG = 2;
 constexpr int kSaApSm = 64;  // longest row summed in shared memory
-// dynamic shared memory: per group of kSaGL lanes 4 * ms sums and ms columns (ms = 0: none)
+// dynamic shared memory: per fine node kSaApG copies of 4 * ms sums and ms columns (ms = 0: none)
 template <typename ST>
-size_t sa_ap_smem(int ms) { return (size_t)(128 / kSaGL) * ms * (4 * sizeof(ST) + sizeof(int)); }
+size_t sa_ap_smem(int ms) { return (size_t)(128 / kSaGL) * ms * (kSaApG * 4 * sizeof(ST) + sizeof(int)); }
 template <typename KT, typename ST>
 __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, const int* dof_off, const int* node_off,
                                                const int* rowptr, const int* colind, const KT* A,
@@ -1058,8 +1066,9 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
                                                const int* apnnz, const int* apoff, ST* AP, const int* sel, int ms) {
   extern __shared__ __align__(16) unsigned char sa_smem[];
   const int gi = threadIdx.x / kSaGL;
-  ST* g_acc = reinterpret_cast<ST*>(sa_smem) + (size_t)gi * 4 * ms;
-  int* g_col = reinterpret_cast<int*>(reinterpret_cast<ST*>(sa_smem) + (size_t)(128 / kSaGL) * 4 * ms) + gi * ms;
+  ST* g_acc = reinterpret_cast<ST*>(sa_smem) + (size_t)gi * kSaApG * 4 * ms;
+  int* g_col = reinterpret_cast<int*>(reinterpret_cast<ST*>(sa_smem) + (size_t)(128 / kSaGL) * kSaApG * 4 * ms) +
+               gi * ms;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) / kSaGL, lane = threadIdx.x % kSaGL;
   if (g >= nfn) return;  // whole groups leave together
   const unsigned gmask = ((1u << kSaGL) - 1u) << ((threadIdx.x & 31) & ~(kSaGL - 1));
@@ -1070,49 +1079,76 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
   const int ar = apn_ptr[g], dA = apn_ptr[g + 1] - ar;
   const size_t ars = (size_t)2 * apnnz[s];  // AP row stride between c = 0 and c = 1
   ST* r0 = AP + apoff[s] + 2 * (size_t)(ar - apbase[s]);
-  const bool sm = dA <= ms;  // uniform over the group
-  ST* o0 = sm ? g_acc : r0;
-  const size_t o1 = sm ? (size_t)2 * dA : ars;  // offset of row c = 1
+  const bool sm = ms > 0;  // every row of the launch fits (ms is the level's longest row)
+  const int ng = sm ? kSaApG : 1, gw = kSaGL / ng;  // lane groups, lanes per group
+  const int q = lane / gw, ql = lane % gw;
+  ST* o0 = sm ? g_acc + (size_t)q * 4 * dA : r0;  // this group's copy
+  const size_t o1 = sm ? (size_t)2 * dA : ars;   // offset of row c = 1
   const int* acol = apn_col + ar;
   if (sm) {
     for (int t = lane; t < dA; t += kSaGL) g_col[t] = acol[t];
     acol = g_col;
   }
-  for (int t = lane; t < 2 * dA; t += kSaGL) {
-    o0[t] = 0;
-    o0[o1 + t] = 0;
+  for (int t = lane; t < (sm ? kSaApG * 4 * dA : 2 * dA); t += kSaGL) {
+    if (sm) g_acc[t] = 0;
+    else { r0[t] = 0; r0[ars + t] = 0; }
   }
   const bool m0 = mask && mask[i0], m1 = mask && mask[i1];
   if (!(m0 && m1)) {
     const int q0 = rowptr[i0], q1 = rowptr[i1], deg = (rowptr[i0 + 1] - q0) >> 1;
     const size_t prs = (size_t)2 * pnnz[s];  // P row stride between c2 = 0 and c2 = 1
-    for (int k = 0; k < deg; ++k) {
-      const int ju = colind[q0 + k], jv = ju + nn;  // u and v dofs of neighbour node h
-      const bool cu = mask && mask[ju], cv = mask && mask[jv];
-      const ST a00 = (m0 || cu) ? ST(0) : (ST)A[q0 + k], a01 = (m0 || cv) ? ST(0) : (ST)A[q0 + deg + k];
-      const ST a10 = (m1 || cu) ? ST(0) : (ST)A[q1 + k], a11 = (m1 || cv) ? ST(0) : (ST)A[q1 + deg + k];
-      if (a00 == ST(0) && a01 == ST(0) && a10 == ST(0) && a11 == ST(0)) continue;  // uniform over the group
-      const int h = no + (ju - d0);
-      const int pj = pn_ptr[h], dPj = pn_ptr[h + 1] - pj;
-      const ST* ph = P + poff[s] + 2 * (size_t)(pj - pbase[s]);
-      __syncwarp(gmask);  // the previous neighbour's updates (and the zeroed rows) are visible to the group
-      for (int t = lane; t < dPj; t += kSaGL) {
-        const int kk = sa_find(acol, dA, pn_col[pj + t]);
-        if (kk < 0) continue;
-#pragma unroll
-        for (int c3 = 0; c3 < 2; ++c3) {
-          const ST p0 = ph[c3 * dPj + t], p1 = ph[prs + c3 * dPj + t];
-          o0[c3 * dA + kk] += a00 * p0 + a01 * p1;
-          o0[o1 + c3 * dA + kk] += a10 * p0 + a11 * p1;
+    const ST* Ps = P + poff[s];
+    const int pb = pbase[s];
+    for (int k0 = 0; k0 < deg; k0 += kSaGL) {
+      // lane k loads neighbour k0 + k
+      ST b00 = 0, b01 = 0, b10 = 0, b11 = 0;
+      int bpj = 0, bdP = 0;
+      if (k0 + lane < deg) {
+        const int k = k0 + lane;
+        const int ju = colind[q0 + k], jv = ju + nn;  // u and v dofs of neighbour node h
+        const bool cu = mask && mask[ju], cv = mask && mask[jv];
+        b00 = (m0 || cu) ? ST(0) : (ST)A[q0 + k];
+        b01 = (m0 || cv) ? ST(0) : (ST)A[q0 + deg + k];
+        b10 = (m1 || cu) ? ST(0) : (ST)A[q1 + k];
+        b11 = (m1 || cv) ? ST(0) : (ST)A[q1 + deg + k];
+        const int h = no + (ju - d0);
+        bpj = pn_ptr[h];
+        bdP = pn_ptr[h + 1] - bpj;
+      }
+      const int nk = min(kSaGL, deg - k0);
+      for (int e0 = 0; e0 < nk; e0 += ng) {
+        const int e = e0 + q;  // this group's neighbour (lanes past nk read zeros)
+        const ST a00 = __shfl_sync(gmask, b00, e, kSaGL), a01 = __shfl_sync(gmask, b01, e, kSaGL);
+        const ST a10 = __shfl_sync(gmask, b10, e, kSaGL), a11 = __shfl_sync(gmask, b11, e, kSaGL);
+        const int pj = __shfl_sync(gmask, bpj, e, kSaGL), dPj = __shfl_sync(gmask, bdP, e, kSaGL);
+        __syncwarp(gmask);  // the previous neighbours' updates (and the zeroed rows) are visible
+        if (e >= nk || (a00 == ST(0) && a01 == ST(0) && a10 == ST(0) && a11 == ST(0))) continue;
+        const ST* ph = Ps + 2 * (size_t)(pj - pb);
+        for (int t = ql; t < dPj; t += gw) {
+          // the P entries load beside the column, ahead of the search
+          const int colp = pn_col[pj + t];
+          const ST p00 = ph[t], p01 = ph[dPj + t], p10 = ph[prs + t], p11 = ph[prs + dPj + t];
+          const int kk = sa_find(acol, dA, colp);
+          if (kk < 0) continue;
+          o0[kk] += a00 * p00 + a01 * p10;
+          o0[dA + kk] += a00 * p01 + a01 * p11;
+          o0[o1 + kk] += a10 * p00 + a11 * p10;
+          o0[o1 + dA + kk] += a10 * p01 + a11 * p11;
         }
       }
     }
   }
-  if (sm) {  // one write of the two rows
+  if (sm) {  // one write of the two rows, the group copies added in order
     __syncwarp(gmask);
     for (int t = lane; t < 2 * dA; t += kSaGL) {
-      r0[t] = o0[t];
-      r0[ars + t] = o0[o1 + t];
+      ST v0 = g_acc[t], v1 = g_acc[2 * dA + t];
+#pragma unroll
+      for (int c = 1; c < kSaApG; ++c) {
+        v0 += g_acc[(size_t)c * 4 * dA + t];
+        v1 += g_acc[(size_t)c * 4 * dA + 2 * dA + t];
+      }
+      r0[t] = v0;
+      r0[ars + t] = v1;
     }
   }
 }
@@ -1144,11 +1180,15 @@ __global__ void k_sa_PT(int nc, const int* cdof_sys, const int* cdof_off, const 
 
 // coarse operator rows: Ac((c2,J),:) = sum over P'((c2,J), (c,g)) AP((c,g),:), into the coarse
 // level's CSR.  One warp per coarse node J: its two rows share the column list (sorted, in
-// shared memory with the four blocks of FP64 sums) and the fine nodes g of P'(J,:).  The
-// lanes first load the fine-node data of 32 list entries; then the entries go in order, and
-// for each the lanes take the entries of AP(g,:), whose columns are distinct, so the targets
-// are distinct: a fixed summation order without atomics.
+// shared memory) and the fine nodes g of P'(J,:).  The lanes first load the fine-node data of 32
+// list entries.  The warp is split into kSaAcG groups of kSaAcW lanes: group q takes the entries
+// q, q + kSaAcG, ... in order, its lanes the entries of AP(g,:), whose columns are distinct, and
+// sums into the group's own copy of the four FP64 blocks; the copies are added in group order at
+// the end.  A fixed summation order without atomics.
 constexpr int kSaAcWarps = 4;
+constexpr int kSaAcG = 4, kSaAcW = 32 / kSaAcG;
+// dynamic shared memory of a CTA for coarse rows of at most md nodes
+inline size_t sa_ac_smem(int md) { return (size_t)kSaAcWarps * md * (kSaAcG * 4 * sizeof(double) + sizeof(int)); }
 template <typename KT, typename ST>
 __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* cnode_sys, const int* cdof_off,
                                                            const int* cnode_off, const int* crowptr,
@@ -1156,9 +1196,9 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
                                                            const int* ptn_fine, const int* ptbase, const int* pnnz,
                                                            const int* poff, const ST* PT, const int* apn_ptr,
                                                            const int* apn_col, const int* apbase, const int* apnnz,
-                                                           const int* apoff, const ST* AP, KT* Ac, const int* sel) {
-  __shared__ int s_col[kSaAcWarps][kSaMaxDeg];
-  __shared__ double s_acc[kSaAcWarps][4 * kSaMaxDeg];
+                                                           const int* apoff, const ST* AP, KT* Ac, const int* sel,
+                                                           int md) {
+  extern __shared__ __align__(16) unsigned char sa_smem[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int J = blockIdx.x * kSaAcWarps + wid;
   if (J >= ncn) return;  // whole warps leave together
@@ -1166,17 +1206,16 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
   if (sel && !sel[s]) return;  // whole warps
   const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno;
   const int R0 = cdof_off[s] + (J - cno), R1 = R0 + cnn;
-  const int cr0 = crowptr[R0], cr1 = crowptr[R1], degc = min((crowptr[R0 + 1] - cr0) >> 1, kSaMaxDeg);
+  const int cr0 = crowptr[R0], cr1 = crowptr[R1], degc = min((crowptr[R0 + 1] - cr0) >> 1, md);
   const int cbase = cdof_off[s] - cno;  // u-column dof of coarse node K: cbase + K
-  int* col = s_col[wid];
-  double* acc = s_acc[wid];  // block (c2, c3) at (2 c2 + c3) degc
-  for (int t = lane; t < degc; t += 32) {
-    col[t] = ccolind[cr0 + t] - cbase;
-    acc[t] = 0;
-    acc[degc + t] = 0;
-    acc[2 * degc + t] = 0;
-    acc[3 * degc + t] = 0;
-  }
+  double* acc = reinterpret_cast<double*>(sa_smem) + (size_t)wid * kSaAcG * 4 * md;
+  int* col = reinterpret_cast<int*>(reinterpret_cast<double*>(sa_smem) + (size_t)kSaAcWarps * kSaAcG * 4 * md) +
+             wid * md;
+  // copy q, block (c2, c3) at acc[(4 q + 2 c2 + c3) degc + pos]
+  for (int t = lane; t < kSaAcG * 4 * degc; t += 32) acc[t] = 0;
+  for (int t = lane; t < degc; t += 32) col[t] = ccolind[cr0 + t] - cbase;
+  const int q = lane / kSaAcW, ql = lane % kSaAcW;
+  double* ga = acc + (size_t)q * 4 * degc;
   const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
   const size_t prs = (size_t)2 * pnnz[s], ars = (size_t)2 * apnnz[s];
   const ST* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);  // P'((c2,J),(c,u)) = t0[c2 prs + c dT + u]
@@ -1196,28 +1235,37 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
       w11 = t0[prs + dT + my];
     }
     const int nstep = min(32, dT - u0);
-    for (int e = 0; e < nstep; ++e) {
+    for (int e0 = 0; e0 < nstep; e0 += kSaAcG) {
+      const int e = e0 + q;  // this group's entry (lanes past nstep hold dA = 0)
       const int ar = __shfl_sync(0xffffffffu, g_ar, e), dA = __shfl_sync(0xffffffffu, g_dA, e);
       const double v00 = __shfl_sync(0xffffffffu, w00, e), v01 = __shfl_sync(0xffffffffu, w01, e);
       const double v10 = __shfl_sync(0xffffffffu, w10, e), v11 = __shfl_sync(0xffffffffu, w11, e);
       const ST* a0 = apb + 2 * (size_t)(ar - apb0);  // AP((c,g),(c3,kk)) = a0[c ars + c3 dA + kk]
-      __syncwarp();  // the previous entry's sums are visible to the warp
-      for (int kk = lane; kk < dA; kk += 32) {
-        const int pos = sa_find(col, degc, apn_col[ar + kk]);
-        if (pos < 0) continue;
+      __syncwarp();  // the previous entries' sums (and the zeroed copies) are visible to the warp
+      for (int kk = ql; kk < dA; kk += kSaAcW) {
+        // the AP entries load beside the column, ahead of the search
+        const int cK = apn_col[ar + kk];
         const double x00 = (double)a0[kk], x01 = (double)a0[dA + kk], x10 = (double)a0[ars + kk],
                      x11 = (double)a0[ars + dA + kk];
-        acc[pos] += v00 * x00 + v01 * x10;
-        acc[degc + pos] += v00 * x01 + v01 * x11;
-        acc[2 * degc + pos] += v10 * x00 + v11 * x10;
-        acc[3 * degc + pos] += v10 * x01 + v11 * x11;
+        const int pos = sa_find(col, degc, cK);
+        if (pos < 0) continue;
+        ga[pos] += v00 * x00 + v01 * x10;
+        ga[degc + pos] += v00 * x01 + v01 * x11;
+        ga[2 * degc + pos] += v10 * x00 + v11 * x10;
+        ga[3 * degc + pos] += v10 * x01 + v11 * x11;
       }
     }
   }
   __syncwarp();
   for (int t = lane; t < 2 * degc; t += 32) {
-    Ac[cr0 + t] = (KT)acc[t];
-    Ac[cr1 + t] = (KT)acc[2 * degc + t];
+    double a0 = acc[t], a1 = acc[2 * degc + t];
+#pragma unroll
+    for (int c = 1; c < kSaAcG; ++c) {
+      a0 += acc[(size_t)c * 4 * degc + t];
+      a1 += acc[(size_t)c * 4 * degc + 2 * degc + t];
+    }
+    Ac[cr0 + t] = (KT)a0;
+    Ac[cr1 + t] = (KT)a1;
   }
 }
 
@@ -1357,9 +1405,10 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
                                        F.ptbase, F.pn_ptr, F.pbase, F.pnnz, F.poff, Pv, PTv,
                                        sizeof(KT) == 4 ? nullptr : F.sa_plo, sizeof(KT) == 4 ? nullptr : F.sa_ptlo,
                                        psel), ++*launches;
-      k_sa_Ac<KT, ST><<<(C.nn + kSaAcWarps - 1) / kSaAcWarps, 32 * kSaAcWarps, 0, st>>>(C.nn, C.node_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr,
-                                       F.ptn_fine, F.ptbase, F.pnnz, F.poff, PTv, F.apn_ptr, F.apn_col, F.apbase,
-                                       F.apnnz, F.apoff, APv, (KT*)C.A, sel), ++*launches;
+      k_sa_Ac<KT, ST><<<(C.nn + kSaAcWarps - 1) / kSaAcWarps, 32 * kSaAcWarps, sa_ac_smem(F.ac_maxdeg), st>>>(
+          C.nn, C.node_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr, F.ptn_fine, F.ptbase, F.pnnz,
+          F.poff, PTv, F.apn_ptr, F.apn_col, F.apbase, F.apnnz, F.apoff, APv, (KT*)C.A, sel, F.ac_maxdeg),
+          ++*launches;
     }
     l1(a->nlev - 1);
   } else {
@@ -1550,6 +1599,19 @@ int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* 
     UA_CUDA_TRY(cudaFuncSetAttribute(k_amg_dense_inverse<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   else
     UA_CUDA_TRY(cudaFuncSetAttribute(k_amg_dense_inverse<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  if (a->sa) {  // the set-up's shared-memory rows, sized by the hierarchy's longest ones
+    int smd = 0;
+    for (int l = 0; l + 1 < a->nlev; ++l) smd = std::max(smd, a->lev[l].ac_maxdeg);
+    const int sac = (int)sa_ac_smem(smd);
+    const int sap = fp32 ? (int)sa_ap_smem<float>(kSaApSm) : (int)sa_ap_smem<double>(kSaApSm);
+    if (fp32) {
+      UA_CUDA_TRY(cudaFuncSetAttribute(k_sa_Ac<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sac));
+      UA_CUDA_TRY(cudaFuncSetAttribute(k_sa_AP<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sap));
+    } else {
+      UA_CUDA_TRY(cudaFuncSetAttribute(k_sa_Ac<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sac));
+      UA_CUDA_TRY(cudaFuncSetAttribute(k_sa_AP<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sap));
+    }
+  }
   auto run = [&](long long* l) {
     return fp32 ? numeric_t<float, float>(m, rowptr0, colind0, (const float*)K0, cmask, sel, psel, l)
                 : numeric_t<double, double>(m, rowptr0, colind0, (const double*)K0, cmask, sel, psel, l);

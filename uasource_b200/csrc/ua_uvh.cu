@@ -39,8 +39,8 @@ __device__ __forceinline__ double supg_tau(const UvhPhys& P, double v, double l,
   return P.tau_mult * tau;
 }
 
-// GEN: any sliding law and the melange terms; else Weertman (the general code stays out of the
-// Weertman build)
+// GEN: any sliding law and the melange terms (Weertman chosen at run time); else Weertman only
+// (the general code stays out of that build)
 template <int NOD, bool WITHK, typename KT, bool GEN>
 __global__ void __launch_bounds__(NOD == 3 ? 512 : 320) uvh_patch_kernel(DevMesh M, QuadTable Q, UvhPhys P,
                                                                           UvhIn in, UvOut out) {
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(NOD == 3 ? 512 : 320) uvh_patch_kernel(DevMesh
       double eta, Ev;
       effective_viscosity(P.uv, Aint, nint, exx, eyy, exy, eta, Ev, cube);  // :149
       Drag d;  // :150
-      if (!GEN) {
+      if (!GEN || (P.uv.law == UA_SLIDING_WEERTMAN && !P.uv.melange)) {
         d = basal_drag_weertman(P.uv, Heint, deltaint, uint, vint, Cint, mint, cube);
       } else {
         int gn[NOD];
@@ -349,8 +349,12 @@ template <int NOD, bool WITHK, typename KT>
 static cudaError_t launch_t(const ua_mesh* m, const UvhPhys& P, const UvhIn& in, const UvOut& out) {
   const int E = m->dm.max_patch_elems;
   size_t sm = uvh_patch_smem(NOD, WITHK, sizeof(KT) == 4, E);
-  const bool gen = P.uv.law != UA_SLIDING_WEERTMAN || P.uv.melange;
-  auto kern = gen ? uvh_patch_kernel<NOD, WITHK, KT, true> : uvh_patch_kernel<NOD, WITHK, KT, false>;
+  // the residual-only pass keeps the general build: without the tangent its Weertman-only build
+  // spills more registers than the general one
+  auto kern = uvh_patch_kernel<NOD, WITHK, KT, true>;
+  if constexpr (WITHK) {
+    if (P.uv.law == UA_SLIDING_WEERTMAN && !P.uv.melange) kern = uvh_patch_kernel<NOD, WITHK, KT, false>;
+  }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   int threads = ((E * NOD + 31) / 32) * 32;
