@@ -78,10 +78,13 @@ struct AmgLevel {
   // apn: fine node -> coarse nodes of A P; ptn: coarse node -> (fine node, position in pn)
   int *sa_agg = nullptr, *pn_ptr = nullptr, *pn_col = nullptr, *apn_ptr = nullptr, *apn_col = nullptr;
   int *ptn_ptr = nullptr, *ptn_fine = nullptr, *ptn_k = nullptr;
-  int *pbase = nullptr, *pnnz = nullptr, *poff = nullptr, *apbase = nullptr, *apnnz = nullptr, *apoff = nullptr,
-      *ptbase = nullptr;
-  double *sa_p = nullptr, *sa_pt = nullptr, *sa_ap = nullptr;  // values: 4 per node-level entry
-  float *sa_plo = nullptr, *sa_ptlo = nullptr;  // FP32 copies of P and P' for the mixed-precision transfers
+  int *pbase = nullptr, *pnnz = nullptr, *poff = nullptr, *apbase = nullptr, *apnnz = nullptr, *apoff = nullptr;
+  double *sa_p = nullptr, *sa_ap = nullptr;  // set-up values (FP64 form): 4 per node-level entry
+  float* sa_plo = nullptr;                   // set-up values of P (mixed form)
+  // P in the transfer layout, one quad per node-level entry: pn order (sa_q*) and ptn order
+  // (sa_qt*); BF16 quads for the mixed form, FP64 quads for the FP64 form (allocated on first use)
+  long long np = 0;  // node-level prolongator entries of the level (all systems)
+  void *sa_qh = nullptr, *sa_qth = nullptr, *sa_qd = nullptr, *sa_qtd = nullptr;
 };
 
 // one active-block list to compact: blocks blk_off[s] .. blk_off[s+1] of every system s with
@@ -124,6 +127,9 @@ struct Sell {
 struct Amg {
   int nsys = 0, nlev = 0, maxdn = 0;
   Sell sell;
+  // node slices of the coarse levels 1 .. nlev-2 (smoothed hierarchies): BF16 copies of the
+  // coarse operators for the mixed-precision V-cycle's residual and smoothing there
+  std::vector<Sell> csell;
   // active-block lists: rows[l] (level-l row blocks, depth > l; level 0 = the handle's blocks),
   // fnodes[l] (level-l node blocks, depth > l), cnodes[l] (level-(l+1) node blocks, depth > l)
   bool act_ready = false;
@@ -482,8 +488,7 @@ static int amg_build(ua_mesh* m, bool smoothed) {
       F.ptn_ptr = upload(m, a, g_ptnp[l], ok);
       F.ptn_fine = upload(m, a, g_ptnf[l], ok);
       F.ptn_k = upload(m, a, g_ptnk[l], ok);
-      std::vector<int> pbase(nsys), pnnz(nsys), poff(nsys + 1, 0), apbase(nsys), apnnz(nsys), apoff(nsys + 1, 0),
-          ptbase(nsys);
+      std::vector<int> pbase(nsys), pnnz(nsys), poff(nsys + 1, 0), apbase(nsys), apnnz(nsys), apoff(nsys + 1, 0);
       for (int s = 0; s < nsys; ++s) {
         pbase[s] = g_pnp[l][F.node_off[s]];
         pnnz[s] = g_pnp[l][F.node_off[s + 1]] - pbase[s];
@@ -491,11 +496,9 @@ static int amg_build(ua_mesh* m, bool smoothed) {
         apbase[s] = g_apnp[l][F.node_off[s]];
         apnnz[s] = g_apnp[l][F.node_off[s + 1]] - apbase[s];
         apoff[s + 1] = apoff[s] + 4 * apnnz[s];
-        ptbase[s] = g_ptnp[l][C.node_off[s]];
       }
       F.pbase = upload(m, a, pbase, ok); F.pnnz = upload(m, a, pnnz, ok); F.poff = upload(m, a, poff, ok);
       F.apbase = upload(m, a, apbase, ok); F.apnnz = upload(m, a, apnnz, ok); F.apoff = upload(m, a, apoff, ok);
-      F.ptbase = upload(m, a, ptbase, ok);
       F.ap_maxrow = 0;
       for (size_t i = 0; i + 1 < g_apnp[l].size(); ++i)
         F.ap_maxrow = std::max(F.ap_maxrow, g_apnp[l][i + 1] - g_apnp[l][i]);
@@ -503,10 +506,9 @@ static int amg_build(ua_mesh* m, bool smoothed) {
       for (size_t I = 0; I + 1 < g_ptr[l + 1].size(); ++I)
         F.ac_maxdeg = std::max(F.ac_maxdeg, g_ptr[l + 1][I + 1] - g_ptr[l + 1][I]);
       F.sa_p = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
-      F.sa_pt = (double*)dalloc(m, a, sizeof(double) * (size_t)poff[nsys], ok);
+      F.np = g_pnp[l].back();
       F.sa_ap = (double*)dalloc(m, a, sizeof(double) * (size_t)apoff[nsys], ok);
       F.sa_plo = (float*)dalloc(m, a, sizeof(float) * (size_t)poff[nsys], ok);
-      F.sa_ptlo = (float*)dalloc(m, a, sizeof(float) * (size_t)poff[nsys], ok);
     }
     pb[l] = a->lev[l].b;
     px2[l] = a->lev[l].x2;
@@ -837,8 +839,9 @@ struct SellDev {
   const int *sb_sys, *sb_n0, *sb_cnt, *sb_rbu, *sb_rbv, *perm;
   const long long* sl_off;
   const int* cols;
-  const int *dof_off, *node_off;  // per system
+  const int *dof_off, *node_off;  // per system, of the slices' level
   unsigned long long* dbg;        // first bounds violation (debug build)
+  int lev;                        // the level (residual and smoothing: systems deeper than it)
 };
 
 // The four values of a slot (blocks uu, uv, vu, vv) are adjacent, so a lane reads them with one
@@ -904,6 +907,45 @@ __global__ void __launch_bounds__(256) k_sell_fill(SellDev S, const DevMesh dm, 
   }
 }
 
+// Coarse-level slice values (and, once, the columns) from the level's CSR: row (c, I) holds the
+// u block then the v block of deg(I) entries.  Same slice layout as the finest level.
+template <typename KT>
+__global__ void __launch_bounds__(256) k_csell_fill(SellDev S, const int* rowptr, const int* colind, const KT* A,
+                                                    __nv_bfloat16* vlo, int* cols, const int* sel) {
+  const int sb = blockIdx.x;
+  const int w = threadIdx.x >> 5, t = threadIdx.x & 31, pos = w * 32 + t;
+  const int sl = sb * kSellSlices + w;
+  const long long o0 = S.sl_off[sl];
+  const int W = (int)((S.sl_off[sl + 1] - o0) >> 5);
+  if (W == 0) return;  // empty slice (warp-uniform)
+  const int s = S.sb_sys[sb];
+  if (sel && A && !sel[s]) return;  // values of the systems of this Newton step only
+  const int no = S.node_off[s], nn = S.node_off[s + 1] - no, d0 = S.dof_off[s];
+  const bool has = pos < S.sb_cnt[sb];
+  int R0 = d0, q0 = 0, q1 = 0, deg = 0;
+  if (has) {
+    R0 = d0 + (S.perm[S.sb_n0[sb] + pos] - no);
+    q0 = rowptr[R0];
+    q1 = rowptr[R0 + nn];
+    deg = (rowptr[R0 + 1] - q0) >> 1;
+  }
+  for (int k = 0; k < W; ++k) {
+    const bool in = has && k < deg;
+    const long long d = o0 + 32LL * k + t;
+    if (cols) cols[d] = in ? colind[q0 + k] : R0;
+    if (!A) continue;
+    float e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+    if (in) {
+      e0 = (float)A[q0 + k];
+      e1 = (float)A[q0 + deg + k];
+      e2 = (float)A[q1 + k];
+      e3 = (float)A[q1 + deg + k];
+    }
+    vlo[4 * d] = __float2bfloat16_rn(e0); vlo[4 * d + 1] = __float2bfloat16_rn(e1);
+    vlo[4 * d + 2] = __float2bfloat16_rn(e2); vlo[4 * d + 3] = __float2bfloat16_rn(e3);
+  }
+}
+
 // Finest-level row products over the node slices, both rows (u, v) of a node per thread.
 //   MODE 0 (PCG SpMV):    out = mask(K x); partial x.out
 //   MODE 1 (AMG residual): out = mask(b - K x)                 (systems deeper than level 0)
@@ -922,7 +964,7 @@ __global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 6 : 0) k_sell(SellDev S
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
     const int sb = act.map ? act.map[vb] : vb;
     const int s = S.sb_sys[sb];
-    const bool live = sel[s] && !done[s] && (MODE == 0 || depth[s] > 0);
+    const bool live = sel[s] && !done[s] && (MODE == 0 || depth[s] > S.lev);
     if (MODE == 1 && !live) continue;  // uniform over the block
     double pv = 0;
     if (live && pos < S.sb_cnt[sb]) {
@@ -1041,6 +1083,51 @@ __global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int
   }
 }
 
+// P in the transfer layout: per node-level entry (fine node g, coarse node K) one quad of
+// P((c,g),(c2,K)) in the order (c,c2) = (0,0), (0,1), (1,0), (1,1), read with one load.  The mixed
+// form keeps BF16 quads (its set-up then reads the same rounded values, so the coarse operator is
+// the Galerkin product of the prolongator the V-cycle applies), the FP64 form FP64 quads.
+struct alignas(8) PQuadH {
+  __nv_bfloat162 r0, r1;
+};
+struct alignas(16) PQuadD {
+  double2 r0, r1;
+};
+template <typename VT>
+struct PQuadOf {
+  using T = PQuadD;
+};
+template <>
+struct PQuadOf<float> {
+  using T = PQuadH;
+};
+__device__ __forceinline__ void pq_get(const PQuadH* q, double (&v)[4]) {
+  const uint2 u = __ldg(reinterpret_cast<const uint2*>(q));
+  const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+  const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void pq_get(const PQuadH* q, float (&v)[4]) {
+  const uint2 u = __ldg(reinterpret_cast<const uint2*>(q));
+  const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+  const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void pq_get(const PQuadD* q, double (&v)[4]) {
+  const double2 a = __ldg(&q->r0), b = __ldg(&q->r1);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void pq_set(PQuadH* q, double v0, double v1, double v2, double v3) {
+  PQuadH h;
+  h.r0 = __floats2bfloat162_rn((float)v0, (float)v1);
+  h.r1 = __floats2bfloat162_rn((float)v2, (float)v3);
+  *q = h;
+}
+__device__ __forceinline__ void pq_set(PQuadD* q, double v0, double v1, double v2, double v3) {
+  q->r0 = make_double2(v0, v1);
+  q->r1 = make_double2(v2, v3);
+}
+
 // A P rows: AP(i,:) = sum over unmasked columns j of A(i,j) P(j,:), kSaGL lanes per fine node g.
 // Both rows (c = 0, 1) of the node share its neighbour list, so each neighbour h contributes
 // A((c,g),(c2,h)) P((c2,h),:) to four output blocks (c, c3) at once.  The lanes first load the
@@ -1061,9 +1148,9 @@ template <typename KT, typename ST>
 __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, const int* dof_off, const int* node_off,
                                                const int* rowptr, const int* colind, const KT* A,
                                                const unsigned char* mask, const int* pn_ptr, const int* pn_col,
-                                               const int* pbase, const int* pnnz, const int* poff, const ST* P,
-                                               const int* apn_ptr, const int* apn_col, const int* apbase,
-                                               const int* apnnz, const int* apoff, ST* AP, const int* sel, int ms) {
+                                               const typename PQuadOf<KT>::T* Q, const int* apn_ptr,
+                                               const int* apn_col, const int* apbase, const int* apnnz,
+                                               const int* apoff, ST* AP, const int* sel, int ms) {
   extern __shared__ __align__(16) unsigned char sa_smem[];
   const int gi = threadIdx.x / kSaGL;
   ST* g_acc = reinterpret_cast<ST*>(sa_smem) + (size_t)gi * kSaApG * 4 * ms;
@@ -1096,9 +1183,6 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
   const bool m0 = mask && mask[i0], m1 = mask && mask[i1];
   if (!(m0 && m1)) {
     const int q0 = rowptr[i0], q1 = rowptr[i1], deg = (rowptr[i0 + 1] - q0) >> 1;
-    const size_t prs = (size_t)2 * pnnz[s];  // P row stride between c2 = 0 and c2 = 1
-    const ST* Ps = P + poff[s];
-    const int pb = pbase[s];
     for (int k0 = 0; k0 < deg; k0 += kSaGL) {
       // lane k loads neighbour k0 + k
       ST b00 = 0, b01 = 0, b10 = 0, b11 = 0;
@@ -1123,11 +1207,12 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
         const int pj = __shfl_sync(gmask, bpj, e, kSaGL), dPj = __shfl_sync(gmask, bdP, e, kSaGL);
         __syncwarp(gmask);  // the previous neighbours' updates (and the zeroed rows) are visible
         if (e >= nk || (a00 == ST(0) && a01 == ST(0) && a10 == ST(0) && a11 == ST(0))) continue;
-        const ST* ph = Ps + 2 * (size_t)(pj - pb);
         for (int t = ql; t < dPj; t += gw) {
           // the P entries load beside the column, ahead of the search
           const int colp = pn_col[pj + t];
-          const ST p00 = ph[t], p01 = ph[dPj + t], p10 = ph[prs + t], p11 = ph[prs + dPj + t];
+          double pq[4];
+          pq_get(Q + pj + t, pq);
+          const ST p00 = (ST)pq[0], p01 = (ST)pq[1], p10 = (ST)pq[2], p11 = (ST)pq[3];
           const int kk = sa_find(acol, dA, colp);
           if (kk < 0) continue;
           o0[kk] += a00 * p00 + a01 * p10;
@@ -1153,29 +1238,30 @@ __global__ void __launch_bounds__(128) k_sa_AP(int nfn, const int* node_sys, con
   }
 }
 
-// transpose values: P'(R = (c2, J), (c, u)) = P((c, fine node u of J), (c2, J)), and FP32 copies
-// of both (every P entry is the image of exactly one P' entry)
-template <typename ST>
-__global__ void k_sa_PT(int nc, const int* cdof_sys, const int* cdof_off, const int* cnode_off, const int* ptn_ptr,
-                        const int* ptn_fine, const int* ptn_k, const int* ptbase, const int* pn_ptr,
-                        const int* pbase, const int* pnnz, const int* poff, const ST* P, ST* PT, float* Plo,
-                        float* PTlo, const int* sel) {
-  const int R = blockIdx.x * blockDim.x + threadIdx.x;
-  if (R >= nc) return;
-  int s, c2, J;
-  sa_decode(R, cdof_sys, cdof_off, cnode_off, s, c2, J);
+// quads of the prolongator rows of fine node g (pn order): thread per fine node
+template <typename ST, typename QT>
+__global__ void k_sa_quads(int nfn, const int* node_sys, const int* pn_ptr, const int* pbase, const int* pnnz,
+                           const int* poff, const ST* P, QT* Q, const int* sel) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nfn) return;
+  const int s = node_sys[g];
   if (sel && !sel[s]) return;
-  const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
-  const size_t t0 = poff[s] + (size_t)c2 * 2 * pnnz[s] + 2 * (size_t)(tr - ptbase[s]);
-  for (int c = 0; c < 2; ++c)
-    for (int u = 0; u < dT; ++u) {
-      const int g = ptn_fine[tr + u], pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
-      const size_t pi = poff[s] + (size_t)c * 2 * pnnz[s] + 2 * (size_t)(pr - pbase[s]) + c2 * dP + ptn_k[tr + u];
-      const ST v = P[pi];
-      PT[t0 + c * dT + u] = v;
-      if (PTlo) PTlo[t0 + c * dT + u] = (float)v;  // FP32 copies for the transfers of a FP64 set-up
-      if (Plo) Plo[pi] = (float)v;
-    }
+  const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
+  const size_t prs = (size_t)2 * pnnz[s];  // row c = 1 after row c = 0
+  const ST* p0 = P + poff[s] + 2 * (size_t)(pr - pbase[s]);  // row c: [c2 = 0 (dP)][c2 = 1 (dP)]
+  for (int k = 0; k < dP; ++k)
+    pq_set(Q + pr + k, (double)p0[k], (double)p0[dP + k], (double)p0[prs + k], (double)p0[prs + dP + k]);
+}
+
+// the same quads in ptn order (coarse node J, its fine nodes u): thread per coarse node; every
+// P entry is the image of exactly one ptn entry
+template <typename QT>
+__global__ void k_sa_qt(int ncn, const int* cnode_sys, const int* ptn_ptr, const int* ptn_fine, const int* ptn_k,
+                        const int* pn_ptr, const QT* Q, QT* QTr, const int* sel) {
+  const int J = blockIdx.x * blockDim.x + threadIdx.x;
+  if (J >= ncn) return;
+  if (sel && !sel[cnode_sys[J]]) return;
+  for (int u = ptn_ptr[J]; u < ptn_ptr[J + 1]; ++u) QTr[u] = Q[pn_ptr[ptn_fine[u]] + ptn_k[u]];
 }
 
 // coarse operator rows: Ac((c2,J),:) = sum over P'((c2,J), (c,g)) AP((c,g),:), into the coarse
@@ -1193,8 +1279,8 @@ template <typename KT, typename ST>
 __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* cnode_sys, const int* cdof_off,
                                                            const int* cnode_off, const int* crowptr,
                                                            const int* ccolind, const int* ptn_ptr,
-                                                           const int* ptn_fine, const int* ptbase, const int* pnnz,
-                                                           const int* poff, const ST* PT, const int* apn_ptr,
+                                                           const int* ptn_fine, const typename PQuadOf<KT>::T* QTr,
+                                                           const int* apn_ptr,
                                                            const int* apn_col, const int* apbase, const int* apnnz,
                                                            const int* apoff, const ST* AP, KT* Ac, const int* sel,
                                                            int md) {
@@ -1217,8 +1303,7 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
   const int q = lane / kSaAcW, ql = lane % kSaAcW;
   double* ga = acc + (size_t)q * 4 * degc;
   const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
-  const size_t prs = (size_t)2 * pnnz[s], ars = (size_t)2 * apnnz[s];
-  const ST* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);  // P'((c2,J),(c,u)) = t0[c2 prs + c dT + u]
+  const size_t ars = (size_t)2 * apnnz[s];
   const ST* apb = AP + apoff[s];
   const int apb0 = apbase[s];
   for (int u0 = 0; u0 < dT; u0 += 32) {
@@ -1229,10 +1314,13 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
       const int g = ptn_fine[tr + my];
       g_ar = apn_ptr[g];
       g_dA = apn_ptr[g + 1] - g_ar;
-      w00 = t0[my];
-      w01 = t0[dT + my];
-      w10 = t0[prs + my];
-      w11 = t0[prs + dT + my];
+      // w(c2, c) = P'((c2,J),(c,g)) = P((c,g),(c2,J)), quad entry 2 c + c2
+      double pq[4];
+      pq_get(QTr + tr + my, pq);
+      w00 = pq[0];
+      w01 = pq[2];
+      w10 = pq[1];
+      w11 = pq[3];
     }
     const int nstep = min(32, dT - u0);
     for (int e0 = 0; e0 < nstep; e0 += kSaAcG) {
@@ -1269,56 +1357,83 @@ __global__ void __launch_bounds__(32 * kSaAcWarps) k_sa_Ac(int ncn, const int* c
   }
 }
 
+// The transfers are gather chains (list entry -> node block -> P list -> vector entries).  They
+// load what a node block needs (its system, its nodes' P lists) ahead of the system's flags, and
+// take the entries of a P list in chunks of kSaChunk (half that in FP64): the chunk's columns and
+// P quads load together, then its vector entries, then the sums in list order.
+constexpr int kSaChunk = 4;
+
 // restriction b_c = P' res (coarse pre-smoothing x_c = invd b_c unless lc is the system's coarsest),
 // kSaRL lanes per coarse node: both rows (c2 = 0, 1) of the node share the fine-node list and
-// the gathered residuals; a lane sum in a fixed order
+// the gathered residuals; a lane sum in a fixed order.  A CTA of 32 kSaRL threads takes one node
+// block (kAmgNB = 32 coarse nodes) per pass.
 constexpr int kSaRL = 8;
 template <typename VT>
-__global__ void __launch_bounds__(256) k_sa_restrict(const int* nb_start, const int* nb_sys, ActList act,
-                                                     const int* cdof_off, const int* cnode_off, const int* depth,
-                                                     int lc, const int* sel, const int* done, const int* ptn_ptr,
-                                                     const int* ptn_fine, const int* ptbase, const int* pnnz,
-                                                     const int* poff, const VT* PT, const int* fdof_off,
-                                                     const int* fnode_off, const VT* res, const VT* cinvd, VT* cb,
-                                                     VT* cx) {
-  const int sub = threadIdx.x / kSaRL, lane = threadIdx.x % kSaRL, nsub = blockDim.x / kSaRL;
+__global__ void __launch_bounds__(32 * kSaRL, 4) k_sa_restrict(const int* nb_start, const int* nb_sys, ActList act,
+                                                            const int* cdof_off, const int* cnode_off,
+                                                            const int* depth, int lc, const int* sel,
+                                                            const int* done, const int* ptn_ptr,
+                                                            const int* ptn_fine,
+                                                            const typename PQuadOf<VT>::T* QTr,
+                                                            const int* fdof_off, const int* fnode_off,
+                                                            const VT* res, const VT* cinvd, VT* cb, VT* cx) {
+  static_assert(kAmgNB == 32, "one coarse node per kSaRL-lane group of a 32 kSaRL-thread CTA");
+  constexpr int CH = sizeof(VT) == 4 ? kSaChunk : kSaChunk / 2;  // FP64 chunks held to the register budget
+  const int sub = threadIdx.x / kSaRL, lane = threadIdx.x % kSaRL;
   const int nv = act.cnt ? *act.cnt : gridDim.x;  // list entries, else one node block per CTA
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
     const int b = act.map ? act.map[vb] : vb;
     const int s = nb_sys[b];
+    const int J = nb_start[b] + sub;
+    const bool valid = J < nb_start[b + 1];
+    int tr = 0, t1 = 0;
+    if (valid) {  // ahead of the flags
+      tr = ptn_ptr[J];
+      t1 = ptn_ptr[J + 1];
+    }
     if (!sel[s] || done[s]) continue;  // uniform over the block
-    const int n0 = nb_start[b], n1 = nb_start[b + 1];
     const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno, cd = cdof_off[s];
-    const size_t rs = (size_t)2 * pnnz[s];  // P' row stride between c2 = 0 and c2 = 1
     const int fno = fnode_off[s], fnn = fnode_off[s + 1] - fno, fd = fdof_off[s];
     const bool presmooth = depth[s] > lc;
-    for (int J0 = n0; J0 < n1; J0 += nsub) {  // same trip count for every thread of the block
-      const int J = J0 + sub;
-      const bool valid = J < n1;
-      double a0 = 0, a1 = 0;
-      if (valid) {
-        const int tr = ptn_ptr[J], dT = ptn_ptr[J + 1] - tr;
-        const VT* t0 = PT + poff[s] + 2 * (size_t)(tr - ptbase[s]);
-        for (int u = lane; u < dT; u += kSaRL) {
-          const int f = fd + (ptn_fine[tr + u] - fno);
-          const double r0 = (double)res[f], r1 = (double)res[f + fnn];
-          a0 += (double)t0[u] * r0 + (double)t0[dT + u] * r1;
-          a1 += (double)t0[rs + u] * r0 + (double)t0[rs + dT + u] * r1;
-        }
-      }
+    double a0 = 0, a1 = 0;
+    for (int u0 = tr + lane; u0 < t1; u0 += kSaRL * CH) {
+      int f[CH];
+      VT q[CH][4];  // P((c,g),(c2,J)) at 2 c + c2 (BF16 quads widen exactly to FP32)
 #pragma unroll
-      for (int o = kSaRL / 2; o > 0; o >>= 1) {
-        a0 += __shfl_down_sync(0xffffffffu, a0, o, kSaRL);
-        a1 += __shfl_down_sync(0xffffffffu, a1, o, kSaRL);
-      }
-      if (valid && lane == 0) {
-        const int R0 = cd + (J - cno), R1 = R0 + cnn;
-        cb[R0] = (VT)a0;
-        cb[R1] = (VT)a1;
-        if (presmooth) {
-          cx[R0] = (VT)((double)cinvd[R0] * a0);
-          cx[R1] = (VT)((double)cinvd[R1] * a1);
+      for (int k = 0; k < CH; ++k) {
+        const int u = u0 + k * kSaRL;
+        f[k] = -1;
+        if (u < t1) {
+          f[k] = fd + (ptn_fine[u] - fno);
+          pq_get(QTr + u, q[k]);
         }
+      }
+      VT r0[CH], r1[CH];
+#pragma unroll
+      for (int k = 0; k < CH; ++k)
+        if (f[k] >= 0) {
+          r0[k] = res[f[k]];
+          r1[k] = res[f[k] + fnn];
+        }
+#pragma unroll
+      for (int k = 0; k < CH; ++k)
+        if (f[k] >= 0) {
+          a0 += (double)q[k][0] * (double)r0[k] + (double)q[k][2] * (double)r1[k];
+          a1 += (double)q[k][1] * (double)r0[k] + (double)q[k][3] * (double)r1[k];
+        }
+    }
+#pragma unroll
+    for (int o = kSaRL / 2; o > 0; o >>= 1) {
+      a0 += __shfl_down_sync(0xffffffffu, a0, o, kSaRL);
+      a1 += __shfl_down_sync(0xffffffffu, a1, o, kSaRL);
+    }
+    if (valid && lane == 0) {
+      const int R0 = cd + (J - cno), R1 = R0 + cnn;
+      cb[R0] = (VT)a0;
+      cb[R1] = (VT)a1;
+      if (presmooth) {
+        cx[R0] = (VT)((double)cinvd[R0] * a0);
+        cx[R1] = (VT)((double)cinvd[R1] * a1);
       }
     }
   }
@@ -1326,39 +1441,63 @@ __global__ void __launch_bounds__(256) k_sa_restrict(const int* nb_start, const 
 
 // prolongation x += P x_c on level l (systems deeper than l; masked rows have zero P rows),
 // one thread per fine node of a node block: both rows share the coarse-node list and the gathered x_c
-// (one warp per node block, kSaPW warps per CTA)
+// (one warp per node block of kAmgNB = 32 nodes, kSaPW warps per CTA)
 constexpr int kSaPW = 8;
 template <typename VT>
-__global__ void __launch_bounds__(32 * kSaPW) k_sa_prolong(int nnb, const int* nb_start, const int* nb_sys,
+__global__ void __launch_bounds__(32 * kSaPW, 4) k_sa_prolong(int nnb, const int* nb_start, const int* nb_sys,
                                                            ActList act, const int* dof_off, const int* node_off,
                                                            const int* depth, int l, const int* sel, const int* done,
-                                                           const int* pn_ptr, const int* pn_col, const int* pbase,
-                                                           const int* pnnz, const int* poff, const VT* P,
-                                                           const int* cdof_off, const int* cnode_off, const VT* xc,
+                                                           const int* pn_ptr, const int* pn_col,
+                                                           const typename PQuadOf<VT>::T* Q, const int* cdof_off,
+                                                           const int* cnode_off, const VT* xc,
                                                            VT* x) {
+  static_assert(kAmgNB == 32, "one fine node per lane");
+  constexpr int CH = sizeof(VT) == 4 ? kSaChunk : kSaChunk / 2;  // FP64 chunks held to the register budget
   const int nv = act.cnt ? *act.cnt : nnb;  // list entries, else every node block
   const int lane = threadIdx.x & 31;
   for (int vb = blockIdx.x * kSaPW + (threadIdx.x >> 5); vb < nv; vb += gridDim.x * kSaPW) {
     const int b = act.map ? act.map[vb] : vb;
     const int s = nb_sys[b];
+    const int g = nb_start[b] + lane;
+    const bool valid = g < nb_start[b + 1];
+    int pr = 0, pe = 0;
+    if (valid) {  // ahead of the flags
+      pr = pn_ptr[g];
+      pe = pn_ptr[g + 1];
+    }
     if (!sel[s] || done[s] || depth[s] <= l) continue;  // uniform over the warp
-    const size_t rs = (size_t)2 * pnnz[s];  // P row stride between c = 0 and c = 1
+    if (!valid) continue;
     const int cno = cnode_off[s], cnn = cnode_off[s + 1] - cno, cd = cdof_off[s];
     const int no = node_off[s], nn = node_off[s + 1] - no, d0 = dof_off[s];
-    for (int g = nb_start[b] + lane; g < nb_start[b + 1]; g += 32) {
-      const int pr = pn_ptr[g], dP = pn_ptr[g + 1] - pr;
-      const VT* p0 = P + poff[s] + 2 * (size_t)(pr - pbase[s]);
-      const int i0 = d0 + (g - no), i1 = i0 + nn;
-      double a0 = (double)x[i0], a1 = (double)x[i1];
-      for (int k = 0; k < dP; ++k) {
-        const int K = cd + (pn_col[pr + k] - cno);
-        const double xu = (double)xc[K], xv = (double)xc[K + cnn];
-        a0 += (double)p0[k] * xu + (double)p0[dP + k] * xv;
-        a1 += (double)p0[rs + k] * xu + (double)p0[rs + dP + k] * xv;
+    const int i0 = d0 + (g - no), i1 = i0 + nn;
+    double a0 = (double)x[i0], a1 = (double)x[i1];
+    for (int k0 = pr; k0 < pe; k0 += CH) {
+      int K[CH];
+      VT q[CH][4];  // P((c,g),(c2,K)) at 2 c + c2 (BF16 quads widen exactly to FP32)
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        K[k] = -1;
+        if (k0 + k < pe) {
+          K[k] = cd + (pn_col[k0 + k] - cno);
+          pq_get(Q + k0 + k, q[k]);
+        }
       }
-      x[i0] = (VT)a0;
-      x[i1] = (VT)a1;
+      VT xu[CH], xv[CH];
+#pragma unroll
+      for (int k = 0; k < CH; ++k)
+        if (K[k] >= 0) {
+          xu[k] = xc[K[k]];
+          xv[k] = xc[K[k] + cnn];
+        }
+#pragma unroll
+      for (int k = 0; k < CH; ++k)
+        if (K[k] >= 0) {
+          a0 += (double)q[k][0] * (double)xu[k] + (double)q[k][1] * (double)xv[k];
+          a1 += (double)q[k][2] * (double)xu[k] + (double)q[k][3] * (double)xv[k];
+        }
     }
+    x[i0] = (VT)a0;
+    x[i1] = (VT)a1;
   }
 }
 
@@ -1387,27 +1526,29 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
       const KT* A = l == 0 ? K0 : (const KT*)F.A;
       const unsigned char* mk = l == 0 ? cmask : nullptr;
       l1(l);
-      const int nbf = (F.ndof + 127) / 128, nbc = (C.ndof + 127) / 128;
-      // the mixed form sets up in FP32 into the arrays its transfers read (sa_plo, sa_ptlo); the
-      // FP64 form in FP64, with FP32 copies
+      const int nbf = (F.ndof + 127) / 128;
+      // the mixed form sets up in FP32, the FP64 form in FP64; P then goes into the transfer
+      // layout (quads, pn and ptn order), which A P, the coarse operator and the V-cycle read
       using ST = typename std::conditional<sizeof(KT) == 4, float, double>::type;
+      using QT = typename PQuadOf<KT>::T;
       ST* Pv = sizeof(KT) == 4 ? (ST*)F.sa_plo : (ST*)F.sa_p;
-      ST* PTv = sizeof(KT) == 4 ? (ST*)F.sa_ptlo : (ST*)F.sa_pt;
       ST* APv = (ST*)F.sa_ap;
+      QT* Qv = (QT*)(sizeof(KT) == 4 ? F.sa_qh : F.sa_qd);
+      QT* QTv = (QT*)(sizeof(KT) == 4 ? F.sa_qth : F.sa_qtd);
       k_sa_P<KT, VT, ST><<<nbf, 128, 0, st>>>(F.ndof, F.dof_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk,
                                               (const VT*)F.invd, F.sa_agg, F.pn_ptr, F.pn_col, F.pbase, F.pnnz,
                                               F.poff, Pv, psel), ++*launches;
+      k_sa_quads<ST, QT><<<(F.nn + 127) / 128, 128, 0, st>>>(F.nn, F.node_sys, F.pn_ptr, F.pbase, F.pnnz, F.poff,
+                                                            Pv, Qv, psel), ++*launches;
+      k_sa_qt<QT><<<(C.nn + 127) / 128, 128, 0, st>>>(C.nn, C.node_sys, F.ptn_ptr, F.ptn_fine, F.ptn_k, F.pn_ptr,
+                                                      Qv, QTv, psel), ++*launches;
       const int ms = F.ap_maxrow <= kSaApSm ? F.ap_maxrow : 0;  // rows summed in shared memory
-      k_sa_AP<KT, ST><<<(int)(((long long)F.nn * kSaGL + 127) / 128), 128, sa_ap_smem<ST>(ms), st>>>(F.nn, F.node_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr,
-                                       F.pn_col, F.pbase, F.pnnz, F.poff, Pv, F.apn_ptr, F.apn_col, F.apbase,
-                                       F.apnnz, F.apoff, APv, sel, ms), ++*launches;
-      k_sa_PT<ST><<<nbc, 128, 0, st>>>(C.ndof, C.dof_sys, C.d_dof_off, C.d_node_off, F.ptn_ptr, F.ptn_fine, F.ptn_k,
-                                       F.ptbase, F.pn_ptr, F.pbase, F.pnnz, F.poff, Pv, PTv,
-                                       sizeof(KT) == 4 ? nullptr : F.sa_plo, sizeof(KT) == 4 ? nullptr : F.sa_ptlo,
-                                       psel), ++*launches;
+      k_sa_AP<KT, ST><<<(int)(((long long)F.nn * kSaGL + 127) / 128), 128, sa_ap_smem<ST>(ms), st>>>(
+          F.nn, F.node_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr, F.pn_col, Qv, F.apn_ptr, F.apn_col,
+          F.apbase, F.apnnz, F.apoff, APv, sel, ms), ++*launches;
       k_sa_Ac<KT, ST><<<(C.nn + kSaAcWarps - 1) / kSaAcWarps, 32 * kSaAcWarps, sa_ac_smem(F.ac_maxdeg), st>>>(
-          C.nn, C.node_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr, F.ptn_fine, F.ptbase, F.pnnz,
-          F.poff, PTv, F.apn_ptr, F.apn_col, F.apbase, F.apnnz, F.apoff, APv, (KT*)C.A, sel, F.ac_maxdeg),
+          C.nn, C.node_sys, C.d_dof_off, C.d_node_off, C.rowptr, C.colind, F.ptn_ptr, F.ptn_fine, QTv, F.apn_ptr,
+          F.apn_col, F.apbase, F.apnnz, F.apoff, APv, (KT*)C.A, sel, F.ac_maxdeg),
           ++*launches;
     }
     l1(a->nlev - 1);
@@ -1432,7 +1573,72 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
 
 static SellDev sell_dev(const ua_mesh* m, const Sell& S) {
   return SellDev{S.sb_sys, S.sb_n0, S.sb_cnt, S.sb_rbu, S.sb_rbv, S.perm, S.sl_off, S.cols,
-                 m->dm.sys_dof_off, m->dm.sys_node_off, m->dm.dbg};
+                 m->dm.sys_dof_off, m->dm.sys_node_off, m->dm.dbg, 0};
+}
+static SellDev csell_dev(const ua_mesh* m, const Sell& S, const AmgLevel& L, int l) {
+  return SellDev{S.sb_sys, S.sb_n0, S.sb_cnt, nullptr, nullptr, S.perm, S.sl_off, S.cols,
+                 L.d_dof_off, L.d_node_off, m->dm.dbg, l};
+}
+
+// Node slices of the coarse levels that run a residual and a smoothing pass (1 .. nlev-2) and
+// hold at least kCsellMinNodes nodes (below that the CSR row blocks, finer-grained than the slice
+// blocks of 256 nodes, spread better over the SMs): per system, blocks of kSellNodes nodes
+// ordered by decreasing degree, slices of 32 (the finest level's layout; node degrees from the
+// level's CSR).
+constexpr int kCsellMinNodes = 131072;
+static void csell_init(ua_mesh* m) {
+  Amg* a = m->amg;
+  const int nsys = a->nsys;
+  a->csell.assign(std::max(a->nlev, 1), Sell());
+  for (int l = 1; l + 1 < a->nlev; ++l) {
+    AmgLevel& L = a->lev[l];
+    Sell& S = a->csell[l];
+    if (L.nn < kCsellMinNodes) continue;
+    std::vector<int> rowptr(L.ndof + 1);
+    if (cudaMemcpy(rowptr.data(), L.rowptr, sizeof(int) * rowptr.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      S.failed = true;
+      return;
+    }
+    std::vector<int> sb_sys, sb_n0, sb_cnt, perm(std::max(L.nn, 1)), idx;
+    std::vector<long long> sl_off(1, 0);
+    S.h_sys_sb_off.assign(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) {
+      const int no = L.node_off[s], nn = L.node_off[s + 1] - no, d0 = L.dof_off[s];
+      auto deg = [&](int g) { return (rowptr[d0 + (g - no) + 1] - rowptr[d0 + (g - no)]) >> 1; };
+      for (int n0 = no; n0 < no + nn; n0 += kSellNodes) {
+        const int cnt = std::min(kSellNodes, no + nn - n0);
+        idx.resize(cnt);
+        for (int k = 0; k < cnt; ++k) idx[k] = n0 + k;
+        std::stable_sort(idx.begin(), idx.end(), [&](int p, int q) { return deg(p) > deg(q); });
+        for (int k = 0; k < cnt; ++k) perm[n0 + k] = idx[k];
+        for (int j = 0; j < kSellSlices; ++j) {
+          int W = 0;
+          for (int k = j * 32; k < std::min(cnt, j * 32 + 32); ++k) W = std::max(W, deg(idx[k]));
+          sl_off.push_back(sl_off.back() + 32LL * W);
+        }
+        sb_sys.push_back(s);
+        sb_n0.push_back(n0);
+        sb_cnt.push_back(cnt);
+      }
+      S.h_sys_sb_off[s + 1] = (int)sb_sys.size();
+    }
+    bool ok = true;
+    S.nsb = (int)sb_sys.size();
+    S.slots = sl_off.back();
+    S.sb_sys = upload(m, a, sb_sys, ok);
+    S.sb_n0 = upload(m, a, sb_n0, ok);
+    S.sb_cnt = upload(m, a, sb_cnt, ok);
+    S.perm = upload(m, a, perm, ok);
+    S.sl_off = upload(m, a, sl_off, ok);
+    S.cols = (int*)dalloc(m, a, sizeof(int) * (size_t)S.slots, ok);
+    S.vlo = (__nv_bfloat16*)dalloc(m, a, sizeof(__nv_bfloat16) * 4 * (size_t)S.slots, ok);
+    if (!ok) { S.failed = true; return; }
+    if (S.nsb)
+      k_csell_fill<float><<<S.nsb, 256, 0, m->stream>>>(csell_dev(m, S, L, l), L.rowptr, L.colind, nullptr,
+                                                       nullptr, S.cols, nullptr);
+    if (cudaGetLastError() != cudaSuccess) { S.failed = true; return; }
+    S.ready = true;
+  }
 }
 
 int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
@@ -1496,6 +1702,7 @@ int amg_sell_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { S.failed = true; return set_error(UA_ERR_CUDA, "node slices: %s", cudaGetErrorString(e)); }
   S.ready = true;
+  if (a->sa) csell_init(m);  // the coarse levels keep their CSR passes if this fails
   return UA_OK;
 }
 
@@ -1517,6 +1724,14 @@ int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* lau
     k_sell_fill<double><<<S.nsb, 256, 0, m->stream>>>(sell_dev(m, S), m->dm, (const double*)K0, S.v64,
                                                        lo ? S.vlo : nullptr, nullptr, sel);
   ++*launches;
+  if (lo && fp32)  // the coarse operators of this Newton step's set-up (FP32) into their BF16 slices
+    for (int l = 1; l < (int)a->csell.size(); ++l) {
+      const Sell& C = a->csell[l];
+      if (!C.ready || !C.nsb) continue;
+      const AmgLevel& L = a->lev[l];
+      k_csell_fill<float><<<C.nsb, 256, 0, m->stream>>>(csell_dev(m, C, L, l), L.rowptr, L.colind,
+                                                       (const float*)L.A, C.vlo, nullptr, sel), ++*launches;
+    }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(UA_ERR_CUDA, "node slices: %s", cudaGetErrorString(e));
   return UA_OK;
@@ -1525,13 +1740,14 @@ int amg_sell_fill(ua_mesh* m, const void* K0, bool fp32, bool lo, long long* lau
 // Grid of a slice kernel: one slice block per CTA, or, list-driven, the CTAs resident at once
 // (per-instantiation occupancy, so that no partial second wave trails the list loop).
 template <typename KT, typename VT, int MODE>
-static int sell_grid(const Amg* a, bool listed) {
-  if (!listed) return a->sell.nsb;
+static int sell_grid(const Amg* a, bool listed, int nsb = -1) {
+  if (nsb < 0) nsb = a->sell.nsb;
+  if (!listed) return nsb;
   static int occ = 0;
   if (!occ && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sell<KT, VT, MODE>, 256, 0) != cudaSuccess ||
                occ < 1))
     occ = 1;
-  return std::max(1, std::min(a->sell.nsb, occ * a->nsm));
+  return std::max(1, std::min(nsb, occ * a->nsm));
 }
 
 void amg_sell_partials(const ua_mesh* m, const double** spart, const int** sys_sl_off) {
@@ -1612,6 +1828,18 @@ int amg_numeric(ua_mesh* m, const int* rowptr0, const int* colind0, const void* 
       UA_CUDA_TRY(cudaFuncSetAttribute(k_sa_AP<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sap));
     }
   }
+  if (a->sa) {  // the transfer quads of this precision, allocated before any capture
+    bool ok = true;
+    for (int l = 0; l + 1 < a->nlev; ++l) {
+      AmgLevel& F = a->lev[l];
+      void*& q = fp32 ? F.sa_qh : F.sa_qd;
+      void*& qt = fp32 ? F.sa_qth : F.sa_qtd;
+      const size_t qb = fp32 ? sizeof(PQuadH) : sizeof(PQuadD);
+      if (!q) q = dalloc(m, a, qb * (size_t)std::max(F.np, 1LL), ok);
+      if (!qt) qt = dalloc(m, a, qb * (size_t)std::max(F.np, 1LL), ok);
+    }
+    if (!ok) return set_error(UA_ERR_OOM, "AMG: device allocation of the transfer values failed");
+  }
   auto run = [&](long long* l) {
     return fp32 ? numeric_t<float, float>(m, rowptr0, colind0, (const float*)K0, cmask, sel, psel, l)
                 : numeric_t<double, double>(m, rowptr0, colind0, (const double*)K0, cmask, sel, psel, l);
@@ -1646,11 +1874,10 @@ void amg_restart_P(ua_mesh* m, const std::vector<int>& run) {
     if (run[s]) a->p_age[s] = 0;
 }
 
-// the transfer values in the vector precision
+// the transfer quads of the vector precision
 template <typename VT>
-static const VT* sa_vals(const double* v64, const float* v32) {
-  if constexpr (std::is_same<VT, float>::value) return v32;
-  else return v64;
+static const typename PQuadOf<VT>::T* sa_quads(void* qd, void* qh) {
+  return (const typename PQuadOf<VT>::T*)(std::is_same<VT, float>::value ? qh : qd);
 }
 
 // Finest-level residual (MODE 1: W = mask(r - K x0)) or smoothing (MODE 2: z = mask(x + invd (r - K x)),
@@ -1677,6 +1904,20 @@ static void sell_pass(ua_mesh* m, const AmgPcgView& v, bool useact, const VT* in
                                                       invd, v.cmask, out, pcopy, part);
 }
 
+// Coarse-level residual (MODE 1) or smoothing (MODE 2, no partials) over level l's BF16 node slices.
+template <typename VT, int MODE>
+static void csell_pass(ua_mesh* m, const AmgPcgView& v, int l, bool useact, const VT* x, const VT* b,
+                       const VT* invd, VT* out) {
+  Amg* a = m->amg;
+  const Sell& S = a->csell[l];
+  if (!S.nsb) return;
+  const bool la = useact && S.act.map;
+  const ActList L = la ? S.act : ActList{};
+  k_sell<__nv_bfloat16, VT, MODE><<<sell_grid<__nv_bfloat16, VT, MODE>(a, la, S.nsb), 256, 0, m->stream>>>(
+      csell_dev(m, S, a->lev[l], l), S.nsb, L, v.sel, v.done, a->d_depth, S.vlo, x, b, invd, nullptr, out, nullptr,
+      nullptr);
+}
+
 template <typename KT, typename VT>
 static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
   Amg* a = m->amg;
@@ -1699,11 +1940,15 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
   const bool useact = v.act && a->act_ready;
   auto rows_act = [&](int l) { return useact ? a->rows[l] : ActList{}; };
   auto rows_grid = [&](int l) { return useact ? act_grid(nrb(l), a->nsm) : nrb(l); };
+  // coarse levels on BF16 node slices: the mixed-precision cycle with node slices at the finest level
+  auto cslices = [&](int l) { return v.sell && v.sell_lo && l < (int)a->csell.size() && a->csell[l].ready; };
   for (int l = 0; l + 1 < nl; ++l) {  // down: residual of level l, aggregated into level l+1
     const AmgLevel& C = a->lev[l + 1];
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 0);
     if (l == 0 && v.sell)
       sell_pass<KT, VT, 1>(m, v, useact, (const VT*)nullptr, W(0));
+    else if (l > 0 && cslices(l))
+      csell_pass<VT, 1>(m, v, l, useact, X(l), B(l), nullptr, W(l));
     else
     dispatch_lpr(l == 0 ? lpr0 : lprc, [&](auto L) {
       if (l == 0 && v.K0lo)
@@ -1720,8 +1965,7 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     if (a->sa)
       k_sa_restrict<VT><<<useact ? act_grid(C.nnb, a->nsm) : C.nnb, 256, 0, st>>>(
           C.nb_start, C.nb_sys, useact ? a->cnodes[l] : ActList{}, C.d_dof_off, C.d_node_off, a->d_depth, l + 1,
-          v.sel, v.done, F.ptn_ptr, F.ptn_fine, F.ptbase, F.pnnz, F.poff, sa_vals<VT>(F.sa_pt, F.sa_ptlo),
-          F.d_dof_off, F.d_node_off, W(l), (const VT*)C.invd, (VT*)C.b, (VT*)C.x), ++*launches;
+          v.sel, v.done, F.ptn_ptr, F.ptn_fine, sa_quads<VT>(F.sa_qtd, F.sa_qth), F.d_dof_off, F.d_node_off, W(l), (const VT*)C.invd, (VT*)C.b, (VT*)C.x), ++*launches;
     else
       k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done,
                                                              C.mptr, C.mlist, W(l), (const VT*)C.invd, (VT*)C.b,
@@ -1736,7 +1980,7 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
       k_sa_prolong<VT><<<useact ? act_grid((F.nnb + kSaPW - 1) / kSaPW, a->nsm) : (F.nnb + kSaPW - 1) / kSaPW,
                          32 * kSaPW, 0, st>>>(
           F.nnb, F.nb_start, F.nb_sys, useact ? a->fnodes[l] : ActList{}, F.d_dof_off, F.d_node_off, a->d_depth, l,
-          v.sel, v.done, F.pn_ptr, F.pn_col, F.pbase, F.pnnz, F.poff, sa_vals<VT>(F.sa_p, F.sa_plo), C.d_dof_off,
+          v.sel, v.done, F.pn_ptr, F.pn_col, sa_quads<VT>(F.sa_qd, F.sa_qh), C.d_dof_off,
           C.d_node_off, (const VT*)C.x2, X(l)), ++*launches;
     else
       k_amg_correct<VT><<<nrb(l), 256, 0, st>>>(rbs(l), rbsys(l), v.sel, v.done, a->d_depth, l, X(l),
@@ -1747,6 +1991,8 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 1, 0);
     if (l == 0 && v.sell)
       sell_pass<KT, VT, 2>(m, v, useact, (const VT*)F.invd, out);
+    else if (l > 0 && cslices(l))
+      csell_pass<VT, 2>(m, v, l, useact, X(l), B(l), (const VT*)F.invd, out);
     else
     dispatch_lpr(l == 0 ? lpr0 : lprc, [&](auto L) {
       if (l == 0 && v.K0lo)
@@ -1939,6 +2185,8 @@ int amg_act_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
       a->cnodes[l] = make(a->lev[l + 1].h_sys_nb_off, l);
     }
   if (a->sell.ready) a->sell.act = make(a->sell.h_sys_sb_off, -1);  // node slice blocks: every active system
+  for (int l = 1; l < (int)a->csell.size(); ++l)
+    if (a->csell[l].ready) a->csell[l].act = make(a->csell[l].h_sys_sb_off, l);  // depth > l
   a->d_specs = upload(m, a, specs, ok);
   a->nspecs = (int)specs.size();
   if (!ok) return set_error(UA_ERR_OOM, "active lists: device allocation failed");
