@@ -188,6 +188,10 @@ typedef struct ua_fields {
     const double *q, *muk, *V0;
     /* melange: ocean velocity, drag and exponent; atmosphere the same (IncludeMelangeModelPhysics) */
     const double *uo, *vo, *Co, *mo, *ua, *va, *Ca, *ma;
+    /* uv Newton (ua_uv_newton, ua_uv_newton_batch): where the solution goes, same location as
+       the inputs; NULL = into ub, vb.  With both set, ub and vb are read only (the start
+       velocities).  The uvh calls ignore them. */
+    double *ub_out, *vb_out;
 } ua_fields;
 
 /* Boundary conditions (BCs2MLC.m, CreateLuv.m).  Index base as the mesh.  Fixed nodes, ties

@@ -166,6 +166,19 @@ def test_batch_is_bit_identical_to_alone():
     for k, (ub, vb, info) in enumerate(out):
         assert info.converged
         assert np.array_equal(np.concatenate([ub, vb]), alone[k])
+    # caller-owned output arrays (ua_fields.ub_out/vb_out): same solutions, start velocities untouched
+    Fs = [ua.Fields.from_problem(P) for P in probs]
+    for F in Fs:
+        F.ub = np.full(F.ub.shape, 5.0)
+        F.vb = np.full(F.vb.shape, -2.0)
+    dst = [(np.full(P.Nnodes, np.nan), np.full(P.Nnodes, np.nan)) for P in probs]
+    out2 = ua.uv_batch(ctrl, batch, Fs, [ua.BCs.from_problem(P) for P in probs], out=dst)
+    for k, (ub, vb, info) in enumerate(out2):
+        assert info.converged and ub is dst[k][0] and vb is dst[k][1]
+        assert np.all(Fs[k].ub == 5.0) and np.all(Fs[k].vb == -2.0)
+        ref = ua.uv(ctrl, ua.CreateMUA(probs[k].coordinates, probs[k].connectivity), ua.BCs.from_problem(probs[k]),
+                    Fs[k].copy())[0]
+        assert np.array_equal(ub, ref.ub) and np.array_equal(vb, ref.vb)
 
 
 def test_repeat_is_deterministic():

@@ -3130,8 +3130,8 @@ static int newton_common(ua_mesh* m, const ua_params* p, ua_fields* F, const ua_
     ua_fields& f = F[nF == 1 ? 0 : s];
     const int d0 = m->h_dof_off[s], nn = m->sys[s].nn;
     auto kind = f.location == UA_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-    UA_CUDA_TRY(cudaMemcpyAsync(f.ub, w->X + d0, nn * sizeof(double), kind, m->stream));
-    UA_CUDA_TRY(cudaMemcpyAsync(f.vb, w->X + d0 + nn, nn * sizeof(double), kind, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(f.ub_out ? f.ub_out : f.ub, w->X + d0, nn * sizeof(double), kind, m->stream));
+    UA_CUDA_TRY(cudaMemcpyAsync(f.vb_out ? f.vb_out : f.vb, w->X + d0 + nn, nn * sizeof(double), kind, m->stream));
     if (lam_io && lam_io[s]) {
       int nc_s = w->h_sys_con_off[s + 1] - w->h_sys_con_off[s];
       if (nl_io[s] >= nc_s && nc_s > 0)

@@ -104,7 +104,7 @@ class ua_fields(C.Structure):
                 ("dadh", _dp), ("h1", _dp), ("dt", C.c_double),
                 ("q", _dp), ("muk", _dp), ("V0", _dp),
                 ("uo", _dp), ("vo", _dp), ("Co", _dp), ("mo", _dp), ("ua", _dp), ("va", _dp), ("Ca", _dp),
-                ("ma", _dp)]
+                ("ma", _dp), ("ub_out", _dp), ("vb_out", _dp)]
 
 
 class ua_measurements(C.Structure):

@@ -217,7 +217,7 @@ class _Keep:
         return L.iptr(a)
 
 
-def _c_fields(F: Fields, keep: _Keep, Nn: int):
+def _c_fields(F: Fields, keep: _Keep, Nn: int, copy_uv=True):
     cf = L.ua_fields()
     cf.location = L.UA_HOST
 
@@ -227,8 +227,9 @@ def _c_fields(F: Fields, keep: _Keep, Nn: int):
 
     for name in ("h", "S", "B", "rho", "AGlen", "n", "C", "m"):
         setattr(cf, name, keep.d(full(getattr(F, name))))
-    ub = _f64(F.ub).copy()
-    vb = _f64(F.vb).copy()
+    # the solution overwrites ub, vb unless the caller gives output arrays (copy_uv=False)
+    ub = _f64(F.ub).copy() if copy_uv else _f64(F.ub)
+    vb = _f64(F.vb).copy() if copy_uv else _f64(F.vb)
     keep.refs += [ub, vb]
     cf.ub = L.dptr(ub)
     cf.vb = L.dptr(vb)
@@ -478,8 +479,13 @@ def uv(ctrl: CtrlVar, mua: MUA, bcs: BCs, F: Fields, l=None, return_K=False, ret
     return Fo, lam, K, Rv, _report(rep, recs, upd)
 
 
-def uv_batch(ctrl: CtrlVar, mua: MUA, Fs, bcss):
+def uv_batch(ctrl: CtrlVar, mua: MUA, Fs, bcss, out=None):
     """Batched uv Newton: all systems of a batch handle in the same launches.
+
+    ``out`` (optional): per system a pair ``(ub, vb)`` of caller-owned float64 arrays of the
+    system's node count that receive the solution (``ua_fields.ub_out/vb_out``); ``Fs[s].ub/vb``
+    are then read in place as the start velocities (no copies: pinned host buffers stay pinned).
+    Without it the solution goes into fresh copies of ``Fs[s].ub/vb``.
 
     Returns a list of ``(ub, vb, RunInfo)``.
     """
@@ -491,8 +497,21 @@ def uv_batch(ctrl: CtrlVar, mua: MUA, Fs, bcss):
     outs = []
     reps = (L.ua_newton_report * ns)()
     recs = []
+    if out is not None and len(out) != ns:
+        raise ValueError(f"uv_batch: out holds {len(out)} pairs for {ns} systems")
     for s in range(ns):
-        cf, ub, vb = _c_fields(Fs[s], keep, mua.Nnodes(s))
+        if out is None:
+            cf, ub, vb = _c_fields(Fs[s], keep, mua.Nnodes(s))
+        else:
+            cf, ub, vb = _c_fields(Fs[s], keep, mua.Nnodes(s), copy_uv=False)
+            ub, vb = out[s]
+            for a in (ub, vb):
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+                        and a.size == mua.Nnodes(s)):
+                    raise ValueError("uv_batch: out arrays must be contiguous float64 of the node count")
+            keep.refs += [ub, vb]
+            cf.ub_out = L.dptr(ub)
+            cf.vb_out = L.dptr(vb)
         cfs[s] = cf
         cbs[s] = _c_bcs(bcss[s], keep)
         outs.append((ub, vb))
