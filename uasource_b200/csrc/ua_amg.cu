@@ -662,6 +662,7 @@ __global__ void __launch_bounds__(256) k_amg_dense_apply(const int* sel, const i
                                                          const int* dn_arr, const int* doff, int* const* lev_dofoff,
                                                          void* const* lev_b, void* const* lev_x2,
                                                          const double* dense) {
+  pdl_enter();
   __shared__ double sb[kAmgMaxDense];
   const int s = blockIdx.x;
   if (!sel[s] || done[s]) return;
@@ -737,6 +738,7 @@ __global__ void __launch_bounds__(256) k_amg_residual(const int* rb_start, const
                                                       const int* rowptr, const int* colind, const KT* A,
                                                       const VT* b, const VT* x, const unsigned char* cmask, VT* res,
                                                       const int* dof_off) {
+  pdl_enter();
   const int nv = act.cnt ? *act.cnt : gridDim.x;  // list entries, else one block per CTA
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
     const int blk = act.map ? act.map[vb] : vb;
@@ -792,6 +794,7 @@ __global__ void __launch_bounds__(256) k_amg_smooth(const int* rb_start, const i
                                                     const int* rowptr, const int* colind, const KT* A, const VT* b,
                                                     const VT* xp, const VT* invd, const unsigned char* cmask, VT* out,
                                                     VT* pcopy, double* part, const int* dof_off) {
+  pdl_enter();
   __shared__ double red[8];
   const int nv = act.cnt ? *act.cnt : gridDim.x;  // list entries, else one block per CTA
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
@@ -959,6 +962,7 @@ __global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 6 : 0) k_sell(SellDev S
                                               const int* depth, const KT* vals, const VT* x, const VT* b,
                                               const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
                                               double* part) {
+  pdl_enter();
   const int nv = act.cnt ? *act.cnt : nsb;
   const int w = threadIdx.x >> 5, t = threadIdx.x & 31, pos = w * 32 + t;
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
@@ -1377,6 +1381,7 @@ __global__ void __launch_bounds__(32 * kSaRL, 4) k_sa_restrict(const int* nb_sta
                                                             const typename PQuadOf<VT>::T* QTr,
                                                             const int* fdof_off, const int* fnode_off,
                                                             const VT* res, const VT* cinvd, VT* cb, VT* cx) {
+  pdl_enter();
   static_assert(kAmgNB == 32, "one coarse node per kSaRL-lane group of a 32 kSaRL-thread CTA");
   constexpr int CH = sizeof(VT) == 4 ? kSaChunk : kSaChunk / 2;  // FP64 chunks held to the register budget
   const int sub = threadIdx.x / kSaRL, lane = threadIdx.x % kSaRL;
@@ -1451,6 +1456,7 @@ __global__ void __launch_bounds__(32 * kSaPW, 4) k_sa_prolong(int nnb, const int
                                                            const typename PQuadOf<VT>::T* Q, const int* cdof_off,
                                                            const int* cnode_off, const VT* xc,
                                                            VT* x) {
+  pdl_enter();
   static_assert(kAmgNB == 32, "one fine node per lane");
   constexpr int CH = sizeof(VT) == 4 ? kSaChunk : kSaChunk / 2;  // FP64 chunks held to the register budget
   const int nv = act.cnt ? *act.cnt : nnb;  // list entries, else every node block
@@ -1763,11 +1769,11 @@ int amg_sell_spmv(ua_mesh* m, bool fp32, bool act, const int* sel, const int* do
   const ActList L = useact ? S.act : ActList{};
   if (!S.nsb) return UA_OK;
   if (fp32)
-    k_sell<float, float, 0><<<sell_grid<float, float, 0>(a, useact), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v32,
+    launch_pdl(k_sell<float, float, 0>, sell_grid<float, float, 0>(a, useact), 256, 0, m->stream, sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v32,
                                                          (const float*)p, nullptr, nullptr, cmask, (float*)q,
                                                          nullptr, S.spart);
   else
-    k_sell<double, double, 0><<<sell_grid<double, double, 0>(a, useact), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v64,
+    launch_pdl(k_sell<double, double, 0>, sell_grid<double, double, 0>(a, useact), 256, 0, m->stream, sell_dev(m, S), S.nsb, L, sel, done, a->d_depth, S.v64,
                                                            (const double*)p, nullptr, nullptr, cmask, (double*)q,
                                                            nullptr, S.spart);
   ++*launches;
@@ -1897,10 +1903,10 @@ static void sell_pass(ua_mesh* m, const AmgPcgView& v, bool useact, const VT* in
   if constexpr (std::is_same<KT, float>::value) vk = S.v32;
   else vk = S.v64;
   if (v.sell_lo)
-    k_sell<__nv_bfloat16, VT, MODE><<<sell_grid<__nv_bfloat16, VT, MODE>(a, la), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, v.sel, v.done, a->d_depth,
+    launch_pdl(k_sell<__nv_bfloat16, VT, MODE>, sell_grid<__nv_bfloat16, VT, MODE>(a, la), 256, 0, m->stream, sell_dev(m, S), S.nsb, L, v.sel, v.done, a->d_depth,
                                                                  S.vlo, x, b, invd, v.cmask, out, pcopy, part);
   else
-    k_sell<KT, VT, MODE><<<sell_grid<KT, VT, MODE>(a, la), 256, 0, m->stream>>>(sell_dev(m, S), S.nsb, L, v.sel, v.done, a->d_depth, vk, x, b,
+    launch_pdl(k_sell<KT, VT, MODE>, sell_grid<KT, VT, MODE>(a, la), 256, 0, m->stream, sell_dev(m, S), S.nsb, L, v.sel, v.done, a->d_depth, vk, x, b,
                                                       invd, v.cmask, out, pcopy, part);
 }
 
@@ -1913,8 +1919,7 @@ static void csell_pass(ua_mesh* m, const AmgPcgView& v, int l, bool useact, cons
   if (!S.nsb) return;
   const bool la = useact && S.act.map;
   const ActList L = la ? S.act : ActList{};
-  k_sell<__nv_bfloat16, VT, MODE><<<sell_grid<__nv_bfloat16, VT, MODE>(a, la, S.nsb), 256, 0, m->stream>>>(
-      csell_dev(m, S, a->lev[l], l), S.nsb, L, v.sel, v.done, a->d_depth, S.vlo, x, b, invd, nullptr, out, nullptr,
+  launch_pdl(k_sell<__nv_bfloat16, VT, MODE>, sell_grid<__nv_bfloat16, VT, MODE>(a, la, S.nsb), 256, 0, m->stream, csell_dev(m, S, a->lev[l], l), S.nsb, L, v.sel, v.done, a->d_depth, S.vlo, x, b, invd, nullptr, out, nullptr,
       nullptr);
 }
 
@@ -1952,34 +1957,28 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     else
     dispatch_lpr(l == 0 ? lpr0 : lprc, [&](auto L) {
       if (l == 0 && v.K0lo)
-        k_amg_residual<__nv_bfloat16, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
-            rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
+        launch_pdl(k_amg_residual<__nv_bfloat16, VT, decltype(L)::value>, rows_grid(l), 256, 0, st, rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
             mask(l), W(l), doff(l));
       else
-        k_amg_residual<KT, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
-            rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l), doff(l));
+        launch_pdl(k_amg_residual<KT, VT, decltype(L)::value>, rows_grid(l), 256, 0, st, rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), mask(l), W(l), doff(l));
     });
     ++*launches;
     if (l == 0 && v.mark) v.mark(v.mark_ctx, 0, 1);
     const AmgLevel& F = a->lev[l];
     if (a->sa)
-      k_sa_restrict<VT><<<useact ? act_grid(C.nnb, a->nsm) : C.nnb, 256, 0, st>>>(
-          C.nb_start, C.nb_sys, useact ? a->cnodes[l] : ActList{}, C.d_dof_off, C.d_node_off, a->d_depth, l + 1,
+      launch_pdl(k_sa_restrict<VT>, useact ? act_grid(C.nnb, a->nsm) : C.nnb, 256, 0, st, C.nb_start, C.nb_sys, useact ? a->cnodes[l] : ActList{}, C.d_dof_off, C.d_node_off, a->d_depth, l + 1,
           v.sel, v.done, F.ptn_ptr, F.ptn_fine, sa_quads<VT>(F.sa_qtd, F.sa_qth), F.d_dof_off, F.d_node_off, W(l), (const VT*)C.invd, (VT*)C.b, (VT*)C.x), ++*launches;
     else
       k_amg_gather<VT><<<(C.ndof + 127) / 128, 128, 0, st>>>(C.ndof, C.dof_sys, a->d_depth, l + 1, v.sel, v.done,
                                                              C.mptr, C.mlist, W(l), (const VT*)C.invd, (VT*)C.b,
                                                              (VT*)C.x), ++*launches;
   }
-  k_amg_dense_apply<VT><<<dim3(a->nsys, (a->maxdn + 31) / 32), 256, 0, st>>>(
-      v.sel, v.done, a->d_depth, a->d_dn, a->d_doff, a->d_lev_dofoff, a->d_lev_b, a->d_lev_x2, a->dense), ++*launches;
+  launch_pdl(k_amg_dense_apply<VT>, dim3(a->nsys, (a->maxdn + 31) / 32), 256, 0, st, v.sel, v.done, a->d_depth, a->d_dn, a->d_doff, a->d_lev_dofoff, a->d_lev_b, a->d_lev_x2, a->dense), ++*launches;
   for (int l = nl - 2; l >= 0; --l) {  // up: correction from level l+1's post-smoothed x2, then smoothing
     const AmgLevel& F = a->lev[l];
     const AmgLevel& C = a->lev[l + 1];
     if (a->sa)
-      k_sa_prolong<VT><<<useact ? act_grid((F.nnb + kSaPW - 1) / kSaPW, a->nsm) : (F.nnb + kSaPW - 1) / kSaPW,
-                         32 * kSaPW, 0, st>>>(
-          F.nnb, F.nb_start, F.nb_sys, useact ? a->fnodes[l] : ActList{}, F.d_dof_off, F.d_node_off, a->d_depth, l,
+      launch_pdl(k_sa_prolong<VT>, useact ? act_grid((F.nnb + kSaPW - 1) / kSaPW, a->nsm) : (F.nnb + kSaPW - 1) / kSaPW, 32 * kSaPW, 0, st, F.nnb, F.nb_start, F.nb_sys, useact ? a->fnodes[l] : ActList{}, F.d_dof_off, F.d_node_off, a->d_depth, l,
           v.sel, v.done, F.pn_ptr, F.pn_col, sa_quads<VT>(F.sa_qd, F.sa_qh), C.d_dof_off,
           C.d_node_off, (const VT*)C.x2, X(l)), ++*launches;
     else
@@ -1996,12 +1995,10 @@ static int vcycle_t(ua_mesh* m, const AmgPcgView& v, long long* launches) {
     else
     dispatch_lpr(l == 0 ? lpr0 : lprc, [&](auto L) {
       if (l == 0 && v.K0lo)
-        k_amg_smooth<__nv_bfloat16, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
-            rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
+        launch_pdl(k_amg_smooth<__nv_bfloat16, VT, decltype(L)::value>, rows_grid(l), 256, 0, st, rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), (const __nv_bfloat16*)v.K0lo, B(l), X(l),
             (const VT*)F.invd, mask(l), out, pcopy, part, doff(l));
       else
-        k_amg_smooth<KT, VT, decltype(L)::value><<<rows_grid(l), 256, 0, st>>>(
-            rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), (const VT*)F.invd,
+        launch_pdl(k_amg_smooth<KT, VT, decltype(L)::value>, rows_grid(l), 256, 0, st, rbs(l), rbsys(l), rows_act(l), v.sel, v.done, a->d_depth, l, rp(l), ci(l), A(l), B(l), X(l), (const VT*)F.invd,
             mask(l), out, pcopy, part, doff(l));
     });
     ++*launches;
@@ -2123,6 +2120,7 @@ __device__ int block_excl_scan(int v, int* sh, int& total) {
 // one warp per active system writes its block ids, the lanes striding over them
 __global__ void __launch_bounds__(1024) k_act_compact(const ActSpec* specs, int nsys, const int* sel,
                                                       const int* done, const int* depth) {
+  pdl_enter();
   __shared__ int sh[32];
   __shared__ int s_ex[1024], s_n[1024], s_b0[1024];
   const ActSpec sp = specs[blockIdx.x];
@@ -2196,7 +2194,7 @@ int amg_act_init(ua_mesh* m, const std::vector<int>& sys_rb_off0) {
 
 void amg_act_compact(ua_mesh* m, const int* sel, const int* done, long long* launches) {
   Amg* a = m->amg;
-  k_act_compact<<<a->nspecs, 1024, 0, m->stream>>>(a->d_specs, a->nsys, sel, done, a->d_depth), ++*launches;
+  launch_pdl(k_act_compact, a->nspecs, 1024, 0, m->stream, a->d_specs, a->nsys, sel, done, a->d_depth), ++*launches;
 }
 
 ActList amg_act_rows0(const ua_mesh* m) { return m->amg && m->amg->act_ready ? m->amg->rows[0] : ActList{}; }

@@ -25,6 +25,29 @@
 
 namespace ua {
 
+// Programmatic dependent launch for the short kernels of a PCG step: launched with
+// launch_pdl, a kernel may be scheduled while the kernel before it on the stream drains; it
+// first calls pdl_enter, which waits for that kernel's completion and memory (a no-op for an
+// ordinary launch) and then lets the next kernel be scheduled in turn.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... a) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<A&&>(a)...);
+}
+
 constexpr int kMaxNip = 16;
 constexpr int kMaxNod = 6;
 

@@ -430,6 +430,7 @@ __global__ void __launch_bounds__(256) k_pcg_update1(const int* rb_start, const 
                                                      const int* sel, const int* done, const double* sysv,
                                                      int nsys, double* x, VT* r, VT* z, const VT* p, const VT* q,
                                                      const VT* invd, double* part) {
+  pdl_enter();
   const int nv = act.cnt ? *act.cnt : gridDim.x;
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
     const int blk = act.map ? act.map[vb] : vb;
@@ -455,6 +456,7 @@ template <typename VT>
 __global__ void __launch_bounds__(256) k_pcg_update2(const int* rb_start, const int* rb_sys, ActList act,
                                                      const int* sel, const int* done, const double* sysv, int nsys,
                                                      VT* p, const VT* z) {
+  pdl_enter();
   const int nv = act.cnt ? *act.cnt : gridDim.x;
   for (int vb = blockIdx.x; vb < nv; vb += gridDim.x) {
     const int blk = act.map ? act.map[vb] : vb;
@@ -495,6 +497,7 @@ __device__ __forceinline__ void sys_sum(const double* part, int nrb, int b0, int
 __global__ void k_pcg_reduce(int stage, const int* sys_rb_off, int nrb, const int* sel, int* done, int* its,
                              int* status, double* sysv, int nsys, const double* part, int maxit,
                              const double* spart = nullptr, const int* sys_sl_off = nullptr) {
+  pdl_enter();
   const int s = blockIdx.x;
   if (!sel[s] || (stage > 0 && done[s])) return;
   const int b0 = sys_rb_off[s], b1 = sys_rb_off[s + 1];
@@ -576,6 +579,7 @@ __global__ void k_con_particular(int nc, const int* con_dof, const int* con_sys,
 template <typename VT>
 __global__ void k_pair_project(int npair, const int* pair_rows, const int* con_dof, const int* con_sys,
                                const int* sel, const int* done, ConPairs cp, VT* z) {
+  pdl_enter();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= npair) return;
   const int c = pair_rows[k];
@@ -1506,24 +1510,24 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
       ++g_launches;
     }
     prof_end(m, ev);
-    k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+    launch_pdl(k_pcg_reduce, w->nsys, kRedThreads, 0, m->stream, 1, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                           w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
     if (w->npair)
-      k_pair_project<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
+      launch_pdl(k_pair_project<VT>, npb, 256, 0, m->stream, w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
                                                      w->done, cp, q), ++g_launches;
-    k_pcg_update1<VT><<<grid0, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->sysv,
+    launch_pdl(k_pcg_update1<VT>, grid0, 256, 0, m->stream, w->rb_start, w->rb_sys, w->nrb, act0, w->sel, w->done, w->sysv,
                                                      w->nsys, w->dX, r, zj, pp, q, invd, w->part), ++g_launches;
     if (amg) {
       int rc = amg_vcycle(m, fp32, view, &g_launches);
       if (rc) return rc;
       if (w->npair)
-        k_pair_project<VT><<<npb, 256, 0, m->stream>>>(w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
+        launch_pdl(k_pair_project<VT>, npb, 256, 0, m->stream, w->npair, w->pair_rows, w->con_dof, w->con_sys, w->sel,
                                                        w->done, cp, z), ++g_launches;
     }
-    k_pcg_reduce<<<w->nsys, kRedThreads, 0, m->stream>>>(2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
+    launch_pdl(k_pcg_reduce, w->nsys, kRedThreads, 0, m->stream, 2, w->sys_rb_off, w->nrb, w->sel, w->done, w->its,
                                                           w->status, w->sysv, w->nsys, w->part, p->krylov_maxit, spart, sys_sl_off), ++g_launches;
     if (view.act) amg_act_compact(m, w->sel, w->done, &g_launches);
-    k_pcg_update2<VT><<<grid0, 256, 0, m->stream>>>(w->rb_start, w->rb_sys, act0, w->sel, w->done, w->sysv,
+    launch_pdl(k_pcg_update2<VT>, grid0, 256, 0, m->stream, w->rb_start, w->rb_sys, act0, w->sel, w->done, w->sysv,
                                                      w->nsys, pp, z), ++g_launches;
     return UA_OK;
   };
