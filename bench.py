@@ -513,7 +513,11 @@ def run_ours(args):
             "classes_gbs": {c: (v[2] / (v[0] / 1000) / 1e9 if v[0] > 0 else None) for c, v in cand.items()},
             # device time of the timed classes over the profiled solve's whole device time (the rest:
             # coarse AMG levels, smoothed transfers, AMG set-up, vector updates and reductions)
-            "timed_classes_share_of_device_time": total_k / max(float(prof_info.device_ms), 1e-12)}
+            "timed_classes_share_of_device_time": total_k / max(float(prof_info.device_ms), 1e-12),
+            # the profiled solve's device time by phase (event ranges on the library's stream):
+            # tangent and residual assemblies, AMG numeric set-ups with the node-slice fills, the
+            # Krylov iterations (SpMV, V-cycles, vector updates, reductions, the per-chunk checks)
+            "device_split": _device_split(prof, float(prof_info.device_ms))}
 
     cpu, vs_oracle = None, None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -719,6 +723,13 @@ def _timed_calls(fn, steps, warmup):
         torch.cuda.synchronize()
         per.append(e0.elapsed_time(e1))
     return per, out
+
+
+def _device_split(prof, device_ms):
+    asm = prof["asmK_ms"] + prof["asmR_ms"]
+    parts = {"assembly": asm, "amg_setup": prof.get("setup_ms", 0.0), "krylov": prof.get("krylov_ms", 0.0)}
+    parts["other"] = max(device_ms - sum(parts.values()), 0.0)
+    return {k: {"ms": v, "share": v / max(device_ms, 1e-12)} for k, v in parts.items()}
 
 
 def run_uv1m(args):

@@ -254,6 +254,10 @@ typedef struct ua_newton_report {
     int32_t n_hpos;                  /* uvhActiveSetConstraints: the size of the final active set */
     int32_t hpos_capacity;           /* capacity of hpos_node */
     int32_t* hpos_node;              /* caller-owned, may be NULL: the final BCs1.hPosNode (0-based) */
+    /* profile=1, uv solves: the AMG numeric set-ups with the node-slice fills, and the whole
+       Krylov iterations (SpMV, V-cycles, vector updates, reductions), summed launch-range times */
+    double ksetup_ms, kkrylov_ms;
+    int32_t ksetup_n, kkrylov_n;
 } ua_newton_report;
 
 /* --------------------------------------------------------------------- */

@@ -64,7 +64,8 @@ struct Prof {
   long long* d_act = nullptr;
   int act_cap = 0;
 };
-enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2, PK_AMGR = 3, PK_AMGP = 4, PK_COUNT = 5 };
+enum { PK_ASMK = 0, PK_ASMR = 1, PK_SPMV = 2, PK_AMGR = 3, PK_AMGP = 4, PK_SETUP = 5, PK_KRYLOV = 6, PK_COUNT = 7 };
+constexpr int PK_WORK = 5;  // classes with work counts (ua_newton_report.kwork_*)
 constexpr int kRedThreads = 256;
 // per-system scalars; SV_RH = |rhat|^2, SV_RST = BiCGStab restart pending, SV_NRST = restarts so far
 enum { SV_RZ = 0, SV_PQ, SV_ALPHA, SV_BETA, SV_RR, SV_RR0, SV_TOL2, SV_NORM, SV_FF, SV_FD, SV_OMEGA, SV_RH, SV_RST,
@@ -220,7 +221,9 @@ static void prof_report(ua_newton_report* r, const double* kms, const int* kn, c
   r->kspmv_ms = kms[PK_SPMV]; r->kspmv_n = kn[PK_SPMV];
   r->kamgR_ms = kms[PK_AMGR]; r->kamgR_n = kn[PK_AMGR];
   r->kamgP_ms = kms[PK_AMGP]; r->kamgP_n = kn[PK_AMGP];
-  for (int k = 0; k < PK_COUNT; ++k) { r->kwork_nnz[k] = knnz[k]; r->kwork_rows[k] = krows[k]; }
+  r->ksetup_ms = kms[PK_SETUP]; r->ksetup_n = kn[PK_SETUP];
+  r->kkrylov_ms = kms[PK_KRYLOV]; r->kkrylov_n = kn[PK_KRYLOV];
+  for (int k = 0; k < PK_WORK; ++k) { r->kwork_nnz[k] = knnz[k]; r->kwork_rows[k] = krows[k]; }
 }
 
 static void prof_end(ua_mesh* m, cudaEvent_t* ev) {
@@ -1403,8 +1406,11 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     // prolongator refresh: every Newton step in FP64 (the Newton trajectory of the reference's
     // direct solves), every fourth in the mixed form, unless set
     const int prefresh = p->amg_P_refresh > 0 ? p->amg_P_refresh : (fp32 ? 4 : 1);
+    cudaEvent_t ev[2];
+    prof_begin(m, PK_SETUP, ev);
     int rc = amg_numeric(m, w->rowptr, w->colind, K, fp32, w->cmask, &g_launches, w->sel, &w->h_sel, prefresh,
                          !w->no_graph && !p->profile);
+    prof_end(m, ev);
     if (rc) return rc;
   } else {
     k_invdiag<KT, VT><<<(N + 255) / 256, 256, 0, m->stream>>>(N, K, w->diagpos, w->cmask, (VT*)w->invd), ++g_launches;
@@ -1433,7 +1439,10 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   const int* sys_sl_off = nullptr;
   if (sell) amg_sell_partials(m, &spart, &sys_sl_off);
   if (sell) {
+    cudaEvent_t ev[2];
+    prof_begin(m, PK_SETUP, ev);
     int rc = amg_sell_fill(m, K, fp32, fp32 && p->precond_bf16, &g_launches, w->sel);
+    prof_end(m, ev);
     if (rc) return rc;
     view.sell = true;
     view.sell_lo = fp32 && p->precond_bf16;
@@ -1449,6 +1458,8 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
   }
   const ActList act0 = view.act ? amg_act_rows0(m) : ActList{};
   const int grid0 = view.act ? act_grid(w->nrb, w->nsm) : w->nrb;
+  cudaEvent_t kev[2];  // the Krylov iterations, from the initial residual to the last chunk
+  prof_begin(m, PK_KRYLOV, kev);
   dispatch_lpr(lpr, [&](auto L) {
     if (uvlay)
       k_pcg_init<KT, VT, decltype(L)::value, true><<<w->nrb, 256, 0, m->stream>>>(
@@ -1577,6 +1588,7 @@ static int pcg_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, cons
     for (int s = 0; s < w->nsys; ++s) all = all && (w->h_int[s] || !its_out[s]);
     if (all || it >= p->krylov_maxit + chunk) break;
   }
+  prof_end(m, kev);
   if (w->nc)
     k_con_multiplier<KT><<<(w->nc + 255) / 256, 256, 0, m->stream>>>(w->nc, w->con_dof, w->con_sys, w->sel,
                                                                      w->rowptr, w->colind, K, w->dX, w->frhs,

@@ -142,7 +142,8 @@ class ua_newton_report(C.Structure):
                 ("updates", C.POINTER(C.c_double)), ("update_stride", C.c_int64),
                 ("active_set_iterations", C.c_int32), ("active_set_cyclical", C.c_int32),
                 ("active_set_converged", C.c_int32), ("n_hpos", C.c_int32), ("hpos_capacity", C.c_int32),
-                ("hpos_node", _ip)]
+                ("hpos_node", _ip), ("ksetup_ms", C.c_double), ("kkrylov_ms", C.c_double),
+                ("ksetup_n", C.c_int32), ("kkrylov_n", C.c_int32)]
 
 
 UA_TUNE_MAX = 48

@@ -437,7 +437,8 @@ def _report(rep, recs, updates=None):
                         gamma=it.gamma, r0=it.r0, r=it.r, rForce=it.rForce, rWork=it.rWork))
     kern = dict(asmK_ms=rep.kasmK_ms, asmK_n=rep.kasmK_n, asmR_ms=rep.kasmR_ms, asmR_n=rep.kasmR_n,
                 spmv_ms=rep.kspmv_ms, spmv_n=rep.kspmv_n, amgR_ms=rep.kamgR_ms, amgR_n=rep.kamgR_n,
-                amgP_ms=rep.kamgP_ms, amgP_n=rep.kamgP_n,
+                amgP_ms=rep.kamgP_ms, amgP_n=rep.kamgP_n, setup_ms=rep.ksetup_ms, setup_n=rep.ksetup_n,
+                krylov_ms=rep.kkrylov_ms, krylov_n=rep.kkrylov_n,
                 work_nnz=dict(zip(("asmK", "asmR", "spmv", "amgR", "amgP"), list(rep.kwork_nnz))),
                 work_rows=dict(zip(("asmK", "asmR", "spmv", "amgR", "amgP"), list(rep.kwork_rows))))
     return RunInfo(bool(rep.converged), rep.iterations, rep.backtrack_steps, rep.krylov_its_total,
