@@ -955,12 +955,14 @@ __global__ void __launch_bounds__(256) k_csell_fill(SellDev S, const int* rowptr
 //   MODE 2 (AMG smoothing): out = mask(x + invd (b - K x)), pcopy = out; partial b.out
 // The partials go per slice: part[slice block * kSellSlices + warp].  List-driven when act.cnt is
 // set (the CTAs loop over the active slice blocks), else one slice block per CTA.
-// The slot loop is unrolled six deep, so a thread has six column loads and their gathers in
-// flight (measured on B200 against three deep at 40 registers and six CTAs per SM: SpMV 3.41 ->
-// 3.77 TB/s, smoothing 2.88 -> 3.11 TB/s).  FP32 vectors: at most 48 registers, five CTAs (40
-// warps) per SM; FP64 vectors: the compiler's choice.
+// The slot loop is unrolled eight deep (a P1 slice's width in one pass), so a thread has eight
+// column loads and their gathers in flight.  FP32 vectors: the SpMV (FP32 values) at most 64
+// registers, four CTAs per SM; the BF16 passes at most 48, five CTAs per SM; FP64 vectors: the
+// compiler's choice.  Measured on B200 (256-mesh batch, algorithmic bytes): three deep at 40
+// registers, SpMV 3.41 and smoothing 2.88 TB/s; eight deep, SpMV 4.10 at four CTAs per SM and
+// the BF16 passes 3.56 at five.
 template <typename KT, typename VT, int MODE>
-__global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 5 : 0) k_sell(SellDev S, int nsb, ActList act, const int* sel, const int* done,
+__global__ void __launch_bounds__(256, sizeof(VT) == 4 ? (MODE == 0 ? 4 : 5) : 0) k_sell(SellDev S, int nsb, ActList act, const int* sel, const int* done,
                                               const int* depth, const KT* vals, const VT* x, const VT* b,
                                               const VT* invd, const unsigned char* cmask, VT* out, VT* pcopy,
                                               double* part) {
@@ -989,7 +991,7 @@ __global__ void __launch_bounds__(256, sizeof(VT) == 4 ? 5 : 0) k_sell(SellDev S
       const int* cp = S.cols + o0 + t;
       const KT* vp = vals + 4 * (o0 + t);
       double au = 0, av = 0;
-#pragma unroll 6
+#pragma unroll 8
       for (int k = 0; k < W; ++k) {
         int j = __ldg(cp + 32 * k);
         bool okj = true;
