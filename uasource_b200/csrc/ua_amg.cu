@@ -1081,13 +1081,17 @@ __global__ void k_sa_P(int nf, const int* dof_sys, const int* dof_off, const int
   const int k0 = sa_find(pn_col + pr, dP, agg[g]);
   if (k0 >= 0) row[c * dP + k0] = 1;
   const ST f = (ST)(kSaOmega * (double)invd[i]);
-  for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
-    const int j = colind[q];
-    if (mask && mask[j]) continue;
-    int s2, c2, h;
-    sa_decode(j, dof_sys, dof_off, node_off, s2, c2, h);
-    const int k = sa_find(pn_col + pr, dP, agg[h]);
-    if (k >= 0) row[c2 * dP + k] -= f * (ST)A[q];
+  // the row holds the u block then the v block of the node's deg neighbours (the same nodes in
+  // the same order), so one search per neighbour serves both blocks; each target still sums its
+  // block's entries in row order
+  const int q0 = rowptr[i], deg = (rowptr[i + 1] - q0) >> 1;
+  const int d0 = dof_off[s], no = node_off[s], nn = node_off[s + 1] - no;
+  for (int k = 0; k < deg; ++k) {
+    const int ju = colind[q0 + k];
+    const int kk = sa_find(pn_col + pr, dP, agg[no + (ju - d0)]);
+    if (kk < 0) continue;
+    if (!(mask && mask[ju])) row[kk] -= f * (ST)A[q0 + k];
+    if (!(mask && mask[ju + nn])) row[dP + kk] -= f * (ST)A[q0 + deg + k];
   }
 }
 
@@ -1262,15 +1266,16 @@ __global__ void k_sa_quads(int nfn, const int* node_sys, const int* pn_ptr, cons
     pq_set(Q + pr + k, (double)p0[k], (double)p0[dP + k], (double)p0[prs + k], (double)p0[prs + dP + k]);
 }
 
-// the same quads in ptn order (coarse node J, its fine nodes u): thread per coarse node; every
-// P entry is the image of exactly one ptn entry
+// the same quads in ptn order (coarse node J, its fine nodes u): thread per ptn entry (its
+// system is its fine node's); every P entry is the image of exactly one ptn entry
 template <typename QT>
-__global__ void k_sa_qt(int ncn, const int* cnode_sys, const int* ptn_ptr, const int* ptn_fine, const int* ptn_k,
+__global__ void k_sa_qt(long long np, const int* fnode_sys, const int* ptn_fine, const int* ptn_k,
                         const int* pn_ptr, const QT* Q, QT* QTr, const int* sel) {
-  const int J = blockIdx.x * blockDim.x + threadIdx.x;
-  if (J >= ncn) return;
-  if (sel && !sel[cnode_sys[J]]) return;
-  for (int u = ptn_ptr[J]; u < ptn_ptr[J + 1]; ++u) QTr[u] = Q[pn_ptr[ptn_fine[u]] + ptn_k[u]];
+  const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (u >= np) return;
+  const int g = ptn_fine[u];
+  if (sel && !sel[fnode_sys[g]]) return;
+  QTr[u] = Q[pn_ptr[g] + ptn_k[u]];
 }
 
 // coarse operator rows: Ac((c2,J),:) = sum over P'((c2,J), (c,g)) AP((c,g),:), into the coarse
@@ -1551,8 +1556,8 @@ static int numeric_t(ua_mesh* m, const int* rowptr0, const int* colind0, const K
                                               F.poff, Pv, psel), ++*launches;
       k_sa_quads<ST, QT><<<(F.nn + 127) / 128, 128, 0, st>>>(F.nn, F.node_sys, F.pn_ptr, F.pbase, F.pnnz, F.poff,
                                                             Pv, Qv, psel), ++*launches;
-      k_sa_qt<QT><<<(C.nn + 127) / 128, 128, 0, st>>>(C.nn, C.node_sys, F.ptn_ptr, F.ptn_fine, F.ptn_k, F.pn_ptr,
-                                                      Qv, QTv, psel), ++*launches;
+      k_sa_qt<QT><<<(int)((F.np + 255) / 256), 256, 0, st>>>(F.np, F.node_sys, F.ptn_fine, F.ptn_k, F.pn_ptr, Qv,
+                                                               QTv, psel), ++*launches;
       const int ms = F.ap_maxrow <= kSaApSm ? F.ap_maxrow : 0;  // rows summed in shared memory
       k_sa_AP<KT, ST><<<(int)(((long long)F.nn * kSaGL + 127) / 128), 128, sa_ap_smem<ST>(ms), st>>>(
           F.nn, F.node_sys, F.d_dof_off, F.d_node_off, rp, ci, A, mk, F.pn_ptr, F.pn_col, Qv, F.apn_ptr, F.apn_col,
