@@ -2284,6 +2284,18 @@ __global__ void k_gm_reduce(const int* sys_rb_off, int nrb, const int* sel, cons
   if (threadIdx.x == 0) out[(size_t)s * ld + i] = o[0];
 }
 
+// out = w / sqrt(nrm[s*ld]) per system (0 where the norm is 0)
+__global__ void __launch_bounds__(256) k_gm_scale_norm(const int* rb_start, const int* rb_sys, const int* sel,
+                                                       const int* done, const double* w, double* out,
+                                                       const double* nrm, int ld) {
+  const int blk = blockIdx.x;
+  const int s = rb_sys[blk];
+  if (!sel[s] || done[s]) return;
+  const double hn = sqrt(fmax(nrm[(size_t)s * ld], 0.0));
+  const double sc = hn > 0 ? 1.0 / hn : 0.0;
+  for (int i = rb_start[blk] + threadIdx.x; i < rb_start[blk + 1]; i += blockDim.x) out[i] = w[i] * sc;
+}
+
 // w -= sum_i coef[s*ld + i] V_i (i < nv)
 __global__ void __launch_bounds__(256) k_gm_orth(const int* rb_start, const int* rb_sys, const int* sel,
                                                  const int* done, double* w, const double* V, size_t ldv, int nv,
@@ -2446,7 +2458,7 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
     w->gm_z = walloc<double>(m, ldv);
     w->gm_u = walloc<double>(m, ldv);
     w->gm_part = walloc<double>(m, (size_t)(mr + 1) * w->nrb);
-    w->gm_coef = walloc<double>(m, (size_t)nsys * ld);
+    w->gm_coef = walloc<double>(m, (size_t)3 * nsys * ld);  // two orthogonalisation passes and the norm
     w->gm_scal = walloc<double>(m, (size_t)nsys * ld);
     w->gm_act = walloc<int>(m, nsys);
     w->gm_ny = walloc<int>(m, nsys);
@@ -2514,8 +2526,14 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
   };
   // host-side reduction results
   std::vector<double> hco((size_t)nsys * ld), hco2((size_t)nsys * ld), hnrm((size_t)nsys * ld), hsc(nsys),
-      hy((size_t)nsys * ld);
+      hy((size_t)nsys * ld), hco3((size_t)3 * nsys * ld);
+  bool flags_changed = false;
   std::vector<int> hact(nsys), hny(nsys), hdone(nsys);
+  // per-system sums of nv partial arrays into coef (device), without a host copy
+  auto reduce_dev = [&](const double* part, int nv, double* coef) {
+    k_gm_reduce<<<dim3(nsys, nv), kRedThreads, 0, st>>>(w->sys_rb_off, w->nrb, w->sel, w->done, part, coef, ld),
+        ++g_launches;
+  };
   auto reduce_to_host = [&](const double* part, int nv, std::vector<double>& dst) -> int {
     k_gm_reduce<<<dim3(nsys, nv), kRedThreads, 0, st>>>(w->sys_rb_off, w->nrb, w->sel, w->done, part, w->gm_coef,
                                                         ld), ++g_launches;
@@ -2591,16 +2609,31 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
       project(zv);
       spmv(zv, wv);
       project(wv);
+      // classical Gram-Schmidt twice, then the norm and the next basis vector w / |w|, all on the
+      // device (coefficients in gm_coef: pass 1, pass 2, norm); one host copy per Arnoldi step
+      // for the Hessenberg column, the rotations and the convergence test
+      double* const cf[3] = {w->gm_coef, w->gm_coef + (size_t)nsys * ld, w->gm_coef + (size_t)2 * nsys * ld};
       for (int pass = 0; pass < 2; ++pass) {
         k_gm_dots<<<dim3(w->nrb, j + 1), 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, wv, V, ldv,
                                                        w->gm_part), ++g_launches;
-        if ((rc = reduce_to_host(w->gm_part, j + 1, pass ? hco2 : hco))) return rc;
-        k_gm_orth<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, wv, V, ldv, j + 1, w->gm_coef,
+        reduce_dev(w->gm_part, j + 1, cf[pass]);
+        k_gm_orth<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, wv, V, ldv, j + 1, cf[pass],
                                           ld), ++g_launches;
       }
       k_gm_dots<<<dim3(w->nrb, 1), 256, 0, st>>>(w->rb_start, w->rb_sys, w->nrb, w->sel, w->done, wv, wv, 0,
                                                  w->gm_part), ++g_launches;
-      if ((rc = reduce_to_host(w->gm_part, 1, hnrm))) return rc;
+      reduce_dev(w->gm_part, 1, cf[2]);
+      // V_{j+1} = w / |w| for every system still in the cycle (a system whose cycle ends here
+      // never reads it)
+      if (j + 1 < mr)
+        k_gm_scale_norm<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, wv,
+                                                V + (size_t)(j + 1) * ldv, cf[2], ld), ++g_launches;
+      UA_CUDA_TRY(cudaMemcpyAsync(hco3.data(), w->gm_coef, sizeof(double) * 3 * nsys * ld, cudaMemcpyDeviceToHost,
+                                  st));
+      UA_CUDA_TRY(cudaStreamSynchronize(st));
+      std::copy(hco3.begin(), hco3.begin() + (size_t)nsys * ld, hco.begin());
+      std::copy(hco3.begin() + (size_t)nsys * ld, hco3.begin() + (size_t)2 * nsys * ld, hco2.begin());
+      std::copy(hco3.begin() + (size_t)2 * nsys * ld, hco3.end(), hnrm.begin());
       bool more = false;
       for (int s = 0; s < nsys; ++s) {
         GmSys& G = S[s];
@@ -2626,16 +2659,16 @@ static int gmres_t(ua_mesh* m, const ua_params* p, const KT* K, int* its_out, co
         const double res = std::fabs(G.g[j + 1]);
         if (res <= G.tol * G.beta0 || hn == 0.0 || !(res == res) || G.its >= p->krylov_maxit || j + 1 == mr) {
           G.cycle_done = true;
+          flags_changed = true;
         } else {
           more = true;
-          hsc[s] = 1.0 / hn;
         }
       }
       if (!more) break;
-      if ((rc = upload_flags())) return rc;
-      UA_CUDA_TRY(cudaMemcpyAsync(w->gm_scal, hsc.data(), sizeof(double) * nsys, cudaMemcpyHostToDevice, st));
-      k_gm_scale<<<w->nrb, 256, 0, st>>>(w->rb_start, w->rb_sys, w->sel, w->done, wv, V + (size_t)(j + 1) * ldv,
-                                         w->gm_scal), ++g_launches;
+      if (flags_changed) {
+        if ((rc = upload_flags())) return rc;
+        flags_changed = false;
+      }
     }
     // x += M^-1 (V y), y from the triangular system of each active system
     for (int s = 0; s < nsys; ++s) {
