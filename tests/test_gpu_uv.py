@@ -337,6 +337,11 @@ def test_graph_replay_equals_direct_launches(precision, rtol):
         Fo, _, _, _, info = ua.uv(ctrl, mua, ua.BCs.from_problem(P), ua.Fields.from_problem(P))
         assert info.converged
         out.append(np.concatenate([Fo.ub, Fo.vb]))
+        if prof:  # phase timings: the set-ups and the Krylov ranges, which hold the SpMVs
+            k = info.kernels
+            assert k["setup_n"] >= info.iterations and k["setup_ms"] > 0
+            assert k["krylov_n"] >= info.iterations and k["krylov_ms"] >= k["spmv_ms"] > 0
+            assert k["krylov_ms"] + k["setup_ms"] < info.device_ms
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
