@@ -511,6 +511,9 @@ def run_ours(args):
             "kernel_share_of_timed_classes": {c: v[0] / max(total_k, 1e-12) for c, v in cand.items()},
             "fp64_assembly": fp64, "fp64_peak_source": "148 SMs x 64 DFMA/clock x 2 flops x max SM clock, of nominal",
             "classes_gbs": {c: (v[2] / (v[0] / 1000) / 1e9 if v[0] > 0 else None) for c, v in cand.items()},
+            # the same per class as a fraction of the measured HBM copy bandwidth
+            "classes_frac": {c: (v[2] / (v[0] / 1000) / 1e9 / hbm_peak if v[0] > 0 else None)
+                             for c, v in cand.items()},
             # device time of the timed classes over the profiled solve's whole device time (the rest:
             # coarse AMG levels, smoothed transfers, AMG set-up, vector updates and reductions)
             "timed_classes_share_of_device_time": total_k / max(float(prof_info.device_ms), 1e-12),
